@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Throughput of the D3Q27 thermal LBM time step on B200 (MLUPS and HBM GB/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One "step" is one full lattice time step of the workload (collide, stream, boundary,
+moments over every fluid cell).  Workload: config 1 -- the single-component thermal
+D3Q27 Taylor-Green vortex, 64^3 interior cells, FP64, Ma 0.1, Re 400 (seeded synthetic
+state, numpy PCG64 seed 20261203).  The state is larger than L2 (the two population
+buffers alone are 2 x 54 x 66^3 x 8 B = 248 MB), so no L2 flush is needed between steps.
+
+* value: MLUPS of K steps with the state resident in HBM, device-timed with CUDA events
+  on the library's stream; max over ranks.
+* e2e: the same steps through the reference-facing phase calls of the C ABI
+  (collide/streaming/tms_bc/calculate_moment), with the AoS state uploaded from pinned
+  host memory at the start, and the whole AoS state plus the status word read back every
+  10 steps (the output cadence of the reference's Taylor-Green setup, setup.cpp:146);
+  host wall clock.
+* roofline: the dominant kernel's algorithmic bytes per launch / its mean launch time.
+* cpu_baseline: the reference's own solver (oracle/_ref) on the host cores, bounded sample.
+
+Under torchrun (N > 1) every rank runs an independent replica of the workload on its own
+GPU (the path is not domain-decomposed yet): weak scaling, value = all ranks' cells.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "lattice-boltzmann-method_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "MLUPS (D3Q27 thermal LBM step, 1 B200)"
+# algorithmic bytes per cell and launch (one read + one write of every population, plus
+# the moment record the stream kernel must store)
+BYTES_COLLIDE_FP64 = 2 * 54 * 8          # 864
+BYTES_STREAM_FP64 = 54 * 8 + 6 * 8       # 480
+BYTES_STEP_FP64 = 2 * 54 * 8             # 864: one read + one write of the populations
+OUTPUT_EVERY = 10
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=64, help="interior cells per axis")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def workload(N):
+    import workloads
+    cells, prm = workloads.tgv_sc(N)
+    return cells, prm
+
+
+def fluid_cells(cells):
+    return int((cells["type"] == 0).sum())
+
+
+def cpu_reference_run(cells, prm, steps, warmup, threads):
+    """Times the reference's own solver (oracle/_ref) -- or, where it was not built, the C
+    oracle port -- for `steps` steps after `warmup`; returns (seconds, kind)."""
+    from oracle import refsc, sc
+    N3 = [s - 2 for s in cells.shape]
+    if refsc.available():
+        refsc.set_threads(threads)
+        ref = refsc.RefSC(*N3, prm["nu"], prm["R"], prm["gamma"], prm["prtl"], cells.dtype)
+        ref.cells[...] = cells
+        ref.init()
+        if warmup:
+            ref.loop(warmup)
+        t0 = time.perf_counter()
+        ref.loop(steps)
+        dt = time.perf_counter() - t0
+        ref.close()
+        return dt, "reference"
+    sc.set_threads(threads)
+    a = cells.copy()
+    o = sc.OracleSC(a, prm["nu"], prm["R"], prm["gamma"], prm["prtl"])
+    o.init()
+    if warmup:
+        o.loop(warmup)
+    t0 = time.perf_counter()
+    o.loop(steps)
+    return time.perf_counter() - t0, "port"
+
+
+def cpu_baseline(cells, prm, target_s=10.0):
+    threads = os.cpu_count() or 1
+    t1, kind = cpu_reference_run(cells, prm, 1, 1, threads)
+    n = max(2, min(200, int(target_s / max(t1, 1e-3))))
+    dt, kind = cpu_reference_run(cells, prm, n, 0, threads)
+    ncell = fluid_cells(cells)
+    return {"value": ncell * n / dt / 1e6, "unit": "MLUPS", "cores": threads, "kind": kind,
+            "sample": f"{n} steps of the same 64^3 state after Init + 1 warm-up step, "
+                      f"{threads} OpenMP threads, {dt:.1f} s"}
+
+
+# ---------------------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------------------
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    cells, prm = workload(args.N)
+    threads = os.cpu_count() or 1
+    dt, kind = cpu_reference_run(cells, prm, args.steps, args.warmup, threads)
+    ncell = fluid_cells(cells)
+    v = ncell * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Taylor-Green vortex)",
+        "config": {"workload": f"tgv{args.N}_sc_fp64", "cells": ncell, "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} steps after {args.warmup} warm-up steps"},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, dist):
+    import numpy as np
+
+    import lbmgpu
+    device = dist.local
+    cells, prm = workload(args.N)
+    Nx, Ny, Nz = cells.shape
+    ncell = fluid_cells(cells)
+    lat = lbmgpu.Lattice(Nx, Ny, Nz, prm["nu"], prm["R"], prm["gamma"], prm["prtl"], device=device)
+    lat.upload(cells)
+    lat.init()
+    lat.time_steps(max(3, args.warmup))
+
+    # ---- device-timed resident run
+    dist.barrier()
+    clk = Clocks(device)
+    clk.start()
+    ms = lat.time_steps(args.steps)
+    clocks = clk.stop()
+    status = lat.synchronize()
+    ms = dist.max(ms)
+
+    # ---- per-kernel times (separate short run with per-launch events)
+    kk = min(args.steps, 200)
+    lat.profile(True)
+    lat.time_steps(kk)
+    launches, kms = lat.kernel_times()
+    lat.profile(False)
+    per_step_launches = (launches[0] + launches[1] + launches[2]) / kk
+    avg = {"k_sc_collide": kms[0] / max(launches[0], 1), "k_sc_stream_moment": kms[1] / max(launches[1], 1)}
+    dom = max(avg, key=avg.get)
+    alg = (BYTES_COLLIDE_FP64 if dom == "k_sc_collide" else BYTES_STREAM_FP64) * ncell
+    peak, peak_kind = peaks()
+    achieved = alg / (avg[dom] * 1e-3) / 1e9
+    lat.close()
+
+    # ---- end to end through the reference-facing phase calls, host buffers
+    e2e = None
+    try:
+        import torch
+        pinned = torch.empty(cells.nbytes, dtype=torch.uint8, pin_memory=True)
+        host = np.frombuffer(pinned.numpy(), dtype=cells.dtype).reshape(cells.shape)
+    except Exception:
+        host = np.empty_like(cells)
+    host[...] = cells
+    lat = lbmgpu.Lattice(Nx, Ny, Nz, prm["nu"], prm["R"], prm["gamma"], prm["prtl"], device=device)
+    lat.upload(host)
+    lat.init()
+    for _ in range(max(3, args.warmup)):
+        lat.collide(); lat.streaming(); lat.tms_bc(); lat.calculate_moment()
+    lat.synchronize()
+    host[...] = cells
+    dist.barrier()
+    t0 = time.perf_counter()
+    lat.upload(host)
+    lat.init()
+    nread = 0
+    for s in range(1, args.steps + 1):
+        lat.collide()
+        lat.streaming()
+        lat.tms_bc()
+        lat.calculate_moment()
+        if s % OUTPUT_EVERY == 0:
+            lat.status()
+            lat.download(host)
+            nread += 1
+    lat.synchronize()
+    wall = dist.max(time.perf_counter() - t0)
+    lat.close()
+    e2e = {"value": dist.world * ncell * args.steps / wall / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": cells.nbytes / args.steps,
+           "d2h_bytes_per_step": (cells.nbytes + 4) * nread / args.steps,
+           "note": f"upload of the AoS state once, phase calls per step, AoS download + status every {OUTPUT_EVERY} steps"}
+
+    if dist.rank != 0:
+        return
+    value = dist.world * ncell * args.steps / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Taylor-Green vortex, numpy PCG64 seed 20261203)",
+        "config": {"workload": f"tgv{args.N}_sc_fp64: single-component thermal D3Q27, {args.N}^3 periodic, "
+                               f"Ma 0.1, Re 400, FP64 (config 1)",
+                   "cells": ncell, "parallelism": f"replicas{dist.world}",
+                   "l2": "state larger than L2 (248 MB of populations), no flush"},
+        "hbm_gbs_step": ncell * BYTES_STEP_FP64 / (ms / args.steps * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": ncu_traffic(dom),
+                     "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_launch": alg,
+                     "mean_launch_ms": avg[dom], "kernel_ms": avg},
+        "gpu_launches": int(round(per_step_launches * args.steps)),
+        "status": status,
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    if dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(cells, prm)
+        except Exception as exc:  # the baseline never decides the GPU number
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

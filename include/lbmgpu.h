@@ -1,0 +1,130 @@
+/* lbmgpu -- B200 (sm_100a) implementation of the per-timestep hot path of the
+ * compressible thermal D3Q27 lattice-Boltzmann solver farrasarira/Lattice-Boltzmann-Method.
+ *
+ * C ABI: plain pointers and sizes, no C++ or CUDA types.  One handle owns the device
+ * state of one LBM object on one GPU and one CUDA stream.  Every call returns an int:
+ *   0                 success
+ *   negative          API misuse (LBMGPU_E_*), nothing was launched
+ *   positive          device status bits (LBMGPU_ST_*) raised by the kernels
+ * Nothing throws across the ABI.  A handle is not thread-safe.
+ *
+ * How the reference's driver reaches it: the LBM member functions that make up one time
+ * step (src/headers/lbm.hpp:152-197, called in src/lbm-main.cpp:149-196) keep their
+ * signatures and forward here.  The C++ mirror in
+ * lattice-boltzmann-method_b200/host/lbm_gpu.hpp does exactly that.
+ */
+#ifndef LBMGPU_H
+#define LBMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBMGPU_ABI_VERSION 1
+
+/* ---- error codes ------------------------------------------------------------- */
+#define LBMGPU_OK 0
+#define LBMGPU_E_ARG (-1)        /* bad argument or descriptor                       */
+#define LBMGPU_E_CUDA (-2)       /* a CUDA runtime call failed                        */
+#define LBMGPU_E_NODEV (-3)      /* no usable CUDA device / kernel image              */
+#define LBMGPU_E_PHASE (-4)      /* phase calls out of the reference's step order     */
+#define LBMGPU_E_STATE (-5)      /* no state uploaded / initialised yet               */
+#define LBMGPU_E_UNSUPPORTED (-6) /* configuration not implemented                   */
+#define LBMGPU_E_VERSION (-7)    /* descriptor abi_version mismatch                   */
+
+/* ---- device status bits (sticky until lbmgpu_status(..., clear=1)) ------------ */
+#define LBMGPU_ST_NAN 0x1u          /* non-finite density, velocity or temperature     */
+#define LBMGPU_ST_NEG_STATE 0x2u    /* density or temperature <= 0                     */
+#define LBMGPU_ST_TAU_UNSTABLE 0x4u /* 1/omega <= 1/2 (the reference prints these:
+                                       src/lbm-collision.cpp:33-34)                   */
+
+/* ---- precision of the population storage ------------------------------------- */
+#define LBMGPU_FP64 0
+#define LBMGPU_FP32 1
+
+/* Byte offsets of the fields of the caller's MIXTURE record (src/headers/lbm.hpp:56-88).
+ * Fill with sizeof/offsetof from the caller's own class; -1 marks a field the
+ * configuration does not have (f/fpc are absent when MULTICOMP is on). */
+typedef struct lbmgpu_mixture_layout {
+    size_t size;
+    long type, f, fpc, p_tensor, rho, u, v, w, p, g, gpc, rhoe, energy_flux, temp, HRR;
+} lbmgpu_mixture_layout;
+
+typedef struct lbmgpu_desc {
+    int abi_version;      /* LBMGPU_ABI_VERSION                                           */
+    int device;           /* CUDA device ordinal                                          */
+    int Nx, Ny, Nz;       /* lattice INCLUDING the ghost layer (LBM::Nx, lbm-main.cpp:19-21) */
+    int n_species;        /* 0: single component (MULTICOMP off)                          */
+    int precision;        /* LBMGPU_FP64 or LBMGPU_FP32                                   */
+    int dt_sim;           /* LBM::dt_sim (lbm.hpp:113), 1 in the reference                */
+    double nu;            /* single component: kinematic viscosity (lbm.hpp:117)          */
+    double gas_const;     /* gas constant R (lbm.hpp:118)                                 */
+    double gamma;         /* cp/cv (lbm.hpp:119)                                          */
+    double prtl;          /* Prandtl number (lbm.hpp:121)                                 */
+    lbmgpu_mixture_layout mix;
+} lbmgpu_desc;
+
+typedef struct lbmgpu lbmgpu_t;
+
+/* Creates the device state for one LBM object.  Replaces the allocation done by
+ * LBM::LBM(Nx,Ny,Nz,nu) (src/lbm-main.cpp:16-35). */
+int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out);
+int lbmgpu_destroy(lbmgpu_t *h);
+
+/* Copies the caller's AoS cell array (LBM::mixture_data, lbm.hpp:134; Nx*Ny*Nz records in
+ * the reference's [i][j][k] order, k fastest) to the device: cell types, populations and
+ * moments.  The next Collide uses the uploaded populations and moments as they stand,
+ * exactly as the reference's first step after Init or read_restart does. */
+int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos);
+
+/* Writes the current state back into the caller's AoS array at a step boundary:
+ * populations f, g (post-stream, post-boundary), fpc, gpc (post-collision) and the
+ * moments of every fluid cell; the stored moments (rho, u, v, w, p, temp) of every cell. */
+int lbmgpu_download(lbmgpu_t *h, void *mixture_aos);
+
+/* LBM::Init (src/lbm-init.cpp:8-82) on the uploaded setup fields. */
+int lbmgpu_init(lbmgpu_t *h);
+
+/* The reference's per-step phases, called in its order (src/lbm-main.cpp:157-181).
+ * Collide launches the collision kernel; Streaming and TMS_BC record the phase;
+ * calculate_moment launches the fused streaming + boundary + moment kernel.  Calls out
+ * of order return LBMGPU_E_PHASE. */
+int lbmgpu_collide_species(lbmgpu_t *h);  /* LBM::Collide_Species, lbm-collision.cpp:334 */
+int lbmgpu_collide(lbmgpu_t *h);          /* LBM::Collide, lbm-collision.cpp:9 / :191    */
+int lbmgpu_streaming(lbmgpu_t *h);        /* LBM::Streaming, lbm-streaming.cpp:3         */
+int lbmgpu_tms_bc(lbmgpu_t *h);           /* LBM::TMS_BC, lbm-bc.cpp:122                 */
+int lbmgpu_calculate_moment(lbmgpu_t *h); /* LBM::calculate_moment, lbm-moment.cpp:11    */
+
+/* nsteps complete time steps (the body of LBM::loop, lbm-main.cpp:153-194, without the
+ * output cadence).  Asynchronous on the handle's stream. */
+int lbmgpu_step(lbmgpu_t *h, int nsteps);
+
+/* lbmgpu_step bracketed by CUDA events on the handle's stream: *ms receives the device
+ * time of the nsteps steps (the call waits for them to finish). */
+int lbmgpu_time_steps(lbmgpu_t *h, int nsteps, double *ms);
+
+/* Waits for the handle's stream.  Returns the device status bits as a positive value. */
+int lbmgpu_synchronize(lbmgpu_t *h);
+
+/* Reads (and optionally clears) the sticky device status bits. */
+int lbmgpu_status(lbmgpu_t *h, uint32_t *flags, int clear);
+
+/* Per-kernel device timing.  When enabled, every launch is bracketed by CUDA events on
+ * the handle's stream; lbmgpu_kernel_times returns, per kernel kind, the number of
+ * launches and the summed device milliseconds since the last reset.
+ * Kinds: 0 collide, 1 stream+boundary+moment, 2 other. */
+int lbmgpu_profile(lbmgpu_t *h, int enable);
+int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
+
+/* Bytes of device memory held by the handle. */
+int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes);
+
+const char *lbmgpu_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBMGPU_H */

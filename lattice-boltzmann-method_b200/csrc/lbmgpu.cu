@@ -1,0 +1,938 @@
+// lbmgpu: B200 (sm_100a) device implementation of the D3Q27 thermal LBM time step and
+// the C ABI declared in include/lbmgpu.h.
+//
+// Reference path replaced (farrasarira/Lattice-Boltzmann-Method, single component):
+//   LBM::Collide            src/lbm-collision.cpp:9-99     -> k_sc_collide
+//   LBM::Streaming          src/lbm-streaming.cpp:3-119    -> k_sc_stream_moment (pull)
+//   LBM::TMS_BC             src/lbm-bc.cpp:341-460, 809-938, 1111-1229 -> k_sc_stream_moment
+//   LBM::calculate_moment   src/lbm-moment.cpp:11-125      -> k_sc_stream_moment
+//   LBM::Init               src/lbm-init.cpp:8-82          -> k_sc_init
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/lbmgpu.h"
+#include "sc_kernels.cuh"
+
+using namespace lbm;
+
+namespace {
+
+constexpr int kBlock = 128;
+
+// ----------------------------------------------------------------------------------
+// Collision (reference LBM::Collide, single component, src/lbm-collision.cpp:9-99)
+// ----------------------------------------------------------------------------------
+__device__ __forceinline__ double qdev_at(const double *__restrict__ mom, long nc, long n, int a, double R) {
+    const double rho = mom[M_RHO * nc + n];
+    const double ua = mom[(M_U + a) * nc + n];
+    const double T = mom[M_T * nc + n];
+    return rho * ua * (1.0 - 3.0 * R * T) - rho * (ua * ua * ua);
+}
+
+__device__ __forceinline__ bool wall_like(int t) {
+    return t == T_S || t == T_A || t == T_FS || t == T_P || t == T_O || t == T_O_C;
+}
+
+// fd_central (reference src/headers/FD.hpp:108-127) with dx = 1.
+__device__ __forceinline__ double fd_central(double sl, double sc, double sr, int tl, int tr) {
+    if (wall_like(tl)) return (tr == T_P) ? 0.0 : (sr - sc);
+    if (wall_like(tr)) return (tl == T_P) ? 0.0 : (sc - sl);
+    return (sr - sl) / 2.0;
+}
+
+template <bool LOCAL>
+__global__ void __launch_bounds__(kBlock) k_sc_collide(ScGeom g, ScPhys P, const int8_t *__restrict__ type,
+                                                       const uint8_t *__restrict__ cflag, const int *__restrict__ bid,
+                                                       const double *__restrict__ src, double *__restrict__ dst,
+                                                       const double *__restrict__ mom, const double *__restrict__ minit,
+                                                       const double *__restrict__ bst, long nb, unsigned *status) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.ncell) return;
+    const uint8_t cf = cflag[n];
+    if (!(cf & CF_FLUID)) return;
+    const long nc = g.ncell;
+    double f[27], ge[27];
+    if (LOCAL) {
+#pragma unroll
+        for (int l = 0; l < 27; ++l) {
+            f[l] = src[(long)l * nc + n];
+            ge[l] = src[(long)(27 + l) * nc + n];
+        }
+    } else if (cf & CF_BOUND) {
+        const long b = bid[n];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) {
+            f[l] = bst[(long)l * nb + b];
+            ge[l] = bst[(long)(27 + l) * nb + b];
+        }
+    } else {
+        pull_cell(g, type, cf, n, src, (const double *)nullptr, 0, f, ge);
+    }
+
+    const double rho = mom[M_RHO * nc + n];
+    const double vel[3] = {mom[M_U * nc + n], mom[M_V * nc + n], mom[M_W * nc + n]};
+    const double T = mom[M_T * nc + n];
+    const double p = mom[M_P * nc + n];
+    double Pt[6], rhoe;
+    if (LOCAL) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) Pt[a] = minit[(long)a * nc + n];
+        rhoe = minit[6 * nc + n];
+    } else {
+        ScSums s;
+        sums_sc(f, ge, s);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) Pt[a] = s.P[a];
+        rhoe = s.re;
+    }
+
+    const double dt = P.dt;
+    const double theta = P.R * T;
+    const double mu = P.nu * rho;
+    const double kappa = mu * P.cp / P.prtl;
+    const double om1 = 2 * p * P.cp * dt / (p * P.cp * dt + 2 * kappa);
+    const double om = 2 * p * dt / (p * dt + 2 * mu);
+    if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) raise_status(status, LBMGPU_ST_TAU_UNSTABLE);
+    const double Uint = rhoe / rho - 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+
+    // face-neighbour difference of rho u_a (1 - 3 R T) - rho u_a^3 (src/lbm-collision.cpp:64-67)
+    double dQ[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const long off = a == 0 ? g.si : (a == 1 ? g.sj : 1);
+        const long nlo = n - off, nhi = n + off;
+        dQ[a] = fd_central(qdev_at(mom, nc, nlo, a, P.R), qdev_at(mom, nc, n, a, P.R), qdev_at(mom, nc, nhi, a, P.R),
+                           type[nlo], type[nhi]);
+    }
+    // deviation of the pressure tensor from equilibrium, full symmetric index map
+    const double Pfull[3][3] = {{Pt[0], Pt[1], Pt[2]}, {Pt[1], Pt[3], Pt[4]}, {Pt[2], Pt[4], Pt[5]}};
+    double dq[3], corr[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        double s = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s += vel[a] * (Pfull[a][b] - ((a == b ? p : 0.0) + rho * vel[a] * vel[b]));
+        dq[b] = s + 0.5 * dt * vel[b] * dQ[b];
+        corr[b] = dt * (2 - om) / (2 * rho * om) * dQ[b];
+    }
+    AxisF<double> F;
+    axis_feq(F, vel, theta, corr);
+    AxisG<double> G;
+    axis_geq(G, Uint, theta, vel);
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        const double fe = feq_l(l, rho, F);
+        dst[(long)l * nc + n] = (1.0 - om) * f[l] + om * fe;
+        const double gq = geq_l(l, rho, G);
+        const double gs = (csq(l) == 1) ? gq + 0.5 * (cx(l) * dq[0] + cy(l) * dq[1] + cz(l) * dq[2]) : gq;
+        dst[(long)(27 + l) * nc + n] = ge[l] + om1 * (gq - ge[l]) + (om - om1) * (gq - gs);
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// Streaming + boundary treatment + moments (reference LBM::Streaming, LBM::TMS_BC and
+// LBM::calculate_moment fused; src/lbm-moment.cpp:11-125 for the moments).
+// ----------------------------------------------------------------------------------
+// Moments of the post-stream populations (reference LBM::calculate_moment,
+// src/lbm-moment.cpp:11-125) stored into the moment planes, with the state checks.
+__device__ __forceinline__ void store_moments_sc(const ScGeom &g, const ScPhys &P, long n, const double f[27],
+                                                 const double ge[27], double *__restrict__ mom_nxt,
+                                                 unsigned *status) {
+    const long nc = g.ncell;
+    ScSums s;
+    sums_sc(f, ge, s);
+    const double rho = s.rho;
+    const double u = s.j[0] / rho, v = s.j[1] / rho, w = s.j[2] / rho;
+    const double Uint = s.re / rho - 0.5 * (u * u + v * v + w * w);
+    const double T = Uint / P.cv;
+    const double p = rho * P.R * T;
+    mom_nxt[M_RHO * nc + n] = rho;
+    mom_nxt[M_U * nc + n] = u;
+    mom_nxt[M_V * nc + n] = v;
+    mom_nxt[M_W * nc + n] = w;
+    mom_nxt[M_T * nc + n] = T;
+    mom_nxt[M_P * nc + n] = p;
+    if (!isfinite(rho) || !isfinite(T) || !isfinite(u) || !isfinite(v) || !isfinite(w))
+        raise_status(status, LBMGPU_ST_NAN);
+    else if (!(rho > 0.0) || !(T > 0.0))
+        raise_status(status, LBMGPU_ST_NEG_STATE);
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_sc_stream_moment(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
+                       const int *__restrict__ bid, const double *__restrict__ src, const double *__restrict__ mom_cur,
+                       double *__restrict__ mom_nxt, const double *__restrict__ bst_cur, double *__restrict__ bst_nxt,
+                       long nb, unsigned *status) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.ncell) return;
+    const uint8_t cf = cflag[n];
+    if (!(cf & CF_FLUID)) return;
+    if (cf & CF_BOUND) return;  // boundary cells: k_sc_stream_moment_bound
+    double f[27], ge[27];
+    pull_cell(g, type, cf, n, src, (const double *)nullptr, 0, f, ge);
+    store_moments_sc(g, P, n, f, ge, mom_nxt, status);
+}
+
+// The same for the cells next to solid/inflow/outflow cells (compact list `blist`): pull
+// with the persisting populations, TMS boundary treatment, moments.
+__global__ void __launch_bounds__(kBlock)
+    k_sc_stream_moment_bound(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
+                             const long *__restrict__ blist, const double *__restrict__ src,
+                             const double *__restrict__ mom_cur, double *__restrict__ mom_nxt,
+                             const double *__restrict__ bst_cur, double *__restrict__ bst_nxt, long nb,
+                             unsigned *status) {
+    const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const long n = blist[b];
+    double f[27], ge[27];
+    pull_cell(g, type, cflag[n], n, src, bst_cur + b, nb, f, ge);
+    tms_cell_sc(g, P, type, mom_cur, n, f, ge);
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        bst_nxt[(long)l * nb + b] = f[l];
+        bst_nxt[(long)(27 + l) * nb + b] = ge[l];
+    }
+    store_moments_sc(g, P, n, f, ge, mom_nxt, status);
+}
+
+// ----------------------------------------------------------------------------------
+// Init (reference LBM::Init, single component, src/lbm-init.cpp:8-82)
+// ----------------------------------------------------------------------------------
+// Moment-form energy equilibrium (reference calculate_geq(l, rhoe, q, R, theta),
+// src/lbm-edf.cpp:100-138) for a diagonal R tensor R = r*I (all Init ever passes).
+__device__ __forceinline__ double geq_moment_diag(int l, double rhoe, const double q[3], double rdiag, double theta) {
+    const double c[3] = {(double)cx(l), (double)cy(l), (double)cz(l)};
+    double val = rhoe + (q[0] * c[0] + q[1] * c[1] + q[2] * c[2]) / theta;
+    double contr = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) contr += (rdiag - rhoe * theta) * (c[a] * c[a] - theta);
+    val += contr / (2.0 * theta * theta);
+    double wgt = 1.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) wgt *= (c[m] == 0.0) ? (1.0 - theta) : theta / 2.0;
+    val *= wgt;
+    const int c2 = csq(l);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const double Bm = (c2 == 0) ? 1.0 : (c2 == 1 ? -0.5 * fabs(c[m]) : 0.0);
+        val += Bm * ((1.0 - 3.0 * theta) / (2.0 * theta) * (rdiag - theta * rhoe));
+    }
+    return val;
+}
+
+__global__ void __launch_bounds__(kBlock)
+    k_sc_init(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
+              const int *__restrict__ bid, double *__restrict__ pop, double *__restrict__ mom0,
+              double *__restrict__ mom1, double *__restrict__ minit, double *__restrict__ bst, long nb) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= g.ncell) return;
+    const int t = type[n];
+    if (!(t == T_F || t == T_S || t == T_I || t == T_O || t == T_Q)) return;
+    const long nc = g.ncell;
+    const double p = mom0[M_P * nc + n];
+    const double T = mom0[M_T * nc + n];
+    const double rho = p / (P.R * T);
+    mom0[M_RHO * nc + n] = rho;
+    mom1[M_RHO * nc + n] = rho;
+    if (!(cflag[n] & CF_FLUID)) return;
+    const double theta = P.R * T;
+    const double rhoe = rho * (P.cv * T);
+    const double H = P.cp * T;
+    minit[0 * nc + n] = p;
+    minit[1 * nc + n] = 0.0;
+    minit[2 * nc + n] = 0.0;
+    minit[3 * nc + n] = p;
+    minit[4 * nc + n] = 0.0;
+    minit[5 * nc + n] = p;
+    minit[6 * nc + n] = rhoe;
+    const double q[3] = {H * rho * mom0[M_U * nc + n], H * rho * mom0[M_V * nc + n], H * rho * mom0[M_W * nc + n]};
+    const double vel0[3] = {0.0, 0.0, 0.0}, zero[3] = {0.0, 0.0, 0.0};
+    AxisF<double> F;
+    axis_feq(F, vel0, theta, zero);
+    const long b = (cflag[n] & CF_BOUND) ? bid[n] : -1;
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        const double fv = feq_l(l, rho, F);
+        const double gv = geq_moment_diag(l, rhoe, q, H * p, theta);
+        pop[(long)l * nc + n] = fv;
+        pop[(long)(27 + l) * nc + n] = gv;
+        if (b >= 0) {
+            bst[(long)l * nb + b] = fv;
+            bst[(long)(27 + l) * nb + b] = gv;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------------
+// AoS <-> SoA packing for upload/download (the caller's MIXTURE records)
+// ----------------------------------------------------------------------------------
+struct MixOff {
+    long size, type, f, fpc, p_tensor, rho, u, v, w, p, g, gpc, rhoe, energy_flux, temp;
+};
+
+__device__ __forceinline__ double ld(const char *rec, long off) { return *reinterpret_cast<const double *>(rec + off); }
+__device__ __forceinline__ void st(char *rec, long off, double v) { *reinterpret_cast<double *>(rec + off) = v; }
+
+__global__ void k_sc_unpack(ScGeom g, MixOff o, const char *__restrict__ stage, long n0, long n1,
+                            const uint8_t *__restrict__ cflag, const int *__restrict__ bid, double *__restrict__ pop,
+                            double *__restrict__ mom0, double *__restrict__ mom1, double *__restrict__ minit,
+                            double *__restrict__ bst, long nb) {
+    const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= n1) return;
+    const char *rec = stage + (n - n0) * o.size;
+    const long nc = g.ncell;
+    const long offs[M_N] = {o.rho, o.u, o.v, o.w, o.temp, o.p};
+#pragma unroll
+    for (int m = 0; m < M_N; ++m) {
+        const double v = ld(rec, offs[m]);
+        mom0[(long)m * nc + n] = v;
+        mom1[(long)m * nc + n] = v;
+    }
+    if (!(cflag[n] & CF_FLUID)) return;
+    const int pi[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+    for (int a = 0; a < 6; ++a) minit[(long)a * nc + n] = ld(rec, o.p_tensor + 8 * (3 * pi[a][0] + pi[a][1]));
+    minit[6 * nc + n] = ld(rec, o.rhoe);
+    const long b = (cflag[n] & CF_BOUND) ? bid[n] : -1;
+    for (int l = 0; l < 27; ++l) {
+        const double fv = ld(rec, o.f + 8 * l), gv = ld(rec, o.g + 8 * l);
+        pop[(long)l * nc + n] = fv;
+        pop[(long)(27 + l) * nc + n] = gv;
+        if (b >= 0) {
+            bst[(long)l * nb + b] = fv;
+            bst[(long)(27 + l) * nb + b] = gv;
+        }
+    }
+}
+
+template <bool LOCAL>
+__global__ void k_sc_pack(ScGeom g, MixOff o, char *__restrict__ stage, long n0, long n1,
+                          const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
+                          const int *__restrict__ bid, const double *__restrict__ pop, const double *__restrict__ mom,
+                          const double *__restrict__ minit, const double *__restrict__ bst, long nb) {
+    const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= n1) return;
+    char *rec = stage + (n - n0) * o.size;
+    const long nc = g.ncell;
+    const long offs[M_N] = {o.rho, o.u, o.v, o.w, o.temp, o.p};
+#pragma unroll
+    for (int m = 0; m < M_N; ++m) st(rec, offs[m], mom[(long)m * nc + n]);
+    const uint8_t cf = cflag[n];
+    if (!(cf & CF_FLUID)) return;
+    double f[27], ge[27];
+    if (LOCAL) {
+        for (int l = 0; l < 27; ++l) {
+            f[l] = pop[(long)l * nc + n];
+            ge[l] = pop[(long)(27 + l) * nc + n];
+        }
+    } else if (cf & CF_BOUND) {
+        const long b = bid[n];
+        for (int l = 0; l < 27; ++l) {
+            f[l] = bst[(long)l * nb + b];
+            ge[l] = bst[(long)(27 + l) * nb + b];
+        }
+    } else {
+        pull_cell(g, type, cf, n, pop, (const double *)nullptr, 0, f, ge);
+    }
+    for (int l = 0; l < 27; ++l) {
+        st(rec, o.f + 8 * l, f[l]);
+        st(rec, o.g + 8 * l, ge[l]);
+        if (!LOCAL) {
+            st(rec, o.fpc + 8 * l, pop[(long)l * nc + n]);
+            st(rec, o.gpc + 8 * l, pop[(long)(27 + l) * nc + n]);
+        }
+    }
+    double Pt[6], re;
+    if (LOCAL) {
+        for (int a = 0; a < 6; ++a) Pt[a] = minit[(long)a * nc + n];
+        re = minit[6 * nc + n];
+    } else {
+        ScSums s;
+        sums_sc(f, ge, s);
+        for (int a = 0; a < 6; ++a) Pt[a] = s.P[a];
+        re = s.re;
+        for (int a = 0; a < 3; ++a) st(rec, o.energy_flux + 8 * a, s.q[a]);
+    }
+    const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+    for (int a = 0; a < 9; ++a) st(rec, o.p_tensor + 8 * a, Pt[full[a]]);
+    st(rec, o.rhoe, re);
+}
+
+// ----------------------------------------------------------------------------------
+// Host side
+// ----------------------------------------------------------------------------------
+enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3 };
+enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_NKINDS = 3 };
+
+struct EvPair {
+    cudaEvent_t a, b;
+    int kind;
+};
+
+}  // namespace
+
+struct lbmgpu {
+    lbmgpu_desc d{};
+    cudaStream_t stream = nullptr;
+    ScGeom g{};
+    ScPhys P{};
+    MixOff mo{};
+    int8_t *type = nullptr;
+    uint8_t *cflag = nullptr;
+    int *bid = nullptr;
+    long *blist = nullptr;
+    long nb = 0;
+    double *pop[2] = {nullptr, nullptr};
+    double *mom[2] = {nullptr, nullptr};
+    double *minit = nullptr;
+    double *bst[2] = {nullptr, nullptr};
+    unsigned *status = nullptr;
+    char *stage = nullptr;
+    size_t stage_cells = 0;
+    char *bounce = nullptr;  // pinned host bounce buffer for downloads
+    int cur = 0;
+    bool local = true;
+    bool have_state = false;
+    int phase = PH_BOUNDARY;
+    bool prof = false;
+    std::vector<EvPair> pending, pool;
+    long launches[K_NKINDS] = {0, 0, 0};
+    double ms[K_NKINDS] = {0, 0, 0};
+    size_t bytes = 0;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+    (void)cudaGetLastError();
+    if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDevice || e == cudaErrorNoDevice ||
+        e == cudaErrorInsufficientDriver)
+        return LBMGPU_E_NODEV;
+    return LBMGPU_E_CUDA;
+}
+
+#define CK(x)                                   \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_); \
+    } while (0)
+
+template <typename T>
+int dalloc(lbmgpu *h, T **p, size_t count) {
+    CK(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
+    h->bytes += count * sizeof(T);
+    return 0;
+}
+
+void ev_begin(lbmgpu *h, int kind, EvPair &ep) {
+    if (!h->prof) return;
+    if (h->pool.empty()) {
+        EvPair e{};
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+        h->pool.push_back(e);
+    }
+    ep = h->pool.back();
+    h->pool.pop_back();
+    ep.kind = kind;
+    cudaEventRecord(ep.a, h->stream);
+}
+
+void ev_end(lbmgpu *h, EvPair &ep) {
+    if (!h->prof) return;
+    cudaEventRecord(ep.b, h->stream);
+    h->pending.push_back(ep);
+}
+
+void ev_drain(lbmgpu *h) {
+    for (auto &e : h->pending) {
+        float t = 0.f;
+        if (cudaEventSynchronize(e.b) == cudaSuccess && cudaEventElapsedTime(&t, e.a, e.b) == cudaSuccess) {
+            h->ms[e.kind] += t;
+            h->launches[e.kind] += 1;
+        }
+        h->pool.push_back(e);
+    }
+    h->pending.clear();
+}
+
+unsigned grid_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+int launch_collide(lbmgpu *h) {
+    const int c = h->cur, x = 1 - c;
+    EvPair ep{};
+    ev_begin(h, K_COLLIDE, ep);
+    if (h->local)
+        k_sc_collide<true><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(
+            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->minit, h->bst[c], h->nb,
+            h->status);
+    else
+        k_sc_collide<false><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(
+            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->minit, h->bst[c], h->nb,
+            h->status);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int launch_stream_moment(lbmgpu *h) {
+    const int c = h->cur, x = 1 - c;
+    EvPair ep{};
+    ev_begin(h, K_STREAM_MOMENT, ep);
+    k_sc_stream_moment<<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(h->g, h->P, h->type, h->cflag, h->bid,
+                                                                        h->pop[x], h->mom[c], h->mom[x], h->bst[c],
+                                                                        h->bst[x], h->nb, h->status);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    if (h->nb > 0) {
+        EvPair eb{};
+        ev_begin(h, K_OTHER, eb);
+        k_sc_stream_moment_bound<<<grid_for(h->nb), kBlock, 0, h->stream>>>(
+            h->g, h->P, h->type, h->cflag, h->blist, h->pop[x], h->mom[c], h->mom[x], h->bst[c], h->bst[x], h->nb,
+            h->status);
+        ev_end(h, eb);
+        CK(cudaGetLastError());
+    }
+    h->cur = x;
+    h->local = false;
+    return 0;
+}
+
+bool valid_layout(const lbmgpu_mixture_layout &m) {
+    const long need[] = {m.type, m.f, m.fpc, m.p_tensor, m.rho, m.u, m.v, m.w, m.p, m.g, m.gpc, m.rhoe,
+                         m.energy_flux, m.temp};
+    if (m.size == 0 || (m.size % 8) != 0) return false;
+    for (long o : need)
+        if (o < 0 || (size_t)o >= m.size) return false;
+    const long dbl[] = {m.f, m.fpc, m.p_tensor, m.rho, m.u, m.v, m.w, m.p, m.g, m.gpc, m.rhoe, m.energy_flux, m.temp};
+    for (long o : dbl)
+        if (o % 8) return false;
+    // every field must lie inside the record: arrays of 27, 9 and 3 doubles, scalars, a short type
+    const long ext[][2] = {{m.f, 216}, {m.fpc, 216}, {m.g, 216}, {m.gpc, 216}, {m.p_tensor, 72}, {m.energy_flux, 24},
+                           {m.rho, 8}, {m.u, 8}, {m.v, 8}, {m.w, 8}, {m.p, 8}, {m.rhoe, 8}, {m.temp, 8}, {m.type, 2}};
+    for (const auto &e : ext)
+        if ((size_t)(e[0] + e[1]) > m.size) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *lbmgpu_error_string(int code) {
+    switch (code) {
+        case LBMGPU_OK: return "ok";
+        case LBMGPU_E_ARG: return "invalid argument or descriptor";
+        case LBMGPU_E_CUDA: return "CUDA runtime error";
+        case LBMGPU_E_NODEV: return "no usable CUDA device or kernel image (sm_100a build)";
+        case LBMGPU_E_PHASE: return "phase called out of the reference's step order";
+        case LBMGPU_E_STATE: return "no state uploaded yet";
+        case LBMGPU_E_UNSUPPORTED: return "configuration not supported";
+        case LBMGPU_E_VERSION: return "descriptor abi_version mismatch";
+        default: return code > 0 ? "device status bits raised" : "unknown error";
+    }
+}
+
+int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
+    if (!desc || !out) return LBMGPU_E_ARG;
+    *out = nullptr;
+    if (desc->abi_version != LBMGPU_ABI_VERSION) return LBMGPU_E_VERSION;
+    if (desc->Nx < 3 || desc->Ny < 3 || desc->Nz < 3) return LBMGPU_E_ARG;
+    if (desc->n_species != 0) return LBMGPU_E_UNSUPPORTED;
+    if (desc->precision != LBMGPU_FP64) return LBMGPU_E_UNSUPPORTED;
+    if (!(desc->gamma > 1.0) || !(desc->gas_const > 0.0) || !(desc->prtl > 0.0) || !(desc->nu >= 0.0) ||
+        desc->dt_sim <= 0)
+        return LBMGPU_E_ARG;
+    if (!valid_layout(desc->mix)) return LBMGPU_E_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        (void)cudaGetLastError();
+        return LBMGPU_E_NODEV;
+    }
+    if (desc->device < 0 || desc->device >= ndev) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(desc->device));
+    lbmgpu *h = new (std::nothrow) lbmgpu();
+    if (!h) return LBMGPU_E_ARG;
+    h->d = *desc;
+    h->g.Nx = desc->Nx;
+    h->g.Ny = desc->Ny;
+    h->g.Nz = desc->Nz;
+    h->g.sj = desc->Nz;
+    h->g.si = (long)desc->Ny * desc->Nz;
+    h->g.ncell = (long)desc->Nx * desc->Ny * desc->Nz;
+    h->P.nu = desc->nu;
+    h->P.R = desc->gas_const;
+    h->P.gamma = desc->gamma;
+    h->P.prtl = desc->prtl;
+    h->P.dt = desc->dt_sim;
+    h->P.cv = desc->gas_const / (desc->gamma - 1.0);
+    h->P.cp = h->P.cv + desc->gas_const;
+    const lbmgpu_mixture_layout &m = desc->mix;
+    h->mo = MixOff{(long)m.size, m.type, m.f, m.fpc, m.p_tensor, m.rho, m.u, m.v, m.w, m.p, m.g, m.gpc, m.rhoe,
+                   m.energy_flux, m.temp};
+    const long nc = h->g.ncell;
+    int rc = 0;
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_fail(e);
+    if (!rc) rc = dalloc(h, &h->type, nc);
+    if (!rc) rc = dalloc(h, &h->cflag, nc);
+    if (!rc) rc = dalloc(h, &h->bid, nc);
+    for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->pop[b], 54 * (size_t)nc);
+    for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->mom[b], (size_t)M_N * nc);
+    if (!rc) rc = dalloc(h, &h->minit, 7 * (size_t)nc);
+    if (!rc) rc = dalloc(h, &h->status, 1);
+    if (!rc) {
+        e = cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream);
+        if (e != cudaSuccess) rc = cuda_fail(e);
+    }
+    if (!rc) {
+        // staging for AoS transfers: up to 64 MiB of records per chunk
+        h->stage_cells = std::max<size_t>(1, std::min<size_t>((size_t)nc, (64u << 20) / m.size));
+        rc = dalloc(h, &h->stage, h->stage_cells * m.size);
+        if (!rc) {
+            e = cudaMallocHost(reinterpret_cast<void **>(&h->bounce), h->stage_cells * m.size);
+            if (e != cudaSuccess) rc = cuda_fail(e);
+        }
+    }
+    if (rc) {
+        lbmgpu_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_destroy(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    cudaSetDevice(h->d.device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto &e : h->pending) h->pool.push_back(e);
+    for (auto &e : h->pool) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    cudaFree(h->type);
+    cudaFree(h->cflag);
+    cudaFree(h->bid);
+    cudaFree(h->blist);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(h->pop[b]);
+        cudaFree(h->mom[b]);
+        cudaFree(h->bst[b]);
+    }
+    cudaFree(h->minit);
+    cudaFree(h->status);
+    cudaFree(h->stage);
+    if (h->bounce) cudaFreeHost(h->bounce);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    (void)cudaGetLastError();
+    delete h;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos) {
+    if (!h || !mixture_aos) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    const ScGeom &g = h->g;
+    const long nc = g.ncell;
+    const size_t rs = h->mo.size;
+    const char *host = static_cast<const char *>(mixture_aos);
+    // cell types and the per-cell classification, computed on the host once per upload
+    std::vector<int8_t> ty(nc);
+    for (long n = 0; n < nc; ++n) {
+        short t;
+        std::memcpy(&t, host + n * rs + h->mo.type, sizeof(short));
+        if (t < 0 || t > 9) return LBMGPU_E_ARG;
+        ty[n] = (int8_t)t;
+    }
+    std::vector<uint8_t> cf(nc, 0);
+    std::vector<int> bidh(nc, -1);
+    std::vector<long> blh;
+    long nb = 0;
+    for (int i = 0; i < g.Nx; ++i)
+        for (int j = 0; j < g.Ny; ++j)
+            for (int k = 0; k < g.Nz; ++k) {
+                const long n = (long)i * g.si + (long)j * g.sj + k;
+                if (ty[n] != T_F) continue;
+                if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
+                    return LBMGPU_E_ARG;  // a fluid cell on the outermost layer has no ghost neighbour
+                uint8_t c = CF_FLUID;
+                for (int l = 0; l < 27; ++l) {
+                    const long s = n - (long)cx(l) * g.si - (long)cy(l) * g.sj - cz(l);
+                    const int t = ty[s];
+                    if (t != T_F) c |= CF_SLOW;
+                    if (t == T_S || t == T_I || t == T_O || t == T_I_C || t == T_O_C) c |= CF_BOUND;
+                    const int si = i - cx(l), sj = j - cy(l), sk = k - cz(l);
+                    if (si == 0 || sj == 0 || sk == 0 || si == g.Nx - 1 || sj == g.Ny - 1 || sk == g.Nz - 1)
+                        c |= CF_SLOW;
+                }
+                if (c & CF_BOUND) {
+                    bidh[n] = (int)nb++;
+                    blh.push_back(n);
+                }
+                cf[n] = c;
+            }
+    // (re)size the boundary store
+    if (nb != h->nb || !h->bst[0]) {
+        for (int b = 0; b < 2; ++b) {
+            if (h->bst[b]) {
+                cudaFree(h->bst[b]);
+                h->bytes -= 54 * (size_t)h->nb * sizeof(double);
+                h->bst[b] = nullptr;
+            }
+        }
+        if (h->blist) {
+            cudaFree(h->blist);
+            h->bytes -= (size_t)std::max<long>(h->nb, 1) * sizeof(long);
+            h->blist = nullptr;
+        }
+        h->nb = nb;
+        for (int b = 0; b < 2; ++b) {
+            int rc = dalloc(h, &h->bst[b], 54 * (size_t)std::max<long>(nb, 1));
+            if (rc) return rc;
+        }
+        int rc = dalloc(h, &h->blist, (size_t)std::max<long>(nb, 1));
+        if (rc) return rc;
+    }
+    if (nb > 0) CK(cudaMemcpyAsync(h->blist, blh.data(), nb * sizeof(long), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->type, ty.data(), nc, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->cflag, cf.data(), nc, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->bid, bidh.data(), nc * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    h->cur = 0;
+    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
+        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells);
+        CK(cudaMemcpyAsync(h->stage, host + n0 * rs, (n1 - n0) * rs, cudaMemcpyHostToDevice, h->stream));
+        EvPair ep{};
+        ev_begin(h, K_OTHER, ep);
+        k_sc_unpack<<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->cflag, h->bid,
+                                                                 h->pop[0], h->mom[0], h->mom[1], h->minit, h->bst[0],
+                                                                 h->nb);
+        ev_end(h, ep);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    h->local = true;
+    h->have_state = true;
+    h->phase = PH_BOUNDARY;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_download(lbmgpu_t *h, void *mixture_aos) {
+    if (!h || !mixture_aos) return LBMGPU_E_ARG;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    const ScGeom &g = h->g;
+    const long nc = g.ncell;
+    const size_t rs = h->mo.size;
+    char *host = static_cast<char *>(mixture_aos);
+    std::vector<int8_t> ty(nc);
+    CK(cudaMemcpyAsync(ty.data(), h->type, nc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int c = h->cur;
+    const long mof[M_N] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.temp, h->mo.p};
+    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
+        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells);
+        EvPair ep{};
+        ev_begin(h, K_OTHER, ep);
+        if (h->local)
+            k_sc_pack<true><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->type,
+                                                                         h->cflag, h->bid, h->pop[c], h->mom[c],
+                                                                         h->minit, h->bst[c], h->nb);
+        else
+            k_sc_pack<false><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->type,
+                                                                          h->cflag, h->bid, h->pop[c], h->mom[c],
+                                                                          h->minit, h->bst[c], h->nb);
+        ev_end(h, ep);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h->bounce, h->stage, (n1 - n0) * rs, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        // merge: fluid cells take the whole record except the type; the others only
+        // their stored moments (ghost populations are not represented on the device)
+        for (long n = n0; n < n1; ++n) {
+            const char *srec = h->bounce + (n - n0) * rs;
+            char *drec = host + n * rs;
+            if (ty[n] == T_F) {
+                const size_t skip = (h->mo.type == 0) ? 8 : 0;
+                if (skip) std::memcpy(drec + skip, srec + skip, rs - skip);
+                else {
+                    short t;
+                    std::memcpy(&t, drec + h->mo.type, sizeof(short));
+                    std::memcpy(drec, srec, rs);
+                    std::memcpy(drec + h->mo.type, &t, sizeof(short));
+                }
+            } else {
+                for (int m = 0; m < M_N; ++m) std::memcpy(drec + mof[m], srec + mof[m], sizeof(double));
+            }
+        }
+    }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_init(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    if (h->cur != 0) {
+        // Init always rebuilds the state in buffer 0 from the stored moments
+        const long nc = h->g.ncell;
+        CK(cudaMemcpyAsync(h->mom[0], h->mom[1], (size_t)M_N * nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->stream));
+        h->cur = 0;
+    }
+    EvPair ep{};
+    ev_begin(h, K_OTHER, ep);
+    k_sc_init<<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(h->g, h->P, h->type, h->cflag, h->bid, h->pop[0],
+                                                              h->mom[0], h->mom[1], h->minit, h->bst[0], h->nb);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    h->local = true;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_collide_species(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    return LBMGPU_E_UNSUPPORTED;  // single component: the reference's loop has no species phase
+}
+
+int lbmgpu_collide(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    int rc = launch_collide(h);
+    if (rc) return rc;
+    h->phase = PH_COLLIDED;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_streaming(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (h->phase != PH_COLLIDED) return LBMGPU_E_PHASE;
+    h->phase = PH_STREAMED;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_tms_bc(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (h->phase != PH_STREAMED) return LBMGPU_E_PHASE;
+    h->phase = PH_BC;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_calculate_moment(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (h->phase != PH_BC) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    int rc = launch_stream_moment(h);
+    if (rc) return rc;
+    h->phase = PH_BOUNDARY;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_step(lbmgpu_t *h, int nsteps) {
+    if (!h || nsteps < 0) return LBMGPU_E_ARG;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = launch_collide(h);
+        if (!rc) rc = launch_stream_moment(h);
+        if (rc) return rc;
+    }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_time_steps(lbmgpu_t *h, int nsteps, double *ms) {
+    if (!h || !ms || nsteps < 0) return LBMGPU_E_ARG;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    int rc = 0;
+    cudaError_t e = cudaEventRecord(a, h->stream);
+    if (e != cudaSuccess) rc = cuda_fail(e);
+    for (int s = 0; s < nsteps && !rc; ++s) {
+        rc = launch_collide(h);
+        if (!rc) rc = launch_stream_moment(h);
+    }
+    if (!rc) {
+        e = cudaEventRecord(b, h->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float t = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+        if (e != cudaSuccess) rc = cuda_fail(e);
+        *ms = t;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
+int lbmgpu_synchronize(lbmgpu_t *h) {
+    if (!h) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    CK(cudaStreamSynchronize(h->stream));
+    ev_drain(h);
+    unsigned f = 0;
+    CK(cudaMemcpyAsync(&f, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return (int)f;
+}
+
+int lbmgpu_status(lbmgpu_t *h, uint32_t *flags, int clear) {
+    if (!h || !flags) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned f = 0;
+    CK(cudaMemcpyAsync(&f, h->status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *flags = f;
+    if (clear) {
+        CK(cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_profile(lbmgpu_t *h, int enable) {
+    if (!h) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    CK(cudaStreamSynchronize(h->stream));
+    ev_drain(h);
+    h->prof = enable != 0;
+    for (int k = 0; k < K_NKINDS; ++k) {
+        h->launches[k] = 0;
+        h->ms[k] = 0.0;
+    }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms) {
+    if (!h || nkinds < 0 || (nkinds > 0 && (!launches || !ms))) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    CK(cudaStreamSynchronize(h->stream));
+    ev_drain(h);
+    for (int k = 0; k < nkinds && k < K_NKINDS; ++k) {
+        launches[k] = h->launches[k];
+        ms[k] = h->ms[k];
+    }
+    return K_NKINDS;
+}
+
+int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes) {
+    if (!h || !bytes) return LBMGPU_E_ARG;
+    *bytes = h->bytes;
+    return LBMGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+"""Python binding of liblbmgpu.so (the C ABI in include/lbmgpu.h), through ctypes.
+
+The library is the product: every call below goes straight to the sm_100a kernels.
+There is no fallback -- if the shared library or a CUDA device is missing, the calls
+raise ``LbmGpuError``.
+
+The cell arrays exchanged with the device use the reference's own cell record
+(class MIXTURE, src/headers/lbm.hpp:56-88), so a state can move between this library and
+the reference solver (Init, restart files, VTK output) without conversion.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbmgpu.so")
+ABI_VERSION = 1
+
+FP64, FP32 = 0, 1
+ST_NAN, ST_NEG_STATE, ST_TAU_UNSTABLE = 0x1, 0x2, 0x4
+KIND_COLLIDE, KIND_STREAM_MOMENT, KIND_OTHER = 0, 1, 2
+
+# The single-component MIXTURE record (1024 bytes; offsets as laid out by g++/x86-64).
+MIXTURE_SC = np.dtype({
+    "names": ["type", "f", "fpc", "p_tensor", "rho", "u", "v", "w", "p", "g", "gpc", "rhoe",
+              "energy_flux", "temp"],
+    "formats": ["<i2", ("<f8", 27), ("<f8", 27), ("<f8", (3, 3)), "<f8", "<f8", "<f8", "<f8", "<f8",
+                ("<f8", 27), ("<f8", 27), "<f8", ("<f8", 3), "<f8"],
+    "offsets": [0, 8, 224, 440, 512, 520, 528, 536, 544, 552, 768, 984, 992, 1016],
+    "itemsize": 1024,
+})
+
+EXPORTS = [
+    "lbmgpu_create", "lbmgpu_destroy", "lbmgpu_upload", "lbmgpu_download", "lbmgpu_init",
+    "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
+    "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
+    "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
+]
+
+
+class MixtureLayout(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_size_t)] + [(n, ctypes.c_long) for n in (
+        "type", "f", "fpc", "p_tensor", "rho", "u", "v", "w", "p", "g", "gpc", "rhoe", "energy_flux",
+        "temp", "HRR")]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("abi_version", ctypes.c_int), ("device", ctypes.c_int), ("Nx", ctypes.c_int),
+                ("Ny", ctypes.c_int), ("Nz", ctypes.c_int), ("n_species", ctypes.c_int),
+                ("precision", ctypes.c_int), ("dt_sim", ctypes.c_int), ("nu", ctypes.c_double),
+                ("gas_const", ctypes.c_double), ("gamma", ctypes.c_double), ("prtl", ctypes.c_double),
+                ("mix", MixtureLayout)]
+
+
+class LbmGpuError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__(f"{what}: {error_string(code)} ({code})")
+
+
+_lib = None
+
+
+def lib():
+    """Loads liblbmgpu.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.lbmgpu_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(vp)]
+        for name in ("lbmgpu_destroy", "lbmgpu_init", "lbmgpu_collide_species", "lbmgpu_collide",
+                     "lbmgpu_streaming", "lbmgpu_tms_bc", "lbmgpu_calculate_moment", "lbmgpu_synchronize"):
+            getattr(L, name).argtypes = [vp]
+        L.lbmgpu_upload.argtypes = [vp, vp]
+        L.lbmgpu_download.argtypes = [vp, vp]
+        L.lbmgpu_step.argtypes = [vp, ctypes.c_int]
+        L.lbmgpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.lbmgpu_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]
+        L.lbmgpu_profile.argtypes = [vp, ctypes.c_int]
+        L.lbmgpu_kernel_times.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
+                                          ctypes.POINTER(ctypes.c_double)]
+        L.lbmgpu_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+        L.lbmgpu_error_string.argtypes = [ctypes.c_int]
+        L.lbmgpu_error_string.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def error_string(code):
+    return lib().lbmgpu_error_string(code).decode()
+
+
+def layout_of(dtype):
+    """MixtureLayout (byte offsets) of a numpy structured dtype; -1 for absent fields."""
+    lay = MixtureLayout()
+    lay.size = dtype.itemsize
+    for name, _ in MixtureLayout._fields_[1:]:
+        setattr(lay, name, dtype.fields[name][1] if name in dtype.fields else -1)
+    return lay
+
+
+def _check(rc, what):
+    if rc < 0:
+        raise LbmGpuError(rc, what)
+    return rc
+
+
+class Lattice:
+    """One LBM object on one GPU: the device counterpart of the reference's ``LBM`` class.
+
+    ``Nx, Ny, Nz`` include the ghost layer (the reference's LBM::Nx etc.).
+    """
+
+    def __init__(self, Nx, Ny, Nz, nu, gas_const=1.0, gamma=1.4, prtl=0.5, device=0,
+                 precision=FP64, dtype=MIXTURE_SC, dt_sim=1):
+        d = Desc()
+        d.abi_version = ABI_VERSION
+        d.device = device
+        d.Nx, d.Ny, d.Nz = Nx, Ny, Nz
+        d.n_species = 0
+        d.precision = precision
+        d.dt_sim = dt_sim
+        d.nu, d.gas_const, d.gamma, d.prtl = nu, gas_const, gamma, prtl
+        d.mix = layout_of(dtype)
+        self.dtype = dtype
+        self.shape = (Nx, Ny, Nz)
+        self.h = ctypes.c_void_p()
+        _check(lib().lbmgpu_create(ctypes.byref(d), ctypes.byref(self.h)), "lbmgpu_create")
+
+    # -- state transfer ---------------------------------------------------------------
+    def _cells_ptr(self, cells):
+        if cells.dtype != self.dtype or cells.shape != self.shape or not cells.flags.c_contiguous:
+            raise ValueError("cell array must be a C-contiguous %s array of shape %s" % (self.dtype, self.shape))
+        return cells.ctypes.data
+
+    def upload(self, cells):
+        _check(lib().lbmgpu_upload(self.h, self._cells_ptr(cells)), "lbmgpu_upload")
+
+    def download(self, cells):
+        _check(lib().lbmgpu_download(self.h, self._cells_ptr(cells)), "lbmgpu_download")
+
+    # -- the reference's phases -------------------------------------------------------
+    def init(self):
+        _check(lib().lbmgpu_init(self.h), "lbmgpu_init")
+
+    def collide_species(self):
+        return lib().lbmgpu_collide_species(self.h)
+
+    def collide(self):
+        _check(lib().lbmgpu_collide(self.h), "lbmgpu_collide")
+
+    def streaming(self):
+        _check(lib().lbmgpu_streaming(self.h), "lbmgpu_streaming")
+
+    def tms_bc(self):
+        _check(lib().lbmgpu_tms_bc(self.h), "lbmgpu_tms_bc")
+
+    def calculate_moment(self):
+        _check(lib().lbmgpu_calculate_moment(self.h), "lbmgpu_calculate_moment")
+
+    def step(self, n=1):
+        _check(lib().lbmgpu_step(self.h, n), "lbmgpu_step")
+
+    def time_steps(self, n):
+        """Runs n steps and returns their device time in ms (CUDA events on the handle's
+        stream)."""
+        ms = ctypes.c_double()
+        _check(lib().lbmgpu_time_steps(self.h, n, ctypes.byref(ms)), "lbmgpu_time_steps")
+        return ms.value
+
+    def synchronize(self):
+        return _check(lib().lbmgpu_synchronize(self.h), "lbmgpu_synchronize")
+
+    def status(self, clear=False):
+        f = ctypes.c_uint32()
+        _check(lib().lbmgpu_status(self.h, ctypes.byref(f), int(clear)), "lbmgpu_status")
+        return f.value
+
+    # -- timing -------------------------------------------------------------------------
+    def profile(self, enable=True):
+        _check(lib().lbmgpu_profile(self.h, int(enable)), "lbmgpu_profile")
+
+    def kernel_times(self):
+        launches = (ctypes.c_long * 3)()
+        ms = (ctypes.c_double * 3)()
+        _check(lib().lbmgpu_kernel_times(self.h, 3, launches, ms), "lbmgpu_kernel_times")
+        return list(launches), list(ms)
+
+    def device_bytes(self):
+        b = ctypes.c_size_t()
+        _check(lib().lbmgpu_device_bytes(self.h, ctypes.byref(b)), "lbmgpu_device_bytes")
+        return b.value
+
+    def close(self):
+        if self.h:
+            lib().lbmgpu_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,111 @@
+"""Seeded synthetic initial states (the workloads of the parity tests and the bench).
+
+Each state is an AoS cell array with the reference's single-component MIXTURE layout
+(src/headers/lbm.hpp:56-88), the form the reference's case setups (src/setup.cpp) leave
+before LBM::run: cell types and the macroscopic fields u, v, w, p, temp.  It is ready for
+the device upload and for the reference solver alike.
+
+Seeds: numpy PCG64 with seed 20261203 unless stated otherwise.  No external dataset is
+involved.
+"""
+import math
+
+import numpy as np
+
+SEED = 20261203
+TYPE_F, TYPE_S, TYPE_P, TYPE_A, TYPE_FS, TYPE_I, TYPE_O, TYPE_I_C, TYPE_O_C, TYPE_Q = range(10)
+
+# Byte layout of the single-component MIXTURE record (1024 bytes).
+MIXTURE_SC = np.dtype({
+    "names": ["type", "f", "fpc", "p_tensor", "rho", "u", "v", "w", "p", "g", "gpc", "rhoe",
+              "energy_flux", "temp"],
+    "formats": ["<i2", ("<f8", 27), ("<f8", 27), ("<f8", (3, 3)), "<f8", "<f8", "<f8", "<f8", "<f8",
+                ("<f8", 27), ("<f8", 27), "<f8", ("<f8", 3), "<f8"],
+    "offsets": [0, 8, 224, 440, 512, 520, 528, 536, 544, 552, 768, 984, 992, 1016],
+    "itemsize": 1024,
+})
+
+
+def blank_sc(NX, NY, NZ):
+    """Cells as the reference constructor leaves them (lbm.hpp:59-83): fluid type,
+    rho = 1, zero velocity, p = T = 1/3; populations zero."""
+    c = np.zeros((NX + 2, NY + 2, NZ + 2), dtype=MIXTURE_SC)
+    c["type"] = TYPE_F
+    c["rho"] = 1.0
+    c["p"] = 1.0 / 3.0
+    c["temp"] = 1.0 / 3.0
+    return c
+
+
+def tgv_sc(N, Ma=0.1, Re=400.0, R=0.1, T0=1.0, gamma=1.4, prtl=0.71, noise=1e-3, seed=SEED,
+           NY=None, NZ=None):
+    """Single-component 3-D Taylor-Green vortex in a periodic box (N^3 interior cells).
+
+    u = U sin x cos y cos z, v = -U cos x sin y cos z, w = 0 with x = 2 pi i / N over the
+    reference's array index (as in the reference's TAYLOR_GREEN_3D setup, setup.cpp:94-148);
+    rho = 1, T = 1 with gas constant R = 0.1, so theta = R T = 0.1; U = Ma * sqrt(gamma theta);
+    nu = U (N / 2 pi) / Re; p = (p0 + rho U^2/16 (cos 2x + cos 2y)(cos 2z + 2)) (1 + xi)
+    with seeded uniform xi in [-noise, noise] (the density noise reaches rho through
+    Init's rho = p / (R T)).  At theta = 1/3 the reference's own single-component scheme
+    diverges within 100 steps for Re >= 25 at 32^3 (and at 64^3, Re = 400); theta = 0.1 runs
+    the 64^3, Re = 400, Ma = 0.1 case stably for 1000 steps.
+    """
+    NY = NY or N
+    NZ = NZ or N
+    c = blank_sc(N, NY, NZ)
+    Nx, Ny, Nz = c.shape
+    theta = R * T0
+    U = Ma * math.sqrt(gamma * theta)
+    nu = U * (N / (2.0 * math.pi)) / Re
+    i, j, k = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    ghost = (i == 0) | (i == Nx - 1) | (j == 0) | (j == Ny - 1) | (k == 0) | (k == Nz - 1)
+    c["type"][ghost] = TYPE_P
+    x = 2.0 * math.pi * i / N
+    y = 2.0 * math.pi * j / NY
+    z = 2.0 * math.pi * k / NZ
+    rng = np.random.Generator(np.random.PCG64(seed))
+    xi = rng.uniform(-noise, noise, size=c.shape)
+    fl = ~ghost
+    rho0 = 1.0
+    p0 = rho0 * R * T0
+    c["u"][fl] = (U * np.sin(x) * np.cos(y) * np.cos(z))[fl]
+    c["v"][fl] = (-U * np.cos(x) * np.sin(y) * np.cos(z))[fl]
+    c["w"][fl] = 0.0
+    p = (p0 + rho0 * U * U / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)) * (1.0 + xi)
+    c["p"][fl] = p[fl]
+    c["temp"][fl] = T0
+    params = dict(nu=nu, R=R, gamma=gamma, prtl=prtl, U=U)
+    return c, params
+
+
+def channel_sc(NX=24, NY=10, NZ=8, u_in=0.05, R=0.1, T0=1.0, T_wall=0.9, gamma=1.4, prtl=0.71,
+               nu=0.02, seed=SEED, noise=1e-3, freeslip_z=False):
+    """Single-component channel exercising every single-component boundary type:
+    inflow ghost (TYPE_I, prescribed u, T) at i = 0, outflow ghost (TYPE_O, prescribed p)
+    at i = Nx-1, solid walls (TYPE_S, wall temperature T_wall) at j = 0 and an adiabatic
+    wall (TYPE_A) at j = Ny-1; z is periodic, or free-slip (TYPE_FS) when freeslip_z.
+    The interior starts at rest with seeded pressure noise."""
+    c = blank_sc(NX, NY, NZ)
+    Nx, Ny, Nz = c.shape
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p0 = R * T0
+    c["temp"] = T0
+    c["p"] = p0 * (1.0 + rng.uniform(-noise, noise, size=c.shape))
+    t = c["type"]
+    if freeslip_z:
+        t[:, :, 0] = TYPE_FS
+        t[:, :, Nz - 1] = TYPE_FS
+    else:
+        t[:, :, 0] = TYPE_P
+        t[:, :, Nz - 1] = TYPE_P
+    t[:, 0, :] = TYPE_S
+    t[:, Ny - 1, :] = TYPE_A
+    t[0, :, :] = TYPE_I
+    t[Nx - 1, :, :] = TYPE_O
+    c["u"][0, :, :] = u_in
+    c["temp"][0, :, :] = T0
+    c["temp"][:, 0, :] = T_wall
+    c["p"][Nx - 1, :, :] = p0
+    c["u"][1:Nx - 1, 1:Ny - 1, 1:Nz - 1] = 0.0
+    params = dict(nu=nu, R=R, gamma=gamma, prtl=prtl)
+    return c, params

@@ -1,0 +1,145 @@
+"""Generates the golden fixtures in this directory from the reference's OWN code.
+
+Run from the repository root (needs the reference tree, built by ``make -C oracle ref``):
+
+    python tests/golden/make_golden.py
+
+It drives ``oracle/_ref/libref_sc.so`` -- the reference's single-component sources
+compiled unchanged -- on seeded inputs and records:
+
+* ``kat_sc.npz``           known answers of calculate_feq, calculate_geq (both forms),
+                           calculate_gstr and the FD stencils on seeded random arguments;
+* ``sc_tgv12.npz``         12^3 Taylor-Green vortex (Re 10), fields after 1 and 50 steps;
+* ``sc_channel.npz``       24x10x8 channel with inflow/outflow/solid/adiabatic cells,
+                           fields after 1 and 40 steps;
+* ``sc_channel_fs.npz``    the same channel with free-slip z walls;
+* ``sc_tgv64.npz``         the 64^3, Re 400, Ma 0.1 Taylor-Green vortex: fields on every
+                           4th cell per axis and whole-field sums after 100 and 1000 steps.
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import cases, refsc  # noqa: E402
+
+FIELDS = ["rho", "u", "v", "w", "temp", "p"]
+
+
+def digest(cells):
+    return hashlib.sha256(np.ascontiguousarray(cells).tobytes()).hexdigest()
+
+
+def run_ref(cells, params, checkpoints, sample=None, pop_cells=None):
+    NX, NY, NZ = [s - 2 for s in cells.shape]
+    ref = refsc.RefSC(NX, NY, NZ, params["nu"], params["R"], params["gamma"], params["prtl"], cases.MIXTURE_SC)
+    ref.cells[...] = cells
+    ref.init()
+    out = {}
+    done = 0
+    for cp in checkpoints:
+        ref.loop(cp - done)
+        done = cp
+        c = ref.cells
+        sel = c if sample is None else c[sample]
+        for f in FIELDS:
+            out[f"{f}_{cp}"] = np.ascontiguousarray(sel[f])
+        fl = c["type"] == cases.TYPE_F
+        out[f"sum_mass_{cp}"] = np.sum(c["rho"][fl])
+        out[f"sum_ke_{cp}"] = 0.5 * np.sum(c["rho"][fl] * (c["u"][fl] ** 2 + c["v"][fl] ** 2 + c["w"][fl] ** 2))
+        out[f"sum_rhoe_{cp}"] = np.sum(c["rhoe"][fl])
+        if pop_cells is not None:
+            idx = tuple(pop_cells.T)
+            out[f"f_{cp}"] = np.ascontiguousarray(c["f"][idx])
+            out[f"g_{cp}"] = np.ascontiguousarray(c["g"][idx])
+            out[f"fpc_{cp}"] = np.ascontiguousarray(c["fpc"][idx])
+            out[f"gpc_{cp}"] = np.ascontiguousarray(c["gpc"][idx])
+            out[f"p_tensor_{cp}"] = np.ascontiguousarray(c["p_tensor"][idx])
+            out[f"rhoe_{cp}"] = np.ascontiguousarray(c["rhoe"][idx])
+    ref.close()
+    return out
+
+
+def pick_cells(cells, n, seed):
+    fl = np.argwhere(cells["type"] == cases.TYPE_F)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return fl[rng.choice(len(fl), size=min(n, len(fl)), replace=False)]
+
+
+def kat(seed=cases.SEED, n=64):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = {}
+    # product-form feq and polynomial geq on physically plausible arguments
+    L = rng.integers(0, 27, size=n)
+    rho = rng.uniform(0.5, 2.0, size=n)
+    u = rng.uniform(-0.2, 0.2, size=(n, 3))
+    theta = rng.uniform(0.02, 0.4, size=n)
+    corr = rng.uniform(-0.01, 0.01, size=(n, 3))
+    U = rng.uniform(0.05, 2.0, size=n)
+    out.update(L=L, rho=rho, u=u, theta=theta, corr=corr, U=U)
+    out["feq"] = np.array([refsc.feq(int(L[i]), rho[i], u[i], theta[i], corr[i]) for i in range(n)])
+    out["geq"] = np.array([refsc.geq_poly(int(L[i]), rho[i], U[i], theta[i], u[i]) for i in range(n)])
+    # the whole 27-direction sets for a few states
+    out["geq_all"] = np.array([[refsc.geq_poly(l, rho[i], U[i], theta[i], u[i]) for l in range(27)] for i in range(8)])
+    out["feq_all"] = np.array([[refsc.feq(l, rho[i], u[i], theta[i], corr[i]) for l in range(27)] for i in range(8)])
+    # moment-form geq on symmetric R
+    rhoe = rng.uniform(0.5, 3.0, size=n)
+    q = rng.uniform(-0.3, 0.3, size=(n, 3))
+    A = rng.uniform(-0.2, 0.2, size=(n, 3, 3))
+    R = np.einsum("nij,nkj->nik", A, A) + np.eye(3)[None] * rng.uniform(0.2, 1.0, size=(n, 1, 1))
+    out.update(rhoe=rhoe, q=q, R=R)
+    out["geq_moment"] = np.array([refsc.geq_moment(int(L[i]), rhoe[i], q[i], R[i], theta[i]) for i in range(n)])
+    geqv = rng.uniform(-1, 1, size=n)
+    dq = rng.uniform(-0.1, 0.1, size=(n, 3))
+    out.update(geqv=geqv, dq=dq)
+    out["gstr"] = np.array([refsc.gstr(int(L[i]), geqv[i], dq[i]) for i in range(n)])
+    # FD stencils over every pair of neighbour types
+    types = np.arange(10)
+    tl, tr = np.meshgrid(types, types, indexing="ij")
+    tl = tl.ravel()
+    tr = tr.ravel()
+    m = len(tl)
+    s = rng.uniform(-1, 1, size=(m, 3))
+    vel = rng.uniform(-0.1, 0.1, size=m)
+    out.update(fd_tl=tl, fd_tr=tr, fd_s=s, fd_vel=vel)
+    out["fd_central"] = np.array([refsc.fd_central(s[i, 0], s[i, 1], s[i, 2], 1.0, vel[i], int(tl[i]), int(tr[i]))
+                                  for i in range(m)])
+    out["fd_fuw"] = np.array([refsc.fd_fuw(s[i, 0], s[i, 1], s[i, 2], 1.0, vel[i], int(tl[i]), int(tr[i]))
+                              for i in range(m)])
+    out["fd_uw"] = np.array([refsc.fd_uw(s[i, 0], s[i, 1], s[i, 2], 1.0, vel[i]) for i in range(m)])
+    return out
+
+
+def main():
+    if not refsc.available():
+        raise SystemExit("oracle/_ref/libref_sc.so missing: run `make -C oracle ref` first")
+    refsc.set_threads(os.cpu_count() or 1)
+    np.savez_compressed(os.path.join(HERE, "kat_sc.npz"), **kat())
+
+    cells, params = cases.tgv_sc(12, Re=10.0)
+    out = run_ref(cells, params, [1, 50], pop_cells=pick_cells(cells, 32, 1))
+    out.update(input_sha256=digest(cells), pop_cells=pick_cells(cells, 32, 1))
+    np.savez_compressed(os.path.join(HERE, "sc_tgv12.npz"), **out)
+
+    for name, fs in (("sc_channel.npz", False), ("sc_channel_fs.npz", True)):
+        cells, params = cases.channel_sc(freeslip_z=fs)
+        pc = pick_cells(cells, 48, 2)
+        out = run_ref(cells, params, [1, 40], pop_cells=pc)
+        out.update(input_sha256=digest(cells), pop_cells=pc)
+        np.savez_compressed(os.path.join(HERE, name), **out)
+
+    cells, params = cases.tgv_sc(64)
+    sample = (slice(1, 65, 4), slice(1, 65, 4), slice(1, 65, 4))
+    out = run_ref(cells, params, [100, 1000], sample=sample)
+    out.update(input_sha256=digest(cells))
+    np.savez_compressed(os.path.join(HERE, "sc_tgv64.npz"), **out)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
