@@ -45,6 +45,45 @@ extern "C" {
 #define LBMGPU_FP64 0
 #define LBMGPU_FP32 1
 
+/* ---- gas mechanism ------------------------------------------------------------
+ * Flat tables of one ideal-gas mechanism in SI units (kmol, m, s, J, K), the data the
+ * reference obtains from Cantera (src/lbm-main.cpp:79-117).  Filled by a loader from the
+ * repository's Cantera-YAML mechanisms (src/reaction-mech/*.yaml): NASA-7 thermo, gas
+ * transport parameters, and elementary / three-body / falloff (Lindemann, Troe) reactions
+ * with mass-action rate laws.  Species are listed in the caller's order. */
+#define LBMGPU_MAX_SPECIES 12
+#define LBMGPU_MAX_REACTIONS 48
+#define LBMGPU_MAX_RSPEC 3     /* species per side of a reaction */
+
+enum { LBMGPU_RXN_ELEMENTARY = 0, LBMGPU_RXN_THREEBODY = 1, LBMGPU_RXN_FALLOFF = 2 };
+enum { LBMGPU_GEOM_ATOM = 0, LBMGPU_GEOM_LINEAR = 1, LBMGPU_GEOM_NONLINEAR = 2 };
+
+typedef struct lbmgpu_mech {
+    int n_species, n_reactions;
+    char name[LBMGPU_MAX_SPECIES][16];
+    double W[LBMGPU_MAX_SPECIES];                 /* molar mass, kg/kmol                 */
+    double T_lo[LBMGPU_MAX_SPECIES], T_mid[LBMGPU_MAX_SPECIES], T_hi[LBMGPU_MAX_SPECIES];
+    double nasa_lo[LBMGPU_MAX_SPECIES][7];        /* NASA-7 coefficients below T_mid     */
+    double nasa_hi[LBMGPU_MAX_SPECIES][7];        /* NASA-7 coefficients above T_mid     */
+    int geometry[LBMGPU_MAX_SPECIES];             /* LBMGPU_GEOM_*                       */
+    double well_depth[LBMGPU_MAX_SPECIES];        /* epsilon / k_B, K                    */
+    double diameter[LBMGPU_MAX_SPECIES];          /* Lennard-Jones sigma, m              */
+    double dipole[LBMGPU_MAX_SPECIES];            /* C m                                 */
+    double polarizability[LBMGPU_MAX_SPECIES];    /* m^3                                 */
+    double rot_relax[LBMGPU_MAX_SPECIES];         /* Z_rot at 298 K                      */
+    int elements[LBMGPU_MAX_SPECIES][4];          /* atoms of H, O, N, Ar per molecule   */
+    int rtype[LBMGPU_MAX_REACTIONS];              /* LBMGPU_RXN_*                        */
+    int reversible[LBMGPU_MAX_REACTIONS];
+    int n_reac[LBMGPU_MAX_REACTIONS], n_prod[LBMGPU_MAX_REACTIONS];
+    int reac[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_RSPEC], prod[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_RSPEC];
+    double nu_reac[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_RSPEC], nu_prod[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_RSPEC];
+    double A[LBMGPU_MAX_REACTIONS], b[LBMGPU_MAX_REACTIONS], Ea[LBMGPU_MAX_REACTIONS]; /* k (or k_inf), Ea in J/kmol */
+    double A0[LBMGPU_MAX_REACTIONS], b0[LBMGPU_MAX_REACTIONS], Ea0[LBMGPU_MAX_REACTIONS]; /* falloff k_0 */
+    int troe_n[LBMGPU_MAX_REACTIONS];             /* 0 Lindemann, 3 or 4 Troe parameters  */
+    double troe[LBMGPU_MAX_REACTIONS][4];         /* a, T***, T*, T**                    */
+    double eff[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_SPECIES]; /* third-body efficiencies      */
+} lbmgpu_mech;
+
 /* Byte offsets of the fields of the caller's MIXTURE record (src/headers/lbm.hpp:56-88).
  * Fill with sizeof/offsetof from the caller's own class; -1 marks a field the
  * configuration does not have (f/fpc are absent when MULTICOMP is on). */

@@ -1,0 +1,288 @@
+// Ideal-gas thermodynamics, mixture-averaged transport and mass-action kinetics of one
+// mechanism (the physical-property evaluations the reference obtains from Cantera 3.x:
+// ThermoPhase, MixTransport, GasKinetics; call sites src/lbm-collision.cpp:236-247,
+// 364-467, src/lbm-moment.cpp:219-368, src/lbm-edf.cpp:177-186).
+//
+// Written from the published methods, in FP64, for both host and device:
+//  * thermo: NASA 7-coefficient polynomials (McBride, Gordon & Reno, NASA TM-4513):
+//      cp/R = a1 + a2 T + a3 T^2 + a4 T^3 + a5 T^4,  h/RT = a1 + a2 T/2 + ... + a6/T,
+//      s/R = a1 ln T + a2 T + a3 T^2/2 + a4 T^3/3 + a5 T^4/4 + a7;
+//    T from (u, v) by Newton iteration on u(T) (what setState_UV solves).
+//  * transport: Chapman-Enskog species viscosities and binary diffusion coefficients with
+//    the Neufeld, Janzen & Aziz (1972) fits of the Lennard-Jones collision integrals
+//    Omega(2,2)* and Omega(1,1)*, Brokaw's dipole correction, the polar/non-polar
+//    combining rules of the CHEMKIN transport formulation (Kee et al., SAND86-8246);
+//    species conductivities by the Warnatz/CHEMKIN translational-rotational-vibrational
+//    split with the Parker-Brau-Jonkman rotational-relaxation temperature dependence;
+//    mixture viscosity by Wilke's rule, mixture conductivity by the
+//    Mathur-Tondon-Saxena average.
+//  * kinetics: modified Arrhenius rates, third-body and Lindemann/Troe fall-off
+//    (Gilbert, Luther & Troe 1983), reverse rates from equilibrium constants of the
+//    NASA-7 Gibbs energies at 1 atm.
+// Transport and kinetics have no pinned reference values (Cantera is not available);
+// tests check them against physical identities and literature values.
+#pragma once
+#include <math.h>
+
+#include "../../include/lbmgpu.h"
+
+#if defined(__CUDACC__)
+#define GAS_HD __host__ __device__ __forceinline__
+#else
+#define GAS_HD inline
+#endif
+
+namespace gas {
+
+constexpr double kR = 8314.46261815324;       // J / (kmol K)  (Cantera::GasConstant)
+constexpr double kOneAtm = 101325.0;          // Pa
+constexpr double kBoltz = 1.380649e-23;       // J / K
+constexpr double kNA = 6.02214076e26;         // 1 / kmol
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kEps0 = 8.8541878128e-12;    // F / m
+constexpr int MAXS = LBMGPU_MAX_SPECIES;
+constexpr int MAXR = LBMGPU_MAX_REACTIONS;
+
+// Mechanism plus the per-species and per-pair transport constants derived from it once
+// on the host (make_tables).
+struct Tables {
+    lbmgpu_mech m;
+    int ns;
+    double invW[MAXS];
+    double visc_pref[MAXS];            // mu_k = visc_pref * sqrt(T) / Omega22(T/eps_k, delta_k)
+    double eps[MAXS];                  // epsilon/k_B of the species, K
+    double delta[MAXS];                // reduced dipole moment delta*_k
+    double diff_pref[MAXS][MAXS];      // D_kj * P = diff_pref * T^1.5 / Omega11(T/eps_kj, delta_kj)
+    double eps_pair[MAXS][MAXS];
+    double delta_pair[MAXS][MAXS];
+    double cvrot_R[MAXS];              // rotational heat capacity / R
+    double zrot298_F298[MAXS];         // Z_rot(298) F(298), Z_rot(T) = this / F(T)
+};
+
+GAS_HD double sq(double x) { return x * x; }
+
+// ---- collision integrals (Neufeld, Janzen & Aziz 1972) with Brokaw's polar term ----
+GAS_HD double omega22(double Ts, double delta) {
+    const double o = 1.16145 * pow(Ts, -0.14874) + 0.52487 * exp(-0.77320 * Ts) + 2.16178 * exp(-2.43787 * Ts);
+    return o + 0.2 * delta * delta / Ts;
+}
+GAS_HD double omega11(double Ts, double delta) {
+    const double o = 1.06036 * pow(Ts, -0.15610) + 0.19300 * exp(-0.47635 * Ts) + 1.03587 * exp(-1.52996 * Ts) +
+                     1.76474 * exp(-3.89411 * Ts);
+    return o + 0.19 * delta * delta / Ts;
+}
+
+// Parker-Brau-Jonkman temperature function of the rotational collision number.
+GAS_HD double parker_F(double eps_over_T) {
+    const double x = eps_over_T;
+    return 1.0 + 0.5 * pow(kPi, 1.5) * sqrt(x) + (0.25 * kPi * kPi + 2.0) * x + pow(kPi, 1.5) * x * sqrt(x);
+}
+
+// Host-side construction of the derived constants.
+inline void make_tables(const lbmgpu_mech &m, Tables &t) {
+    t.m = m;
+    t.ns = m.n_species;
+    for (int k = 0; k < t.ns; ++k) {
+        t.invW[k] = 1.0 / m.W[k];
+        const double mk = m.W[k] / kNA;                 // kg per molecule
+        const double s = m.diameter[k];
+        t.visc_pref[k] = (5.0 / 16.0) * sqrt(kPi * mk * kBoltz) / (kPi * s * s);
+        t.eps[k] = m.well_depth[k];
+        const double epsJ = m.well_depth[k] * kBoltz;
+        t.delta[k] = (epsJ > 0 && s > 0) ? 0.5 * m.dipole[k] * m.dipole[k] / (4.0 * kPi * kEps0 * epsJ * s * s * s) : 0.0;
+        t.cvrot_R[k] = m.geometry[k] == LBMGPU_GEOM_ATOM ? 0.0 : (m.geometry[k] == LBMGPU_GEOM_LINEAR ? 1.0 : 1.5);
+        t.zrot298_F298[k] = m.rot_relax[k] * parker_F(m.well_depth[k] / 298.0);
+    }
+    for (int k = 0; k < t.ns; ++k)
+        for (int j = 0; j < t.ns; ++j) {
+            double epsk = m.well_depth[k], epsj = m.well_depth[j];
+            double sk = m.diameter[k], sj = m.diameter[j];
+            double xi = 1.0;
+            // polar / non-polar pair: induced-dipole correction of the combining rules
+            const bool pk = m.dipole[k] > 0, pj = m.dipole[j] > 0;
+            if (pk != pj) {
+                const int p = pk ? k : j, n = pk ? j : k;
+                const double alpha_n = m.polarizability[n] / (m.diameter[n] * m.diameter[n] * m.diameter[n]);
+                const double epsp = m.well_depth[p] * kBoltz, sp3 = pow(m.diameter[p], 3);
+                const double mu_p = m.dipole[p] / sqrt(4.0 * kPi * kEps0 * epsp * sp3);
+                xi = 1.0 + 0.25 * alpha_n * mu_p * mu_p * sqrt(m.well_depth[p] / m.well_depth[n]);
+            }
+            t.eps_pair[k][j] = sqrt(epsk * epsj) * xi * xi;
+            const double skj = 0.5 * (sk + sj) * pow(xi, -1.0 / 6.0);
+            const double mred = (m.W[k] * m.W[j] / (m.W[k] + m.W[j])) / kNA;
+            t.diff_pref[k][j] = (3.0 / 16.0) * sqrt(2.0 * kPi * pow(kBoltz, 3) / mred) / (kPi * skj * skj);
+            t.delta_pair[k][j] = sqrt(t.delta[k] * t.delta[j]);
+        }
+}
+
+// ---- thermo ----------------------------------------------------------------------
+GAS_HD const double *nasa(const Tables &t, int k, double T) {
+    return T < t.m.T_mid[k] ? t.m.nasa_lo[k] : t.m.nasa_hi[k];
+}
+GAS_HD double cp_R(const Tables &t, int k, double T) {
+    const double *a = nasa(t, k, T);
+    return a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4])));
+}
+GAS_HD double h_RT(const Tables &t, int k, double T) {
+    const double *a = nasa(t, k, T);
+    return a[0] + T * (a[1] / 2 + T * (a[2] / 3 + T * (a[3] / 4 + T * a[4] / 5))) + a[5] / T;
+}
+GAS_HD double s_R(const Tables &t, int k, double T) {
+    const double *a = nasa(t, k, T);
+    return a[0] * log(T) + T * (a[1] + T * (a[2] / 2 + T * (a[3] / 3 + T * a[4] / 4))) + a[6];
+}
+
+// mean molar mass from mass fractions (1 / sum Y/W; Cantera's meanMolecularWeight with
+// normalised fractions)
+GAS_HD double meanW_Y(const Tables &t, const double *Y) {
+    double s = 0.0, sy = 0.0;
+    for (int k = 0; k < t.ns; ++k) {
+        s += Y[k] * t.invW[k];
+        sy += Y[k];
+    }
+    return sy / s;
+}
+GAS_HD double cp_mass(const Tables &t, const double *Y, double T) {
+    double c = 0.0;
+    for (int k = 0; k < t.ns; ++k) c += Y[k] * cp_R(t, k, T) * t.invW[k];
+    return c * kR;
+}
+GAS_HD double int_energy_mass(const Tables &t, const double *Y, double T) {
+    double u = 0.0;
+    for (int k = 0; k < t.ns; ++k) u += Y[k] * (h_RT(t, k, T) - 1.0) * t.invW[k];
+    return u * kR * T;
+}
+GAS_HD double cv_mass(const Tables &t, const double *Y, double T) {
+    double c = 0.0;
+    for (int k = 0; k < t.ns; ++k) c += Y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
+    return c * kR;
+}
+
+// T with int_energy_mass(Y, T) = u: damped Newton from T0, at most `maxit` iterations.
+// Returns the number of iterations, or -1 when the iteration cap was reached.
+GAS_HD int T_from_u(const Tables &t, const double *Y, double u, double T0, double rtol, int maxit, double &T) {
+    T = T0 > 0 ? T0 : 300.0;
+    for (int it = 0; it < maxit; ++it) {
+        const double f = int_energy_mass(t, Y, T) - u;
+        const double cv = cv_mass(t, Y, T);
+        double dT = -f / cv;
+        if (dT > 500.0) dT = 500.0;
+        if (dT < -0.5 * T) dT = -0.5 * T;
+        T += dT;
+        if (fabs(dT) <= rtol * T) return it + 1;
+    }
+    return -1;
+}
+
+// ---- transport ---------------------------------------------------------------------
+GAS_HD double species_visc(const Tables &t, int k, double T) {
+    return t.visc_pref[k] * sqrt(T) / omega22(T / t.eps[k], t.delta[k]);
+}
+// D_kj at (T, P), m^2/s
+GAS_HD double binary_diff(const Tables &t, int k, int j, double T, double P) {
+    return t.diff_pref[k][j] * T * sqrt(T) / (P * omega11(T / t.eps_pair[k][j], t.delta_pair[k][j]));
+}
+
+// Wilke's mixing rule with the species viscosities mu[] and mole fractions X[].
+GAS_HD double wilke(const Tables &t, const double *X, const double *mu) {
+    double s = 0.0;
+    for (int k = 0; k < t.ns; ++k) {
+        double d = 0.0;
+        for (int j = 0; j < t.ns; ++j) {
+            const double f = 1.0 + sqrt(mu[k] / mu[j]) * sqrt(sqrt(t.m.W[j] / t.m.W[k]));
+            d += X[j] * f * f / sqrt(8.0 * (1.0 + t.m.W[k] / t.m.W[j]));
+        }
+        s += X[k] * mu[k] / d;
+    }
+    return s;
+}
+
+// Species thermal conductivity (Warnatz / CHEMKIN), W/(m K).
+GAS_HD double species_cond(const Tables &t, int k, double T, double P, double mu_k) {
+    const double W = t.m.W[k];
+    const double rho = P * W / (kR * T);
+    const double Dkk = binary_diff(t, k, k, T, P);
+    const double rdm = rho * Dkk / mu_k;
+    const double cv_R = cp_R(t, k, T) - 1.0;
+    if (t.m.geometry[k] == LBMGPU_GEOM_ATOM) return mu_k / W * kR * 2.5 * 1.5;
+    const double cvrot = t.cvrot_R[k];
+    const double cvvib = cv_R - 1.5 - cvrot;
+    const double zrot = t.zrot298_F298[k] / parker_F(t.eps[k] / T);
+    const double A = 2.5 - rdm;
+    const double B = zrot + (2.0 / kPi) * (5.0 / 3.0 * cvrot + rdm);
+    const double ftr = 2.5 * (1.0 - (2.0 / kPi) * (cvrot / 1.5) * (A / B));
+    const double frot = rdm * (1.0 + (2.0 / kPi) * (A / B));
+    return mu_k / W * kR * (ftr * 1.5 + frot * cvrot + rdm * cvvib);
+}
+
+GAS_HD double mix_cond(const Tables &t, const double *X, double T, double P, const double *mu) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < t.ns; ++k) {
+        const double lk = species_cond(t, k, T, P, mu[k]);
+        s1 += X[k] * lk;
+        s2 += X[k] / lk;
+    }
+    return 0.5 * (s1 + 1.0 / s2);
+}
+
+// ---- kinetics ----------------------------------------------------------------------
+// Net molar production rates wdot[k] (kmol/m^3/s) at (T, concentrations C[k] kmol/m^3).
+GAS_HD void net_production(const Tables &t, double T, const double *C, double *wdot) {
+    const lbmgpu_mech &m = t.m;
+    double g_RT[MAXS];
+    for (int k = 0; k < t.ns; ++k) {
+        g_RT[k] = h_RT(t, k, T) - s_R(t, k, T);
+        wdot[k] = 0.0;
+    }
+    double Ctot = 0.0;
+    for (int k = 0; k < t.ns; ++k) Ctot += C[k];
+    const double logT = log(T), invRT = 1.0 / (kR * T);
+    const double log_cref = log(kOneAtm / (kR * T));
+    for (int r = 0; r < m.n_reactions; ++r) {
+        double kf = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
+        double M = 1.0;
+        if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
+            M = 0.0;
+            for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
+        }
+        if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
+            const double k0 = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
+            const double Pr = k0 * M / kf;
+            double F = 1.0;
+            if (m.troe_n[r] >= 3) {
+                const double a = m.troe[r][0], T3 = m.troe[r][1], T1 = m.troe[r][2];
+                double Fc = (1.0 - a) * exp(-T / T3) + a * exp(-T / T1);
+                if (m.troe_n[r] == 4) Fc += exp(-m.troe[r][3] / T);
+                const double lFc = log10(fmax(Fc, 1e-300));
+                const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+                const double lPr = log10(fmax(Pr, 1e-300));
+                const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+                F = pow(10.0, lFc / (1.0 + x * x));
+            }
+            kf = kf * (Pr / (1.0 + Pr)) * F;
+            M = 1.0;
+        }
+        double fwd = kf * M, rev = 0.0;
+        for (int j = 0; j < m.n_reac[r]; ++j) fwd *= pow(C[m.reac[r][j]], m.nu_reac[r][j]);
+        if (m.reversible[r]) {
+            double dG = 0.0, dnu = 0.0;
+            for (int j = 0; j < m.n_prod[r]; ++j) {
+                dG += m.nu_prod[r][j] * g_RT[m.prod[r][j]];
+                dnu += m.nu_prod[r][j];
+            }
+            for (int j = 0; j < m.n_reac[r]; ++j) {
+                dG -= m.nu_reac[r][j] * g_RT[m.reac[r][j]];
+                dnu -= m.nu_reac[r][j];
+            }
+            const double kr = kf * M * exp(dG - dnu * log_cref);  // kf / Kc
+            rev = kr;
+            for (int j = 0; j < m.n_prod[r]; ++j) rev *= pow(C[m.prod[r][j]], m.nu_prod[r][j]);
+        }
+        const double q = fwd - rev;
+        for (int j = 0; j < m.n_reac[r]; ++j) wdot[m.reac[r][j]] -= m.nu_reac[r][j] * q;
+        for (int j = 0; j < m.n_prod[r]; ++j) wdot[m.prod[r][j]] += m.nu_prod[r][j] * q;
+    }
+    (void)Ctot;
+}
+
+}  // namespace gas

@@ -25,16 +25,6 @@ namespace {
 
 constexpr int kBlock = 128;
 
-// ----------------------------------------------------------------------------------
-// Collision (reference LBM::Collide, single component, src/lbm-collision.cpp:9-99)
-// ----------------------------------------------------------------------------------
-__device__ __forceinline__ double qdev_at(const double *__restrict__ mom, long nc, long n, int a, double R) {
-    const double rho = mom[M_RHO * nc + n];
-    const double ua = mom[(M_U + a) * nc + n];
-    const double T = mom[M_T * nc + n];
-    return rho * ua * (1.0 - 3.0 * R * T) - rho * (ua * ua * ua);
-}
-
 __device__ __forceinline__ bool wall_like(int t) {
     return t == T_S || t == T_A || t == T_FS || t == T_P || t == T_O || t == T_O_C;
 }
@@ -46,51 +36,39 @@ __device__ __forceinline__ double fd_central(double sl, double sc, double sr, in
     return (sr - sl) / 2.0;
 }
 
+// ----------------------------------------------------------------------------------
+// Collision (reference LBM::Collide, single component, src/lbm-collision.cpp:9-99).
+// Reads the step record of the cell and the Q terms of its six face neighbours, then
+// streams through the 27 directions: fetch f_l, g_l (pulled from the last collision's
+// output, or the special-cell store, or -- in local mode -- in place), relax, store.
+// ----------------------------------------------------------------------------------
+// Population q (0..53: f then g) of cell n at the start of the collision: in place
+// (local mode), from the special-cell store, or pulled from the upstream cell.
+__device__ __forceinline__ double fetch_pop(const double *__restrict__ src, const double *__restrict__ bst, long nc,
+                                            long nb, long n, long b, const PullSrc &ps, int q, bool local,
+                                            bool special) {
+    if (local) return src[(long)q * nc + n];
+    if (special) return bst[(long)q * nb + b];
+    return src[(long)q * nc + pull_at(ps, q % 27)];
+}
+
 template <bool LOCAL>
-__global__ void __launch_bounds__(kBlock) k_sc_collide(ScGeom g, ScPhys P, const int8_t *__restrict__ type,
-                                                       const uint8_t *__restrict__ cflag, const int *__restrict__ bid,
-                                                       const double *__restrict__ src, double *__restrict__ dst,
-                                                       const double *__restrict__ mom, const double *__restrict__ minit,
-                                                       const double *__restrict__ bst, long nb, unsigned *status) {
+__global__ void __launch_bounds__(kBlock, 4)
+    k_sc_collide(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
+                 const int *__restrict__ bid, const double *__restrict__ src, double *__restrict__ dst,
+                 const double *__restrict__ mom, const double *__restrict__ bst, long nb, unsigned *status) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.ncell) return;
     const uint8_t cf = cflag[n];
     if (!(cf & CF_FLUID)) return;
     const long nc = g.ncell;
-    double f[27], ge[27];
-    if (LOCAL) {
-#pragma unroll
-        for (int l = 0; l < 27; ++l) {
-            f[l] = src[(long)l * nc + n];
-            ge[l] = src[(long)(27 + l) * nc + n];
-        }
-    } else if (cf & CF_BOUND) {
-        const long b = bid[n];
-#pragma unroll
-        for (int l = 0; l < 27; ++l) {
-            f[l] = bst[(long)l * nb + b];
-            ge[l] = bst[(long)(27 + l) * nb + b];
-        }
-    } else {
-        pull_cell(g, type, cf, n, src, (const double *)nullptr, 0, f, ge);
-    }
 
     const double rho = mom[M_RHO * nc + n];
     const double vel[3] = {mom[M_U * nc + n], mom[M_V * nc + n], mom[M_W * nc + n]};
     const double T = mom[M_T * nc + n];
     const double p = mom[M_P * nc + n];
-    double Pt[6], rhoe;
-    if (LOCAL) {
-#pragma unroll
-        for (int a = 0; a < 6; ++a) Pt[a] = minit[(long)a * nc + n];
-        rhoe = minit[6 * nc + n];
-    } else {
-        ScSums s;
-        sums_sc(f, ge, s);
-#pragma unroll
-        for (int a = 0; a < 6; ++a) Pt[a] = s.P[a];
-        rhoe = s.re;
-    }
+    const double S[3] = {mom[M_SX * nc + n], mom[M_SY * nc + n], mom[M_SZ * nc + n]};
+    const double Uint = mom[M_UINT * nc + n];
 
     const double dt = P.dt;
     const double theta = P.R * T;
@@ -99,106 +77,88 @@ __global__ void __launch_bounds__(kBlock) k_sc_collide(ScGeom g, ScPhys P, const
     const double om1 = 2 * p * P.cp * dt / (p * P.cp * dt + 2 * kappa);
     const double om = 2 * p * dt / (p * dt + 2 * mu);
     if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) raise_status(status, LBMGPU_ST_TAU_UNSTABLE);
-    const double Uint = rhoe / rho - 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
 
-    // face-neighbour difference of rho u_a (1 - 3 R T) - rho u_a^3 (src/lbm-collision.cpp:64-67)
-    double dQ[3];
+    double dq[3], corr[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const long off = a == 0 ? g.si : (a == 1 ? g.sj : 1);
         const long nlo = n - off, nhi = n + off;
-        dQ[a] = fd_central(qdev_at(mom, nc, nlo, a, P.R), qdev_at(mom, nc, n, a, P.R), qdev_at(mom, nc, nhi, a, P.R),
-                           type[nlo], type[nhi]);
-    }
-    // deviation of the pressure tensor from equilibrium, full symmetric index map
-    const double Pfull[3][3] = {{Pt[0], Pt[1], Pt[2]}, {Pt[1], Pt[3], Pt[4]}, {Pt[2], Pt[4], Pt[5]}};
-    double dq[3], corr[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-        double s = 0.0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) s += vel[a] * (Pfull[a][b] - ((a == b ? p : 0.0) + rho * vel[a] * vel[b]));
-        dq[b] = s + 0.5 * dt * vel[b] * dQ[b];
-        corr[b] = dt * (2 - om) / (2 * rho * om) * dQ[b];
+        const double *Q = mom + (long)(M_QX + a) * nc;
+        const double dQ = fd_central(Q[nlo], Q[n], Q[nhi], type[nlo], type[nhi]);
+        dq[a] = S[a] + 0.5 * dt * vel[a] * dQ;
+        corr[a] = dt * (2 - om) / (2 * rho * om) * dQ;
     }
     AxisF<double> F;
     axis_feq(F, vel, theta, corr);
     AxisG<double> G;
     axis_geq(G, Uint, theta, vel);
+
+    const bool special = cf & CF_SPECIAL;
+    PullSrc ps;
+    if (!LOCAL && !special) pull_src(g, n, ps);
+    const long b = special ? (long)bid[n] : 0;
+    // Each population set is fetched with all 27 loads issued back to back before any is
+    // used (the kernel is bound by memory latency; this keeps 27 loads in flight per
+    // thread), then relaxed and stored.
+    double v[27];
+#pragma unroll
+    for (int l = 0; l < 27; ++l) v[l] = fetch_pop(src, bst, nc, nb, n, b, ps, l, LOCAL, special);
+#pragma unroll
+    for (int l = 0; l < 27; ++l) dst[(long)l * nc + n] = (1.0 - om) * v[l] + om * feq_l(l, rho, F);
+#pragma unroll
+    for (int l = 0; l < 27; ++l) v[l] = fetch_pop(src, bst, nc, nb, n, b, ps, 27 + l, LOCAL, special);
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
-        const double fe = feq_l(l, rho, F);
-        dst[(long)l * nc + n] = (1.0 - om) * f[l] + om * fe;
         const double gq = geq_l(l, rho, G);
         const double gs = (csq(l) == 1) ? gq + 0.5 * (cx(l) * dq[0] + cy(l) * dq[1] + cz(l) * dq[2]) : gq;
-        dst[(long)(27 + l) * nc + n] = ge[l] + om1 * (gq - ge[l]) + (om - om1) * (gq - gs);
+        dst[(long)(27 + l) * nc + n] = v[l] + om1 * (gq - v[l]) + (om - om1) * (gq - gs);
     }
 }
 
 // ----------------------------------------------------------------------------------
-// Streaming + boundary treatment + moments (reference LBM::Streaming, LBM::TMS_BC and
-// LBM::calculate_moment fused; src/lbm-moment.cpp:11-125 for the moments).
+// Streaming + moments for the cells with no boundary neighbour (reference LBM::Streaming
+// and LBM::calculate_moment, src/lbm-streaming.cpp:88-117, src/lbm-moment.cpp:11-125).
 // ----------------------------------------------------------------------------------
-// Moments of the post-stream populations (reference LBM::calculate_moment,
-// src/lbm-moment.cpp:11-125) stored into the moment planes, with the state checks.
-__device__ __forceinline__ void store_moments_sc(const ScGeom &g, const ScPhys &P, long n, const double f[27],
-                                                 const double ge[27], double *__restrict__ mom_nxt,
-                                                 unsigned *status) {
-    const long nc = g.ncell;
-    ScSums s;
-    sums_sc(f, ge, s);
-    const double rho = s.rho;
-    const double u = s.j[0] / rho, v = s.j[1] / rho, w = s.j[2] / rho;
-    const double Uint = s.re / rho - 0.5 * (u * u + v * v + w * w);
-    const double T = Uint / P.cv;
-    const double p = rho * P.R * T;
-    mom_nxt[M_RHO * nc + n] = rho;
-    mom_nxt[M_U * nc + n] = u;
-    mom_nxt[M_V * nc + n] = v;
-    mom_nxt[M_W * nc + n] = w;
-    mom_nxt[M_T * nc + n] = T;
-    mom_nxt[M_P * nc + n] = p;
-    if (!isfinite(rho) || !isfinite(T) || !isfinite(u) || !isfinite(v) || !isfinite(w))
-        raise_status(status, LBMGPU_ST_NAN);
-    else if (!(rho > 0.0) || !(T > 0.0))
-        raise_status(status, LBMGPU_ST_NEG_STATE);
-}
-
-__global__ void __launch_bounds__(kBlock)
-    k_sc_stream_moment(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
-                       const int *__restrict__ bid, const double *__restrict__ src, const double *__restrict__ mom_cur,
-                       double *__restrict__ mom_nxt, const double *__restrict__ bst_cur, double *__restrict__ bst_nxt,
-                       long nb, unsigned *status) {
+__global__ void __launch_bounds__(kBlock, 4)
+    k_sc_stream_moment(ScGeom g, ScPhys P, const uint8_t *__restrict__ cflag, const double *__restrict__ src,
+                       double *__restrict__ mom_nxt, unsigned *status) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.ncell) return;
-    const uint8_t cf = cflag[n];
-    if (!(cf & CF_FLUID)) return;
-    if (cf & CF_BOUND) return;  // boundary cells: k_sc_stream_moment_bound
-    double f[27], ge[27];
-    pull_cell(g, type, cf, n, src, (const double *)nullptr, 0, f, ge);
-    store_moments_sc(g, P, n, f, ge, mom_nxt, status);
+    if (cflag[n] != CF_FLUID) return;  // not fluid, or special (k_sc_stream_moment_special)
+    const long nc = g.ncell;
+    PullSrc ps;
+    pull_src(g, n, ps);
+    ScSums s;
+    sums_init(s);
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        const long sidx = pull_at(ps, l);
+        sums_add(s, l, src[(long)l * nc + sidx], src[(long)(27 + l) * nc + sidx]);
+    }
+    store_record_sc(g, P, n, s, mom_nxt, status);
 }
 
-// The same for the cells next to solid/inflow/outflow cells (compact list `blist`): pull
-// with the persisting populations, TMS boundary treatment, moments.
+// The same for the special cells (compact list): streaming with bounce-back, free-slip
+// and persisting populations, the TMS boundary treatment (reference LBM::TMS_BC), moments.
 __global__ void __launch_bounds__(kBlock)
-    k_sc_stream_moment_bound(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
-                             const long *__restrict__ blist, const double *__restrict__ src,
-                             const double *__restrict__ mom_cur, double *__restrict__ mom_nxt,
-                             const double *__restrict__ bst_cur, double *__restrict__ bst_nxt, long nb,
-                             unsigned *status) {
+    k_sc_stream_moment_special(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const long *__restrict__ blist,
+                               const double *__restrict__ src, const double *__restrict__ mom_cur,
+                               double *__restrict__ mom_nxt, const double *__restrict__ bst_cur,
+                               double *__restrict__ bst_nxt, long nb, unsigned *status) {
     const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
     const long n = blist[b];
     double f[27], ge[27];
-    pull_cell(g, type, cflag[n], n, src, bst_cur + b, nb, f, ge);
+    pull_special(g, type, n, src, bst_cur + b, nb, f, ge);
     tms_cell_sc(g, P, type, mom_cur, n, f, ge);
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
         bst_nxt[(long)l * nb + b] = f[l];
         bst_nxt[(long)(27 + l) * nb + b] = ge[l];
     }
-    store_moments_sc(g, P, n, f, ge, mom_nxt, status);
+    ScSums s;
+    sums_sc(f, ge, s);
+    store_record_sc(g, P, n, s, mom_nxt, status);
 }
 
 // ----------------------------------------------------------------------------------
@@ -226,10 +186,15 @@ __device__ __forceinline__ double geq_moment_diag(int l, double rhoe, const doub
     return val;
 }
 
+__device__ __forceinline__ void put_record_both(double *m0, double *m1, long nc, long n, int field, double v) {
+    m0[(long)field * nc + n] = v;
+    m1[(long)field * nc + n] = v;
+}
+
 __global__ void __launch_bounds__(kBlock)
     k_sc_init(ScGeom g, ScPhys P, const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
               const int *__restrict__ bid, double *__restrict__ pop, double *__restrict__ mom0,
-              double *__restrict__ mom1, double *__restrict__ minit, double *__restrict__ bst, long nb) {
+              double *__restrict__ mom1, double *__restrict__ bst, long nb) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.ncell) return;
     const int t = type[n];
@@ -238,24 +203,25 @@ __global__ void __launch_bounds__(kBlock)
     const double p = mom0[M_P * nc + n];
     const double T = mom0[M_T * nc + n];
     const double rho = p / (P.R * T);
-    mom0[M_RHO * nc + n] = rho;
-    mom1[M_RHO * nc + n] = rho;
+    const double u[3] = {mom0[M_U * nc + n], mom0[M_V * nc + n], mom0[M_W * nc + n]};
+    put_record_both(mom0, mom1, nc, n, M_RHO, rho);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) put_record_both(mom0, mom1, nc, n, M_QX + a, qdev(rho, u[a], T, P.R));
     if (!(cflag[n] & CF_FLUID)) return;
     const double theta = P.R * T;
     const double rhoe = rho * (P.cv * T);
     const double H = P.cp * T;
-    minit[0 * nc + n] = p;
-    minit[1 * nc + n] = 0.0;
-    minit[2 * nc + n] = 0.0;
-    minit[3 * nc + n] = p;
-    minit[4 * nc + n] = 0.0;
-    minit[5 * nc + n] = p;
-    minit[6 * nc + n] = rhoe;
-    const double q[3] = {H * rho * mom0[M_U * nc + n], H * rho * mom0[M_V * nc + n], H * rho * mom0[M_W * nc + n]};
+    const double P6[6] = {p, 0.0, 0.0, p, 0.0, p};
+    double S[3], Uint;
+    coll_inputs(rho, u, p, P6, rhoe, S, Uint);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) put_record_both(mom0, mom1, nc, n, M_SX + a, S[a]);
+    put_record_both(mom0, mom1, nc, n, M_UINT, Uint);
+    const double q[3] = {H * rho * u[0], H * rho * u[1], H * rho * u[2]};
     const double vel0[3] = {0.0, 0.0, 0.0}, zero[3] = {0.0, 0.0, 0.0};
     AxisF<double> F;
     axis_feq(F, vel0, theta, zero);
-    const long b = (cflag[n] & CF_BOUND) ? bid[n] : -1;
+    const long b = (cflag[n] & CF_SPECIAL) ? bid[n] : -1;
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
         const double fv = feq_l(l, rho, F);
@@ -279,27 +245,31 @@ struct MixOff {
 __device__ __forceinline__ double ld(const char *rec, long off) { return *reinterpret_cast<const double *>(rec + off); }
 __device__ __forceinline__ void st(char *rec, long off, double v) { *reinterpret_cast<double *>(rec + off) = v; }
 
-__global__ void k_sc_unpack(ScGeom g, MixOff o, const char *__restrict__ stage, long n0, long n1,
+__global__ void k_sc_unpack(ScGeom g, ScPhys P, MixOff o, const char *__restrict__ stage, long n0, long n1,
                             const uint8_t *__restrict__ cflag, const int *__restrict__ bid, double *__restrict__ pop,
-                            double *__restrict__ mom0, double *__restrict__ mom1, double *__restrict__ minit,
-                            double *__restrict__ bst, long nb) {
+                            double *__restrict__ mom0, double *__restrict__ mom1, double *__restrict__ bst, long nb) {
     const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n1) return;
     const char *rec = stage + (n - n0) * o.size;
     const long nc = g.ncell;
-    const long offs[M_N] = {o.rho, o.u, o.v, o.w, o.temp, o.p};
-#pragma unroll
-    for (int m = 0; m < M_N; ++m) {
-        const double v = ld(rec, offs[m]);
-        mom0[(long)m * nc + n] = v;
-        mom1[(long)m * nc + n] = v;
-    }
+    const double rho = ld(rec, o.rho), T = ld(rec, o.temp), p = ld(rec, o.p);
+    const double u[3] = {ld(rec, o.u), ld(rec, o.v), ld(rec, o.w)};
+    put_record_both(mom0, mom1, nc, n, M_RHO, rho);
+    put_record_both(mom0, mom1, nc, n, M_U, u[0]);
+    put_record_both(mom0, mom1, nc, n, M_V, u[1]);
+    put_record_both(mom0, mom1, nc, n, M_W, u[2]);
+    put_record_both(mom0, mom1, nc, n, M_T, T);
+    put_record_both(mom0, mom1, nc, n, M_P, p);
+    for (int a = 0; a < 3; ++a) put_record_both(mom0, mom1, nc, n, M_QX + a, qdev(rho, u[a], T, P.R));
     if (!(cflag[n] & CF_FLUID)) return;
     const int pi[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-#pragma unroll
-    for (int a = 0; a < 6; ++a) minit[(long)a * nc + n] = ld(rec, o.p_tensor + 8 * (3 * pi[a][0] + pi[a][1]));
-    minit[6 * nc + n] = ld(rec, o.rhoe);
-    const long b = (cflag[n] & CF_BOUND) ? bid[n] : -1;
+    double P6[6];
+    for (int a = 0; a < 6; ++a) P6[a] = ld(rec, o.p_tensor + 8 * (3 * pi[a][0] + pi[a][1]));
+    double S[3], Uint;
+    coll_inputs(rho, u, p, P6, ld(rec, o.rhoe), S, Uint);
+    for (int a = 0; a < 3; ++a) put_record_both(mom0, mom1, nc, n, M_SX + a, S[a]);
+    put_record_both(mom0, mom1, nc, n, M_UINT, Uint);
+    const long b = (cflag[n] & CF_SPECIAL) ? bid[n] : -1;
     for (int l = 0; l < 27; ++l) {
         const double fv = ld(rec, o.f + 8 * l), gv = ld(rec, o.g + 8 * l);
         pop[(long)l * nc + n] = fv;
@@ -311,57 +281,61 @@ __global__ void k_sc_unpack(ScGeom g, MixOff o, const char *__restrict__ stage, 
     }
 }
 
-template <bool LOCAL>
-__global__ void k_sc_pack(ScGeom g, MixOff o, char *__restrict__ stage, long n0, long n1,
+// Pack modes: what the populations in pop[] are and which derived fields to produce.
+enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
+
+template <int MODE>
+__global__ void k_sc_pack(ScGeom g, ScPhys P, MixOff o, char *__restrict__ stage, long n0, long n1,
                           const int8_t *__restrict__ type, const uint8_t *__restrict__ cflag,
                           const int *__restrict__ bid, const double *__restrict__ pop, const double *__restrict__ mom,
-                          const double *__restrict__ minit, const double *__restrict__ bst, long nb) {
+                          const double *__restrict__ bst, long nb) {
     const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n1) return;
     char *rec = stage + (n - n0) * o.size;
     const long nc = g.ncell;
-    const long offs[M_N] = {o.rho, o.u, o.v, o.w, o.temp, o.p};
-#pragma unroll
-    for (int m = 0; m < M_N; ++m) st(rec, offs[m], mom[(long)m * nc + n]);
+    const long offs[6] = {o.rho, o.u, o.v, o.w, o.temp, o.p};
+    const int fld[6] = {M_RHO, M_U, M_V, M_W, M_T, M_P};
+    for (int m = 0; m < 6; ++m) st(rec, offs[m], mom[(long)fld[m] * nc + n]);
     const uint8_t cf = cflag[n];
     if (!(cf & CF_FLUID)) return;
-    double f[27], ge[27];
-    if (LOCAL) {
-        for (int l = 0; l < 27; ++l) {
-            f[l] = pop[(long)l * nc + n];
-            ge[l] = pop[(long)(27 + l) * nc + n];
-        }
-    } else if (cf & CF_BOUND) {
-        const long b = bid[n];
-        for (int l = 0; l < 27; ++l) {
-            f[l] = bst[(long)l * nb + b];
-            ge[l] = bst[(long)(27 + l) * nb + b];
-        }
-    } else {
-        pull_cell(g, type, cf, n, pop, (const double *)nullptr, 0, f, ge);
-    }
+    const bool special = cf & CF_SPECIAL;
+    PullSrc ps;
+    if (MODE == PK_STEPPED && !special) pull_src(g, n, ps);
+    const long b = special ? (long)bid[n] : 0;
+    ScSums s;
+    sums_init(s);
     for (int l = 0; l < 27; ++l) {
-        st(rec, o.f + 8 * l, f[l]);
-        st(rec, o.g + 8 * l, ge[l]);
-        if (!LOCAL) {
+        double fv, gv;
+        if (MODE != PK_STEPPED) {
+            fv = pop[(long)l * nc + n];
+            gv = pop[(long)(27 + l) * nc + n];
+        } else if (special) {
+            fv = bst[(long)l * nb + b];
+            gv = bst[(long)(27 + l) * nb + b];
+        } else {
+            const long sidx = pull_at(ps, l);
+            fv = pop[(long)l * nc + sidx];
+            gv = pop[(long)(27 + l) * nc + sidx];
+        }
+        st(rec, o.f + 8 * l, fv);
+        st(rec, o.g + 8 * l, gv);
+        if (MODE == PK_STEPPED) {
             st(rec, o.fpc + 8 * l, pop[(long)l * nc + n]);
             st(rec, o.gpc + 8 * l, pop[(long)(27 + l) * nc + n]);
+            sums_add(s, l, fv, gv);
         }
     }
-    double Pt[6], re;
-    if (LOCAL) {
-        for (int a = 0; a < 6; ++a) Pt[a] = minit[(long)a * nc + n];
-        re = minit[6 * nc + n];
-    } else {
-        ScSums s;
-        sums_sc(f, ge, s);
-        for (int a = 0; a < 6; ++a) Pt[a] = s.P[a];
-        re = s.re;
-        for (int a = 0; a < 3; ++a) st(rec, o.energy_flux + 8 * a, s.q[a]);
-    }
     const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-    for (int a = 0; a < 9; ++a) st(rec, o.p_tensor + 8 * a, Pt[full[a]]);
-    st(rec, o.rhoe, re);
+    if (MODE == PK_STEPPED) {
+        for (int a = 0; a < 9; ++a) st(rec, o.p_tensor + 8 * a, s.P[full[a]]);
+        st(rec, o.rhoe, s.re);
+        for (int a = 0; a < 3; ++a) st(rec, o.energy_flux + 8 * a, s.q[a]);
+    } else if (MODE == PK_INIT) {
+        // Init leaves p_tensor = p I and rhoe = rho cv T (src/lbm-init.cpp:30-43)
+        const double p = mom[M_P * nc + n], rho = mom[M_RHO * nc + n], T = mom[M_T * nc + n];
+        for (int a = 0; a < 9; ++a) st(rec, o.p_tensor + 8 * a, (a % 4 == 0) ? p : 0.0);
+        st(rec, o.rhoe, rho * (P.cv * T));
+    }
 }
 
 // ----------------------------------------------------------------------------------
@@ -390,14 +364,13 @@ struct lbmgpu {
     long nb = 0;
     double *pop[2] = {nullptr, nullptr};
     double *mom[2] = {nullptr, nullptr};
-    double *minit = nullptr;
     double *bst[2] = {nullptr, nullptr};
     unsigned *status = nullptr;
     char *stage = nullptr;
     size_t stage_cells = 0;
     char *bounce = nullptr;  // pinned host bounce buffer for downloads
     int cur = 0;
-    bool local = true;
+    int pack_mode = PK_UPLOADED;  // what pop[cur] holds (uploaded / Init / stepped)
     bool have_state = false;
     int phase = PH_BOUNDARY;
     bool prof = false;
@@ -468,14 +441,12 @@ int launch_collide(lbmgpu *h) {
     const int c = h->cur, x = 1 - c;
     EvPair ep{};
     ev_begin(h, K_COLLIDE, ep);
-    if (h->local)
+    if (h->pack_mode != PK_STEPPED)
         k_sc_collide<true><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(
-            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->minit, h->bst[c], h->nb,
-            h->status);
+            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->bst[c], h->nb, h->status);
     else
         k_sc_collide<false><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(
-            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->minit, h->bst[c], h->nb,
-            h->status);
+            h->g, h->P, h->type, h->cflag, h->bid, h->pop[c], h->pop[x], h->mom[c], h->bst[c], h->nb, h->status);
     ev_end(h, ep);
     CK(cudaGetLastError());
     return 0;
@@ -485,22 +456,20 @@ int launch_stream_moment(lbmgpu *h) {
     const int c = h->cur, x = 1 - c;
     EvPair ep{};
     ev_begin(h, K_STREAM_MOMENT, ep);
-    k_sc_stream_moment<<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(h->g, h->P, h->type, h->cflag, h->bid,
-                                                                        h->pop[x], h->mom[c], h->mom[x], h->bst[c],
-                                                                        h->bst[x], h->nb, h->status);
+    k_sc_stream_moment<<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(h->g, h->P, h->cflag, h->pop[x],
+                                                                        h->mom[x], h->status);
     ev_end(h, ep);
     CK(cudaGetLastError());
     if (h->nb > 0) {
         EvPair eb{};
         ev_begin(h, K_OTHER, eb);
-        k_sc_stream_moment_bound<<<grid_for(h->nb), kBlock, 0, h->stream>>>(
-            h->g, h->P, h->type, h->cflag, h->blist, h->pop[x], h->mom[c], h->mom[x], h->bst[c], h->bst[x], h->nb,
-            h->status);
+        k_sc_stream_moment_special<<<grid_for(h->nb), kBlock, 0, h->stream>>>(
+            h->g, h->P, h->type, h->blist, h->pop[x], h->mom[c], h->mom[x], h->bst[c], h->bst[x], h->nb, h->status);
         ev_end(h, eb);
         CK(cudaGetLastError());
     }
     h->cur = x;
-    h->local = false;
+    h->pack_mode = PK_STEPPED;
     return 0;
 }
 
@@ -550,6 +519,7 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
         desc->dt_sim <= 0)
         return LBMGPU_E_ARG;
     if (!valid_layout(desc->mix)) return LBMGPU_E_ARG;
+    if ((double)desc->Nx * desc->Ny * desc->Nz > 2147483647.0) return LBMGPU_E_UNSUPPORTED;  // 32-bit cell offsets
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
         (void)cudaGetLastError();
@@ -585,7 +555,6 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     if (!rc) rc = dalloc(h, &h->bid, nc);
     for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->pop[b], 54 * (size_t)nc);
     for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->mom[b], (size_t)M_N * nc);
-    if (!rc) rc = dalloc(h, &h->minit, 7 * (size_t)nc);
     if (!rc) rc = dalloc(h, &h->status, 1);
     if (!rc) {
         e = cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream);
@@ -626,7 +595,6 @@ int lbmgpu_destroy(lbmgpu_t *h) {
         cudaFree(h->mom[b]);
         cudaFree(h->bst[b]);
     }
-    cudaFree(h->minit);
     cudaFree(h->status);
     cudaFree(h->stage);
     if (h->bounce) cudaFreeHost(h->bounce);
@@ -662,17 +630,16 @@ int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos) {
                 if (ty[n] != T_F) continue;
                 if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
                     return LBMGPU_E_ARG;  // a fluid cell on the outermost layer has no ghost neighbour
+                // special: a boundary cell upstream (solid, adiabatic, free-slip, inflow,
+                // outflow); the others stream with the branch-free periodic pull
                 uint8_t c = CF_FLUID;
                 for (int l = 0; l < 27; ++l) {
                     const long s = n - (long)cx(l) * g.si - (long)cy(l) * g.sj - cz(l);
                     const int t = ty[s];
-                    if (t != T_F) c |= CF_SLOW;
-                    if (t == T_S || t == T_I || t == T_O || t == T_I_C || t == T_O_C) c |= CF_BOUND;
-                    const int si = i - cx(l), sj = j - cy(l), sk = k - cz(l);
-                    if (si == 0 || sj == 0 || sk == 0 || si == g.Nx - 1 || sj == g.Ny - 1 || sk == g.Nz - 1)
-                        c |= CF_SLOW;
+                    if (t == T_S || t == T_A || t == T_FS || t == T_I || t == T_O || t == T_I_C || t == T_O_C)
+                        c |= CF_SPECIAL;
                 }
-                if (c & CF_BOUND) {
+                if (c & CF_SPECIAL) {
                     bidh[n] = (int)nb++;
                     blh.push_back(n);
                 }
@@ -710,14 +677,14 @@ int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos) {
         CK(cudaMemcpyAsync(h->stage, host + n0 * rs, (n1 - n0) * rs, cudaMemcpyHostToDevice, h->stream));
         EvPair ep{};
         ev_begin(h, K_OTHER, ep);
-        k_sc_unpack<<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->cflag, h->bid,
-                                                                 h->pop[0], h->mom[0], h->mom[1], h->minit, h->bst[0],
+        k_sc_unpack<<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->P, h->mo, h->stage, n0, n1, h->cflag,
+                                                                 h->bid, h->pop[0], h->mom[0], h->mom[1], h->bst[0],
                                                                  h->nb);
         ev_end(h, ep);
         CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(h->stream));
-    h->local = true;
+    h->pack_mode = PK_UPLOADED;
     h->have_state = true;
     h->phase = PH_BOUNDARY;
     return LBMGPU_OK;
@@ -736,19 +703,22 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos) {
     CK(cudaMemcpyAsync(ty.data(), h->type, nc, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     const int c = h->cur;
-    const long mof[M_N] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.temp, h->mo.p};
+    const long mof[6] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.temp, h->mo.p};
     for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
         const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells);
         EvPair ep{};
         ev_begin(h, K_OTHER, ep);
-        if (h->local)
-            k_sc_pack<true><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->type,
-                                                                         h->cflag, h->bid, h->pop[c], h->mom[c],
-                                                                         h->minit, h->bst[c], h->nb);
+        const unsigned gb = grid_for(n1 - n0);
+        if (h->pack_mode == PK_STEPPED)
+            k_sc_pack<PK_STEPPED><<<gb, kBlock, 0, h->stream>>>(g, h->P, h->mo, h->stage, n0, n1, h->type, h->cflag,
+                                                                h->bid, h->pop[c], h->mom[c], h->bst[c], h->nb);
+        else if (h->pack_mode == PK_INIT)
+            k_sc_pack<PK_INIT><<<gb, kBlock, 0, h->stream>>>(g, h->P, h->mo, h->stage, n0, n1, h->type, h->cflag,
+                                                             h->bid, h->pop[c], h->mom[c], h->bst[c], h->nb);
         else
-            k_sc_pack<false><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(g, h->mo, h->stage, n0, n1, h->type,
-                                                                          h->cflag, h->bid, h->pop[c], h->mom[c],
-                                                                          h->minit, h->bst[c], h->nb);
+            k_sc_pack<PK_UPLOADED><<<gb, kBlock, 0, h->stream>>>(g, h->P, h->mo, h->stage, n0, n1, h->type,
+                                                                 h->cflag, h->bid, h->pop[c], h->mom[c], h->bst[c],
+                                                                 h->nb);
         ev_end(h, ep);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h->bounce, h->stage, (n1 - n0) * rs, cudaMemcpyDeviceToHost, h->stream));
@@ -758,17 +728,22 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos) {
         for (long n = n0; n < n1; ++n) {
             const char *srec = h->bounce + (n - n0) * rs;
             char *drec = host + n * rs;
-            if (ty[n] == T_F) {
-                const size_t skip = (h->mo.type == 0) ? 8 : 0;
-                if (skip) std::memcpy(drec + skip, srec + skip, rs - skip);
-                else {
-                    short t;
-                    std::memcpy(&t, drec + h->mo.type, sizeof(short));
-                    std::memcpy(drec, srec, rs);
-                    std::memcpy(drec + h->mo.type, &t, sizeof(short));
-                }
+            if (ty[n] == T_F && h->pack_mode == PK_STEPPED) {
+                // every field of a stepped fluid cell was produced: the whole record but the type
+                short t;
+                std::memcpy(&t, drec + h->mo.type, sizeof(short));
+                std::memcpy(drec, srec, rs);
+                std::memcpy(drec + h->mo.type, &t, sizeof(short));
             } else {
-                for (int m = 0; m < M_N; ++m) std::memcpy(drec + mof[m], srec + mof[m], sizeof(double));
+                for (int m = 0; m < 6; ++m) std::memcpy(drec + mof[m], srec + mof[m], sizeof(double));
+                if (ty[n] == T_F) {
+                    std::memcpy(drec + h->mo.f, srec + h->mo.f, 27 * sizeof(double));
+                    std::memcpy(drec + h->mo.g, srec + h->mo.g, 27 * sizeof(double));
+                    if (h->pack_mode == PK_INIT) {
+                        std::memcpy(drec + h->mo.p_tensor, srec + h->mo.p_tensor, 9 * sizeof(double));
+                        std::memcpy(drec + h->mo.rhoe, srec + h->mo.rhoe, sizeof(double));
+                    }
+                }
             }
         }
     }
@@ -790,10 +765,10 @@ int lbmgpu_init(lbmgpu_t *h) {
     EvPair ep{};
     ev_begin(h, K_OTHER, ep);
     k_sc_init<<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(h->g, h->P, h->type, h->cflag, h->bid, h->pop[0],
-                                                              h->mom[0], h->mom[1], h->minit, h->bst[0], h->nb);
+                                                              h->mom[0], h->mom[1], h->bst[0], h->nb);
     ev_end(h, ep);
     CK(cudaGetLastError());
-    h->local = true;
+    h->pack_mode = PK_INIT;
     return LBMGPU_OK;
 }
 

@@ -1,0 +1,186 @@
+"""Loader of the repository's Cantera-YAML gas mechanisms into the flat ``lbmgpu_mech``
+tables of include/lbmgpu.h (SI units: kmol, m, s, J, K).
+
+It replaces ``Cantera::newSolution(file, phase)`` (reference src/lbm-main.cpp:84) for the
+subset of the YAML format the reference's mechanisms use (src/reaction-mech/*.yaml, written
+by Cantera 3.0.0's ck2yaml): ``ideal-gas`` thermo with NASA-7 polynomials, ``gas``
+transport parameters, and elementary / ``three-body`` / ``falloff`` (Lindemann and Troe)
+reactions with optional ``duplicate`` and ``efficiencies`` entries.
+
+``load(path, species)`` extracts the listed species, keeps the reactions closed over them
+and drops third-body efficiencies of absent species (the reference's 9-species H2/O2/N2
+set comes from nh3.yaml this way).
+"""
+import ctypes
+import re
+
+import yaml
+
+MAX_SPECIES = 12
+MAX_REACTIONS = 48
+MAX_RSPEC = 3
+RXN_ELEMENTARY, RXN_THREEBODY, RXN_FALLOFF = 0, 1, 2
+GEOM = {"atom": 0, "linear": 1, "nonlinear": 2}
+
+# IUPAC standard atomic weights (kg/kmol) of the elements these mechanisms contain
+ATOMIC_WEIGHT = {"H": 1.008, "O": 15.999, "N": 14.007, "Ar": 39.95, "He": 4.002602, "C": 12.011}
+ELEMENT_SLOT = {"H": 0, "O": 1, "N": 2, "Ar": 3}
+DEBYE = 3.33564e-30          # C m
+CAL = 4.184                  # J
+
+H2_AIR_9 = ["H2", "H", "O2", "O", "H2O", "OH", "H2O2", "HO2", "N2"]
+
+
+class Mech(ctypes.Structure):
+    S, R, K = MAX_SPECIES, MAX_REACTIONS, MAX_RSPEC
+    _fields_ = [
+        ("n_species", ctypes.c_int), ("n_reactions", ctypes.c_int),
+        ("name", (ctypes.c_char * 16) * S),
+        ("W", ctypes.c_double * S),
+        ("T_lo", ctypes.c_double * S), ("T_mid", ctypes.c_double * S), ("T_hi", ctypes.c_double * S),
+        ("nasa_lo", (ctypes.c_double * 7) * S), ("nasa_hi", (ctypes.c_double * 7) * S),
+        ("geometry", ctypes.c_int * S),
+        ("well_depth", ctypes.c_double * S), ("diameter", ctypes.c_double * S),
+        ("dipole", ctypes.c_double * S), ("polarizability", ctypes.c_double * S),
+        ("rot_relax", ctypes.c_double * S),
+        ("elements", (ctypes.c_int * 4) * S),
+        ("rtype", ctypes.c_int * R), ("reversible", ctypes.c_int * R),
+        ("n_reac", ctypes.c_int * R), ("n_prod", ctypes.c_int * R),
+        ("reac", (ctypes.c_int * K) * R), ("prod", (ctypes.c_int * K) * R),
+        ("nu_reac", (ctypes.c_double * K) * R), ("nu_prod", (ctypes.c_double * K) * R),
+        ("A", ctypes.c_double * R), ("b", ctypes.c_double * R), ("Ea", ctypes.c_double * R),
+        ("A0", ctypes.c_double * R), ("b0", ctypes.c_double * R), ("Ea0", ctypes.c_double * R),
+        ("troe_n", ctypes.c_int * R), ("troe", (ctypes.c_double * 4) * R),
+        ("eff", (ctypes.c_double * S) * R),
+    ]
+
+    def species_names(self):
+        return [self.name[k].value.decode() for k in range(self.n_species)]
+
+
+def _parse_side(side):
+    """'H2O2 (+M)' / 'O + O + M' / '2 OH' -> ({species: coefficient}, third_body_kind)."""
+    tb = None
+    side = side.strip()
+    if re.search(r"\(\+\s*M\s*\)", side):
+        tb = "falloff"
+        side = re.sub(r"\(\+\s*M\s*\)", "", side)
+    out = {}
+    for tok in side.split(" + "):
+        tok = tok.strip()
+        if not tok:
+            continue
+        if tok == "M":
+            tb = tb or "three-body"
+            continue
+        m = re.match(r"^(\d+(?:\.\d+)?)\s+(\S+)$", tok) or re.match(r"^(\d+(?:\.\d+)?)(\S+)$", tok)
+        if m and not tok[0].isalpha():
+            nu, sp = float(m.group(1)), m.group(2)
+        else:
+            nu, sp = 1.0, tok
+        out[sp] = out.get(sp, 0.0) + nu
+    return out, tb
+
+
+def _convert_A(A, order, conc_factor):
+    # (cm^3/mol)^(order-1) / s  ->  (m^3/kmol)^(order-1) / s
+    return A * conc_factor ** (order - 1)
+
+
+def load(path, species=H2_AIR_9):
+    """Reads a Cantera-YAML mechanism and returns a filled ``Mech`` for `species`."""
+    doc = yaml.safe_load(open(path))
+    units = doc.get("units", {})
+    length = {"cm": 1e-2, "m": 1.0}[units.get("length", "m")]
+    qty = {"mol": 1e-3, "kmol": 1.0}[units.get("quantity", "kmol")]
+    conc_factor = length ** 3 / qty          # 1 cm^3/mol = 1e-3 m^3/kmol
+    ea_unit = units.get("activation-energy", "J/kmol")
+    ea_factor = {"cal/mol": CAL * 1e3, "kcal/mol": CAL * 1e6, "J/mol": 1e3, "J/kmol": 1.0}[ea_unit]
+
+    if len(species) > MAX_SPECIES:
+        raise ValueError("too many species")
+    by_name = {s["name"]: s for s in doc["species"]}
+    m = Mech()
+    m.n_species = len(species)
+    idx = {}
+    for k, name in enumerate(species):
+        if name not in by_name:
+            raise KeyError(f"species {name} is not in {path}")
+        s = by_name[name]
+        idx[name] = k
+        m.name[k].value = name.encode()
+        comp = s["composition"]
+        m.W[k] = sum(ATOMIC_WEIGHT[e] * n for e, n in comp.items())
+        for e, n in comp.items():
+            if e in ELEMENT_SLOT:
+                m.elements[k][ELEMENT_SLOT[e]] = int(n)
+        th = s["thermo"]
+        if th["model"] != "NASA7":
+            raise ValueError(f"{name}: only NASA7 thermo is supported")
+        tr_ = th["temperature-ranges"]
+        m.T_lo[k], m.T_mid[k], m.T_hi[k] = tr_[0], tr_[1], tr_[-1]
+        for j in range(7):
+            m.nasa_lo[k][j] = th["data"][0][j]
+            m.nasa_hi[k][j] = th["data"][1][j] if len(th["data"]) > 1 else th["data"][0][j]
+        tp = s.get("transport", {})
+        m.geometry[k] = GEOM[tp.get("geometry", "atom")]
+        m.well_depth[k] = tp.get("well-depth", 0.0)
+        m.diameter[k] = tp.get("diameter", 0.0) * 1e-10
+        m.dipole[k] = tp.get("dipole", 0.0) * DEBYE
+        m.polarizability[k] = tp.get("polarizability", 0.0) * 1e-30
+        m.rot_relax[k] = tp.get("rotational-relaxation", 0.0)
+
+    nr = 0
+    for r in doc.get("reactions", []):
+        eq = r["equation"]
+        rev = "<=>" in eq or ("=" in eq and "=>" not in eq)
+        lhs, rhs = re.split(r"<=>|=>|=", eq, maxsplit=1)
+        reac, tb1 = _parse_side(lhs)
+        prod, tb2 = _parse_side(rhs)
+        if not (set(reac) | set(prod)) <= set(species):
+            continue
+        if nr >= MAX_REACTIONS:
+            raise ValueError("too many reactions")
+        kind = r.get("type", "elementary")
+        if kind not in ("elementary", "three-body", "falloff"):
+            raise ValueError(f"reaction type {kind} not supported: {eq}")
+        if len(reac) > MAX_RSPEC or len(prod) > MAX_RSPEC:
+            raise ValueError(f"too many species in {eq}")
+        m.rtype[nr] = {"elementary": RXN_ELEMENTARY, "three-body": RXN_THREEBODY, "falloff": RXN_FALLOFF}[kind]
+        m.reversible[nr] = int(rev)
+        m.n_reac[nr] = len(reac)
+        m.n_prod[nr] = len(prod)
+        for j, (sp, nu) in enumerate(reac.items()):
+            m.reac[nr][j] = idx[sp]
+            m.nu_reac[nr][j] = nu
+        for j, (sp, nu) in enumerate(prod.items()):
+            m.prod[nr][j] = idx[sp]
+            m.nu_prod[nr][j] = nu
+        order = sum(reac.values())
+        if kind == "falloff":
+            hi, lo = r["high-P-rate-constant"], r["low-P-rate-constant"]
+            m.A[nr] = _convert_A(hi["A"], order, conc_factor)
+            m.b[nr] = hi["b"]
+            m.Ea[nr] = hi["Ea"] * ea_factor
+            m.A0[nr] = _convert_A(lo["A"], order + 1, conc_factor)
+            m.b0[nr] = lo["b"]
+            m.Ea0[nr] = lo["Ea"] * ea_factor
+            if "Troe" in r:
+                t = r["Troe"]
+                vals = [t["A"], t["T3"], t["T1"]] + ([t["T2"]] if "T2" in t else [])
+                m.troe_n[nr] = len(vals)
+                for j, v in enumerate(vals):
+                    m.troe[nr][j] = v
+        else:
+            rc = r["rate-constant"]
+            m.A[nr] = _convert_A(rc["A"], order + (1 if kind == "three-body" else 0), conc_factor)
+            m.b[nr] = rc["b"]
+            m.Ea[nr] = rc["Ea"] * ea_factor
+        for k in range(m.n_species):
+            m.eff[nr][k] = 1.0 if kind in ("three-body", "falloff") else 0.0
+        for sp, e in r.get("efficiencies", {}).items():
+            if sp in idx:
+                m.eff[nr][idx[sp]] = e
+        nr += 1
+    m.n_reactions = nr
+    return m
