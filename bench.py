@@ -52,7 +52,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--N", type=int, default=64, help="interior cells per axis")
+    ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
+    ap.add_argument("--workload", choices=["tgv", "mix", "react"], default="tgv",
+                    help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
+                         "mix: 9-species H2/air mixing layer, FP64, periodic (config 2 without its NSCBC "
+                         "faces, 128^3); react: the same with the reference's explicit chemistry and a "
+                         "1800 K slab")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -244,6 +249,132 @@ def run_reference(args, dist):
     print(json.dumps(line), flush=True)
 
 
+MC_BYTES_STEP_FP64 = 2 * 27 * 10 * 8 + 16  # one read + one write of 270 populations + T (FP64)
+
+
+def mc_workload(args):
+    import mech
+    import workloads
+    m = mech.h2_air_9()
+    kw = {"T_hi": 1800.0} if args.workload == "react" else {}
+    mix, sp = workloads.mixing_layer_mc(m, N=args.N, **kw)
+    return m, mix, sp
+
+
+def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
+    """The reference's own multicomponent solver on the Cantera-API shim (oracle/_ref)."""
+    import workloads
+    from oracle import refmc
+    refmc.set_threads(threads, reaction)
+    N3 = [s_ - 2 for s_ in mix.shape]
+    ref = refmc.RefMC(*N3, m, workloads.FLAME_UNITS, workloads.MIXTURE_MC, workloads.SPECIES, reaction=reaction)
+    ref.cells[...] = mix
+    for a in range(len(sp)):
+        ref.species[a][...] = sp[a]
+    ref.init()
+    if warmup:
+        ref.loop(warmup)
+    t0 = time.perf_counter()
+    ref.loop(steps)
+    dt = time.perf_counter() - t0
+    ref.close()
+    return dt
+
+
+def run_ours_mc(args, dist):
+    import numpy as np
+
+    import lbmgpu
+    import workloads
+    device = dist.local
+    reaction = args.workload == "react"
+    m, mix, sp = mc_workload(args)
+    ncell = fluid_cells(mix)
+    chem = lbmgpu.CHEM_REF_EXPLICIT if reaction else lbmgpu.CHEM_OFF
+
+    def lattice():
+        return lbmgpu.Lattice(*mix.shape, mech=m, dtype=workloads.MIXTURE_MC, species_dtype=workloads.SPECIES,
+                              dx_dt=workloads.FLAME_UNITS, chem=chem, device=device)
+
+    lat = lattice()
+    lat.upload(mix, sp)
+    lat.init()
+    lat.time_steps(max(3, args.warmup))
+    dist.barrier()
+    clk = Clocks(device)
+    clk.start()
+    ms = lat.time_steps(args.steps)
+    clocks = clk.stop()
+    status = lat.synchronize()
+    ms = dist.max(ms)
+    kk = min(args.steps, 20)
+    lat.profile(True)
+    lat.time_steps(kk)
+    launches, kms = lat.kernel_times()
+    lat.profile(False)
+    lat.close()
+    avg = {"k_mc_collide": kms[0] / max(launches[0], 1), "k_mc_stream": kms[1] / max(launches[1], 1)}
+    dom = max(avg, key=avg.get)
+    per_cell = {"k_mc_collide": 2 * 27 * 10 * 8, "k_mc_stream": 27 * 10 * 8 + 16 * 8}[dom]
+    alg = per_cell * ncell
+    peak, peak_kind = peaks()
+    achieved = alg / (avg[dom] * 1e-3) / 1e9
+
+    # end to end: upload, Init, phase calls, one AoS download (the reference's flame
+    # setups write output every 1000 steps, setup.cpp:2852)
+    hm = mix.copy()
+    hs = [a.copy() for a in sp]
+    lat = lattice()
+    dist.barrier()
+    t0 = time.perf_counter()
+    lat.upload(hm, hs)
+    lat.init()
+    for s_ in range(args.steps):
+        lat.collide_species()
+        lat.collide()
+        lat.streaming()
+        lat.tms_bc()
+        lat.calculate_moment()
+    lat.synchronize()
+    lat.download(hm, hs)
+    wall = dist.max(time.perf_counter() - t0)
+    lat.close()
+    nbytes = mix.nbytes + sum(a.nbytes for a in sp)
+    e2e = {"value": dist.world * ncell * args.steps / wall / 1e6, "unit": "MLUPS",
+           "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+           "note": "AoS upload + Init, phase calls per step, one AoS download"}
+    if dist.rank != 0:
+        return
+    value = dist.world * ncell * args.steps / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
+        "config": {"workload": f"{args.workload}{args.N}_mc9_fp64: 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
+                               f"dx 20 um, dt 1 ns, " + ("reference explicit chemistry" if reaction else "non-reacting"),
+                   "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush"},
+        "hbm_gbs_step": ncell * MC_BYTES_STEP_FP64 / (ms / args.steps * 1e-3) / 1e9,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": ncu_traffic(dom), "peak_source": f"{peak_kind} hbm_gbs",
+                     "alg_bytes_per_launch": alg, "mean_launch_ms": avg[dom], "kernel_ms": avg},
+        "gpu_launches": int(round((launches[0] + launches[1] + launches[2]) / kk * args.steps)),
+        "status": status, "clocks": clocks, "e2e": e2e,
+    }
+    if dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = os.cpu_count() or 1
+            n = 3
+            dt = mc_cpu_run(m, mix, sp, n, 1, threads, reaction)
+            line["cpu_baseline"] = {"value": ncell * n / dt / 1e6, "unit": "MLUPS", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"{n} steps after 1 warm-up step, reference multicomponent LBM + "
+                                              f"Cantera-API shim, {threads} OpenMP threads, {dt:.1f} s"}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, dist):
     import numpy as np
 
@@ -350,12 +481,16 @@ def run_ours(args, dist):
 
 def main():
     args = parse()
+    if args.N is None:
+        args.N = 64 if args.workload == "tgv" else 128
     dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)
-        else:
+        elif args.workload == "tgv":
             run_ours(args, dist)
+        else:
+            run_ours_mc(args, dist)
     finally:
         dist.close()
 

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define LBMGPU_ABI_VERSION 1
+#define LBMGPU_ABI_VERSION 2
 
 /* ---- error codes ------------------------------------------------------------- */
 #define LBMGPU_OK 0
@@ -40,6 +40,7 @@ extern "C" {
 #define LBMGPU_ST_NEG_STATE 0x2u    /* density or temperature <= 0                     */
 #define LBMGPU_ST_TAU_UNSTABLE 0x4u /* 1/omega <= 1/2 (the reference prints these:
                                        src/lbm-collision.cpp:33-34)                   */
+#define LBMGPU_ST_NEWTON 0x8u       /* temperature Newton iteration hit its cap        */
 
 /* ---- precision of the population storage ------------------------------------- */
 #define LBMGPU_FP64 0
@@ -92,6 +93,18 @@ typedef struct lbmgpu_mixture_layout {
     long type, f, fpc, p_tensor, rho, u, v, w, p, g, gpc, rhoe, energy_flux, temp, HRR;
 } lbmgpu_mixture_layout;
 
+/* Byte offsets of the caller's SPECIES record (src/headers/lbm.hpp:90-102). */
+typedef struct lbmgpu_species_layout {
+    size_t size;
+    long X, rho, f, fpc, u, v, w;
+} lbmgpu_species_layout;
+
+/* Chemistry of the species collision (multicomponent). */
+#define LBMGPU_CHEM_OFF 0           /* REACTION off                                     */
+#define LBMGPU_CHEM_REF_EXPLICIT 1  /* the reference's scheme: two explicit half steps of
+                                       the net production rates with T from (u, v) in
+                                       between (src/lbm-collision.cpp:370-399)          */
+
 typedef struct lbmgpu_desc {
     int abi_version;      /* LBMGPU_ABI_VERSION                                           */
     int device;           /* CUDA device ordinal                                          */
@@ -104,6 +117,12 @@ typedef struct lbmgpu_desc {
     double gamma;         /* cp/cv (lbm.hpp:119)                                          */
     double prtl;          /* Prandtl number (lbm.hpp:121)                                 */
     lbmgpu_mixture_layout mix;
+    /* multicomponent (n_species > 0) */
+    lbmgpu_species_layout spc;
+    const lbmgpu_mech *mech;  /* species in the LBM's order; copied at create            */
+    float units_m, units_kg, units_s, units_K; /* the caller's Units_Conv base units
+                                                  (src/headers/units.hpp:10)             */
+    int chem_mode;            /* LBMGPU_CHEM_*                                           */
 } lbmgpu_desc;
 
 typedef struct lbmgpu lbmgpu_t;
@@ -113,18 +132,25 @@ typedef struct lbmgpu lbmgpu_t;
 int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out);
 int lbmgpu_destroy(lbmgpu_t *h);
 
-/* Copies the caller's AoS cell array (LBM::mixture_data, lbm.hpp:134; Nx*Ny*Nz records in
- * the reference's [i][j][k] order, k fastest) to the device: cell types, populations and
- * moments.  The next Collide uses the uploaded populations and moments as they stand,
- * exactly as the reference's first step after Init or read_restart does. */
-int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos);
+/* Copies the caller's AoS cell arrays to the device: the mixture records
+ * (LBM::mixture_data, lbm.hpp:134) and, multicomponent, one species array per species
+ * (LBM::species_data[a], lbm.hpp:136; NULL when single component).  Nx*Ny*Nz records
+ * each, in the reference's [i][j][k] order, k fastest.  The next Collide uses the
+ * uploaded populations and moments as they stand, exactly as the reference's first step
+ * after Init or read_restart does. */
+int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos, const void *const *species_aos);
 
-/* Writes the current state back into the caller's AoS array at a step boundary:
- * populations f, g (post-stream, post-boundary), fpc, gpc (post-collision) and the
- * moments of every fluid cell; the stored moments (rho, u, v, w, p, temp) of every cell. */
-int lbmgpu_download(lbmgpu_t *h, void *mixture_aos);
+/* Writes the current state back into the caller's AoS arrays at a step boundary:
+ * populations (post-stream, post-boundary), post-collision populations and moments of
+ * every fluid cell; the stored moments of every other cell. */
+int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos);
 
-/* LBM::Init (src/lbm-init.cpp:8-82) on the uploaded setup fields. */
+/* The base units units.set_m_kg_s(dx, dt) sets (src/headers/units.hpp:32-44), with its
+ * float rounding: out = {m, kg, s, K}. */
+int lbmgpu_units_from_dx_dt(float dx, float dt, float *out4);
+
+/* LBM::Init (src/lbm-init.cpp:8-82 single component, :85-146 multicomponent) on the
+ * uploaded setup fields. */
 int lbmgpu_init(lbmgpu_t *h);
 
 /* The reference's per-step phases, called in its order (src/lbm-main.cpp:157-181).

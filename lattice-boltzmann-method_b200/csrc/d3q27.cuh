@@ -2,6 +2,14 @@
 #pragma once
 #include <cstdint>
 
+// The per-cell functions are also built for the host (tests); there the CUDA execution
+// space qualifiers are empty.
+#if !defined(__CUDACC__) && !defined(__host__)
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
 namespace lbm {
 
 // Cell-type codes, identical to the reference's (src/headers/defines.hpp:140-149): the
@@ -36,7 +44,7 @@ struct AxisF {
 };
 
 template <typename R>
-__device__ __forceinline__ void axis_feq(AxisF<R> &F, const R u[3], R theta, const R corr[3]) {
+__host__ __device__ __forceinline__ void axis_feq(AxisF<R> &F, const R u[3], R theta, const R corr[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const R z = theta + u[a] * u[a] + corr[a];
@@ -47,7 +55,7 @@ __device__ __forceinline__ void axis_feq(AxisF<R> &F, const R u[3], R theta, con
 }
 
 template <typename R>
-__device__ __forceinline__ R feq_l(int l, R rho, const AxisF<R> &F) {
+__host__ __device__ __forceinline__ R feq_l(int l, R rho, const AxisF<R> &F) {
     return rho * F.v[0][cidx(cx(l))] * F.v[1][cidx(cy(l))] * F.v[2][cidx(cz(l))];
 }
 
@@ -64,7 +72,7 @@ struct AxisG {
 };
 
 template <typename R>
-__device__ __forceinline__ void axis_geq(AxisG<R> &G, R U, R theta, const R u[3]) {
+__host__ __device__ __forceinline__ void axis_geq(AxisG<R> &G, R U, R theta, const R u[3]) {
     G.E = U + R(0.5) * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -81,7 +89,7 @@ __device__ __forceinline__ void axis_geq(AxisG<R> &G, R U, R theta, const R u[3]
 }
 
 template <typename R>
-__device__ __forceinline__ R geq_l(int l, R rho, const AxisG<R> &G) {
+__host__ __device__ __forceinline__ R geq_l(int l, R rho, const AxisG<R> &G) {
     const int ix = cidx(cx(l)), iy = cidx(cy(l)), iz = cidx(cz(l));
     const R px = G.P[0][ix], py = G.P[1][iy], pz = G.P[2][iz];
     const R r = G.E * px * py * pz + G.A[0][ix] * py * pz + px * G.A[1][iy] * pz + px * py * G.A[2][iz];

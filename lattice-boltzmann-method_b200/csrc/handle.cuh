@@ -1,0 +1,141 @@
+// The lbmgpu handle: device state of one LBM object plus the host-side helpers shared by
+// the single-component (lbmgpu.cu) and multicomponent (mc.cu) translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/lbmgpu.h"
+#include "gas.cuh"
+#include "sc_kernels.cuh"
+#include "units.cuh"
+
+namespace lbmh {
+
+constexpr int kBlock = 128;
+
+enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SPECIES = 4 };
+enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_NKINDS = 3 };
+// What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
+// values after at least one step.
+enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
+
+struct EvPair {
+    cudaEvent_t a, b;
+    int kind;
+};
+
+// Byte offsets of the caller's MIXTURE fields (-1: absent).
+struct MixOff {
+    long size, type, f, fpc, p_tensor, rho, u, v, w, p, g, gpc, rhoe, energy_flux, temp, HRR;
+};
+struct SpOff {
+    long size, X, rho, f, fpc, u, v, w;
+};
+
+}  // namespace lbmh
+
+struct lbmgpu {
+    lbmgpu_desc d{};
+    cudaStream_t stream = nullptr;
+    lbm::ScGeom g{};
+    lbm::ScPhys P{};
+    lbmh::MixOff mo{};
+    lbmh::SpOff so{};
+    int8_t *type = nullptr;
+    uint8_t *cflag = nullptr;
+    int *bid = nullptr;
+    long *blist = nullptr;
+    long nb = 0;
+    double *pop[2] = {nullptr, nullptr};
+    double *mom[2] = {nullptr, nullptr};  // single component: the step record; multicomponent: rec
+    double *bst[2] = {nullptr, nullptr};
+    unsigned *status = nullptr;
+    char *stage = nullptr;
+    size_t stage_cells = 0;
+    size_t stage_bytes = 0;
+    char *bounce = nullptr;  // pinned host bounce buffer for downloads
+    int cur = 0;
+    int pack_mode = lbmh::PK_UPLOADED;
+    bool have_state = false;
+    int phase = lbmh::PH_BOUNDARY;
+    bool prof = false;
+    std::vector<lbmh::EvPair> pending, pool;
+    long launches[lbmh::K_NKINDS] = {0, 0, 0};
+    double ms[lbmh::K_NKINDS] = {0, 0, 0};
+    size_t bytes = 0;
+    // multicomponent
+    int ns = 0;
+    int nrec = 0;
+    int chem = 0;
+    lbm::UnitsF U{};
+    gas::Tables *tab = nullptr;  // device copy
+};
+
+namespace lbmh {
+
+inline int cuda_fail(cudaError_t e) {
+    (void)cudaGetLastError();
+    if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDevice || e == cudaErrorNoDevice ||
+        e == cudaErrorInsufficientDriver)
+        return LBMGPU_E_NODEV;
+    return LBMGPU_E_CUDA;
+}
+
+#define CK(x)                                        \
+    do {                                             \
+        cudaError_t e_ = (x);                        \
+        if (e_ != cudaSuccess) return lbmh::cuda_fail(e_); \
+    } while (0)
+
+template <typename T>
+int dalloc(lbmgpu *h, T **p, size_t count) {
+    CK(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
+    h->bytes += count * sizeof(T);
+    return 0;
+}
+
+inline void ev_begin(lbmgpu *h, int kind, EvPair &ep) {
+    if (!h->prof) return;
+    if (h->pool.empty()) {
+        EvPair e{};
+        cudaEventCreate(&e.a);
+        cudaEventCreate(&e.b);
+        h->pool.push_back(e);
+    }
+    ep = h->pool.back();
+    h->pool.pop_back();
+    ep.kind = kind;
+    cudaEventRecord(ep.a, h->stream);
+}
+
+inline void ev_end(lbmgpu *h, EvPair &ep) {
+    if (!h->prof) return;
+    cudaEventRecord(ep.b, h->stream);
+    h->pending.push_back(ep);
+}
+
+inline void ev_drain(lbmgpu *h) {
+    for (auto &e : h->pending) {
+        float t = 0.f;
+        if (cudaEventSynchronize(e.b) == cudaSuccess && cudaEventElapsedTime(&t, e.a, e.b) == cudaSuccess) {
+            h->ms[e.kind] += t;
+            h->launches[e.kind] += 1;
+        }
+        h->pool.push_back(e);
+    }
+    h->pending.clear();
+}
+
+inline unsigned grid_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+// multicomponent entry points (mc.cu)
+int mc_setup(lbmgpu *h);
+int mc_upload(lbmgpu *h, const void *mix, const void *const *species);
+int mc_download(lbmgpu *h, void *mix, void *const *species);
+int mc_init(lbmgpu *h);
+int mc_launch_collide(lbmgpu *h);
+int mc_launch_stream(lbmgpu *h);
+void mc_release(lbmgpu *h);
+
+}  // namespace lbmh

@@ -17,13 +17,18 @@
 #include <vector>
 
 #include "../../include/lbmgpu.h"
+#include "handle.cuh"
 #include "sc_kernels.cuh"
 
 using namespace lbm;
+using lbmh::MixOff;
 
 namespace {
 
-constexpr int kBlock = 128;
+using lbmh::kBlock;
+using lbmh::PK_UPLOADED;
+using lbmh::PK_INIT;
+using lbmh::PK_STEPPED;
 
 __device__ __forceinline__ bool wall_like(int t) {
     return t == T_S || t == T_A || t == T_FS || t == T_P || t == T_O || t == T_O_C;
@@ -238,9 +243,6 @@ __global__ void __launch_bounds__(kBlock)
 // ----------------------------------------------------------------------------------
 // AoS <-> SoA packing for upload/download (the caller's MIXTURE records)
 // ----------------------------------------------------------------------------------
-struct MixOff {
-    long size, type, f, fpc, p_tensor, rho, u, v, w, p, g, gpc, rhoe, energy_flux, temp;
-};
 
 __device__ __forceinline__ double ld(const char *rec, long off) { return *reinterpret_cast<const double *>(rec + off); }
 __device__ __forceinline__ void st(char *rec, long off, double v) { *reinterpret_cast<double *>(rec + off) = v; }
@@ -280,9 +282,6 @@ __global__ void k_sc_unpack(ScGeom g, ScPhys P, MixOff o, const char *__restrict
         }
     }
 }
-
-// Pack modes: what the populations in pop[] are and which derived fields to produce.
-enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
 
 template <int MODE>
 __global__ void k_sc_pack(ScGeom g, ScPhys P, MixOff o, char *__restrict__ stage, long n0, long n1,
@@ -338,106 +337,13 @@ __global__ void k_sc_pack(ScGeom g, ScPhys P, MixOff o, char *__restrict__ stage
     }
 }
 
-// ----------------------------------------------------------------------------------
-// Host side
-// ----------------------------------------------------------------------------------
-enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3 };
-enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_NKINDS = 3 };
-
-struct EvPair {
-    cudaEvent_t a, b;
-    int kind;
-};
-
 }  // namespace
 
-struct lbmgpu {
-    lbmgpu_desc d{};
-    cudaStream_t stream = nullptr;
-    ScGeom g{};
-    ScPhys P{};
-    MixOff mo{};
-    int8_t *type = nullptr;
-    uint8_t *cflag = nullptr;
-    int *bid = nullptr;
-    long *blist = nullptr;
-    long nb = 0;
-    double *pop[2] = {nullptr, nullptr};
-    double *mom[2] = {nullptr, nullptr};
-    double *bst[2] = {nullptr, nullptr};
-    unsigned *status = nullptr;
-    char *stage = nullptr;
-    size_t stage_cells = 0;
-    char *bounce = nullptr;  // pinned host bounce buffer for downloads
-    int cur = 0;
-    int pack_mode = PK_UPLOADED;  // what pop[cur] holds (uploaded / Init / stepped)
-    bool have_state = false;
-    int phase = PH_BOUNDARY;
-    bool prof = false;
-    std::vector<EvPair> pending, pool;
-    long launches[K_NKINDS] = {0, 0, 0};
-    double ms[K_NKINDS] = {0, 0, 0};
-    size_t bytes = 0;
-};
-
 namespace {
-
-int cuda_fail(cudaError_t e) {
-    (void)cudaGetLastError();
-    if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorInvalidDevice || e == cudaErrorNoDevice ||
-        e == cudaErrorInsufficientDriver)
-        return LBMGPU_E_NODEV;
-    return LBMGPU_E_CUDA;
-}
-
-#define CK(x)                                   \
-    do {                                        \
-        cudaError_t e_ = (x);                   \
-        if (e_ != cudaSuccess) return cuda_fail(e_); \
-    } while (0)
-
-template <typename T>
-int dalloc(lbmgpu *h, T **p, size_t count) {
-    CK(cudaMalloc(reinterpret_cast<void **>(p), count * sizeof(T)));
-    h->bytes += count * sizeof(T);
-    return 0;
-}
-
-void ev_begin(lbmgpu *h, int kind, EvPair &ep) {
-    if (!h->prof) return;
-    if (h->pool.empty()) {
-        EvPair e{};
-        cudaEventCreate(&e.a);
-        cudaEventCreate(&e.b);
-        h->pool.push_back(e);
-    }
-    ep = h->pool.back();
-    h->pool.pop_back();
-    ep.kind = kind;
-    cudaEventRecord(ep.a, h->stream);
-}
-
-void ev_end(lbmgpu *h, EvPair &ep) {
-    if (!h->prof) return;
-    cudaEventRecord(ep.b, h->stream);
-    h->pending.push_back(ep);
-}
-
-void ev_drain(lbmgpu *h) {
-    for (auto &e : h->pending) {
-        float t = 0.f;
-        if (cudaEventSynchronize(e.b) == cudaSuccess && cudaEventElapsedTime(&t, e.a, e.b) == cudaSuccess) {
-            h->ms[e.kind] += t;
-            h->launches[e.kind] += 1;
-        }
-        h->pool.push_back(e);
-    }
-    h->pending.clear();
-}
-
-unsigned grid_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+using namespace lbmh;
 
 int launch_collide(lbmgpu *h) {
+    if (h->ns > 0) return lbmh::mc_launch_collide(h);
     const int c = h->cur, x = 1 - c;
     EvPair ep{};
     ev_begin(h, K_COLLIDE, ep);
@@ -453,6 +359,7 @@ int launch_collide(lbmgpu *h) {
 }
 
 int launch_stream_moment(lbmgpu *h) {
+    if (h->ns > 0) return lbmh::mc_launch_stream(h);
     const int c = h->cur, x = 1 - c;
     EvPair ep{};
     ev_begin(h, K_STREAM_MOMENT, ep);
@@ -473,6 +380,25 @@ int launch_stream_moment(lbmgpu *h) {
     return 0;
 }
 
+// Every index the kernels follow must lie inside the tables.
+bool valid_mech(const lbmgpu_mech &m) {
+    if (m.n_species < 1 || m.n_species > LBMGPU_MAX_SPECIES) return false;
+    if (m.n_reactions < 0 || m.n_reactions > LBMGPU_MAX_REACTIONS) return false;
+    for (int k = 0; k < m.n_species; ++k)
+        if (!(m.W[k] > 0) || !(m.T_mid[k] > 0) || !(m.diameter[k] > 0) || !(m.well_depth[k] > 0)) return false;
+    for (int r = 0; r < m.n_reactions; ++r) {
+        if (m.rtype[r] < 0 || m.rtype[r] > 2) return false;
+        if (m.n_reac[r] < 1 || m.n_reac[r] > LBMGPU_MAX_RSPEC || m.n_prod[r] < 1 || m.n_prod[r] > LBMGPU_MAX_RSPEC)
+            return false;
+        for (int j = 0; j < m.n_reac[r]; ++j)
+            if (m.reac[r][j] < 0 || m.reac[r][j] >= m.n_species) return false;
+        for (int j = 0; j < m.n_prod[r]; ++j)
+            if (m.prod[r][j] < 0 || m.prod[r][j] >= m.n_species) return false;
+        if (m.troe_n[r] != 0 && m.troe_n[r] != 3 && m.troe_n[r] != 4) return false;
+    }
+    return true;
+}
+
 bool valid_layout(const lbmgpu_mixture_layout &m) {
     const long need[] = {m.type, m.f, m.fpc, m.p_tensor, m.rho, m.u, m.v, m.w, m.p, m.g, m.gpc, m.rhoe,
                          m.energy_flux, m.temp};
@@ -491,6 +417,8 @@ bool valid_layout(const lbmgpu_mixture_layout &m) {
 }
 
 }  // namespace
+
+using namespace lbmh;
 
 extern "C" {
 
@@ -513,12 +441,21 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     *out = nullptr;
     if (desc->abi_version != LBMGPU_ABI_VERSION) return LBMGPU_E_VERSION;
     if (desc->Nx < 3 || desc->Ny < 3 || desc->Nz < 3) return LBMGPU_E_ARG;
-    if (desc->n_species != 0) return LBMGPU_E_UNSUPPORTED;
     if (desc->precision != LBMGPU_FP64) return LBMGPU_E_UNSUPPORTED;
-    if (!(desc->gamma > 1.0) || !(desc->gas_const > 0.0) || !(desc->prtl > 0.0) || !(desc->nu >= 0.0) ||
-        desc->dt_sim <= 0)
-        return LBMGPU_E_ARG;
-    if (!valid_layout(desc->mix)) return LBMGPU_E_ARG;
+    if (desc->dt_sim <= 0) return LBMGPU_E_ARG;
+    if (desc->n_species == 0) {
+        if (!(desc->gamma > 1.0) || !(desc->gas_const > 0.0) || !(desc->prtl > 0.0) || !(desc->nu >= 0.0))
+            return LBMGPU_E_ARG;
+        if (!valid_layout(desc->mix)) return LBMGPU_E_ARG;
+    } else {
+        if (!desc->mech || desc->mech->n_species != desc->n_species) return LBMGPU_E_ARG;
+        if (!valid_mech(*desc->mech)) return LBMGPU_E_ARG;
+        if (desc->n_species != 9) return LBMGPU_E_UNSUPPORTED;  // kernels are built for 9 species
+        if (desc->chem_mode != LBMGPU_CHEM_OFF && desc->chem_mode != LBMGPU_CHEM_REF_EXPLICIT)
+            return LBMGPU_E_UNSUPPORTED;
+        if (!(desc->units_m > 0.f) || !(desc->units_kg > 0.f) || !(desc->units_s > 0.f) || !(desc->units_K > 0.f))
+            return LBMGPU_E_ARG;
+    }
     if ((double)desc->Nx * desc->Ny * desc->Nz > 2147483647.0) return LBMGPU_E_UNSUPPORTED;  // 32-bit cell offsets
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -544,8 +481,8 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     h->P.cv = desc->gas_const / (desc->gamma - 1.0);
     h->P.cp = h->P.cv + desc->gas_const;
     const lbmgpu_mixture_layout &m = desc->mix;
-    h->mo = MixOff{(long)m.size, m.type, m.f, m.fpc, m.p_tensor, m.rho, m.u, m.v, m.w, m.p, m.g, m.gpc, m.rhoe,
-                   m.energy_flux, m.temp};
+    h->mo = MixOff{(long)m.size, m.type, m.f,   m.fpc,  m.p_tensor,    m.rho,  m.u,  m.v,
+                   m.w,           m.p,    m.g,   m.gpc,  m.rhoe,        m.energy_flux, m.temp, m.HRR};
     const long nc = h->g.ncell;
     int rc = 0;
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -553,19 +490,25 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     if (!rc) rc = dalloc(h, &h->type, nc);
     if (!rc) rc = dalloc(h, &h->cflag, nc);
     if (!rc) rc = dalloc(h, &h->bid, nc);
-    for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->pop[b], 54 * (size_t)nc);
-    for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->mom[b], (size_t)M_N * nc);
+    if (desc->n_species == 0) {
+        for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->pop[b], 54 * (size_t)nc);
+        for (int b = 0; b < 2 && !rc; ++b) rc = dalloc(h, &h->mom[b], (size_t)M_N * nc);
+    } else if (!rc) {
+        rc = lbmh::mc_setup(h);
+    }
     if (!rc) rc = dalloc(h, &h->status, 1);
     if (!rc) {
         e = cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream);
         if (e != cudaSuccess) rc = cuda_fail(e);
     }
     if (!rc) {
-        // staging for AoS transfers: up to 64 MiB of records per chunk
-        h->stage_cells = std::max<size_t>(1, std::min<size_t>((size_t)nc, (64u << 20) / m.size));
-        rc = dalloc(h, &h->stage, h->stage_cells * m.size);
+        // staging for AoS transfers: up to 64 MiB of records (mixture + species) per chunk
+        const size_t per_cell = m.size + (size_t)desc->n_species * desc->spc.size;
+        h->stage_cells = std::max<size_t>(1, std::min<size_t>((size_t)nc, (64u << 20) / per_cell));
+        h->stage_bytes = h->stage_cells * per_cell;
+        rc = dalloc(h, &h->stage, h->stage_bytes);
         if (!rc) {
-            e = cudaMallocHost(reinterpret_cast<void **>(&h->bounce), h->stage_cells * m.size);
+            e = cudaMallocHost(reinterpret_cast<void **>(&h->bounce), h->stage_bytes);
             if (e != cudaSuccess) rc = cuda_fail(e);
         }
     }
@@ -598,14 +541,16 @@ int lbmgpu_destroy(lbmgpu_t *h) {
     cudaFree(h->status);
     cudaFree(h->stage);
     if (h->bounce) cudaFreeHost(h->bounce);
+    lbmh::mc_release(h);
     if (h->stream) cudaStreamDestroy(h->stream);
     (void)cudaGetLastError();
     delete h;
     return LBMGPU_OK;
 }
 
-int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos) {
+int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos, const void *const *species_aos) {
     if (!h || !mixture_aos) return LBMGPU_E_ARG;
+    if (h->ns > 0) return lbmh::mc_upload(h, mixture_aos, species_aos);
     CK(cudaSetDevice(h->d.device));
     const ScGeom &g = h->g;
     const long nc = g.ncell;
@@ -686,14 +631,15 @@ int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos) {
     CK(cudaStreamSynchronize(h->stream));
     h->pack_mode = PK_UPLOADED;
     h->have_state = true;
-    h->phase = PH_BOUNDARY;
+    h->phase = lbmh::PH_BOUNDARY;
     return LBMGPU_OK;
 }
 
-int lbmgpu_download(lbmgpu_t *h, void *mixture_aos) {
+int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos) {
     if (!h || !mixture_aos) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;
-    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->ns > 0) return lbmh::mc_download(h, mixture_aos, species_aos);
     CK(cudaSetDevice(h->d.device));
     const ScGeom &g = h->g;
     const long nc = g.ncell;
@@ -753,8 +699,9 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos) {
 int lbmgpu_init(lbmgpu_t *h) {
     if (!h) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;
-    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
     CK(cudaSetDevice(h->d.device));
+    if (h->ns > 0) return lbmh::mc_init(h);
     if (h->cur != 0) {
         // Init always rebuilds the state in buffer 0 from the stored moments
         const long nc = h->g.ncell;
@@ -772,15 +719,21 @@ int lbmgpu_init(lbmgpu_t *h) {
     return LBMGPU_OK;
 }
 
+// Multicomponent: Collide_Species and Collide run as one fused kernel, launched by
+// lbmgpu_collide; Collide_Species must come first (src/lbm-main.cpp:157-163).
 int lbmgpu_collide_species(lbmgpu_t *h) {
     if (!h) return LBMGPU_E_ARG;
-    return LBMGPU_E_UNSUPPORTED;  // single component: the reference's loop has no species phase
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;  // single component: no species phase in the loop
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
+    h->phase = PH_SPECIES;
+    return LBMGPU_OK;
 }
 
 int lbmgpu_collide(lbmgpu_t *h) {
     if (!h) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;
-    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->phase != (h->ns > 0 ? PH_SPECIES : lbmh::PH_BOUNDARY)) return LBMGPU_E_PHASE;
     CK(cudaSetDevice(h->d.device));
     int rc = launch_collide(h);
     if (rc) return rc;
@@ -808,14 +761,14 @@ int lbmgpu_calculate_moment(lbmgpu_t *h) {
     CK(cudaSetDevice(h->d.device));
     int rc = launch_stream_moment(h);
     if (rc) return rc;
-    h->phase = PH_BOUNDARY;
+    h->phase = lbmh::PH_BOUNDARY;
     return LBMGPU_OK;
 }
 
 int lbmgpu_step(lbmgpu_t *h, int nsteps) {
     if (!h || nsteps < 0) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;
-    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
     CK(cudaSetDevice(h->d.device));
     for (int s = 0; s < nsteps; ++s) {
         int rc = launch_collide(h);
@@ -828,7 +781,7 @@ int lbmgpu_step(lbmgpu_t *h, int nsteps) {
 int lbmgpu_time_steps(lbmgpu_t *h, int nsteps, double *ms) {
     if (!h || !ms || nsteps < 0) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;
-    if (h->phase != PH_BOUNDARY) return LBMGPU_E_PHASE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
     CK(cudaSetDevice(h->d.device));
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
@@ -902,6 +855,16 @@ int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms) {
         ms[k] = h->ms[k];
     }
     return K_NKINDS;
+}
+
+int lbmgpu_units_from_dx_dt(float dx, float dt, float *out4) {
+    if (!out4 || !(dx > 0.f) || !(dt > 0.f)) return LBMGPU_E_ARG;
+    const lbm::UnitsF u = lbm::units_from_dx_dt(dx, dt);
+    out4[0] = u.m;
+    out4[1] = u.kg;
+    out4[2] = u.s;
+    out4[3] = u.K;
+    return LBMGPU_OK;
 }
 
 int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes) {

@@ -1,0 +1,537 @@
+// Multicomponent thermal D3Q27 step, per-cell logic (the reference with MULTICOMP on).
+// Every function here is host/device: the kernels in lbmgpu.cu call them once per cell,
+// and the tests build them for the host to compare with the reference's own solver.
+//
+// Device state (structure of arrays, cell index n = (i*Ny + j)*Nz + k):
+//   pop[2]: 27*(NS+1) planes -- species a, direction l at plane 27a + l; the energy
+//           population g at plane 27 NS + l.  Post-collision values of the last step, or
+//           (after an upload or Init, "local" mode) the populations themselves; the other
+//           buffer then keeps the uploaded fpc, which the reference's skip rule for
+//           vanishing species (src/lbm-collision.cpp:512-513) leaves in place.
+//   rec[2]: MC_NREC(NS) planes per cell -- the state calculate_moment leaves
+//           (src/lbm-moment.cpp:193-377): rho, u, v, w, T, p, rhoE, the pressure tensor
+//           (6), HRR, then per species rho_a, j_a (3: sum f_a c, the moment the species
+//           collision divides by rho_a, src/lbm-collision.cpp:446-454), u_a (3: the
+//           Stefan-Maxwell velocities) and X_a.  Double-buffered like the
+//           single-component record.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "d3q27.cuh"
+#include "gas.cuh"
+#include "units.cuh"
+
+#if defined(__CUDACC__)
+#define MC_HD __host__ __device__ __forceinline__
+#define MC_HDN __host__ __device__
+#else
+#define MC_HD inline
+#define MC_HDN inline
+#endif
+
+namespace lbm {
+
+constexpr double kSpeciesMin = 1e-8;   // SPECIES_MIN, src/headers/defines.hpp:96
+
+enum : int {
+    RM_RHO = 0, RM_U = 1, RM_V = 2, RM_W = 3, RM_T = 4, RM_P = 5, RM_RHOE = 6, RM_P00 = 7, // P00 P01 P02 P11 P12 P22
+    RM_HRR = 13, RM_SP = 14, RM_SPN = 8                                                    // per species block
+};
+enum : int { RS_RHO = 0, RS_JX = 1, RS_UX = 4, RS_X = 7 };
+MC_HD int mc_nrec(int ns) { return RM_SP + RM_SPN * ns; }
+MC_HD int rs(int a, int f) { return RM_SP + RM_SPN * a + f; }
+
+enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1 };
+
+struct McArgs {
+    int Nx, Ny, Nz;
+    long ncell, sj, si;
+    int ns, dt, chem;
+    UnitsF U;
+    const gas::Tables *tab;
+    const int8_t *type;
+    const uint8_t *cflag;
+    const double *pop_src;   // collide: pop[cur]; stream: the collide's output
+    double *pop_dst;         // collide: pop[nxt]
+    const double *pop_prev;  // collide: fpc of the previous step (skip rule); null in local mode
+    const double *rec_cur;
+    double *rec_nxt;
+    unsigned *status;
+    int local;
+};
+
+MC_HD double rec(const McArgs &A, const double *r, int plane, long n) { return r[(long)plane * A.ncell + n]; }
+
+MC_HD void atomic_status(unsigned *s, unsigned bits) {
+#if defined(__CUDA_ARCH__)
+    atomicOr(s, bits);
+#else
+    *s |= bits;
+#endif
+}
+
+MC_HD bool fluid_like(int t) { return t == T_F || t == T_I || t == T_O || t == T_I_C || t == T_O_C; }
+
+MC_HD bool mc_wall_like(int t) {
+    return t == T_S || t == T_A || t == T_FS || t == T_P || t == T_O || t == T_O_C;
+}
+// fd_central (src/headers/FD.hpp:108-127), dx = 1
+MC_HD double mc_fd_central(double sl, double sc, double sr, int tl, int tr) {
+    if (mc_wall_like(tl)) return (tr == T_P) ? 0.0 : (sr - sc);
+    if (mc_wall_like(tr)) return (tl == T_P) ? 0.0 : (sc - sl);
+    return (sr - sl) / 2.0;
+}
+// fd_fuw (src/FD.cpp:5-23), dx = 1
+MC_HD bool fuw_blocked(int t) { return mc_wall_like(t) || t == T_I || t == T_I_C; }
+MC_HD double mc_fd_fuw(double sl, double sc, double sr, double vel, int tl, int tr) {
+    if (vel > 0) return fuw_blocked(tl) ? 0.0 : (sc - sl);
+    return fuw_blocked(tr) ? 0.0 : (sr - sc);
+}
+
+MC_HD void decode(const McArgs &A, long n, int &i, int &j, int &k) {
+    i = (int)(n / A.si);
+    j = (int)((n / A.sj) % A.Ny);
+    k = (int)(n % A.Nz);
+}
+
+// Periodic pull source of direction l for a cell with no boundary neighbour
+// (src/lbm-streaming.cpp:88-117).
+MC_HD long mc_pull_src(const McArgs &A, int i, int j, int k, int l) {
+    int in = i - cx(l), jn = j - cy(l), kn = k - cz(l);
+    if (in == 0) in = A.Nx - 2; else if (in == A.Nx - 1) in = 1;
+    if (jn == 0) jn = A.Ny - 2; else if (jn == A.Ny - 1) jn = 1;
+    if (kn == 0) kn = A.Nz - 2; else if (kn == A.Nz - 1) kn = 1;
+    return (long)in * A.si + (long)jn * A.sj + kn;
+}
+
+// Cantera's setMassFractions: clip negatives, normalise.  Returns the mean molar mass.
+template <int NS>
+MC_HD double set_mass_fractions(const gas::Tables &t, const double *y, double *Y, double *X) {
+    double s = 0.0;
+    for (int k = 0; k < NS; ++k) {
+        Y[k] = y[k] > 0.0 ? y[k] : 0.0;
+        s += Y[k];
+    }
+    for (int k = 0; k < NS; ++k) Y[k] /= s;
+    double sw = 0.0;
+    for (int k = 0; k < NS; ++k) sw += Y[k] / t.m.W[k];
+    const double W = 1.0 / sw;
+    for (int k = 0; k < NS; ++k) X[k] = Y[k] / t.m.W[k] * W;
+    return W;
+}
+
+// ------------------------------------------------------------------------------------
+// Streaming + moments (reference LBM::Streaming and the multicomponent
+// LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one fluid cell of a periodic
+// lattice.
+// ------------------------------------------------------------------------------------
+template <int NS>
+MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
+    const gas::Tables &t = *A.tab;
+    const long nc = A.ncell;
+    int i, j, k;
+    decode(A, n, i, j, k);
+    // -- old state, as the reference's Cantera object is set at the start (lbm-moment.cpp:219-221)
+    double Yo_raw[NS], Yo[NS], Xo[NS];
+    const double rho_old = rec(A, A.rec_cur, RM_RHO, n);
+    for (int a = 0; a < NS; ++a) Yo_raw[a] = rec(A, A.rec_cur, rs(a, RS_RHO), n) / rho_old;
+    const double Wold = set_mass_fractions<NS>(t, Yo_raw, Yo, Xo);
+    const double T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
+    const double rho_si = si_rho(A.U, (float)rho_old);
+    const double P_si = rho_si * gas::kR * T_si / Wold;
+
+    // -- pulled populations: sums per species and of g
+    double rho_a[NS], j_a[NS][3];
+    double P6[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < NS; ++a) {
+        double r = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+        for (int l = 0; l < 27; ++l) {
+            const double fv = A.pop_src[(long)(27 * a + l) * nc + mc_pull_src(A, i, j, k, l)];
+            r += fv;
+            jx += fv * cx(l);
+            jy += fv * cy(l);
+            jz += fv * cz(l);
+            if (cx(l)) P6[0] += fv;
+            if (cx(l) * cy(l)) P6[1] += cx(l) * cy(l) * fv;
+            if (cx(l) * cz(l)) P6[2] += cx(l) * cz(l) * fv;
+            if (cy(l)) P6[3] += fv;
+            if (cy(l) * cz(l)) P6[4] += cy(l) * cz(l) * fv;
+            if (cz(l)) P6[5] += fv;
+        }
+        rho_a[a] = r;
+        j_a[a][0] = jx;
+        j_a[a][1] = jy;
+        j_a[a][2] = jz;
+    }
+    double rhoe = 0.0;
+#pragma unroll
+    for (int l = 0; l < 27; ++l) rhoe += A.pop_src[(long)(27 * NS + l) * nc + mc_pull_src(A, i, j, k, l)];
+
+    double rho = 0, ru = 0, rv = 0, rw = 0, rho_s[NS];
+    for (int a = 0; a < NS; ++a) {
+        rho_s[a] = rho_a[a] > kSpeciesMin ? rho_a[a] : kSpeciesMin;
+        rho += rho_a[a];
+        ru += j_a[a][0];
+        rv += j_a[a][1];
+        rw += j_a[a][2];
+    }
+    const double u = ru / rho, v = rv / rho, w = rw / rho;
+
+    // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky
+    double M[NS][NS];
+    const double p_old = rec(A, A.rec_cur, RM_P, n);
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < NS; ++b) {
+            if (b == a) {
+                M[a][b] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
+            } else {
+                const int lo = a > b ? a : b, hi = a > b ? b : a;  // D stored for b <= a
+                const double D = u_nu(A.U, (float)gas::binary_diff(t, lo, hi, T_si, P_si));
+                M[a][b] = -1.0 * A.dt / 2.0 * p_old * rec(A, A.rec_cur, rs(a, RS_X), n) *
+                          rec(A, A.rec_cur, rs(b, RS_X), n) / D;
+            }
+        }
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < NS; ++b)
+            if (b != a) M[a][a] -= M[a][b];
+    for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor
+        double d = M[c][c];
+        for (int q = 0; q < c; ++q) d -= M[c][q] * M[c][q];
+        M[c][c] = sqrt(d);
+        for (int r = c + 1; r < NS; ++r) {
+            double s = M[r][c];
+            for (int q = 0; q < c; ++q) s -= M[r][q] * M[c][q];
+            M[r][c] = s / M[c][c];
+        }
+    }
+    double usm[NS][3];
+    for (int dmn = 0; dmn < 3; ++dmn) {
+        double y[NS];
+        for (int r = 0; r < NS; ++r) {
+            double s = j_a[r][dmn];
+            for (int q = 0; q < r; ++q) s -= M[r][q] * y[q];
+            y[r] = s / M[r][r];
+        }
+        for (int r = NS - 1; r >= 0; --r) {
+            double s = y[r];
+            for (int q = r + 1; q < NS; ++q) s -= M[q][r] * usm[q][dmn];
+            usm[r][dmn] = s / M[r][r];
+        }
+    }
+
+    // -- temperature from the internal energy (setState_UV, lbm-moment.cpp:346-368)
+    double Yr[NS], Y[NS], X[NS];
+    for (int a = 0; a < NS; ++a) Yr[a] = rho_s[a] / rho;
+    const double Wn = set_mass_fractions<NS>(t, Yr, Y, X);
+    double e = rhoe / rho;
+    for (int a = 0; a < NS; ++a)
+        e = e - 0.5 * rho_s[a] / rho * (usm[a][0] * usm[a][0] + usm[a][1] * usm[a][1] + usm[a][2] * usm[a][2]);
+    const double u_si = si_energy_mass(A.U, (float)e);
+    const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
+    const double rho_n_si = 1.0 / vol;
+    double Tn;
+    const int it = gas::T_from_u(t, Y, u_si, T_si, 1e-14, 100, Tn);
+    if (it < 0) atomic_status(A.status, LBMGPU_ST_NEWTON);
+    const double Pn = rho_n_si * gas::kR * Tn / Wn;
+
+    double *R = A.rec_nxt;
+    R[(long)RM_RHO * nc + n] = rho;
+    R[(long)RM_U * nc + n] = u;
+    R[(long)RM_V * nc + n] = v;
+    R[(long)RM_W * nc + n] = w;
+    R[(long)RM_T * nc + n] = u_temp(A.U, (float)Tn);
+    R[(long)RM_P * nc + n] = u_p(A.U, (float)Pn);
+    R[(long)RM_RHOE * nc + n] = rhoe;
+    for (int q = 0; q < 6; ++q) R[(long)(RM_P00 + q) * nc + n] = P6[q];
+    for (int a = 0; a < NS; ++a) {
+        R[(long)rs(a, RS_RHO) * nc + n] = rho_s[a];
+        for (int d = 0; d < 3; ++d) {
+            R[(long)rs(a, RS_JX + d) * nc + n] = j_a[a][d];
+            R[(long)rs(a, RS_UX + d) * nc + n] = usm[a][d];
+        }
+        R[(long)rs(a, RS_X) * nc + n] = X[a];
+    }
+    if (!isfinite(rho) || !isfinite(Tn) || !isfinite(u) || !isfinite(v) || !isfinite(w))
+        atomic_status(A.status, LBMGPU_ST_NAN);
+    else if (!(rho > 0.0) || !(Tn > 0.0))
+        atomic_status(A.status, LBMGPU_ST_NEG_STATE);
+}
+
+// ------------------------------------------------------------------------------------
+// Collision: species (LBM::Collide_Species, src/lbm-collision.cpp:334-526) and energy
+// (LBM::Collide, src/lbm-collision.cpp:191-332) of one fluid cell, fused.
+// ------------------------------------------------------------------------------------
+template <int NS>
+MC_HDN void mc_collide_cell(const McArgs &A, long n) {
+    const gas::Tables &t = *A.tab;
+    const long nc = A.ncell;
+    const double *Rc = A.rec_cur;
+    int i, j, k;
+    decode(A, n, i, j, k);
+    const double rho = rec(A, Rc, RM_RHO, n);
+    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
+    const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n), rhoe = rec(A, Rc, RM_RHOE, n);
+    double rho_a[NS], ua[NS][3], Xs[NS];
+    for (int a = 0; a < NS; ++a) {
+        rho_a[a] = rec(A, Rc, rs(a, RS_RHO), n);
+        for (int d = 0; d < 3; ++d) ua[a][d] = rec(A, Rc, rs(a, RS_UX + d), n);
+        Xs[a] = rec(A, Rc, rs(a, RS_X), n);
+    }
+    // Cantera state (lbm-collision.cpp:364-367 and :236-238)
+    double Yr[NS], Y[NS], X[NS];
+    for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] / rho;
+    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
+    const double T_si = si_temp(A.U, (float)Tl);
+    const double rho_si = si_rho(A.U, (float)rho);
+    const double P_si = rho_si * gas::kR * T_si / W;
+    const double dt = A.dt;
+
+    // internal energy without the species kinetic energy (lbm-collision.cpp:260-263, 373-376)
+    double Uint = rhoe / rho;
+    for (int a = 0; a < NS; ++a)
+        Uint = Uint - 0.5 * rho_a[a] / rho * (ua[a][0] * ua[a][0] + ua[a][1] * ua[a][1] + ua[a][2] * ua[a][2]);
+
+    // -- chemistry: two explicit half steps with T from (u, v) in between (lbm-collision.cpp:370-399)
+    double drho[NS];
+    for (int a = 0; a < NS; ++a) drho[a] = 0.0;
+    if (A.chem == CHEM_REF_EXPLICIT) {
+        double Tc = T_si, rc = rho_si, Yc[NS], Xc[NS];
+        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+        for (int sub = 0; sub < 2; ++sub) {
+            double C[gas::MAXS], wd[gas::MAXS];
+            for (int a = 0; a < NS; ++a) C[a] = rc * Yc[a] / t.m.W[a];
+            gas::net_production(t, Tc, C, wd);
+            for (int a = 0; a < NS; ++a) drho[a] += dt / 2.0 * (double)u_rho_dot(A.U, (float)(wd[a] * t.m.W[a]));
+            double yy[NS];
+            for (int a = 0; a < NS; ++a) yy[a] = (rho_a[a] + drho[a]) / rho;
+            set_mass_fractions<NS>(t, yy, Yc, Xc);
+            const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
+            rc = 1.0 / vol;
+            double Tn;
+            if (gas::T_from_u(t, Yc, si_energy_mass(A.U, (float)Uint), Tc, 1e-14, 100, Tn) < 0)
+                atomic_status(A.status, LBMGPU_ST_NEWTON);
+            Tc = Tn;
+        }
+        double hrr = 0.0;
+        for (int a = 0; a < NS; ++a)
+            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
+        A.rec_nxt[(long)RM_HRR * nc + n] = hrr;
+    }
+
+    // -- species viscosities, Wilke weights, relaxation rates (lbm-collision.cpp:402-430)
+    double mu_k[NS];
+    for (int a = 0; a < NS; ++a) mu_k[a] = gas::species_visc(t, a, T_si);
+    double om_a[NS];
+    for (int a = 0; a < NS; ++a) {
+        double denom = 0.0;
+        for (int b = 0; b < NS; ++b) {
+            // phi[a][b] of the reference (computed for b >= a, mirrored for b < a)
+            double phi;
+            if (b >= a) {
+                const double f1 = 1.0 + sqrt(mu_k[a] / mu_k[b]) * sqrt(sqrt(t.m.W[b] / t.m.W[a]));
+                phi = f1 * f1 / sqrt(8.0 * (1.0 + t.m.W[a] / t.m.W[b]));
+            } else {
+                const double f1 = 1.0 + sqrt(mu_k[b] / mu_k[a]) * sqrt(sqrt(t.m.W[a] / t.m.W[b]));
+                const double pba = f1 * f1 / sqrt(8.0 * (1.0 + t.m.W[b] / t.m.W[a]));
+                phi = mu_k[a] / mu_k[b] * t.m.W[b] / t.m.W[a] * pba;
+            }
+            denom = denom + Xs[b] * phi;
+        }
+        const double visc = Xs[a] * (double)u_mu(A.U, (float)mu_k[a]) / denom;
+        om_a[a] = 2 * Xs[a] * p * dt / (Xs[a] * p * dt + 2 * visc);
+    }
+
+    // -- Maxwell-Stefan force (lbm-collision.cpp:433-471)
+    double F[NS][3], ux[NS][3];
+    for (int a = 0; a < NS; ++a) {
+        for (int d = 0; d < 3; ++d) {
+            ux[a][d] = rec(A, Rc, rs(a, RS_JX + d), n) / rho_a[a];
+            F[a][d] = 0.0;
+        }
+        for (int b = 0; b < NS; ++b) {
+            const int lo = a > b ? a : b, hi = a > b ? b : a;
+            const double D = u_nu(A.U, (float)gas::binary_diff(t, lo, hi, T_si, P_si));
+            for (int d = 0; d < 3; ++d) F[a][d] += -1.0 * p * Xs[a] * Xs[b] / D * (ua[a][d] - ua[b][d]);
+        }
+        for (int d = 0; d < 3; ++d) F[a][d] = F[a][d] * dt / rho_a[a];
+    }
+
+    // -- neighbour data for the FD terms
+    long nbl[3], nbh[3];
+    int tl[3], th[3];
+    for (int d = 0; d < 3; ++d) {
+        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
+        nbl[d] = n - off;
+        nbh[d] = n + off;
+        tl[d] = A.type[nbl[d]];
+        th[d] = A.type[nbh[d]];
+    }
+
+    // -- species collision (lbm-collision.cpp:479-519)
+    for (int a = 0; a < NS; ++a) {
+        const double Ra = u_cp(A.U, (float)(gas::kR / t.m.W[a]));
+        const double theta = Ra * Tl;
+        double corr[3];
+        for (int d = 0; d < 3; ++d) {
+            const int pu = rs(a, RS_UX + d);
+            auto Qa = [&](long m) {
+                const double r = rec(A, Rc, rs(a, RS_RHO), m), uu = rec(A, Rc, pu, m);
+                return r * uu * (1.0 - 3.0 * Ra * rec(A, Rc, RM_T, m)) - r * (uu * uu * uu);
+            };
+            const double dQ = mc_fd_central(Qa(nbl[d]), Qa(n), Qa(nbh[d]), tl[d], th[d]);
+            corr[d] = dt * (2.0 - om_a[a]) / (2.0 * rho_a[a] * om_a[a]) * dQ;
+        }
+        AxisF<double> Fe, Fd, Fr;
+        axis_feq(Fe, ux[a], theta, corr);
+        const double udu[3] = {ux[a][0] + F[a][0], ux[a][1] + F[a][1], ux[a][2] + F[a][2]};
+        axis_feq(Fd, udu, theta, corr);
+        const double zero[3] = {0.0, 0.0, 0.0};
+        axis_feq(Fr, um, theta, zero);
+        const double om = om_a[a];
+        for (int l = 0; l < 27; ++l) {
+            const long plane = (long)(27 * a + l) * nc;
+            const double fv = A.local ? A.pop_src[plane + n] : A.pop_src[plane + mc_pull_src(A, i, j, k, l)];
+            const double fe = feq_l(l, rho_a[a], Fe);
+            const double fd = feq_l(l, rho_a[a], Fd);
+            const double fr = A.chem == CHEM_REF_EXPLICIT ? feq_l(l, drho[a], Fr) : 0.0;
+            if (rho_a[a] <= kSpeciesMin && fr <= 0.0) {
+                if (!A.local) A.pop_dst[plane + n] = A.pop_prev[plane + n];
+                continue;
+            }
+            A.pop_dst[plane + n] = fv + om * (fe - fv) + (fd - fe) + fr;
+        }
+    }
+
+    // -- energy collision (lbm-collision.cpp:231-324)
+    const double cp = u_cp(A.U, (float)gas::cp_mass(t, Y, T_si));
+    const double gasconstant = u_cp(A.U, (float)(gas::kR / W));
+    const double mu = u_mu(A.U, (float)gas::wilke(t, X, mu_k));
+    const double lam = u_cond(A.U, (float)gas::mix_cond(t, X, T_si, P_si, mu_k));
+    const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
+    const double om1 = 2 * p * cp * dt / (p * cp * dt + 2 * lam);
+    const double om = 2 * p * dt / (p * dt + 2 * mu);
+    if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) atomic_status(A.status, LBMGPU_ST_TAU_UNSTABLE);
+    double qd[3] = {0, 0, 0}, qc[3] = {0, 0, 0};
+    for (int a = 0; a < NS; ++a) {
+        const double ha = u_energy_mass(A.U, (float)(gas::h_RT(t, a, T_si) * gas::kR * T_si / t.m.W[a]));
+        for (int d = 0; d < 3; ++d) {
+            qd[d] += om1 / (-om + om1) * ha * rho_a[a] * (ua[a][d] - um[d]);
+            const double Yl = rec(A, Rc, rs(a, RS_RHO), nbl[d]) / rec(A, Rc, RM_RHO, nbl[d]);
+            const double Yc = rho_a[a] / rho;
+            const double Yh = rec(A, Rc, rs(a, RS_RHO), nbh[d]) / rec(A, Rc, RM_RHO, nbh[d]);
+            const double dY = mc_fd_fuw(Yl, Yc, Yh, ua[a][d] - um[d], tl[d], th[d]);
+            qc[d] += 0.5 * (2.0 - om1) / (-om + om1) * dt * p * ha * dY;
+        }
+    }
+    // mixture gas constant of a neighbour from its composition (lbm-collision.cpp:207-215)
+    auto gc_nb = [&](long m) {
+        if (!fluid_like(A.type[m])) return 0.0;
+        double sYW = 0.0, sY = 0.0;
+        const double rm = rec(A, Rc, RM_RHO, m);
+        for (int a = 0; a < NS; ++a) {
+            const double Ya = rec(A, Rc, rs(a, RS_RHO), m) / rm;
+            sYW += Ya / t.m.W[a];
+            sY += Ya;
+        }
+        return (double)u_cp(A.U, (float)(gas::kR * sYW / sY));
+    };
+    const double P6[6] = {rec(A, Rc, RM_P00, n), rec(A, Rc, RM_P00 + 1, n), rec(A, Rc, RM_P00 + 2, n),
+                          rec(A, Rc, RM_P00 + 3, n), rec(A, Rc, RM_P00 + 4, n), rec(A, Rc, RM_P00 + 5, n)};
+    const double Pf[3][3] = {{P6[0], P6[1], P6[2]}, {P6[1], P6[3], P6[4]}, {P6[2], P6[4], P6[5]}};
+    double dq[3];
+    for (int d = 0; d < 3; ++d) {
+        const int pu = RM_U + d;
+        const double Ql = rec(A, Rc, RM_RHO, nbl[d]) * rec(A, Rc, pu, nbl[d]) *
+                              (1.0 - 3.0 * gc_nb(nbl[d]) * rec(A, Rc, RM_T, nbl[d])) -
+                          rec(A, Rc, RM_RHO, nbl[d]) * (rec(A, Rc, pu, nbl[d]) * rec(A, Rc, pu, nbl[d]) * rec(A, Rc, pu, nbl[d]));
+        const double Qc = rho * um[d] * (1.0 - 3.0 * gasconstant * Tl) - rho * (um[d] * um[d] * um[d]);
+        const double Qh = rec(A, Rc, RM_RHO, nbh[d]) * rec(A, Rc, pu, nbh[d]) *
+                              (1.0 - 3.0 * gc_nb(nbh[d]) * rec(A, Rc, RM_T, nbh[d])) -
+                          rec(A, Rc, RM_RHO, nbh[d]) * (rec(A, Rc, pu, nbh[d]) * rec(A, Rc, pu, nbh[d]) * rec(A, Rc, pu, nbh[d]));
+        const double dQ = mc_fd_central(Ql, Qc, Qh, tl[d], th[d]);
+        double s = 0.0;
+        for (int b = 0; b < 3; ++b) s += um[b] * (Pf[b][d] - ((b == d ? p : 0.0) + rho * um[b] * um[d]));
+        dq[d] = s + qd[d] + qc[d] + 0.5 * dt * um[d] * dQ;
+    }
+    AxisG<double> G;
+    axis_geq(G, Uint, theta, um);
+    for (int l = 0; l < 27; ++l) {
+        const long plane = (long)(27 * NS + l) * nc;
+        const double gv = A.local ? A.pop_src[plane + n] : A.pop_src[plane + mc_pull_src(A, i, j, k, l)];
+        const double gq = geq_l(l, rho, G);
+        const double gs = (csq(l) == 1) ? gq + 0.5 * (cx(l) * dq[0] + cy(l) * dq[1] + cz(l) * dq[2]) : gq;
+        A.pop_dst[plane + n] = gv + om1 * (gq - gv) + (om - om1) * (gq - gs);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Init (reference LBM::Init, multicomponent, src/lbm-init.cpp:85-146).  Writes the
+// record planes it changes into both record buffers and the populations into pop[0].
+// ------------------------------------------------------------------------------------
+template <int NS>
+MC_HDN void mc_init_cell(const McArgs &A, long n, double *rec0, double *rec1, double *pop0) {
+    const int ty = A.type[n];
+    if (!(ty == T_F || ty == T_I || ty == T_I_C || ty == T_O || ty == T_O_C)) return;
+    const gas::Tables &t = *A.tab;
+    const long nc = A.ncell;
+    double Xin[NS], X[NS], Y[NS];
+    double s = 0.0;
+    for (int a = 0; a < NS; ++a) {
+        Xin[a] = rec0[(long)rs(a, RS_X) * nc + n];
+        X[a] = Xin[a] > 0.0 ? Xin[a] : 0.0;
+        s += X[a];
+    }
+    double W = 0.0;
+    for (int a = 0; a < NS; ++a) {
+        X[a] /= s;
+        W += X[a] * t.m.W[a];
+    }
+    for (int a = 0; a < NS; ++a) Y[a] = X[a] * t.m.W[a] / W;
+    const double T_si = si_temp(A.U, (float)rec0[(long)RM_T * nc + n]);
+    const double P_si = si_p(A.U, (float)rec0[(long)RM_P * nc + n]);
+    const double dens = P_si * W / (gas::kR * T_si);
+    const double rho = u_rho(A.U, (float)dens);
+    const double vel[3] = {rec0[(long)RM_U * nc + n], rec0[(long)RM_V * nc + n], rec0[(long)RM_W * nc + n]};
+    const double U = u_energy_mass(A.U, (float)gas::int_energy_mass(t, Y, T_si));
+    const double rhoe = rho * (U + 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]));
+    const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
+    double *R2[2] = {rec0, rec1};
+    for (int b = 0; b < 2; ++b) {
+        R2[b][(long)RM_RHO * nc + n] = rho;
+        R2[b][(long)RM_RHOE * nc + n] = rhoe;
+    }
+    const bool fluid = ty == T_F;
+    AxisG<double> G;
+    axis_geq(G, U, theta, vel);
+    if (fluid)
+        for (int l = 0; l < 27; ++l) pop0[(long)(27 * NS + l) * nc + n] = geq_l(l, rho, G);
+    const double zero[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < NS; ++a) {
+        double ra = Y[a] * rho;
+        ra = ra > kSpeciesMin ? ra : kSpeciesMin;
+        const double tha = u_energy_mass(A.U, (float)(gas::kR * T_si / t.m.W[a]));
+        for (int b = 0; b < 2; ++b) {
+            R2[b][(long)rs(a, RS_RHO) * nc + n] = ra;
+            for (int d = 0; d < 3; ++d) R2[b][(long)rs(a, RS_UX + d) * nc + n] = vel[d];
+        }
+        AxisF<double> Fe;
+        axis_feq(Fe, vel, tha, zero);
+        double jx = 0, jy = 0, jz = 0;
+        for (int l = 0; l < 27; ++l) {
+            const double fv = feq_l(l, ra, Fe);
+            if (fluid) pop0[(long)(27 * a + l) * nc + n] = fv;
+            jx += fv * cx(l);
+            jy += fv * cy(l);
+            jz += fv * cz(l);
+        }
+        for (int b = 0; b < 2; ++b) {
+            R2[b][(long)rs(a, RS_JX) * nc + n] = jx;
+            R2[b][(long)rs(a, RS_JX + 1) * nc + n] = jy;
+            R2[b][(long)rs(a, RS_JX + 2) * nc + n] = jz;
+        }
+    }
+}
+
+}  // namespace lbm

@@ -198,7 +198,7 @@ __device__ __forceinline__ void local_state_sc(const ScGeom &g, const ScPhys &P,
 // Tamm-Mott-Smith boundary treatment of one fluid cell (reference LBM::TMS_BC, single
 // component: outflow src/lbm-bc.cpp:341-460, inflow :809-938, solid :1111-1229), applied
 // in the reference's pass order.  `mom` holds the previous step's record.
-__device__ void tms_cell_sc(const ScGeom &g, const ScPhys &P, const int8_t *__restrict__ type,
+static __device__ void tms_cell_sc(const ScGeom &g, const ScPhys &P, const int8_t *__restrict__ type,
                             const double *__restrict__ mom, long n, double f[27], double ge[27]) {
     const long nc = g.ncell;
     const int i = (int)(n / g.si);

@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblbmgpu.so")
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 FP64, FP32 = 0, 1
 ST_NAN, ST_NEG_STATE, ST_TAU_UNSTABLE = 0x1, 0x2, 0x4
@@ -36,7 +36,10 @@ EXPORTS = [
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
+    "lbmgpu_units_from_dx_dt",
 ]
+CHEM_OFF, CHEM_REF_EXPLICIT = 0, 1
+ST_NEWTON = 0x8
 
 
 class MixtureLayout(ctypes.Structure):
@@ -45,12 +48,18 @@ class MixtureLayout(ctypes.Structure):
         "temp", "HRR")]
 
 
+class SpeciesLayout(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_size_t)] + [(n, ctypes.c_long) for n in ("X", "rho", "f", "fpc", "u", "v", "w")]
+
+
 class Desc(ctypes.Structure):
     _fields_ = [("abi_version", ctypes.c_int), ("device", ctypes.c_int), ("Nx", ctypes.c_int),
                 ("Ny", ctypes.c_int), ("Nz", ctypes.c_int), ("n_species", ctypes.c_int),
                 ("precision", ctypes.c_int), ("dt_sim", ctypes.c_int), ("nu", ctypes.c_double),
                 ("gas_const", ctypes.c_double), ("gamma", ctypes.c_double), ("prtl", ctypes.c_double),
-                ("mix", MixtureLayout)]
+                ("mix", MixtureLayout), ("spc", SpeciesLayout), ("mech", ctypes.c_void_p),
+                ("units_m", ctypes.c_float), ("units_kg", ctypes.c_float), ("units_s", ctypes.c_float),
+                ("units_K", ctypes.c_float), ("chem_mode", ctypes.c_int)]
 
 
 class LbmGpuError(RuntimeError):
@@ -72,8 +81,9 @@ def lib():
         for name in ("lbmgpu_destroy", "lbmgpu_init", "lbmgpu_collide_species", "lbmgpu_collide",
                      "lbmgpu_streaming", "lbmgpu_tms_bc", "lbmgpu_calculate_moment", "lbmgpu_synchronize"):
             getattr(L, name).argtypes = [vp]
-        L.lbmgpu_upload.argtypes = [vp, vp]
-        L.lbmgpu_download.argtypes = [vp, vp]
+        L.lbmgpu_upload.argtypes = [vp, vp, vp]
+        L.lbmgpu_download.argtypes = [vp, vp, vp]
+        L.lbmgpu_units_from_dx_dt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
         L.lbmgpu_step.argtypes = [vp, ctypes.c_int]
         L.lbmgpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.lbmgpu_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int]
@@ -100,6 +110,21 @@ def layout_of(dtype):
     return lay
 
 
+def species_layout_of(dtype):
+    lay = SpeciesLayout()
+    lay.size = dtype.itemsize
+    for name, _ in SpeciesLayout._fields_[1:]:
+        setattr(lay, name, dtype.fields[name][1])
+    return lay
+
+
+def units_from_dx_dt(dx, dt):
+    """(m, kg, s, K) as the reference's units.set_m_kg_s(dx, dt) leaves them."""
+    out = (ctypes.c_float * 4)()
+    _check(lib().lbmgpu_units_from_dx_dt(dx, dt, out), "lbmgpu_units_from_dx_dt")
+    return tuple(out)
+
+
 def _check(rc, what):
     if rc < 0:
         raise LbmGpuError(rc, what)
@@ -112,18 +137,31 @@ class Lattice:
     ``Nx, Ny, Nz`` include the ghost layer (the reference's LBM::Nx etc.).
     """
 
-    def __init__(self, Nx, Ny, Nz, nu, gas_const=1.0, gamma=1.4, prtl=0.5, device=0,
-                 precision=FP64, dtype=MIXTURE_SC, dt_sim=1):
+    def __init__(self, Nx, Ny, Nz, nu=0.0, gas_const=1.0, gamma=1.4, prtl=0.5, device=0,
+                 precision=FP64, dtype=MIXTURE_SC, dt_sim=1, mech=None, species_dtype=None, dx_dt=None,
+                 chem=CHEM_OFF):
+        """Single component: nu, gas_const, gamma, prtl.  Multicomponent: `mech` (a
+        mech.Mech table), `dtype`/`species_dtype` (the MIXTURE and SPECIES records) and
+        `dx_dt` (the arguments of the reference's units.set_m_kg_s(dx, dt))."""
         d = Desc()
         d.abi_version = ABI_VERSION
         d.device = device
         d.Nx, d.Ny, d.Nz = Nx, Ny, Nz
-        d.n_species = 0
         d.precision = precision
         d.dt_sim = dt_sim
         d.nu, d.gas_const, d.gamma, d.prtl = nu, gas_const, gamma, prtl
         d.mix = layout_of(dtype)
+        self.ns = 0
+        if mech is not None:
+            self.ns = mech.n_species
+            self._mech = mech
+            d.n_species = mech.n_species
+            d.mech = ctypes.addressof(mech)
+            d.spc = species_layout_of(species_dtype)
+            d.units_m, d.units_kg, d.units_s, d.units_K = units_from_dx_dt(*dx_dt)
+            d.chem_mode = chem
         self.dtype = dtype
+        self.species_dtype = species_dtype
         self.shape = (Nx, Ny, Nz)
         self.h = ctypes.c_void_p()
         _check(lib().lbmgpu_create(ctypes.byref(d), ctypes.byref(self.h)), "lbmgpu_create")
@@ -134,11 +172,23 @@ class Lattice:
             raise ValueError("cell array must be a C-contiguous %s array of shape %s" % (self.dtype, self.shape))
         return cells.ctypes.data
 
-    def upload(self, cells):
-        _check(lib().lbmgpu_upload(self.h, self._cells_ptr(cells)), "lbmgpu_upload")
+    def _species_ptrs(self, species):
+        if self.ns == 0:
+            return None
+        if species is None or len(species) != self.ns:
+            raise ValueError("one species array per species is required")
+        for sp in species:
+            if sp.dtype != self.species_dtype or sp.shape != self.shape or not sp.flags.c_contiguous:
+                raise ValueError("species arrays must be C-contiguous %s arrays of shape %s"
+                                 % (self.species_dtype, self.shape))
+        return (ctypes.c_void_p * self.ns)(*[sp.ctypes.data for sp in species])
 
-    def download(self, cells):
-        _check(lib().lbmgpu_download(self.h, self._cells_ptr(cells)), "lbmgpu_download")
+    def upload(self, cells, species=None):
+        _check(lib().lbmgpu_upload(self.h, self._cells_ptr(cells), self._species_ptrs(species)), "lbmgpu_upload")
+
+    def download(self, cells, species=None):
+        _check(lib().lbmgpu_download(self.h, self._cells_ptr(cells), self._species_ptrs(species)),
+               "lbmgpu_download")
 
     # -- the reference's phases -------------------------------------------------------
     def init(self):

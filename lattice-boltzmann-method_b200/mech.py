@@ -184,3 +184,81 @@ def load(path, species=H2_AIR_9):
         nr += 1
     m.n_reactions = nr
     return m
+
+
+def to_dict(m):
+    """The table as plain lists (JSON-serialisable)."""
+    out = {}
+    for name, ctype in Mech._fields_:
+        v = getattr(m, name)
+        if isinstance(v, int):
+            out[name] = v
+        elif name == "name":
+            out[name] = [m.name[k].value.decode() for k in range(MAX_SPECIES)]
+        else:
+            out[name] = _to_list(v)
+    return out
+
+
+def _to_list(v):
+    try:
+        return [_to_list(x) for x in v]
+    except TypeError:
+        return v
+
+
+def from_dict(d):
+    m = Mech()
+    for name, ctype in Mech._fields_:
+        v = d[name]
+        if isinstance(v, int):
+            setattr(m, name, v)
+        elif name == "name":
+            for k, s in enumerate(v):
+                m.name[k].value = s.encode()
+        else:
+            _fill(getattr(m, name), v)
+    return m
+
+
+def _fill(arr, v):
+    for i, x in enumerate(v):
+        if isinstance(x, list):
+            _fill(arr[i], x)
+        else:
+            arr[i] = x
+
+
+def save_json(m, path, source=""):
+    import json
+    d = to_dict(m)
+    d["_source"] = source
+    with open(path, "w") as fh:
+        json.dump(d, fh, separators=(",", ":"))
+
+
+def load_json(path):
+    import json
+    with open(path) as fh:
+        return from_dict(json.load(fh))
+
+
+DATA = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "data")
+H2_AIR_9_JSON = __import__("os").path.join(DATA, "h2_air_9.json")
+
+
+def h2_air_9():
+    """The 9-species H2/O2/N2 mechanism (23 reactions) extracted from the reference's
+    src/reaction-mech/nh3.yaml; regenerate with
+    ``python lattice-boltzmann-method_b200/mech.py <path to nh3.yaml>``."""
+    return load_json(H2_AIR_9_JSON)
+
+
+if __name__ == "__main__":
+    import sys
+    os_ = __import__("os")
+    os_.makedirs(DATA, exist_ok=True)
+    m = load(sys.argv[1], H2_AIR_9)
+    save_json(m, H2_AIR_9_JSON, source="nh3.yaml (farrasarira/Lattice-Boltzmann-Method src/reaction-mech), "
+                                       "species " + " ".join(H2_AIR_9))
+    print("wrote", H2_AIR_9_JSON, m.n_species, "species", m.n_reactions, "reactions")

@@ -109,3 +109,109 @@ def channel_sc(NX=24, NY=10, NZ=8, u_in=0.05, R=0.1, T0=1.0, T_wall=0.9, gamma=1
     c["u"][1:Nx - 1, 1:Ny - 1, 1:Nz - 1] = 0.0
     params = dict(nu=nu, R=R, gamma=gamma, prtl=prtl)
     return c, params
+
+
+# ---------------------------------------------------------------------------------------
+# Multicomponent states (MULTICOMP on): the mixture record (600 bytes) and one species
+# record per species (472 bytes), src/headers/lbm.hpp:56-102.
+# ---------------------------------------------------------------------------------------
+MIXTURE_MC = np.dtype({
+    "names": ["type", "p_tensor", "rho", "u", "v", "w", "p", "g", "gpc", "rhoe", "energy_flux", "temp", "HRR"],
+    "formats": ["<i2", ("<f8", (3, 3)), "<f8", "<f8", "<f8", "<f8", "<f8", ("<f8", 27), ("<f8", 27), "<f8",
+                ("<f8", 3), "<f8", "<f8"],
+    "offsets": [0, 8, 80, 88, 96, 104, 112, 120, 336, 552, 560, 584, 592],
+    "itemsize": 600,
+})
+SPECIES = np.dtype({
+    "names": ["X", "rho", "f", "fpc", "u", "v", "w"],
+    "formats": ["<f8", "<f8", ("<f8", 27), ("<f8", 27), "<f8", "<f8", "<f8"],
+    "offsets": [0, 8, 16, 232, 448, 456, 464],
+    "itemsize": 472,
+})
+
+# lattice units of the reference's flame cases (units.set_m_kg_s(20e-6, 1e-9), setup.cpp:2758):
+# dx = 20 um, dt = 1 ns, temperature unit 12000 K (units.hpp:32-44)
+FLAME_UNITS = (20e-6, 1e-9)
+K_UNIT = 12000.0
+ONE_ATM = 101325.0
+SPECIES_MIN = 1e-8
+
+
+def p_lattice(p_si, units=FLAME_UNITS):
+    """units.p(): SI pressure to lattice units, in float arithmetic like the reference."""
+    m = np.float32(units[0])
+    s = np.float32(units[1])
+    kg = np.float32(float(m) ** 3)
+    return float(np.float32(p_si) * (m * (s * s)) / kg)
+
+
+def t_lattice(T_si):
+    """units.temp(): SI temperature to lattice units (float)."""
+    return float(np.float32(T_si) / np.float32(K_UNIT))
+
+
+def u_lattice(u_si, units=FLAME_UNITS):
+    m = np.float32(units[0])
+    s = np.float32(units[1])
+    return float(np.float32(u_si) * s / m)
+
+
+def _blank_mc(NX, NY, NZ, ns):
+    shape = (NX + 2, NY + 2, NZ + 2)
+    mix = np.zeros(shape, dtype=MIXTURE_MC)
+    mix["type"] = TYPE_F
+    mix["rho"] = 1.0
+    mix["p"] = 1.0 / 3.0
+    mix["temp"] = 1.0 / 3.0
+    sp = [np.zeros(shape, dtype=SPECIES) for _ in range(ns)]
+    return mix, sp
+
+
+def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=1000.0, amp=0.1, width=1.5,
+                    u_si=0.0, seed=SEED, periodic_x=True):
+    """Seeded sinusoidal H2/air interface (the non-reacting mixing case): H2 mass fraction
+    from 0 to Y_H2 (balance air, O2:N2 = 0.233:0.767 by mass), T from T_lo to T_hi across a
+    tanh interface at x0 + A sin(2 pi y/L + phi1) sin(2 pi z/L + phi2) with random phases;
+    p = 1 atm; the remaining species at mole fraction 1e-8.  With periodic_x the domain
+    holds a hot H2 slab between two such interfaces (fully periodic box)."""
+    NY = NY or N
+    NZ = NZ or N
+    names = mech.species_names()
+    ns = len(names)
+    mix, sp = _blank_mc(N, NY, NZ, ns)
+    Nx, Ny, Nz = mix.shape
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ph = rng.uniform(0, 2 * np.pi, size=4)
+    i, j, k = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    ghost = (i == 0) | (i == Nx - 1) | (j == 0) | (j == Ny - 1) | (k == 0) | (k == Nz - 1)
+    mix["type"][ghost] = TYPE_P
+    A = amp * N
+    y2 = 2 * np.pi * j / NY
+    z2 = 2 * np.pi * k / NZ
+    x0 = 0.3 * N + A * np.sin(y2 + ph[0]) * np.sin(z2 + ph[1])
+    x1 = 0.7 * N + A * np.sin(y2 + ph[2]) * np.sin(z2 + ph[3])
+    if periodic_x:
+        s = 0.5 * (1 + np.tanh((i - x0) / width)) * 0.5 * (1 + np.tanh((x1 - i) / width))
+    else:
+        s = 0.5 * (1 + np.tanh((i - x0) / width))
+    W = np.array([mech.W[kk] for kk in range(ns)])
+    Y = np.zeros(mix.shape + (ns,))
+    Y[..., names.index("H2")] = Y_H2 * s
+    air = 1.0 - Y[..., names.index("H2")]
+    Y[..., names.index("O2")] = 0.233 * air
+    Y[..., names.index("N2")] = 0.767 * air
+    X = Y / W
+    X /= X.sum(-1, keepdims=True)
+    for a, n in enumerate(names):
+        if n not in ("H2", "O2", "N2"):
+            X[..., a] = SPECIES_MIN
+    X[..., names.index("H2")] = np.maximum(X[..., names.index("H2")], SPECIES_MIN)
+    X /= X.sum(-1, keepdims=True)
+    fl = ~ghost
+    T = T_lo + (T_hi - T_lo) * s
+    mix["temp"][fl] = np.float32(T[fl] / K_UNIT).astype(np.float64)
+    mix["p"][fl] = p_lattice(ONE_ATM)
+    mix["u"][fl] = u_lattice(u_si)
+    for a in range(ns):
+        sp[a]["X"][fl] = X[..., a][fl]
+    return mix, sp

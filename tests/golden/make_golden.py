@@ -14,7 +14,11 @@ compiled unchanged -- on seeded inputs and records:
                            fields after 1 and 40 steps;
 * ``sc_channel_fs.npz``    the same channel with free-slip z walls;
 * ``sc_tgv64.npz``         the 64^3, Re 400, Ma 0.1 Taylor-Green vortex: fields on every
-                           4th cell per axis and whole-field sums after 100 and 1000 steps.
+                           4th cell per axis and whole-field sums after 100 and 1000 steps;
+* ``mc_mix8.npz``          8^3 periodic 9-species H2/air mixing layer (REACTION off), the
+                           reference's multicomponent solver on the Cantera-API shim, fields
+                           after 1 and 40 steps;
+* ``mc_react8.npz``        the same with REACTION on and an 1800 K hot slab, 30 steps.
 """
 import hashlib
 import os
@@ -26,7 +30,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle import cases, refsc  # noqa: E402
+from oracle import cases, refmc, refsc  # noqa: E402
+
+sys.path.insert(0, os.path.join(ROOT, "lattice-boltzmann-method_b200"))
+import mech as mechmod  # noqa: E402
+
+MECH_PATH = "/root/reference/src/reaction-mech/nh3.yaml"
+MC_FIELDS = ["rho", "u", "v", "w", "temp", "p", "rhoe", "HRR"]
 
 FIELDS = ["rho", "u", "v", "w", "temp", "p"]
 
@@ -115,7 +125,49 @@ def kat(seed=cases.SEED, n=64):
     return out
 
 
+def run_ref_mc(mix, sp, m, checkpoints, reaction, pop_cells):
+    NX, NY, NZ = [s_ - 2 for s_ in mix.shape]
+    ref = refmc.RefMC(NX, NY, NZ, m, cases.FLAME_UNITS, cases.MIXTURE_MC, cases.SPECIES, reaction=reaction)
+    ref.cells[...] = mix
+    for a in range(len(sp)):
+        ref.species[a][...] = sp[a]
+    ref.init()
+    out = {}
+    done = 0
+    idx = tuple(pop_cells.T)
+    for cp in checkpoints:
+        ref.loop(cp - done)
+        done = cp
+        for f in MC_FIELDS:
+            out[f"{f}_{cp}"] = np.ascontiguousarray(ref.cells[f])
+        out[f"sp_rho_{cp}"] = np.stack([ref.species[a]["rho"] for a in range(len(sp))])
+        out[f"sp_X_{cp}"] = np.stack([ref.species[a]["X"] for a in range(len(sp))])
+        out[f"sp_u_{cp}"] = np.stack([ref.species[a]["u"] for a in range(len(sp))])
+        out[f"sp_f_{cp}"] = np.stack([ref.species[a]["f"][idx] for a in range(len(sp))])
+        out[f"sp_fpc_{cp}"] = np.stack([ref.species[a]["fpc"][idx] for a in range(len(sp))])
+        out[f"g_{cp}"] = np.ascontiguousarray(ref.cells["g"][idx])
+        out[f"p_tensor_{cp}"] = np.ascontiguousarray(ref.cells["p_tensor"][idx])
+    ref.close()
+    return out
+
+
+def mc_digest(mix, sp):
+    h = hashlib.sha256(np.ascontiguousarray(mix).tobytes())
+    for a in sp:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
 def main():
+    only = sys.argv[1] if len(sys.argv) > 1 else "all"   # "sc", "mc" or "all"
+    if only in ("all", "sc"):
+        make_sc()
+    if only in ("all", "mc"):
+        make_mc()
+    print("fixtures written to", HERE)
+
+
+def make_sc():
     if not refsc.available():
         raise SystemExit("oracle/_ref/libref_sc.so missing: run `make -C oracle ref` first")
     refsc.set_threads(os.cpu_count() or 1)
@@ -138,7 +190,18 @@ def main():
     out = run_ref(cells, params, [100, 1000], sample=sample)
     out.update(input_sha256=digest(cells))
     np.savez_compressed(os.path.join(HERE, "sc_tgv64.npz"), **out)
-    print("fixtures written to", HERE)
+
+
+def make_mc():
+    m = mechmod.h2_air_9()
+    refmc.set_threads(os.cpu_count() or 1)
+    for name, reaction, kw, cps in (("mc_mix8.npz", False, {}, [1, 40]),
+                                    ("mc_react8.npz", True, {"T_hi": 1800.0}, [1, 30])):
+        mix, sp = cases.mixing_layer_mc(m, N=8, **kw)
+        pc = pick_cells(mix, 16, 3)
+        out = run_ref_mc(mix, sp, m, cps, reaction, pc)
+        out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
+        np.savez_compressed(os.path.join(HERE, name), **out)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,84 @@
+"""Helpers shared by the multicomponent tests: the seeded inputs of the fixtures and the
+host build of the device's per-cell functions (tests/host/mc_host.cpp)."""
+import ctypes
+import hashlib
+import os
+import subprocess
+
+import numpy as np
+
+import mech
+import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+CSRC = os.path.join(ROOT, "lattice-boltzmann-method_b200", "csrc")
+NS = 9
+NREC = 14 + 8 * NS
+CASES = {
+    "mc_mix8.npz": (False, {}, [1, 40]),
+    "mc_react8.npz": (True, {"T_hi": 1800.0}, [1, 30]),
+}
+
+
+def case(fixture):
+    reaction, kw, cps = CASES[fixture]
+    m = mech.h2_air_9()
+    mix, sp = W.mixing_layer_mc(m, N=8, **kw)
+    return m, mix, sp, reaction, cps
+
+
+def digest(mix, sp):
+    h = hashlib.sha256(np.ascontiguousarray(mix).tobytes())
+    for a in sp:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def rel(got, want, scale=None):
+    scale = max(np.max(np.abs(want)) if scale is None else scale, 1e-300)
+    return float(np.max(np.abs(got - want)) / scale)
+
+
+def build_host_lib(tmpdir):
+    out = os.path.join(str(tmpdir), "libmchost.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC,
+                    os.path.join(ROOT, "tests", "host", "mc_host.cpp"), "-o", out], check=True)
+    return ctypes.CDLL(out)
+
+
+def soa_state(mix, sp):
+    """The device record/population planes of an AoS state (as the upload builds them)."""
+    nc = mix.size
+    rec = np.zeros((NREC, nc))
+    f = lambda a: np.ascontiguousarray(a).reshape(-1)  # noqa: E731
+    for q, k in enumerate(["rho", "u", "v", "w", "temp", "p", "rhoe"]):
+        rec[q] = f(mix[k])
+    P = mix["p_tensor"].reshape(-1, 9)
+    for q, (a, b) in enumerate([(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]):
+        rec[7 + q] = P[:, 3 * a + b]
+    rec[13] = f(mix["HRR"])
+    for a in range(NS):
+        base = 14 + 8 * a
+        rec[base] = f(sp[a]["rho"])
+        rec[base + 4] = f(sp[a]["u"])
+        rec[base + 5] = f(sp[a]["v"])
+        rec[base + 6] = f(sp[a]["w"])
+        rec[base + 7] = f(sp[a]["X"])
+    return rec
+
+
+def host_run(L, m, mix, sp, reaction, steps):
+    rec0 = soa_state(mix, sp)
+    rec1 = rec0.copy()
+    nc = mix.size
+    pop0 = np.zeros((27 * (NS + 1), nc))
+    pop1 = np.zeros_like(pop0)
+    typ = np.ascontiguousarray(mix["type"].astype(np.int8).reshape(-1))
+    st = ctypes.c_uint(0)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    L.mc_host_run.restype = ctypes.c_int
+    cur = L.mc_host_run(*mix.shape, P(typ), ctypes.byref(m), ctypes.c_float(W.FLAME_UNITS[0]),
+                        ctypes.c_float(W.FLAME_UNITS[1]), int(reaction), steps, P(pop0), P(pop1), P(rec0),
+                        P(rec1), 1, ctypes.byref(st))
+    return (rec0, rec1)[cur], st.value
