@@ -167,13 +167,16 @@ def _blank_mc(NX, NY, NZ, ns):
     return mix, sp
 
 
-def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=1000.0, amp=0.1, width=1.5,
+def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=1000.0, amp=0.1, width=None,
                     u_si=0.0, seed=SEED, periodic_x=True):
     """Seeded sinusoidal H2/air interface (the non-reacting mixing case): H2 mass fraction
     from 0 to Y_H2 (balance air, O2:N2 = 0.233:0.767 by mass), T from T_lo to T_hi across a
     tanh interface at x0 + A sin(2 pi y/L + phi1) sin(2 pi z/L + phi2) with random phases;
     p = 1 atm; the remaining species at mole fraction 1e-8.  With periodic_x the domain
-    holds a hot H2 slab between two such interfaces (fully periodic box)."""
+    holds a hot H2 slab between two such interfaces (fully periodic box).  The tanh width
+    defaults to max(1.5, N/8) cells: sharper 300 K -> 1000 K fronts drive the reference's own
+    solver unstable within a few steps at 32^3."""
+    width = max(1.5, N / 8.0) if width is None else width
     NY = NY or N
     NZ = NZ or N
     names = mech.species_names()
