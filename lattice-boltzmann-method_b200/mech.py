@@ -261,4 +261,7 @@ if __name__ == "__main__":
     m = load(sys.argv[1], H2_AIR_9)
     save_json(m, H2_AIR_9_JSON, source="nh3.yaml (farrasarira/Lattice-Boltzmann-Method src/reaction-mech), "
                                        "species " + " ".join(H2_AIR_9))
+    # the raw struct, for C/C++ callers: fread(&mech, sizeof(lbmgpu_mech), 1, f)
+    with open(H2_AIR_9_JSON[:-5] + ".bin", "wb") as fh:
+        fh.write(bytes(m))
     print("wrote", H2_AIR_9_JSON, m.n_species, "species", m.n_reactions, "reactions")
