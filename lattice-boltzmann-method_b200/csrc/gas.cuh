@@ -8,7 +8,11 @@
 //      cp/R = a1 + a2 T + a3 T^2 + a4 T^3 + a5 T^4,  h/RT = a1 + a2 T/2 + ... + a6/T,
 //      s/R = a1 ln T + a2 T + a3 T^2/2 + a4 T^3/3 + a5 T^4/4 + a7;
 //    T from (u, v) by Newton iteration on u(T) (what setState_UV solves).
-//  * transport: Chapman-Enskog species viscosities and binary diffusion coefficients with
+//  * transport: as CHEMKIN's TRANFIT and Cantera do, the kinetic-theory expressions below
+//    are evaluated at 50 temperatures and fitted once (make_tables) by degree-4
+//    polynomials in ln T: ln mu_k, ln lambda_k and ln(D_kj P); the per-cell evaluation is
+//    then one polynomial and one exp per property.  The kinetic theory:
+//    Chapman-Enskog species viscosities and binary diffusion coefficients with
 //    the Neufeld, Janzen & Aziz (1972) fits of the Lennard-Jones collision integrals
 //    Omega(2,2)* and Omega(1,1)*, Brokaw's dipole correction, the polar/non-polar
 //    combining rules of the CHEMKIN transport formulation (Kee et al., SAND86-8246);
@@ -57,7 +61,18 @@ struct Tables {
     double delta_pair[MAXS][MAXS];
     double cvrot_R[MAXS];              // rotational heat capacity / R
     double zrot298_F298[MAXS];         // Z_rot(298) F(298), Z_rot(T) = this / F(T)
+    // fits in x = ln T - kFitX0 (Horner order c[4] x^4 + ... + c[0])
+    double fit_visc[MAXS][5];          // ln mu_k           [Pa s]
+    double fit_cond[MAXS][5];          // ln lambda_k       [W/(m K)]
+    double fit_diff[MAXS][MAXS][5];    // ln (D_kj * P)     [m^2 Pa / s]
+    // per-species constants of the lattice collision, set by the device setup
+    double Ra_lat[MAXS];               // units.cp(R / W_a)
+    double sqrt4W[MAXS][MAXS];         // sqrt(sqrt(W_b / W_a))   (Wilke factor, reference order)
+    double wilke_den[MAXS][MAXS];      // sqrt(8 (1 + W_a / W_b))
 };
+
+constexpr double kFitTlo = 200.0, kFitThi = 3500.0, kFitX0 = 7.0;
+constexpr int kFitN = 50;
 
 GAS_HD double sq(double x) { return x * x; }
 
@@ -78,8 +93,7 @@ GAS_HD double parker_F(double eps_over_T) {
     return 1.0 + 0.5 * pow(kPi, 1.5) * sqrt(x) + (0.25 * kPi * kPi + 2.0) * x + pow(kPi, 1.5) * x * sqrt(x);
 }
 
-// Host-side construction of the derived constants.
-inline void make_tables(const lbmgpu_mech &m, Tables &t) {
+inline void make_tables_base(const lbmgpu_mech &m, Tables &t) {
     t.m = m;
     t.ns = m.n_species;
     for (int k = 0; k < t.ns; ++k) {
@@ -174,13 +188,25 @@ GAS_HD int T_from_u(const Tables &t, const double *Y, double u, double T0, doubl
     return -1;
 }
 
-// ---- transport ---------------------------------------------------------------------
-GAS_HD double species_visc(const Tables &t, int k, double T) {
+// ---- transport: kinetic theory (evaluated at setup only) ---------------------------
+inline double species_visc_kt(const Tables &t, int k, double T) {
     return t.visc_pref[k] * sqrt(T) / omega22(T / t.eps[k], t.delta[k]);
 }
+inline double binary_diff_kt(const Tables &t, int k, int j, double T, double P) {
+    return t.diff_pref[k][j] * T * sqrt(T) / (P * omega11(T / t.eps_pair[k][j], t.delta_pair[k][j]));
+}
+
+// ---- transport: fitted (per cell) --------------------------------------------------
+GAS_HD double fit_eval(const double *c, double x) { return c[0] + x * (c[1] + x * (c[2] + x * (c[3] + x * c[4]))); }
+GAS_HD double lnT_x(double T) { return log(T) - kFitX0; }
+GAS_HD double species_visc(const Tables &t, int k, double T) { return exp(fit_eval(t.fit_visc[k], lnT_x(T))); }
+GAS_HD double species_visc_x(const Tables &t, int k, double x) { return exp(fit_eval(t.fit_visc[k], x)); }
 // D_kj at (T, P), m^2/s
 GAS_HD double binary_diff(const Tables &t, int k, int j, double T, double P) {
-    return t.diff_pref[k][j] * T * sqrt(T) / (P * omega11(T / t.eps_pair[k][j], t.delta_pair[k][j]));
+    return exp(fit_eval(t.fit_diff[k][j], lnT_x(T))) / P;
+}
+GAS_HD double binary_diff_x(const Tables &t, int k, int j, double x, double P) {
+    return exp(fit_eval(t.fit_diff[k][j], x)) / P;
 }
 
 // Wilke's mixing rule with the species viscosities mu[] and mole fractions X[].
@@ -189,19 +215,19 @@ GAS_HD double wilke(const Tables &t, const double *X, const double *mu) {
     for (int k = 0; k < t.ns; ++k) {
         double d = 0.0;
         for (int j = 0; j < t.ns; ++j) {
-            const double f = 1.0 + sqrt(mu[k] / mu[j]) * sqrt(sqrt(t.m.W[j] / t.m.W[k]));
-            d += X[j] * f * f / sqrt(8.0 * (1.0 + t.m.W[k] / t.m.W[j]));
+            const double f = 1.0 + sqrt(mu[k] / mu[j]) * t.sqrt4W[k][j];
+            d += X[j] * f * f / t.wilke_den[k][j];
         }
         s += X[k] * mu[k] / d;
     }
     return s;
 }
 
-// Species thermal conductivity (Warnatz / CHEMKIN), W/(m K).
-GAS_HD double species_cond(const Tables &t, int k, double T, double P, double mu_k) {
+// Species thermal conductivity (Warnatz / CHEMKIN), W/(m K), from kinetic theory.
+inline double species_cond_kt(const Tables &t, int k, double T, double P, double mu_k) {
     const double W = t.m.W[k];
     const double rho = P * W / (kR * T);
-    const double Dkk = binary_diff(t, k, k, T, P);
+    const double Dkk = binary_diff_kt(t, k, k, T, P);
     const double rdm = rho * Dkk / mu_k;
     const double cv_R = cp_R(t, k, T) - 1.0;
     if (t.m.geometry[k] == LBMGPU_GEOM_ATOM) return mu_k / W * kR * 2.5 * 1.5;
@@ -215,10 +241,16 @@ GAS_HD double species_cond(const Tables &t, int k, double T, double P, double mu
     return mu_k / W * kR * (ftr * 1.5 + frot * cvrot + rdm * cvvib);
 }
 
+GAS_HD double species_cond(const Tables &t, int k, double T) { return exp(fit_eval(t.fit_cond[k], lnT_x(T))); }
+GAS_HD double species_cond_x(const Tables &t, int k, double x) { return exp(fit_eval(t.fit_cond[k], x)); }
+
+// Mixture conductivity (Mathur-Tondon-Saxena average of the species values).
 GAS_HD double mix_cond(const Tables &t, const double *X, double T, double P, const double *mu) {
+    (void)P;
+    (void)mu;
     double s1 = 0.0, s2 = 0.0;
     for (int k = 0; k < t.ns; ++k) {
-        const double lk = species_cond(t, k, T, P, mu[k]);
+        const double lk = species_cond(t, k, T);
         s1 += X[k] * lk;
         s2 += X[k] / lk;
     }
@@ -283,6 +315,71 @@ GAS_HD void net_production(const Tables &t, double T, const double *C, double *w
         for (int j = 0; j < m.n_prod[r]; ++j) wdot[m.prod[r][j]] += m.nu_prod[r][j] * q;
     }
     (void)Ctot;
+}
+
+// Least-squares polynomial fit (degree 4) of y(x) on n points; normal equations solved
+// by Gaussian elimination with partial pivoting (host, setup only).
+inline void polyfit4(const double *x, const double *y, int n, double *c) {
+    double A[5][6] = {};
+    for (int i = 0; i < n; ++i) {
+        double p[5] = {1.0, x[i], x[i] * x[i], x[i] * x[i] * x[i], x[i] * x[i] * x[i] * x[i]};
+        for (int r = 0; r < 5; ++r) {
+            for (int q = 0; q < 5; ++q) A[r][q] += p[r] * p[q];
+            A[r][5] += p[r] * y[i];
+        }
+    }
+    for (int col = 0; col < 5; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 5; ++r)
+            if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
+        for (int q = 0; q < 6; ++q) {
+            const double tmp = A[col][q];
+            A[col][q] = A[piv][q];
+            A[piv][q] = tmp;
+        }
+        for (int r = col + 1; r < 5; ++r) {
+            const double f = A[r][col] / A[col][col];
+            for (int q = col; q < 6; ++q) A[r][q] -= f * A[col][q];
+        }
+    }
+    for (int r = 4; r >= 0; --r) {
+        double v = A[r][5];
+        for (int q = r + 1; q < 5; ++q) v -= A[r][q] * c[q];
+        c[r] = v / A[r][r];
+    }
+}
+
+// Host-side construction of the derived constants and the transport fits.
+inline void make_tables(const lbmgpu_mech &m, Tables &t) {
+    make_tables_base(m, t);
+    double x[kFitN], y[kFitN];
+    const double P = kOneAtm;
+    for (int k = 0; k < t.ns; ++k) {
+        for (int i = 0; i < kFitN; ++i) {
+            const double T = kFitTlo + (kFitThi - kFitTlo) * i / (kFitN - 1);
+            x[i] = log(T) - kFitX0;
+            y[i] = log(species_visc_kt(t, k, T));
+        }
+        polyfit4(x, y, kFitN, t.fit_visc[k]);
+        for (int i = 0; i < kFitN; ++i) {
+            const double T = kFitTlo + (kFitThi - kFitTlo) * i / (kFitN - 1);
+            y[i] = log(species_cond_kt(t, k, T, P, species_visc_kt(t, k, T)));
+        }
+        polyfit4(x, y, kFitN, t.fit_cond[k]);
+        for (int j = 0; j < t.ns; ++j) {
+            for (int i = 0; i < kFitN; ++i) {
+                const double T = kFitTlo + (kFitThi - kFitTlo) * i / (kFitN - 1);
+                y[i] = log(binary_diff_kt(t, k, j, T, P) * P);
+            }
+            polyfit4(x, y, kFitN, t.fit_diff[k][j]);
+        }
+    }
+    for (int a = 0; a < t.ns; ++a)
+        for (int b = 0; b < t.ns; ++b) {
+            t.sqrt4W[a][b] = sqrt(sqrt(m.W[b] / m.W[a]));
+            t.wilke_den[a][b] = sqrt(8.0 * (1.0 + m.W[a] / m.W[b]));
+        }
+    for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = 0.0;
 }
 
 }  // namespace gas

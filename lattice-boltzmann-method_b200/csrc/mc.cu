@@ -208,6 +208,7 @@ int mc_setup(lbmgpu *h) {
     }
     gas::Tables *ht = new gas::Tables();
     gas::make_tables(*d.mech, *ht);
+    set_lattice_constants(*ht, h->U);
     int rc = dalloc(h, &h->tab, 1);
     if (!rc) {
         cudaError_t e = cudaMemcpy(h->tab, ht, sizeof(gas::Tables), cudaMemcpyHostToDevice);

@@ -63,6 +63,11 @@ struct McArgs {
 
 MC_HD double rec(const McArgs &A, const double *r, int plane, long n) { return r[(long)plane * A.ncell + n]; }
 
+// Per-species constants of the lattice collision that depend on the units (host, setup).
+inline void set_lattice_constants(gas::Tables &t, const UnitsF &U) {
+    for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = u_cp(U, (float)(gas::kR / t.m.W[a]));
+}
+
 MC_HD void atomic_status(unsigned *s, unsigned bits) {
 #if defined(__CUDA_ARCH__)
     atomicOr(s, bits);
@@ -182,17 +187,17 @@ MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
     // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky
     double M[NS][NS];
     const double p_old = rec(A, A.rec_cur, RM_P, n);
-    for (int a = 0; a < NS; ++a)
-        for (int b = 0; b < NS; ++b) {
-            if (b == a) {
-                M[a][b] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
-            } else {
-                const int lo = a > b ? a : b, hi = a > b ? b : a;  // D stored for b <= a
-                const double D = u_nu(A.U, (float)gas::binary_diff(t, lo, hi, T_si, P_si));
-                M[a][b] = -1.0 * A.dt / 2.0 * p_old * rec(A, A.rec_cur, rs(a, RS_X), n) *
-                          rec(A, A.rec_cur, rs(b, RS_X), n) / D;
-            }
+    const double xT = gas::lnT_x(T_si);
+    double Xold[NS];
+    for (int a = 0; a < NS; ++a) Xold[a] = rec(A, A.rec_cur, rs(a, RS_X), n);
+    for (int a = 0; a < NS; ++a) {
+        M[a][a] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
+        for (int b = 0; b < a; ++b) {  // D_ab of the reference's lower triangle, one per pair
+            const double D = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            M[a][b] = -1.0 * A.dt / 2.0 * p_old * Xold[a] * Xold[b] / D;
+            M[b][a] = -1.0 * A.dt / 2.0 * p_old * Xold[b] * Xold[a] / D;
         }
+    }
     for (int a = 0; a < NS; ++a)
         for (int b = 0; b < NS; ++b)
             if (b != a) M[a][a] -= M[a][b];
@@ -321,29 +326,35 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
     }
 
     // -- species viscosities, Wilke weights, relaxation rates (lbm-collision.cpp:402-430)
+    const double xT = gas::lnT_x(T_si);
     double mu_k[NS];
-    for (int a = 0; a < NS; ++a) mu_k[a] = gas::species_visc(t, a, T_si);
+    for (int a = 0; a < NS; ++a) mu_k[a] = gas::species_visc_x(t, a, xT);
+    // Wilke weights phi[a][b] as the reference forms them: for b >= a directly, for b < a
+    // from phi[b][a] (lbm-collision.cpp:408-417)
+    double phi[NS][NS];
+    for (int a = 0; a < NS; ++a)
+        for (int b = a; b < NS; ++b) {
+            const double f1 = 1.0 + sqrt(mu_k[a] / mu_k[b]) * t.sqrt4W[a][b];
+            phi[a][b] = f1 * f1 / t.wilke_den[a][b];
+            phi[b][a] = mu_k[b] / mu_k[a] * t.m.W[a] / t.m.W[b] * phi[a][b];
+        }
     double om_a[NS];
     for (int a = 0; a < NS; ++a) {
         double denom = 0.0;
-        for (int b = 0; b < NS; ++b) {
-            // phi[a][b] of the reference (computed for b >= a, mirrored for b < a)
-            double phi;
-            if (b >= a) {
-                const double f1 = 1.0 + sqrt(mu_k[a] / mu_k[b]) * sqrt(sqrt(t.m.W[b] / t.m.W[a]));
-                phi = f1 * f1 / sqrt(8.0 * (1.0 + t.m.W[a] / t.m.W[b]));
-            } else {
-                const double f1 = 1.0 + sqrt(mu_k[b] / mu_k[a]) * sqrt(sqrt(t.m.W[a] / t.m.W[b]));
-                const double pba = f1 * f1 / sqrt(8.0 * (1.0 + t.m.W[b] / t.m.W[a]));
-                phi = mu_k[a] / mu_k[b] * t.m.W[b] / t.m.W[a] * pba;
-            }
-            denom = denom + Xs[b] * phi;
-        }
+        for (int b = 0; b < NS; ++b) denom = denom + Xs[b] * phi[a][b];
         const double visc = Xs[a] * (double)u_mu(A.U, (float)mu_k[a]) / denom;
         om_a[a] = 2 * Xs[a] * p * dt / (Xs[a] * p * dt + 2 * visc);
     }
 
     // -- Maxwell-Stefan force (lbm-collision.cpp:433-471)
+    double Dl[NS][NS];  // lattice D_ab, one evaluation per pair (the diagonal term vanishes)
+    for (int a = 0; a < NS; ++a) {
+        Dl[a][a] = u_nu(A.U, (float)gas::binary_diff_x(t, a, a, xT, P_si));
+        for (int b = 0; b < a; ++b) {
+            Dl[a][b] = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            Dl[b][a] = Dl[a][b];
+        }
+    }
     double F[NS][3], ux[NS][3];
     for (int a = 0; a < NS; ++a) {
         for (int d = 0; d < 3; ++d) {
@@ -351,8 +362,7 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
             F[a][d] = 0.0;
         }
         for (int b = 0; b < NS; ++b) {
-            const int lo = a > b ? a : b, hi = a > b ? b : a;
-            const double D = u_nu(A.U, (float)gas::binary_diff(t, lo, hi, T_si, P_si));
+            const double D = Dl[a][b];
             for (int d = 0; d < 3; ++d) F[a][d] += -1.0 * p * Xs[a] * Xs[b] / D * (ua[a][d] - ua[b][d]);
         }
         for (int d = 0; d < 3; ++d) F[a][d] = F[a][d] * dt / rho_a[a];
@@ -371,7 +381,7 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
 
     // -- species collision (lbm-collision.cpp:479-519)
     for (int a = 0; a < NS; ++a) {
-        const double Ra = u_cp(A.U, (float)(gas::kR / t.m.W[a]));
+        const double Ra = t.Ra_lat[a];
         const double theta = Ra * Tl;
         double corr[3];
         for (int d = 0; d < 3; ++d) {

@@ -9,7 +9,8 @@ void gp_set_mech(const lbmgpu_mech *m) { gas::make_tables(*m, g_t); }
 double gp_species_visc(int k, double T) { return gas::species_visc(g_t, k, T); }
 double gp_binary_diff(int k, int j, double T, double P) { return gas::binary_diff(g_t, k, j, T, P); }
 double gp_species_cond(int k, double T, double P) {
-    return gas::species_cond(g_t, k, T, P, gas::species_visc(g_t, k, T));
+    (void)P;
+    return gas::species_cond(g_t, k, T);
 }
 double gp_mix_visc(const double *X, double T) {
     double mu[gas::MAXS];

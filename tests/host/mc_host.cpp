@@ -14,6 +14,8 @@ extern "C" int mc_host_run(int Nx, int Ny, int Nz, const signed char *type, cons
     gas::make_tables(*mech, tab);
     if (mech->n_species != 9) return -1;
     McArgs A{};
+    const UnitsF U = units_from_dx_dt(dx, dt);
+    set_lattice_constants(tab, U);
     A.Nx = Nx;
     A.Ny = Ny;
     A.Nz = Nz;
@@ -23,7 +25,7 @@ extern "C" int mc_host_run(int Nx, int Ny, int Nz, const signed char *type, cons
     A.ns = 9;
     A.dt = 1;
     A.chem = chem;
-    A.U = units_from_dx_dt(dx, dt);
+    A.U = U;
     A.tab = &tab;
     A.type = reinterpret_cast<const int8_t *>(type);
     A.status = status;
