@@ -186,6 +186,22 @@ def fluid_cells(cells):
     return int((cells["type"] == 0).sum())
 
 
+class stdout_to_stderr:
+    """Routes the process's file-descriptor-level stdout to stderr (the reference's own
+    solver prints progress with std::cout; the bench's stdout carries one JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
 def cpu_reference_run(cells, prm, steps, warmup, threads):
     """Times the reference's own solver (oracle/_ref) -- or, where it was not built, the C
     oracle port -- for `steps` steps after `warmup`; returns (seconds, kind)."""
@@ -233,7 +249,8 @@ def run_reference(args, dist):
         return
     cells, prm = workload(args.N)
     threads = os.cpu_count() or 1
-    dt, kind = cpu_reference_run(cells, prm, args.steps, args.warmup, threads)
+    with stdout_to_stderr():
+        dt, kind = cpu_reference_run(cells, prm, args.steps, args.warmup, threads)
     ncell = fluid_cells(cells)
     v = ncell * args.steps / dt / 1e6
     line = {
@@ -365,7 +382,8 @@ def run_ours_mc(args, dist):
         try:
             threads = os.cpu_count() or 1
             n = 3
-            dt = mc_cpu_run(m, mix, sp, n, 1, threads, reaction)
+            with stdout_to_stderr():
+                dt = mc_cpu_run(m, mix, sp, n, 1, threads, reaction)
             line["cpu_baseline"] = {"value": ncell * n / dt / 1e6, "unit": "MLUPS", "cores": threads,
                                     "kind": "reference",
                                     "sample": f"{n} steps after 1 warm-up step, reference multicomponent LBM + "
@@ -473,7 +491,8 @@ def run_ours(args, dist):
     }
     if dist.world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline(cells, prm)
+            with stdout_to_stderr():
+                line["cpu_baseline"] = cpu_baseline(cells, prm)
         except Exception as exc:  # the baseline never decides the GPU number
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
     print(json.dumps(line), flush=True)

@@ -1,0 +1,142 @@
+// Stiff per-cell chemistry over one lattice time step: the constant-volume,
+// constant-internal-energy reactor
+//     dY_k/dt = wdot_k W_k / rho,
+//     dT/dt   = -sum_k e_k wdot_k W_k / (rho c_v),   e_k = h_k - R T / W_k (per mass),
+// integrated with the two-stage L-stable Rosenbrock method ROS2 (Verwer, Spee, Blom &
+// Hundsdorfer, SIAM J. Sci. Comput. 20 (1999) 1456; gamma = 1 + 1/sqrt 2):
+//     (I - gamma h J) k1 = F(y)
+//     (I - gamma h J) k2 = F(y + h k1) - 2 k1
+//     y+ = y + 3/2 h k1 + 1/2 h k2,   error estimate e = 1/2 h (k1 + k2)  (vs. the embedded
+//     first-order y + h k1),
+// with a finite-difference Jacobian, a partial-pivot LU of the (nS+1)^2 system in FP64,
+// step-size control on the error norm, and a hard cap on the number of sub-steps (the
+// caller raises a status bit when it is reached; nothing spins).
+#pragma once
+#include <math.h>
+
+#include "gas.cuh"
+
+namespace gas {
+
+constexpr int kChemMaxSub = 256;
+
+// right-hand side of the reactor state y = (Y_0..Y_{ns-1}, T) at density rho (kg/m^3)
+GAS_HD void reactor_rhs(const Tables &t, double rho, const double *y, double *F) {
+    const int ns = t.ns;
+    double C[MAXS], w[MAXS];
+    const double T = y[ns];
+    for (int k = 0; k < ns; ++k) C[k] = rho * y[k] * t.invW[k];
+    net_production(t, T, C, w);
+    double cv = 0.0, s = 0.0;
+    for (int k = 0; k < ns; ++k) {
+        F[k] = w[k] * t.m.W[k] / rho;
+        cv += y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
+        s += (h_RT(t, k, T) - 1.0) * kR * T * w[k];   // e_k W_k = h_k,molar - R T
+    }
+    cv *= kR;
+    F[ns] = -s / (rho * cv);
+}
+
+// LU with partial pivoting of an n x n matrix (row-major, stride MAXS+1); returns false
+// on a zero pivot.
+GAS_HD bool lu_factor(double (*M)[MAXS + 1], int n, int *piv) {
+    for (int c = 0; c < n; ++c) {
+        int p = c;
+        for (int r = c + 1; r < n; ++r)
+            if (fabs(M[r][c]) > fabs(M[p][c])) p = r;
+        piv[c] = p;
+        if (M[p][c] == 0.0) return false;
+        if (p != c)
+            for (int q = 0; q < n; ++q) {
+                const double tmp = M[c][q];
+                M[c][q] = M[p][q];
+                M[p][q] = tmp;
+            }
+        for (int r = c + 1; r < n; ++r) {
+            const double f = M[r][c] / M[c][c];
+            M[r][c] = f;
+            for (int q = c + 1; q < n; ++q) M[r][q] -= f * M[c][q];
+        }
+    }
+    return true;
+}
+
+// The factorisation swaps whole rows (multipliers included), so all interchanges are
+// applied to b before the forward substitution.
+GAS_HD void lu_solve(const double (*M)[MAXS + 1], int n, const int *piv, double *b) {
+    for (int c = 0; c < n; ++c) {
+        const double tmp = b[c];
+        b[c] = b[piv[c]];
+        b[piv[c]] = tmp;
+    }
+    for (int r = 1; r < n; ++r)
+        for (int q = 0; q < r; ++q) b[r] -= M[r][q] * b[q];
+    for (int r = n - 1; r >= 0; --r) {
+        double v = b[r];
+        for (int q = r + 1; q < n; ++q) v -= M[r][q] * b[q];
+        b[r] = v / M[r][r];
+    }
+}
+
+// Advances (Y, T) over dt seconds at constant density rho.  Returns the number of
+// accepted sub-steps, or -1 if the sub-step cap was reached (state is left at the last
+// accepted point).
+GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                        double atol = 1e-10, double atol_T = 1e-3) {
+    const int ns = t.ns, n = ns + 1;
+    const double gam = 1.0 + 1.0 / sqrt(2.0);
+    double y[MAXS + 1], F0[MAXS + 1], Fp[MAXS + 1], yp[MAXS + 1], k1[MAXS + 1], k2[MAXS + 1];
+    double M[MAXS + 1][MAXS + 1];
+    int piv[MAXS + 1];
+    for (int k = 0; k < ns; ++k) y[k] = Y[k];
+    y[ns] = T;
+    double tt = 0.0, h = dt;
+    int acc = 0;
+    bool done = false;
+    for (int it = 0; it < kChemMaxSub && !done; ++it) {
+        const bool last = tt + h >= dt;
+        if (last) h = dt - tt;
+        reactor_rhs(t, rho, y, F0);
+        // finite-difference Jacobian, column by column
+        for (int c = 0; c < n; ++c) {
+            for (int q = 0; q < n; ++q) yp[q] = y[q];
+            const double eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
+            yp[c] += eps;
+            reactor_rhs(t, rho, yp, Fp);
+            for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
+        }
+        for (int r = 0; r < n; ++r) M[r][r] += 1.0;
+        if (!lu_factor(M, n, piv)) {
+            h *= 0.25;
+            continue;
+        }
+        for (int q = 0; q < n; ++q) k1[q] = F0[q];
+        lu_solve(M, n, piv, k1);
+        for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
+        reactor_rhs(t, rho, yp, Fp);
+        for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
+        lu_solve(M, n, piv, k2);
+        double err = 0.0;
+        for (int q = 0; q < n; ++q) {
+            const double ynew = y[q] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
+            const double sc = (q < ns ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
+            const double e = 0.5 * h * (k1[q] + k2[q]) / sc;
+            err = fmax(err, fabs(e));
+            yp[q] = ynew;
+        }
+        if (err <= 1.0) {
+            for (int q = 0; q < n; ++q) y[q] = yp[q];
+            tt = last ? dt : tt + h;  // the last step lands on dt exactly
+            done = last;
+            ++acc;
+        }
+        // second-order controller with safety factor, growth limited to 4x, shrink to 1/5
+        const double fac = err > 0.0 ? 0.9 / sqrt(err) : 4.0;
+        h *= fmin(4.0, fmax(0.2, fac));
+    }
+    for (int k = 0; k < ns; ++k) Y[k] = y[k];
+    T = y[ns];
+    return done ? acc : -1;
+}
+
+}  // namespace gas

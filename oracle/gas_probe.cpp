@@ -1,6 +1,7 @@
 // C entry points onto the gas-property library (lattice-boltzmann-method_b200/csrc/gas.cuh)
 // compiled for the host, for the property tests.  Test infrastructure only.
 #include "../lattice-boltzmann-method_b200/csrc/gas.cuh"
+#include "../lattice-boltzmann-method_b200/csrc/chem.cuh"
 
 static gas::Tables g_t;
 
@@ -30,4 +31,6 @@ double gp_s_R(int k, double T) { return gas::s_R(g_t, k, T); }
 double gp_cp_R(int k, double T) { return gas::cp_R(g_t, k, T); }
 int gp_T_from_u(const double *Y, double u, double T0, double *T) { return gas::T_from_u(g_t, Y, u, T0, 1e-14, 100, *T); }
 void gp_wdot(double T, const double *C, double *w) { gas::net_production(g_t, T, C, w); }
+void gp_reactor_rhs(double rho, const double *y, double *F) { gas::reactor_rhs(g_t, rho, y, F); }
+int gp_ros2(double rho, double *Y, double *T, double dt) { return gas::ros2_advance(g_t, rho, Y, *T, dt); }
 }
