@@ -55,9 +55,11 @@ def parse():
     ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
     ap.add_argument("--workload", choices=["tgv", "mix", "react"], default="tgv",
                     help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
-                         "mix: 9-species H2/air mixing layer, FP64, periodic (config 2 without its NSCBC "
+                         "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
                          "1800 K slab")
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+                    help="multicomponent population storage (fp32: shifted FP32 populations, FP64 records)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -266,7 +268,19 @@ def run_reference(args, dist):
     print(json.dumps(line), flush=True)
 
 
-MC_BYTES_STEP_FP64 = 2 * 27 * 10 * 8 + 16  # one read + one write of 270 populations + T (FP64)
+
+
+def mc_bytes(kernel, pop_bytes, reaction=False):
+    """Algorithmic bytes per fluid cell of one multicomponent launch (9 species): every
+    population (270 planes of `pop_bytes`) read once and, by the collide, written once;
+    the FP64 record planes each kernel must read or write once per cell.
+      collide: 58 record planes of the cell + 40 read once by its neighbours (rho, rho_a,
+               the 30 face-difference terms) [+ HRR written, with chemistry]
+      stream : 21 record planes read (rho, T, p, rho_a, X_a) + 88 written"""
+    if kernel == "k_mc_collide":
+        return 2 * 270 * pop_bytes + (58 + 40 + (1 if reaction else 0)) * 8
+    return 270 * pop_bytes + (21 + 88) * 8
+
 
 
 def mc_workload(args):
@@ -309,9 +323,12 @@ def run_ours_mc(args, dist):
     ncell = fluid_cells(mix)
     chem = lbmgpu.CHEM_REF_EXPLICIT if reaction else lbmgpu.CHEM_OFF
 
+    prec = lbmgpu.FP32 if args.precision == "fp32" else lbmgpu.FP64
+    pop_bytes = 4 if args.precision == "fp32" else 8
+
     def lattice():
         return lbmgpu.Lattice(*mix.shape, mech=m, dtype=workloads.MIXTURE_MC, species_dtype=workloads.SPECIES,
-                              dx_dt=workloads.FLAME_UNITS, chem=chem, device=device)
+                              dx_dt=workloads.FLAME_UNITS, chem=chem, device=device, precision=prec)
 
     lat = lattice()
     lat.upload(mix, sp)
@@ -332,8 +349,7 @@ def run_ours_mc(args, dist):
     lat.close()
     avg = {"k_mc_collide": kms[0] / max(launches[0], 1), "k_mc_stream": kms[1] / max(launches[1], 1)}
     dom = max(avg, key=avg.get)
-    per_cell = {"k_mc_collide": 2 * 27 * 10 * 8, "k_mc_stream": 27 * 10 * 8 + 16 * 8}[dom]
-    alg = per_cell * ncell
+    alg = mc_bytes(dom, pop_bytes, reaction) * ncell
     peak, peak_kind = peaks()
     achieved = alg / (avg[dom] * 1e-3) / 1e9
 
@@ -368,10 +384,12 @@ def run_ours_mc(args, dist):
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
-        "config": {"workload": f"{args.workload}{args.N}_mc9_fp64: 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
+        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}: 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
                                f"dx 20 um, dt 1 ns, " + ("reference explicit chemistry" if reaction else "non-reacting"),
-                   "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush"},
-        "hbm_gbs_step": ncell * MC_BYTES_STEP_FP64 / (ms / args.steps * 1e-3) / 1e9,
+                   "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
+                   "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
+        "hbm_gbs_step": ncell * (mc_bytes("k_mc_collide", pop_bytes, reaction) + mc_bytes("k_mc_stream", pop_bytes))
+        / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic(dom), "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": alg, "mean_launch_ms": avg[dom], "kernel_ms": avg},

@@ -43,8 +43,11 @@ extern "C" {
 #define LBMGPU_ST_NEWTON 0x8u       /* temperature Newton iteration hit its cap        */
 
 /* ---- precision of the population storage ------------------------------------- */
-#define LBMGPU_FP64 0
-#define LBMGPU_FP32 1
+#define LBMGPU_FP64 0   /* the reference's doubles; results bit-faithful                */
+#define LBMGPU_FP32 1   /* multicomponent only: populations stored in float as deviations
+                           from a per-plane shift (the plane's mean over the fluid cells,
+                           re-taken at upload and Init), the per-cell record in float; all
+                           arithmetic stays FP64.  Halves the state and its traffic.       */
 
 /* ---- gas mechanism ------------------------------------------------------------
  * Flat tables of one ideal-gas mechanism in SI units (kmol, m, s, J, K), the data the

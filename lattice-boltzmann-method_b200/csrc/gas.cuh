@@ -209,18 +209,34 @@ GAS_HD double binary_diff_x(const Tables &t, int k, int j, double x, double P) {
     return exp(fit_eval(t.fit_diff[k][j], x)) / P;
 }
 
-// Wilke's mixing rule with the species viscosities mu[] and mole fractions X[].
-GAS_HD double wilke(const Tables &t, const double *X, const double *mu) {
+// Wilke weights phi[a][b] = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^(1/4))^2 / sqrt(8 (1 + W_a/W_b)),
+// formed for b >= a and mirrored through phi[b][a] = mu_b/mu_a W_a/W_b phi[a][b] -- the
+// way the reference's species collision forms them (src/lbm-collision.cpp:408-417); the
+// mixture viscosity uses the same matrix.
+GAS_HD void wilke_phi(const Tables &t, const double *mu, double (*phi)[MAXS]) {
+    for (int a = 0; a < t.ns; ++a)
+        for (int b = a; b < t.ns; ++b) {
+            const double f1 = 1.0 + sqrt(mu[a] / mu[b]) * t.sqrt4W[a][b];
+            phi[a][b] = f1 * f1 / t.wilke_den[a][b];
+            phi[b][a] = mu[b] / mu[a] * t.m.W[a] / t.m.W[b] * phi[a][b];
+        }
+}
+
+// Wilke's mixing rule: mu = sum_k X_k mu_k / sum_j X_j phi_kj.
+GAS_HD double wilke_from_phi(const Tables &t, const double *X, const double *mu, const double (*phi)[MAXS]) {
     double s = 0.0;
     for (int k = 0; k < t.ns; ++k) {
         double d = 0.0;
-        for (int j = 0; j < t.ns; ++j) {
-            const double f = 1.0 + sqrt(mu[k] / mu[j]) * t.sqrt4W[k][j];
-            d += X[j] * f * f / t.wilke_den[k][j];
-        }
+        for (int j = 0; j < t.ns; ++j) d += X[j] * phi[k][j];
         s += X[k] * mu[k] / d;
     }
     return s;
+}
+
+GAS_HD double wilke(const Tables &t, const double *X, const double *mu) {
+    double phi[MAXS][MAXS];
+    wilke_phi(t, mu, phi);
+    return wilke_from_phi(t, X, mu, phi);
 }
 
 // Species thermal conductivity (Warnatz / CHEMKIN), W/(m K), from kinetic theory.

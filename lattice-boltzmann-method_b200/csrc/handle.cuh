@@ -70,6 +70,10 @@ struct lbmgpu {
     int chem = 0;
     lbm::UnitsF U{};
     gas::Tables *tab = nullptr;  // device copy
+    bool fp32 = false;           // FP32 population storage: pop32 instead of pop
+    float *pop32[2] = {nullptr, nullptr};
+    double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
+    long nfluid = 0;
 };
 
 namespace lbmh {

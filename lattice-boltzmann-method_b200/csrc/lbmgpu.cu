@@ -441,7 +441,8 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     *out = nullptr;
     if (desc->abi_version != LBMGPU_ABI_VERSION) return LBMGPU_E_VERSION;
     if (desc->Nx < 3 || desc->Ny < 3 || desc->Nz < 3) return LBMGPU_E_ARG;
-    if (desc->precision != LBMGPU_FP64) return LBMGPU_E_UNSUPPORTED;
+    if (desc->precision != LBMGPU_FP64 && desc->precision != LBMGPU_FP32) return LBMGPU_E_ARG;
+    if (desc->precision == LBMGPU_FP32 && desc->n_species == 0) return LBMGPU_E_UNSUPPORTED;  // FP32: multicomponent
     if (desc->dt_sim <= 0) return LBMGPU_E_ARG;
     if (desc->n_species == 0) {
         if (!(desc->gamma > 1.0) || !(desc->gas_const > 0.0) || !(desc->prtl > 0.0) || !(desc->nu >= 0.0))

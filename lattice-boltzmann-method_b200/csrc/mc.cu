@@ -8,6 +8,10 @@
 //   LBM::Init                              src/lbm-init.cpp:85-146 -> k_mc_init
 // This path covers periodic lattices (fluid cells and periodic ghosts); the other cell
 // types are rejected at upload with LBMGPU_E_UNSUPPORTED.
+//
+// Storage: FP64 (bit-faithful to the reference) or FP32 (LBMGPU_FP32: populations in
+// float as deviations from a per-plane shift; the per-cell record stays FP64, and all
+// arithmetic is FP64).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -18,31 +22,60 @@
 namespace {
 
 using namespace lbm;
-using lbmh::kBlock;
-using lbmh::MixOff;
-using lbmh::SpOff;
+using namespace lbmh;
 
 constexpr int NS9 = 9;
 
-template <int NS>
-__global__ void __launch_bounds__(kBlock) k_mc_collide(McArgs A) {
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_collide(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
     mc_collide_cell<NS>(A, n);
 }
 
-template <int NS>
-__global__ void __launch_bounds__(kBlock) k_mc_stream(McArgs A) {
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_stream(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
     mc_stream_moment_cell<NS>(A, n);
 }
 
-template <int NS>
-__global__ void __launch_bounds__(kBlock) k_mc_init(McArgs A, double *rec0, double *rec1, double *pop0) {
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_init(McArgsT<S, double> A, double *rec0, double *rec1, S *pop0) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell) return;
     mc_init_cell<NS>(A, n, rec0, rec1, pop0);
+}
+
+// FP32 storage: new per-plane shift = mean over the fluid cells of the decoded population
+// (one block per plane, fixed reduction order, so the result is deterministic) ...
+constexpr int kMeanBlock = 256;
+template <typename S>
+__global__ void __launch_bounds__(kMeanBlock) k_plane_mean(McArgsT<S, double> A, const S *pop, double *shift_new,
+                                                           long nfluid) {
+    __shared__ double red[kMeanBlock];
+    const int q = blockIdx.x;
+    double s = 0.0;
+    for (long n = threadIdx.x; n < A.ncell; n += kMeanBlock)
+        if (A.cflag[n] == CF_FLUID) s += ldpop(A, pop, q, n);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = kMeanBlock / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) shift_new[q] = nfluid > 0 ? red[0] / (double)nfluid : 0.0;
+}
+
+// ... and both population buffers re-encoded from the old shift to the new one.
+template <typename S>
+__global__ void k_reshift(long total, long ncell, S *p0, S *p1, const double *old_s, const double *new_s) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const int q = (int)(i / ncell);
+    const double d = old_s[q] - new_s[q];
+    p0[i] = (S)((double)p0[i] + d);
+    p1[i] = (S)((double)p1[i] + d);
 }
 
 __device__ __forceinline__ double ldd(const char *rec, long off) { return *reinterpret_cast<const double *>(rec + off); }
@@ -50,67 +83,65 @@ __device__ __forceinline__ void std_(char *rec, long off, double v) { *reinterpr
 
 // Staging layout of a chunk of cnt cells: cnt mixture records, then cnt records of each
 // species in turn.
-template <int NS>
-__global__ void k_mc_unpack(McArgs A, MixOff mo, SpOff so, const char *__restrict__ stage, long n0, long n1,
-                            double *rec0, double *rec1, double *pop0, double *pop1) {
+template <int NS, typename S>
+__global__ void k_mc_unpack(McArgsT<S, double> A, MixOff mo, SpOff so, const char *__restrict__ stage, long n0, long n1,
+                            double *rec0, double *rec1, S *pop0, S *pop1) {
     const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n1) return;
-    const long cnt = n1 - n0, nc = A.ncell;
+    const long cnt = n1 - n0;
     const char *mr = stage + (n - n0) * mo.size;
-    auto put = [&](int plane, double v) {
-        rec0[(long)plane * nc + n] = v;
-        rec1[(long)plane * nc + n] = v;
+    auto pr = [&](int plane, double v) {
+        put(A, rec0, plane, n, v);
+        put(A, rec1, plane, n, v);
     };
-    put(RM_RHO, ldd(mr, mo.rho));
-    put(RM_U, ldd(mr, mo.u));
-    put(RM_V, ldd(mr, mo.v));
-    put(RM_W, ldd(mr, mo.w));
-    put(RM_T, ldd(mr, mo.temp));
-    put(RM_P, ldd(mr, mo.p));
-    put(RM_RHOE, ldd(mr, mo.rhoe));
+    const double rho = ldd(mr, mo.rho), T = ldd(mr, mo.temp);
+    const double um[3] = {ldd(mr, mo.u), ldd(mr, mo.v), ldd(mr, mo.w)};
+    pr(RM_RHO, rho);
+    pr(RM_U, um[0]);
+    pr(RM_V, um[1]);
+    pr(RM_W, um[2]);
+    pr(RM_T, T);
+    pr(RM_P, ldd(mr, mo.p));
+    pr(RM_RHOE, ldd(mr, mo.rhoe));
     const int pi[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-    for (int q = 0; q < 6; ++q) put(RM_P00 + q, ldd(mr, mo.p_tensor + 8 * (3 * pi[q][0] + pi[q][1])));
-    put(RM_HRR, ldd(mr, mo.HRR));
+    for (int q = 0; q < 6; ++q) pr(RM_P00 + q, ldd(mr, mo.p_tensor + 8 * (3 * pi[q][0] + pi[q][1])));
+    pr(RM_HRR, ldd(mr, mo.HRR));
     const bool fluid = A.cflag[n] == CF_FLUID;
+    double rho_a[NS], ua[NS][3];
     for (int a = 0; a < NS; ++a) {
         const char *sr = stage + cnt * mo.size + ((long)a * cnt + (n - n0)) * so.size;
-        put(rs(a, RS_RHO), ldd(sr, so.rho));
-        put(rs(a, RS_UX), ldd(sr, so.u));
-        put(rs(a, RS_UX + 1), ldd(sr, so.v));
-        put(rs(a, RS_UX + 2), ldd(sr, so.w));
-        put(rs(a, RS_X), ldd(sr, so.X));
-        double jx = 0, jy = 0, jz = 0;
-        for (int l = 0; l < 27; ++l) {
-            const double fv = ldd(sr, so.f + 8 * l);
-            if (fluid) {
-                pop0[(long)(27 * a + l) * nc + n] = fv;
-                pop1[(long)(27 * a + l) * nc + n] = ldd(sr, so.fpc + 8 * l);
+        rho_a[a] = ldd(sr, so.rho);
+        ua[a][0] = ldd(sr, so.u);
+        ua[a][1] = ldd(sr, so.v);
+        ua[a][2] = ldd(sr, so.w);
+        pr(rs(a, RS_RHO), rho_a[a]);
+        for (int d = 0; d < 3; ++d) pr(rs(a, RS_UX + d), ua[a][d]);
+        pr(rs(a, RS_X), ldd(sr, so.X));
+        if (fluid)
+            for (int l = 0; l < 27; ++l) {
+                stpop(A, pop0, 27 * a + l, n, ldd(sr, so.f + 8 * l));
+                stpop(A, pop1, 27 * a + l, n, ldd(sr, so.fpc + 8 * l));
             }
-            jx += fv * cx(l);
-            jy += fv * cy(l);
-            jz += fv * cz(l);
-        }
-        put(rs(a, RS_JX), jx);
-        put(rs(a, RS_JX + 1), jy);
-        put(rs(a, RS_JX + 2), jz);
     }
+    store_face_terms<NS>(A, rec0, n, A.type[n], rho, um, T, rho_a, ua);
+    store_face_terms<NS>(A, rec1, n, A.type[n], rho, um, T, rho_a, ua);
     if (fluid)
         for (int l = 0; l < 27; ++l) {
-            pop0[(long)(27 * NS + l) * nc + n] = ldd(mr, mo.g + 8 * l);
-            pop1[(long)(27 * NS + l) * nc + n] = ldd(mr, mo.gpc + 8 * l);
+            stpop(A, pop0, 27 * NS + l, n, ldd(mr, mo.g + 8 * l));
+            stpop(A, pop1, 27 * NS + l, n, ldd(mr, mo.gpc + 8 * l));
         }
 }
 
 // pop_now: what the cell's populations are taken from (pulled when `stepped`, in place
 // otherwise); pop_pc: the post-collision populations (fpc, gpc).
-template <int NS>
-__global__ void k_mc_pack(McArgs A, MixOff mo, SpOff so, char *__restrict__ stage, long n0, long n1,
-                          const double *rec, const double *pop_now, const double *pop_pc, int stepped) {
+template <int NS, typename S>
+__global__ void k_mc_pack(McArgsT<S, double> A, MixOff mo, SpOff so, char *__restrict__ stage, long n0, long n1,
+                          const double *rec, const S *pop_now, const S *pop_pc, int stepped) {
     const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n1) return;
-    const long cnt = n1 - n0, nc = A.ncell;
+    const long cnt = n1 - n0;
     char *mr = stage + (n - n0) * mo.size;
-    auto get = [&](int plane) { return rec[(long)plane * nc + n]; };
+    auto get = [&](int plane) { return (double)rec[(long)plane * A.ncell + n]; };
     std_(mr, mo.rho, get(RM_RHO));
     std_(mr, mo.u, get(RM_U));
     std_(mr, mo.v, get(RM_V));
@@ -122,8 +153,8 @@ __global__ void k_mc_pack(McArgs A, MixOff mo, SpOff so, char *__restrict__ stag
     const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     for (int q = 0; q < 9; ++q) std_(mr, mo.p_tensor + 8 * q, get(RM_P00 + full[q]));
     const bool fluid = A.cflag[n] == CF_FLUID;
-    int i, j, k;
-    decode(A, n, i, j, k);
+    McPull pp;
+    mc_pull(A, n, pp);
     for (int a = 0; a < NS; ++a) {
         char *sr = stage + cnt * mo.size + ((long)a * cnt + (n - n0)) * so.size;
         std_(sr, so.rho, get(rs(a, RS_RHO)));
@@ -133,18 +164,18 @@ __global__ void k_mc_pack(McArgs A, MixOff mo, SpOff so, char *__restrict__ stag
         std_(sr, so.X, get(rs(a, RS_X)));
         if (!fluid) continue;
         for (int l = 0; l < 27; ++l) {
-            const long plane = (long)(27 * a + l) * nc;
-            std_(sr, so.f + 8 * l, stepped ? pop_now[plane + mc_pull_src(A, i, j, k, l)] : pop_now[plane + n]);
-            std_(sr, so.fpc + 8 * l, pop_pc[plane + n]);
+            const int plane = 27 * a + l;
+            std_(sr, so.f + 8 * l, ldpop(A, pop_now, plane, stepped ? pull_idx(pp, l) : n));
+            std_(sr, so.fpc + 8 * l, ldpop(A, pop_pc, plane, n));
         }
     }
     if (!fluid) return;
     double q3[3] = {0, 0, 0};
     for (int l = 0; l < 27; ++l) {
-        const long plane = (long)(27 * NS + l) * nc;
-        const double gv = stepped ? pop_now[plane + mc_pull_src(A, i, j, k, l)] : pop_now[plane + n];
+        const int plane = 27 * NS + l;
+        const double gv = ldpop(A, pop_now, plane, stepped ? pull_idx(pp, l) : n);
         std_(mr, mo.g + 8 * l, gv);
-        std_(mr, mo.gpc + 8 * l, pop_pc[plane + n]);
+        std_(mr, mo.gpc + 8 * l, ldpop(A, pop_pc, plane, n));
         q3[0] += gv * cx(l);
         q3[1] += gv * cy(l);
         q3[2] += gv * cz(l);
@@ -152,8 +183,9 @@ __global__ void k_mc_pack(McArgs A, MixOff mo, SpOff so, char *__restrict__ stag
     for (int q = 0; q < 3; ++q) std_(mr, mo.energy_flux + 8 * q, q3[q]);
 }
 
-McArgs base_args(lbmgpu *h) {
-    McArgs A{};
+template <typename S>
+McArgsT<S, double> base_args(lbmgpu *h) {
+    McArgsT<S, double> A{};
     A.Nx = h->g.Nx;
     A.Ny = h->g.Ny;
     A.Nz = h->g.Nz;
@@ -168,8 +200,14 @@ McArgs base_args(lbmgpu *h) {
     A.type = h->type;
     A.cflag = h->cflag;
     A.status = h->status;
+    A.shift = h->fp32 ? h->shift[0] : nullptr;
     return A;
 }
+
+// The two storage types' buffers behind one accessor.
+template <typename S> S *popb(lbmgpu *h, int b);
+template <> double *popb<double>(lbmgpu *h, int b) { return h->pop[b]; }
+template <> float *popb<float>(lbmgpu *h, int b) { return h->pop32[b]; }
 
 bool valid_mc_layout(const lbmgpu_mixture_layout &m, const lbmgpu_species_layout &s) {
     if (m.size == 0 || m.size % 8 || s.size == 0 || s.size % 8) return false;
@@ -185,6 +223,104 @@ bool valid_mc_layout(const lbmgpu_mixture_layout &m, const lbmgpu_species_layout
     return true;
 }
 
+// FP32 storage: move both population buffers onto the mean of the current state.
+int rebase_shift(lbmgpu *h) {
+    if (!h->fp32) return 0;
+    McArgsT<float, double> A = base_args<float>(h);
+    const int np = 27 * (h->ns + 1);
+    k_plane_mean<float><<<np, kMeanBlock, 0, h->stream>>>(A, h->pop32[h->cur], h->shift[1], h->nfluid);
+    CK(cudaGetLastError());
+    const long total = (long)np * h->g.ncell;
+    k_reshift<float><<<grid_for(total), kBlock, 0, h->stream>>>(total, h->g.ncell, h->pop32[0], h->pop32[1],
+                                                                h->shift[0], h->shift[1]);
+    CK(cudaGetLastError());
+    std::swap(h->shift[0], h->shift[1]);
+    return 0;
+}
+
+template <typename S>
+int upload_t(lbmgpu *h, const char *hm, const void *const *species) {
+    const long nc = h->g.ncell;
+    const size_t ms = h->mo.size, ss = h->so.size;
+    McArgsT<S, double> A = base_args<S>(h);
+    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
+        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells), cnt = n1 - n0;
+        CK(cudaMemcpyAsync(h->stage, hm + n0 * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
+        for (int a = 0; a < h->ns; ++a)
+            CK(cudaMemcpyAsync(h->stage + cnt * ms + (size_t)a * cnt * ss,
+                               static_cast<const char *>(species[a]) + n0 * ss, cnt * ss, cudaMemcpyHostToDevice,
+                               h->stream));
+        EvPair ep{};
+        ev_begin(h, K_OTHER, ep);
+        k_mc_unpack<NS9, S><<<grid_for(cnt), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[0],
+                                                                     h->mom[1], popb<S>(h, 0), popb<S>(h, 1));
+        ev_end(h, ep);
+        CK(cudaGetLastError());
+    }
+    return 0;
+}
+
+template <typename S>
+int pack_chunk(lbmgpu *h, long n0, long n1, bool stepped) {
+    McArgsT<S, double> A = base_args<S>(h);
+    const int c = h->cur;
+    const S *pc = stepped ? popb<S>(h, c) : popb<S>(h, 1 - c);
+    EvPair ep{};
+    ev_begin(h, K_OTHER, ep);
+    k_mc_pack<NS9, S><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[c],
+                                                                   popb<S>(h, c), pc, stepped ? 1 : 0);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+template <typename S>
+int init_t(lbmgpu *h) {
+    McArgsT<S, double> A = base_args<S>(h);
+    const int c = h->cur;
+    EvPair ep{};
+    ev_begin(h, K_OTHER, ep);
+    k_mc_init<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A, h->mom[c], h->mom[1 - c],
+                                                                      popb<S>(h, c));
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+template <typename S>
+int collide_t(lbmgpu *h) {
+    const int c = h->cur, x = 1 - c;
+    McArgsT<S, double> A = base_args<S>(h);
+    const bool local = h->pack_mode != PK_STEPPED;
+    A.pop_src = popb<S>(h, c);
+    A.pop_dst = popb<S>(h, x);
+    A.pop_prev = local ? nullptr : popb<S>(h, c);
+    A.rec_cur = h->mom[c];
+    A.rec_nxt = h->mom[x];
+    A.local = local ? 1 : 0;
+    EvPair ep{};
+    ev_begin(h, K_COLLIDE, ep);
+    k_mc_collide<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+template <typename S>
+int stream_t(lbmgpu *h) {
+    const int c = h->cur, x = 1 - c;
+    McArgsT<S, double> A = base_args<S>(h);
+    A.pop_src = popb<S>(h, x);
+    A.rec_cur = h->mom[c];
+    A.rec_nxt = h->mom[x];
+    EvPair ep{};
+    ev_begin(h, K_STREAM_MOMENT, ep);
+    k_mc_stream<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
 }  // namespace
 
 namespace lbmh {
@@ -195,16 +331,28 @@ int mc_setup(lbmgpu *h) {
     h->ns = d.n_species;
     h->nrec = mc_nrec(h->ns);
     h->chem = d.chem_mode;
+    h->fp32 = d.precision == LBMGPU_FP32;
     h->U = UnitsF{d.units_m, d.units_kg, d.units_s, d.units_K};
     const lbmgpu_species_layout &s = d.spc;
     h->so = SpOff{(long)s.size, s.X, s.rho, s.f, s.fpc, s.u, s.v, s.w};
     const long nc = h->g.ncell;
     const size_t np = 27 * (size_t)(h->ns + 1);
     for (int b = 0; b < 2; ++b) {
-        int rc = dalloc(h, &h->pop[b], np * nc);
+        int rc = h->fp32 ? dalloc(h, &h->pop32[b], np * nc) : dalloc(h, &h->pop[b], np * nc);
         if (rc) return rc;
         rc = dalloc(h, &h->mom[b], (size_t)h->nrec * nc);
         if (rc) return rc;
+        // the face-difference planes of cells the kernels never write (ghosts) are read
+        // but not used, and the ghosts' populations are never read; zero them all so they
+        // hold no stale bits
+        CK(cudaMemset(h->mom[b], 0, (size_t)h->nrec * nc * sizeof(double)));
+        CK(cudaMemset(h->fp32 ? (void *)h->pop32[b] : (void *)h->pop[b], 0,
+                      np * nc * (h->fp32 ? sizeof(float) : sizeof(double))));
+        if (h->fp32) {
+            rc = dalloc(h, &h->shift[b], np);
+            if (rc) return rc;
+            CK(cudaMemset(h->shift[b], 0, np * sizeof(double)));
+        }
     }
     gas::Tables *ht = new gas::Tables();
     gas::make_tables(*d.mech, *ht);
@@ -221,6 +369,12 @@ int mc_setup(lbmgpu *h) {
 void mc_release(lbmgpu *h) {
     if (h->tab) cudaFree(h->tab);
     h->tab = nullptr;
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(h->pop32[b]);
+        cudaFree(h->shift[b]);
+        h->pop32[b] = nullptr;
+        h->shift[b] = nullptr;
+    }
 }
 
 int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
@@ -230,7 +384,7 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
     CK(cudaSetDevice(h->d.device));
     const lbm::ScGeom &g = h->g;
     const long nc = g.ncell;
-    const size_t ms = h->mo.size, ss = h->so.size;
+    const size_t ms = h->mo.size;
     const char *hm = static_cast<const char *>(mix);
     std::vector<int8_t> ty(nc);
     std::vector<uint8_t> cf(nc, 0);
@@ -241,6 +395,7 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
         if (t != T_F && t != T_P) return LBMGPU_E_UNSUPPORTED;  // periodic lattices only
         ty[n] = (int8_t)t;
     }
+    long nfluid = 0;
     for (int i = 0; i < g.Nx; ++i)
         for (int j = 0; j < g.Ny; ++j)
             for (int k = 0; k < g.Nz; ++k) {
@@ -249,26 +404,17 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
                 if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
                     return LBMGPU_E_ARG;
                 cf[n] = CF_FLUID;
+                ++nfluid;
             }
+    h->nfluid = nfluid;
     CK(cudaMemcpyAsync(h->type, ty.data(), nc, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cflag, cf.data(), nc, cudaMemcpyHostToDevice, h->stream));
-    McArgs A = base_args(h);
-    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
-        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells), cnt = n1 - n0;
-        CK(cudaMemcpyAsync(h->stage, hm + n0 * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
-        for (int a = 0; a < h->ns; ++a)
-            CK(cudaMemcpyAsync(h->stage + cnt * ms + (size_t)a * cnt * ss,
-                               static_cast<const char *>(species[a]) + n0 * ss, cnt * ss, cudaMemcpyHostToDevice,
-                               h->stream));
-        EvPair ep{};
-        ev_begin(h, K_OTHER, ep);
-        k_mc_unpack<NS9><<<grid_for(cnt), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[0],
-                                                                  h->mom[1], h->pop[0], h->pop[1]);
-        ev_end(h, ep);
-        CK(cudaGetLastError());
-    }
-    CK(cudaStreamSynchronize(h->stream));
+    int rc = h->fp32 ? upload_t<float>(h, hm, species) : upload_t<double>(h, hm, species);
+    if (rc) return rc;
     h->cur = 0;
+    rc = rebase_shift(h);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
     h->pack_mode = PK_UPLOADED;
     h->have_state = true;
     h->phase = PH_BOUNDARY;
@@ -285,21 +431,14 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
     std::vector<uint8_t> cf(nc);
     CK(cudaMemcpyAsync(cf.data(), h->cflag, nc, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    McArgs A = base_args(h);
-    const int c = h->cur;
     const bool stepped = h->pack_mode == PK_STEPPED;
-    const double *pc = stepped ? h->pop[c] : h->pop[1 - c];
     const long mfld[] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.p, h->mo.temp, h->mo.rhoe, h->mo.HRR};
     const long sfld[] = {h->so.X, h->so.rho, h->so.u, h->so.v, h->so.w};
     char *hm = static_cast<char *>(mix);
     for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
         const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells), cnt = n1 - n0;
-        EvPair ep{};
-        ev_begin(h, K_OTHER, ep);
-        k_mc_pack<NS9><<<grid_for(cnt), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[c],
-                                                                h->pop[c], pc, stepped ? 1 : 0);
-        ev_end(h, ep);
-        CK(cudaGetLastError());
+        const int rc = h->fp32 ? pack_chunk<float>(h, n0, n1, stepped) : pack_chunk<double>(h, n0, n1, stepped);
+        if (rc) return rc;
         const size_t bytes = cnt * (ms + (size_t)h->ns * ss);
         CK(cudaMemcpyAsync(h->bounce, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
@@ -311,7 +450,6 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
                 std::memcpy(&t, drec + h->mo.type, sizeof(short));
                 std::memcpy(drec, srec, ms);
                 std::memcpy(drec + h->mo.type, &t, sizeof(short));
-                for (int q = 0; q < 9; ++q) (void)q;
             } else {
                 for (long o : mfld) std::memcpy(drec + o, srec + o, sizeof(double));
                 std::memcpy(drec + h->mo.p_tensor, srec + h->mo.p_tensor, 9 * sizeof(double));
@@ -330,47 +468,20 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
 }
 
 int mc_init(lbmgpu *h) {
-    McArgs A = base_args(h);
-    const int c = h->cur;
-    EvPair ep{};
-    ev_begin(h, K_OTHER, ep);
-    k_mc_init<NS9><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A, h->mom[c], h->mom[1 - c], h->pop[c]);
-    ev_end(h, ep);
-    CK(cudaGetLastError());
+    int rc = h->fp32 ? init_t<float>(h) : init_t<double>(h);
+    if (rc) return rc;
+    rc = rebase_shift(h);
+    if (rc) return rc;
     h->pack_mode = PK_INIT;
     return LBMGPU_OK;
 }
 
-int mc_launch_collide(lbmgpu *h) {
-    const int c = h->cur, x = 1 - c;
-    McArgs A = base_args(h);
-    const bool local = h->pack_mode != PK_STEPPED;
-    A.pop_src = h->pop[c];
-    A.pop_dst = h->pop[x];
-    A.pop_prev = local ? nullptr : h->pop[c];
-    A.rec_cur = h->mom[c];
-    A.rec_nxt = h->mom[x];
-    A.local = local ? 1 : 0;
-    EvPair ep{};
-    ev_begin(h, K_COLLIDE, ep);
-    k_mc_collide<NS9><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
-    ev_end(h, ep);
-    CK(cudaGetLastError());
-    return 0;
-}
+int mc_launch_collide(lbmgpu *h) { return h->fp32 ? collide_t<float>(h) : collide_t<double>(h); }
 
 int mc_launch_stream(lbmgpu *h) {
-    const int c = h->cur, x = 1 - c;
-    McArgs A = base_args(h);
-    A.pop_src = h->pop[x];
-    A.rec_cur = h->mom[c];
-    A.rec_nxt = h->mom[x];
-    EvPair ep{};
-    ev_begin(h, K_STREAM_MOMENT, ep);
-    k_mc_stream<NS9><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
-    ev_end(h, ep);
-    CK(cudaGetLastError());
-    h->cur = x;
+    const int rc = h->fp32 ? stream_t<float>(h) : stream_t<double>(h);
+    if (rc) return rc;
+    h->cur = 1 - h->cur;
     h->pack_mode = PK_STEPPED;
     return 0;
 }

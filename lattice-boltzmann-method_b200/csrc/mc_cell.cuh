@@ -1,19 +1,24 @@
 // Multicomponent thermal D3Q27 step, per-cell logic (the reference with MULTICOMP on).
-// Every function here is host/device: the kernels in lbmgpu.cu call them once per cell,
-// and the tests build them for the host to compare with the reference's own solver.
+// Every function here is host/device: the kernels in mc.cu call them once per cell, and
+// the tests build them for the host to compare with the reference's own solver.
 //
-// Device state (structure of arrays, cell index n = (i*Ny + j)*Nz + k):
+// Device state (structure of arrays, cell index n = (i*Ny + j)*Nz + k); populations stored
+// as AT::P (double: the bit-faithful FP64 mode; float: the FP32 mode), records as AT::R:
 //   pop[2]: 27*(NS+1) planes -- species a, direction l at plane 27a + l; the energy
 //           population g at plane 27 NS + l.  Post-collision values of the last step, or
 //           (after an upload or Init, "local" mode) the populations themselves; the other
 //           buffer then keeps the uploaded fpc, which the reference's skip rule for
-//           vanishing species (src/lbm-collision.cpp:512-513) leaves in place.
-//   rec[2]: MC_NREC(NS) planes per cell -- the state calculate_moment leaves
+//           vanishing species (src/lbm-collision.cpp:512-513) leaves in place.  With a
+//           shift table a population is stored as its deviation from the plane's shift
+//           (the mean of that population over the fluid cells at upload or Init) and
+//           decoded to FP64 for all arithmetic.
+//   rec[2]: mc_nrec(NS) planes per cell -- the state calculate_moment leaves
 //           (src/lbm-moment.cpp:193-377): rho, u, v, w, T, p, rhoE, the pressure tensor
-//           (6), HRR, then per species rho_a, j_a (3: sum f_a c, the moment the species
-//           collision divides by rho_a, src/lbm-collision.cpp:446-454), u_a (3: the
-//           Stefan-Maxwell velocities) and X_a.  Double-buffered like the
-//           single-component record.
+//           (6), HRR; the mixture face-difference term Q_a (src/lbm-collision.cpp:296-300,
+//           with the composition gas constant a neighbour's value carries); then per
+//           species rho_a, u_a (3: the Stefan-Maxwell velocities), X_a and the species
+//           face-difference term Q_{a,x|y|z} (src/lbm-collision.cpp:487-489).  The
+//           neighbours of a cell read only the Q terms of their axis, rho_a and rho.
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -35,16 +40,19 @@ namespace lbm {
 constexpr double kSpeciesMin = 1e-8;   // SPECIES_MIN, src/headers/defines.hpp:96
 
 enum : int {
-    RM_RHO = 0, RM_U = 1, RM_V = 2, RM_W = 3, RM_T = 4, RM_P = 5, RM_RHOE = 6, RM_P00 = 7, // P00 P01 P02 P11 P12 P22
-    RM_HRR = 13, RM_SP = 14, RM_SPN = 8                                                    // per species block
+    RM_RHO = 0, RM_U = 1, RM_V = 2, RM_W = 3, RM_T = 4, RM_P = 5, RM_RHOE = 6, RM_P00 = 7,  // P00 P01 P02 P11 P12 P22
+    RM_HRR = 13, RM_QX = 14, RM_SP = 17, RM_SPN = 8                                          // per species block
 };
-enum : int { RS_RHO = 0, RS_JX = 1, RS_UX = 4, RS_X = 7 };
+enum : int { RS_RHO = 0, RS_UX = 1, RS_X = 4, RS_QX = 5 };
 MC_HD int mc_nrec(int ns) { return RM_SP + RM_SPN * ns; }
 MC_HD int rs(int a, int f) { return RM_SP + RM_SPN * a + f; }
 
 enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1 };
 
-struct McArgs {
+template <typename P_, typename R_>
+struct McArgsT {
+    using P = P_;          // population storage type
+    using R = R_;          // record storage type
     int Nx, Ny, Nz;
     long ncell, sj, si;
     int ns, dt, chem;
@@ -52,20 +60,33 @@ struct McArgs {
     const gas::Tables *tab;
     const int8_t *type;
     const uint8_t *cflag;
-    const double *pop_src;   // collide: pop[cur]; stream: the collide's output
-    double *pop_dst;         // collide: pop[nxt]
-    const double *pop_prev;  // collide: fpc of the previous step (skip rule); null in local mode
-    const double *rec_cur;
-    double *rec_nxt;
+    const P *pop_src;      // collide: pop[cur]; stream: the collide's output
+    P *pop_dst;            // collide: pop[nxt]
+    const P *pop_prev;     // collide: fpc of the previous step (skip rule); null in local mode
+    const R *rec_cur;
+    R *rec_nxt;
+    const double *shift;   // per population plane, or null (no shift)
     unsigned *status;
     int local;
 };
+using McArgs = McArgsT<double, double>;
 
-MC_HD double rec(const McArgs &A, const double *r, int plane, long n) { return r[(long)plane * A.ncell + n]; }
-
-// Per-species constants of the lattice collision that depend on the units (host, setup).
-inline void set_lattice_constants(gas::Tables &t, const UnitsF &U) {
-    for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = u_cp(U, (float)(gas::kR / t.m.W[a]));
+template <class AT, typename T>
+MC_HD double rec(const AT &A, const T *r, int plane, long n) {
+    return (double)r[(long)plane * A.ncell + n];
+}
+template <class AT, typename T>
+MC_HD void put(const AT &A, T *r, int plane, long n, double v) {
+    r[(long)plane * A.ncell + n] = (T)v;
+}
+template <class AT, typename T>
+MC_HD double ldpop(const AT &A, const T *p, int plane, long idx) {
+    const double v = (double)p[(long)plane * A.ncell + idx];
+    return A.shift ? v + A.shift[plane] : v;
+}
+template <class AT, typename T>
+MC_HD void stpop(const AT &A, T *p, int plane, long idx, double v) {
+    p[(long)plane * A.ncell + idx] = (T)(A.shift ? v - A.shift[plane] : v);
 }
 
 MC_HD void atomic_status(unsigned *s, unsigned bits) {
@@ -74,6 +95,11 @@ MC_HD void atomic_status(unsigned *s, unsigned bits) {
 #else
     *s |= bits;
 #endif
+}
+
+// Per-species constants of the lattice collision that depend on the units (host, setup).
+inline void set_lattice_constants(gas::Tables &t, const UnitsF &U) {
+    for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = u_cp(U, (float)(gas::kR / t.m.W[a]));
 }
 
 MC_HD bool fluid_like(int t) { return t == T_F || t == T_I || t == T_O || t == T_I_C || t == T_O_C; }
@@ -94,21 +120,28 @@ MC_HD double mc_fd_fuw(double sl, double sc, double sr, double vel, int tl, int 
     return fuw_blocked(tr) ? 0.0 : (sr - sc);
 }
 
-MC_HD void decode(const McArgs &A, long n, int &i, int &j, int &k) {
-    i = (int)(n / A.si);
-    j = (int)((n / A.sj) % A.Ny);
-    k = (int)(n % A.Nz);
+// Periodic pull sources of a cell with no boundary neighbour (src/lbm-streaming.cpp:88-117):
+// per axis the upstream coordinate for c = 0, +1, -1 with the reference's wrap.
+struct McPull {
+    long X[3], Y[3], Z[3];
+};
+template <class AT>
+MC_HD void mc_pull(const AT &A, long n, McPull &p) {
+    const int i = (int)(n / A.si), j = (int)((n / A.sj) % A.Ny), k = (int)(n % A.Nz);
+    const int im = (i - 1 == 0) ? A.Nx - 2 : i - 1, ip = (i + 1 == A.Nx - 1) ? 1 : i + 1;
+    const int jm = (j - 1 == 0) ? A.Ny - 2 : j - 1, jp = (j + 1 == A.Ny - 1) ? 1 : j + 1;
+    const int km = (k - 1 == 0) ? A.Nz - 2 : k - 1, kp = (k + 1 == A.Nz - 1) ? 1 : k + 1;
+    p.X[0] = (long)i * A.si;
+    p.X[1] = (long)im * A.si;
+    p.X[2] = (long)ip * A.si;
+    p.Y[0] = (long)j * A.sj;
+    p.Y[1] = (long)jm * A.sj;
+    p.Y[2] = (long)jp * A.sj;
+    p.Z[0] = k;
+    p.Z[1] = km;
+    p.Z[2] = kp;
 }
-
-// Periodic pull source of direction l for a cell with no boundary neighbour
-// (src/lbm-streaming.cpp:88-117).
-MC_HD long mc_pull_src(const McArgs &A, int i, int j, int k, int l) {
-    int in = i - cx(l), jn = j - cy(l), kn = k - cz(l);
-    if (in == 0) in = A.Nx - 2; else if (in == A.Nx - 1) in = 1;
-    if (jn == 0) jn = A.Ny - 2; else if (jn == A.Ny - 1) jn = 1;
-    if (kn == 0) kn = A.Nz - 2; else if (kn == A.Nz - 1) kn = 1;
-    return (long)in * A.si + (long)jn * A.sj + kn;
-}
+MC_HD long pull_idx(const McPull &p, int l) { return p.X[cidx(cx(l))] + p.Y[cidx(cy(l))] + p.Z[cidx(cz(l))]; }
 
 // Cantera's setMassFractions: clip negatives, normalise.  Returns the mean molar mass.
 template <int NS>
@@ -126,17 +159,42 @@ MC_HD double set_mass_fractions(const gas::Tables &t, const double *y, double *Y
     return W;
 }
 
+// The face-difference terms a cell offers its neighbours: species Q_{a,d} with the species
+// gas constant (src/lbm-collision.cpp:487-489) and the mixture Q_d with the composition
+// gas constant a neighbour uses (src/lbm-collision.cpp:207-215, 296-300; zero gas constant
+// for cells that are not fluid-like).
+template <int NS, class AT>
+MC_HD void store_face_terms(const AT &A, typename AT::R *R, long n, int ty, double rho, const double u[3], double T,
+                            const double *rho_a, const double (*ua)[3]) {
+    const gas::Tables &t = *A.tab;
+    double gc = 0.0;
+    if (fluid_like(ty)) {
+        double sYW = 0.0, sY = 0.0;
+        for (int a = 0; a < NS; ++a) {
+            const double Ya = rho_a[a] / rho;
+            sYW += Ya / t.m.W[a];
+            sY += Ya;
+        }
+        gc = (double)u_cp(A.U, (float)(gas::kR * sYW / sY));
+    }
+    for (int d = 0; d < 3; ++d)
+        put(A, R, RM_QX + d, n, rho * u[d] * (1.0 - 3.0 * gc * T) - rho * (u[d] * u[d] * u[d]));
+    for (int a = 0; a < NS; ++a) {
+        const double Ra = t.Ra_lat[a];
+        for (int d = 0; d < 3; ++d)
+            put(A, R, rs(a, RS_QX + d), n,
+                rho_a[a] * ua[a][d] * (1.0 - 3.0 * Ra * T) - rho_a[a] * (ua[a][d] * ua[a][d] * ua[a][d]));
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // Streaming + moments (reference LBM::Streaming and the multicomponent
 // LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one fluid cell of a periodic
 // lattice.
 // ------------------------------------------------------------------------------------
-template <int NS>
-MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
+template <int NS, class AT>
+MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
     const gas::Tables &t = *A.tab;
-    const long nc = A.ncell;
-    int i, j, k;
-    decode(A, n, i, j, k);
     // -- old state, as the reference's Cantera object is set at the start (lbm-moment.cpp:219-221)
     double Yo_raw[NS], Yo[NS], Xo[NS];
     const double rho_old = rec(A, A.rec_cur, RM_RHO, n);
@@ -147,23 +205,27 @@ MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
     const double P_si = rho_si * gas::kR * T_si / Wold;
 
     // -- pulled populations: sums per species and of g
+    McPull pp;
+    mc_pull(A, n, pp);
     double rho_a[NS], j_a[NS][3];
     double P6[6] = {0, 0, 0, 0, 0, 0};
     for (int a = 0; a < NS; ++a) {
+        double fv[27];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) fv[l] = ldpop(A, A.pop_src, 27 * a + l, pull_idx(pp, l));
         double r = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
         for (int l = 0; l < 27; ++l) {
-            const double fv = A.pop_src[(long)(27 * a + l) * nc + mc_pull_src(A, i, j, k, l)];
-            r += fv;
-            jx += fv * cx(l);
-            jy += fv * cy(l);
-            jz += fv * cz(l);
-            if (cx(l)) P6[0] += fv;
-            if (cx(l) * cy(l)) P6[1] += cx(l) * cy(l) * fv;
-            if (cx(l) * cz(l)) P6[2] += cx(l) * cz(l) * fv;
-            if (cy(l)) P6[3] += fv;
-            if (cy(l) * cz(l)) P6[4] += cy(l) * cz(l) * fv;
-            if (cz(l)) P6[5] += fv;
+            r += fv[l];
+            jx += fv[l] * cx(l);
+            jy += fv[l] * cy(l);
+            jz += fv[l] * cz(l);
+            if (cx(l)) P6[0] += fv[l];
+            if (cx(l) * cy(l)) P6[1] += cx(l) * cy(l) * fv[l];
+            if (cx(l) * cz(l)) P6[2] += cx(l) * cz(l) * fv[l];
+            if (cy(l)) P6[3] += fv[l];
+            if (cy(l) * cz(l)) P6[4] += cy(l) * cz(l) * fv[l];
+            if (cz(l)) P6[5] += fv[l];
         }
         rho_a[a] = r;
         j_a[a][0] = jx;
@@ -172,7 +234,7 @@ MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
     }
     double rhoe = 0.0;
 #pragma unroll
-    for (int l = 0; l < 27; ++l) rhoe += A.pop_src[(long)(27 * NS + l) * nc + mc_pull_src(A, i, j, k, l)];
+    for (int l = 0; l < 27; ++l) rhoe += ldpop(A, A.pop_src, 27 * NS + l, pull_idx(pp, l));
 
     double rho = 0, ru = 0, rv = 0, rw = 0, rho_s[NS];
     for (int a = 0; a < NS; ++a) {
@@ -240,24 +302,24 @@ MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
     const int it = gas::T_from_u(t, Y, u_si, T_si, 1e-14, 100, Tn);
     if (it < 0) atomic_status(A.status, LBMGPU_ST_NEWTON);
     const double Pn = rho_n_si * gas::kR * Tn / Wn;
+    const double Tl = u_temp(A.U, (float)Tn);
 
-    double *R = A.rec_nxt;
-    R[(long)RM_RHO * nc + n] = rho;
-    R[(long)RM_U * nc + n] = u;
-    R[(long)RM_V * nc + n] = v;
-    R[(long)RM_W * nc + n] = w;
-    R[(long)RM_T * nc + n] = u_temp(A.U, (float)Tn);
-    R[(long)RM_P * nc + n] = u_p(A.U, (float)Pn);
-    R[(long)RM_RHOE * nc + n] = rhoe;
-    for (int q = 0; q < 6; ++q) R[(long)(RM_P00 + q) * nc + n] = P6[q];
+    typename AT::R *R = A.rec_nxt;
+    put(A, R, RM_RHO, n, rho);
+    put(A, R, RM_U, n, u);
+    put(A, R, RM_V, n, v);
+    put(A, R, RM_W, n, w);
+    put(A, R, RM_T, n, Tl);
+    put(A, R, RM_P, n, u_p(A.U, (float)Pn));
+    put(A, R, RM_RHOE, n, rhoe);
+    for (int q = 0; q < 6; ++q) put(A, R, RM_P00 + q, n, P6[q]);
     for (int a = 0; a < NS; ++a) {
-        R[(long)rs(a, RS_RHO) * nc + n] = rho_s[a];
-        for (int d = 0; d < 3; ++d) {
-            R[(long)rs(a, RS_JX + d) * nc + n] = j_a[a][d];
-            R[(long)rs(a, RS_UX + d) * nc + n] = usm[a][d];
-        }
-        R[(long)rs(a, RS_X) * nc + n] = X[a];
+        put(A, R, rs(a, RS_RHO), n, rho_s[a]);
+        for (int d = 0; d < 3; ++d) put(A, R, rs(a, RS_UX + d), n, usm[a][d]);
+        put(A, R, rs(a, RS_X), n, X[a]);
     }
+    const double um[3] = {u, v, w};
+    store_face_terms<NS>(A, R, n, T_F, rho, um, Tl, rho_s, usm);
     if (!isfinite(rho) || !isfinite(Tn) || !isfinite(u) || !isfinite(v) || !isfinite(w))
         atomic_status(A.status, LBMGPU_ST_NAN);
     else if (!(rho > 0.0) || !(Tn > 0.0))
@@ -268,13 +330,10 @@ MC_HDN void mc_stream_moment_cell(const McArgs &A, long n) {
 // Collision: species (LBM::Collide_Species, src/lbm-collision.cpp:334-526) and energy
 // (LBM::Collide, src/lbm-collision.cpp:191-332) of one fluid cell, fused.
 // ------------------------------------------------------------------------------------
-template <int NS>
-MC_HDN void mc_collide_cell(const McArgs &A, long n) {
+template <int NS, class AT>
+MC_HDN void mc_collide_cell(const AT &A, long n) {
     const gas::Tables &t = *A.tab;
-    const long nc = A.ncell;
-    const double *Rc = A.rec_cur;
-    int i, j, k;
-    decode(A, n, i, j, k);
+    const typename AT::R *Rc = A.rec_cur;
     const double rho = rec(A, Rc, RM_RHO, n);
     const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
     const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n), rhoe = rec(A, Rc, RM_RHOE, n);
@@ -322,22 +381,15 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
         double hrr = 0.0;
         for (int a = 0; a < NS; ++a)
             hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
-        A.rec_nxt[(long)RM_HRR * nc + n] = hrr;
+        put(A, A.rec_nxt, RM_HRR, n, hrr);
     }
 
     // -- species viscosities, Wilke weights, relaxation rates (lbm-collision.cpp:402-430)
     const double xT = gas::lnT_x(T_si);
     double mu_k[NS];
     for (int a = 0; a < NS; ++a) mu_k[a] = gas::species_visc_x(t, a, xT);
-    // Wilke weights phi[a][b] as the reference forms them: for b >= a directly, for b < a
-    // from phi[b][a] (lbm-collision.cpp:408-417)
-    double phi[NS][NS];
-    for (int a = 0; a < NS; ++a)
-        for (int b = a; b < NS; ++b) {
-            const double f1 = 1.0 + sqrt(mu_k[a] / mu_k[b]) * t.sqrt4W[a][b];
-            phi[a][b] = f1 * f1 / t.wilke_den[a][b];
-            phi[b][a] = mu_k[b] / mu_k[a] * t.m.W[a] / t.m.W[b] * phi[a][b];
-        }
+    double phi[gas::MAXS][gas::MAXS];
+    gas::wilke_phi(t, mu_k, phi);
     double om_a[NS];
     for (int a = 0; a < NS; ++a) {
         double denom = 0.0;
@@ -346,29 +398,22 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
         om_a[a] = 2 * Xs[a] * p * dt / (Xs[a] * p * dt + 2 * visc);
     }
 
-    // -- Maxwell-Stefan force (lbm-collision.cpp:433-471)
-    double Dl[NS][NS];  // lattice D_ab, one evaluation per pair (the diagonal term vanishes)
-    for (int a = 0; a < NS; ++a) {
-        Dl[a][a] = u_nu(A.U, (float)gas::binary_diff_x(t, a, a, xT, P_si));
+    // -- Maxwell-Stefan force (lbm-collision.cpp:433-471); the diagonal term vanishes
+    double F[NS][3];
+    for (int a = 0; a < NS; ++a)
+        for (int d = 0; d < 3; ++d) F[a][d] = 0.0;
+    for (int a = 0; a < NS; ++a)
         for (int b = 0; b < a; ++b) {
-            Dl[a][b] = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
-            Dl[b][a] = Dl[a][b];
+            const double D = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            for (int d = 0; d < 3; ++d) {
+                F[a][d] += -1.0 * p * Xs[a] * Xs[b] / D * (ua[a][d] - ua[b][d]);
+                F[b][d] += -1.0 * p * Xs[b] * Xs[a] / D * (ua[b][d] - ua[a][d]);
+            }
         }
-    }
-    double F[NS][3], ux[NS][3];
-    for (int a = 0; a < NS; ++a) {
-        for (int d = 0; d < 3; ++d) {
-            ux[a][d] = rec(A, Rc, rs(a, RS_JX + d), n) / rho_a[a];
-            F[a][d] = 0.0;
-        }
-        for (int b = 0; b < NS; ++b) {
-            const double D = Dl[a][b];
-            for (int d = 0; d < 3; ++d) F[a][d] += -1.0 * p * Xs[a] * Xs[b] / D * (ua[a][d] - ua[b][d]);
-        }
+    for (int a = 0; a < NS; ++a)
         for (int d = 0; d < 3; ++d) F[a][d] = F[a][d] * dt / rho_a[a];
-    }
 
-    // -- neighbour data for the FD terms
+    // -- neighbours along each axis
     long nbl[3], nbh[3];
     int tl[3], th[3];
     for (int d = 0; d < 3; ++d) {
@@ -378,119 +423,116 @@ MC_HDN void mc_collide_cell(const McArgs &A, long n) {
         tl[d] = A.type[nbl[d]];
         th[d] = A.type[nbh[d]];
     }
+    McPull pp;
+    if (!A.local) mc_pull(A, n, pp);
 
-    // -- species collision (lbm-collision.cpp:479-519)
+    // -- species collision (lbm-collision.cpp:446-519)
     for (int a = 0; a < NS; ++a) {
+        double fv[27];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) fv[l] = ldpop(A, A.pop_src, 27 * a + l, A.local ? n : pull_idx(pp, l));
+        // bare species velocity sum f c / rho_a (lbm-collision.cpp:446-454)
+        double ux[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int l = 0; l < 27; ++l) {
+            ux[0] += fv[l] * cx(l);
+            ux[1] += fv[l] * cy(l);
+            ux[2] += fv[l] * cz(l);
+        }
+        for (int d = 0; d < 3; ++d) ux[d] = ux[d] / rho_a[a];
         const double Ra = t.Ra_lat[a];
         const double theta = Ra * Tl;
         double corr[3];
         for (int d = 0; d < 3; ++d) {
-            const int pu = rs(a, RS_UX + d);
-            auto Qa = [&](long m) {
-                const double r = rec(A, Rc, rs(a, RS_RHO), m), uu = rec(A, Rc, pu, m);
-                return r * uu * (1.0 - 3.0 * Ra * rec(A, Rc, RM_T, m)) - r * (uu * uu * uu);
-            };
-            const double dQ = mc_fd_central(Qa(nbl[d]), Qa(n), Qa(nbh[d]), tl[d], th[d]);
+            const int pq = rs(a, RS_QX + d);
+            const double Qc = rho_a[a] * ua[a][d] * (1.0 - 3.0 * Ra * Tl) - rho_a[a] * (ua[a][d] * ua[a][d] * ua[a][d]);
+            const double dQ = mc_fd_central(rec(A, Rc, pq, nbl[d]), Qc, rec(A, Rc, pq, nbh[d]), tl[d], th[d]);
             corr[d] = dt * (2.0 - om_a[a]) / (2.0 * rho_a[a] * om_a[a]) * dQ;
         }
         AxisF<double> Fe, Fd, Fr;
-        axis_feq(Fe, ux[a], theta, corr);
-        const double udu[3] = {ux[a][0] + F[a][0], ux[a][1] + F[a][1], ux[a][2] + F[a][2]};
+        axis_feq(Fe, ux, theta, corr);
+        const double udu[3] = {ux[0] + F[a][0], ux[1] + F[a][1], ux[2] + F[a][2]};
         axis_feq(Fd, udu, theta, corr);
         const double zero[3] = {0.0, 0.0, 0.0};
         axis_feq(Fr, um, theta, zero);
         const double om = om_a[a];
+        const bool skip_all = rho_a[a] <= kSpeciesMin && A.chem != CHEM_REF_EXPLICIT;
+#pragma unroll
         for (int l = 0; l < 27; ++l) {
-            const long plane = (long)(27 * a + l) * nc;
-            const double fv = A.local ? A.pop_src[plane + n] : A.pop_src[plane + mc_pull_src(A, i, j, k, l)];
-            const double fe = feq_l(l, rho_a[a], Fe);
-            const double fd = feq_l(l, rho_a[a], Fd);
+            const int plane = 27 * a + l;
             const double fr = A.chem == CHEM_REF_EXPLICIT ? feq_l(l, drho[a], Fr) : 0.0;
-            if (rho_a[a] <= kSpeciesMin && fr <= 0.0) {
-                if (!A.local) A.pop_dst[plane + n] = A.pop_prev[plane + n];
+            if (skip_all || (rho_a[a] <= kSpeciesMin && fr <= 0.0)) {
+                if (!A.local) A.pop_dst[(long)plane * A.ncell + n] = A.pop_prev[(long)plane * A.ncell + n];
                 continue;
             }
-            A.pop_dst[plane + n] = fv + om * (fe - fv) + (fd - fe) + fr;
+            const double fe = feq_l(l, rho_a[a], Fe);
+            const double fd = feq_l(l, rho_a[a], Fd);
+            stpop(A, A.pop_dst, plane, n, fv[l] + om * (fe - fv[l]) + (fd - fe) + fr);
         }
     }
 
     // -- energy collision (lbm-collision.cpp:231-324)
     const double cp = u_cp(A.U, (float)gas::cp_mass(t, Y, T_si));
     const double gasconstant = u_cp(A.U, (float)(gas::kR / W));
-    const double mu = u_mu(A.U, (float)gas::wilke(t, X, mu_k));
+    const double mu = u_mu(A.U, (float)gas::wilke_from_phi(t, X, mu_k, phi));
     const double lam = u_cond(A.U, (float)gas::mix_cond(t, X, T_si, P_si, mu_k));
     const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
     const double om1 = 2 * p * cp * dt / (p * cp * dt + 2 * lam);
     const double om = 2 * p * dt / (p * dt + 2 * mu);
     if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) atomic_status(A.status, LBMGPU_ST_TAU_UNSTABLE);
     double qd[3] = {0, 0, 0}, qc[3] = {0, 0, 0};
+    const double rl[3] = {rec(A, Rc, RM_RHO, nbl[0]), rec(A, Rc, RM_RHO, nbl[1]), rec(A, Rc, RM_RHO, nbl[2])};
+    const double rh[3] = {rec(A, Rc, RM_RHO, nbh[0]), rec(A, Rc, RM_RHO, nbh[1]), rec(A, Rc, RM_RHO, nbh[2])};
     for (int a = 0; a < NS; ++a) {
         const double ha = u_energy_mass(A.U, (float)(gas::h_RT(t, a, T_si) * gas::kR * T_si / t.m.W[a]));
+        const int pr = rs(a, RS_RHO);
         for (int d = 0; d < 3; ++d) {
             qd[d] += om1 / (-om + om1) * ha * rho_a[a] * (ua[a][d] - um[d]);
-            const double Yl = rec(A, Rc, rs(a, RS_RHO), nbl[d]) / rec(A, Rc, RM_RHO, nbl[d]);
+            const double Yl = rec(A, Rc, pr, nbl[d]) / rl[d];
             const double Yc = rho_a[a] / rho;
-            const double Yh = rec(A, Rc, rs(a, RS_RHO), nbh[d]) / rec(A, Rc, RM_RHO, nbh[d]);
+            const double Yh = rec(A, Rc, pr, nbh[d]) / rh[d];
             const double dY = mc_fd_fuw(Yl, Yc, Yh, ua[a][d] - um[d], tl[d], th[d]);
             qc[d] += 0.5 * (2.0 - om1) / (-om + om1) * dt * p * ha * dY;
         }
     }
-    // mixture gas constant of a neighbour from its composition (lbm-collision.cpp:207-215)
-    auto gc_nb = [&](long m) {
-        if (!fluid_like(A.type[m])) return 0.0;
-        double sYW = 0.0, sY = 0.0;
-        const double rm = rec(A, Rc, RM_RHO, m);
-        for (int a = 0; a < NS; ++a) {
-            const double Ya = rec(A, Rc, rs(a, RS_RHO), m) / rm;
-            sYW += Ya / t.m.W[a];
-            sY += Ya;
-        }
-        return (double)u_cp(A.U, (float)(gas::kR * sYW / sY));
-    };
-    const double P6[6] = {rec(A, Rc, RM_P00, n), rec(A, Rc, RM_P00 + 1, n), rec(A, Rc, RM_P00 + 2, n),
-                          rec(A, Rc, RM_P00 + 3, n), rec(A, Rc, RM_P00 + 4, n), rec(A, Rc, RM_P00 + 5, n)};
+    double P6[6];
+    for (int q = 0; q < 6; ++q) P6[q] = rec(A, Rc, RM_P00 + q, n);
     const double Pf[3][3] = {{P6[0], P6[1], P6[2]}, {P6[1], P6[3], P6[4]}, {P6[2], P6[4], P6[5]}};
     double dq[3];
     for (int d = 0; d < 3; ++d) {
-        const int pu = RM_U + d;
-        const double Ql = rec(A, Rc, RM_RHO, nbl[d]) * rec(A, Rc, pu, nbl[d]) *
-                              (1.0 - 3.0 * gc_nb(nbl[d]) * rec(A, Rc, RM_T, nbl[d])) -
-                          rec(A, Rc, RM_RHO, nbl[d]) * (rec(A, Rc, pu, nbl[d]) * rec(A, Rc, pu, nbl[d]) * rec(A, Rc, pu, nbl[d]));
         const double Qc = rho * um[d] * (1.0 - 3.0 * gasconstant * Tl) - rho * (um[d] * um[d] * um[d]);
-        const double Qh = rec(A, Rc, RM_RHO, nbh[d]) * rec(A, Rc, pu, nbh[d]) *
-                              (1.0 - 3.0 * gc_nb(nbh[d]) * rec(A, Rc, RM_T, nbh[d])) -
-                          rec(A, Rc, RM_RHO, nbh[d]) * (rec(A, Rc, pu, nbh[d]) * rec(A, Rc, pu, nbh[d]) * rec(A, Rc, pu, nbh[d]));
-        const double dQ = mc_fd_central(Ql, Qc, Qh, tl[d], th[d]);
+        const double dQ = mc_fd_central(rec(A, Rc, RM_QX + d, nbl[d]), Qc, rec(A, Rc, RM_QX + d, nbh[d]), tl[d], th[d]);
         double s = 0.0;
         for (int b = 0; b < 3; ++b) s += um[b] * (Pf[b][d] - ((b == d ? p : 0.0) + rho * um[b] * um[d]));
         dq[d] = s + qd[d] + qc[d] + 0.5 * dt * um[d] * dQ;
     }
     AxisG<double> G;
     axis_geq(G, Uint, theta, um);
+    double gv[27];
+#pragma unroll
+    for (int l = 0; l < 27; ++l) gv[l] = ldpop(A, A.pop_src, 27 * NS + l, A.local ? n : pull_idx(pp, l));
+#pragma unroll
     for (int l = 0; l < 27; ++l) {
-        const long plane = (long)(27 * NS + l) * nc;
-        const double gv = A.local ? A.pop_src[plane + n] : A.pop_src[plane + mc_pull_src(A, i, j, k, l)];
         const double gq = geq_l(l, rho, G);
         const double gs = (csq(l) == 1) ? gq + 0.5 * (cx(l) * dq[0] + cy(l) * dq[1] + cz(l) * dq[2]) : gq;
-        A.pop_dst[plane + n] = gv + om1 * (gq - gv) + (om - om1) * (gq - gs);
+        stpop(A, A.pop_dst, 27 * NS + l, n, gv[l] + om1 * (gq - gv[l]) + (om - om1) * (gq - gs));
     }
 }
 
 // ------------------------------------------------------------------------------------
 // Init (reference LBM::Init, multicomponent, src/lbm-init.cpp:85-146).  Writes the
-// record planes it changes into both record buffers and the populations into pop[0].
+// record planes it changes into both record buffers and the populations into pop0.
 // ------------------------------------------------------------------------------------
-template <int NS>
-MC_HDN void mc_init_cell(const McArgs &A, long n, double *rec0, double *rec1, double *pop0) {
+template <int NS, class AT>
+MC_HDN void mc_init_cell(const AT &A, long n, typename AT::R *rec0, typename AT::R *rec1, typename AT::P *pop0) {
     const int ty = A.type[n];
     if (!(ty == T_F || ty == T_I || ty == T_I_C || ty == T_O || ty == T_O_C)) return;
     const gas::Tables &t = *A.tab;
-    const long nc = A.ncell;
-    double Xin[NS], X[NS], Y[NS];
+    double X[NS], Y[NS];
     double s = 0.0;
     for (int a = 0; a < NS; ++a) {
-        Xin[a] = rec0[(long)rs(a, RS_X) * nc + n];
-        X[a] = Xin[a] > 0.0 ? Xin[a] : 0.0;
+        const double xa = rec(A, rec0, rs(a, RS_X), n);
+        X[a] = xa > 0.0 ? xa : 0.0;
         s += X[a];
     }
     double W = 0.0;
@@ -499,49 +541,44 @@ MC_HDN void mc_init_cell(const McArgs &A, long n, double *rec0, double *rec1, do
         W += X[a] * t.m.W[a];
     }
     for (int a = 0; a < NS; ++a) Y[a] = X[a] * t.m.W[a] / W;
-    const double T_si = si_temp(A.U, (float)rec0[(long)RM_T * nc + n]);
-    const double P_si = si_p(A.U, (float)rec0[(long)RM_P * nc + n]);
+    const double Tl = rec(A, rec0, RM_T, n);
+    const double T_si = si_temp(A.U, (float)Tl);
+    const double P_si = si_p(A.U, (float)rec(A, rec0, RM_P, n));
     const double dens = P_si * W / (gas::kR * T_si);
     const double rho = u_rho(A.U, (float)dens);
-    const double vel[3] = {rec0[(long)RM_U * nc + n], rec0[(long)RM_V * nc + n], rec0[(long)RM_W * nc + n]};
+    const double vel[3] = {rec(A, rec0, RM_U, n), rec(A, rec0, RM_V, n), rec(A, rec0, RM_W, n)};
     const double U = u_energy_mass(A.U, (float)gas::int_energy_mass(t, Y, T_si));
     const double rhoe = rho * (U + 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]));
     const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
-    double *R2[2] = {rec0, rec1};
+    typename AT::R *R2[2] = {rec0, rec1};
     for (int b = 0; b < 2; ++b) {
-        R2[b][(long)RM_RHO * nc + n] = rho;
-        R2[b][(long)RM_RHOE * nc + n] = rhoe;
+        put(A, R2[b], RM_RHO, n, rho);
+        put(A, R2[b], RM_RHOE, n, rhoe);
     }
     const bool fluid = ty == T_F;
     AxisG<double> G;
     axis_geq(G, U, theta, vel);
     if (fluid)
-        for (int l = 0; l < 27; ++l) pop0[(long)(27 * NS + l) * nc + n] = geq_l(l, rho, G);
+        for (int l = 0; l < 27; ++l) stpop(A, pop0, 27 * NS + l, n, geq_l(l, rho, G));
     const double zero[3] = {0.0, 0.0, 0.0};
+    double ra_all[NS], ua_all[NS][3];
     for (int a = 0; a < NS; ++a) {
         double ra = Y[a] * rho;
         ra = ra > kSpeciesMin ? ra : kSpeciesMin;
+        ra_all[a] = ra;
         const double tha = u_energy_mass(A.U, (float)(gas::kR * T_si / t.m.W[a]));
         for (int b = 0; b < 2; ++b) {
-            R2[b][(long)rs(a, RS_RHO) * nc + n] = ra;
-            for (int d = 0; d < 3; ++d) R2[b][(long)rs(a, RS_UX + d) * nc + n] = vel[d];
+            put(A, R2[b], rs(a, RS_RHO), n, ra);
+            for (int d = 0; d < 3; ++d) put(A, R2[b], rs(a, RS_UX + d), n, vel[d]);
         }
-        AxisF<double> Fe;
-        axis_feq(Fe, vel, tha, zero);
-        double jx = 0, jy = 0, jz = 0;
-        for (int l = 0; l < 27; ++l) {
-            const double fv = feq_l(l, ra, Fe);
-            if (fluid) pop0[(long)(27 * a + l) * nc + n] = fv;
-            jx += fv * cx(l);
-            jy += fv * cy(l);
-            jz += fv * cz(l);
-        }
-        for (int b = 0; b < 2; ++b) {
-            R2[b][(long)rs(a, RS_JX) * nc + n] = jx;
-            R2[b][(long)rs(a, RS_JX + 1) * nc + n] = jy;
-            R2[b][(long)rs(a, RS_JX + 2) * nc + n] = jz;
+        for (int d = 0; d < 3; ++d) ua_all[a][d] = vel[d];
+        if (fluid) {
+            AxisF<double> Fe;
+            axis_feq(Fe, vel, tha, zero);
+            for (int l = 0; l < 27; ++l) stpop(A, pop0, 27 * a + l, n, feq_l(l, ra, Fe));
         }
     }
+    for (int b = 0; b < 2; ++b) store_face_terms<NS>(A, R2[b], n, ty, rho, vel, Tl, ra_all, ua_all);
 }
 
 }  // namespace lbm

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 CSRC = os.path.join(ROOT, "lattice-boltzmann-method_b200", "csrc")
 NS = 9
-NREC = 14 + 8 * NS
+SP0 = 17          # first per-species record plane
+NREC = SP0 + 8 * NS
 CASES = {
     "mc_mix8.npz": (False, {}, [1, 40]),
     "mc_react8.npz": (True, {"T_hi": 1800.0}, [1, 30]),
@@ -48,7 +49,8 @@ def build_host_lib(tmpdir):
 
 
 def soa_state(mix, sp):
-    """The device record/population planes of an AoS state (as the upload builds them)."""
+    """The device record planes of an AoS state (the planes the upload fills from it; the
+    face-difference terms stay zero until Init computes them)."""
     nc = mix.size
     rec = np.zeros((NREC, nc))
     f = lambda a: np.ascontiguousarray(a).reshape(-1)  # noqa: E731
@@ -59,26 +61,33 @@ def soa_state(mix, sp):
         rec[7 + q] = P[:, 3 * a + b]
     rec[13] = f(mix["HRR"])
     for a in range(NS):
-        base = 14 + 8 * a
+        base = SP0 + 8 * a
         rec[base] = f(sp[a]["rho"])
-        rec[base + 4] = f(sp[a]["u"])
-        rec[base + 5] = f(sp[a]["v"])
-        rec[base + 6] = f(sp[a]["w"])
-        rec[base + 7] = f(sp[a]["X"])
+        rec[base + 1] = f(sp[a]["u"])
+        rec[base + 2] = f(sp[a]["v"])
+        rec[base + 3] = f(sp[a]["w"])
+        rec[base + 4] = f(sp[a]["X"])
     return rec
 
 
-def host_run(L, m, mix, sp, reaction, steps):
+def host_run(L, m, mix, sp, reaction, steps, precision="fp64", shift=True):
+    """Init + `steps` steps of the host build (populations in FP64 or, "fp32", in FP32);
+    returns (record planes, status)."""
+    dt = np.float64 if precision == "fp64" else np.float32
     rec0 = soa_state(mix, sp)
     rec1 = rec0.copy()
     nc = mix.size
-    pop0 = np.zeros((27 * (NS + 1), nc))
+    pop0 = np.zeros((27 * (NS + 1), nc), dt)
     pop1 = np.zeros_like(pop0)
     typ = np.ascontiguousarray(mix["type"].astype(np.int8).reshape(-1))
     st = ctypes.c_uint(0)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
-    L.mc_host_run.restype = ctypes.c_int
-    cur = L.mc_host_run(*mix.shape, P(typ), ctypes.byref(m), ctypes.c_float(W.FLAME_UNITS[0]),
-                        ctypes.c_float(W.FLAME_UNITS[1]), int(reaction), steps, P(pop0), P(pop1), P(rec0),
-                        P(rec1), 1, ctypes.byref(st))
+    args = [*mix.shape, P(typ), ctypes.byref(m), ctypes.c_float(W.FLAME_UNITS[0]),
+            ctypes.c_float(W.FLAME_UNITS[1]), int(reaction), steps, P(pop0), P(pop1), P(rec0), P(rec1)]
+    if precision == "fp64":
+        L.mc_host_run.restype = ctypes.c_int
+        cur = L.mc_host_run(*args, ctypes.byref(st))
+    else:
+        L.mc_host_run32.restype = ctypes.c_int
+        cur = L.mc_host_run32(*args, int(shift), ctypes.byref(st))
     return (rec0, rec1)[cur], st.value

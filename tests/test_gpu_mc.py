@@ -85,3 +85,34 @@ def test_gpu_mc_rejects_boundary_types_and_orders_phases():
         lat.tms_bc()
         lat.calculate_moment()
         assert lat.synchronize() == 0
+
+
+@pytest.mark.parametrize("fixture", ["mc_mix8.npz", "mc_react8.npz"])
+def test_gpu_mc_fp32_storage_within_tolerance(fixture):
+    """FP32 population storage on the device against the device's FP64 mode after 200
+    steps: rho, T, p, rhoe within 1e-5 relative, u within 5e-5 of the largest velocity,
+    every Y_k within 1e-5 absolute."""
+    m, mix, sp, reaction, _ = case(fixture)
+    res = {}
+    for prec in (lbmgpu.FP64, lbmgpu.FP32):
+        with lbmgpu.Lattice(*mix.shape, mech=m, dtype=W.MIXTURE_MC, species_dtype=W.SPECIES, dx_dt=W.FLAME_UNITS,
+                            chem=lbmgpu.CHEM_REF_EXPLICIT if reaction else lbmgpu.CHEM_OFF, precision=prec) as lat:
+            lat.upload(mix, sp)
+            lat.init()
+            lat.step(200)
+            assert lat.synchronize() == 0
+            c = mix.copy()
+            s = [a.copy() for a in sp]
+            lat.download(c, s)
+            res[prec] = (c, s)
+    (c64, s64), (c32, s32) = res[lbmgpu.FP64], res[lbmgpu.FP32]
+    fl = mix["type"] == 0
+    for k in ("rho", "temp", "p", "rhoe"):
+        assert rel(c32[k][fl], c64[k][fl]) < 1e-5, k
+    vs = max(np.abs(c64[k][fl]).max() for k in "uvw")
+    for k in "uvw":
+        assert rel(c32[k][fl], c64[k][fl], vs) < 5e-5, k
+    for a in range(NS):
+        Y64 = s64[a]["rho"][fl] / c64["rho"][fl]
+        Y32 = s32[a]["rho"][fl] / c32["rho"][fl]
+        assert np.abs(Y64 - Y32).max() < 1e-5, a
