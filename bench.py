@@ -58,6 +58,8 @@ def parse():
                          "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
                          "1800 K slab")
+    ap.add_argument("--chem", choices=["ref", "rosenbrock"], default="ref",
+                    help="react workload: the reference's explicit scheme or the ROS2 stiff integrator")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="multicomponent population storage (fp32: shifted FP32 populations, FP64 records)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -321,7 +323,9 @@ def run_ours_mc(args, dist):
     reaction = args.workload == "react"
     m, mix, sp = mc_workload(args)
     ncell = fluid_cells(mix)
-    chem = lbmgpu.CHEM_REF_EXPLICIT if reaction else lbmgpu.CHEM_OFF
+    chem = lbmgpu.CHEM_OFF
+    if reaction:
+        chem = lbmgpu.CHEM_ROSENBROCK if args.chem == "rosenbrock" else lbmgpu.CHEM_REF_EXPLICIT
 
     prec = lbmgpu.FP32 if args.precision == "fp32" else lbmgpu.FP64
     pop_bytes = 4 if args.precision == "fp32" else 8
@@ -384,8 +388,9 @@ def run_ours_mc(args, dist):
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
-        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}: 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
-                               f"dx 20 um, dt 1 ns, " + ("reference explicit chemistry" if reaction else "non-reacting"),
+        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + ": 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
+                               f"dx 20 um, dt 1 ns, " + (("ROS2 stiff chemistry" if args.chem == "rosenbrock" else
+                                                          "reference explicit chemistry") if reaction else "non-reacting"),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
                    "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
         "hbm_gbs_step": ncell * (mc_bytes("k_mc_collide", pop_bytes, reaction) + mc_bytes("k_mc_stream", pop_bytes))

@@ -41,6 +41,7 @@ extern "C" {
 #define LBMGPU_ST_TAU_UNSTABLE 0x4u /* 1/omega <= 1/2 (the reference prints these:
                                        src/lbm-collision.cpp:33-34)                   */
 #define LBMGPU_ST_NEWTON 0x8u       /* temperature Newton iteration hit its cap        */
+#define LBMGPU_ST_CHEM 0x10u        /* stiff chemistry hit its sub-step cap            */
 
 /* ---- precision of the population storage ------------------------------------- */
 #define LBMGPU_FP64 0   /* the reference's doubles; results bit-faithful                */
@@ -107,6 +108,13 @@ typedef struct lbmgpu_species_layout {
 #define LBMGPU_CHEM_REF_EXPLICIT 1  /* the reference's scheme: two explicit half steps of
                                        the net production rates with T from (u, v) in
                                        between (src/lbm-collision.cpp:370-399)          */
+#define LBMGPU_CHEM_ROSENBROCK 2    /* no counterpart in the reference: the constant-
+                                       density, constant-energy reactor integrated over
+                                       the whole step by the L-stable two-stage
+                                       Rosenbrock method ROS2 with step-size control
+                                       (rtol 1e-5; at most 256 sub-steps, then
+                                       LBMGPU_ST_CHEM), its density change entering the
+                                       species collision like the reference's            */
 
 typedef struct lbmgpu_desc {
     int abi_version;      /* LBMGPU_ABI_VERSION                                           */

@@ -452,7 +452,8 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
         if (!desc->mech || desc->mech->n_species != desc->n_species) return LBMGPU_E_ARG;
         if (!valid_mech(*desc->mech)) return LBMGPU_E_ARG;
         if (desc->n_species != 9) return LBMGPU_E_UNSUPPORTED;  // kernels are built for 9 species
-        if (desc->chem_mode != LBMGPU_CHEM_OFF && desc->chem_mode != LBMGPU_CHEM_REF_EXPLICIT)
+        if (desc->chem_mode != LBMGPU_CHEM_OFF && desc->chem_mode != LBMGPU_CHEM_REF_EXPLICIT &&
+            desc->chem_mode != LBMGPU_CHEM_ROSENBROCK)
             return LBMGPU_E_UNSUPPORTED;
         if (!(desc->units_m > 0.f) || !(desc->units_kg > 0.f) || !(desc->units_s > 0.f) || !(desc->units_K > 0.f))
             return LBMGPU_E_ARG;

@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "d3q27.cuh"
+#include "chem.cuh"
 #include "gas.cuh"
 #include "units.cuh"
 
@@ -47,7 +48,7 @@ enum : int { RS_RHO = 0, RS_UX = 1, RS_X = 4, RS_QX = 5 };
 MC_HD int mc_nrec(int ns) { return RM_SP + RM_SPN * ns; }
 MC_HD int rs(int a, int f) { return RM_SP + RM_SPN * a + f; }
 
-enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1 };
+enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1, CHEM_ROSENBROCK = 2 };
 
 template <typename P_, typename R_>
 struct McArgsT {
@@ -382,6 +383,20 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         for (int a = 0; a < NS; ++a)
             hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
         put(A, A.rec_nxt, RM_HRR, n, hrr);
+    } else if (A.chem == CHEM_ROSENBROCK) {
+        // stiff alternative: the constant-(rho, e) reactor over the whole lattice step with
+        // ROS2 (chem.cuh); the density change and the heat release enter the collision the
+        // same way as the reference's explicit increments
+        double Yc[gas::MAXS], Tc = T_si;
+        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+        if (gas::ros2_advance(t, rho_si, Yc, Tc, (double)dt * (double)A.U.s) < 0)
+            atomic_status(A.status, LBMGPU_ST_CHEM);
+        double hrr = 0.0;
+        for (int a = 0; a < NS; ++a) {
+            drho[a] = rho * (Yc[a] - Y[a]);
+            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
+        }
+        put(A, A.rec_nxt, RM_HRR, n, hrr);
     }
 
     // -- species viscosities, Wilke weights, relaxation rates (lbm-collision.cpp:402-430)
@@ -456,11 +471,11 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         const double zero[3] = {0.0, 0.0, 0.0};
         axis_feq(Fr, um, theta, zero);
         const double om = om_a[a];
-        const bool skip_all = rho_a[a] <= kSpeciesMin && A.chem != CHEM_REF_EXPLICIT;
+        const bool skip_all = rho_a[a] <= kSpeciesMin && A.chem == CHEM_OFF;
 #pragma unroll
         for (int l = 0; l < 27; ++l) {
             const int plane = 27 * a + l;
-            const double fr = A.chem == CHEM_REF_EXPLICIT ? feq_l(l, drho[a], Fr) : 0.0;
+            const double fr = A.chem != CHEM_OFF ? feq_l(l, drho[a], Fr) : 0.0;
             if (skip_all || (rho_a[a] <= kSpeciesMin && fr <= 0.0)) {
                 if (!A.local) A.pop_dst[(long)plane * A.ncell + n] = A.pop_prev[(long)plane * A.ncell + n];
                 continue;

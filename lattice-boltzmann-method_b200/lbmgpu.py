@@ -38,8 +38,8 @@ EXPORTS = [
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
     "lbmgpu_units_from_dx_dt",
 ]
-CHEM_OFF, CHEM_REF_EXPLICIT = 0, 1
-ST_NEWTON = 0x8
+CHEM_OFF, CHEM_REF_EXPLICIT, CHEM_ROSENBROCK = 0, 1, 2
+ST_NEWTON, ST_CHEM = 0x8, 0x10
 
 
 class MixtureLayout(ctypes.Structure):

@@ -116,3 +116,28 @@ def test_gpu_mc_fp32_storage_within_tolerance(fixture):
         Y64 = s64[a]["rho"][fl] / c64["rho"][fl]
         Y32 = s32[a]["rho"][fl] / c32["rho"][fl]
         assert np.abs(Y64 - Y32).max() < 1e-5, a
+
+
+def test_gpu_mc_rosenbrock_matches_host_build(tmp_path):
+    """CHEM_ROSENBROCK on the device against the same per-cell functions built for the host
+    (FP64, 10 steps of the reacting fixture); the adaptive sub-step control is the only
+    place where rounding differences could change a decision, hence 1e-7."""
+    from mc_common import SP0, build_host_lib, host_run
+    m, mix, sp, _, _ = case("mc_react8.npz")
+    R, st = host_run(build_host_lib(tmp_path), m, mix, sp, lbmgpu.CHEM_ROSENBROCK, 10)
+    assert st == 0
+    with lbmgpu.Lattice(*mix.shape, mech=m, dtype=W.MIXTURE_MC, species_dtype=W.SPECIES, dx_dt=W.FLAME_UNITS,
+                        chem=lbmgpu.CHEM_ROSENBROCK) as lat:
+        lat.upload(mix, sp)
+        lat.init()
+        lat.step(10)
+        assert lat.synchronize() == 0
+        c = mix.copy()
+        s = [a.copy() for a in sp]
+        lat.download(c, s)
+    fl = mix["type"] == 0
+    f1 = fl.reshape(-1)
+    for q, k in ((0, "rho"), (4, "temp"), (5, "p"), (6, "rhoe"), (13, "HRR")):
+        assert rel(c[k][fl], R[q][f1]) < 1e-7, k
+    for a in range(NS):
+        assert rel(s[a]["rho"][fl], R[SP0 + 8 * a][f1]) < 1e-7, a
