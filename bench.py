@@ -388,7 +388,7 @@ def run_ours_mc(args, dist):
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
-        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + ": 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
+        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + f": 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
                                f"dx 20 um, dt 1 ns, " + (("ROS2 stiff chemistry" if args.chem == "rosenbrock" else
                                                           "reference explicit chemistry") if reaction else "non-reacting"),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
