@@ -53,11 +53,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
-    ap.add_argument("--workload", choices=["tgv", "mix", "react"], default="tgv",
+    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan"], default="tgv",
                     help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
                          "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
-                         "1800 K slab")
+                         "1800 K slab; inflow: config 2's shape, the mixing layer between a characteristic "
+                         "inflow and outflow (N^3); chan: config 3's shape, a reacting H2-air channel with "
+                         "NSCBC outflow ends and TMS walls (2N x N/2 x N/2)")
     ap.add_argument("--chem", choices=["ref", "rosenbrock"], default="ref",
                     help="react workload: the reference's explicit scheme or the ROS2 stiff integrator")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
@@ -285,12 +287,21 @@ def mc_bytes(kernel, pop_bytes, reaction=False):
 
 
 
+MC_SHAPES = {"mix": "periodic", "react": "periodic", "inflow": "TYPE_I_C inflow / TYPE_O_C outflow in x, periodic y z",
+             "chan": "TYPE_O_C outflow at both x ends, TMS solid y walls, periodic z"}
+
+
 def mc_workload(args):
     import mech
     import workloads
     m = mech.h2_air_9()
-    kw = {"T_hi": 1800.0} if args.workload == "react" else {}
-    mix, sp = workloads.mixing_layer_mc(m, N=args.N, **kw)
+    if args.workload == "inflow":
+        mix, sp = workloads.inflow_layer_mc(m, NX=args.N, NY=args.N, NZ=args.N)
+    elif args.workload == "chan":
+        mix, sp = workloads.flame_channel_mc(m, NX=2 * args.N, NY=args.N // 2, NZ=args.N // 2)
+    else:
+        kw = {"T_hi": 1800.0} if args.workload == "react" else {}
+        mix, sp = workloads.mixing_layer_mc(m, N=args.N, **kw)
     return m, mix, sp
 
 
@@ -320,7 +331,7 @@ def run_ours_mc(args, dist):
     import lbmgpu
     import workloads
     device = dist.local
-    reaction = args.workload == "react"
+    reaction = args.workload in ("react", "chan")
     m, mix, sp = mc_workload(args)
     ncell = fluid_cells(mix)
     chem = lbmgpu.CHEM_OFF
@@ -388,7 +399,7 @@ def run_ours_mc(args, dist):
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
-        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + f": 9-species H2/O2/N2 D3Q27, {args.N}^3 periodic, "
+        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + f": 9-species H2/O2/N2 D3Q27, {'x'.join(str(s_ - 2) for s_ in mix.shape)} {MC_SHAPES[args.workload]}, "
                                f"dx 20 um, dt 1 ns, " + (("ROS2 stiff chemistry" if args.chem == "rosenbrock" else
                                                           "reference explicit chemistry") if reaction else "non-reacting"),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",

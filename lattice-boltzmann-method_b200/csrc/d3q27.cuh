@@ -18,6 +18,10 @@ enum CellType : int {
     T_F = 0, T_S = 1, T_P = 2, T_A = 3, T_FS = 4, T_I = 5, T_O = 6, T_I_C = 7, T_O_C = 8, T_Q = 9
 };
 
+// Per-cell flags of the device's cell classification: a fluid cell, and one with a
+// boundary cell (anything but fluid or a periodic ghost) upstream along some direction.
+enum : uint8_t { CF_FLUID = 1, CF_SPECIAL = 2 };
+
 // Direction l of the reference's D3Q27 ordering (src/headers/lbm.hpp:49-53), packed two
 // bits per axis (0 -> 0, 1 -> +1, 2 -> -1), x in bits 0-1, y in 2-3, z in 4-5.  All loops
 // over l are unrolled, so these fold to immediates.

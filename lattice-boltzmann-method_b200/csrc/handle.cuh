@@ -72,6 +72,7 @@ struct lbmgpu {
     gas::Tables *tab = nullptr;  // device copy
     bool fp32 = false;           // FP32 population storage: pop32 instead of pop
     float *pop32[2] = {nullptr, nullptr};
+    float *bst32[2] = {nullptr, nullptr};
     double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
     long nfluid = 0;
 };

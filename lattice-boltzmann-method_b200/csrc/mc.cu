@@ -6,8 +6,12 @@
 //   LBM::Streaming + LBM::calculate_moment src/lbm-streaming.cpp, src/lbm-moment.cpp:193-377
 //                                          -> k_mc_stream
 //   LBM::Init                              src/lbm-init.cpp:85-146 -> k_mc_init
-// This path covers periodic lattices (fluid cells and periodic ghosts); the other cell
-// types are rejected at upload with LBMGPU_E_UNSUPPORTED.
+//   LBM::Streaming + LBM::TMS_BC + LBM::calculate_moment of the cells with a boundary
+//   upstream (src/lbm-bc.cpp:122-1110, src/impose_nscbc.cpp) -> k_mc_special
+// Cell types: fluid, periodic ghosts, solid (TMS wall), adiabatic, free-slip, and the
+// characteristic inflow/outflow ghosts TYPE_I_C / TYPE_O_C.  The reference's
+// non-characteristic TYPE_I / TYPE_O rewrite a neighbour's moments from inside the
+// boundary sweep (order dependent) and are rejected at upload with LBMGPU_E_UNSUPPORTED.
 //
 // Storage: FP64 (bit-faithful to the reference) or FP32 (LBMGPU_FP32: populations in
 // float as deviations from a per-plane shift; the per-cell record stays FP64, and all
@@ -17,6 +21,7 @@
 #include <vector>
 
 #include "handle.cuh"
+#include "mc_bc.cuh"
 #include "mc_cell.cuh"
 
 namespace {
@@ -29,8 +34,27 @@ constexpr int NS9 = 9;
 template <int NS, typename S>
 __global__ void __launch_bounds__(kBlock) k_mc_collide(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
+    if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     mc_collide_cell<NS>(A, n);
+}
+
+// the cells with a boundary upstream, one thread each (compact list)
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_special(McArgsT<S, double> A, const long *__restrict__ blist) {
+    const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= A.nb) return;
+    mc_special_cell<NS>(A, blist[b], b);
+}
+
+// the special cells' current populations into the compact store (after upload and Init)
+template <typename S>
+__global__ void k_mc_fill_bst(long ncell, long nb, int np, const long *__restrict__ blist, const S *__restrict__ pop,
+                              S *__restrict__ bst) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long)np * nb) return;
+    const int q = (int)(i / nb);
+    const long b = i - (long)q * nb;
+    bst[i] = pop[(long)q * ncell + blist[b]];
 }
 
 template <int NS, typename S>
@@ -57,7 +81,7 @@ __global__ void __launch_bounds__(kMeanBlock) k_plane_mean(McArgsT<S, double> A,
     const int q = blockIdx.x;
     double s = 0.0;
     for (long n = threadIdx.x; n < A.ncell; n += kMeanBlock)
-        if (A.cflag[n] == CF_FLUID) s += ldpop(A, pop, q, n);
+        if (A.cflag[n] & CF_FLUID) s += ldpop(A, pop, q, n);
     red[threadIdx.x] = s;
     __syncthreads();
     for (int w = kMeanBlock / 2; w > 0; w >>= 1) {
@@ -106,7 +130,7 @@ __global__ void k_mc_unpack(McArgsT<S, double> A, MixOff mo, SpOff so, const cha
     const int pi[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
     for (int q = 0; q < 6; ++q) pr(RM_P00 + q, ldd(mr, mo.p_tensor + 8 * (3 * pi[q][0] + pi[q][1])));
     pr(RM_HRR, ldd(mr, mo.HRR));
-    const bool fluid = A.cflag[n] == CF_FLUID;
+    const bool fluid = A.cflag[n] & CF_FLUID;
     double rho_a[NS], ua[NS][3];
     for (int a = 0; a < NS; ++a) {
         const char *sr = stage + cnt * mo.size + ((long)a * cnt + (n - n0)) * so.size;
@@ -136,7 +160,7 @@ __global__ void k_mc_unpack(McArgsT<S, double> A, MixOff mo, SpOff so, const cha
 // otherwise); pop_pc: the post-collision populations (fpc, gpc).
 template <int NS, typename S>
 __global__ void k_mc_pack(McArgsT<S, double> A, MixOff mo, SpOff so, char *__restrict__ stage, long n0, long n1,
-                          const double *rec, const S *pop_now, const S *pop_pc, int stepped) {
+                          const double *rec, const S *pop_now, const S *pop_pc, const S *bst, int stepped) {
     const long n = n0 + (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n1) return;
     const long cnt = n1 - n0;
@@ -152,9 +176,16 @@ __global__ void k_mc_pack(McArgsT<S, double> A, MixOff mo, SpOff so, char *__res
     std_(mr, mo.HRR, get(RM_HRR));
     const int full[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
     for (int q = 0; q < 9; ++q) std_(mr, mo.p_tensor + 8 * q, get(RM_P00 + full[q]));
-    const bool fluid = A.cflag[n] == CF_FLUID;
+    const bool fluid = A.cflag[n] & CF_FLUID;
+    const bool special = stepped && (A.cflag[n] & CF_SPECIAL);
+    const long bs = special ? (long)A.bid[n] : 0;
     McPull pp;
     mc_pull(A, n, pp);
+    // the cell's populations: kept in the special-cell store, pulled, or in place
+    auto now = [&](int plane, int l) {
+        if (special) return ldpop_b(A, bst, plane, bs);
+        return ldpop(A, pop_now, plane, stepped ? pull_idx(pp, l) : n);
+    };
     for (int a = 0; a < NS; ++a) {
         char *sr = stage + cnt * mo.size + ((long)a * cnt + (n - n0)) * so.size;
         std_(sr, so.rho, get(rs(a, RS_RHO)));
@@ -165,7 +196,7 @@ __global__ void k_mc_pack(McArgsT<S, double> A, MixOff mo, SpOff so, char *__res
         if (!fluid) continue;
         for (int l = 0; l < 27; ++l) {
             const int plane = 27 * a + l;
-            std_(sr, so.f + 8 * l, ldpop(A, pop_now, plane, stepped ? pull_idx(pp, l) : n));
+            std_(sr, so.f + 8 * l, now(plane, l));
             std_(sr, so.fpc + 8 * l, ldpop(A, pop_pc, plane, n));
         }
     }
@@ -173,7 +204,7 @@ __global__ void k_mc_pack(McArgsT<S, double> A, MixOff mo, SpOff so, char *__res
     double q3[3] = {0, 0, 0};
     for (int l = 0; l < 27; ++l) {
         const int plane = 27 * NS + l;
-        const double gv = ldpop(A, pop_now, plane, stepped ? pull_idx(pp, l) : n);
+        const double gv = now(plane, l);
         std_(mr, mo.g + 8 * l, gv);
         std_(mr, mo.gpc + 8 * l, ldpop(A, pop_pc, plane, n));
         q3[0] += gv * cx(l);
@@ -201,6 +232,8 @@ McArgsT<S, double> base_args(lbmgpu *h) {
     A.cflag = h->cflag;
     A.status = h->status;
     A.shift = h->fp32 ? h->shift[0] : nullptr;
+    A.bid = h->bid;
+    A.nb = h->nb;
     return A;
 }
 
@@ -208,6 +241,21 @@ McArgsT<S, double> base_args(lbmgpu *h) {
 template <typename S> S *popb(lbmgpu *h, int b);
 template <> double *popb<double>(lbmgpu *h, int b) { return h->pop[b]; }
 template <> float *popb<float>(lbmgpu *h, int b) { return h->pop32[b]; }
+template <typename S> S *bstb(lbmgpu *h, int b);
+template <> double *bstb<double>(lbmgpu *h, int b) { return h->bst[b]; }
+template <> float *bstb<float>(lbmgpu *h, int b) { return h->bst32[b]; }
+
+// the special cells' populations of pop[cur] into bst[cur]
+template <typename S>
+int fill_bst(lbmgpu *h) {
+    if (h->nb == 0) return 0;
+    const int np = 27 * (h->ns + 1);
+    const long total = (long)np * h->nb;
+    k_mc_fill_bst<S><<<grid_for(total), kBlock, 0, h->stream>>>(h->g.ncell, h->nb, np, h->blist, popb<S>(h, h->cur),
+                                                                bstb<S>(h, h->cur));
+    CK(cudaGetLastError());
+    return 0;
+}
 
 bool valid_mc_layout(const lbmgpu_mixture_layout &m, const lbmgpu_species_layout &s) {
     if (m.size == 0 || m.size % 8 || s.size == 0 || s.size % 8) return false;
@@ -268,7 +316,7 @@ int pack_chunk(lbmgpu *h, long n0, long n1, bool stepped) {
     EvPair ep{};
     ev_begin(h, K_OTHER, ep);
     k_mc_pack<NS9, S><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[c],
-                                                                   popb<S>(h, c), pc, stepped ? 1 : 0);
+                                                                   popb<S>(h, c), pc, bstb<S>(h, c), stepped ? 1 : 0);
     ev_end(h, ep);
     CK(cudaGetLastError());
     return 0;
@@ -298,6 +346,7 @@ int collide_t(lbmgpu *h) {
     A.rec_cur = h->mom[c];
     A.rec_nxt = h->mom[x];
     A.local = local ? 1 : 0;
+    A.bst_cur = bstb<S>(h, c);
     EvPair ep{};
     ev_begin(h, K_COLLIDE, ep);
     k_mc_collide<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
@@ -318,6 +367,15 @@ int stream_t(lbmgpu *h) {
     k_mc_stream<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
     ev_end(h, ep);
     CK(cudaGetLastError());
+    if (h->nb > 0) {
+        A.bst_cur = bstb<S>(h, c);
+        A.bst_nxt = bstb<S>(h, x);
+        EvPair eb{};
+        ev_begin(h, K_OTHER, eb);
+        k_mc_special<NS9, S><<<grid_for(h->nb), kBlock, 0, h->stream>>>(A, h->blist);
+        ev_end(h, eb);
+        CK(cudaGetLastError());
+    }
     return 0;
 }
 
@@ -371,8 +429,10 @@ void mc_release(lbmgpu *h) {
     h->tab = nullptr;
     for (int b = 0; b < 2; ++b) {
         cudaFree(h->pop32[b]);
+        cudaFree(h->bst32[b]);
         cudaFree(h->shift[b]);
         h->pop32[b] = nullptr;
+        h->bst32[b] = nullptr;
         h->shift[b] = nullptr;
     }
 }
@@ -392,10 +452,12 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
         short t;
         std::memcpy(&t, hm + n * ms + h->mo.type, sizeof(short));
         if (t < 0 || t > 9) return LBMGPU_E_ARG;
-        if (t != T_F && t != T_P) return LBMGPU_E_UNSUPPORTED;  // periodic lattices only
+        if (t == T_I || t == T_O || t == T_Q) return LBMGPU_E_UNSUPPORTED;
         ty[n] = (int8_t)t;
     }
-    long nfluid = 0;
+    long nfluid = 0, nb = 0;
+    std::vector<int> bidh(nc, -1);
+    std::vector<long> blh;
     for (int i = 0; i < g.Nx; ++i)
         for (int j = 0; j < g.Ny; ++j)
             for (int k = 0; k < g.Nz; ++k) {
@@ -403,16 +465,55 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
                 if (ty[n] != T_F) continue;
                 if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
                     return LBMGPU_E_ARG;
-                cf[n] = CF_FLUID;
+                uint8_t c = CF_FLUID;
+                for (int l = 0; l < 27; ++l) {
+                    const int t = ty[n - (long)cx(l) * g.si - (long)cy(l) * g.sj - cz(l)];
+                    if (t != T_F && t != T_P) c |= CF_SPECIAL;
+                }
+                if (c & CF_SPECIAL) {
+                    bidh[n] = (int)nb++;
+                    blh.push_back(n);
+                }
+                cf[n] = c;
                 ++nfluid;
             }
+    // the boundary formulas read up to two cells inward along an axis
+    if (nb > 0 && (g.Nx < 5 || g.Ny < 5 || g.Nz < 5)) return LBMGPU_E_UNSUPPORTED;
     h->nfluid = nfluid;
+    if (nb != h->nb || !h->blist) {
+        const size_t np = 27 * (size_t)(h->ns + 1), es = h->fp32 ? sizeof(float) : sizeof(double);
+        for (int b = 0; b < 2; ++b) {
+            void *&p = h->fp32 ? reinterpret_cast<void *&>(h->bst32[b]) : reinterpret_cast<void *&>(h->bst[b]);
+            if (p) {
+                cudaFree(p);
+                h->bytes -= np * (size_t)std::max<long>(h->nb, 1) * es;
+                p = nullptr;
+            }
+        }
+        if (h->blist) {
+            cudaFree(h->blist);
+            h->bytes -= (size_t)std::max<long>(h->nb, 1) * sizeof(long);
+            h->blist = nullptr;
+        }
+        h->nb = nb;
+        for (int b = 0; b < 2; ++b) {
+            const int rc = h->fp32 ? dalloc(h, &h->bst32[b], np * (size_t)std::max<long>(nb, 1))
+                                   : dalloc(h, &h->bst[b], np * (size_t)std::max<long>(nb, 1));
+            if (rc) return rc;
+        }
+        const int rc = dalloc(h, &h->blist, (size_t)std::max<long>(nb, 1));
+        if (rc) return rc;
+    }
+    if (nb > 0) CK(cudaMemcpyAsync(h->blist, blh.data(), nb * sizeof(long), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->bid, bidh.data(), nc * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->type, ty.data(), nc, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cflag, cf.data(), nc, cudaMemcpyHostToDevice, h->stream));
     int rc = h->fp32 ? upload_t<float>(h, hm, species) : upload_t<double>(h, hm, species);
     if (rc) return rc;
     h->cur = 0;
     rc = rebase_shift(h);
+    if (rc) return rc;
+    rc = h->fp32 ? fill_bst<float>(h) : fill_bst<double>(h);
     if (rc) return rc;
     CK(cudaStreamSynchronize(h->stream));
     h->pack_mode = PK_UPLOADED;
@@ -471,6 +572,8 @@ int mc_init(lbmgpu *h) {
     int rc = h->fp32 ? init_t<float>(h) : init_t<double>(h);
     if (rc) return rc;
     rc = rebase_shift(h);
+    if (rc) return rc;
+    rc = h->fp32 ? fill_bst<float>(h) : fill_bst<double>(h);
     if (rc) return rc;
     h->pack_mode = PK_INIT;
     return LBMGPU_OK;

@@ -69,6 +69,12 @@ struct McArgsT {
     const double *shift;   // per population plane, or null (no shift)
     unsigned *status;
     int local;
+    // cells with a boundary upstream ("special"): compact index, and their streamed and
+    // boundary-treated populations, 27 (NS+1) planes of nb entries
+    const int *bid;
+    const P *bst_cur;      // of the current step (collide, and the stale directions)
+    P *bst_nxt;            // written by the special-cell stream kernel
+    long nb;
 };
 using McArgs = McArgsT<double, double>;
 
@@ -88,6 +94,16 @@ MC_HD double ldpop(const AT &A, const T *p, int plane, long idx) {
 template <class AT, typename T>
 MC_HD void stpop(const AT &A, T *p, int plane, long idx, double v) {
     p[(long)plane * A.ncell + idx] = (T)(A.shift ? v - A.shift[plane] : v);
+}
+// the same for the compact special-cell store (planes of nb entries)
+template <class AT, typename T>
+MC_HD double ldpop_b(const AT &A, const T *p, int plane, long b) {
+    const double v = (double)p[(long)plane * A.nb + b];
+    return A.shift ? v + A.shift[plane] : v;
+}
+template <class AT, typename T>
+MC_HD void stpop_b(const AT &A, T *p, int plane, long b, double v) {
+    p[(long)plane * A.nb + b] = (T)(A.shift ? v - A.shift[plane] : v);
 }
 
 MC_HD void atomic_status(unsigned *s, unsigned bits) {
@@ -189,12 +205,12 @@ MC_HD void store_face_terms(const AT &A, typename AT::R *R, long n, int ty, doub
 }
 
 // ------------------------------------------------------------------------------------
-// Streaming + moments (reference LBM::Streaming and the multicomponent
-// LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one fluid cell of a periodic
-// lattice.
+// Moments (the multicomponent LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one
+// fluid cell from its streamed populations; pop(a, l) returns population l of species a
+// (a = NS: the energy set) of the cell.
 // ------------------------------------------------------------------------------------
-template <int NS, class AT>
-MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
+template <int NS, class AT, class Pop>
+MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     const gas::Tables &t = *A.tab;
     // -- old state, as the reference's Cantera object is set at the start (lbm-moment.cpp:219-221)
     double Yo_raw[NS], Yo[NS], Xo[NS];
@@ -205,15 +221,13 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
     const double rho_si = si_rho(A.U, (float)rho_old);
     const double P_si = rho_si * gas::kR * T_si / Wold;
 
-    // -- pulled populations: sums per species and of g
-    McPull pp;
-    mc_pull(A, n, pp);
+    // -- sums per species and of g
     double rho_a[NS], j_a[NS][3];
     double P6[6] = {0, 0, 0, 0, 0, 0};
     for (int a = 0; a < NS; ++a) {
         double fv[27];
 #pragma unroll
-        for (int l = 0; l < 27; ++l) fv[l] = ldpop(A, A.pop_src, 27 * a + l, pull_idx(pp, l));
+        for (int l = 0; l < 27; ++l) fv[l] = pop(a, l);
         double r = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
         for (int l = 0; l < 27; ++l) {
@@ -235,7 +249,7 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
     }
     double rhoe = 0.0;
 #pragma unroll
-    for (int l = 0; l < 27; ++l) rhoe += ldpop(A, A.pop_src, 27 * NS + l, pull_idx(pp, l));
+    for (int l = 0; l < 27; ++l) rhoe += pop(NS, l);
 
     double rho = 0, ru = 0, rv = 0, rw = 0, rho_s[NS];
     for (int a = 0; a < NS; ++a) {
@@ -325,6 +339,15 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
         atomic_status(A.status, LBMGPU_ST_NAN);
     else if (!(rho > 0.0) || !(Tn > 0.0))
         atomic_status(A.status, LBMGPU_ST_NEG_STATE);
+}
+
+// Streaming + moments of a fluid cell of the periodic interior (no boundary upstream):
+// every population pulled from its upstream neighbour.
+template <int NS, class AT>
+MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
+    McPull pp;
+    mc_pull(A, n, pp);
+    mc_moments_cell<NS>(A, n, [&](int a, int l) { return ldpop(A, A.pop_src, 27 * a + l, pull_idx(pp, l)); });
 }
 
 // ------------------------------------------------------------------------------------
@@ -439,13 +462,21 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         th[d] = A.type[nbh[d]];
     }
     McPull pp;
-    if (!A.local) mc_pull(A, n, pp);
+    const bool special = !A.local && (A.cflag[n] & CF_SPECIAL);
+    const long bs = special ? (long)A.bid[n] : 0;
+    if (!A.local && !special) mc_pull(A, n, pp);
+    // the cell's populations after streaming and boundary treatment
+    auto fetch = [&](int plane, int l) {
+        if (A.local) return ldpop(A, A.pop_src, plane, n);
+        if (special) return ldpop_b(A, A.bst_cur, plane, bs);
+        return ldpop(A, A.pop_src, plane, pull_idx(pp, l));
+    };
 
     // -- species collision (lbm-collision.cpp:446-519)
     for (int a = 0; a < NS; ++a) {
         double fv[27];
 #pragma unroll
-        for (int l = 0; l < 27; ++l) fv[l] = ldpop(A, A.pop_src, 27 * a + l, A.local ? n : pull_idx(pp, l));
+        for (int l = 0; l < 27; ++l) fv[l] = fetch(27 * a + l, l);
         // bare species velocity sum f c / rho_a (lbm-collision.cpp:446-454)
         double ux[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -525,7 +556,7 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
     axis_geq(G, Uint, theta, um);
     double gv[27];
 #pragma unroll
-    for (int l = 0; l < 27; ++l) gv[l] = ldpop(A, A.pop_src, 27 * NS + l, A.local ? n : pull_idx(pp, l));
+    for (int l = 0; l < 27; ++l) gv[l] = fetch(27 * NS + l, l);
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
         const double gq = geq_l(l, rho, G);

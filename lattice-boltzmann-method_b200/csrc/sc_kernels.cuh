@@ -31,7 +31,6 @@ enum : int {
     M_RHO = 0, M_U = 1, M_V = 2, M_W = 3, M_T = 4, M_P = 5, M_QX = 6, M_QY = 7, M_QZ = 8,
     M_SX = 9, M_SY = 10, M_SZ = 11, M_UINT = 12, M_N = 13
 };
-enum : uint8_t { CF_FLUID = 1, CF_SPECIAL = 2 };
 
 struct ScGeom {
     int Nx, Ny, Nz;

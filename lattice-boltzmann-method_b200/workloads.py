@@ -218,3 +218,85 @@ def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=10
     for a in range(ns):
         sp[a]["X"][fl] = X[..., a][fl]
     return mix, sp
+
+
+def _mole_fractions(mech, Y_named):
+    """Mole fractions of a composition given by mass fraction per species name (the rest
+    at SPECIES_MIN mole fraction), normalised."""
+    names = mech.species_names()
+    ns = len(names)
+    W = np.array([mech.W[k] for k in range(ns)])
+    Y = np.zeros(ns)
+    for n_, y in Y_named.items():
+        Y[names.index(n_)] = y
+    X = Y / W
+    X /= X.sum()
+    X = np.maximum(X, SPECIES_MIN)
+    return X / X.sum()
+
+
+def flame_channel_mc(mech, NX=32, NY=8, NZ=8, T_u=300.0, T_b=1800.0, T_wall=300.0, width=None, seed=SEED):
+    """Reacting H2-air channel with characteristic boundaries (the shape of config 3):
+    stoichiometric H2-air (X_H2 : X_O2 : X_N2 = 0.2958 : 0.1479 : 0.5563) at 1 atm and
+    T_u, a tanh ignition kernel to T_b at mid-x (width max(1.5, NX/16) cells); x ends are
+    TYPE_O_C ghosts (target pressure 1 atm), y walls TYPE_S at T_wall, z periodic.  A
+    seeded sinusoidal ripple on the kernel position breaks the y/z symmetry."""
+    width = max(1.5, NX / 16.0) if width is None else width
+    names = mech.species_names()
+    ns = len(names)
+    mix, sp = _blank_mc(NX, NY, NZ, ns)
+    Nx, Ny, Nz = mix.shape
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ph = rng.uniform(0, 2 * np.pi, size=2)
+    i, j, k = np.meshgrid(np.arange(Nx), np.arange(Ny), np.arange(Nz), indexing="ij")
+    mix["type"][(k == 0) | (k == Nz - 1)] = TYPE_P
+    mix["type"][(i == 0) | (i == Nx - 1)] = TYPE_O_C
+    mix["type"][(j == 0) | (j == Ny - 1)] = TYPE_S
+    W = np.array([mech.W[kk] for kk in range(ns)])
+    Xu = np.full(ns, SPECIES_MIN)
+    for n_, x in (("H2", 0.2958), ("O2", 0.1479), ("N2", 0.5563)):
+        Xu[names.index(n_)] = x
+    Xu /= Xu.sum()
+    xc = 0.5 * NX + 0.05 * NX * np.sin(2 * np.pi * j / NY + ph[0]) * np.sin(2 * np.pi * k / NZ + ph[1])
+    s = 0.5 * (np.tanh((i - xc + 0.125 * NX) / width) - np.tanh((i - xc - 0.125 * NX) / width))
+    T = T_u + (T_b - T_u) * s
+    solid = mix["type"] == TYPE_S
+    T[solid] = T_wall
+    gas_cells = ~solid
+    mix["temp"][gas_cells] = np.float32(T[gas_cells] / K_UNIT).astype(np.float64)
+    mix["temp"][solid] = t_lattice(T_wall)
+    mix["p"][gas_cells] = p_lattice(ONE_ATM)
+    for a in range(ns):
+        sp[a]["X"][gas_cells] = Xu[a]
+    del W
+    return mix, sp
+
+
+def inflow_layer_mc(mech, NX=32, NY=8, NZ=8, u_in_si=5.0, T_in=300.0, Y_H2=0.03, T_hot=1000.0, width=None,
+                    seed=SEED):
+    """H2/air mixing layer between a characteristic inflow and outflow (the shape of
+    config 2): x = 0 ghosts TYPE_I_C carry the inflow target (air at T_in, u = u_in_si),
+    x = NX+1 ghosts TYPE_O_C the target pressure of 1 atm, y and z periodic.  Inside, the
+    seeded interface of mixing_layer_mc (H2-laden hot gas downstream of x0) advected at
+    the inflow velocity."""
+    width = max(1.5, NX / 8.0) if width is None else width
+    mix, sp = mixing_layer_mc(mech, N=NX, NY=NY, NZ=NZ, Y_H2=Y_H2, T_lo=T_in, T_hi=T_hot, width=width,
+                              u_si=u_in_si, seed=seed, periodic_x=False)
+    Nx = mix.shape[0]
+    ns = len(sp)
+    mix["type"][0] = TYPE_I_C
+    mix["type"][Nx - 1] = TYPE_O_C
+    Xair = _mole_fractions(mech, {"O2": 0.233, "N2": 0.767})
+    for (ii, T, X) in ((0, T_in, Xair), (Nx - 1, None, None)):
+        if X is None:  # outflow ghost: the state next to it, pressure 1 atm
+            mix["temp"][ii] = mix["temp"][ii - 1]
+            mix["u"][ii] = mix["u"][ii - 1]
+            for a in range(ns):
+                sp[a]["X"][ii] = sp[a]["X"][ii - 1]
+        else:
+            mix["temp"][ii] = t_lattice(T)
+            mix["u"][ii] = u_lattice(u_in_si)
+            for a in range(ns):
+                sp[a]["X"][ii] = X[a]
+        mix["p"][ii] = p_lattice(ONE_ATM)
+    return mix, sp

@@ -64,7 +64,7 @@ class ThermoPhase {
         rho_ = rho;
         T_ = P * W_ / (rho * GasConstant);
     }
-    void setState_UV(double u, double v, double tol = 1e-4);
+    void setState_UV(double u, double v, double tol = 1e-9);  // Cantera 3.x default tolerance
     double cp_mass() const { return gas::cp_mass(*t_, Y_.data(), T_); }
     double cv_mass() const { return gas::cv_mass(*t_, Y_.data(), T_); }
     double intEnergy_mass() const { return gas::int_energy_mass(*t_, Y_.data(), T_); }

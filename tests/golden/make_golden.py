@@ -18,7 +18,13 @@ compiled unchanged -- on seeded inputs and records:
 * ``mc_mix8.npz``          8^3 periodic 9-species H2/air mixing layer (REACTION off), the
                            reference's multicomponent solver on the Cantera-API shim, fields
                            after 1 and 40 steps;
-* ``mc_react8.npz``        the same with REACTION on and an 1800 K hot slab, 30 steps.
+* ``mc_react8.npz``        the same with REACTION on and an 1800 K hot slab, 30 steps;
+* ``mc_chan.npz``          10x6x4 reacting H2-air channel: characteristic outflow ghosts
+                           (TYPE_O_C, NSCBC) at both x ends, TMS solid walls at y, periodic
+                           z, an ignition kernel at mid-x; fields after 1, 2 and 20 steps;
+* ``mc_inflow.npz``        10x6x6 mixing layer between a characteristic inflow (TYPE_I_C,
+                           inline LODI) and outflow (TYPE_O_C), periodic y and z, REACTION
+                           off; fields after 1, 2 and 20 steps.
 """
 import hashlib
 import os
@@ -202,6 +208,28 @@ def make_mc():
         out = run_ref_mc(mix, sp, m, cps, reaction, pc)
         out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
         np.savez_compressed(os.path.join(HERE, name), **out)
+    for name, mix_sp, reaction in (("mc_chan.npz", cases.flame_channel_mc(m, NX=10, NY=6, NZ=4), True),
+                                   ("mc_inflow.npz", cases.inflow_layer_mc(m, NX=10, NY=6, NZ=6), False)):
+        mix, sp = mix_sp
+        pc = boundary_cells(mix, 24, 4)
+        out = run_ref_mc(mix, sp, m, [1, 2, 20], reaction, pc)
+        out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
+        np.savez_compressed(os.path.join(HERE, name), **out)
+
+
+def boundary_cells(cells, n, seed):
+    """Fluid cells for the population records: those next to a non-periodic ghost first."""
+    t = cells["type"]
+    fl = np.argwhere(t == cases.TYPE_F)
+    near = []
+    for (i, j, k) in fl:
+        nb = t[i - 1:i + 2, j - 1:j + 2, k - 1:k + 2]
+        near.append(bool(np.any((nb != cases.TYPE_F) & (nb != cases.TYPE_P))))
+    near = np.array(near)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = fl[near][rng.permutation(int(near.sum()))][: n // 2 + n % 2]
+    b = fl[~near][rng.permutation(int((~near).sum()))][: n // 2]
+    return np.concatenate([a, b])
 
 
 if __name__ == "__main__":

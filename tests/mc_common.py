@@ -70,7 +70,7 @@ def soa_state(mix, sp):
     return rec
 
 
-def host_run(L, m, mix, sp, reaction, steps, precision="fp64", shift=True):
+def host_run(L, m, mix, sp, reaction, steps, precision="fp64", shift=True, pops=False):
     """Init + `steps` steps of the host build (populations in FP64 or, "fp32", in FP32);
     returns (record planes, status)."""
     dt = np.float64 if precision == "fp64" else np.float32
@@ -84,10 +84,13 @@ def host_run(L, m, mix, sp, reaction, steps, precision="fp64", shift=True):
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     args = [*mix.shape, P(typ), ctypes.byref(m), ctypes.c_float(W.FLAME_UNITS[0]),
             ctypes.c_float(W.FLAME_UNITS[1]), int(reaction), steps, P(pop0), P(pop1), P(rec0), P(rec1)]
+    fout = np.zeros((27 * (NS + 1), nc)) if pops else None
     if precision == "fp64":
         L.mc_host_run.restype = ctypes.c_int
-        cur = L.mc_host_run(*args, ctypes.byref(st))
+        cur = L.mc_host_run(*args, ctypes.byref(st), P(fout) if pops else None)
     else:
         L.mc_host_run32.restype = ctypes.c_int
         cur = L.mc_host_run32(*args, int(shift), ctypes.byref(st))
+    if pops:
+        return (rec0, rec1)[cur], st.value, fout
     return (rec0, rec1)[cur], st.value
