@@ -546,7 +546,7 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
         for (long n = n0; n < n1; ++n) {
             const char *srec = h->bounce + (n - n0) * ms;
             char *drec = hm + n * ms;
-            if (cf[n] == CF_FLUID) {
+            if (cf[n] & CF_FLUID) {
                 short t;
                 std::memcpy(&t, drec + h->mo.type, sizeof(short));
                 std::memcpy(drec, srec, ms);
@@ -558,7 +558,7 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
             for (int a = 0; a < h->ns; ++a) {
                 const char *ssrc = h->bounce + cnt * ms + ((size_t)a * cnt + (n - n0)) * ss;
                 char *sdst = static_cast<char *>(species[a]) + n * ss;
-                if (cf[n] == CF_FLUID)
+                if (cf[n] & CF_FLUID)
                     std::memcpy(sdst, ssrc, ss);
                 else
                     for (long o : sfld) std::memcpy(sdst + o, ssrc + o, sizeof(double));
