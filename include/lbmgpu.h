@@ -195,6 +195,20 @@ int lbmgpu_status(lbmgpu_t *h, uint32_t *flags, int clear);
 int lbmgpu_profile(lbmgpu_t *h, int enable);
 int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
 
+/* FP64 totals over the fluid cells of the current state (the last complete moments),
+ * no counterpart in the reference's API (its diagnostics reduce the AoS arrays on the
+ * host, OutputKeEns in src/output.cpp):
+ *   out[0] mass sum rho, out[1..3] momentum sum rho u, out[4] total energy (sum rhoE),
+ *   multicomponent also out[5 .. 5+ns-1] the species masses sum rho_a and
+ *   out[5+ns .. 5+ns+3] the element totals sum_a rho_a / W_a * (atoms of H, O, N, Ar),
+ * all in lattice units.  lbmgpu_sums_count gives the number of values (5, or
+ * 5 + n_species + 4); n_out must be at least that.  The reduction order is fixed, so
+ * the totals are reproducible bit for bit.  The first call allocates the handle's
+ * reduction scratch (LBMGPU_SUMS_MAX * 1185 doubles); the call waits for the stream. */
+#define LBMGPU_SUMS_MAX 21
+int lbmgpu_sums_count(const lbmgpu_t *h);
+int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
+
 /* Bytes of device memory held by the handle. */
 int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes);
 

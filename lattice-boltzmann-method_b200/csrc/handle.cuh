@@ -74,6 +74,7 @@ struct lbmgpu {
     float *pop32[2] = {nullptr, nullptr};
     float *bst32[2] = {nullptr, nullptr};
     double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
+    double *sum_scratch = nullptr;          // lbmgpu_sums: block partials and totals
     long nfluid = 0;
 };
 

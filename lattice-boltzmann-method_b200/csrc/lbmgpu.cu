@@ -541,6 +541,7 @@ int lbmgpu_destroy(lbmgpu_t *h) {
         cudaFree(h->bst[b]);
     }
     cudaFree(h->status);
+    cudaFree(h->sum_scratch);
     cudaFree(h->stage);
     if (h->bounce) cudaFreeHost(h->bounce);
     lbmh::mc_release(h);

@@ -36,8 +36,9 @@ EXPORTS = [
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
-    "lbmgpu_units_from_dx_dt",
+    "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums",
 ]
+SUMS_MAX = 21
 CHEM_OFF, CHEM_REF_EXPLICIT, CHEM_ROSENBROCK = 0, 1, 2
 ST_NEWTON, ST_CHEM = 0x8, 0x10
 
@@ -91,6 +92,8 @@ def lib():
         L.lbmgpu_kernel_times.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_long),
                                           ctypes.POINTER(ctypes.c_double)]
         L.lbmgpu_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
+        L.lbmgpu_sums_count.argtypes = [vp]
+        L.lbmgpu_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         L.lbmgpu_error_string.argtypes = [ctypes.c_int]
         L.lbmgpu_error_string.restype = ctypes.c_char_p
         _lib = L
@@ -236,6 +239,16 @@ class Lattice:
         ms = (ctypes.c_double * 3)()
         _check(lib().lbmgpu_kernel_times(self.h, 3, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
+
+    # -- conserved sums -------------------------------------------------------------------
+    def sums(self):
+        """FP64 totals over the fluid cells: mass, momentum (3), total energy, then
+        (multicomponent) the species masses and the H, O, N, Ar element totals."""
+        k = lib().lbmgpu_sums_count(self.h)
+        _check(k if k < 0 else 0, "lbmgpu_sums_count")
+        out = (ctypes.c_double * k)()
+        _check(lib().lbmgpu_sums(self.h, out, k), "lbmgpu_sums")
+        return list(out)
 
     def device_bytes(self):
         b = ctypes.c_size_t()
