@@ -209,6 +209,17 @@ int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
 int lbmgpu_sums_count(const lbmgpu_t *h);
 int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
 
+/* lbmgpu_sums without any device allocation, no counterpart in the reference: the
+ * reduction scratch is a fixed device array of the library (199,080 bytes per device)
+ * instead of handle memory, for callers that cannot allocate after setup (a lattice that
+ * fills the device, a monitoring loop that must not synchronise the device through
+ * cudaMalloc, a host whose pool owns all device memory).  Same values, bit for bit, as
+ * lbmgpu_sums.  n_out must lie in [lbmgpu_sums_count(h), LBMGPU_SUMS_MAX], else
+ * LBMGPU_E_ARG.  The scratch is shared by every handle on the device: calls that overlap
+ * on one device race, so serialise them.  The first call on a device resolves the
+ * scratch's address; make it before any stream capture begins. */
+int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
+
 /* Bytes of device memory held by the handle. */
 int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes);
 

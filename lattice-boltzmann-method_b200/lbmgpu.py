@@ -36,7 +36,7 @@ EXPORTS = [
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
-    "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums",
+    "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums", "lbmgpu_sums_noalloc",
 ]
 SUMS_MAX = 21
 CHEM_OFF, CHEM_REF_EXPLICIT, CHEM_ROSENBROCK = 0, 1, 2
@@ -94,6 +94,7 @@ def lib():
         L.lbmgpu_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_size_t)]
         L.lbmgpu_sums_count.argtypes = [vp]
         L.lbmgpu_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        L.lbmgpu_sums_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         L.lbmgpu_error_string.argtypes = [ctypes.c_int]
         L.lbmgpu_error_string.restype = ctypes.c_char_p
         _lib = L
@@ -249,6 +250,16 @@ class Lattice:
         out = (ctypes.c_double * k)()
         _check(lib().lbmgpu_sums(self.h, out, k), "lbmgpu_sums")
         return list(out)
+
+    def sums_noalloc(self, n_out=None):
+        """The same totals through lbmgpu_sums_noalloc (fixed device scratch, no
+        allocation); n_out defaults to the handle's count."""
+        k = lib().lbmgpu_sums_count(self.h)
+        _check(k if k < 0 else 0, "lbmgpu_sums_count")
+        n = k if n_out is None else n_out
+        out = (ctypes.c_double * max(n, 1))()
+        _check(lib().lbmgpu_sums_noalloc(self.h, out, n), "lbmgpu_sums_noalloc")
+        return list(out)[:k]
 
     def device_bytes(self):
         b = ctypes.c_size_t()
