@@ -2,22 +2,27 @@
 """Throughput of the D3Q27 thermal LBM time step on B200 (MLUPS and HBM GB/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload inflow|chan|mix|react|tgv] [--N n] [--precision fp64|fp32]
 
 One "step" is one full lattice time step of the workload (collide, stream, boundary,
-moments over every fluid cell).  Workload: config 1 -- the single-component thermal
-D3Q27 Taylor-Green vortex, 64^3 interior cells, FP64, Ma 0.1, Re 400 (seeded synthetic
-state, numpy PCG64 seed 20261203).  The state is larger than L2 (the two population
-buffers alone are 2 x 54 x 66^3 x 8 B = 248 MB), so no L2 flush is needed between steps.
+moments over every fluid cell).  Default workload: config 2 -- the non-reacting
+9-species H2/O2/N2 mixing layer, 128^3 interior cells, FP64, characteristic (NSCBC)
+inflow and outflow in x, periodic y and z, a seeded sinusoidal interface (Y_H2 0 -> 0.03,
+T 300 -> 1000 K, p = 1 atm), dx = 20 um, dt = 1 ns.  The state (about 5 GB in FP64) is far
+larger than L2, so no L2 flush is needed between steps.  --workload tgv is config 1 (the
+single-component Taylor-Green vortex, 64^3, FP64, Ma 0.1, Re 400); chan is config 3's
+reacting channel shape (NSCBC outlets, TMS walls); mix/react are periodic boxes.
 
 * value: MLUPS of K steps with the state resident in HBM, device-timed with CUDA events
   on the library's stream; max over ranks.
-* e2e: the same steps through the reference-facing phase calls of the C ABI
-  (collide/streaming/tms_bc/calculate_moment), with the AoS state uploaded from pinned
-  host memory at the start, and the whole AoS state plus the status word read back every
-  10 steps (the output cadence of the reference's Taylor-Green setup, setup.cpp:146);
-  host wall clock.
+* e2e: the same steps through the reference-facing calls of the C ABI: AoS upload and
+  Init from host memory, per step the five phase calls and a device->host read of the
+  step's result (multicomponent: the conserved totals of lbmgpu_sums; config 1: the
+  whole AoS state and the status word every 10 steps, the output cadence of the
+  reference's Taylor-Green setup, setup.cpp:146), host wall clock.
 * roofline: the dominant kernel's algorithmic bytes per launch / its mean launch time.
-* cpu_baseline: the reference's own solver (oracle/_ref) on the host cores, bounded sample.
+* cpu_baseline: the reference's own solver (oracle/_ref; multicomponent on the
+  Cantera-API shim) on the host cores, a bounded sample (a slab of the workload).
 
 Under torchrun (N > 1) every rank runs an independent replica of the workload on its own
 GPU (the path is not domain-decomposed yet): weak scaling, value = all ranks' cells.
@@ -37,7 +42,7 @@ for _p in (ROOT, PKG):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-METRIC = "MLUPS (D3Q27 thermal LBM step, 1 B200)"
+METRIC = "MLUPS & HBM GB/s, D3Q27 reacting, 1 B200; surrogate vs plain chem at ≤1% err"
 # algorithmic bytes per cell and launch (one read + one write of every population, plus
 # the moment record the stream kernel must store)
 BYTES_COLLIDE_FP64 = 2 * 54 * 8          # 864
@@ -49,11 +54,11 @@ OUTPUT_EVERY = 10
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=None, help="default 1000 (tgv) or 200 (multicomponent)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
-    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan"], default="tgv",
+    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan"], default="inflow",
                     help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
                          "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
@@ -250,8 +255,48 @@ def cpu_baseline(cells, prm, target_s=10.0):
 # ---------------------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------------------
+def run_reference_mc(args, dist):
+    """The reference's multicomponent solver (reference LBM + Cantera-API shim) on the
+    host cores, each step over a slab of the workload sized so that the whole
+    --steps/--warmup run takes about two minutes."""
+    threads = os.cpu_count() or 1
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    cross, m = mc_cpu_sample(args, budget, threads)
+    m, mix, sp = mc_workload(args, cross=cross)
+    ncell = fluid_cells(mix)
+    with stdout_to_stderr():
+        dt = mc_cpu_run(m, mix, sp, args.steps, args.warmup, threads, mc_reaction(args))
+    v = ncell * args.steps / dt / 1e6
+    shape = "x".join(str(s_ - 2) for s_ in mix.shape)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
+        "config": {"workload": mc_workload_name(args, ncell_shape=shape), "cells": ncell, "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": threads, "kind": "reference",
+                         "sample": f"{shape} slab of the {args.N}-cell-long workload, {args.steps} steps after "
+                                   f"{args.warmup} warm-up steps, reference multicomponent LBM + Cantera-API shim"},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def mc_workload_name(args, ncell_shape):
+    reaction = mc_reaction(args)
+    chem = ""
+    if reaction:
+        chem = "ROS2 stiff chemistry" if args.chem == "rosenbrock" else "reference explicit chemistry"
+    return (f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "")
+            + f": 9-species H2/O2/N2 D3Q27, {ncell_shape} {MC_SHAPES[args.workload]}, dx 20 um, dt 1 ns, "
+            + (chem if reaction else "non-reacting"))
+
+
 def run_reference(args, dist):
     if dist.rank != 0:
+        return
+    if args.workload != "tgv":
+        run_reference_mc(args, dist)
         return
     cells, prm = workload(args.N)
     threads = os.cpu_count() or 1
@@ -291,18 +336,44 @@ MC_SHAPES = {"mix": "periodic", "react": "periodic", "inflow": "TYPE_I_C inflow 
              "chan": "TYPE_O_C outflow at both x ends, TMS solid y walls, periodic z"}
 
 
-def mc_workload(args):
+def mc_workload(args, cross=None):
+    """The multicomponent workload; `cross` shrinks the two transverse axes (a slab of the
+    same case, for the bounded CPU samples)."""
     import mech
     import workloads
     m = mech.h2_air_9()
+    N = args.N
     if args.workload == "inflow":
-        mix, sp = workloads.inflow_layer_mc(m, NX=args.N, NY=args.N, NZ=args.N)
+        c = cross or N
+        mix, sp = workloads.inflow_layer_mc(m, NX=N, NY=c, NZ=c)
     elif args.workload == "chan":
-        mix, sp = workloads.flame_channel_mc(m, NX=2 * args.N, NY=args.N // 2, NZ=args.N // 2)
+        c = cross or N // 2
+        mix, sp = workloads.flame_channel_mc(m, NX=2 * N, NY=c, NZ=c)
     else:
+        c = cross or N
         kw = {"T_hi": 1800.0} if args.workload == "react" else {}
-        mix, sp = workloads.mixing_layer_mc(m, N=args.N, **kw)
+        mix, sp = workloads.mixing_layer_mc(m, N=N, NY=c, NZ=c, **kw)
     return m, mix, sp
+
+
+def mc_reaction(args):
+    return args.workload in ("react", "chan")
+
+
+def mc_cpu_sample(args, budget_s, threads):
+    """The reference's multicomponent solver on a slab of the workload (full extent along
+    x, the transverse axes shrunk so that one step takes about budget_s): returns
+    (slab cells, seconds per step measured over `steps`, description)."""
+    m, mix, sp = mc_workload(args, cross=8)
+    reaction = mc_reaction(args)
+    with stdout_to_stderr():
+        t8 = mc_cpu_run(m, mix, sp, 1, 1, threads, reaction)
+    rate = fluid_cells(mix) / max(t8, 1e-6)  # cells per second
+    nx = mix.shape[0] - 2
+    cross = int(max(4, min(args.N, (rate * budget_s / nx) ** 0.5)))
+    if args.workload == "chan":
+        cross = min(cross, args.N // 2)
+    return cross, m
 
 
 def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
@@ -331,7 +402,7 @@ def run_ours_mc(args, dist):
     import lbmgpu
     import workloads
     device = dist.local
-    reaction = args.workload in ("react", "chan")
+    reaction = mc_reaction(args)
     m, mix, sp = mc_workload(args)
     ncell = fluid_cells(mix)
     chem = lbmgpu.CHEM_OFF
@@ -368,8 +439,10 @@ def run_ours_mc(args, dist):
     peak, peak_kind = peaks()
     achieved = alg / (avg[dom] * 1e-3) / 1e9
 
-    # end to end: upload, Init, phase calls, one AoS download (the reference's flame
-    # setups write output every 1000 steps, setup.cpp:2852)
+    # end to end through the reference-facing calls: AoS upload + Init from host memory,
+    # the five phase calls per step with the step's conserved totals read back
+    # (lbmgpu_sums), one AoS download at the end (the reference's flame setups write
+    # output every 1000 steps, setup.cpp:2852); host wall clock
     hm = mix.copy()
     hs = [a.copy() for a in sp]
     lat = lattice()
@@ -383,14 +456,17 @@ def run_ours_mc(args, dist):
         lat.streaming()
         lat.tms_bc()
         lat.calculate_moment()
+        tot = lat.sums()
     lat.synchronize()
     lat.download(hm, hs)
     wall = dist.max(time.perf_counter() - t0)
     lat.close()
     nbytes = mix.nbytes + sum(a.nbytes for a in sp)
     e2e = {"value": dist.world * ncell * args.steps / wall / 1e6, "unit": "MLUPS",
-           "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
-           "note": "AoS upload + Init, phase calls per step, one AoS download"}
+           "h2d_bytes_per_step": nbytes / args.steps,
+           "d2h_bytes_per_step": nbytes / args.steps + 8 * len(tot),
+           "note": "AoS upload + Init, per step the five phase calls and the conserved totals read back, "
+                   "one AoS download"}
     if dist.rank != 0:
         return
     value = dist.world * ncell * args.steps / (ms * 1e-3) / 1e6
@@ -398,10 +474,8 @@ def run_ours_mc(args, dist):
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded sinusoidal H2/air interface, numpy PCG64 seed 20261203)",
-        "config": {"workload": f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "") + f": 9-species H2/O2/N2 D3Q27, {'x'.join(str(s_ - 2) for s_ in mix.shape)} {MC_SHAPES[args.workload]}, "
-                               f"dx 20 um, dt 1 ns, " + (("ROS2 stiff chemistry" if args.chem == "rosenbrock" else
-                                                          "reference explicit chemistry") if reaction else "non-reacting"),
+        "data": "synthetic (seeded H2/air cases of the reference's flame setups, numpy PCG64 seed 20261203)",
+        "config": {"workload": mc_workload_name(args, "x".join(str(s_ - 2) for s_ in mix.shape)),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
                    "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
         "hbm_gbs_step": ncell * (mc_bytes("k_mc_collide", pop_bytes, reaction) + mc_bytes("k_mc_stream", pop_bytes))
@@ -415,12 +489,15 @@ def run_ours_mc(args, dist):
     if dist.world == 1 and not args.no_cpu_baseline:
         try:
             threads = os.cpu_count() or 1
-            n = 3
+            n = 5
+            cross, _ = mc_cpu_sample(args, 3.0, threads)
+            m2, mix2, sp2 = mc_workload(args, cross=cross)
             with stdout_to_stderr():
-                dt = mc_cpu_run(m, mix, sp, n, 1, threads, reaction)
-            line["cpu_baseline"] = {"value": ncell * n / dt / 1e6, "unit": "MLUPS", "cores": threads,
+                dt = mc_cpu_run(m2, mix2, sp2, n, 1, threads, reaction)
+            line["cpu_baseline"] = {"value": fluid_cells(mix2) * n / dt / 1e6, "unit": "MLUPS", "cores": threads,
                                     "kind": "reference",
-                                    "sample": f"{n} steps after 1 warm-up step, reference multicomponent LBM + "
+                                    "sample": f"{'x'.join(str(s_ - 2) for s_ in mix2.shape)} slab of the workload, "
+                                              f"{n} steps after 1 warm-up step, reference multicomponent LBM + "
                                               f"Cantera-API shim, {threads} OpenMP threads, {dt:.1f} s"}
         except Exception as exc:
             line["cpu_baseline"] = {"value": None, "error": str(exc)}
@@ -536,6 +613,8 @@ def main():
     args = parse()
     if args.N is None:
         args.N = 64 if args.workload == "tgv" else 128
+    if args.steps is None:
+        args.steps = 1000 if args.workload == "tgv" else 200
     dist = Dist()
     try:
         if args.impl == "reference":
