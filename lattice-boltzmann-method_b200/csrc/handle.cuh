@@ -15,7 +15,9 @@ namespace lbmh {
 constexpr int kBlock = 128;
 
 enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SPECIES = 4 };
-enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_NKINDS = 3 };
+// per-kernel timing classes; multicomponent: K_COLLIDE is the population update
+// (k_mc_relax) and K_PROPS the collision parameters (k_mc_props)
+enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_NKINDS = 4 };
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.
 enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
@@ -61,8 +63,8 @@ struct lbmgpu {
     int phase = lbmh::PH_BOUNDARY;
     bool prof = false;
     std::vector<lbmh::EvPair> pending, pool;
-    long launches[lbmh::K_NKINDS] = {0, 0, 0};
-    double ms[lbmh::K_NKINDS] = {0, 0, 0};
+    long launches[lbmh::K_NKINDS] = {};
+    double ms[lbmh::K_NKINDS] = {};
     size_t bytes = 0;
     // multicomponent
     int ns = 0;
@@ -75,6 +77,7 @@ struct lbmgpu {
     float *bst32[2] = {nullptr, nullptr};
     double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
     double *sum_scratch = nullptr;          // lbmgpu_sums: block partials and totals
+    double *props = nullptr;                // multicomponent collision parameters
     long nfluid = 0;
 };
 

@@ -31,11 +31,25 @@ using namespace lbmh;
 
 constexpr int NS9 = 9;
 
-template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_collide(McArgsT<S, double> A) {
+// collision parameters of every fluid cell, one instance per chemistry mode
+template <int NS, int CHEM, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
-    mc_collide_cell<NS>(A, n);
+    mc_props_cell<NS, CHEM>(A, n);
+}
+
+// BGK update: blockIdx.y selects the population set (species 0..NS-1, NS = energy), the
+// x dimension the cells, so a warp reads one set's planes at 32 consecutive cells
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_relax(McArgsT<S, double> A) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
+    const int a = blockIdx.y;
+    if (a < NS)
+        mc_relax_species<NS>(A, n, a);
+    else
+        mc_relax_energy<NS>(A, n);
 }
 
 // the cells with a boundary upstream, one thread each (compact list)
@@ -234,6 +248,7 @@ McArgsT<S, double> base_args(lbmgpu *h) {
     A.shift = h->fp32 ? h->shift[0] : nullptr;
     A.bid = h->bid;
     A.nb = h->nb;
+    A.props = h->props;
     return A;
 }
 
@@ -348,9 +363,20 @@ int collide_t(lbmgpu *h) {
     A.local = local ? 1 : 0;
     A.bst_cur = bstb<S>(h, c);
     EvPair ep{};
-    ev_begin(h, K_COLLIDE, ep);
-    k_mc_collide<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
+    ev_begin(h, K_PROPS, ep);
+    const unsigned gp = grid_for(h->g.ncell);
+    if (h->chem == CHEM_REF_EXPLICIT)
+        k_mc_props<NS9, CHEM_REF_EXPLICIT, S><<<gp, kBlock, 0, h->stream>>>(A);
+    else if (h->chem == CHEM_ROSENBROCK)
+        k_mc_props<NS9, CHEM_ROSENBROCK, S><<<gp, kBlock, 0, h->stream>>>(A);
+    else
+        k_mc_props<NS9, CHEM_OFF, S><<<gp, kBlock, 0, h->stream>>>(A);
     ev_end(h, ep);
+    CK(cudaGetLastError());
+    EvPair er{};
+    ev_begin(h, K_COLLIDE, er);
+    k_mc_relax<NS9, S><<<dim3(grid_for(h->g.ncell), NS9 + 1), kBlock, 0, h->stream>>>(A);
+    ev_end(h, er);
     CK(cudaGetLastError());
     return 0;
 }
@@ -400,6 +426,10 @@ int mc_setup(lbmgpu *h) {
         if (rc) return rc;
         rc = dalloc(h, &h->mom[b], (size_t)h->nrec * nc);
         if (rc) return rc;
+        if (b == 0) {
+            rc = dalloc(h, &h->props, (size_t)pr_count<NS9>() * nc);
+            if (rc) return rc;
+        }
         // the face-difference planes of cells the kernels never write (ghosts) are read
         // but not used, and the ghosts' populations are never read; zero them all so they
         // hold no stale bits
@@ -427,6 +457,8 @@ int mc_setup(lbmgpu *h) {
 void mc_release(lbmgpu *h) {
     if (h->tab) cudaFree(h->tab);
     h->tab = nullptr;
+    cudaFree(h->props);
+    h->props = nullptr;
     for (int b = 0; b < 2; ++b) {
         cudaFree(h->pop32[b]);
         cudaFree(h->bst32[b]);

@@ -75,6 +75,7 @@ struct McArgsT {
     const P *bst_cur;      // of the current step (collide, and the stale directions)
     P *bst_nxt;            // written by the special-cell stream kernel
     long nb;
+    double *props;         // collision parameters per cell (mc_props_cell -> mc_relax_*)
 };
 using McArgs = McArgsT<double, double>;
 
@@ -352,12 +353,30 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 
 // ------------------------------------------------------------------------------------
 // Collision: species (LBM::Collide_Species, src/lbm-collision.cpp:334-526) and energy
-// (LBM::Collide, src/lbm-collision.cpp:191-332) of one fluid cell, fused.
+// (LBM::Collide, src/lbm-collision.cpp:191-332), in two parts:
+//   mc_props_cell    per cell: chemistry, transport, relaxation rates, the Maxwell-Stefan
+//                    velocity shift and the energy-flux correction -> the props planes;
+//   mc_relax_species per (cell, species) and mc_relax_energy per cell: the BGK update of
+//                    the 27 populations of one set from the props planes.
+// Props planes (FP64, per cell): om_a (NS), F_a,d (3 NS), drho_a (NS), omega, omega_1,
+// theta, U, dq_d (3).
 // ------------------------------------------------------------------------------------
-template <int NS, class AT>
-MC_HDN void mc_collide_cell(const AT &A, long n) {
+template <int NS> MC_HD constexpr int pr_om(int a) { return a; }
+template <int NS> MC_HD constexpr int pr_f(int a, int d) { return NS + 3 * a + d; }
+template <int NS> MC_HD constexpr int pr_drho(int a) { return 4 * NS + a; }
+template <int NS> MC_HD constexpr int pr_omm() { return 5 * NS; }
+template <int NS> MC_HD constexpr int pr_om1() { return 5 * NS + 1; }
+template <int NS> MC_HD constexpr int pr_theta() { return 5 * NS + 2; }
+template <int NS> MC_HD constexpr int pr_uint() { return 5 * NS + 3; }
+template <int NS> MC_HD constexpr int pr_dq(int d) { return 5 * NS + 4 + d; }
+template <int NS> MC_HD constexpr int pr_count() { return 5 * NS + 7; }
+
+template <int NS, int CHEM, class AT>
+MC_HDN void mc_props_cell(const AT &A, long n) {
     const gas::Tables &t = *A.tab;
     const typename AT::R *Rc = A.rec_cur;
+    double *Pr = A.props;
+    auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
     const double rho = rec(A, Rc, RM_RHO, n);
     const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
     const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n), rhoe = rec(A, Rc, RM_RHOE, n);
@@ -382,9 +401,9 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         Uint = Uint - 0.5 * rho_a[a] / rho * (ua[a][0] * ua[a][0] + ua[a][1] * ua[a][1] + ua[a][2] * ua[a][2]);
 
     // -- chemistry: two explicit half steps with T from (u, v) in between (lbm-collision.cpp:370-399)
-    double drho[NS];
-    for (int a = 0; a < NS; ++a) drho[a] = 0.0;
-    if (A.chem == CHEM_REF_EXPLICIT) {
+    if (CHEM == CHEM_REF_EXPLICIT) {
+        double drho[NS];
+        for (int a = 0; a < NS; ++a) drho[a] = 0.0;
         double Tc = T_si, rc = rho_si, Yc[NS], Xc[NS];
         for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
         for (int sub = 0; sub < 2; ++sub) {
@@ -403,10 +422,12 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
             Tc = Tn;
         }
         double hrr = 0.0;
-        for (int a = 0; a < NS; ++a)
+        for (int a = 0; a < NS; ++a) {
             hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
+            prp(pr_drho<NS>(a), drho[a]);
+        }
         put(A, A.rec_nxt, RM_HRR, n, hrr);
-    } else if (A.chem == CHEM_ROSENBROCK) {
+    } else if (CHEM == CHEM_ROSENBROCK) {
         // stiff alternative: the constant-(rho, e) reactor over the whole lattice step with
         // ROS2 (chem.cuh); the density change and the heat release enter the collision the
         // same way as the reference's explicit increments
@@ -416,24 +437,41 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
             atomic_status(A.status, LBMGPU_ST_CHEM);
         double hrr = 0.0;
         for (int a = 0; a < NS; ++a) {
-            drho[a] = rho * (Yc[a] - Y[a]);
-            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
+            const double dr = rho * (Yc[a] - Y[a]);
+            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * dr;
+            prp(pr_drho<NS>(a), dr);
         }
         put(A, A.rec_nxt, RM_HRR, n, hrr);
     }
 
-    // -- species viscosities, Wilke weights, relaxation rates (lbm-collision.cpp:402-430)
+    // -- species viscosities; Wilke weights phi_ab = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^1/4)^2 /
+    // sqrt(8 (1 + W_a/W_b)) formed for b >= a and mirrored, phi_ba = mu_b/mu_a W_a/W_b phi_ab
+    // (lbm-collision.cpp:402-430).  Each weight enters the two row sums the reference forms
+    // with it -- sum_b Xs_b phi_ab for the species rates, sum_b X_b phi_ab for the mixture
+    // viscosity -- pair by pair; every row still receives its terms in the order b = 0..NS-1.
     const double xT = gas::lnT_x(T_si);
     double mu_k[NS];
     for (int a = 0; a < NS; ++a) mu_k[a] = gas::species_visc_x(t, a, xT);
-    double phi[gas::MAXS][gas::MAXS];
-    gas::wilke_phi(t, mu_k, phi);
-    double om_a[NS];
+    double den_s[NS], den_m[NS];
+    for (int a = 0; a < NS; ++a) den_s[a] = den_m[a] = 0.0;
+    for (int a = 0; a < NS; ++a)
+        for (int b = a; b < NS; ++b) {
+            const double f1 = 1.0 + sqrt(mu_k[a] / mu_k[b]) * t.sqrt4W[a][b];
+            const double pab = f1 * f1 / t.wilke_den[a][b];
+            const double pba = mu_k[b] / mu_k[a] * t.m.W[a] / t.m.W[b] * pab;
+            if (b == a) {
+                den_s[a] = den_s[a] + Xs[a] * pba;
+                den_m[a] += X[a] * pba;
+            } else {
+                den_s[a] = den_s[a] + Xs[b] * pab;
+                den_m[a] += X[b] * pab;
+                den_s[b] = den_s[b] + Xs[a] * pba;
+                den_m[b] += X[a] * pba;
+            }
+        }
     for (int a = 0; a < NS; ++a) {
-        double denom = 0.0;
-        for (int b = 0; b < NS; ++b) denom = denom + Xs[b] * phi[a][b];
-        const double visc = Xs[a] * (double)u_mu(A.U, (float)mu_k[a]) / denom;
-        om_a[a] = 2 * Xs[a] * p * dt / (Xs[a] * p * dt + 2 * visc);
+        const double visc = Xs[a] * (double)u_mu(A.U, (float)mu_k[a]) / den_s[a];
+        prp(pr_om<NS>(a), 2 * Xs[a] * p * dt / (Xs[a] * p * dt + 2 * visc));
     }
 
     // -- Maxwell-Stefan force (lbm-collision.cpp:433-471); the diagonal term vanishes
@@ -449,9 +487,9 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
             }
         }
     for (int a = 0; a < NS; ++a)
-        for (int d = 0; d < 3; ++d) F[a][d] = F[a][d] * dt / rho_a[a];
+        for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * dt / rho_a[a]);
 
-    // -- neighbours along each axis
+    // -- energy collision parameters (lbm-collision.cpp:231-316)
     long nbl[3], nbh[3];
     int tl[3], th[3];
     for (int d = 0; d < 3; ++d) {
@@ -461,66 +499,11 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         tl[d] = A.type[nbl[d]];
         th[d] = A.type[nbh[d]];
     }
-    McPull pp;
-    const bool special = !A.local && (A.cflag[n] & CF_SPECIAL);
-    const long bs = special ? (long)A.bid[n] : 0;
-    if (!A.local && !special) mc_pull(A, n, pp);
-    // the cell's populations after streaming and boundary treatment
-    auto fetch = [&](int plane, int l) {
-        if (A.local) return ldpop(A, A.pop_src, plane, n);
-        if (special) return ldpop_b(A, A.bst_cur, plane, bs);
-        return ldpop(A, A.pop_src, plane, pull_idx(pp, l));
-    };
-
-    // -- species collision (lbm-collision.cpp:446-519)
-    for (int a = 0; a < NS; ++a) {
-        double fv[27];
-#pragma unroll
-        for (int l = 0; l < 27; ++l) fv[l] = fetch(27 * a + l, l);
-        // bare species velocity sum f c / rho_a (lbm-collision.cpp:446-454)
-        double ux[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int l = 0; l < 27; ++l) {
-            ux[0] += fv[l] * cx(l);
-            ux[1] += fv[l] * cy(l);
-            ux[2] += fv[l] * cz(l);
-        }
-        for (int d = 0; d < 3; ++d) ux[d] = ux[d] / rho_a[a];
-        const double Ra = t.Ra_lat[a];
-        const double theta = Ra * Tl;
-        double corr[3];
-        for (int d = 0; d < 3; ++d) {
-            const int pq = rs(a, RS_QX + d);
-            const double Qc = rho_a[a] * ua[a][d] * (1.0 - 3.0 * Ra * Tl) - rho_a[a] * (ua[a][d] * ua[a][d] * ua[a][d]);
-            const double dQ = mc_fd_central(rec(A, Rc, pq, nbl[d]), Qc, rec(A, Rc, pq, nbh[d]), tl[d], th[d]);
-            corr[d] = dt * (2.0 - om_a[a]) / (2.0 * rho_a[a] * om_a[a]) * dQ;
-        }
-        AxisF<double> Fe, Fd, Fr;
-        axis_feq(Fe, ux, theta, corr);
-        const double udu[3] = {ux[0] + F[a][0], ux[1] + F[a][1], ux[2] + F[a][2]};
-        axis_feq(Fd, udu, theta, corr);
-        const double zero[3] = {0.0, 0.0, 0.0};
-        axis_feq(Fr, um, theta, zero);
-        const double om = om_a[a];
-        const bool skip_all = rho_a[a] <= kSpeciesMin && A.chem == CHEM_OFF;
-#pragma unroll
-        for (int l = 0; l < 27; ++l) {
-            const int plane = 27 * a + l;
-            const double fr = A.chem != CHEM_OFF ? feq_l(l, drho[a], Fr) : 0.0;
-            if (skip_all || (rho_a[a] <= kSpeciesMin && fr <= 0.0)) {
-                if (!A.local) A.pop_dst[(long)plane * A.ncell + n] = A.pop_prev[(long)plane * A.ncell + n];
-                continue;
-            }
-            const double fe = feq_l(l, rho_a[a], Fe);
-            const double fd = feq_l(l, rho_a[a], Fd);
-            stpop(A, A.pop_dst, plane, n, fv[l] + om * (fe - fv[l]) + (fd - fe) + fr);
-        }
-    }
-
-    // -- energy collision (lbm-collision.cpp:231-324)
+    double mu = 0.0;  // Wilke mixture viscosity sum_k X_k mu_k / sum_j X_j phi_kj
+    for (int k = 0; k < NS; ++k) mu += X[k] * mu_k[k] / den_m[k];
     const double cp = u_cp(A.U, (float)gas::cp_mass(t, Y, T_si));
     const double gasconstant = u_cp(A.U, (float)(gas::kR / W));
-    const double mu = u_mu(A.U, (float)gas::wilke_from_phi(t, X, mu_k, phi));
+    mu = u_mu(A.U, (float)mu);
     const double lam = u_cond(A.U, (float)gas::mix_cond(t, X, T_si, P_si, mu_k));
     const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
     const double om1 = 2 * p * cp * dt / (p * cp * dt + 2 * lam);
@@ -544,16 +527,108 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
     double P6[6];
     for (int q = 0; q < 6; ++q) P6[q] = rec(A, Rc, RM_P00 + q, n);
     const double Pf[3][3] = {{P6[0], P6[1], P6[2]}, {P6[1], P6[3], P6[4]}, {P6[2], P6[4], P6[5]}};
-    double dq[3];
     for (int d = 0; d < 3; ++d) {
         const double Qc = rho * um[d] * (1.0 - 3.0 * gasconstant * Tl) - rho * (um[d] * um[d] * um[d]);
         const double dQ = mc_fd_central(rec(A, Rc, RM_QX + d, nbl[d]), Qc, rec(A, Rc, RM_QX + d, nbh[d]), tl[d], th[d]);
         double s = 0.0;
         for (int b = 0; b < 3; ++b) s += um[b] * (Pf[b][d] - ((b == d ? p : 0.0) + rho * um[b] * um[d]));
-        dq[d] = s + qd[d] + qc[d] + 0.5 * dt * um[d] * dQ;
+        prp(pr_dq<NS>(d), s + qd[d] + qc[d] + 0.5 * dt * um[d] * dQ);
     }
+    prp(pr_omm<NS>(), om);
+    prp(pr_om1<NS>(), om1);
+    prp(pr_theta<NS>(), theta);
+    prp(pr_uint<NS>(), Uint);
+}
+
+// The cell's populations of one set after streaming and boundary treatment: in place
+// (local mode), from the special-cell store, or pulled from the upstream cells.
+template <class AT>
+struct McFetch {
+    const AT &A;
+    long n, b;
+    bool special;
+    McPull pp;
+    MC_HD McFetch(const AT &A_, long n_) : A(A_), n(n_), b(0), special(false) {
+        special = !A.local && (A.cflag[n] & CF_SPECIAL);
+        if (special) b = (long)A.bid[n];
+        if (!A.local && !special) mc_pull(A, n, pp);
+    }
+    MC_HD double operator()(int plane, int l) const {
+        if (A.local) return ldpop(A, A.pop_src, plane, n);
+        if (special) return ldpop_b(A, A.bst_cur, plane, b);
+        return ldpop(A, A.pop_src, plane, pull_idx(pp, l));
+    }
+};
+
+// BGK update of species a at cell n (lbm-collision.cpp:446-519).
+template <int NS, class AT>
+MC_HDN void mc_relax_species(const AT &A, long n, int a) {
+    const gas::Tables &t = *A.tab;
+    const typename AT::R *Rc = A.rec_cur;
+    const double *Pr = A.props;
+    auto prg = [&](int plane) { return Pr[(long)plane * A.ncell + n]; };
+    const double rho_a = rec(A, Rc, rs(a, RS_RHO), n);
+    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
+    const double Tl = rec(A, Rc, RM_T, n);
+    const double om = prg(pr_om<NS>(a));
+    const double dt = A.dt;
+    const McFetch<AT> fetch(A, n);
+    double fv[27];
+#pragma unroll
+    for (int l = 0; l < 27; ++l) fv[l] = fetch(27 * a + l, l);
+    // bare species velocity sum f c / rho_a (lbm-collision.cpp:446-454)
+    double ux[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        ux[0] += fv[l] * cx(l);
+        ux[1] += fv[l] * cy(l);
+        ux[2] += fv[l] * cz(l);
+    }
+    for (int d = 0; d < 3; ++d) ux[d] = ux[d] / rho_a;
+    const double theta = t.Ra_lat[a] * Tl;
+    double corr[3];
+    for (int d = 0; d < 3; ++d) {  // FD of the face terms the stream kernel stored (lbm-collision.cpp:487-497)
+        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
+        const int pq = rs(a, RS_QX + d);
+        const double dQ = mc_fd_central(rec(A, Rc, pq, n - off), rec(A, Rc, pq, n), rec(A, Rc, pq, n + off),
+                                        A.type[n - off], A.type[n + off]);
+        corr[d] = dt * (2.0 - om) / (2.0 * rho_a * om) * dQ;
+    }
+    AxisF<double> Fe, Fd, Fr;
+    axis_feq(Fe, ux, theta, corr);
+    const double udu[3] = {ux[0] + prg(pr_f<NS>(a, 0)), ux[1] + prg(pr_f<NS>(a, 1)), ux[2] + prg(pr_f<NS>(a, 2))};
+    axis_feq(Fd, udu, theta, corr);
+    const double zero[3] = {0.0, 0.0, 0.0};
+    axis_feq(Fr, um, theta, zero);
+    const double drho = A.chem != CHEM_OFF ? prg(pr_drho<NS>(a)) : 0.0;
+    const bool skip_all = rho_a <= kSpeciesMin && A.chem == CHEM_OFF;
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        const int plane = 27 * a + l;
+        const double fr = A.chem != CHEM_OFF ? feq_l(l, drho, Fr) : 0.0;
+        if (skip_all || (rho_a <= kSpeciesMin && fr <= 0.0)) {
+            if (!A.local) A.pop_dst[(long)plane * A.ncell + n] = A.pop_prev[(long)plane * A.ncell + n];
+            continue;
+        }
+        const double fe = feq_l(l, rho_a, Fe);
+        const double fd = feq_l(l, rho_a, Fd);
+        stpop(A, A.pop_dst, plane, n, fv[l] + om * (fe - fv[l]) + (fd - fe) + fr);
+    }
+}
+
+// Update of the energy populations at cell n (lbm-collision.cpp:317-324).
+template <int NS, class AT>
+MC_HDN void mc_relax_energy(const AT &A, long n) {
+    const typename AT::R *Rc = A.rec_cur;
+    const double *Pr = A.props;
+    auto prg = [&](int plane) { return Pr[(long)plane * A.ncell + n]; };
+    const double rho = rec(A, Rc, RM_RHO, n);
+    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
+    const double om = prg(pr_omm<NS>()), om1 = prg(pr_om1<NS>());
+    const double dq[3] = {prg(pr_dq<NS>(0)), prg(pr_dq<NS>(1)), prg(pr_dq<NS>(2))};
     AxisG<double> G;
-    axis_geq(G, Uint, theta, um);
+    axis_geq(G, prg(pr_uint<NS>()), prg(pr_theta<NS>()), um);
+    const McFetch<AT> fetch(A, n);
     double gv[27];
 #pragma unroll
     for (int l = 0; l < 27; ++l) gv[l] = fetch(27 * NS + l, l);
@@ -563,6 +638,19 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         const double gs = (csq(l) == 1) ? gq + 0.5 * (cx(l) * dq[0] + cy(l) * dq[1] + cz(l) * dq[2]) : gq;
         stpop(A, A.pop_dst, 27 * NS + l, n, gv[l] + om1 * (gq - gv[l]) + (om - om1) * (gq - gs));
     }
+}
+
+// The whole collision of one cell (host build and tests): props, then every set.
+template <int NS, class AT>
+MC_HDN void mc_collide_cell(const AT &A, long n) {
+    if (A.chem == CHEM_REF_EXPLICIT)
+        mc_props_cell<NS, CHEM_REF_EXPLICIT>(A, n);
+    else if (A.chem == CHEM_ROSENBROCK)
+        mc_props_cell<NS, CHEM_ROSENBROCK>(A, n);
+    else
+        mc_props_cell<NS, CHEM_OFF>(A, n);
+    for (int a = 0; a < NS; ++a) mc_relax_species<NS>(A, n, a);
+    mc_relax_energy<NS>(A, n);
 }
 
 // ------------------------------------------------------------------------------------

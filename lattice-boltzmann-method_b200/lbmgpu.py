@@ -236,9 +236,11 @@ class Lattice:
         _check(lib().lbmgpu_profile(self.h, int(enable)), "lbmgpu_profile")
 
     def kernel_times(self):
-        launches = (ctypes.c_long * 3)()
-        ms = (ctypes.c_double * 3)()
-        _check(lib().lbmgpu_kernel_times(self.h, 3, launches, ms), "lbmgpu_kernel_times")
+        """Per kernel kind (0 collide / population update, 1 stream+boundary+moment,
+        2 other, 3 multicomponent collision parameters): launches and device ms."""
+        launches = (ctypes.c_long * 4)()
+        ms = (ctypes.c_double * 4)()
+        _check(lib().lbmgpu_kernel_times(self.h, 4, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------

@@ -59,6 +59,8 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
     A.cflag = cf.data();
     A.bid = bid.data();
     A.nb = (long)blist.size();
+    std::vector<double> props((size_t)pr_count<9>() * A.ncell);
+    A.props = props.data();
     for (long n = 0; n < A.ncell; ++n) mc_init_cell<9>(A, n, rec0, rec1, pop0);
     const int np = 27 * 10;
     std::vector<double> sh(np, 0.0);
