@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
 // BGK update: blockIdx.y selects the population set (species 0..NS-1, NS = energy), the
 // x dimension the cells, so a warp reads one set's planes at 32 consecutive cells
 template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_relax(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, 4) k_mc_relax(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     const int a = blockIdx.y;

@@ -481,9 +481,11 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
     for (int a = 0; a < NS; ++a)
         for (int b = 0; b < a; ++b) {
             const double D = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            // the reference's -p X_a X_b / D_ab, once per ordered pair
+            const double kab = -1.0 * p * Xs[a] * Xs[b] / D, kba = -1.0 * p * Xs[b] * Xs[a] / D;
             for (int d = 0; d < 3; ++d) {
-                F[a][d] += -1.0 * p * Xs[a] * Xs[b] / D * (ua[a][d] - ua[b][d]);
-                F[b][d] += -1.0 * p * Xs[b] * Xs[a] / D * (ua[b][d] - ua[a][d]);
+                F[a][d] += kab * (ua[a][d] - ua[b][d]);
+                F[b][d] += kba * (ua[b][d] - ua[a][d]);
             }
         }
     for (int a = 0; a < NS; ++a)
@@ -541,22 +543,42 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
 }
 
 // The cell's populations of one set after streaming and boundary treatment: in place
-// (local mode), from the special-cell store, or pulled from the upstream cells.
+// (local mode), from the special-cell store, or pulled from the upstream cells.  The
+// mode is resolved once into a base pointer, a plane stride and a per-axis offset table,
+// so the 27 loads are branch-free and issue back to back.
 template <class AT>
 struct McFetch {
-    const AT &A;
-    long n, b;
-    bool special;
-    McPull pp;
-    MC_HD McFetch(const AT &A_, long n_) : A(A_), n(n_), b(0), special(false) {
-        special = !A.local && (A.cflag[n] & CF_SPECIAL);
-        if (special) b = (long)A.bid[n];
-        if (!A.local && !special) mc_pull(A, n, pp);
+    using P = typename AT::P;
+    const P *src;
+    long stride;
+    int X[3], Y[3], Z[3];
+    const double *shift;
+    MC_HD McFetch(const AT &A, long n) : shift(A.shift) {
+        const bool special = !A.local && (A.cflag[n] & CF_SPECIAL);
+        if (A.local || special) {
+            const int base = special ? A.bid[n] : (int)n;
+            src = special ? A.bst_cur : A.pop_src;
+            stride = special ? A.nb : A.ncell;
+            for (int c = 0; c < 3; ++c) {
+                X[c] = base;
+                Y[c] = 0;
+                Z[c] = 0;
+            }
+        } else {
+            McPull pp;
+            mc_pull(A, n, pp);
+            src = A.pop_src;
+            stride = A.ncell;
+            for (int c = 0; c < 3; ++c) {
+                X[c] = (int)pp.X[c];
+                Y[c] = (int)pp.Y[c];
+                Z[c] = (int)pp.Z[c];
+            }
+        }
     }
     MC_HD double operator()(int plane, int l) const {
-        if (A.local) return ldpop(A, A.pop_src, plane, n);
-        if (special) return ldpop_b(A, A.bst_cur, plane, b);
-        return ldpop(A, A.pop_src, plane, pull_idx(pp, l));
+        const double v = (double)src[(long)plane * stride + (X[cidx(cx(l))] + Y[cidx(cy(l))] + Z[cidx(cz(l))])];
+        return shift ? v + shift[plane] : v;
     }
 };
 
