@@ -174,14 +174,17 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+def ncu_traffic(kernel, cells):
+    """DRAM bytes of one launch of `kernel` over `cells` fluid cells, scaled from the
+    committed ncu capture (profiles/ncu_traffic.txt: bytes of one captured launch and the
+    cells it processed; the traffic of these kernels grows in proportion to the cells),
+    or None."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     try:
         for line in open(p):
             parts = line.split()
-            if len(parts) >= 3 and parts[0] == "traffic_bytes_per_launch" and parts[1] == kernel:
-                return float(parts[2])
+            if len(parts) >= 5 and parts[0] == "traffic" and parts[1] == kernel and parts[3] == "cells":
+                return float(parts[2]) / float(parts[4]) * cells
     except OSError:
         pass
     return None
@@ -488,7 +491,7 @@ def run_ours_mc(args, dist):
         "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_stream", "k_mc_props"))
         / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic(dom), "peak_source": f"{peak_kind} hbm_gbs",
+                     "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell), "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": alg, "mean_launch_ms": avg[dom], "kernel_ms": avg},
         "gpu_launches": int(round(sum(launches) / kk * args.steps)),
         "status": status, "clocks": clocks, "e2e": e2e,
@@ -599,7 +602,7 @@ def run_ours(args, dist):
                    "l2": "state larger than L2 (248 MB of populations), no flush"},
         "hbm_gbs_step": ncell * BYTES_STEP_FP64 / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic(dom),
+                     "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell),
                      "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_launch": alg,
                      "mean_launch_ms": avg[dom], "kernel_ms": avg},
         "gpu_launches": int(round(per_step_launches * args.steps)),

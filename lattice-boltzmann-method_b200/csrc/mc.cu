@@ -398,7 +398,7 @@ int stream_t(lbmgpu *h) {
         A.bst_nxt = bstb<S>(h, x);
         EvPair eb{};
         ev_begin(h, K_OTHER, eb);
-        k_mc_special<NS9, S><<<grid_for(h->nb), kBlock, 0, h->stream>>>(A, h->blist);
+        k_mc_special<NS9, S><<<(unsigned)((h->nb + 31) / 32), 32, 0, h->stream>>>(A, h->blist);
         ev_end(h, eb);
         CK(cudaGetLastError());
     }
