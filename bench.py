@@ -330,13 +330,14 @@ def mc_bytes(kernel, pop_bytes, reaction=False):
                    the parameters om_a, F_a (3) [, drho_a]; shared u (3), T, rho; the
                    energy set's 7 parameters -> 9 * (4 + 4) + 5 + 7 = 84 planes [+ 9]
       k_mc_stream: 21 record planes read (rho, T, p, rho_a, X_a) + 88 written
-      k_mc_props : 58 record planes of the cell + 40 read once by its neighbours, 52
-                   parameter planes written [+ HRR]"""
+      k_mc_props : 58 record planes of the cell + 40 read once by its neighbours, 88
+                   parameter planes written (52 + the 36 D_ab) [+ HRR]
+      (k_mc_stream also reads the 36 D_ab planes)"""
     if kernel == "k_mc_relax":
         return 2 * 270 * pop_bytes + (84 + (9 if reaction else 0)) * 8
     if kernel == "k_mc_props":
-        return (58 + 40 + 52 + (1 if reaction else 0)) * 8
-    return 270 * pop_bytes + (21 + 88) * 8
+        return (58 + 40 + 88 + (1 if reaction else 0)) * 8
+    return 270 * pop_bytes + (21 + 36 + 88) * 8
 
 
 

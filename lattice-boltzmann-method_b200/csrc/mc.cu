@@ -72,7 +72,7 @@ __global__ void k_mc_fill_bst(long ncell, long nb, int np, const long *__restric
 }
 
 template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_stream(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, 3) k_mc_stream(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
     mc_stream_moment_cell<NS>(A, n);

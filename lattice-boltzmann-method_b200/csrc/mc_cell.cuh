@@ -205,6 +205,21 @@ MC_HD void store_face_terms(const AT &A, typename AT::R *R, long n, int ty, doub
     }
 }
 
+// Collision parameter planes (written by mc_props_cell, below).
+template <int NS> MC_HD constexpr int pr_om(int a) { return a; }
+template <int NS> MC_HD constexpr int pr_f(int a, int d) { return NS + 3 * a + d; }
+template <int NS> MC_HD constexpr int pr_drho(int a) { return 4 * NS + a; }
+template <int NS> MC_HD constexpr int pr_omm() { return 5 * NS; }
+template <int NS> MC_HD constexpr int pr_om1() { return 5 * NS + 1; }
+template <int NS> MC_HD constexpr int pr_theta() { return 5 * NS + 2; }
+template <int NS> MC_HD constexpr int pr_uint() { return 5 * NS + 3; }
+template <int NS> MC_HD constexpr int pr_dq(int d) { return 5 * NS + 4 + d; }
+// the lattice binary diffusion coefficients D_ab (b < a) at the record's state: the
+// collision uses them for the Maxwell-Stefan shift, and the stream kernel that follows
+// for its Stefan-Maxwell matrix -- both evaluate them at the same (T, p, composition)
+template <int NS> MC_HD constexpr int pr_d(int a, int b) { return 5 * NS + 7 + a * (a - 1) / 2 + b; }
+template <int NS> MC_HD constexpr int pr_count() { return 5 * NS + 7 + NS * (NS - 1) / 2; }
+
 // ------------------------------------------------------------------------------------
 // Moments (the multicomponent LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one
 // fluid cell from its streamed populations; pop(a, l) returns population l of species a
@@ -213,14 +228,9 @@ MC_HD void store_face_terms(const AT &A, typename AT::R *R, long n, int ty, doub
 template <int NS, class AT, class Pop>
 MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     const gas::Tables &t = *A.tab;
-    // -- old state, as the reference's Cantera object is set at the start (lbm-moment.cpp:219-221)
-    double Yo_raw[NS], Yo[NS], Xo[NS];
-    const double rho_old = rec(A, A.rec_cur, RM_RHO, n);
-    for (int a = 0; a < NS; ++a) Yo_raw[a] = rec(A, A.rec_cur, rs(a, RS_RHO), n) / rho_old;
-    const double Wold = set_mass_fractions<NS>(t, Yo_raw, Yo, Xo);
+    // -- old temperature, where the reference's Newton iteration starts (lbm-moment.cpp:219-221);
+    // the old state's diffusion coefficients come from the collision parameters
     const double T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
-    const double rho_si = si_rho(A.U, (float)rho_old);
-    const double P_si = rho_si * gas::kR * T_si / Wold;
 
     // -- sums per species and of g
     double rho_a[NS], j_a[NS][3];
@@ -262,16 +272,16 @@ MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     }
     const double u = ru / rho, v = rv / rho, w = rw / rho;
 
-    // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky
+    // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky, with
+    // the D_ab the collision of this step evaluated at the same old state (T, p, Y)
     double M[NS][NS];
     const double p_old = rec(A, A.rec_cur, RM_P, n);
-    const double xT = gas::lnT_x(T_si);
     double Xold[NS];
     for (int a = 0; a < NS; ++a) Xold[a] = rec(A, A.rec_cur, rs(a, RS_X), n);
     for (int a = 0; a < NS; ++a) {
         M[a][a] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
         for (int b = 0; b < a; ++b) {  // D_ab of the reference's lower triangle, one per pair
-            const double D = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            const double D = A.props[(long)pr_d<NS>(a, b) * A.ncell + n];
             M[a][b] = -1.0 * A.dt / 2.0 * p_old * Xold[a] * Xold[b] / D;
             M[b][a] = -1.0 * A.dt / 2.0 * p_old * Xold[b] * Xold[a] / D;
         }
@@ -359,17 +369,8 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 //   mc_relax_species per (cell, species) and mc_relax_energy per cell: the BGK update of
 //                    the 27 populations of one set from the props planes.
 // Props planes (FP64, per cell): om_a (NS), F_a,d (3 NS), drho_a (NS), omega, omega_1,
-// theta, U, dq_d (3).
+// theta, U, dq_d (3), D_ab (NS (NS-1) / 2).
 // ------------------------------------------------------------------------------------
-template <int NS> MC_HD constexpr int pr_om(int a) { return a; }
-template <int NS> MC_HD constexpr int pr_f(int a, int d) { return NS + 3 * a + d; }
-template <int NS> MC_HD constexpr int pr_drho(int a) { return 4 * NS + a; }
-template <int NS> MC_HD constexpr int pr_omm() { return 5 * NS; }
-template <int NS> MC_HD constexpr int pr_om1() { return 5 * NS + 1; }
-template <int NS> MC_HD constexpr int pr_theta() { return 5 * NS + 2; }
-template <int NS> MC_HD constexpr int pr_uint() { return 5 * NS + 3; }
-template <int NS> MC_HD constexpr int pr_dq(int d) { return 5 * NS + 4 + d; }
-template <int NS> MC_HD constexpr int pr_count() { return 5 * NS + 7; }
 
 template <int NS, int CHEM, class AT>
 MC_HDN void mc_props_cell(const AT &A, long n) {
@@ -481,6 +482,7 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
     for (int a = 0; a < NS; ++a)
         for (int b = 0; b < a; ++b) {
             const double D = u_nu(A.U, (float)gas::binary_diff_x(t, a, b, xT, P_si));
+            prp(pr_d<NS>(a, b), D);
             // the reference's -p X_a X_b / D_ab, once per ordered pair
             const double kab = -1.0 * p * Xs[a] * Xs[b] / D, kba = -1.0 * p * Xs[b] * Xs[a] / D;
             for (int d = 0; d < 3; ++d) {
