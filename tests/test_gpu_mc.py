@@ -181,3 +181,34 @@ def test_gpu_mc_rejects_noncharacteristic_open_types():
         with lattice(m, bad, False) as lat:
             with pytest.raises(lbmgpu.LbmGpuError):
                 lat.upload(bad, sp)
+
+
+@pytest.mark.parametrize("fixture", ["mc_chan.npz", "mc_inflow.npz"])
+def test_gpu_mc_fp32_storage_with_boundaries(fixture):
+    """FP32 population storage with characteristic inflow/outflow and TMS walls (the
+    boundary cells' kept populations are stored in float too) against the FP64 mode after
+    20 steps: 1e-5 relative for rho, T, p, rhoE, 1e-4 of the largest velocity, 1e-5
+    absolute for every Y_k."""
+    from test_mc_host import bc_case
+    m, mix, sp, reaction = bc_case(fixture)
+    res = {}
+    for prec in (lbmgpu.FP64, lbmgpu.FP32):
+        with lbmgpu.Lattice(*mix.shape, mech=m, dtype=W.MIXTURE_MC, species_dtype=W.SPECIES, dx_dt=W.FLAME_UNITS,
+                            chem=lbmgpu.CHEM_REF_EXPLICIT if reaction else lbmgpu.CHEM_OFF, precision=prec) as lat:
+            lat.upload(mix, sp)
+            lat.init()
+            lat.step(20)
+            assert lat.synchronize() == 0
+            c = mix.copy()
+            s = [a.copy() for a in sp]
+            lat.download(c, s)
+            res[prec] = (c, s)
+    (c64, s64), (c32, s32) = res[lbmgpu.FP64], res[lbmgpu.FP32]
+    fl = mix["type"] == 0
+    for k in ("rho", "temp", "p", "rhoe"):
+        assert rel(c32[k][fl], c64[k][fl]) < 1e-5, k
+    vs = max(np.abs(c64[k][fl]).max() for k in "uvw")
+    for k in "uvw":
+        assert rel(c32[k][fl], c64[k][fl], vs) < 1e-4, k
+    for a in range(NS):
+        assert np.abs(s64[a]["rho"][fl] / c64["rho"][fl] - s32[a]["rho"][fl] / c32["rho"][fl]).max() < 1e-5, a
