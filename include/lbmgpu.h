@@ -221,6 +221,54 @@ int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
  * scratch's address; make it before any stream capture begins. */
 int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
 
+/* ---- chemistry surrogate (LBMGPU_CHEM_ROSENBROCK handles) --------------------------
+ * No counterpart in the reference.  A small network learns the stiff integrator's step
+ *   (T [K], ln p [Pa], Y_0..Y_8, dt [s])  ->  (dY_0..dY_8, dT [K])
+ * (12 -> 128 -> 128 -> 128 -> 10, GELU, BF16 weights and activations, FP32 accumulation,
+ * standardised inputs and outputs) from samples the integrator writes during the run,
+ * then replaces it cell by cell: the predicted dY is projected onto changes that conserve
+ * every element, cells whose features leave the training box (widened by 5 %) or whose
+ * prediction is not finite run the integrator, and 1 in audit_period cells (0: none) runs
+ * it as well, takes its result and scores the prediction (L1 error of dY).
+ *
+ * lbmgpu_surrogate_collect: while enabled, each step's integrator writes the features and
+ *   targets of every stride-th cell (a different subset each step) to a device sample set
+ *   of `capacity` rows; collection stops when it is full.
+ * lbmgpu_surrogate_load_samples: replaces the sample set by n host rows (x: n x 12 raw
+ *   features, y: n x 10 raw targets).
+ * lbmgpu_surrogate_train: Adam (beta 0.9/0.999) on the mean squared standardised error,
+ *   `epochs` passes over the samples in shuffled minibatches of `batch` (a multiple of 64)
+ *   rows; the standardisation and gate box are fitted on the first call or with refit;
+ *   *loss = the last epoch's mean loss.
+ * lbmgpu_surrogate_enable: the surrogate on (after training) or off; resets the audit
+ *   counters of lbmgpu_surrogate_stats.
+ * lbmgpu_surrogate_eval: the network on n host rows of raw features (x: n x 12) ->
+ *   raw predictions (y: n x 10), before projection.
+ * lbmgpu_surrogate_params: get (set = 0) or set the parameters, packed as W1 [128][12],
+ *   b1 [128], W2 [128][128], b2, W3 [128][128], b3, W4 [10][128], b4 [10], then x_mean,
+ *   x_std, x_lo, x_hi [12 each], y_mean, y_std [10 each] (LBMGPU_SUR_NPARAMS floats);
+ *   setting resets Adam and marks the surrogate trained. */
+#define LBMGPU_SUR_NPARAMS 36046
+typedef struct lbmgpu_surrogate_report {
+    long samples;             /* rows in the sample set                                   */
+    long train_steps;         /* Adam steps so far                                        */
+    double last_loss;         /* last epoch's mean standardised squared error             */
+    long cells_predicted;     /* cell updates taken from the network                      */
+    long cells_integrated;    /* cell updates the gate sent to the integrator             */
+    long cells_audited;       /* cell updates integrated to score the network             */
+    double audit_rel_err;     /* over the audited cells: sum |dY_net - dY_int|_1 / sum |dY_int|_1 */
+    double audit_max_abs_err; /* largest |dY_net - dY_int|_1 of an audited cell           */
+    double audit_dY;          /* sum |dY_int|_1 over the audited cells                   */
+    int enabled, collecting;
+} lbmgpu_surrogate_report;
+int lbmgpu_surrogate_collect(lbmgpu_t *h, int enable, int stride, long capacity);
+int lbmgpu_surrogate_load_samples(lbmgpu_t *h, const float *x, const float *y, long n);
+int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigned seed, int refit, double *loss);
+int lbmgpu_surrogate_enable(lbmgpu_t *h, int enable, int audit_period);
+int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y);
+int lbmgpu_surrogate_params(lbmgpu_t *h, float *buf, long n, int set);
+int lbmgpu_surrogate_stats(lbmgpu_t *h, lbmgpu_surrogate_report *out);
+
 /* Bytes of device memory held by the handle. */
 int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes);
 

@@ -12,6 +12,7 @@
 
 namespace lbmh {
 
+struct SurState;  // chemistry surrogate (surrogate.cu)
 constexpr int kBlock = 128;
 
 enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SPECIES = 4 };
@@ -78,6 +79,7 @@ struct lbmgpu {
     double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
     double *sum_scratch = nullptr;          // lbmgpu_sums: block partials and totals
     double *props = nullptr;                // multicomponent collision parameters
+    lbmh::SurState *sur = nullptr;          // chemistry surrogate, created on first use
     long nfluid = 0;
 };
 

@@ -23,6 +23,7 @@
 #include "handle.cuh"
 #include "mc_bc.cuh"
 #include "mc_cell.cuh"
+#include "surrogate_host.cuh"
 
 namespace {
 
@@ -362,6 +363,8 @@ int collide_t(lbmgpu *h) {
     A.rec_nxt = h->mom[x];
     A.local = local ? 1 : 0;
     A.bst_cur = bstb<S>(h, c);
+    const int rs_ = sur_prepare_t<S>(h, A);
+    if (rs_) return rs_;
     EvPair ep{};
     ev_begin(h, K_PROPS, ep);
     const unsigned gp = grid_for(h->g.ncell);
@@ -455,6 +458,7 @@ int mc_setup(lbmgpu *h) {
 }
 
 void mc_release(lbmgpu *h) {
+    sur_release(h);
     if (h->tab) cudaFree(h->tab);
     h->tab = nullptr;
     cudaFree(h->props);
@@ -618,6 +622,7 @@ int mc_launch_stream(lbmgpu *h) {
     if (rc) return rc;
     h->cur = 1 - h->cur;
     h->pack_mode = PK_STEPPED;
+    sur_after_step(h);
     return 0;
 }
 

@@ -25,6 +25,7 @@
 
 #include "d3q27.cuh"
 #include "chem.cuh"
+#include "surrogate.cuh"
 #include "gas.cuh"
 #include "units.cuh"
 
@@ -76,6 +77,7 @@ struct McArgsT {
     P *bst_nxt;            // written by the special-cell stream kernel
     long nb;
     double *props;         // collision parameters per cell (mc_props_cell -> mc_relax_*)
+    SurArgs sur;           // chemistry surrogate (LBMGPU_CHEM_ROSENBROCK only)
 };
 using McArgs = McArgsT<double, double>;
 
@@ -105,6 +107,26 @@ MC_HD double ldpop_b(const AT &A, const T *p, int plane, long b) {
 template <class AT, typename T>
 MC_HD void stpop_b(const AT &A, T *p, int plane, long b, double v) {
     p[(long)plane * A.nb + b] = (T)(A.shift ? v - A.shift[plane] : v);
+}
+
+// Adds `flag` (0 or 1) to a counter; on the device one atomic per warp.
+MC_HD void count_flag(double *c, bool flag) {
+#if defined(__CUDA_ARCH__)
+    const unsigned act = __activemask();
+    const unsigned votes = __ballot_sync(act, flag);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && votes) atomicAdd(c, (double)__popc(votes));
+#else
+    *c += flag ? 1.0 : 0.0;
+#endif
+}
+MC_HD void add_max(double *sum, double *mx, double v) {
+#if defined(__CUDA_ARCH__)
+    atomicAdd(sum, v);
+    atomicMax(reinterpret_cast<unsigned long long *>(mx), (unsigned long long)__double_as_longlong(v));
+#else
+    *sum += v;
+    if (v > *mx) *mx = v;
+#endif
 }
 
 MC_HD void atomic_status(unsigned *s, unsigned bits) {
@@ -432,10 +454,66 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         // stiff alternative: the constant-(rho, e) reactor over the whole lattice step with
         // ROS2 (chem.cuh); the density change and the heat release enter the collision the
         // same way as the reference's explicit increments
-        double Yc[gas::MAXS], Tc = T_si;
-        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
-        if (gas::ros2_advance(t, rho_si, Yc, Tc, (double)dt * (double)A.U.s) < 0)
-            atomic_status(A.status, LBMGPU_ST_CHEM);
+        //
+        // With the surrogate on (sur.mode 1) the network's dY, dT replace the integrator,
+        // projected onto changes that conserve every element exactly; cells outside the
+        // training box, non-finite predictions and the audited cells run the integrator
+        // (the audited ones also score the prediction against it).  Teacher steps can
+        // write (features, targets) samples for training.
+        const SurArgs &S = A.sur;
+        const double dt_si = (double)dt * (double)A.U.s;
+        double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
+        bool have_pred = false;
+        if (S.mode == 1 && !S.gate[n]) {
+            const float *pr = S.pred + n * kSurOutPad;
+            double dY[NS];
+            have_pred = isfinite(pr[NS]);
+            for (int a = 0; a < NS; ++a) {
+                dY[a] = (double)pr[a];
+                have_pred = have_pred && isfinite(dY[a]);
+            }
+            for (int a = 0; a < NS; ++a) {
+                double sp = 0.0;
+                for (int b = 0; b < NS; ++b) sp += S.proj[a * NS + b] * dY[b];
+                Yp[a] = Y[a] + sp;
+            }
+            Tp = T_si + (double)pr[NS];
+        }
+        const bool audit = have_pred && S.audit_period > 0 && sur_hash((unsigned)n, S.step) % S.audit_period == 0;
+        if (!have_pred || audit) {
+            for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+            if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
+        } else {
+            for (int a = 0; a < NS; ++a) Yc[a] = Yp[a];
+            Tc = Tp;
+        }
+        if (S.mode == 1) {
+            if (audit) {  // L1 error of the predicted dY and L1 size of the integrator's dY
+                double num = 0.0, den = 0.0;
+                for (int a = 0; a < NS; ++a) {
+                    num += fabs(Yp[a] - Yc[a]);
+                    den += fabs(Yc[a] - Y[a]);
+                }
+                add_max(&S.audit[0], &S.audit[2], num);
+#if defined(__CUDA_ARCH__)
+                atomicAdd(&S.audit[1], den);
+#else
+                S.audit[1] += den;
+#endif
+            }
+            count_flag(&S.audit[3], audit);
+            count_flag(&S.audit[4], have_pred && !audit);
+            count_flag(&S.audit[5], !have_pred);
+        }
+        if (S.ds_x && !have_pred && (long)(n % S.ds_stride) == S.ds_phase) {
+            const long row = S.ds_base + n / S.ds_stride;
+            if (row < S.ds_cap) {
+                sur_features<NS>(T_si, P_si, Y, dt_si, S.ds_x + row * kSurIn);
+                for (int a = 0; a < NS; ++a) S.ds_y[row * kSurOut + a] = (float)(Yc[a] - Y[a]);
+                S.ds_y[row * kSurOut + NS] = (float)(Tc - T_si);
+                S.ds_valid[row] = 1;
+            }
+        }
         double hrr = 0.0;
         for (int a = 0; a < NS; ++a) {
             const double dr = rho * (Yc[a] - Y[a]);

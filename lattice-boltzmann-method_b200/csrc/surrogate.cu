@@ -1,0 +1,1020 @@
+// Chemistry surrogate: network kernels, training and the C entry points.
+//
+// No counterpart in the reference (whose chemistry is Cantera's explicit rates): an MLP
+// that learns the stiff ROS2 integrator's step (T, ln p, Y_k, dt) -> (dY_k, dT) from
+// samples the integrator itself writes while the run proceeds (mc_cell.cuh, teacher
+// steps), then stands in for it with an input-box gate, an element-conserving projection
+// and an audited sample (mc_cell.cuh, mode 1).
+//
+// Tensor-core kernels, BF16 operands with FP32 accumulation (mma.sync m16n8k16):
+//   k_sur_mlp   the whole network for a batch of cells in one kernel: the weights are
+//               staged once per block in shared memory, each warp carries 16 cells through
+//               the four layers with the activations in registers (the accumulator
+//               fragment of one layer is the operand fragment of the next);
+//   k_gemm_tn   C = A B^T for training (forward, input gradients, weight gradients);
+//   elementwise bias/GELU forward and backward, the MSE loss gradient, column sums for
+//   the bias gradients, Adam on FP32 master weights with BF16 copies.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "handle.cuh"
+#include "mc_cell.cuh"
+#include "surrogate_host.cuh"
+
+namespace lbmh {
+
+using namespace lbm;
+
+namespace {
+
+constexpr int kSurBlock = 128;                 // 4 warps, 16 cells each per tile
+constexpr int kW1 = kSurHid * kSurInPad;       // elements of the padded weight tensors
+constexpr int kW2 = kSurHid * kSurLd;
+constexpr int kW4 = kSurOutPad * kSurLd;
+constexpr int kNParams = kW1 + 2 * kW2 + kW4 + 3 * kSurHid + kSurOutPad;
+
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const unsigned *>(&v);
+}
+
+__host__ __device__ inline float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ inline float gelu_grad(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// -------------------------------------------------------------------------------------
+// Inference: features of every cell, then the fused network.
+// -------------------------------------------------------------------------------------
+template <int NS, typename S>
+__global__ void k_sur_features(McArgsT<S, double> A, const SurNorm *__restrict__ nrm, __nv_bfloat16 *__restrict__ X,
+                               uint8_t *__restrict__ gate, long mpad) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= mpad) return;
+    float x[kSurInPad] = {};
+    bool out_of_box = true;
+    if (n < A.ncell && (A.cflag[n] & CF_FLUID)) {
+        const gas::Tables &t = *A.tab;
+        const double rho = rec(A, A.rec_cur, RM_RHO, n);
+        double Yr[NS], Y[NS], Xm[NS];
+        for (int a = 0; a < NS; ++a) Yr[a] = rec(A, A.rec_cur, rs(a, RS_RHO), n) / rho;
+        const double W = set_mass_fractions<NS>(t, Yr, Y, Xm);
+        const double T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
+        const double rho_si = si_rho(A.U, (float)rho);
+        const double P_si = rho_si * gas::kR * T_si / W;
+        sur_features<NS>(T_si, P_si, Y, (double)A.dt * (double)A.U.s, x);
+        out_of_box = false;
+        for (int q = 0; q < kSurIn; ++q) {
+            const float w = nrm->x_hi[q] - nrm->x_lo[q];
+            if (w > 0.f && (x[q] < nrm->x_lo[q] - 0.05f * w || x[q] > nrm->x_hi[q] + 0.05f * w)) out_of_box = true;
+            x[q] = (x[q] - nrm->x_mean[q]) / nrm->x_std[q];
+        }
+    }
+    for (int q = 0; q < kSurInPad; ++q) X[n * kSurInPad + q] = __float2bfloat16(x[q]);
+    if (n < A.ncell) gate[n] = out_of_box ? 1 : 0;
+}
+
+// Raw features (rows of kSurIn floats) -> standardised BF16 rows.
+__global__ void k_sur_standardise(const float *__restrict__ x, long m, long mpad, const SurNorm *__restrict__ nrm,
+                                  __nv_bfloat16 *__restrict__ X) {
+    const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= mpad) return;
+    for (int q = 0; q < kSurInPad; ++q) {
+        float v = 0.f;
+        if (r < m && q < kSurIn) v = (x[r * kSurIn + q] - nrm->x_mean[q]) / nrm->x_std[q];
+        X[r * kSurInPad + q] = __float2bfloat16(v);
+    }
+}
+
+struct SurNet {  // device pointers of the BF16 weights and FP32 biases
+    const __nv_bfloat16 *w1, *w2, *w3, *w4;
+    const float *b1, *b2, *b3, *b4;
+};
+
+// One layer of the fused network for a warp's 16 rows: acc[16 n-tiles][4] = A W^T + b,
+// with A given as fragments of NK k-slices and W (row stride LD) in shared memory.
+template <int NK, int NT, int LD>
+__device__ __forceinline__ void mlp_layer(const unsigned (*afr)[4], const __nv_bfloat16 *W, const float *b,
+                                          float (*acc)[4], int gid, int tig) {
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+        const float b0 = b[8 * j + 2 * tig], b1 = b[8 * j + 2 * tig + 1];
+        acc[j][0] = b0;
+        acc[j][1] = b1;
+        acc[j][2] = b0;
+        acc[j][3] = b1;
+    }
+#pragma unroll
+    for (int s = 0; s < NK; ++s)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+            const __nv_bfloat16 *wr = W + (8 * j + gid) * LD + 16 * s + 2 * tig;
+            const unsigned b0 = *reinterpret_cast<const unsigned *>(wr);
+            const unsigned b1 = *reinterpret_cast<const unsigned *>(wr + 8);
+            mma_bf16(acc[j], afr[s], b0, b1);
+        }
+}
+
+// GELU of a 16 x 128 accumulator and its repacking as the next layer's operand fragments:
+// the accumulator of n-tiles 2s and 2s+1 is exactly the operand fragment of k-slice s.
+__device__ __forceinline__ void gelu_to_frag(const float (*acc)[4], unsigned (*afr)[4]) {
+#pragma unroll
+    for (int s = 0; s < kSurHid / 16; ++s) {
+        afr[s][0] = pack_bf16(gelu_f(acc[2 * s][0]), gelu_f(acc[2 * s][1]));
+        afr[s][1] = pack_bf16(gelu_f(acc[2 * s][2]), gelu_f(acc[2 * s][3]));
+        afr[s][2] = pack_bf16(gelu_f(acc[2 * s + 1][0]), gelu_f(acc[2 * s + 1][1]));
+        afr[s][3] = pack_bf16(gelu_f(acc[2 * s + 1][2]), gelu_f(acc[2 * s + 1][3]));
+    }
+}
+
+// X [mpad][16] standardised BF16 -> pred [mpad][16] in SI units (outputs 10..15 zero).
+__global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm *__restrict__ nrm,
+                                                       const __nv_bfloat16 *__restrict__ X, float *__restrict__ pred,
+                                                       long ntiles) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16 *w1 = reinterpret_cast<__nv_bfloat16 *>(smem);
+    __nv_bfloat16 *w2 = w1 + kW1;
+    __nv_bfloat16 *w3 = w2 + kW2;
+    __nv_bfloat16 *w4 = w3 + kW2;
+    float *bb = reinterpret_cast<float *>(w4 + kW4);  // b1 b2 b3 (128 each), b4 (16), y_mean, y_std
+    {
+        const unsigned *src[4] = {reinterpret_cast<const unsigned *>(net.w1), reinterpret_cast<const unsigned *>(net.w2),
+                                  reinterpret_cast<const unsigned *>(net.w3), reinterpret_cast<const unsigned *>(net.w4)};
+        unsigned *dst[4] = {reinterpret_cast<unsigned *>(w1), reinterpret_cast<unsigned *>(w2),
+                            reinterpret_cast<unsigned *>(w3), reinterpret_cast<unsigned *>(w4)};
+        const int cnt[4] = {kW1 / 2, kW2 / 2, kW2 / 2, kW4 / 2};
+        for (int t = 0; t < 4; ++t)
+            for (int i = threadIdx.x; i < cnt[t]; i += kSurBlock) dst[t][i] = src[t][i];
+        for (int i = threadIdx.x; i < kSurHid; i += kSurBlock) {
+            bb[i] = net.b1[i];
+            bb[kSurHid + i] = net.b2[i];
+            bb[2 * kSurHid + i] = net.b3[i];
+        }
+        if (threadIdx.x < kSurOutPad) {
+            bb[3 * kSurHid + threadIdx.x] = net.b4[threadIdx.x];
+            bb[3 * kSurHid + kSurOutPad + threadIdx.x] = nrm->y_mean[threadIdx.x];
+            bb[3 * kSurHid + 2 * kSurOutPad + threadIdx.x] = nrm->y_std[threadIdx.x];
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const float *ym = bb + 3 * kSurHid + kSurOutPad, *ys = ym + kSurOutPad;
+    for (long tile = (long)blockIdx.x * 4 + warp; tile < ntiles; tile += (long)gridDim.x * 4) {
+        const long r0 = tile * 16;
+        unsigned a1[1][4];
+        {
+            const __nv_bfloat16 *xr = X + (r0 + gid) * kSurInPad + 2 * tig;
+            a1[0][0] = *reinterpret_cast<const unsigned *>(xr);
+            a1[0][1] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInPad);
+            a1[0][2] = *reinterpret_cast<const unsigned *>(xr + 8);
+            a1[0][3] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInPad + 8);
+        }
+        float acc[kSurHid / 8][4];
+        unsigned afr[kSurHid / 16][4];
+        mlp_layer<1, kSurHid / 8, kSurInPad>(a1, w1, bb, acc, gid, tig);
+        gelu_to_frag(acc, afr);
+        mlp_layer<kSurHid / 16, kSurHid / 8, kSurLd>(afr, w2, bb + kSurHid, acc, gid, tig);
+        gelu_to_frag(acc, afr);
+        mlp_layer<kSurHid / 16, kSurHid / 8, kSurLd>(afr, w3, bb + 2 * kSurHid, acc, gid, tig);
+        gelu_to_frag(acc, afr);
+        float out[kSurOutPad / 8][4];
+        mlp_layer<kSurHid / 16, kSurOutPad / 8, kSurLd>(afr, w4, bb + 3 * kSurHid, out, gid, tig);
+#pragma unroll
+        for (int j = 0; j < kSurOutPad / 8; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = 8 * j + 2 * tig;
+                const long r = r0 + gid + 8 * h;
+                pred[r * kSurOutPad + c] = out[j][2 * h] * ys[c] + ym[c];
+                pred[r * kSurOutPad + c + 1] = out[j][2 * h + 1] * ys[c + 1] + ym[c + 1];
+            }
+    }
+}
+
+constexpr size_t kMlpSmem = (size_t)(kW1 + 2 * kW2 + kW4) * 2 + (size_t)(3 * kSurHid + 3 * kSurOutPad) * 4;
+
+// -------------------------------------------------------------------------------------
+// Training kernels.
+// -------------------------------------------------------------------------------------
+// C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T, A and B BF16 row-major with leading dimensions
+// lda, ldb (even), K a multiple of 16.  Block: 4 warps, each 16 rows x 64 columns.
+__global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict__ Am, int lda,
+                                                 const __nv_bfloat16 *__restrict__ Bm, int ldb, float *__restrict__ C,
+                                                 int ldc, int M, int N, int K) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    const int r0 = blockIdx.y * 64 + warp * 16, n0 = blockIdx.x * 64;
+    float acc[8][4] = {};
+    auto lda32 = [&](int r, int k) -> unsigned {
+        return r < M ? *reinterpret_cast<const unsigned *>(Am + (long)r * lda + k) : 0u;
+    };
+    auto ldb32 = [&](int n, int k) -> unsigned {
+        return n < N ? *reinterpret_cast<const unsigned *>(Bm + (long)n * ldb + k) : 0u;
+    };
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        unsigned a[4];
+        a[0] = lda32(r0 + gid, k0 + 2 * tig);
+        a[1] = lda32(r0 + gid + 8, k0 + 2 * tig);
+        a[2] = lda32(r0 + gid, k0 + 8 + 2 * tig);
+        a[3] = lda32(r0 + gid + 8, k0 + 8 + 2 * tig);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int nn = n0 + 8 * j + gid;
+            mma_bf16(acc[j], a, ldb32(nn, k0 + 2 * tig), ldb32(nn, k0 + 8 + 2 * tig));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int r = r0 + gid + 8 * h, c = n0 + 8 * j + 2 * tig;
+            if (r < M && c < N) C[(long)r * ldc + c] = acc[j][2 * h];
+            if (r < M && c + 1 < N) C[(long)r * ldc + c + 1] = acc[j][2 * h + 1];
+        }
+}
+
+// Z = C + b; H = GELU(Z) in BF16 (rows of width W).
+__global__ void k_bias_gelu(const float *__restrict__ C, const float *__restrict__ b, float *__restrict__ Z,
+                            __nv_bfloat16 *__restrict__ H, long rows, int W) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * W) return;
+    const float z = C[i] + b[i % W];
+    Z[i] = z;
+    H[i] = __float2bfloat16(gelu_f(z));
+}
+
+// Output layer: out = C + b4; dOut = 2 (out - y) / (valid * kSurOut) on the valid rows and
+// real outputs, 0 elsewhere; the squared errors summed per block into part[].
+__global__ void k_out_loss(const float *__restrict__ C, const float *__restrict__ b4, const float *__restrict__ Yt,
+                           const uint8_t *__restrict__ valid, float nvalid, float *__restrict__ dOut,
+                           double *__restrict__ part, long rows) {
+    __shared__ double red[256];
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double se = 0.0;
+    if (i < rows * kSurOutPad) {
+        const long r = i / kSurOutPad;
+        const int c = (int)(i % kSurOutPad);
+        float g = 0.f;
+        if (c < kSurOut && valid[r]) {
+            const float e = C[i] + b4[c] - Yt[i];
+            se = (double)e * e;
+            g = 2.f * e / (nvalid * kSurOut);
+        }
+        dOut[i] = g;
+    }
+    red[threadIdx.x] = se;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// dZ = dH * GELU'(Z) (FP32 in, BF16 and FP32 out).
+__global__ void k_gelu_bwd(const float *__restrict__ dH, const float *__restrict__ Z, float *__restrict__ dZ,
+                           __nv_bfloat16 *__restrict__ dZb, long n) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float g = dH[i] * gelu_grad(Z[i]);
+    dZ[i] = g;
+    dZb[i] = __float2bfloat16(g);
+}
+
+__global__ void k_f32_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ b, long n) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __float2bfloat16(a[i]);
+}
+
+// out[c][r] = in[r][c] (BF16), in: rows x cols with leading dimension ldi, out: ldo.
+__global__ void k_transpose_bf16(const __nv_bfloat16 *__restrict__ in, int ldi, __nv_bfloat16 *__restrict__ out,
+                                 int ldo, int rows, int cols) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int r = by + y, c = bx + threadIdx.x;
+        tile[y][threadIdx.x] = (r < rows && c < cols) ? in[(long)r * ldi + c] : __float2bfloat16(0.f);
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int c = bx + y, r = by + threadIdx.x;
+        if (c < cols && r < rows) out[(long)c * ldo + r] = tile[threadIdx.x][y];
+    }
+}
+
+// db[c] = sum_r dZ[r][c], one thread per column, rows summed in order.
+__global__ void k_colsum(const float *__restrict__ dZ, long rows, int W, float *__restrict__ db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= W) return;
+    double s = 0.0;
+    for (long r = 0; r < rows; ++r) s += dZ[r * W + c];
+    db[c] = (float)s;
+}
+
+// Adam on FP32 master parameters; the BF16 copy (if any) follows.  g at gradient stride.
+__global__ void k_adam(float *__restrict__ w, float *__restrict__ m, float *__restrict__ v,
+                       const float *__restrict__ g, __nv_bfloat16 *__restrict__ wb, long n, float lr, float b1,
+                       float b2, float c1, float c2, float eps) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+// Batch rows from the sample set: standardised BF16 features and FP32 targets.
+__global__ void k_gather_batch(const float *__restrict__ dx, const float *__restrict__ dy, const int *__restrict__ idx,
+                               int nb, int B, const SurNorm *__restrict__ nrm, __nv_bfloat16 *__restrict__ Xb,
+                               float *__restrict__ Yb, uint8_t *__restrict__ vb) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= B) return;
+    const bool ok = r < nb;
+    const long s = ok ? idx[r] : 0;
+    for (int q = 0; q < kSurInPad; ++q) {
+        const float v = (ok && q < kSurIn) ? (dx[s * kSurIn + q] - nrm->x_mean[q]) / nrm->x_std[q] : 0.f;
+        Xb[(long)r * kSurInPad + q] = __float2bfloat16(v);
+    }
+    for (int q = 0; q < kSurOutPad; ++q)
+        Yb[(long)r * kSurOutPad + q] = (ok && q < kSurOut) ? (dy[s * kSurOut + q] - nrm->y_mean[q]) / nrm->y_std[q] : 0.f;
+    vb[r] = ok ? 1 : 0;
+}
+
+inline unsigned blocks(long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+}  // namespace
+
+// -------------------------------------------------------------------------------------
+// Host side.
+// -------------------------------------------------------------------------------------
+struct SurState {
+    // parameters: FP32 master (w), Adam moments (m, v), gradients (g), BF16 copies of the
+    // weight tensors; one contiguous block each in the order w1 w2 w3 w4 b1 b2 b3 b4
+    float *w = nullptr, *m = nullptr, *v = nullptr, *g = nullptr;
+    __nv_bfloat16 *wb = nullptr;
+    SurNorm *nrm = nullptr;
+    SurNorm nrm_h{};
+    double *proj = nullptr;
+    double *audit = nullptr;
+    // samples
+    float *ds_x = nullptr, *ds_y = nullptr;
+    uint8_t *ds_valid = nullptr;
+    long ds_cap = 0, ds_next = 0;
+    int collect = 0, stride = 64, collect_steps = 0;
+    // inference
+    __nv_bfloat16 *feat = nullptr;
+    uint8_t *gate = nullptr;
+    float *pred = nullptr;
+    long mpad = 0;
+    int enabled = 0;
+    unsigned audit_period = 100;
+    unsigned step = 0;
+    bool trained = false;
+    long adam_t = 0, train_steps = 0;
+    double last_loss = 0.0;
+};
+
+namespace {
+
+size_t off_w(int t) {  // element offset of tensor t (0..3 weights, 4..7 biases)
+    const size_t sz[8] = {kW1, kW2, kW2, kW4, kSurHid, kSurHid, kSurHid, kSurOutPad};
+    size_t o = 0;
+    for (int i = 0; i < t; ++i) o += sz[i];
+    return o;
+}
+
+// The projection I - A^T (A A^T)^-1 A with A_jk = (atoms of element j in species k) / W_k
+// over the elements present: dY -> the nearest change that conserves every element.
+void make_projection(const lbmgpu_mech &m, double *P) {
+    const int ns = m.n_species;
+    std::vector<std::vector<double>> Arows;
+    for (int e = 0; e < 4; ++e) {
+        std::vector<double> r(ns);
+        double nz = 0.0;
+        for (int k = 0; k < ns; ++k) {
+            r[k] = m.elements[k][e] / m.W[k];
+            nz += fabs(r[k]);
+        }
+        if (nz > 0.0) Arows.push_back(r);
+    }
+    const int ne = (int)Arows.size();
+    std::vector<double> G(ne * ne), Gi(ne * ne, 0.0);
+    for (int i = 0; i < ne; ++i)
+        for (int j = 0; j < ne; ++j) {
+            double s = 0.0;
+            for (int k = 0; k < ns; ++k) s += Arows[i][k] * Arows[j][k];
+            G[i * ne + j] = s;
+        }
+    for (int i = 0; i < ne; ++i) Gi[i * ne + i] = 1.0;
+    for (int c = 0; c < ne; ++c) {  // Gauss-Jordan with partial pivoting (G is SPD, small)
+        int p = c;
+        for (int r = c + 1; r < ne; ++r)
+            if (fabs(G[r * ne + c]) > fabs(G[p * ne + c])) p = r;
+        for (int q = 0; q < ne; ++q) {
+            std::swap(G[c * ne + q], G[p * ne + q]);
+            std::swap(Gi[c * ne + q], Gi[p * ne + q]);
+        }
+        const double d = G[c * ne + c];
+        for (int q = 0; q < ne; ++q) {
+            G[c * ne + q] /= d;
+            Gi[c * ne + q] /= d;
+        }
+        for (int r = 0; r < ne; ++r)
+            if (r != c) {
+                const double f = G[r * ne + c];
+                for (int q = 0; q < ne; ++q) {
+                    G[r * ne + q] -= f * G[c * ne + q];
+                    Gi[r * ne + q] -= f * Gi[c * ne + q];
+                }
+            }
+    }
+    for (int a = 0; a < ns; ++a)
+        for (int b = 0; b < ns; ++b) {
+            double s = 0.0;
+            for (int i = 0; i < ne; ++i)
+                for (int j = 0; j < ne; ++j) s += Arows[i][a] * Gi[i * ne + j] * Arows[j][b];
+            P[a * ns + b] = (a == b ? 1.0 : 0.0) - s;
+        }
+}
+
+void default_norm(SurNorm &n) {
+    for (int q = 0; q < kSurInPad; ++q) {
+        n.x_mean[q] = 0.f;
+        n.x_std[q] = 1.f;
+        n.x_lo[q] = 0.f;
+        n.x_hi[q] = 0.f;
+    }
+    for (int q = 0; q < kSurOutPad; ++q) {
+        n.y_mean[q] = 0.f;
+        n.y_std[q] = 1.f;
+    }
+}
+
+int upload_params(lbmgpu *h) {  // FP32 master -> BF16 copies of the weight tensors
+    SurState &s = *h->sur;
+    const long nw = (long)off_w(4);
+    k_f32_to_bf16<<<blocks(nw), 256, 0, h->stream>>>(s.w, s.wb, nw);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int init_params(lbmgpu *h, unsigned seed) {  // Kaiming-uniform weights, zero biases, fresh Adam
+    SurState &s = *h->sur;
+    std::vector<float> w(kNParams, 0.f);
+    std::mt19937_64 rng(seed);
+    const int fan_in[4] = {kSurIn, kSurHid, kSurHid, kSurHid};
+    const int rows[4] = {kSurHid, kSurHid, kSurHid, kSurOut};
+    const int ld[4] = {kSurInPad, kSurLd, kSurLd, kSurLd};
+    for (int t = 0; t < 4; ++t) {
+        const double bound = std::sqrt(6.0 / fan_in[t]) * (t == 3 ? 0.1 : 1.0);
+        std::uniform_real_distribution<double> U(-bound, bound);
+        for (int r = 0; r < rows[t]; ++r)
+            for (int k = 0; k < fan_in[t]; ++k) w[off_w(t) + (size_t)r * ld[t] + k] = (float)U(rng);
+    }
+    CK(cudaMemcpyAsync(s.w, w.data(), kNParams * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(s.m, 0, kNParams * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(s.v, 0, kNParams * sizeof(float), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    s.adam_t = 0;
+    return upload_params(h);
+}
+
+SurNet net_of(const SurState &s) {
+    SurNet n;
+    n.w1 = s.wb + off_w(0);
+    n.w2 = s.wb + off_w(1);
+    n.w3 = s.wb + off_w(2);
+    n.w4 = s.wb + off_w(3);
+    n.b1 = s.w + off_w(4);
+    n.b2 = s.w + off_w(5);
+    n.b3 = s.w + off_w(6);
+    n.b4 = s.w + off_w(7);
+    return n;
+}
+
+int run_mlp(lbmgpu *h, const __nv_bfloat16 *X, float *pred, long mpad) {
+    SurState &s = *h->sur;
+    CK(cudaFuncSetAttribute(k_sur_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem));
+    const long ntiles = mpad / 16;
+    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>((ntiles + 3) / 4, 148 * 2));
+    k_sur_mlp<<<grid, kSurBlock, kMlpSmem, h->stream>>>(net_of(s), s.nrm, X, pred, ntiles);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace
+
+int sur_create(lbmgpu *h) {
+    if (h->sur) return 0;
+    if (h->ns != 9) return LBMGPU_E_UNSUPPORTED;
+    SurState *s = new SurState();
+    h->sur = s;
+    int rc = 0;
+    if (!rc) rc = dalloc(h, &s->w, kNParams);
+    if (!rc) rc = dalloc(h, &s->m, kNParams);
+    if (!rc) rc = dalloc(h, &s->v, kNParams);
+    if (!rc) rc = dalloc(h, &s->g, kNParams);
+    if (!rc) rc = dalloc(h, &s->wb, off_w(4));
+    if (!rc) rc = dalloc(h, &s->nrm, 1);
+    if (!rc) rc = dalloc(h, &s->proj, 81);
+    if (!rc) rc = dalloc(h, &s->audit, 6);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(s->g, 0, kNParams * sizeof(float), h->stream));
+    CK(cudaMemsetAsync(s->audit, 0, 6 * sizeof(double), h->stream));
+    default_norm(s->nrm_h);
+    CK(cudaMemcpyAsync(s->nrm, &s->nrm_h, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
+    double P[81];
+    make_projection(*h->d.mech, P);
+    CK(cudaMemcpyAsync(s->proj, P, sizeof P, cudaMemcpyHostToDevice, h->stream));
+    return init_params(h, 20261203u);
+}
+
+void sur_release(lbmgpu *h) {
+    SurState *s = h->sur;
+    if (!s) return;
+    cudaFree(s->w);
+    cudaFree(s->m);
+    cudaFree(s->v);
+    cudaFree(s->g);
+    cudaFree(s->wb);
+    cudaFree(s->nrm);
+    cudaFree(s->proj);
+    cudaFree(s->audit);
+    cudaFree(s->ds_x);
+    cudaFree(s->ds_y);
+    cudaFree(s->ds_valid);
+    cudaFree(s->feat);
+    cudaFree(s->gate);
+    cudaFree(s->pred);
+    delete s;
+    h->sur = nullptr;
+}
+
+// Fills the per-step surrogate arguments of the collision-parameter kernel; with the
+// surrogate on, computes every cell's features and the network's predictions first.
+template <typename S>
+int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
+    SurArgs &a = A.sur;
+    std::memset(&a, 0, sizeof a);
+    SurState *s = h->sur;
+    if (!s || h->chem != CHEM_ROSENBROCK) return 0;
+    a.proj = s->proj;
+    a.audit = s->audit;
+    a.audit_period = s->audit_period;
+    a.step = s->step;
+    a.dt_si = (double)h->d.dt_sim * (double)h->U.s;
+    if (s->collect && s->ds_x) {
+        a.ds_x = s->ds_x;
+        a.ds_y = s->ds_y;
+        a.ds_valid = s->ds_valid;
+        a.ds_cap = s->ds_cap;
+        a.ds_stride = s->stride;
+        a.ds_phase = (int)((7L * s->collect_steps) % s->stride);
+        a.ds_base = s->ds_next;
+    }
+    if (s->enabled) {
+        const long mpad = ((h->g.ncell + 15) / 16) * 16;
+        if (mpad != s->mpad) {
+            cudaFree(s->feat);
+            cudaFree(s->gate);
+            cudaFree(s->pred);
+            s->feat = nullptr;
+            s->gate = nullptr;
+            s->pred = nullptr;
+            int rc = dalloc(h, &s->feat, (size_t)mpad * kSurInPad);
+            if (!rc) rc = dalloc(h, &s->gate, (size_t)mpad);
+            if (!rc) rc = dalloc(h, &s->pred, (size_t)mpad * kSurOutPad);
+            if (rc) return rc;
+            s->mpad = mpad;
+        }
+        k_sur_features<9, S><<<blocks(mpad, 128), 128, 0, h->stream>>>(A, s->nrm, s->feat, s->gate, mpad);
+        CK(cudaGetLastError());
+        const int rc = run_mlp(h, s->feat, s->pred, mpad);
+        if (rc) return rc;
+        a.mode = 1;
+        a.pred = s->pred;
+        a.gate = s->gate;
+    }
+    return 0;
+}
+template int sur_prepare_t<double>(lbmgpu *, McArgsT<double, double> &);
+template int sur_prepare_t<float>(lbmgpu *, McArgsT<float, double> &);
+
+void sur_after_step(lbmgpu *h) {
+    SurState *s = h->sur;
+    if (!s || h->chem != CHEM_ROSENBROCK) return;
+    if (s->collect && s->ds_x) {
+        s->ds_next += (h->g.ncell + s->stride - 1) / s->stride;
+        s->collect_steps += 1;
+        if (s->ds_next >= s->ds_cap) s->collect = 0;  // full
+    }
+    s->step += 1;
+}
+
+}  // namespace lbmh
+
+using namespace lbmh;
+
+namespace {
+
+int sur_check(lbmgpu *h) {
+    if (!h) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    CK(cudaSetDevice(h->d.device));
+    return sur_create(h);
+}
+
+// Standardisation from the valid samples: mean and standard deviation per feature and
+// target (floor 1e-12 of the mean's scale, 1 for a constant feature), the feature box.
+int fit_norm(lbmgpu *h, long n) {
+    SurState &s = *h->sur;
+    std::vector<float> x((size_t)n * kSurIn), y((size_t)n * kSurOut);
+    std::vector<uint8_t> v(n);
+    CK(cudaMemcpyAsync(x.data(), s.ds_x, x.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(y.data(), s.ds_y, y.size() * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(v.data(), s.ds_valid, n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    SurNorm &N = s.nrm_h;
+    default_norm(N);
+    long cnt = 0;
+    std::vector<double> sx(kSurIn, 0.0), sxx(kSurIn, 0.0), sy(kSurOut, 0.0), syy(kSurOut, 0.0);
+    std::vector<double> lo(kSurIn, 1e300), hi(kSurIn, -1e300);
+    for (long r = 0; r < n; ++r) {
+        if (!v[r]) continue;
+        ++cnt;
+        for (int q = 0; q < kSurIn; ++q) {
+            const double a = x[r * kSurIn + q];
+            sx[q] += a;
+            sxx[q] += a * a;
+            lo[q] = std::min(lo[q], a);
+            hi[q] = std::max(hi[q], a);
+        }
+        for (int q = 0; q < kSurOut; ++q) {
+            const double a = y[r * kSurOut + q];
+            sy[q] += a;
+            syy[q] += a * a;
+        }
+    }
+    if (cnt < 2) return LBMGPU_E_STATE;
+    for (int q = 0; q < kSurIn; ++q) {
+        const double mu = sx[q] / cnt, var = std::max(0.0, sxx[q] / cnt - mu * mu);
+        N.x_mean[q] = (float)mu;
+        N.x_std[q] = var > 1e-24 * (mu * mu + 1e-300) ? (float)std::sqrt(var) : 1.f;
+        N.x_lo[q] = (float)lo[q];
+        N.x_hi[q] = (float)hi[q];
+    }
+    for (int q = 0; q < kSurOut; ++q) {
+        const double mu = sy[q] / cnt, var = std::max(0.0, syy[q] / cnt - mu * mu);
+        N.y_mean[q] = (float)mu;
+        N.y_std[q] = var > 0.0 ? (float)std::sqrt(var) : 1.f;
+    }
+    CK(cudaMemcpyAsync(s.nrm, &N, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+int ensure_samples(lbmgpu *h, long cap) {
+    SurState &s = *h->sur;
+    if (s.ds_cap >= cap && s.ds_x) return 0;
+    cudaFree(s.ds_x);
+    cudaFree(s.ds_y);
+    cudaFree(s.ds_valid);
+    s.ds_x = s.ds_y = nullptr;
+    s.ds_valid = nullptr;
+    int rc = dalloc(h, &s.ds_x, (size_t)cap * kSurIn);
+    if (!rc) rc = dalloc(h, &s.ds_y, (size_t)cap * kSurOut);
+    if (!rc) rc = dalloc(h, &s.ds_valid, (size_t)cap);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(s.ds_valid, 0, (size_t)cap, h->stream));
+    s.ds_cap = cap;
+    s.ds_next = 0;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbmgpu_surrogate_collect(lbmgpu_t *h, int enable, int stride, long capacity) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (h->chem != CHEM_ROSENBROCK) return LBMGPU_E_UNSUPPORTED;
+    SurState &s = *h->sur;
+    if (!enable) {
+        s.collect = 0;
+        return LBMGPU_OK;
+    }
+    if (stride < 1 || capacity < 16) return LBMGPU_E_ARG;
+    rc = ensure_samples(h, capacity);
+    if (rc) return rc;
+    s.stride = stride;
+    s.collect = s.ds_next < s.ds_cap ? 1 : 0;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_load_samples(lbmgpu_t *h, const float *x, const float *y, long n) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (!x || !y || n < 2) return LBMGPU_E_ARG;
+    rc = ensure_samples(h, n);
+    if (rc) return rc;
+    SurState &s = *h->sur;
+    CK(cudaMemcpyAsync(s.ds_x, x, (size_t)n * kSurIn * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(s.ds_y, y, (size_t)n * kSurOut * 4, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(s.ds_valid, 1, (size_t)n, h->stream));
+    if (s.ds_cap > n) CK(cudaMemsetAsync(s.ds_valid + n, 0, (size_t)(s.ds_cap - n), h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    s.ds_next = n;
+    s.collect = 0;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigned seed, int refit, double *loss) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    SurState &s = *h->sur;
+    if (epochs < 0 || batch < 64 || batch % 64 || !(lr > 0.f)) return LBMGPU_E_ARG;
+    const long n = std::min(s.ds_next, s.ds_cap);
+    if (!s.ds_x || n < 2) return LBMGPU_E_STATE;
+    if (refit || !s.trained) {
+        rc = fit_norm(h, n);
+        if (rc) return rc;
+    }
+    // valid rows, shuffled per epoch with a seeded generator
+    std::vector<uint8_t> v(n);
+    CK(cudaMemcpyAsync(v.data(), s.ds_valid, n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> rows;
+    for (long r = 0; r < n; ++r)
+        if (v[r]) rows.push_back((int)r);
+    if (rows.size() < 2) return LBMGPU_E_STATE;
+    const int B = batch;
+    // batch buffers
+    int *idx = nullptr;
+    __nv_bfloat16 *Xb = nullptr, *H1 = nullptr, *H2 = nullptr, *H3 = nullptr, *dZb = nullptr, *T1 = nullptr,
+                  *T2 = nullptr, *Wt = nullptr;
+    float *Yb = nullptr, *C = nullptr, *Z1 = nullptr, *Z2 = nullptr, *Z3 = nullptr, *dA = nullptr, *dZ = nullptr;
+    uint8_t *vb = nullptr;
+    double *part = nullptr;
+    const long BH = (long)B * kSurHid;
+    const unsigned nparts = blocks((long)B * kSurOutPad);
+    auto all = [&]() {
+        int r = dalloc(h, &idx, B);
+        if (!r) r = dalloc(h, &Xb, (size_t)B * kSurInPad);
+        if (!r) r = dalloc(h, &Yb, (size_t)B * kSurOutPad);
+        if (!r) r = dalloc(h, &vb, B);
+        if (!r) r = dalloc(h, &H1, BH);
+        if (!r) r = dalloc(h, &H2, BH);
+        if (!r) r = dalloc(h, &H3, BH);
+        if (!r) r = dalloc(h, &Z1, BH);
+        if (!r) r = dalloc(h, &Z2, BH);
+        if (!r) r = dalloc(h, &Z3, BH);
+        if (!r) r = dalloc(h, &C, BH);
+        if (!r) r = dalloc(h, &dA, BH);
+        if (!r) r = dalloc(h, &dZ, BH);
+        if (!r) r = dalloc(h, &dZb, BH);
+        if (!r) r = dalloc(h, &T1, BH);
+        if (!r) r = dalloc(h, &T2, BH);
+        if (!r) r = dalloc(h, &Wt, (size_t)kSurHid * kSurLd);
+        if (!r) r = dalloc(h, &part, nparts);
+        return r;
+    };
+    rc = all();
+    std::mt19937_64 rng(seed);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    SurNet net = net_of(s);
+    double epoch_loss = 0.0;
+    std::vector<double> parts(nparts);
+    const int ldw[4] = {kSurInPad, kSurLd, kSurLd, kSurLd};
+    const int kin[4] = {kSurInPad, kSurHid, kSurHid, kSurHid};
+    const int nout[4] = {kSurHid, kSurHid, kSurHid, kSurOutPad};
+    dim3 tb(32, 8);
+    for (int ep = 0; ep < epochs && !rc; ++ep) {
+        std::shuffle(rows.begin(), rows.end(), rng);
+        double sum_se = 0.0;
+        long sum_n = 0;
+        for (size_t b0 = 0; b0 < rows.size() && !rc; b0 += B) {
+            const int nb = (int)std::min<size_t>(B, rows.size() - b0);
+            if (cudaMemcpyAsync(idx, rows.data() + b0, nb * sizeof(int), cudaMemcpyHostToDevice, h->stream)) {
+                rc = LBMGPU_E_CUDA;
+                break;
+            }
+            k_gather_batch<<<blocks(B), 256, 0, h->stream>>>(s.ds_x, s.ds_y, idx, nb, B, s.nrm, Xb, Yb, vb);
+            // forward
+            const __nv_bfloat16 *in = Xb;
+            __nv_bfloat16 *Hs[3] = {H1, H2, H3};
+            float *Zs[3] = {Z1, Z2, Z3};
+            const __nv_bfloat16 *Ws[4] = {net.w1, net.w2, net.w3, net.w4};
+            const float *bs[4] = {net.b1, net.b2, net.b3, net.b4};
+            for (int L = 0; L < 3; ++L) {
+                k_gemm_tn<<<dim3((nout[L] + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(
+                    in, L == 0 ? kSurInPad : kSurHid, Ws[L], ldw[L], C, kSurHid, B, nout[L], kin[L]);
+                k_bias_gelu<<<blocks(BH), 256, 0, h->stream>>>(C, bs[L], Zs[L], Hs[L], B, kSurHid);
+                in = Hs[L];
+            }
+            k_gemm_tn<<<dim3(1, (B + 63) / 64), 128, 0, h->stream>>>(H3, kSurHid, net.w4, kSurLd, C, kSurOutPad, B,
+                                                                       kSurOutPad, kSurHid);
+            k_out_loss<<<nparts, 256, 0, h->stream>>>(C, net.b4, Yb, vb, (float)nb, dA, part, B);
+            // backward: dA holds dL/d(pre-activation) of the current layer (FP32), rows x nout
+            float *gw[4] = {s.g + off_w(0), s.g + off_w(1), s.g + off_w(2), s.g + off_w(3)};
+            float *gb[4] = {s.g + off_w(4), s.g + off_w(5), s.g + off_w(6), s.g + off_w(7)};
+            for (int L = 3; L >= 0; --L) {
+                const int no = nout[L], ki = kin[L];
+                // bias gradient
+                k_colsum<<<blocks(no, 128), 128, 0, h->stream>>>(dA, B, no, gb[L]);
+                // dZ^T [no][B] and input^T [ki][B] for the weight gradient dW = dZ^T in
+                k_f32_to_bf16<<<blocks((long)B * no), 256, 0, h->stream>>>(dA, dZb, (long)B * no);
+                k_transpose_bf16<<<dim3((no + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(dZb, no, T1, B, B, no);
+                const __nv_bfloat16 *inp = L == 0 ? Xb : Hs[L - 1];
+                k_transpose_bf16<<<dim3((ki + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(
+                    inp, L == 0 ? kSurInPad : kSurHid, T2, B, B, ki);
+                k_gemm_tn<<<dim3((ki + 63) / 64, (no + 63) / 64), 128, 0, h->stream>>>(T1, B, T2, B, gw[L], ldw[L], no,
+                                                                                        ki, B);
+                if (L == 0) break;
+                // dH_prev = dZ W  (W^T [ki][no] as the B operand), then through GELU'
+                k_transpose_bf16<<<dim3((ki + 31) / 32, (no + 31) / 32), tb, 0, h->stream>>>(Ws[L], ldw[L], Wt, kSurLd,
+                                                                                              no, ki);
+                k_gemm_tn<<<dim3((ki + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(dZb, no, Wt, kSurLd, C, kSurHid, B,
+                                                                                       ki, no);
+                k_gelu_bwd<<<blocks(BH), 256, 0, h->stream>>>(C, Zs[L - 1], dA, T1, BH);
+            }
+            // Adam step over every parameter (padding entries have zero gradient)
+            s.adam_t += 1;
+            const float c1 = 1.f - (float)std::pow(b1, (double)s.adam_t), c2 = 1.f - (float)std::pow(b2, (double)s.adam_t);
+            for (int t = 0; t < 8; ++t) {
+                const size_t sz[8] = {kW1, kW2, kW2, kW4, kSurHid, kSurHid, kSurHid, kSurOutPad};
+                const size_t o = off_w(t);
+                k_adam<<<blocks((long)sz[t]), 256, 0, h->stream>>>(s.w + o, s.m + o, s.v + o, s.g + o,
+                                                                   t < 4 ? s.wb + o : nullptr, (long)sz[t], lr, b1, b2,
+                                                                   c1, c2, eps);
+            }
+            if (cudaGetLastError() != cudaSuccess) {
+                rc = LBMGPU_E_CUDA;
+                break;
+            }
+            if (cudaMemcpyAsync(parts.data(), part, nparts * sizeof(double), cudaMemcpyDeviceToHost, h->stream) ||
+                cudaStreamSynchronize(h->stream)) {
+                rc = LBMGPU_E_CUDA;
+                break;
+            }
+            for (double p : parts) sum_se += p;
+            sum_n += (long)nb * kSurOut;
+            s.train_steps += 1;
+        }
+        epoch_loss = sum_n ? sum_se / sum_n : 0.0;
+    }
+    cudaFree(idx);
+    cudaFree(Xb);
+    cudaFree(Yb);
+    cudaFree(vb);
+    cudaFree(H1);
+    cudaFree(H2);
+    cudaFree(H3);
+    cudaFree(Z1);
+    cudaFree(Z2);
+    cudaFree(Z3);
+    cudaFree(C);
+    cudaFree(dA);
+    cudaFree(dZ);
+    cudaFree(dZb);
+    cudaFree(T1);
+    cudaFree(T2);
+    cudaFree(Wt);
+    cudaFree(part);
+    if (rc) return rc;
+    s.trained = true;
+    s.last_loss = epoch_loss;
+    if (loss) *loss = epoch_loss;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_enable(lbmgpu_t *h, int enable, int audit_period) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (h->chem != CHEM_ROSENBROCK) return LBMGPU_E_UNSUPPORTED;
+    if (audit_period < 0) return LBMGPU_E_ARG;
+    SurState &s = *h->sur;
+    if (enable && !s.trained) return LBMGPU_E_STATE;
+    s.enabled = enable ? 1 : 0;
+    s.audit_period = (unsigned)audit_period;
+    CK(cudaMemsetAsync(s.audit, 0, 6 * sizeof(double), h->stream));  // the report counts from here
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (!x || !y || n < 1) return LBMGPU_E_ARG;
+    SurState &s = *h->sur;
+    const long mpad = ((n + 15) / 16) * 16;
+    float *xd = nullptr, *pd = nullptr;
+    __nv_bfloat16 *X = nullptr;
+    rc = dalloc(h, &xd, (size_t)n * kSurIn);
+    if (!rc) rc = dalloc(h, &X, (size_t)mpad * kSurInPad);
+    if (!rc) rc = dalloc(h, &pd, (size_t)mpad * kSurOutPad);
+    if (!rc && cudaMemcpyAsync(xd, x, (size_t)n * kSurIn * 4, cudaMemcpyHostToDevice, h->stream)) rc = LBMGPU_E_CUDA;
+    if (!rc) {
+        k_sur_standardise<<<blocks(mpad), 256, 0, h->stream>>>(xd, n, mpad, s.nrm, X);
+        rc = run_mlp(h, X, pd, mpad);
+    }
+    std::vector<float> out;
+    if (!rc) {
+        out.resize((size_t)mpad * kSurOutPad);
+        if (cudaMemcpyAsync(out.data(), pd, out.size() * 4, cudaMemcpyDeviceToHost, h->stream) ||
+            cudaStreamSynchronize(h->stream))
+            rc = LBMGPU_E_CUDA;
+    }
+    cudaFree(xd);
+    cudaFree(X);
+    cudaFree(pd);
+    if (rc) return rc;
+    for (long r = 0; r < n; ++r)
+        for (int q = 0; q < kSurOut; ++q) y[r * kSurOut + q] = out[r * kSurOutPad + q];
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_params(lbmgpu_t *h, float *buf, long n, int set) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (!buf || n < LBMGPU_SUR_NPARAMS) return LBMGPU_E_ARG;
+    SurState &s = *h->sur;
+    // packed layout: W1 [128][12], b1, W2 [128][128], b2, W3, b3, W4 [10][128], b4 [10],
+    // x_mean [12], x_std [12], x_lo [12], x_hi [12], y_mean [10], y_std [10]
+    std::vector<float> w(kNParams);
+    CK(cudaMemcpyAsync(w.data(), s.w, kNParams * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int rows[4] = {kSurHid, kSurHid, kSurHid, kSurOut};
+    const int cols[4] = {kSurIn, kSurHid, kSurHid, kSurHid};
+    const int ld[4] = {kSurInPad, kSurLd, kSurLd, kSurLd};
+    const int nb[4] = {kSurHid, kSurHid, kSurHid, kSurOut};
+    long p = 0;
+    for (int t = 0; t < 4; ++t) {
+        for (int r = 0; r < rows[t]; ++r)
+            for (int k = 0; k < cols[t]; ++k, ++p) {
+                float &d = w[off_w(t) + (size_t)r * ld[t] + k];
+                if (set) d = buf[p]; else buf[p] = d;
+            }
+        for (int r = 0; r < nb[t]; ++r, ++p) {
+            float &d = w[off_w(4 + t) + r];
+            if (set) d = buf[p]; else buf[p] = d;
+        }
+    }
+    SurNorm &N = s.nrm_h;
+    float *fields[6] = {N.x_mean, N.x_std, N.x_lo, N.x_hi, N.y_mean, N.y_std};
+    const int len[6] = {kSurIn, kSurIn, kSurIn, kSurIn, kSurOut, kSurOut};
+    for (int f = 0; f < 6; ++f)
+        for (int q = 0; q < len[f]; ++q, ++p) {
+            if (set) fields[f][q] = buf[p]; else buf[p] = fields[f][q];
+        }
+    if (set) {
+        CK(cudaMemcpyAsync(s.w, w.data(), kNParams * 4, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(s.nrm, &N, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemsetAsync(s.m, 0, kNParams * sizeof(float), h->stream));
+        CK(cudaMemsetAsync(s.v, 0, kNParams * sizeof(float), h->stream));
+        s.adam_t = 0;
+        rc = upload_params(h);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(h->stream));
+        s.trained = true;
+    }
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_stats(lbmgpu_t *h, lbmgpu_surrogate_report *out) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (!out) return LBMGPU_E_ARG;
+    SurState &s = *h->sur;
+    double a[6];
+    CK(cudaMemcpyAsync(a, s.audit, sizeof a, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    out->samples = std::min(s.ds_next, s.ds_cap);
+    out->train_steps = s.train_steps;
+    out->last_loss = s.last_loss;
+    out->cells_audited = (long)a[3];
+    out->cells_predicted = (long)a[4];
+    out->cells_integrated = (long)a[5];
+    out->audit_rel_err = a[1] > 0 ? a[0] / a[1] : 0.0;
+    out->audit_max_abs_err = a[2];
+    out->audit_dY = a[1];
+    out->enabled = s.enabled;
+    out->collecting = s.collect;
+    return LBMGPU_OK;
+}
+
+}  // extern "C"

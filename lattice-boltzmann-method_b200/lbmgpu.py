@@ -37,8 +37,19 @@ EXPORTS = [
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
     "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums", "lbmgpu_sums_noalloc",
+    "lbmgpu_surrogate_collect", "lbmgpu_surrogate_load_samples", "lbmgpu_surrogate_train",
+    "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
 ]
 SUMS_MAX = 21
+SUR_IN, SUR_OUT, SUR_NPARAMS = 12, 10, 36046
+
+
+class SurrogateReport(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_long), ("train_steps", ctypes.c_long), ("last_loss", ctypes.c_double),
+                ("cells_predicted", ctypes.c_long), ("cells_integrated", ctypes.c_long),
+                ("cells_audited", ctypes.c_long), ("audit_rel_err", ctypes.c_double),
+                ("audit_max_abs_err", ctypes.c_double), ("audit_dY", ctypes.c_double), ("enabled", ctypes.c_int),
+                ("collecting", ctypes.c_int)]
 CHEM_OFF, CHEM_REF_EXPLICIT, CHEM_ROSENBROCK = 0, 1, 2
 ST_NEWTON, ST_CHEM = 0x8, 0x10
 
@@ -95,6 +106,15 @@ def lib():
         L.lbmgpu_sums_count.argtypes = [vp]
         L.lbmgpu_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         L.lbmgpu_sums_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.lbmgpu_surrogate_collect.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_long]
+        L.lbmgpu_surrogate_load_samples.argtypes = [vp, fp, fp, ctypes.c_long]
+        L.lbmgpu_surrogate_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
+                                             ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.lbmgpu_surrogate_enable.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.lbmgpu_surrogate_eval.argtypes = [vp, fp, ctypes.c_long, fp]
+        L.lbmgpu_surrogate_params.argtypes = [vp, fp, ctypes.c_long, ctypes.c_int]
+        L.lbmgpu_surrogate_stats.argtypes = [vp, ctypes.POINTER(SurrogateReport)]
         L.lbmgpu_error_string.argtypes = [ctypes.c_int]
         L.lbmgpu_error_string.restype = ctypes.c_char_p
         _lib = L
@@ -252,6 +272,56 @@ class Lattice:
         out = (ctypes.c_double * k)()
         _check(lib().lbmgpu_sums(self.h, out, k), "lbmgpu_sums")
         return list(out)
+
+    # -- chemistry surrogate (CHEM_ROSENBROCK) ------------------------------------------------
+    def surrogate_collect(self, enable=True, stride=1, capacity=1 << 20):
+        """While enabled, each integrator step writes the (features, targets) of every
+        stride-th cell to the device sample set (capacity rows)."""
+        _check(lib().lbmgpu_surrogate_collect(self.h, int(enable), int(stride), int(capacity)),
+               "lbmgpu_surrogate_collect")
+
+    def surrogate_load_samples(self, x, y):
+        """Replaces the sample set: x (n, 12) raw features, y (n, 10) raw targets."""
+        import numpy as np
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.ascontiguousarray(y, dtype=np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(lib().lbmgpu_surrogate_load_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp), len(x)),
+               "lbmgpu_surrogate_load_samples")
+
+    def surrogate_train(self, epochs=10, batch=4096, lr=1e-3, seed=1, refit=False):
+        """Adam epochs over the sample set; returns the last epoch's mean standardised loss."""
+        loss = ctypes.c_double()
+        _check(lib().lbmgpu_surrogate_train(self.h, int(epochs), int(batch), float(lr), int(seed), int(refit),
+                                            ctypes.byref(loss)), "lbmgpu_surrogate_train")
+        return loss.value
+
+    def surrogate_enable(self, enable=True, audit_period=100):
+        _check(lib().lbmgpu_surrogate_enable(self.h, int(enable), int(audit_period)), "lbmgpu_surrogate_enable")
+
+    def surrogate_eval(self, x):
+        """The network on raw features x (n, 12) -> raw predictions (n, 10)."""
+        import numpy as np
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((len(x), SUR_OUT), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(lib().lbmgpu_surrogate_eval(self.h, x.ctypes.data_as(fp), len(x), y.ctypes.data_as(fp)),
+               "lbmgpu_surrogate_eval")
+        return y
+
+    def surrogate_params(self, values=None):
+        """Gets (values None) or sets the packed parameters (SUR_NPARAMS floats)."""
+        import numpy as np
+        buf = np.zeros(SUR_NPARAMS, np.float32) if values is None else np.ascontiguousarray(values, np.float32).copy()
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(lib().lbmgpu_surrogate_params(self.h, buf.ctypes.data_as(fp), len(buf), int(values is not None)),
+               "lbmgpu_surrogate_params")
+        return buf
+
+    def surrogate_stats(self):
+        r = SurrogateReport()
+        _check(lib().lbmgpu_surrogate_stats(self.h, ctypes.byref(r)), "lbmgpu_surrogate_stats")
+        return {k: getattr(r, k) for k, _ in SurrogateReport._fields_}
 
     def sums_noalloc(self, n_out=None):
         """The same totals through lbmgpu_sums_noalloc (fixed device scratch, no

@@ -1,0 +1,179 @@
+"""The chemistry surrogate through the C ABI (lbmgpu_surrogate_*): the fused tensor-core
+forward pass against a torch FP32 reference that rounds operands to BF16 like the device,
+the first Adam step against torch autograd, learning a smooth function, and the whole
+collect -> train -> replace loop on the reacting fixture (audit error, exact element
+conservation of the projected prediction)."""
+import numpy as np
+import pytest
+import torch
+
+import lbmgpu
+import mech
+import workloads as W
+from mc_common import case
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [("W1", (128, 12)), ("b1", (128,)), ("W2", (128, 128)), ("b2", (128,)), ("W3", (128, 128)), ("b3", (128,)),
+          ("W4", (10, 128)), ("b4", (10,)), ("x_mean", (12,)), ("x_std", (12,)), ("x_lo", (12,)), ("x_hi", (12,)),
+          ("y_mean", (10,)), ("y_std", (10,))]
+
+
+def unpack(buf):
+    out, p = {}, 0
+    for k, sh in SHAPES:
+        n = int(np.prod(sh))
+        out[k] = buf[p:p + n].reshape(sh).copy()
+        p += n
+    assert p == lbmgpu.SUR_NPARAMS
+    return out
+
+
+def pack(d):
+    return np.concatenate([np.asarray(d[k], np.float32).reshape(-1) for k, _ in SHAPES])
+
+
+def seeded_params(seed=7):
+    rng = np.random.default_rng(seed)
+    d = {}
+    for k, sh in SHAPES[:8]:
+        fan = sh[1] if len(sh) == 2 else 128
+        d[k] = rng.uniform(-1, 1, sh).astype(np.float32) * (np.sqrt(6.0 / fan) if len(sh) == 2 else 0.1)
+    d["x_mean"] = rng.normal(size=12).astype(np.float32)
+    d["x_std"] = rng.uniform(0.5, 2.0, 12).astype(np.float32)
+    d["x_lo"] = np.full(12, -1e9, np.float32)
+    d["x_hi"] = np.full(12, 1e9, np.float32)
+    d["y_mean"] = rng.normal(size=10).astype(np.float32)
+    d["y_std"] = rng.uniform(0.5, 2.0, 10).astype(np.float32)
+    return d
+
+
+def bf16(t):
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def torch_forward(d, x, round_bf16=True):
+    r = bf16 if round_bf16 else (lambda t: t)
+    t = lambda a: torch.tensor(a, dtype=torch.float32)  # noqa: E731
+    h = r((t(x) - t(d["x_mean"])) / t(d["x_std"]))
+    for L in (1, 2, 3):
+        h = r(torch.nn.functional.gelu(h @ r(t(d[f"W{L}"])).T + t(d[f"b{L}"])))
+    out = h @ r(t(d["W4"])).T + t(d["b4"])
+    return out * t(d["y_std"]) + t(d["y_mean"])
+
+
+def lattice():
+    m, mix, sp, _, _ = case("mc_react8.npz")
+    lat = lbmgpu.Lattice(*mix.shape, mech=m, dtype=W.MIXTURE_MC, species_dtype=W.SPECIES, dx_dt=W.FLAME_UNITS,
+                         chem=lbmgpu.CHEM_ROSENBROCK)
+    return lat, m, mix, sp
+
+
+def test_surrogate_forward_matches_torch_bf16_reference():
+    d = seeded_params()
+    x = np.random.default_rng(3).normal(size=(1000, 12)).astype(np.float32) * d["x_std"] + d["x_mean"]
+    lat, *_ = lattice()
+    with lat:
+        lat.surrogate_params(pack(d))
+        got = lat.surrogate_eval(x)
+        back = unpack(lat.surrogate_params())
+    for k in d:
+        np.testing.assert_array_equal(back[k], d[k])
+    ref = torch_forward(d, x).numpy()
+    err = np.abs((got - ref) / d["y_std"]).max()  # in standardised output units
+    assert err < 2e-2, err
+
+
+def test_surrogate_first_adam_step_follows_torch_gradient():
+    d = seeded_params(11)
+    d["x_lo"][:] = 0.0
+    d["x_hi"][:] = 0.0
+    rng = np.random.default_rng(5)
+    n = 512
+    x = (rng.normal(size=(n, 12)) * d["x_std"] + d["x_mean"]).astype(np.float32)
+    y = (rng.normal(size=(n, 10)) * d["y_std"] + d["y_mean"]).astype(np.float32)
+    lr = 1e-3
+    lat, *_ = lattice()
+    with lat:
+        lat.surrogate_params(pack(d))
+        lat.surrogate_load_samples(x, y)
+        loss = lat.surrogate_train(epochs=1, batch=n, lr=lr, seed=1, refit=False)
+        new = unpack(lat.surrogate_params())
+    # torch: the same standardised MSE, FP32, one gradient
+    P = {k: torch.tensor(d[k], requires_grad=k[0] in "Wb") for k in d}
+    h = (torch.tensor(x) - P["x_mean"]) / P["x_std"]
+    for L in (1, 2, 3):
+        h = torch.nn.functional.gelu(h @ P[f"W{L}"].T + P[f"b{L}"])
+    out = h @ P["W4"].T + P["b4"]
+    tl = ((out - (torch.tensor(y) - P["y_mean"]) / P["y_std"]) ** 2).mean()
+    tl.backward()
+    assert abs(loss - tl.item()) < 0.02 * tl.item()
+    for k in ("W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"):
+        g = P[k].grad.numpy()
+        step = new[k] - d[k]
+        # Adam's first step moves every parameter by lr against the sign of its gradient
+        big = np.abs(g) > 1e-3 * np.abs(g).max()
+        assert np.allclose(np.abs(step[big]), lr, rtol=0.02), k
+        agree = np.sign(step) == -np.sign(g)
+        assert (np.abs(g) * agree).sum() / np.abs(g).sum() > 0.99, k
+
+
+def test_surrogate_learns_a_smooth_map():
+    rng = np.random.default_rng(9)
+    n = 16384
+    x = rng.uniform(-1, 1, size=(n, 12)).astype(np.float32)
+    A = rng.normal(size=(12, 10)).astype(np.float32) / 3
+    y = (np.sin(x @ A) + 0.3 * (x[:, :10] ** 2)).astype(np.float32)
+    lat, *_ = lattice()
+    with lat:
+        lat.surrogate_load_samples(x[:12288], y[:12288])
+        first = lat.surrogate_train(epochs=1, batch=1024, lr=3e-3, seed=2)
+        last = lat.surrogate_train(epochs=40, batch=1024, lr=3e-3, seed=3)
+        pred = lat.surrogate_eval(x[12288:])
+    assert last < 0.05 * first, (first, last)
+    rms = np.sqrt(((pred - y[12288:]) ** 2).mean(0)) / y.std(0)
+    assert rms.max() < 0.25, rms
+
+
+def element_totals(m, s, ns):
+    return np.array([sum(s[5 + a] / m.W[a] * m.elements[a][e] for a in range(ns)) for e in range(3)])
+
+
+def test_surrogate_replaces_the_integrator_on_the_reacting_fixture():
+    lat, m, mix, sp = lattice()
+    with lat:
+        lat.upload(mix, sp)
+        lat.init()
+        lat.surrogate_collect(True, stride=1, capacity=mix.size * 60)
+        lat.step(60)
+        assert lat.synchronize() == 0
+        st = lat.surrogate_stats()
+        assert st["samples"] == mix.size * 60
+        lat.surrogate_collect(False)
+        loss = lat.surrogate_train(epochs=200, batch=1024, lr=2e-3, seed=4)
+        assert loss < 0.05, loss
+        # every cell audited: the integrator's result is used, the network is scored
+        lat.surrogate_enable(True, audit_period=1)
+        lat.step(5)
+        assert lat.synchronize() == 0
+        st = lat.surrogate_stats()
+        assert st["cells_audited"] == 5 * int((mix["type"] == 0).sum())
+        audit_err = st["audit_rel_err"]
+        # the network in charge (no audit): element totals change only through transport,
+        # exactly as in a step of the integrator from the same state
+        c = mix.copy()
+        s_ = [a.copy() for a in sp]
+        lat.download(c, s_)
+        e0 = element_totals(m, lat.sums(), len(sp))
+        lat.surrogate_enable(True, audit_period=0)
+        lat.step(1)
+        assert lat.synchronize() == 0
+        st = lat.surrogate_stats()
+        assert st["cells_predicted"] > 0
+        e_sur = element_totals(m, lat.sums(), len(sp))
+        lat.upload(c, s_)
+        lat.surrogate_enable(False)
+        lat.step(1)
+        e_int = element_totals(m, lat.sums(), len(sp))
+    assert np.all(np.abs((e_sur - e0) - (e_int - e0)) <= 1e-10 * np.abs(e0)), (e_sur - e0, e_int - e0)
+    assert audit_err < 0.05, audit_err
