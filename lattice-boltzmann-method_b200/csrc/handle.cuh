@@ -80,6 +80,7 @@ struct lbmgpu {
     double *sum_scratch = nullptr;          // lbmgpu_sums: block partials and totals
     double *props = nullptr;                // multicomponent collision parameters
     lbmh::SurState *sur = nullptr;          // chemistry surrogate, created on first use
+    lbmgpu_mech mech{};                     // multicomponent: the caller's mechanism, copied at create
     long nfluid = 0;
 };
 

@@ -416,6 +416,7 @@ int mc_setup(lbmgpu *h) {
     const lbmgpu_desc &d = h->d;
     if (!valid_mc_layout(d.mix, d.spc)) return LBMGPU_E_ARG;
     h->ns = d.n_species;
+    h->mech = *d.mech;
     h->nrec = mc_nrec(h->ns);
     h->chem = d.chem_mode;
     h->fp32 = d.precision == LBMGPU_FP32;

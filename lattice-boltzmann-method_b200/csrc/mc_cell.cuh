@@ -472,11 +472,8 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
                 dY[a] = (double)pr[a];
                 have_pred = have_pred && isfinite(dY[a]);
             }
-            for (int a = 0; a < NS; ++a) {
-                double sp = 0.0;
-                for (int b = 0; b < NS; ++b) sp += S.proj[a * NS + b] * dY[b];
-                Yp[a] = Y[a] + sp;
-            }
+            if (have_pred) sur_conserve<NS>(S.elem, rho_a, kSpeciesMin, dY);
+            for (int a = 0; a < NS; ++a) Yp[a] = Y[a] + dY[a];
             Tp = T_si + (double)pr[NS];
         }
         const bool audit = have_pred && S.audit_period > 0 && sur_hash((unsigned)n, S.step) % S.audit_period == 0;

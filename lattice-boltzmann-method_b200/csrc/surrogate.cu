@@ -3,8 +3,9 @@
 // No counterpart in the reference (whose chemistry is Cantera's explicit rates): an MLP
 // that learns the stiff ROS2 integrator's step (T, ln p, Y_k, dt) -> (dY_k, dT) from
 // samples the integrator itself writes while the run proceeds (mc_cell.cuh, teacher
-// steps), then stands in for it with an input-box gate, an element-conserving projection
-// and an audited sample (mc_cell.cuh, mode 1).
+// steps), then stands in for it with an input-box gate, an exactly element-conserving
+// correction of the prediction (sur_conserve, surrogate.cuh) and an audited sample
+// (mc_cell.cuh, mode 1).
 //
 // Tensor-core kernels, BF16 operands with FP32 accumulation (mma.sync m16n8k16):
 //   k_sur_mlp   the whole network for a batch of cells in one kernel: the weights are
@@ -370,7 +371,7 @@ struct SurState {
     __nv_bfloat16 *wb = nullptr;
     SurNorm *nrm = nullptr;
     SurNorm nrm_h{};
-    double *proj = nullptr;
+    double *elem = nullptr;
     double *audit = nullptr;
     // samples
     float *ds_x = nullptr, *ds_y = nullptr;
@@ -397,60 +398,6 @@ size_t off_w(int t) {  // element offset of tensor t (0..3 weights, 4..7 biases)
     size_t o = 0;
     for (int i = 0; i < t; ++i) o += sz[i];
     return o;
-}
-
-// The projection I - A^T (A A^T)^-1 A with A_jk = (atoms of element j in species k) / W_k
-// over the elements present: dY -> the nearest change that conserves every element.
-void make_projection(const lbmgpu_mech &m, double *P) {
-    const int ns = m.n_species;
-    std::vector<std::vector<double>> Arows;
-    for (int e = 0; e < 4; ++e) {
-        std::vector<double> r(ns);
-        double nz = 0.0;
-        for (int k = 0; k < ns; ++k) {
-            r[k] = m.elements[k][e] / m.W[k];
-            nz += fabs(r[k]);
-        }
-        if (nz > 0.0) Arows.push_back(r);
-    }
-    const int ne = (int)Arows.size();
-    std::vector<double> G(ne * ne), Gi(ne * ne, 0.0);
-    for (int i = 0; i < ne; ++i)
-        for (int j = 0; j < ne; ++j) {
-            double s = 0.0;
-            for (int k = 0; k < ns; ++k) s += Arows[i][k] * Arows[j][k];
-            G[i * ne + j] = s;
-        }
-    for (int i = 0; i < ne; ++i) Gi[i * ne + i] = 1.0;
-    for (int c = 0; c < ne; ++c) {  // Gauss-Jordan with partial pivoting (G is SPD, small)
-        int p = c;
-        for (int r = c + 1; r < ne; ++r)
-            if (fabs(G[r * ne + c]) > fabs(G[p * ne + c])) p = r;
-        for (int q = 0; q < ne; ++q) {
-            std::swap(G[c * ne + q], G[p * ne + q]);
-            std::swap(Gi[c * ne + q], Gi[p * ne + q]);
-        }
-        const double d = G[c * ne + c];
-        for (int q = 0; q < ne; ++q) {
-            G[c * ne + q] /= d;
-            Gi[c * ne + q] /= d;
-        }
-        for (int r = 0; r < ne; ++r)
-            if (r != c) {
-                const double f = G[r * ne + c];
-                for (int q = 0; q < ne; ++q) {
-                    G[r * ne + q] -= f * G[c * ne + q];
-                    Gi[r * ne + q] -= f * Gi[c * ne + q];
-                }
-            }
-    }
-    for (int a = 0; a < ns; ++a)
-        for (int b = 0; b < ns; ++b) {
-            double s = 0.0;
-            for (int i = 0; i < ne; ++i)
-                for (int j = 0; j < ne; ++j) s += Arows[i][a] * Gi[i * ne + j] * Arows[j][b];
-            P[a * ns + b] = (a == b ? 1.0 : 0.0) - s;
-        }
 }
 
 void default_norm(SurNorm &n) {
@@ -532,16 +479,18 @@ int sur_create(lbmgpu *h) {
     if (!rc) rc = dalloc(h, &s->g, kNParams);
     if (!rc) rc = dalloc(h, &s->wb, off_w(4));
     if (!rc) rc = dalloc(h, &s->nrm, 1);
-    if (!rc) rc = dalloc(h, &s->proj, 81);
+    if (!rc) rc = dalloc(h, &s->elem, 4 * 9);
     if (!rc) rc = dalloc(h, &s->audit, 6);
     if (rc) return rc;
     CK(cudaMemsetAsync(s->g, 0, kNParams * sizeof(float), h->stream));
     CK(cudaMemsetAsync(s->audit, 0, 6 * sizeof(double), h->stream));
     default_norm(s->nrm_h);
     CK(cudaMemcpyAsync(s->nrm, &s->nrm_h, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
-    double P[81];
-    make_projection(*h->d.mech, P);
-    CK(cudaMemcpyAsync(s->proj, P, sizeof P, cudaMemcpyHostToDevice, h->stream));
+    double E[4 * 9];  // atoms of element e per unit mass of species k
+    for (int e = 0; e < 4; ++e)
+        for (int k = 0; k < 9; ++k) E[e * 9 + k] = h->mech.elements[k][e] / h->mech.W[k];
+    CK(cudaMemcpyAsync(s->elem, E, sizeof E, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return init_params(h, 20261203u);
 }
 
@@ -554,7 +503,7 @@ void sur_release(lbmgpu *h) {
     cudaFree(s->g);
     cudaFree(s->wb);
     cudaFree(s->nrm);
-    cudaFree(s->proj);
+    cudaFree(s->elem);
     cudaFree(s->audit);
     cudaFree(s->ds_x);
     cudaFree(s->ds_y);
@@ -574,7 +523,7 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
     std::memset(&a, 0, sizeof a);
     SurState *s = h->sur;
     if (!s || h->chem != CHEM_ROSENBROCK) return 0;
-    a.proj = s->proj;
+    a.elem = s->elem;
     a.audit = s->audit;
     a.audit_period = s->audit_period;
     a.step = s->step;

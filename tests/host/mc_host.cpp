@@ -135,3 +135,8 @@ extern "C" int mc_host_run32(int Nx, int Ny, int Nz, const signed char *type, co
     return run<float, double>(Nx, Ny, Nz, type, mech, dx, dt, chem, nsteps, pop0, pop1, rec0, rec1, shift, status,
                               nullptr);
 }
+
+// The surrogate's element-conserving correction of a predicted dY (surrogate.cuh).
+extern "C" void sur_conserve_host(const double *elem, const double *rho_a, double floor_rho, double *dY) {
+    lbm::sur_conserve<9>(elem, rho_a, floor_rho, dY);
+}
