@@ -65,8 +65,12 @@ def parse():
                          "1800 K slab; inflow: config 2's shape, the mixing layer between a characteristic "
                          "inflow and outflow (N^3); chan: config 3's shape, a reacting H2-air channel with "
                          "NSCBC outflow ends and TMS walls (2N x N/2 x N/2)")
-    ap.add_argument("--chem", choices=["ref", "rosenbrock"], default="ref",
-                    help="react workload: the reference's explicit scheme or the ROS2 stiff integrator")
+    ap.add_argument("--chem", choices=["ref", "rosenbrock", "surrogate"], default="ref",
+                    help="reacting workloads: the reference's explicit scheme, the ROS2 stiff integrator, or "
+                         "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
+                         "surrogate steps with a 1 %% audit; plain ROS2 timed on the same lattice beside it)")
+    ap.add_argument("--teach", type=int, default=60, help="surrogate: ROS2 teacher steps that collect samples")
+    ap.add_argument("--epochs", type=int, default=8, help="surrogate: training epochs over the samples")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="multicomponent population storage (fp32: shifted FP32 populations, FP64 records)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -289,8 +293,11 @@ def mc_workload_name(args, ncell_shape):
     reaction = mc_reaction(args)
     chem = ""
     if reaction:
-        chem = "ROS2 stiff chemistry" if args.chem == "rosenbrock" else "reference explicit chemistry"
-    return (f"{args.workload}{args.N}_mc9_{args.precision}" + ("_ros2" if reaction and args.chem == "rosenbrock" else "")
+        chem = {"rosenbrock": "ROS2 stiff chemistry",
+                "surrogate": "MLP chemistry surrogate trained online from ROS2 (1 % audit)"}.get(
+                    args.chem, "reference explicit chemistry")
+    return (f"{args.workload}{args.N}_mc9_{args.precision}"
+            + ({"rosenbrock": "_ros2", "surrogate": "_surrogate"}.get(args.chem, "") if reaction else "")
             + f": 9-species H2/O2/N2 D3Q27, {ncell_shape} {MC_SHAPES[args.workload]}, dx 20 um, dt 1 ns, "
             + (chem if reaction else "non-reacting"))
 
@@ -416,7 +423,8 @@ def run_ours_mc(args, dist):
     ncell = fluid_cells(mix)
     chem = lbmgpu.CHEM_OFF
     if reaction:
-        chem = lbmgpu.CHEM_ROSENBROCK if args.chem == "rosenbrock" else lbmgpu.CHEM_REF_EXPLICIT
+        chem = lbmgpu.CHEM_ROSENBROCK if args.chem in ("rosenbrock", "surrogate") else lbmgpu.CHEM_REF_EXPLICIT
+    use_sur = reaction and args.chem == "surrogate"
 
     prec = lbmgpu.FP32 if args.precision == "fp32" else lbmgpu.FP64
     pop_bytes = 4 if args.precision == "fp32" else 8
@@ -428,7 +436,28 @@ def run_ours_mc(args, dist):
     lat = lattice()
     lat.upload(mix, sp)
     lat.init()
+    sur = None
+    if use_sur:
+        # teacher steps (ROS2) writing samples, training, then the surrogate with a 1 % audit
+        cap = 1 << 21
+        stride = max(1, -(-mix.size * args.teach // cap))
+        lat.surrogate_collect(True, stride=stride, capacity=cap)
+        t0 = time.perf_counter()
+        lat.step(args.teach)
+        lat.synchronize()
+        t_teach = time.perf_counter() - t0
+        lat.surrogate_collect(False)
+        t0 = time.perf_counter()
+        loss = lat.surrogate_train(epochs=args.epochs, batch=4096, lr=2e-3, seed=20261203)
+        t_train = time.perf_counter() - t0
+        n_samples = lat.surrogate_stats()["samples"]
+        lat.surrogate_enable(True, audit_period=100)
+        sur_params = lat.surrogate_params()
+        sur = {"teacher_steps": args.teach, "sample_stride": stride, "samples_rows": n_samples,
+               "teacher_s": t_teach, "train_epochs": args.epochs, "train_s": t_train, "train_loss": loss}
     lat.time_steps(max(3, args.warmup))
+    if use_sur:
+        lat.surrogate_enable(True, audit_period=100)  # the audit report covers the timed steps
     dist.barrier()
     clk = Clocks(device)
     clk.start()
@@ -436,11 +465,25 @@ def run_ours_mc(args, dist):
     clocks = clk.stop()
     status = lat.synchronize()
     ms = dist.max(ms)
+    if use_sur:
+        st = lat.surrogate_stats()
+        tot = max(1, st["cells_predicted"] + st["cells_integrated"] + st["cells_audited"])
+        sur.update({"audit_rel_err": st["audit_rel_err"], "audit_max_abs_err": st["audit_max_abs_err"],
+                    "predicted_frac": st["cells_predicted"] / tot, "integrated_frac": st["cells_integrated"] / tot,
+                    "audited_frac": st["cells_audited"] / tot})
     kk = min(args.steps, 20)
     lat.profile(True)
     lat.time_steps(kk)
     launches, kms = lat.kernel_times()
     lat.profile(False)
+    if use_sur:
+        # plain ROS2 on the same lattice and state, for the comparison
+        lat.surrogate_enable(False)
+        kp = min(args.steps, 10)
+        ms_plain = lat.time_steps(kp)
+        sur["plain_chem_mlups"] = ncell * kp / (ms_plain * 1e-3) / 1e6
+        sur["surrogate_ms_per_step"] = kms[4] / max(kk, 1)
+        sur["network_flops_per_cell"] = 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)
     lat.close()
     avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_stream": kms[1] / max(launches[1], 1),
            "k_mc_props": kms[3] / max(launches[3], 1)}
@@ -457,6 +500,9 @@ def run_ours_mc(args, dist):
     hm = mix.copy()
     hs = [a.copy() for a in sp]
     lat = lattice()
+    if use_sur:  # the network trained above, loaded through the API
+        lat.surrogate_params(sur_params)
+        lat.surrogate_enable(True, audit_period=100)
     dist.barrier()
     t0 = time.perf_counter()
     lat.upload(hm, hs)
@@ -496,6 +542,7 @@ def run_ours_mc(args, dist):
                      "alg_bytes_per_launch": alg, "mean_launch_ms": avg[dom], "kernel_ms": avg},
         "gpu_launches": int(round(sum(launches) / kk * args.steps)),
         "status": status, "clocks": clocks, "e2e": e2e,
+        **({"surrogate": sur} if sur else {}),
     }
     if dist.world == 1 and not args.no_cpu_baseline:
         try:

@@ -17,8 +17,9 @@ constexpr int kBlock = 128;
 
 enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SPECIES = 4 };
 // per-kernel timing classes; multicomponent: K_COLLIDE is the population update
-// (k_mc_relax) and K_PROPS the collision parameters (k_mc_props)
-enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_NKINDS = 4 };
+// (k_mc_relax), K_PROPS the collision parameters (k_mc_props), K_SURROGATE the chemistry
+// surrogate's features, network and integrator list
+enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_NKINDS = 5 };
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.
 enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };

@@ -40,6 +40,19 @@ __global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
     mc_props_cell<NS, CHEM>(A, n);
 }
 
+// the cells the collision-parameter kernel left to the chemistry integrator (surrogate
+// on: out-of-box, non-finite and audited cells), integrated in dense warps
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
+    const unsigned cnt = *A.sur.icount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const long n = A.sur.ilist[i];
+        double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
+        mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
+        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+    }
+}
+
 // BGK update: blockIdx.y selects the population set (species 0..NS-1, NS = energy), the
 // x dimension the cells, so a warp reads one set's planes at 32 consecutive cells
 template <int NS, typename S>
@@ -374,6 +387,13 @@ int collide_t(lbmgpu *h) {
         k_mc_props<NS9, CHEM_ROSENBROCK, S><<<gp, kBlock, 0, h->stream>>>(A);
     else
         k_mc_props<NS9, CHEM_OFF, S><<<gp, kBlock, 0, h->stream>>>(A);
+    if (A.sur.ilist) {
+        EvPair ei{};
+        ev_begin(h, K_SURROGATE, ei);
+        k_mc_chem_list<NS9, S><<<148 * 4, kBlock, 0, h->stream>>>(A);
+        ev_end(h, ei);
+        CK(cudaGetLastError());
+    }
     ev_end(h, ep);
     CK(cudaGetLastError());
     EvPair er{};

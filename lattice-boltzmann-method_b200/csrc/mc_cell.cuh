@@ -394,6 +394,106 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // theta, U, dq_d (3), D_ab (NS (NS-1) / 2).
 // ------------------------------------------------------------------------------------
 
+// The chemistry of LBMGPU_CHEM_ROSENBROCK for one cell: the constant-(rho, e) reactor
+// over the whole lattice step with ROS2 (chem.cuh); the density change and the heat
+// release enter the collision the same way as the reference's explicit increments.
+//
+// With the surrogate on (sur.mode 1) the network's dY, dT replace the integrator, made
+// exactly element-conserving (sur_conserve); cells outside the training box, non-finite
+// predictions and the audited cells need the integrator (the audited ones also score the
+// prediction against it).  With `defer` and a list (sur.ilist) such cells are only
+// appended to the list -- k_mc_chem_list integrates them afterwards in dense warps --
+// otherwise they are integrated here.  Teacher steps (mode 0) can write samples.
+template <int NS, class AT>
+MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
+                         double rho_si, double P_si, bool defer) {
+    const gas::Tables &t = *A.tab;
+    const SurArgs &S = A.sur;
+    const double dt_si = (double)A.dt * (double)A.U.s;
+    double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
+    bool have_pred = false;
+    if (S.mode == 1 && !S.gate[n]) {
+        const float *pr = S.pred + n * kSurOutPad;
+        double dY[NS];
+        have_pred = isfinite(pr[NS]);
+        for (int a = 0; a < NS; ++a) {
+            dY[a] = (double)pr[a];
+            have_pred = have_pred && isfinite(dY[a]);
+        }
+        if (have_pred) sur_conserve<NS>(S.elem, rho_a, kSpeciesMin, dY);
+        for (int a = 0; a < NS; ++a) Yp[a] = Y[a] + dY[a];
+        Tp = T_si + (double)pr[NS];
+    }
+    const bool audit = have_pred && S.audit_period > 0 && sur_hash((unsigned)n, S.step) % S.audit_period == 0;
+    if (S.mode == 1 && (defer || !S.ilist)) {
+        count_flag(&S.audit[3], audit);
+        count_flag(&S.audit[4], have_pred && !audit);
+        count_flag(&S.audit[5], !have_pred);
+    }
+    if (!have_pred || audit) {
+        if (defer && S.ilist) {
+#if defined(__CUDA_ARCH__)
+            S.ilist[atomicAdd(S.icount, 1u)] = (int)n;
+#else
+            S.ilist[(*S.icount)++] = (int)n;
+#endif
+            return;
+        }
+        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+        if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
+    } else {
+        for (int a = 0; a < NS; ++a) Yc[a] = Yp[a];
+        Tc = Tp;
+    }
+    if (audit) {  // L1 error of the predicted dY and L1 size of the integrator's dY
+        double num = 0.0, den = 0.0;
+        for (int a = 0; a < NS; ++a) {
+            num += fabs(Yp[a] - Yc[a]);
+            den += fabs(Yc[a] - Y[a]);
+        }
+        add_max(&S.audit[0], &S.audit[2], num);
+#if defined(__CUDA_ARCH__)
+        atomicAdd(&S.audit[1], den);
+#else
+        S.audit[1] += den;
+#endif
+    }
+    if (S.ds_x && !have_pred && (long)(n % S.ds_stride) == S.ds_phase) {
+        const long row = S.ds_base + n / S.ds_stride;
+        if (row < S.ds_cap) {
+            sur_features<NS>(T_si, P_si, Y, dt_si, S.ds_x + row * kSurIn);
+            for (int a = 0; a < NS; ++a) S.ds_y[row * kSurOut + a] = (float)(Yc[a] - Y[a]);
+            S.ds_y[row * kSurOut + NS] = (float)(Tc - T_si);
+            S.ds_valid[row] = 1;
+        }
+    }
+    double hrr = 0.0;
+    for (int a = 0; a < NS; ++a) {
+        const double dr = rho * (Yc[a] - Y[a]);
+        hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * dr;
+        A.props[(long)pr_drho<NS>(a) * A.ncell + n] = dr;
+    }
+    put(A, A.rec_nxt, RM_HRR, n, hrr);
+}
+
+// The chemistry state of a cell from the record, as the collision forms it (Cantera's
+// setMassFractions + setState_TD, lbm-collision.cpp:364-367).
+template <int NS, class AT>
+MC_HD void mc_chem_state(const AT &A, long n, double &rho, double *rho_a, double *Y, double &T_si, double &rho_si,
+                         double &P_si) {
+    const gas::Tables &t = *A.tab;
+    rho = rec(A, A.rec_cur, RM_RHO, n);
+    double Yr[NS], X[NS];
+    for (int a = 0; a < NS; ++a) {
+        rho_a[a] = rec(A, A.rec_cur, rs(a, RS_RHO), n);
+        Yr[a] = rho_a[a] / rho;
+    }
+    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
+    T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
+    rho_si = si_rho(A.U, (float)rho);
+    P_si = rho_si * gas::kR * T_si / W;
+}
+
 template <int NS, int CHEM, class AT>
 MC_HDN void mc_props_cell(const AT &A, long n) {
     const gas::Tables &t = *A.tab;
@@ -451,73 +551,7 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         }
         put(A, A.rec_nxt, RM_HRR, n, hrr);
     } else if (CHEM == CHEM_ROSENBROCK) {
-        // stiff alternative: the constant-(rho, e) reactor over the whole lattice step with
-        // ROS2 (chem.cuh); the density change and the heat release enter the collision the
-        // same way as the reference's explicit increments
-        //
-        // With the surrogate on (sur.mode 1) the network's dY, dT replace the integrator,
-        // projected onto changes that conserve every element exactly; cells outside the
-        // training box, non-finite predictions and the audited cells run the integrator
-        // (the audited ones also score the prediction against it).  Teacher steps can
-        // write (features, targets) samples for training.
-        const SurArgs &S = A.sur;
-        const double dt_si = (double)dt * (double)A.U.s;
-        double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
-        bool have_pred = false;
-        if (S.mode == 1 && !S.gate[n]) {
-            const float *pr = S.pred + n * kSurOutPad;
-            double dY[NS];
-            have_pred = isfinite(pr[NS]);
-            for (int a = 0; a < NS; ++a) {
-                dY[a] = (double)pr[a];
-                have_pred = have_pred && isfinite(dY[a]);
-            }
-            if (have_pred) sur_conserve<NS>(S.elem, rho_a, kSpeciesMin, dY);
-            for (int a = 0; a < NS; ++a) Yp[a] = Y[a] + dY[a];
-            Tp = T_si + (double)pr[NS];
-        }
-        const bool audit = have_pred && S.audit_period > 0 && sur_hash((unsigned)n, S.step) % S.audit_period == 0;
-        if (!have_pred || audit) {
-            for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
-            if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
-        } else {
-            for (int a = 0; a < NS; ++a) Yc[a] = Yp[a];
-            Tc = Tp;
-        }
-        if (S.mode == 1) {
-            if (audit) {  // L1 error of the predicted dY and L1 size of the integrator's dY
-                double num = 0.0, den = 0.0;
-                for (int a = 0; a < NS; ++a) {
-                    num += fabs(Yp[a] - Yc[a]);
-                    den += fabs(Yc[a] - Y[a]);
-                }
-                add_max(&S.audit[0], &S.audit[2], num);
-#if defined(__CUDA_ARCH__)
-                atomicAdd(&S.audit[1], den);
-#else
-                S.audit[1] += den;
-#endif
-            }
-            count_flag(&S.audit[3], audit);
-            count_flag(&S.audit[4], have_pred && !audit);
-            count_flag(&S.audit[5], !have_pred);
-        }
-        if (S.ds_x && !have_pred && (long)(n % S.ds_stride) == S.ds_phase) {
-            const long row = S.ds_base + n / S.ds_stride;
-            if (row < S.ds_cap) {
-                sur_features<NS>(T_si, P_si, Y, dt_si, S.ds_x + row * kSurIn);
-                for (int a = 0; a < NS; ++a) S.ds_y[row * kSurOut + a] = (float)(Yc[a] - Y[a]);
-                S.ds_y[row * kSurOut + NS] = (float)(Tc - T_si);
-                S.ds_valid[row] = 1;
-            }
-        }
-        double hrr = 0.0;
-        for (int a = 0; a < NS; ++a) {
-            const double dr = rho * (Yc[a] - Y[a]);
-            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * dr;
-            prp(pr_drho<NS>(a), dr);
-        }
-        put(A, A.rec_nxt, RM_HRR, n, hrr);
+        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
     }
 
     // -- species viscosities; Wilke weights phi_ab = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^1/4)^2 /

@@ -382,6 +382,8 @@ struct SurState {
     __nv_bfloat16 *feat = nullptr;
     uint8_t *gate = nullptr;
     float *pred = nullptr;
+    int *ilist = nullptr;
+    unsigned *icount = nullptr;
     long mpad = 0;
     int enabled = 0;
     unsigned audit_period = 100;
@@ -511,6 +513,8 @@ void sur_release(lbmgpu *h) {
     cudaFree(s->feat);
     cudaFree(s->gate);
     cudaFree(s->pred);
+    cudaFree(s->ilist);
+    cudaFree(s->icount);
     delete s;
     h->sur = nullptr;
 }
@@ -543,22 +547,34 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
             cudaFree(s->feat);
             cudaFree(s->gate);
             cudaFree(s->pred);
+            cudaFree(s->ilist);
+            cudaFree(s->icount);
             s->feat = nullptr;
             s->gate = nullptr;
             s->pred = nullptr;
+            s->ilist = nullptr;
+            s->icount = nullptr;
             int rc = dalloc(h, &s->feat, (size_t)mpad * kSurInPad);
             if (!rc) rc = dalloc(h, &s->gate, (size_t)mpad);
             if (!rc) rc = dalloc(h, &s->pred, (size_t)mpad * kSurOutPad);
+            if (!rc) rc = dalloc(h, &s->ilist, (size_t)mpad);
+            if (!rc) rc = dalloc(h, &s->icount, 1);
             if (rc) return rc;
             s->mpad = mpad;
         }
+        EvPair ep{};
+        ev_begin(h, K_SURROGATE, ep);
         k_sur_features<9, S><<<blocks(mpad, 128), 128, 0, h->stream>>>(A, s->nrm, s->feat, s->gate, mpad);
         CK(cudaGetLastError());
         const int rc = run_mlp(h, s->feat, s->pred, mpad);
+        ev_end(h, ep);
         if (rc) return rc;
+        CK(cudaMemsetAsync(s->icount, 0, sizeof(unsigned), h->stream));
         a.mode = 1;
         a.pred = s->pred;
         a.gate = s->gate;
+        a.ilist = s->ilist;
+        a.icount = s->icount;
     }
     return 0;
 }

@@ -42,6 +42,8 @@ struct SurArgs {
     long ds_base, ds_cap;
     int ds_stride, ds_phase;
     double dt_si;              // the lattice time step in seconds
+    int *ilist;                // cells left to the integrator (mode 1), appended by the
+    unsigned *icount;          //   collision-parameter kernel, integrated by k_mc_chem_list
 };
 
 // Features of a cell: T (K), ln p (p in Pa), the normalised mass fractions, dt (s).

@@ -257,10 +257,11 @@ class Lattice:
 
     def kernel_times(self):
         """Per kernel kind (0 collide / population update, 1 stream+boundary+moment,
-        2 other, 3 multicomponent collision parameters): launches and device ms."""
-        launches = (ctypes.c_long * 4)()
-        ms = (ctypes.c_double * 4)()
-        _check(lib().lbmgpu_kernel_times(self.h, 4, launches, ms), "lbmgpu_kernel_times")
+        2 other, 3 multicomponent collision parameters, 4 chemistry surrogate): launches
+        and device ms."""
+        launches = (ctypes.c_long * 5)()
+        ms = (ctypes.c_double * 5)()
+        _check(lib().lbmgpu_kernel_times(self.h, 5, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------
