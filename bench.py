@@ -70,7 +70,9 @@ def parse():
                          "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
                          "surrogate steps with a 1 %% audit; plain ROS2 timed on the same lattice beside it)")
     ap.add_argument("--teach", type=int, default=60, help="surrogate: ROS2 teacher steps that collect samples")
-    ap.add_argument("--epochs", type=int, default=8, help="surrogate: training epochs over the samples")
+    ap.add_argument("--epochs", type=int, default=16, help="surrogate: training epochs over the samples")
+    ap.add_argument("--augment", type=float, default=0.5,
+                    help="surrogate: perturbed, integrator-labelled rows added per collected row")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
                     help="multicomponent population storage (fp32: shifted FP32 populations, FP64 records)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -448,13 +450,19 @@ def run_ours_mc(args, dist):
         t_teach = time.perf_counter() - t0
         lat.surrogate_collect(False)
         t0 = time.perf_counter()
+        n_aug = int(args.augment * lat.surrogate_stats()["samples"])
+        if n_aug > 0:
+            lat.surrogate_augment(n_aug, span_y=1.5, span_t=0.01, y_trace=1e-3, seed=20261203)
+        lat.synchronize()
+        t_aug = time.perf_counter() - t0
+        t0 = time.perf_counter()
         loss = lat.surrogate_train(epochs=args.epochs, batch=4096, lr=2e-3, seed=20261203)
         t_train = time.perf_counter() - t0
         n_samples = lat.surrogate_stats()["samples"]
         lat.surrogate_enable(True, audit_period=100)
         sur_params = lat.surrogate_params()
         sur = {"teacher_steps": args.teach, "sample_stride": stride, "samples_rows": n_samples,
-               "teacher_s": t_teach, "train_epochs": args.epochs, "train_s": t_train, "train_loss": loss}
+               "teacher_s": t_teach, "augmented_rows": n_aug, "augment_s": t_aug, "train_epochs": args.epochs, "train_s": t_train, "train_loss": loss}
     lat.time_steps(max(3, args.warmup))
     if use_sur:
         lat.surrogate_enable(True, audit_period=100)  # the audit report covers the timed steps

@@ -227,8 +227,8 @@ int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
  *   (T [K], ln p [Pa], Y_0..Y_8, dt [s])  ->  (dY_0..dY_8, dT [K])
  * (12 -> 128 -> 128 -> 128 -> 10, GELU, BF16 weights and activations, FP32 accumulation,
  * standardised inputs and outputs) from samples the integrator writes during the run,
- * then replaces it cell by cell: the predicted dY is projected onto changes that conserve
- * every element, cells whose features leave the training box (widened by 5 %) or whose
+ * then replaces it cell by cell: the predicted dY is projected (orthogonally) onto changes
+ * that conserve every element, cells whose features leave the training box (widened by 5 %) or whose
  * prediction is not finite run the integrator, and 1 in audit_period cells (0: none) runs
  * it as well, takes its result and scores the prediction (L1 error of dY).
  *
@@ -237,10 +237,18 @@ int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
  *   of `capacity` rows; collection stops when it is full.
  * lbmgpu_surrogate_load_samples: replaces the sample set by n host rows (x: n x 12 raw
  *   features, y: n x 10 raw targets).
+ * lbmgpu_surrogate_samples: copies the first n rows of the sample set to the host (x, y as
+ *   above; valid[r] = 1 where row r was written); n <= the report's `samples`.
+ * lbmgpu_surrogate_augment: appends n rows made from random valid rows of the sample set
+ *   (the set grows as needed): mass fractions below y_trace multiplied by exp(U(-span_y,
+ *   span_y)), T by exp(U(-span_t, span_t)), at the source row's density, renormalised,
+ *   and labelled by the integrator -- states near the visited ones that the run has not
+ *   reached yet, so the network learns how the step depends on each input there.
  * lbmgpu_surrogate_train: Adam (beta 0.9/0.999) on the mean squared standardised error,
  *   `epochs` passes over the samples in shuffled minibatches of `batch` (a multiple of 64)
- *   rows; the standardisation and gate box are fitted on the first call or with refit;
- *   *loss = the last epoch's mean loss.
+ *   rows, the step size decaying from lr to 0 along a half cosine over the call; the
+ *   standardisation and gate box are fitted on the first call or with refit; *loss = the
+ *   last epoch's mean loss.
  * lbmgpu_surrogate_enable: the surrogate on (after training) or off; resets the audit
  *   counters of lbmgpu_surrogate_stats.
  * lbmgpu_surrogate_eval: the network on n host rows of raw features (x: n x 12) ->
@@ -264,6 +272,8 @@ typedef struct lbmgpu_surrogate_report {
 } lbmgpu_surrogate_report;
 int lbmgpu_surrogate_collect(lbmgpu_t *h, int enable, int stride, long capacity);
 int lbmgpu_surrogate_load_samples(lbmgpu_t *h, const float *x, const float *y, long n);
+int lbmgpu_surrogate_samples(lbmgpu_t *h, float *x, float *y, unsigned char *valid, long n);
+int lbmgpu_surrogate_augment(lbmgpu_t *h, long n, float span_y, float span_t, float y_trace, unsigned seed);
 int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigned seed, int refit, double *loss);
 int lbmgpu_surrogate_enable(lbmgpu_t *h, int enable, int audit_period);
 int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y);

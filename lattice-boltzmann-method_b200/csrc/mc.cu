@@ -383,6 +383,8 @@ int collide_t(lbmgpu *h) {
     const unsigned gp = grid_for(h->g.ncell);
     if (h->chem == CHEM_REF_EXPLICIT)
         k_mc_props<NS9, CHEM_REF_EXPLICIT, S><<<gp, kBlock, 0, h->stream>>>(A);
+    else if (h->chem == CHEM_ROSENBROCK && A.sur.mode == 1 && A.sur.ilist)
+        k_mc_props<NS9, CHEM_SURROGATE_STEP, S><<<gp, kBlock, 0, h->stream>>>(A);
     else if (h->chem == CHEM_ROSENBROCK)
         k_mc_props<NS9, CHEM_ROSENBROCK, S><<<gp, kBlock, 0, h->stream>>>(A);
     else

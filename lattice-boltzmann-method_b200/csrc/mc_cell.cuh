@@ -50,6 +50,9 @@ MC_HD int mc_nrec(int ns) { return RM_SP + RM_SPN * ns; }
 MC_HD int rs(int a, int f) { return RM_SP + RM_SPN * a + f; }
 
 enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1, CHEM_ROSENBROCK = 2 };
+// instance of the collision-parameter kernel for ROS2 handles with the surrogate on: every
+// cell the network does not cover goes to the integrator list, none is integrated inline
+constexpr int CHEM_SURROGATE_STEP = 3;
 
 template <typename P_, typename R_>
 struct McArgsT {
@@ -404,7 +407,7 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // prediction against it).  With `defer` and a list (sur.ilist) such cells are only
 // appended to the list -- k_mc_chem_list integrates them afterwards in dense warps --
 // otherwise they are integrated here.  Teacher steps (mode 0) can write samples.
-template <int NS, class AT>
+template <int NS, class AT, bool CAN_INTEGRATE = true>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
     const gas::Tables &t = *A.tab;
@@ -420,7 +423,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
             dY[a] = (double)pr[a];
             have_pred = have_pred && isfinite(dY[a]);
         }
-        if (have_pred) sur_conserve<NS>(S.elem, rho_a, kSpeciesMin, dY);
+        if (have_pred) sur_conserve<NS>(S.proj, dY);
         for (int a = 0; a < NS; ++a) Yp[a] = Y[a] + dY[a];
         Tp = T_si + (double)pr[NS];
     }
@@ -431,7 +434,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
         count_flag(&S.audit[5], !have_pred);
     }
     if (!have_pred || audit) {
-        if (defer && S.ilist) {
+        if (!CAN_INTEGRATE || (defer && S.ilist)) {
 #if defined(__CUDA_ARCH__)
             S.ilist[atomicAdd(S.icount, 1u)] = (int)n;
 #else
@@ -439,8 +442,10 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
 #endif
             return;
         }
-        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
-        if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
+        if (CAN_INTEGRATE) {
+            for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+            if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
+        }
     } else {
         for (int a = 0; a < NS; ++a) Yc[a] = Yp[a];
         Tc = Tp;
@@ -552,6 +557,8 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         put(A, A.rec_nxt, RM_HRR, n, hrr);
     } else if (CHEM == CHEM_ROSENBROCK) {
         mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
+    } else if (CHEM == CHEM_SURROGATE_STEP) {
+        mc_chem_ros2<NS, AT, false>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
     }
 
     // -- species viscosities; Wilke weights phi_ab = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^1/4)^2 /

@@ -357,6 +357,56 @@ __global__ void k_gather_batch(const float *__restrict__ dx, const float *__rest
     vb[r] = ok ? 1 : 0;
 }
 
+// State-space augmentation.  New row i takes a random valid row of the sample set (the
+// source, drawn from the list src_rows of the n_src valid rows), multiplies each mass
+// fraction below y_trace by exp(U(-span_y, span_y)) and T by exp(U(-span_t, span_t)) at
+// the source's density, renormalises the mass fractions, and labels the perturbed state
+// with the integrator over the source's dt.  Rows whose integration fails are left invalid.
+__global__ void k_sur_augment(const gas::Tables *__restrict__ tab, float *__restrict__ ds_x, float *__restrict__ ds_y,
+                              uint8_t *__restrict__ ds_valid, const int *__restrict__ src_rows, long n_src, long base,
+                              long n_new, float span_y, float span_t, float y_trace, unsigned seed) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_new) return;
+    const long row = base + i;
+    unsigned hs = sur_hash((unsigned)i, seed);
+    const long src = src_rows[((unsigned long long)hs * (unsigned long long)n_src) >> 32];
+    const gas::Tables &t = *tab;
+    const float *xs = ds_x + src * kSurIn;
+    const double dt = xs[2 + 9];
+    double T = xs[0], Y[gas::MAXS], iw = 0.0;
+    for (int k = 0; k < 9; ++k) {
+        Y[k] = xs[2 + k];
+        iw += Y[k] / t.m.W[k];
+    }
+    const double rho = exp((double)xs[1]) / (gas::kR * T * iw);
+    auto uni = [&](unsigned salt) {  // uniform in [-1, 1)
+        hs = sur_hash(hs, salt);
+        return (double)hs * (2.0 / 4294967296.0) - 1.0;
+    };
+    double sum = 0.0;
+    for (int k = 0; k < 9; ++k) {
+        const double f = exp(span_y * uni(k + 1));
+        if (Y[k] < y_trace) Y[k] *= f;
+        sum += Y[k];
+    }
+    iw = 0.0;
+    for (int k = 0; k < 9; ++k) {
+        Y[k] /= sum;
+        iw += Y[k] / t.m.W[k];
+    }
+    T *= exp(span_t * uni(97));
+    sur_features<9>(T, rho * gas::kR * T * iw, Y, dt, ds_x + row * kSurIn);
+    double Yc[gas::MAXS], Tc = T;
+    for (int k = 0; k < 9; ++k) Yc[k] = Y[k];
+    if (gas::ros2_advance(t, rho, Yc, Tc, dt) < 0) {
+        ds_valid[row] = 0;
+        return;
+    }
+    for (int k = 0; k < 9; ++k) ds_y[row * kSurOut + k] = (float)(Yc[k] - Y[k]);
+    ds_y[row * kSurOut + 9] = (float)(Tc - T);
+    ds_valid[row] = 1;
+}
+
 inline unsigned blocks(long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 }  // namespace
@@ -371,7 +421,7 @@ struct SurState {
     __nv_bfloat16 *wb = nullptr;
     SurNorm *nrm = nullptr;
     SurNorm nrm_h{};
-    double *elem = nullptr;
+    double *proj = nullptr;
     double *audit = nullptr;
     // samples
     float *ds_x = nullptr, *ds_y = nullptr;
@@ -481,17 +531,20 @@ int sur_create(lbmgpu *h) {
     if (!rc) rc = dalloc(h, &s->g, kNParams);
     if (!rc) rc = dalloc(h, &s->wb, off_w(4));
     if (!rc) rc = dalloc(h, &s->nrm, 1);
-    if (!rc) rc = dalloc(h, &s->elem, 4 * 9);
+    if (!rc) rc = dalloc(h, &s->proj, 9 * 9);
     if (!rc) rc = dalloc(h, &s->audit, 6);
     if (rc) return rc;
     CK(cudaMemsetAsync(s->g, 0, kNParams * sizeof(float), h->stream));
     CK(cudaMemsetAsync(s->audit, 0, 6 * sizeof(double), h->stream));
     default_norm(s->nrm_h);
     CK(cudaMemcpyAsync(s->nrm, &s->nrm_h, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
-    double E[4 * 9];  // atoms of element e per unit mass of species k
-    for (int e = 0; e < 4; ++e)
-        for (int k = 0; k < 9; ++k) E[e * 9 + k] = h->mech.elements[k][e] / h->mech.W[k];
-    CK(cudaMemcpyAsync(s->elem, E, sizeof E, cudaMemcpyHostToDevice, h->stream));
+    double el[9][4], W[9], proj[9 * 9];
+    for (int k = 0; k < 9; ++k) {
+        W[k] = h->mech.W[k];
+        for (int e = 0; e < 4; ++e) el[k][e] = h->mech.elements[k][e];
+    }
+    sur_projector<9>(el, W, proj);
+    CK(cudaMemcpyAsync(s->proj, proj, sizeof proj, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return init_params(h, 20261203u);
 }
@@ -505,7 +558,7 @@ void sur_release(lbmgpu *h) {
     cudaFree(s->g);
     cudaFree(s->wb);
     cudaFree(s->nrm);
-    cudaFree(s->elem);
+    cudaFree(s->proj);
     cudaFree(s->audit);
     cudaFree(s->ds_x);
     cudaFree(s->ds_y);
@@ -527,7 +580,7 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
     std::memset(&a, 0, sizeof a);
     SurState *s = h->sur;
     if (!s || h->chem != CHEM_ROSENBROCK) return 0;
-    a.elem = s->elem;
+    a.proj = s->proj;
     a.audit = s->audit;
     a.audit_period = s->audit_period;
     a.step = s->step;
@@ -671,6 +724,40 @@ int ensure_samples(lbmgpu *h, long cap) {
     return 0;
 }
 
+// Grows the sample set to at least cap rows, keeping the rows written so far.
+int grow_samples(lbmgpu *h, long cap) {
+    SurState &s = *h->sur;
+    if (s.ds_cap >= cap && s.ds_x) return 0;
+    const long keep = s.ds_x ? std::min(s.ds_next, s.ds_cap) : 0;
+    float *x = nullptr, *y = nullptr;
+    uint8_t *v = nullptr;
+    int rc = dalloc(h, &x, (size_t)cap * kSurIn);
+    if (!rc) rc = dalloc(h, &y, (size_t)cap * kSurOut);
+    if (!rc) rc = dalloc(h, &v, (size_t)cap);
+    if (rc) {
+        cudaFree(x);
+        cudaFree(y);
+        cudaFree(v);
+        return rc;
+    }
+    CK(cudaMemsetAsync(v, 0, (size_t)cap, h->stream));
+    if (keep) {
+        CK(cudaMemcpyAsync(x, s.ds_x, (size_t)keep * kSurIn * 4, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(y, s.ds_y, (size_t)keep * kSurOut * 4, cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(v, s.ds_valid, (size_t)keep, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    cudaFree(s.ds_x);
+    cudaFree(s.ds_y);
+    cudaFree(s.ds_valid);
+    s.ds_x = x;
+    s.ds_y = y;
+    s.ds_valid = v;
+    s.ds_cap = cap;
+    s.ds_next = keep;
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -705,6 +792,52 @@ int lbmgpu_surrogate_load_samples(lbmgpu_t *h, const float *x, const float *y, l
     if (s.ds_cap > n) CK(cudaMemsetAsync(s.ds_valid + n, 0, (size_t)(s.ds_cap - n), h->stream));
     CK(cudaStreamSynchronize(h->stream));
     s.ds_next = n;
+    s.collect = 0;
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_samples(lbmgpu_t *h, float *x, float *y, unsigned char *valid, long n) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    SurState &s = *h->sur;
+    if (n < 0 || n > std::min(s.ds_next, s.ds_cap) || (n > 0 && (!x || !y || !valid))) return LBMGPU_E_ARG;
+    if (n == 0) return LBMGPU_OK;
+    CK(cudaMemcpyAsync(x, s.ds_x, (size_t)n * kSurIn * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(y, s.ds_y, (size_t)n * kSurOut * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(valid, s.ds_valid, (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return LBMGPU_OK;
+}
+
+int lbmgpu_surrogate_augment(lbmgpu_t *h, long n, float span_y, float span_t, float y_trace, unsigned seed) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (h->chem != CHEM_ROSENBROCK) return LBMGPU_E_UNSUPPORTED;
+    SurState &s = *h->sur;
+    if (n < 1 || !(span_y >= 0.f) || !(span_t >= 0.f) || !(y_trace >= 0.f)) return LBMGPU_E_ARG;
+    const long n_rows = s.ds_x ? std::min(s.ds_next, s.ds_cap) : 0;
+    if (n_rows < 1) return LBMGPU_E_STATE;
+    std::vector<uint8_t> v(n_rows);
+    CK(cudaMemcpyAsync(v.data(), s.ds_valid, n_rows, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    std::vector<int> src;
+    for (long r = 0; r < n_rows; ++r)
+        if (v[r]) src.push_back((int)r);
+    if (src.empty()) return LBMGPU_E_STATE;
+    rc = grow_samples(h, n_rows + n);
+    if (rc) return rc;
+    int *src_d = nullptr;
+    rc = dalloc(h, &src_d, src.size());
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(src_d, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    k_sur_augment<<<blocks(n, 128), 128, 0, h->stream>>>(h->tab, s.ds_x, s.ds_y, s.ds_valid, src_d, (long)src.size(),
+                                                         n_rows, n, span_y, span_t, y_trace, seed);
+    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e2 = cudaStreamSynchronize(h->stream);
+    cudaFree(src_d);
+    CK(e);
+    CK(e2);
+    s.ds_next = n_rows + n;
     s.collect = 0;
     return LBMGPU_OK;
 }
@@ -769,6 +902,9 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
     const int kin[4] = {kSurInPad, kSurHid, kSurHid, kSurHid};
     const int nout[4] = {kSurHid, kSurHid, kSurHid, kSurOutPad};
     dim3 tb(32, 8);
+    // the step size decays from lr to 0 along a half cosine over the call's Adam steps
+    const long nbatch = ((long)rows.size() + B - 1) / B, total = std::max<long>(1, (long)epochs * nbatch);
+    long step_in_call = 0;
     for (int ep = 0; ep < epochs && !rc; ++ep) {
         std::shuffle(rows.begin(), rows.end(), rng);
         double sum_se = 0.0;
@@ -820,12 +956,15 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
             }
             // Adam step over every parameter (padding entries have zero gradient)
             s.adam_t += 1;
+            const float lr_t =
+                (float)(0.5 * lr * (1.0 + std::cos(3.14159265358979323846 * (double)step_in_call / (double)total)));
+            ++step_in_call;
             const float c1 = 1.f - (float)std::pow(b1, (double)s.adam_t), c2 = 1.f - (float)std::pow(b2, (double)s.adam_t);
             for (int t = 0; t < 8; ++t) {
                 const size_t sz[8] = {kW1, kW2, kW2, kW4, kSurHid, kSurHid, kSurHid, kSurOutPad};
                 const size_t o = off_w(t);
                 k_adam<<<blocks((long)sz[t]), 256, 0, h->stream>>>(s.w + o, s.m + o, s.v + o, s.g + o,
-                                                                   t < 4 ? s.wb + o : nullptr, (long)sz[t], lr, b1, b2,
+                                                                   t < 4 ? s.wb + o : nullptr, (long)sz[t], lr_t, b1, b2,
                                                                    c1, c2, eps);
             }
             if (cudaGetLastError() != cudaSuccess) {

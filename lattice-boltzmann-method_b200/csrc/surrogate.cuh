@@ -34,7 +34,7 @@ struct SurArgs {
                                // of the former (bits), [3] audited, [4] predicted, [5] integrated
     unsigned audit_period;     // 1 in audit_period cells (by a hash of cell and step) is audited
     unsigned step;
-    const double *elem;        // [4][9] atoms of element e per unit mass of species k: E_ek / W_k
+    const double *proj;        // [9][9] projector onto element-conserving changes (sur_projector)
     // sample collection (teacher steps): cells with n % ds_stride == ds_phase write their
     // (features, targets) to row ds_base + n / ds_stride while below ds_cap
     float *ds_x, *ds_y;        // [ds_cap][kSurIn], [ds_cap][kSurOut]
@@ -55,65 +55,71 @@ __host__ __device__ inline void sur_features(double T_si, double P_si, const dou
     x[2 + NS] = (float)dt_si;
 }
 
-// The predicted change dY made exactly element-conserving: species already at the floor
-// (rho_a <= floor) whose prediction is negative are held at zero change -- the LBM would
-// drop such a change (the species collision's skip rule), which is what would break the
-// balance -- and the others take the smallest correction that restores
-//   sum_k E_ek / W_k dY_k = 0   for every element e,
-// dY_free -= A_f^T (A_f A_f^T)^-1 A_f dY_free over the elements the free species carry.
+// The orthogonal projector onto element-conserving changes of the mass fractions,
+//   P = I - A^T (A A^T)^-1 A,   A_ek = E_ek / W_k (atoms of element e per unit mass of k),
+// over the elements some species carries; A P = 0, so P dY conserves every element to
+// rounding, and a dY that already conserves them comes back unchanged.  Formed once on the
+// host from the mechanism (Gauss-Jordan elimination with partial pivoting on the small,
+// symmetric positive definite A A^T); proj is row-major [NS][NS].
 template <int NS>
-__host__ __device__ inline void sur_conserve(const double *elem, const double *rho_a, double floor_rho, double *dY) {
-    bool fixed[NS];
-    for (int k = 0; k < NS; ++k) {
-        fixed[k] = rho_a[k] <= floor_rho && dY[k] < 0.0;
-        if (fixed[k]) dY[k] = 0.0;
-    }
-    // elements carried by some free species
-    int rows[4], ne = 0;
+inline void sur_projector(const double (*elements)[4], const double *W, double *proj) {
+    double A[4][NS];
+    int ne = 0;
     for (int e = 0; e < 4; ++e) {
         bool any = false;
-        for (int k = 0; k < NS; ++k) any = any || (!fixed[k] && elem[e * NS + k] != 0.0);
-        if (any) rows[ne++] = e;
+        for (int k = 0; k < NS; ++k) any = any || elements[k][e] != 0.0;
+        if (!any) continue;
+        for (int k = 0; k < NS; ++k) A[ne][k] = elements[k][e] / W[k];
+        ++ne;
     }
-    if (ne == 0) return;
-    double G[4][5];  // [G | r]
-    for (int i = 0; i < ne; ++i) {
+    double G[4][8];  // [A A^T | I] -> [I | (A A^T)^-1]
+    for (int i = 0; i < ne; ++i)
         for (int j = 0; j < ne; ++j) {
             double g = 0.0;
-            for (int k = 0; k < NS; ++k)
-                if (!fixed[k]) g += elem[rows[i] * NS + k] * elem[rows[j] * NS + k];
+            for (int k = 0; k < NS; ++k) g += A[i][k] * A[j][k];
             G[i][j] = g;
+            G[i][ne + j] = i == j ? 1.0 : 0.0;
         }
-        double r = 0.0;
-        for (int k = 0; k < NS; ++k) r += elem[rows[i] * NS + k] * dY[k];
-        G[i][ne] = r;
-    }
-    for (int c = 0; c < ne; ++c) {  // Gaussian elimination with partial pivoting (G is SPD)
+    for (int c = 0; c < ne; ++c) {
         int p = c;
         for (int r = c + 1; r < ne; ++r)
             if (fabs(G[r][c]) > fabs(G[p][c])) p = r;
-        for (int q = 0; q <= ne; ++q) {
+        for (int q = 0; q < 2 * ne; ++q) {
             const double tmp = G[c][q];
             G[c][q] = G[p][q];
             G[p][q] = tmp;
         }
-        for (int r = c + 1; r < ne; ++r) {
-            const double f = G[r][c] / G[c][c];
-            for (int q = c; q <= ne; ++q) G[r][q] -= f * G[c][q];
+        const double piv = G[c][c];
+        for (int q = 0; q < 2 * ne; ++q) G[c][q] /= piv;
+        for (int r = 0; r < ne; ++r) {
+            if (r == c) continue;
+            const double f = G[r][c];
+            for (int q = 0; q < 2 * ne; ++q) G[r][q] -= f * G[c][q];
         }
     }
-    double lam[4];
-    for (int r = ne - 1; r >= 0; --r) {
-        double v = G[r][ne];
-        for (int q = r + 1; q < ne; ++q) v -= G[r][q] * lam[q];
-        lam[r] = v / G[r][r];
-    }
+    for (int k = 0; k < NS; ++k)
+        for (int l = 0; l < NS; ++l) {
+            double v = k == l ? 1.0 : 0.0;
+            for (int i = 0; i < ne; ++i)
+                for (int j = 0; j < ne; ++j) v -= A[i][k] * G[i][ne + j] * A[j][l];
+            proj[k * NS + l] = v;
+        }
+}
+
+// The predicted change dY made exactly element-conserving: dY <- P dY (the smallest
+// correction in the L2 sense).  Species at the density floor are treated like the others:
+// the LBM's species collision drops a negative change of a floored species whichever
+// chemistry produced it, so the surrogate's change goes through the same rule as the
+// integrator's.
+template <int NS>
+__host__ __device__ inline void sur_conserve(const double *proj, double *dY) {
+    double out[NS];
     for (int k = 0; k < NS; ++k) {
-        if (fixed[k]) continue;
-        double corr = 0.0;
-        for (int i = 0; i < ne; ++i) corr += elem[rows[i] * NS + k] * lam[i];
-        dY[k] -= corr;
+        double v = 0.0;
+        for (int l = 0; l < NS; ++l) v += proj[k * NS + l] * dY[l];
+        out[k] = v;
     }
+    for (int k = 0; k < NS; ++k) dY[k] = out[k];
 }
 
 __host__ __device__ inline unsigned sur_hash(unsigned a, unsigned b) {

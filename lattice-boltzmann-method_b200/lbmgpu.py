@@ -37,7 +37,8 @@ EXPORTS = [
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
     "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums", "lbmgpu_sums_noalloc",
-    "lbmgpu_surrogate_collect", "lbmgpu_surrogate_load_samples", "lbmgpu_surrogate_train",
+    "lbmgpu_surrogate_collect", "lbmgpu_surrogate_load_samples", "lbmgpu_surrogate_samples",
+    "lbmgpu_surrogate_augment", "lbmgpu_surrogate_train",
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
 ]
 SUMS_MAX = 21
@@ -109,6 +110,9 @@ def lib():
         fp = ctypes.POINTER(ctypes.c_float)
         L.lbmgpu_surrogate_collect.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_long]
         L.lbmgpu_surrogate_load_samples.argtypes = [vp, fp, fp, ctypes.c_long]
+        L.lbmgpu_surrogate_samples.argtypes = [vp, fp, fp, ctypes.POINTER(ctypes.c_ubyte), ctypes.c_long]
+        L.lbmgpu_surrogate_augment.argtypes = [vp, ctypes.c_long, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                               ctypes.c_uint]
         L.lbmgpu_surrogate_train.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint,
                                              ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         L.lbmgpu_surrogate_enable.argtypes = [vp, ctypes.c_int, ctypes.c_int]
@@ -290,8 +294,29 @@ class Lattice:
         _check(lib().lbmgpu_surrogate_load_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp), len(x)),
                "lbmgpu_surrogate_load_samples")
 
+    def surrogate_samples(self, n=None):
+        """The first n rows (all by default) of the sample set: (x (n, 12), y (n, 10), valid (n,))."""
+        import numpy as np
+        if n is None:
+            n = self.surrogate_stats()["samples"]
+        x = np.zeros((n, SUR_IN), np.float32)
+        y = np.zeros((n, SUR_OUT), np.float32)
+        v = np.zeros(n, np.uint8)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(lib().lbmgpu_surrogate_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp),
+                                              v.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), n),
+               "lbmgpu_surrogate_samples")
+        return x, y, v.astype(bool)
+
+    def surrogate_augment(self, n, span_y=1.5, span_t=0.01, y_trace=1e-3, seed=1):
+        """Appends n integrator-labelled rows perturbed from random valid sample rows (mass
+        fractions below y_trace by exp(U(-span_y, span_y)), T by exp(U(-span_t, span_t)))."""
+        _check(lib().lbmgpu_surrogate_augment(self.h, int(n), float(span_y), float(span_t), float(y_trace), int(seed)),
+               "lbmgpu_surrogate_augment")
+
     def surrogate_train(self, epochs=10, batch=4096, lr=1e-3, seed=1, refit=False):
-        """Adam epochs over the sample set; returns the last epoch's mean standardised loss."""
+        """Adam epochs over the sample set (step size lr decaying to 0 along a half cosine);
+        returns the last epoch's mean standardised loss."""
         loss = ctypes.c_double()
         _check(lib().lbmgpu_surrogate_train(self.h, int(epochs), int(batch), float(lr), int(seed), int(refit),
                                             ctypes.byref(loss)), "lbmgpu_surrogate_train")

@@ -136,7 +136,26 @@ extern "C" int mc_host_run32(int Nx, int Ny, int Nz, const signed char *type, co
                               nullptr);
 }
 
-// The surrogate's element-conserving correction of a predicted dY (surrogate.cuh).
-extern "C" void sur_conserve_host(const double *elem, const double *rho_a, double floor_rho, double *dY) {
-    lbm::sur_conserve<9>(elem, rho_a, floor_rho, dY);
+// The surrogate's element-conserving projector and its application (surrogate.cuh).
+extern "C" void sur_projector_host(const lbmgpu_mech *mech, double *proj) {
+    double el[9][4], W[9];
+    for (int k = 0; k < 9; ++k) {
+        W[k] = mech->W[k];
+        for (int e = 0; e < 4; ++e) el[k][e] = mech->elements[k][e];
+    }
+    lbm::sur_projector<9>(el, W, proj);
+}
+
+extern "C" void sur_conserve_host(const double *proj, double *dY) { lbm::sur_conserve<9>(proj, dY); }
+
+// One ROS2 step (chem.cuh) of a constant-volume adiabatic reactor per row: rho [kg/m^3],
+// Y [n][9] and T [n] [K] advanced in place over dt [s].  Returns the number of rows whose
+// integration failed.
+extern "C" long ros2_host(const lbmgpu_mech *mech, long n, const double *rho, double *Y, double *T, double dt) {
+    static gas::Tables tab;
+    gas::make_tables(*mech, tab);
+    long bad = 0;
+    for (long r = 0; r < n; ++r)
+        if (gas::ros2_advance(tab, rho[r], Y + 9 * r, T[r], dt) < 0) ++bad;
+    return bad;
 }

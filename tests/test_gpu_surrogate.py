@@ -182,3 +182,46 @@ def test_surrogate_replaces_the_integrator_on_the_reacting_fixture():
     assert np.all(np.abs(e_sur - e0) <= 1e-8 * np.abs(e0)), e_sur - e0
     print("surrogate audit: relative L1 error of dY", audit_err)
     assert audit_err < 0.05, audit_err
+
+
+def test_surrogate_augment_rows_are_integrator_labelled(tmp_path):
+    """lbmgpu_surrogate_augment: the appended rows are perturbed states (mass fractions
+    summing to 1, T within the requested factor of the source rows' range) labelled by the
+    integrator -- the host build of the same ROS2 step (tests/host/mc_host.cpp, ros2_host),
+    started from each row's stored features, gives the same dY and dT to the rounding of
+    the FP32 feature storage."""
+    import ctypes
+
+    from mc_common import build_host_lib
+    lat, m, mix, sp = lattice()
+    with lat:
+        lat.upload(mix, sp)
+        lat.init()
+        lat.surrogate_collect(True, stride=1, capacity=mix.size * 4)
+        lat.step(4)
+        assert lat.synchronize() == 0
+        lat.surrogate_collect(False)
+        n0 = lat.surrogate_stats()["samples"]
+        lat.surrogate_augment(3000, span_y=1.5, span_t=0.01, y_trace=1e-3, seed=3)
+        assert lat.surrogate_stats()["samples"] == n0 + 3000
+        x, y, v = lat.surrogate_samples()
+    src_x = x[:n0][v[:n0]]
+    ax, ay = x[n0:][v[n0:]].astype(np.float64), y[n0:][v[n0:]].astype(np.float64)
+    assert v[n0:].mean() > 0.99
+    assert np.abs(ax[:, 2:11].sum(1) - 1.0).max() < 1e-5
+    assert ax[:, 0].min() >= src_x[:, 0].min() * np.exp(-0.0101)
+    assert ax[:, 0].max() <= src_x[:, 0].max() * np.exp(0.0101)
+    L = build_host_lib(tmp_path)
+    L.ros2_host.restype = ctypes.c_long
+    L.ros2_host.argtypes = [ctypes.POINTER(mech.Mech), ctypes.c_long] + [ctypes.c_void_p] * 3 + [ctypes.c_double]
+    Wk = np.array([m.W[k] for k in range(9)])
+    Y = np.ascontiguousarray(ax[:, 2:11])
+    T = np.ascontiguousarray(ax[:, 0])
+    rho = np.ascontiguousarray(np.exp(ax[:, 1]) / (8314.46261815324 * T * (Y / Wk).sum(1)))
+    Y0, T0 = Y.copy(), T.copy()
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    assert L.ros2_host(ctypes.byref(m), len(T), P(rho), P(Y), P(T), float(ax[0, 11])) == 0
+    dY, dT = Y - Y0, T - T0
+    err = np.abs(dY[:, :8] - ay[:, :8]).sum() / np.abs(dY[:, :8]).sum()
+    assert err < 1e-4, err
+    assert np.abs(dT - ay[:, 9]).max() <= 1e-4 * np.abs(dT).max() + 1e-6

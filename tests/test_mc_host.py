@@ -164,32 +164,32 @@ def test_host_fp32_storage_with_boundaries(hostlib, fixture):
 
 
 def test_surrogate_correction_conserves_elements_exactly(hostlib):
-    """sur_conserve (the correction the surrogate's prediction gets before use): after it,
-    sum_k E_ek / W_k dY_k = 0 for H, O, N to rounding; species at the density floor with a
-    negative prediction get exactly zero change; a prediction that already conserves the
-    elements and touches no floored species comes back unchanged (to rounding)."""
+    """sur_conserve (the correction the surrogate's prediction gets before use) with the
+    projector sur_projector forms from the mechanism: after it, sum_k E_ek / W_k dY_k = 0
+    for H, O, N to rounding; the projector is I - A^T (A A^T)^-1 A over the elements the
+    species carry (numpy, to 1e-12); a prediction that already conserves the elements comes
+    back unchanged (to rounding)."""
     import ctypes
     import mech
     m = mech.h2_air_9()
     E = np.array([[m.elements[k][e] / m.W[k] for k in range(NS)] for e in range(4)])
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    proj = np.zeros(NS * NS)
+    hostlib.sur_projector_host(ctypes.byref(m), P(proj))
+    proj = proj.reshape(NS, NS)
+    A = E[np.abs(E).sum(1) > 0]
+    want = np.eye(NS) - A.T @ np.linalg.solve(A @ A.T, A)
+    assert np.abs(proj - want).max() <= 1e-12 * np.abs(want).max()
     rng = np.random.default_rng(17)
     for trial in range(200):
-        rho_a = rng.uniform(1e-9, 1e-2, NS)
-        floored = rng.random(NS) < 0.3
-        rho_a[floored] = 1e-8
         dY0 = rng.normal(size=NS) * 10.0 ** rng.uniform(-9, -3, NS)
         dY = dY0.copy()
-        hostlib.sur_conserve_host(P(np.ascontiguousarray(E)), P(rho_a), ctypes.c_double(1e-8), P(dY))
+        hostlib.sur_conserve_host(P(np.ascontiguousarray(proj)), P(dY))
         scale = np.abs(E).max(1) * np.abs(dY0).max()
         assert np.all(np.abs(E @ dY) <= 1e-13 * scale + 1e-300), (trial, E @ dY)
-        fixed = floored & (dY0 < 0)
-        assert np.all(dY[fixed] == 0.0)
-    # a conserving prediction without floored negatives is kept
-    rho_a = np.full(NS, 1e-3)
-    A = E[:3]
-    null = np.linalg.svd(A)[2][3:].T  # basis of element-conserving changes
+    # a conserving prediction is kept
+    null = np.linalg.svd(A)[2][A.shape[0]:].T  # basis of element-conserving changes
     dY0 = null @ rng.normal(size=null.shape[1]) * 1e-5
     dY = dY0.copy()
-    hostlib.sur_conserve_host(P(np.ascontiguousarray(E)), P(rho_a), ctypes.c_double(1e-8), P(dY))
+    hostlib.sur_conserve_host(P(np.ascontiguousarray(proj)), P(dY))
     assert np.abs(dY - dY0).max() <= 1e-12 * np.abs(dY0).max()
