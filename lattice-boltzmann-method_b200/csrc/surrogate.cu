@@ -11,7 +11,10 @@
 //   k_sur_mlp   the whole network for a batch of cells in one kernel: the weights are
 //               staged once per block in shared memory, each warp carries 16 cells through
 //               the four layers with the activations in registers (the accumulator
-//               fragment of one layer is the operand fragment of the next);
+//               fragment of one layer is the operand fragment of the next); the first
+//               layer takes each standardised feature as a BF16 value plus a BF16
+//               remainder, two k-slices against the same W1, so the inputs (T above all:
+//               BF16 alone would round 1700 K by several kelvin) enter at ~16 bits;
 //   k_gemm_tn   C = A B^T for training (forward, input gradients, weight gradients);
 //   elementwise bias/GELU forward and backward, the MSE loss gradient, column sums for
 //   the bias gradients, Adam on FP32 master weights with BF16 copies.
@@ -35,6 +38,8 @@ namespace {
 
 constexpr int kSurBlock = 128;                 // 4 warps, 16 cells each per tile
 constexpr int kW1 = kSurHid * kSurInPad;       // elements of the padded weight tensors
+constexpr int kW1Ld = kSurInX + 8;             // row stride of W1 in shared memory: [W1 | W1 | pad]
+constexpr int kW1s = kSurHid * kW1Ld;
 constexpr int kW2 = kSurHid * kSurLd;
 constexpr int kW4 = kSurOutPad * kSurLd;
 constexpr int kNParams = kW1 + 2 * kW2 + kW4 + 3 * kSurHid + kSurOutPad;
@@ -55,6 +60,14 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
 __host__ __device__ inline float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
 __device__ inline float gelu_grad(float z) {
     return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// A standardised feature into slot q of a network input row: its BF16 value and the BF16
+// remainder.
+__device__ __forceinline__ void put_split(__nv_bfloat16 *row, int q, float v) {
+    const __nv_bfloat16 hi = __float2bfloat16(v);
+    row[q] = hi;
+    row[kSurInPad + q] = __float2bfloat16(v - __bfloat162float(hi));
 }
 
 // -------------------------------------------------------------------------------------
@@ -84,11 +97,11 @@ __global__ void k_sur_features(McArgsT<S, double> A, const SurNorm *__restrict__
             x[q] = (x[q] - nrm->x_mean[q]) / nrm->x_std[q];
         }
     }
-    for (int q = 0; q < kSurInPad; ++q) X[n * kSurInPad + q] = __float2bfloat16(x[q]);
+    for (int q = 0; q < kSurInPad; ++q) put_split(X + n * kSurInX, q, x[q]);
     if (n < A.ncell) gate[n] = out_of_box ? 1 : 0;
 }
 
-// Raw features (rows of kSurIn floats) -> standardised BF16 rows.
+// Raw features (rows of kSurIn floats) -> standardised network input rows.
 __global__ void k_sur_standardise(const float *__restrict__ x, long m, long mpad, const SurNorm *__restrict__ nrm,
                                   __nv_bfloat16 *__restrict__ X) {
     const long r = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,7 +109,7 @@ __global__ void k_sur_standardise(const float *__restrict__ x, long m, long mpad
     for (int q = 0; q < kSurInPad; ++q) {
         float v = 0.f;
         if (r < m && q < kSurIn) v = (x[r * kSurIn + q] - nrm->x_mean[q]) / nrm->x_std[q];
-        X[r * kSurInPad + q] = __float2bfloat16(v);
+        put_split(X + r * kSurInX, q, v);
     }
 }
 
@@ -141,13 +154,13 @@ __device__ __forceinline__ void gelu_to_frag(const float (*acc)[4], unsigned (*a
     }
 }
 
-// X [mpad][16] standardised BF16 -> pred [mpad][16] in SI units (outputs 10..15 zero).
+// X [mpad][kSurInX] network input rows -> pred [mpad][16] in SI units (outputs 10..15 zero).
 __global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm *__restrict__ nrm,
                                                        const __nv_bfloat16 *__restrict__ X, float *__restrict__ pred,
                                                        long ntiles) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16 *w1 = reinterpret_cast<__nv_bfloat16 *>(smem);
-    __nv_bfloat16 *w2 = w1 + kW1;
+    __nv_bfloat16 *w1 = reinterpret_cast<__nv_bfloat16 *>(smem);  // [128][kW1Ld]: W1 for values and remainders
+    __nv_bfloat16 *w2 = w1 + kW1s;
     __nv_bfloat16 *w3 = w2 + kW2;
     __nv_bfloat16 *w4 = w3 + kW2;
     float *bb = reinterpret_cast<float *>(w4 + kW4);  // b1 b2 b3 (128 each), b4 (16), y_mean, y_std
@@ -156,8 +169,13 @@ __global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm
                                   reinterpret_cast<const unsigned *>(net.w3), reinterpret_cast<const unsigned *>(net.w4)};
         unsigned *dst[4] = {reinterpret_cast<unsigned *>(w1), reinterpret_cast<unsigned *>(w2),
                             reinterpret_cast<unsigned *>(w3), reinterpret_cast<unsigned *>(w4)};
-        const int cnt[4] = {kW1 / 2, kW2 / 2, kW2 / 2, kW4 / 2};
-        for (int t = 0; t < 4; ++t)
+        for (int i = threadIdx.x; i < kW1 / 2; i += kSurBlock) {  // W1 row r, word c, into both halves
+            const int r = i / (kSurInPad / 2), c = i % (kSurInPad / 2);
+            dst[0][r * (kW1Ld / 2) + c] = src[0][i];
+            dst[0][r * (kW1Ld / 2) + kSurInPad / 2 + c] = src[0][i];
+        }
+        const int cnt[4] = {0, kW2 / 2, kW2 / 2, kW4 / 2};
+        for (int t = 1; t < 4; ++t)
             for (int i = threadIdx.x; i < cnt[t]; i += kSurBlock) dst[t][i] = src[t][i];
         for (int i = threadIdx.x; i < kSurHid; i += kSurBlock) {
             bb[i] = net.b1[i];
@@ -175,17 +193,18 @@ __global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm
     const float *ym = bb + 3 * kSurHid + kSurOutPad, *ys = ym + kSurOutPad;
     for (long tile = (long)blockIdx.x * 4 + warp; tile < ntiles; tile += (long)gridDim.x * 4) {
         const long r0 = tile * 16;
-        unsigned a1[1][4];
-        {
-            const __nv_bfloat16 *xr = X + (r0 + gid) * kSurInPad + 2 * tig;
-            a1[0][0] = *reinterpret_cast<const unsigned *>(xr);
-            a1[0][1] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInPad);
-            a1[0][2] = *reinterpret_cast<const unsigned *>(xr + 8);
-            a1[0][3] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInPad + 8);
+        unsigned a1[2][4];  // k-slice 0: the feature values, 1: the remainders
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const __nv_bfloat16 *xr = X + (r0 + gid) * kSurInX + kSurInPad * s + 2 * tig;
+            a1[s][0] = *reinterpret_cast<const unsigned *>(xr);
+            a1[s][1] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInX);
+            a1[s][2] = *reinterpret_cast<const unsigned *>(xr + 8);
+            a1[s][3] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInX + 8);
         }
         float acc[kSurHid / 8][4];
         unsigned afr[kSurHid / 16][4];
-        mlp_layer<1, kSurHid / 8, kSurInPad>(a1, w1, bb, acc, gid, tig);
+        mlp_layer<2, kSurHid / 8, kW1Ld>(a1, w1, bb, acc, gid, tig);
         gelu_to_frag(acc, afr);
         mlp_layer<kSurHid / 16, kSurHid / 8, kSurLd>(afr, w2, bb + kSurHid, acc, gid, tig);
         gelu_to_frag(acc, afr);
@@ -205,16 +224,16 @@ __global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm
     }
 }
 
-constexpr size_t kMlpSmem = (size_t)(kW1 + 2 * kW2 + kW4) * 2 + (size_t)(3 * kSurHid + 3 * kSurOutPad) * 4;
+constexpr size_t kMlpSmem = (size_t)(kW1s + 2 * kW2 + kW4) * 2 + (size_t)(3 * kSurHid + 3 * kSurOutPad) * 4;
 
 // -------------------------------------------------------------------------------------
 // Training kernels.
 // -------------------------------------------------------------------------------------
-// C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T, A and B BF16 row-major with leading dimensions
-// lda, ldb (even), K a multiple of 16.  Block: 4 warps, each 16 rows x 64 columns.
+// C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T (accum: C +=), A and B BF16 row-major with
+// leading dimensions lda, ldb (even), K a multiple of 16.  Block: 4 warps, each 16 rows x 64 columns.
 __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict__ Am, int lda,
                                                  const __nv_bfloat16 *__restrict__ Bm, int ldb, float *__restrict__ C,
-                                                 int ldc, int M, int N, int K) {
+                                                 int ldc, int M, int N, int K, int accum = 0) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
     const int r0 = blockIdx.y * 64 + warp * 16, n0 = blockIdx.x * 64;
     float acc[8][4] = {};
@@ -241,8 +260,9 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int r = r0 + gid + 8 * h, c = n0 + 8 * j + 2 * tig;
-            if (r < M && c < N) C[(long)r * ldc + c] = acc[j][2 * h];
-            if (r < M && c + 1 < N) C[(long)r * ldc + c + 1] = acc[j][2 * h + 1];
+            if (r < M && c < N) C[(long)r * ldc + c] = acc[j][2 * h] + (accum ? C[(long)r * ldc + c] : 0.f);
+            if (r < M && c + 1 < N)
+                C[(long)r * ldc + c + 1] = acc[j][2 * h + 1] + (accum ? C[(long)r * ldc + c + 1] : 0.f);
         }
 }
 
@@ -340,7 +360,7 @@ __global__ void k_adam(float *__restrict__ w, float *__restrict__ m, float *__re
     if (wb) wb[i] = __float2bfloat16(wi);
 }
 
-// Batch rows from the sample set: standardised BF16 features and FP32 targets.
+// Batch rows from the sample set: network input rows and standardised FP32 targets.
 __global__ void k_gather_batch(const float *__restrict__ dx, const float *__restrict__ dy, const int *__restrict__ idx,
                                int nb, int B, const SurNorm *__restrict__ nrm, __nv_bfloat16 *__restrict__ Xb,
                                float *__restrict__ Yb, uint8_t *__restrict__ vb) {
@@ -350,7 +370,7 @@ __global__ void k_gather_batch(const float *__restrict__ dx, const float *__rest
     const long s = ok ? idx[r] : 0;
     for (int q = 0; q < kSurInPad; ++q) {
         const float v = (ok && q < kSurIn) ? (dx[s * kSurIn + q] - nrm->x_mean[q]) / nrm->x_std[q] : 0.f;
-        Xb[(long)r * kSurInPad + q] = __float2bfloat16(v);
+        put_split(Xb + (long)r * kSurInX, q, v);
     }
     for (int q = 0; q < kSurOutPad; ++q)
         Yb[(long)r * kSurOutPad + q] = (ok && q < kSurOut) ? (dy[s * kSurOut + q] - nrm->y_mean[q]) / nrm->y_std[q] : 0.f;
@@ -607,7 +627,7 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
             s->pred = nullptr;
             s->ilist = nullptr;
             s->icount = nullptr;
-            int rc = dalloc(h, &s->feat, (size_t)mpad * kSurInPad);
+            int rc = dalloc(h, &s->feat, (size_t)mpad * kSurInX);
             if (!rc) rc = dalloc(h, &s->gate, (size_t)mpad);
             if (!rc) rc = dalloc(h, &s->pred, (size_t)mpad * kSurOutPad);
             if (!rc) rc = dalloc(h, &s->ilist, (size_t)mpad);
@@ -873,7 +893,7 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
     const unsigned nparts = blocks((long)B * kSurOutPad);
     auto all = [&]() {
         int r = dalloc(h, &idx, B);
-        if (!r) r = dalloc(h, &Xb, (size_t)B * kSurInPad);
+        if (!r) r = dalloc(h, &Xb, (size_t)B * kSurInX);
         if (!r) r = dalloc(h, &Yb, (size_t)B * kSurOutPad);
         if (!r) r = dalloc(h, &vb, B);
         if (!r) r = dalloc(h, &H1, BH);
@@ -924,7 +944,10 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
             const float *bs[4] = {net.b1, net.b2, net.b3, net.b4};
             for (int L = 0; L < 3; ++L) {
                 k_gemm_tn<<<dim3((nout[L] + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(
-                    in, L == 0 ? kSurInPad : kSurHid, Ws[L], ldw[L], C, kSurHid, B, nout[L], kin[L]);
+                    in, L == 0 ? kSurInX : kSurHid, Ws[L], ldw[L], C, kSurHid, B, nout[L], kin[L]);
+                if (L == 0)  // the remainders' share of the first layer
+                    k_gemm_tn<<<dim3((nout[0] + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(
+                        Xb + kSurInPad, kSurInX, Ws[0], ldw[0], C, kSurHid, B, nout[0], kin[0], 1);
                 k_bias_gelu<<<blocks(BH), 256, 0, h->stream>>>(C, bs[L], Zs[L], Hs[L], B, kSurHid);
                 in = Hs[L];
             }
@@ -943,7 +966,7 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
                 k_transpose_bf16<<<dim3((no + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(dZb, no, T1, B, B, no);
                 const __nv_bfloat16 *inp = L == 0 ? Xb : Hs[L - 1];
                 k_transpose_bf16<<<dim3((ki + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(
-                    inp, L == 0 ? kSurInPad : kSurHid, T2, B, B, ki);
+                    inp, L == 0 ? kSurInX : kSurHid, T2, B, B, ki);  // layer 0: the values' columns
                 k_gemm_tn<<<dim3((ki + 63) / 64, (no + 63) / 64), 128, 0, h->stream>>>(T1, B, T2, B, gw[L], ldw[L], no,
                                                                                         ki, B);
                 if (L == 0) break;
@@ -1029,7 +1052,7 @@ int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y) {
     float *xd = nullptr, *pd = nullptr;
     __nv_bfloat16 *X = nullptr;
     rc = dalloc(h, &xd, (size_t)n * kSurIn);
-    if (!rc) rc = dalloc(h, &X, (size_t)mpad * kSurInPad);
+    if (!rc) rc = dalloc(h, &X, (size_t)mpad * kSurInX);
     if (!rc) rc = dalloc(h, &pd, (size_t)mpad * kSurOutPad);
     if (!rc && cudaMemcpyAsync(xd, x, (size_t)n * kSurIn * 4, cudaMemcpyHostToDevice, h->stream)) rc = LBMGPU_E_CUDA;
     if (!rc) {

@@ -14,6 +14,10 @@
 namespace lbm {
 
 constexpr int kSurIn = 12, kSurInPad = 16;    // features, padded to one MMA k-slice
+constexpr int kSurInX = 2 * kSurInPad;        // a feature row as the network reads it: the BF16
+                                              // value of each standardised feature, then the BF16
+                                              // remainder (feature - value), two k-slices whose sum
+                                              // carries the feature to ~16 significant bits
 constexpr int kSurHid = 128;                  // hidden width
 constexpr int kSurOut = 10, kSurOutPad = 16;  // outputs, padded to two MMA n-tiles
 constexpr int kSurLd = kSurHid + 8;           // row stride (bf16) of the 128-wide weights: no bank conflicts

@@ -1,5 +1,6 @@
 """The chemistry surrogate through the C ABI (lbmgpu_surrogate_*): the fused tensor-core
-forward pass against a torch FP32 reference that rounds operands to BF16 like the device,
+forward pass against a torch FP32 reference that rounds operands to BF16 like the device
+(each feature as a BF16 value plus a BF16 remainder),
 the first Adam step against torch autograd, learning a smooth function, and the whole
 collect -> train -> replace loop on the reacting fixture (audit error, exact element
 conservation of the projected prediction)."""
@@ -55,7 +56,8 @@ def bf16(t):
 def torch_forward(d, x, round_bf16=True):
     r = bf16 if round_bf16 else (lambda t: t)
     t = lambda a: torch.tensor(a, dtype=torch.float32)  # noqa: E731
-    h = r((t(x) - t(d["x_mean"])) / t(d["x_std"]))
+    h = (t(x) - t(d["x_mean"])) / t(d["x_std"])
+    h = r(h) + r(h - r(h))  # the device's BF16 value + BF16 remainder of each feature
     for L in (1, 2, 3):
         h = r(torch.nn.functional.gelu(h @ r(t(d[f"W{L}"])).T + t(d[f"b{L}"])))
     out = h @ r(t(d["W4"])).T + t(d["b4"])
