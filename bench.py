@@ -71,6 +71,9 @@ def parse():
                          "surrogate steps with a 1 %% audit; plain ROS2 timed on the same lattice beside it)")
     ap.add_argument("--teach", type=int, default=60, help="surrogate: ROS2 teacher steps that collect samples")
     ap.add_argument("--epochs", type=int, default=16, help="surrogate: training epochs over the samples")
+    ap.add_argument("--compare", type=int, default=100,
+                    help="surrogate: steps run twice from the same state, with the surrogate and with plain ROS2, "
+                         "to compare peak temperature and integrated heat release")
     ap.add_argument("--augment", type=float, default=0.5,
                     help="surrogate: perturbed, integrator-labelled rows added per collected row")
     ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
@@ -414,6 +417,39 @@ def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
     return dt
 
 
+def surrogate_vs_plain(lat, mix, sp, K):
+    """From the lattice's current state, K steps with the surrogate (1 % audit) and, after
+    restoring the state, K steps of plain ROS2: the north star's comparison -- peak
+    temperature and heat release integrated over the cells and the K steps -- from the
+    device diagnostics (lbmgpu_diagnostics) after every step."""
+    import lbmgpu
+    import workloads
+    c0 = mix.copy()
+    s0 = [a.copy() for a in sp]
+    lat.download(c0, s0)
+    d0 = lat.diagnostics()
+    runs = {}
+    for name, on in (("surrogate", True), ("plain", False)):
+        lat.upload(c0, s0)
+        lat.surrogate_enable(on, audit_period=100)
+        hrr, tpk = 0.0, d0["T_max"]
+        for _ in range(K):
+            lat.step(1)
+            d = lat.diagnostics()
+            hrr += d["hrr"]
+            tpk = max(tpk, d["T_max"])
+        runs[name] = (hrr, tpk, d["T_max"])
+    kelvin = lbmgpu.units_from_dx_dt(*workloads.FLAME_UNITS)[3]
+    (hs, ps, fs), (hp, pp, fp) = runs["surrogate"], runs["plain"]
+    return {"compare_steps": K,
+            "peak_T_K": {"surrogate": ps * kelvin, "plain": pp * kelvin, "start": d0["T_max"] * kelvin},
+            "peak_T_rel_err": abs(ps - pp) / abs(pp),
+            "peak_T_rise_rel_err": abs(ps - pp) / max(abs(pp - d0["T_max"]), 1e-300),
+            "final_T_max_rel_err": abs(fs - fp) / abs(fp),
+            "heat_release_integrated": {"surrogate": hs, "plain": hp, "unit": "lattice (sum over cells and steps)"},
+            "heat_release_rel_err": abs(hs - hp) / max(abs(hp), 1e-300)}
+
+
 def run_ours_mc(args, dist):
     import numpy as np
 
@@ -492,6 +528,8 @@ def run_ours_mc(args, dist):
         sur["plain_chem_mlups"] = ncell * kp / (ms_plain * 1e-3) / 1e6
         sur["surrogate_ms_per_step"] = kms[4] / max(kk, 1)
         sur["network_flops_per_cell"] = 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)
+        if args.compare > 0:
+            sur.update(surrogate_vs_plain(lat, mix, sp, args.compare))
     lat.close()
     avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_stream": kms[1] / max(launches[1], 1),
            "k_mc_props": kms[3] / max(launches[3], 1)}

@@ -222,6 +222,16 @@ int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
  * scratch's address; make it before any stream capture begins. */
 int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
 
+/* Run diagnostics of the current state, reduced on the device (FP64, lattice units, over
+ * the fluid cells): out[0] sum rho |u|^2, out[1] sum rho |curl u|^2 with the wrapped
+ * central differences, out[2] sum rho E -- the reference's OutputKeEns
+ * (src/output.cpp:212-275), which the driver calls at output steps -- then out[3] the sum
+ * of the heat-release field (src/lbm-collision.cpp:395-398; 0 for a single component),
+ * out[4] the peak and out[5] the minimum temperature.  n_out >= LBMGPU_DIAG_COUNT.  Uses
+ * the reduction scratch of lbmgpu_sums; waits for the stream. */
+#define LBMGPU_DIAG_COUNT 6
+int lbmgpu_diagnostics(lbmgpu_t *h, double *out, int n_out);
+
 /* ---- chemistry surrogate (LBMGPU_CHEM_ROSENBROCK handles) --------------------------
  * No counterpart in the reference.  A small network learns the stiff integrator's step
  *   (T [K], ln p [Pa], Y_0..Y_8, dt [s])  ->  (dY_0..dY_8, dT [K])

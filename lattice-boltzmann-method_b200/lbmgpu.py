@@ -36,12 +36,13 @@ EXPORTS = [
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
-    "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums", "lbmgpu_sums_noalloc",
+    "lbmgpu_units_from_dx_dt", "lbmgpu_sums_count", "lbmgpu_sums", "lbmgpu_sums_noalloc", "lbmgpu_diagnostics",
     "lbmgpu_surrogate_collect", "lbmgpu_surrogate_load_samples", "lbmgpu_surrogate_samples",
     "lbmgpu_surrogate_augment", "lbmgpu_surrogate_train",
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
 ]
 SUMS_MAX = 21
+DIAG_COUNT = 6
 SUR_IN, SUR_OUT, SUR_NPARAMS = 12, 10, 36046
 
 
@@ -107,6 +108,7 @@ def lib():
         L.lbmgpu_sums_count.argtypes = [vp]
         L.lbmgpu_sums.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         L.lbmgpu_sums_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+        L.lbmgpu_diagnostics.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         fp = ctypes.POINTER(ctypes.c_float)
         L.lbmgpu_surrogate_collect.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_long]
         L.lbmgpu_surrogate_load_samples.argtypes = [vp, fp, fp, ctypes.c_long]
@@ -348,6 +350,14 @@ class Lattice:
         r = SurrogateReport()
         _check(lib().lbmgpu_surrogate_stats(self.h, ctypes.byref(r)), "lbmgpu_surrogate_stats")
         return {k: getattr(r, k) for k, _ in SurrogateReport._fields_}
+
+    def diagnostics(self):
+        """Device-reduced diagnostics (lattice units): dict of kinetic (sum rho|u|^2),
+        enstrophy (sum rho|curl u|^2), energy (sum rho E), hrr (sum of the heat-release
+        field), T_max, T_min."""
+        out = (ctypes.c_double * DIAG_COUNT)()
+        _check(lib().lbmgpu_diagnostics(self.h, out, DIAG_COUNT), "lbmgpu_diagnostics")
+        return dict(zip(("kinetic", "enstrophy", "energy", "hrr", "T_max", "T_min"), list(out)))
 
     def sums_noalloc(self, n_out=None):
         """The same totals through lbmgpu_sums_noalloc (fixed device scratch, no
