@@ -337,20 +337,23 @@ def run_reference(args, dist):
 def mc_bytes(kernel, pop_bytes, reaction=False):
     """Algorithmic bytes per fluid cell of one multicomponent launch (9 species): every
     population (270 planes of `pop_bytes`) read once and, by the update, written once;
-    the FP64 record and parameter planes each kernel must read or write once per cell.
+    the FP64 record, parameter and sum planes each kernel must read or write once per cell.
       k_mc_relax : 270 populations in and out; per species rho_a, the 3 face terms and
                    the parameters om_a, F_a (3) [, drho_a]; shared u (3), T, rho; the
                    energy set's 7 parameters -> 9 * (4 + 4) + 5 + 7 = 84 planes [+ 9]
-      k_mc_stream: 21 record planes read (rho, T, p, rho_a, X_a) + 88 written
+      k_mc_gather: 270 populations pulled, 91 sum planes written (per species rho_a, j_a,
+                   its P-tensor share; the energy sum)
+      k_mc_solve : the 91 sum planes, 21 record planes (rho, T, p, rho_a, X_a) and the 36
+                   D_ab read, 88 record planes written
       k_mc_props : 58 record planes of the cell + 40 read once by its neighbours, 88
-                   parameter planes written (52 + the 36 D_ab) [+ HRR]
-      (k_mc_stream also reads the 36 D_ab planes)"""
+                   parameter planes written (52 + the 36 D_ab) [+ HRR]"""
     if kernel == "k_mc_relax":
         return 2 * 270 * pop_bytes + (84 + (9 if reaction else 0)) * 8
     if kernel == "k_mc_props":
         return (58 + 40 + 88 + (1 if reaction else 0)) * 8
-    return 270 * pop_bytes + (21 + 36 + 88) * 8
-
+    if kernel == "k_mc_solve":
+        return (91 + 21 + 36 + 88) * 8
+    return 270 * pop_bytes + 91 * 8  # k_mc_gather
 
 
 MC_SHAPES = {"mix": "periodic", "react": "periodic", "inflow": "TYPE_I_C inflow / TYPE_O_C outflow in x, periodic y z",
@@ -531,9 +534,9 @@ def run_ours_mc(args, dist):
         if args.compare > 0:
             sur.update(surrogate_vs_plain(lat, mix, sp, args.compare))
     lat.close()
-    avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_stream": kms[1] / max(launches[1], 1),
-           "k_mc_props": kms[3] / max(launches[3], 1)}
-    hbm_kernels = ("k_mc_relax", "k_mc_stream")
+    avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_gather": kms[1] / max(launches[1], 1),
+           "k_mc_solve": kms[5] / max(launches[5], 1), "k_mc_props": kms[3] / max(launches[3], 1)}
+    hbm_kernels = ("k_mc_relax", "k_mc_gather")
     dom = max(hbm_kernels, key=avg.get)  # the dominant population-moving kernel
     alg = mc_bytes(dom, pop_bytes, reaction) * ncell
     peak, peak_kind = peaks()
@@ -581,7 +584,7 @@ def run_ours_mc(args, dist):
         "config": {"workload": mc_workload_name(args, "x".join(str(s_ - 2) for s_ in mix.shape)),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
                    "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
-        "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_stream", "k_mc_props"))
+        "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_gather", "k_mc_solve", "k_mc_props"))
         / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell), "peak_source": f"{peak_kind} hbm_gbs",

@@ -17,9 +17,13 @@ constexpr int kBlock = 128;
 
 enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SPECIES = 4 };
 // per-kernel timing classes; multicomponent: K_COLLIDE is the population update
-// (k_mc_relax), K_PROPS the collision parameters (k_mc_props), K_SURROGATE the chemistry
-// surrogate's features, network and integrator list
-enum KernelKind { K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_NKINDS = 5 };
+// (k_mc_relax), K_STREAM_MOMENT the pull and population sums of the interior cells
+// (k_mc_gather), K_PROPS the collision parameters (k_mc_props), K_SURROGATE the chemistry
+// surrogate's features, network and integrator list, K_SOLVE the interior cells' moment
+// solve (k_mc_solve)
+enum KernelKind {
+    K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_SOLVE = 5, K_NKINDS = 6
+};
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.
 enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
@@ -80,6 +84,7 @@ struct lbmgpu {
     double *shift[2] = {nullptr, nullptr};  // FP32: per-plane population shift (current, scratch)
     double *sum_scratch = nullptr;          // lbmgpu_sums: block partials and totals
     double *props = nullptr;                // multicomponent collision parameters
+    double *gsum = nullptr;                 // multicomponent: the interior cells' population sums
     lbmh::SurState *sur = nullptr;          // chemistry surrogate, created on first use
     lbmgpu_mech mech{};                     // multicomponent: the caller's mechanism, copied at create
     long nfluid = 0;

@@ -4,7 +4,8 @@
 // Reference path replaced (farrasarira/Lattice-Boltzmann-Method, MULTICOMP on):
 //   LBM::Collide_Species + LBM::Collide   src/lbm-collision.cpp:191-526 -> k_mc_collide
 //   LBM::Streaming + LBM::calculate_moment src/lbm-streaming.cpp, src/lbm-moment.cpp:193-377
-//                                          -> k_mc_stream
+//                                          -> k_mc_gather (pull + population sums per
+//                                             (cell, set)) and k_mc_solve (per cell)
 //   LBM::Init                              src/lbm-init.cpp:85-146 -> k_mc_init
 //   LBM::Streaming + LBM::TMS_BC + LBM::calculate_moment of the cells with a boundary
 //   upstream (src/lbm-bc.cpp:122-1110, src/impose_nscbc.cpp) -> k_mc_special
@@ -85,11 +86,40 @@ __global__ void k_mc_fill_bst(long ncell, long nb, int np, const long *__restric
     bst[i] = pop[(long)q * ncell + blist[b]];
 }
 
+// Interior cells (no boundary upstream): the pull of one population set per thread
+// (blockIdx.y = species, NS = the energy set) and its sums into the gsum planes --
+// species a: rho_a, j_a, its P-tensor share at planes 10a..10a+9; the energy set's sum at
+// plane 10 NS.  A warp reads one set's planes at 32 consecutive cells.
 template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock, 3) k_mc_stream(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, 4) k_mc_gather(McArgsT<S, double> A, double *__restrict__ gs) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
-    mc_stream_moment_cell<NS>(A, n);
+    const int a = blockIdx.y;
+    McPull pp;
+    mc_pull(A, n, pp);
+    if (a < NS) {
+        double fv[27], s[kGsPerSpecies];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) fv[l] = ldpop(A, A.pop_src, 27 * a + l, pull_idx(pp, l));
+        species_sums(fv, s);
+#pragma unroll
+        for (int q = 0; q < kGsPerSpecies; ++q) gs[(long)(kGsPerSpecies * a + q) * A.ncell + n] = s[q];
+    } else {
+        double e = 0.0;
+#pragma unroll
+        for (int l = 0; l < 27; ++l) e += ldpop(A, A.pop_src, 27 * NS + l, pull_idx(pp, l));
+        gs[(long)(kGsPerSpecies * NS) * A.ncell + n] = e;
+    }
+}
+
+// Interior cells: the moment solve from the gathered sums (species velocities from the
+// Stefan-Maxwell system, temperature, the record) -- the same bits as mc_stream_moment_cell.
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock, 2) k_mc_solve(McArgsT<S, double> A, const double *__restrict__ gs) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= A.ncell || A.cflag[n] != CF_FLUID) return;
+    const SumsAt<NS> Sm{gs, A.ncell, n};
+    mc_moments_finish<NS>(A, n, Sm);
 }
 
 template <int NS, typename S>
@@ -415,8 +445,13 @@ int stream_t(lbmgpu *h) {
     A.rec_nxt = h->mom[x];
     EvPair ep{};
     ev_begin(h, K_STREAM_MOMENT, ep);
-    k_mc_stream<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A);
+    k_mc_gather<NS9, S><<<dim3(grid_for(h->g.ncell), NS9 + 1), kBlock, 0, h->stream>>>(A, h->gsum);
     ev_end(h, ep);
+    CK(cudaGetLastError());
+    EvPair es{};
+    ev_begin(h, K_SOLVE, es);
+    k_mc_solve<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A, h->gsum);
+    ev_end(h, es);
     CK(cudaGetLastError());
     if (h->nb > 0) {
         A.bst_cur = bstb<S>(h, c);
@@ -455,6 +490,8 @@ int mc_setup(lbmgpu *h) {
         if (b == 0) {
             rc = dalloc(h, &h->props, (size_t)pr_count<NS9>() * nc);
             if (rc) return rc;
+            rc = dalloc(h, &h->gsum, (size_t)gs_count<NS9>() * nc);
+            if (rc) return rc;
         }
         // the face-difference planes of cells the kernels never write (ghosts) are read
         // but not used, and the ghosts' populations are never read; zero them all so they
@@ -486,6 +523,8 @@ void mc_release(lbmgpu *h) {
     h->tab = nullptr;
     cudaFree(h->props);
     h->props = nullptr;
+    cudaFree(h->gsum);
+    h->gsum = nullptr;
     for (int b = 0; b < 2; ++b) {
         cudaFree(h->pop32[b]);
         cudaFree(h->bst32[b]);

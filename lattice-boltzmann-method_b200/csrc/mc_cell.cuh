@@ -247,50 +247,109 @@ template <int NS> MC_HD constexpr int pr_count() { return 5 * NS + 7 + NS * (NS 
 
 // ------------------------------------------------------------------------------------
 // Moments (the multicomponent LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one
-// fluid cell from its streamed populations; pop(a, l) returns population l of species a
-// (a = NS: the energy set) of the cell.
+// fluid cell from its streamed populations, in two parts: the population sums (per
+// species: rho_a, j_a and its share of the P tensor; the energy set's sum), then the
+// per-cell solve from the sums (Stefan-Maxwell species velocities, temperature, record).
+// The P tensor is summed species by species (each species' share over its 27 directions,
+// then the shares in species order) on every path, so the interior split into a gather
+// kernel and a solve kernel gives the same bits as the one-pass function.
 // ------------------------------------------------------------------------------------
+constexpr int kGsPerSpecies = 10;  // rho_a, j_a (3), P-tensor share (6)
+template <int NS> MC_HD constexpr int gs_count() { return kGsPerSpecies * NS + 1; }
+
+// The sums of one cell held in registers (the one-pass path); SumsAt reads the same
+// values from the gathered planes where they are used.
+template <int NS>
+struct McSums {
+    double ra[NS], ja[NS][3], p6[6], re;
+    MC_HD double rho_a(int a) const { return ra[a]; }
+    MC_HD double j(int a, int d) const { return ja[a][d]; }
+    MC_HD double P6(int q) const { return p6[q]; }
+    MC_HD double rhoe() const { return re; }
+};
+
+// The sums of one species' streamed populations fv[27]: s = (rho_a, j_a (3), P share (6)).
+MC_HD void species_sums(const double *fv, double *s) {
+    double r = 0, jx = 0, jy = 0, jz = 0, p[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int l = 0; l < 27; ++l) {
+        r += fv[l];
+        jx += fv[l] * cx(l);
+        jy += fv[l] * cy(l);
+        jz += fv[l] * cz(l);
+        if (cx(l)) p[0] += fv[l];
+        if (cx(l) * cy(l)) p[1] += cx(l) * cy(l) * fv[l];
+        if (cx(l) * cz(l)) p[2] += cx(l) * cz(l) * fv[l];
+        if (cy(l)) p[3] += fv[l];
+        if (cy(l) * cz(l)) p[4] += cy(l) * cz(l) * fv[l];
+        if (cz(l)) p[5] += fv[l];
+    }
+    s[0] = r;
+    s[1] = jx;
+    s[2] = jy;
+    s[3] = jz;
+    for (int q = 0; q < 6; ++q) s[4 + q] = p[q];
+}
+
+// The gathered sum planes of cell n (k_mc_gather): species a at planes 10a..10a+9, the
+// energy sum at 10 NS; the P tensor adds the species' shares in species order.
+template <int NS>
+struct SumsAt {
+    const double *gs;
+    long ncell, n;
+    MC_HD double at(int plane) const { return gs[(long)plane * ncell + n]; }
+    MC_HD double rho_a(int a) const { return at(kGsPerSpecies * a); }
+    MC_HD double j(int a, int d) const { return at(kGsPerSpecies * a + 1 + d); }
+    MC_HD double P6(int q) const {
+        double v = 0.0;
+        for (int a = 0; a < NS; ++a) v += at(kGsPerSpecies * a + 4 + q);
+        return v;
+    }
+    MC_HD double rhoe() const { return at(kGsPerSpecies * NS); }
+};
+
+template <int NS, class AT, class Sums>
+MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S);
+
 template <int NS, class AT, class Pop>
 MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
+    McSums<NS> S;
+    for (int q = 0; q < 6; ++q) S.p6[q] = 0.0;
+    for (int a = 0; a < NS; ++a) {
+        double fv[27], s[kGsPerSpecies];
+#pragma unroll
+        for (int l = 0; l < 27; ++l) fv[l] = pop(a, l);
+        species_sums(fv, s);
+        S.ra[a] = s[0];
+        for (int d = 0; d < 3; ++d) S.ja[a][d] = s[1 + d];
+        for (int q = 0; q < 6; ++q) S.p6[q] += s[4 + q];
+    }
+    double rhoe = 0.0;
+#pragma unroll
+    for (int l = 0; l < 27; ++l) rhoe += pop(NS, l);
+    S.re = rhoe;
+    mc_moments_finish<NS>(A, n, S);
+}
+
+template <int NS, class AT, class Sums>
+MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S) {
     const gas::Tables &t = *A.tab;
     // -- old temperature, where the reference's Newton iteration starts (lbm-moment.cpp:219-221);
     // the old state's diffusion coefficients come from the collision parameters
     const double T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
 
-    // -- sums per species and of g
-    double rho_a[NS], j_a[NS][3];
-    double P6[6] = {0, 0, 0, 0, 0, 0};
-    for (int a = 0; a < NS; ++a) {
-        double fv[27];
-#pragma unroll
-        for (int l = 0; l < 27; ++l) fv[l] = pop(a, l);
-        double r = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-        for (int l = 0; l < 27; ++l) {
-            r += fv[l];
-            jx += fv[l] * cx(l);
-            jy += fv[l] * cy(l);
-            jz += fv[l] * cz(l);
-            if (cx(l)) P6[0] += fv[l];
-            if (cx(l) * cy(l)) P6[1] += cx(l) * cy(l) * fv[l];
-            if (cx(l) * cz(l)) P6[2] += cx(l) * cz(l) * fv[l];
-            if (cy(l)) P6[3] += fv[l];
-            if (cy(l) * cz(l)) P6[4] += cy(l) * cz(l) * fv[l];
-            if (cz(l)) P6[5] += fv[l];
-        }
-        rho_a[a] = r;
-        j_a[a][0] = jx;
-        j_a[a][1] = jy;
-        j_a[a][2] = jz;
-    }
-    double rhoe = 0.0;
-#pragma unroll
-    for (int l = 0; l < 27; ++l) rhoe += pop(NS, l);
-
+    // the diffusion coefficients first (one load per pair, into the lower triangle that
+    // the Stefan-Maxwell entries then replace row by row), the momenta next
+    double L[NS][NS];  // lower triangle and diagonal only
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < a; ++b) L[a][b] = A.props[(long)pr_d<NS>(a, b) * A.ncell + n];
+    double j_a[NS][3];
     double rho = 0, ru = 0, rv = 0, rw = 0, rho_s[NS];
     for (int a = 0; a < NS; ++a) {
-        rho_s[a] = rho_a[a] > kSpeciesMin ? rho_a[a] : kSpeciesMin;
-        rho += rho_a[a];
+        const double ra = S.rho_a(a);
+        for (int d = 0; d < 3; ++d) j_a[a][d] = S.j(a, d);
+        rho_s[a] = ra > kSpeciesMin ? ra : kSpeciesMin;
+        rho += ra;
         ru += j_a[a][0];
         rv += j_a[a][1];
         rw += j_a[a][2];
@@ -298,30 +357,37 @@ MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     const double u = ru / rho, v = rv / rho, w = rw / rho;
 
     // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky, with
-    // the D_ab the collision of this step evaluated at the same old state (T, p, Y)
-    double M[NS][NS];
+    // the D_ab the collision of this step evaluated at the same old state (T, p, Y).  Every
+    // entry of row a is -dt/2 p X_a X_b / D_ab evaluated in that order, so the lower
+    // triangle (b < a) is the matrix's own entry and the diagonal takes row a's entries,
+    // b = 0..NS-1, as the reference subtracts them; the upper triangle is never stored.
+    // Rows go in order: row a reads D_ab of the rows below it (still untouched) and its
+    // own slots before replacing them.  Every division is the reference's: the boundary
+    // cells' upwind differences switch on the sign of near-zero diffusion velocities, so a
+    // reciprocal in place of a quotient (one rounding apart) moves the results by 1e-9
+    // within two steps.
     const double p_old = rec(A, A.rec_cur, RM_P, n);
     double Xold[NS];
     for (int a = 0; a < NS; ++a) Xold[a] = rec(A, A.rec_cur, rs(a, RS_X), n);
     for (int a = 0; a < NS; ++a) {
-        M[a][a] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
-        for (int b = 0; b < a; ++b) {  // D_ab of the reference's lower triangle, one per pair
-            const double D = A.props[(long)pr_d<NS>(a, b) * A.ncell + n];
-            M[a][b] = -1.0 * A.dt / 2.0 * p_old * Xold[a] * Xold[b] / D;
-            M[b][a] = -1.0 * A.dt / 2.0 * p_old * Xold[b] * Xold[a] / D;
+        double d = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
+        for (int b = 0; b < NS; ++b) {
+            if (b == a) continue;
+            const double D = b < a ? L[a][b] : L[b][a];
+            const double m = -1.0 * A.dt / 2.0 * p_old * Xold[a] * Xold[b] / D;
+            if (b < a) L[a][b] = m;
+            d -= m;
         }
+        L[a][a] = d;
     }
-    for (int a = 0; a < NS; ++a)
-        for (int b = 0; b < NS; ++b)
-            if (b != a) M[a][a] -= M[a][b];
     for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor
-        double d = M[c][c];
-        for (int q = 0; q < c; ++q) d -= M[c][q] * M[c][q];
-        M[c][c] = sqrt(d);
+        double d = L[c][c];
+        for (int q = 0; q < c; ++q) d -= L[c][q] * L[c][q];
+        L[c][c] = sqrt(d);
         for (int r = c + 1; r < NS; ++r) {
-            double s = M[r][c];
-            for (int q = 0; q < c; ++q) s -= M[r][q] * M[c][q];
-            M[r][c] = s / M[c][c];
+            double s = L[r][c];
+            for (int q = 0; q < c; ++q) s -= L[r][q] * L[c][q];
+            L[r][c] = s / L[c][c];
         }
     }
     double usm[NS][3];
@@ -329,13 +395,13 @@ MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
         double y[NS];
         for (int r = 0; r < NS; ++r) {
             double s = j_a[r][dmn];
-            for (int q = 0; q < r; ++q) s -= M[r][q] * y[q];
-            y[r] = s / M[r][r];
+            for (int q = 0; q < r; ++q) s -= L[r][q] * y[q];
+            y[r] = s / L[r][r];
         }
         for (int r = NS - 1; r >= 0; --r) {
             double s = y[r];
-            for (int q = r + 1; q < NS; ++q) s -= M[q][r] * usm[q][dmn];
-            usm[r][dmn] = s / M[r][r];
+            for (int q = r + 1; q < NS; ++q) s -= L[q][r] * usm[q][dmn];
+            usm[r][dmn] = s / L[r][r];
         }
     }
 
@@ -343,6 +409,7 @@ MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     double Yr[NS], Y[NS], X[NS];
     for (int a = 0; a < NS; ++a) Yr[a] = rho_s[a] / rho;
     const double Wn = set_mass_fractions<NS>(t, Yr, Y, X);
+    const double rhoe = S.rhoe();
     double e = rhoe / rho;
     for (int a = 0; a < NS; ++a)
         e = e - 0.5 * rho_s[a] / rho * (usm[a][0] * usm[a][0] + usm[a][1] * usm[a][1] + usm[a][2] * usm[a][2]);
@@ -363,7 +430,7 @@ MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     put(A, R, RM_T, n, Tl);
     put(A, R, RM_P, n, u_p(A.U, (float)Pn));
     put(A, R, RM_RHOE, n, rhoe);
-    for (int q = 0; q < 6; ++q) put(A, R, RM_P00 + q, n, P6[q]);
+    for (int q = 0; q < 6; ++q) put(A, R, RM_P00 + q, n, S.P6(q));
     for (int a = 0; a < NS; ++a) {
         put(A, R, rs(a, RS_RHO), n, rho_s[a]);
         for (int d = 0; d < 3; ++d) put(A, R, rs(a, RS_UX + d), n, usm[a][d]);

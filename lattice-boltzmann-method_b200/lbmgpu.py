@@ -262,12 +262,13 @@ class Lattice:
         _check(lib().lbmgpu_profile(self.h, int(enable)), "lbmgpu_profile")
 
     def kernel_times(self):
-        """Per kernel kind (0 collide / population update, 1 stream+boundary+moment,
-        2 other, 3 multicomponent collision parameters, 4 chemistry surrogate): launches
-        and device ms."""
-        launches = (ctypes.c_long * 5)()
-        ms = (ctypes.c_double * 5)()
-        _check(lib().lbmgpu_kernel_times(self.h, 5, launches, ms), "lbmgpu_kernel_times")
+        """Per kernel kind (0 collide / population update, 1 stream+boundary+moment
+        (multicomponent: the interior pull and sums), 2 other, 3 multicomponent collision
+        parameters, 4 chemistry surrogate, 5 multicomponent moment solve): launches and
+        device ms."""
+        launches = (ctypes.c_long * 6)()
+        ms = (ctypes.c_double * 6)()
+        _check(lib().lbmgpu_kernel_times(self.h, 6, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------
