@@ -139,4 +139,84 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     return done ? acc : -1;
 }
 
+#if defined(__CUDACC__)
+// ros2_advance for one cell by a group of G lanes (G a power of two <= 32, the group's
+// lanes consecutive and aligned within the warp; every lane passes the same arguments).
+// The n + 1 right-hand sides of a sub-step's finite-difference Jacobian (column c
+// perturbed, c < n, and the unperturbed one, index n) are dealt out round robin, index
+// j to lane j % G; each lane then assembles the Jacobian from the group's columns by
+// shuffles and runs the same factorisation, stages and step control -- the arithmetic of
+// ros2_advance value for value, with the Jacobian's evaluations side by side.
+template <int G>
+__device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                                  double atol = 1e-10, double atol_T = 1e-3) {
+    constexpr int kPer = (MAXS + 1 + G) / G;  // right-hand sides per lane, at most
+    const int ns = t.ns, n = ns + 1;
+    const int lane = (int)(threadIdx.x & 31u), g = lane & (G - 1);
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
+    const double gam = 1.0 + 1.0 / sqrt(2.0);
+    double y[MAXS + 1], F0[MAXS + 1], Fp[MAXS + 1], yp[MAXS + 1], k1[MAXS + 1], k2[MAXS + 1];
+    double M[MAXS + 1][MAXS + 1];
+    double Fc[kPer][MAXS + 1], ec[kPer];  // this lane's right-hand sides and their steps
+    int piv[MAXS + 1];
+    for (int k = 0; k < ns; ++k) y[k] = Y[k];
+    y[ns] = T;
+    double tt = 0.0, h = dt;
+    int acc = 0;
+    bool done = false;
+    for (int it = 0; it < kChemMaxSub && !done; ++it) {
+        const bool last = tt + h >= dt;
+        if (last) h = dt - tt;
+        for (int m = 0; m < kPer; ++m) {
+            const int c = g + m * G;  // column c < n, or the unperturbed right-hand side c == n
+            if (c > n) break;
+            for (int q = 0; q < n; ++q) yp[q] = y[q];
+            double eps = 1.0;
+            if (c < n) {
+                eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
+                yp[c] += eps;
+            }
+            ec[m] = eps;
+            reactor_rhs(t, rho, yp, Fc[m]);
+        }
+        for (int r = 0; r < n; ++r) F0[r] = __shfl_sync(gmask, Fc[n / G][r], n % G, G);
+        for (int m = 0; m < kPer; ++m)  // this lane's Jacobian columns
+            if (g + m * G < n)
+                for (int r = 0; r < n; ++r) Fc[m][r] = -gam * h * (Fc[m][r] - F0[r]) / ec[m];
+        for (int c = 0; c < n; ++c)
+            for (int r = 0; r < n; ++r) M[r][c] = __shfl_sync(gmask, Fc[c / G][r], c % G, G);
+        for (int r = 0; r < n; ++r) M[r][r] += 1.0;
+        if (!lu_factor(M, n, piv)) {
+            h *= 0.25;
+            continue;
+        }
+        for (int q = 0; q < n; ++q) k1[q] = F0[q];
+        lu_solve(M, n, piv, k1);
+        for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
+        reactor_rhs(t, rho, yp, Fp);
+        for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
+        lu_solve(M, n, piv, k2);
+        double err = 0.0;
+        for (int q = 0; q < n; ++q) {
+            const double ynew = y[q] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
+            const double sc = (q < ns ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
+            const double e = 0.5 * h * (k1[q] + k2[q]) / sc;
+            err = fmax(err, fabs(e));
+            yp[q] = ynew;
+        }
+        if (err <= 1.0) {
+            for (int q = 0; q < n; ++q) y[q] = yp[q];
+            tt = last ? dt : tt + h;
+            done = last;
+            ++acc;
+        }
+        const double fac = err > 0.0 ? 0.9 / sqrt(err) : 4.0;
+        h *= fmin(4.0, fmax(0.2, fac));
+    }
+    for (int k = 0; k < ns; ++k) Y[k] = y[k];
+    T = y[ns];
+    return done ? acc : -1;
+}
+#endif
+
 }  // namespace gas

@@ -43,14 +43,20 @@ __global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
 
 // the cells the collision-parameter kernel left to the chemistry integrator (surrogate
 // on: out-of-box, non-finite and audited cells), integrated in dense warps
+// The cells the surrogate leaves to the integrator (sur.ilist), kChemGroup lanes per cell:
+// the lanes of a group evaluate the finite-difference Jacobian's columns side by side
+// (gas::ros2_advance_group), so a few thousand listed cells do not wait on serial
+// integrations of one lane each.
+constexpr int kChemGroup = 4;
 template <int NS, typename S>
 __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
     const unsigned cnt = *A.sur.icount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const unsigned groups = gridDim.x * blockDim.x / kChemGroup;
+    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / kChemGroup; i < cnt; i += groups) {
         const long n = A.sur.ilist[i];
         double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
         mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, kChemGroup>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
     }
 }
 
@@ -419,15 +425,15 @@ int collide_t(lbmgpu *h) {
         k_mc_props<NS9, CHEM_ROSENBROCK, S><<<gp, kBlock, 0, h->stream>>>(A);
     else
         k_mc_props<NS9, CHEM_OFF, S><<<gp, kBlock, 0, h->stream>>>(A);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
     if (A.sur.ilist) {
         EvPair ei{};
         ev_begin(h, K_SURROGATE, ei);
-        k_mc_chem_list<NS9, S><<<148 * 4, kBlock, 0, h->stream>>>(A);
+        k_mc_chem_list<NS9, S><<<148 * 8, kBlock, 0, h->stream>>>(A);
         ev_end(h, ei);
         CK(cudaGetLastError());
     }
-    ev_end(h, ep);
-    CK(cudaGetLastError());
     EvPair er{};
     ev_begin(h, K_COLLIDE, er);
     k_mc_relax<NS9, S><<<dim3(grid_for(h->g.ncell), NS9 + 1), kBlock, 0, h->stream>>>(A);

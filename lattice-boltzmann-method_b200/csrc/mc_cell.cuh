@@ -474,10 +474,19 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // prediction against it).  With `defer` and a list (sur.ilist) such cells are only
 // appended to the list -- k_mc_chem_list integrates them afterwards in dense warps --
 // otherwise they are integrated here.  Teacher steps (mode 0) can write samples.
-template <int NS, class AT, bool CAN_INTEGRATE = true>
+//
+// G > 1 (device, the integrator list): a group of G lanes handles the cell together --
+// every lane runs this function with the same arguments, the integration is
+// ros2_advance_group, and only the group's first lane writes the results.
+template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
     const gas::Tables &t = *A.tab;
+#if defined(__CUDA_ARCH__)
+    const bool lead = G == 1 || (threadIdx.x & (G - 1)) == 0;
+#else
+    const bool lead = true;
+#endif
     const SurArgs &S = A.sur;
     const double dt_si = (double)A.dt * (double)A.U.s;
     double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
@@ -511,12 +520,20 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
         }
         if (CAN_INTEGRATE) {
             for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
-            if (gas::ros2_advance(t, rho_si, Yc, Tc, dt_si) < 0) atomic_status(A.status, LBMGPU_ST_CHEM);
+            int rc;
+#if defined(__CUDA_ARCH__)
+            if constexpr (G > 1)
+                rc = gas::ros2_advance_group<G>(t, rho_si, Yc, Tc, dt_si);
+            else
+#endif
+                rc = gas::ros2_advance(t, rho_si, Yc, Tc, dt_si);
+            if (rc < 0 && lead) atomic_status(A.status, LBMGPU_ST_CHEM);
         }
     } else {
         for (int a = 0; a < NS; ++a) Yc[a] = Yp[a];
         Tc = Tp;
     }
+    if (!lead) return;
     if (audit) {  // L1 error of the predicted dY and L1 size of the integrator's dY
         double num = 0.0, den = 0.0;
         for (int a = 0; a < NS; ++a) {
