@@ -42,6 +42,7 @@ extern "C" {
                                        src/lbm-collision.cpp:33-34)                   */
 #define LBMGPU_ST_NEWTON 0x8u       /* temperature Newton iteration hit its cap        */
 #define LBMGPU_ST_CHEM 0x10u        /* stiff chemistry hit its sub-step cap            */
+#define LBMGPU_ST_SURROGATE 0x20u   /* the surrogate network's tensor-core wait ran out */
 
 /* ---- precision of the population storage ------------------------------------- */
 #define LBMGPU_FP64 0   /* the reference's doubles; results bit-faithful                */

@@ -7,15 +7,16 @@
 // correction of the prediction (sur_conserve, surrogate.cuh) and an audited sample
 // (mc_cell.cuh, mode 1).
 //
-// Tensor-core kernels, BF16 operands with FP32 accumulation (mma.sync m16n8k16):
-//   k_sur_mlp   the whole network for a batch of cells in one kernel: the weights are
-//               staged once per block in shared memory, each warp carries 16 cells through
-//               the four layers with the activations in registers (the accumulator
-//               fragment of one layer is the operand fragment of the next); the first
-//               layer takes each standardised feature as a BF16 value plus a BF16
-//               remainder, two k-slices against the same W1, so the inputs (T above all:
-//               BF16 alone would round 1700 K by several kelvin) enter at ~16 bits;
-//   k_gemm_tn   C = A B^T for training (forward, input gradients, weight gradients);
+// Tensor-core kernels, BF16 operands with FP32 accumulation:
+//   k_sur_mlp_tc  the whole network for 128-cell tiles on the 5th-generation tensor cores:
+//                 tcgen05.mma from shared-memory operand tiles into a tensor-memory
+//                 accumulator, one commit per layer on an mbarrier, the bias/GELU epilogue
+//                 from tcgen05.ld back into shared memory as the next layer's operand; the
+//                 first layer takes each standardised feature as a BF16 value plus a BF16
+//                 remainder, two k-slices against the same W1, so the inputs (T above all:
+//                 BF16 alone would round 1700 K by several kelvin) enter at ~16 bits;
+//   k_gemm_tn     C = A B^T for training (forward, input gradients, weight gradients),
+//                 mma.sync m16n8k16;
 //   elementwise bias/GELU forward and backward, the MSE loss gradient, column sums for
 //   the bias gradients, Adam on FP32 master weights with BF16 copies.
 #include <cuda_bf16.h>
@@ -36,10 +37,7 @@ using namespace lbm;
 
 namespace {
 
-constexpr int kSurBlock = 128;                 // 4 warps, 16 cells each per tile
 constexpr int kW1 = kSurHid * kSurInPad;       // elements of the padded weight tensors
-constexpr int kW1Ld = kSurInX + 8;             // row stride of W1 in shared memory: [W1 | W1 | pad]
-constexpr int kW1s = kSurHid * kW1Ld;
 constexpr int kW2 = kSurHid * kSurLd;
 constexpr int kW4 = kSurOutPad * kSurLd;
 constexpr int kNParams = kW1 + 2 * kW2 + kW4 + 3 * kSurHid + kSurOutPad;
@@ -118,113 +116,237 @@ struct SurNet {  // device pointers of the BF16 weights and FP32 biases
     const float *b1, *b2, *b3, *b4;
 };
 
-// One layer of the fused network for a warp's 16 rows: acc[16 n-tiles][4] = A W^T + b,
-// with A given as fragments of NK k-slices and W (row stride LD) in shared memory.
-template <int NK, int NT, int LD>
-__device__ __forceinline__ void mlp_layer(const unsigned (*afr)[4], const __nv_bfloat16 *W, const float *b,
-                                          float (*acc)[4], int gid, int tig) {
-#pragma unroll
-    for (int j = 0; j < NT; ++j) {
-        const float b0 = b[8 * j + 2 * tig], b1 = b[8 * j + 2 * tig + 1];
-        acc[j][0] = b0;
-        acc[j][1] = b1;
-        acc[j][2] = b0;
-        acc[j][3] = b1;
-    }
-#pragma unroll
-    for (int s = 0; s < NK; ++s)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) {
-            const __nv_bfloat16 *wr = W + (8 * j + gid) * LD + 16 * s + 2 * tig;
-            const unsigned b0 = *reinterpret_cast<const unsigned *>(wr);
-            const unsigned b1 = *reinterpret_cast<const unsigned *>(wr + 8);
-            mma_bf16(acc[j], afr[s], b0, b1);
-        }
-}
 
-// GELU of a 16 x 128 accumulator and its repacking as the next layer's operand fragments:
-// the accumulator of n-tiles 2s and 2s+1 is exactly the operand fragment of k-slice s.
-__device__ __forceinline__ void gelu_to_frag(const float (*acc)[4], unsigned (*afr)[4]) {
-#pragma unroll
-    for (int s = 0; s < kSurHid / 16; ++s) {
-        afr[s][0] = pack_bf16(gelu_f(acc[2 * s][0]), gelu_f(acc[2 * s][1]));
-        afr[s][1] = pack_bf16(gelu_f(acc[2 * s][2]), gelu_f(acc[2 * s][3]));
-        afr[s][2] = pack_bf16(gelu_f(acc[2 * s + 1][0]), gelu_f(acc[2 * s + 1][1]));
-        afr[s][3] = pack_bf16(gelu_f(acc[2 * s + 1][2]), gelu_f(acc[2 * s + 1][3]));
+
+// -------------------------------------------------------------------------------------
+// Inference on the 5th-generation tensor cores (tcgen05): 128 cells per tile = the MMA's
+// M.  The four weight tiles sit in shared memory once per CTA; per layer one thread issues
+// tcgen05.mma (BF16 operands from shared memory, FP32 accumulator of 128 lanes x N columns
+// in tensor memory) and commits it to an mbarrier; after the wait each thread -- one per
+// cell row, warp w reading tensor-memory lanes 32w..32w+31 -- takes its row with
+// tcgen05.ld, adds the bias, applies GELU and writes the BF16 row back to shared memory as
+// the next layer's A operand.  Shared-memory operands are K-major without swizzle: element
+// (r, k) of an R x K tile at byte (r / 8) (16 K) + (k / 8) 128 + (r % 8) 16 + (k % 8) 2,
+// i.e. 8 x 16-byte core matrices, the two of one 16-wide K step 128 bytes apart (leading
+// offset) and 8-row groups 16 K bytes apart (stride offset).  Every wait has a time limit:
+// past it the kernel raises LBMGPU_ST_SURROGATE, waits once more for its own tensor-core
+// work, frees its tensor memory and returns.
+// -------------------------------------------------------------------------------------
+constexpr int kTcRows = 128;       // cells per tile (MMA M), one thread each
+constexpr int kTcGroups = 2;       // independent tile groups per CTA (one warpgroup each)
+constexpr uint32_t kTcCols = 128;  // tensor-memory columns per group: the widest accumulator
+constexpr int kTcW1 = 0, kTcW2 = kTcW1 + kSurHid * kSurInX * 2, kTcW3 = kTcW2 + kSurHid * kSurHid * 2,
+              kTcW4 = kTcW3 + kSurHid * kSurHid * 2, kTcG = kTcW4 + kSurOutPad * kSurHid * 2,  // weights, shared
+              kTcA = 0, kTcX = kTcA + kTcRows * kSurHid * 2, kTcGBytes = kTcX + kTcRows * kSurInX * 2,  // per group
+              kTcB = kTcG + kTcGroups * kTcGBytes, kTcBar = kTcB + (3 * kSurHid + 3 * kSurOutPad) * 4,
+              kTcErr = kTcBar + 8 * kTcGroups, kTcSlot = kTcErr + 4 * kTcGroups, kTcSmem = kTcSlot + 8;
+static_assert(kTcG % 16 == 0 && kTcGBytes % 16 == 0 && kTcX % 16 == 0 && kTcBar % 8 == 0,
+              "operand tiles 16-byte, mbarriers 8-byte aligned");
+
+__device__ __forceinline__ uint32_t tc_off(int r, int k, int K) {
+    return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+// shared-memory matrix descriptor: start, leading offset 128 B, stride offset, version 1
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo) {
+    return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M = 128
+__host__ __device__ constexpr uint32_t tc_idesc(int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTcRows >> 4) << 24);
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void group_bar(int g) {  // the 128 threads of tile group g
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(kTcRows) : "memory");
+}
+__device__ __forceinline__ void tc_sync(int g) {  // group's shared writes visible to the tensor core, in step
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    group_bar(g);
+    tc_fence_after();
+}
+// One layer: D (tensor memory) = A (rows x K, shared) B^T (N x K, shared), K / 16 MMAs, then
+// the commit that arrives on the mbarrier when they are done.
+__device__ __forceinline__ void tc_layer(uint32_t tmem, uint32_t a, uint32_t b, int K, int N, uint32_t bar) {
+    const uint32_t idesc = tc_idesc(N);
+    for (int s = 0; s < K / 16; ++s) {
+        const uint64_t ad = tc_desc(a + 256u * s, (uint32_t)K * 16u), bd = tc_desc(b + 256u * s, (uint32_t)K * 16u);
+        const uint32_t acc = s > 0;
+        asm volatile(
+            "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+            : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+// Waits for the mbarrier phase `parity`, at most ~1 s of wall time.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    uint64_t t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > 1000000000ull) return false;
     }
 }
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t *r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t *r) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // X [mpad][kSurInX] network input rows -> pred [mpad][16] in SI units (outputs 10..15 zero).
-__global__ void __launch_bounds__(kSurBlock) k_sur_mlp(SurNet net, const SurNorm *__restrict__ nrm,
-                                                       const __nv_bfloat16 *__restrict__ X, float *__restrict__ pred,
-                                                       long ntiles) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16 *w1 = reinterpret_cast<__nv_bfloat16 *>(smem);  // [128][kW1Ld]: W1 for values and remainders
-    __nv_bfloat16 *w2 = w1 + kW1s;
-    __nv_bfloat16 *w3 = w2 + kW2;
-    __nv_bfloat16 *w4 = w3 + kW2;
-    float *bb = reinterpret_cast<float *>(w4 + kW4);  // b1 b2 b3 (128 each), b4 (16), y_mean, y_std
-    {
-        const unsigned *src[4] = {reinterpret_cast<const unsigned *>(net.w1), reinterpret_cast<const unsigned *>(net.w2),
-                                  reinterpret_cast<const unsigned *>(net.w3), reinterpret_cast<const unsigned *>(net.w4)};
-        unsigned *dst[4] = {reinterpret_cast<unsigned *>(w1), reinterpret_cast<unsigned *>(w2),
-                            reinterpret_cast<unsigned *>(w3), reinterpret_cast<unsigned *>(w4)};
-        for (int i = threadIdx.x; i < kW1 / 2; i += kSurBlock) {  // W1 row r, word c, into both halves
-            const int r = i / (kSurInPad / 2), c = i % (kSurInPad / 2);
-            dst[0][r * (kW1Ld / 2) + c] = src[0][i];
-            dst[0][r * (kW1Ld / 2) + kSurInPad / 2 + c] = src[0][i];
-        }
-        const int cnt[4] = {0, kW2 / 2, kW2 / 2, kW4 / 2};
-        for (int t = 1; t < 4; ++t)
-            for (int i = threadIdx.x; i < cnt[t]; i += kSurBlock) dst[t][i] = src[t][i];
-        for (int i = threadIdx.x; i < kSurHid; i += kSurBlock) {
-            bb[i] = net.b1[i];
-            bb[kSurHid + i] = net.b2[i];
-            bb[2 * kSurHid + i] = net.b3[i];
-        }
-        if (threadIdx.x < kSurOutPad) {
-            bb[3 * kSurHid + threadIdx.x] = net.b4[threadIdx.x];
-            bb[3 * kSurHid + kSurOutPad + threadIdx.x] = nrm->y_mean[threadIdx.x];
-            bb[3 * kSurHid + 2 * kSurOutPad + threadIdx.x] = nrm->y_std[threadIdx.x];
-        }
+// kTcGroups warpgroups per CTA work on their own tiles (own operand buffers, mbarrier and
+// tensor-memory columns) against the shared weights, so one group's epilogue overlaps the
+// other's tensor-core work and epilogue.
+__global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
+    k_sur_mlp_tc(SurNet net, const SurNorm *__restrict__ nrm, const __nv_bfloat16 *__restrict__ X,
+                 float *__restrict__ pred, long mpad, unsigned *__restrict__ status) {
+    extern __shared__ __align__(128) unsigned char sm[];
+    const int tid = threadIdx.x, warp = tid >> 5, g = tid / kTcRows, t = tid % kTcRows;
+    const int nthr = kTcRows * kTcGroups;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(sm);
+    float *bb = reinterpret_cast<float *>(sm + kTcB);  // b1 b2 b3, b4, y_mean, y_std
+    // weights into the canonical layout: W1 as [W1 | W1] (values and remainders), W2, W3, W4
+    for (int i = tid; i < kSurHid * (kSurInX / 8); i += nthr) {
+        const int r = i / (kSurInX / 8), c = i % (kSurInX / 8);
+        *reinterpret_cast<uint4 *>(sm + kTcW1 + tc_off(r, c * 8, kSurInX)) =
+            *reinterpret_cast<const uint4 *>(net.w1 + r * kSurInPad + (c % 2) * 8);
     }
+    for (int i = tid; i < kSurHid * (kSurHid / 8); i += nthr) {
+        const int r = i / (kSurHid / 8), c = i % (kSurHid / 8);
+        *reinterpret_cast<uint4 *>(sm + kTcW2 + tc_off(r, c * 8, kSurHid)) =
+            *reinterpret_cast<const uint4 *>(net.w2 + r * kSurLd + c * 8);
+        *reinterpret_cast<uint4 *>(sm + kTcW3 + tc_off(r, c * 8, kSurHid)) =
+            *reinterpret_cast<const uint4 *>(net.w3 + r * kSurLd + c * 8);
+    }
+    for (int i = tid; i < kSurOutPad * (kSurHid / 8); i += nthr) {
+        const int r = i / (kSurHid / 8), c = i % (kSurHid / 8);
+        *reinterpret_cast<uint4 *>(sm + kTcW4 + tc_off(r, c * 8, kSurHid)) =
+            *reinterpret_cast<const uint4 *>(net.w4 + r * kSurLd + c * 8);
+    }
+    for (int i = tid; i < kSurHid; i += nthr) {
+        bb[i] = net.b1[i];
+        bb[kSurHid + i] = net.b2[i];
+        bb[2 * kSurHid + i] = net.b3[i];
+    }
+    if (tid < kSurOutPad) {
+        bb[3 * kSurHid + tid] = net.b4[tid];
+        bb[3 * kSurHid + kSurOutPad + tid] = nrm->y_mean[tid];
+        bb[3 * kSurHid + 2 * kSurOutPad + tid] = nrm->y_std[tid];
+    }
+    volatile int *err = reinterpret_cast<volatile int *>(sm + kTcErr);
+    if (tid < kTcGroups) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(base + kTcBar + 8u * tid) : "memory");
+        err[tid] = 0;
+    }
+    if (tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kTcSlot),
+                     "r"(kTcCols * kTcGroups)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+    tc_fence_after();
+    const uint32_t tbase = *reinterpret_cast<volatile uint32_t *>(sm + kTcSlot);
+    const uint32_t tmem = tbase + kTcCols * (uint32_t)g;                     // this group's accumulator
+    const uint32_t trow = tmem + ((uint32_t)((warp % 4) * 32) << 16);        // this warp's lane quarter
+    const uint32_t bar = base + kTcBar + 8u * (uint32_t)g;
+    const uint32_t gA = base + kTcG + (uint32_t)(g * kTcGBytes) + kTcA, gX = base + kTcG + (uint32_t)(g * kTcGBytes) + kTcX;
+    unsigned char *smA = sm + kTcG + g * kTcGBytes + kTcA, *smX = sm + kTcG + g * kTcGBytes + kTcX;
     const float *ym = bb + 3 * kSurHid + kSurOutPad, *ys = ym + kSurOutPad;
-    for (long tile = (long)blockIdx.x * 4 + warp; tile < ntiles; tile += (long)gridDim.x * 4) {
-        const long r0 = tile * 16;
-        unsigned a1[2][4];  // k-slice 0: the feature values, 1: the remainders
+    const uint32_t wl[4] = {base + kTcW1, base + kTcW2, base + kTcW3, base + kTcW4};
+    uint32_t phase = 0;
+    bool ok = true;
+    const long ntiles = (mpad + kTcRows - 1) / kTcRows;
+    for (long tile = (long)blockIdx.x * kTcGroups + g; tile < ntiles && ok; tile += (long)gridDim.x * kTcGroups) {
+        const long row = tile * kTcRows + t;
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const __nv_bfloat16 *xr = X + (r0 + gid) * kSurInX + kSurInPad * s + 2 * tig;
-            a1[s][0] = *reinterpret_cast<const unsigned *>(xr);
-            a1[s][1] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInX);
-            a1[s][2] = *reinterpret_cast<const unsigned *>(xr + 8);
-            a1[s][3] = *reinterpret_cast<const unsigned *>(xr + 8 * kSurInX + 8);
+        for (int c = 0; c < kSurInX / 8; ++c) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (row < mpad) v = *reinterpret_cast<const uint4 *>(X + row * kSurInX + c * 8);
+            *reinterpret_cast<uint4 *>(smX + tc_off(t, c * 8, kSurInX)) = v;
         }
-        float acc[kSurHid / 8][4];
-        unsigned afr[kSurHid / 16][4];
-        mlp_layer<2, kSurHid / 8, kW1Ld>(a1, w1, bb, acc, gid, tig);
-        gelu_to_frag(acc, afr);
-        mlp_layer<kSurHid / 16, kSurHid / 8, kSurLd>(afr, w2, bb + kSurHid, acc, gid, tig);
-        gelu_to_frag(acc, afr);
-        mlp_layer<kSurHid / 16, kSurHid / 8, kSurLd>(afr, w3, bb + 2 * kSurHid, acc, gid, tig);
-        gelu_to_frag(acc, afr);
-        float out[kSurOutPad / 8][4];
-        mlp_layer<kSurHid / 16, kSurOutPad / 8, kSurLd>(afr, w4, bb + 3 * kSurHid, out, gid, tig);
+        tc_sync(g);
+        for (int L = 0; L < 4 && ok; ++L) {
+            if (t == 0)
+                tc_layer(tmem, L == 0 ? gX : gA, wl[L], L == 0 ? kSurInX : kSurHid, L == 3 ? kSurOutPad : kSurHid,
+                         bar);
+            if (!tc_wait(bar, phase)) err[g] = 1;
+            group_bar(g);
+            tc_fence_after();
+            ok = err[g] == 0;
+            if (!ok) break;
+            phase ^= 1u;
+            if (L < 3) {
+                const float *b = bb + L * kSurHid;
+#pragma unroll 1
+                for (int cb = 0; cb < kSurHid / 32; ++cb) {
+                    uint32_t r[32];
+                    tc_ld32(trow + (uint32_t)(cb * 32), r);
+                    tc_wait_ld();
 #pragma unroll
-        for (int j = 0; j < kSurOutPad / 8; ++j)
+                    for (int j = 0; j < 32; j += 8) {
+                        uint4 o;
+                        const int k = cb * 32 + j;
+                        o.x = pack_bf16(gelu_f(__uint_as_float(r[j]) + b[k]), gelu_f(__uint_as_float(r[j + 1]) + b[k + 1]));
+                        o.y = pack_bf16(gelu_f(__uint_as_float(r[j + 2]) + b[k + 2]),
+                                        gelu_f(__uint_as_float(r[j + 3]) + b[k + 3]));
+                        o.z = pack_bf16(gelu_f(__uint_as_float(r[j + 4]) + b[k + 4]),
+                                        gelu_f(__uint_as_float(r[j + 5]) + b[k + 5]));
+                        o.w = pack_bf16(gelu_f(__uint_as_float(r[j + 6]) + b[k + 6]),
+                                        gelu_f(__uint_as_float(r[j + 7]) + b[k + 7]));
+                        *reinterpret_cast<uint4 *>(smA + tc_off(t, k, kSurHid)) = o;
+                    }
+                }
+            } else {
+                uint32_t r[16];
+                tc_ld16(trow, r);
+                tc_wait_ld();
+                if (row < mpad) {
+                    const float *b4 = bb + 3 * kSurHid;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int c = 8 * j + 2 * tig;
-                const long r = r0 + gid + 8 * h;
-                pred[r * kSurOutPad + c] = out[j][2 * h] * ys[c] + ym[c];
-                pred[r * kSurOutPad + c + 1] = out[j][2 * h + 1] * ys[c + 1] + ym[c + 1];
+                    for (int c = 0; c < kSurOutPad; c += 4) {
+                        float4 o;
+                        o.x = (__uint_as_float(r[c]) + b4[c]) * ys[c] + ym[c];
+                        o.y = (__uint_as_float(r[c + 1]) + b4[c + 1]) * ys[c + 1] + ym[c + 1];
+                        o.z = (__uint_as_float(r[c + 2]) + b4[c + 2]) * ys[c + 2] + ym[c + 2];
+                        o.w = (__uint_as_float(r[c + 3]) + b4[c + 3]) * ys[c + 3] + ym[c + 3];
+                        *reinterpret_cast<float4 *>(pred + row * kSurOutPad + c) = o;
+                    }
+                }
             }
+            tc_sync(g);
+        }
     }
+    if (!ok) {  // the tensor core may still be working on the timed-out layer: one more bounded wait
+        if (t == 0) atomicOr(status, (unsigned)LBMGPU_ST_SURROGATE);
+        tc_wait(bar, phase);
+        tc_fence_after();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcCols * kTcGroups)
+                     : "memory");
 }
-
-constexpr size_t kMlpSmem = (size_t)(kW1s + 2 * kW2 + kW4) * 2 + (size_t)(3 * kSurHid + 3 * kSurOutPad) * 4;
 
 // -------------------------------------------------------------------------------------
 // Training kernels.
@@ -529,10 +651,10 @@ SurNet net_of(const SurState &s) {
 
 int run_mlp(lbmgpu *h, const __nv_bfloat16 *X, float *pred, long mpad) {
     SurState &s = *h->sur;
-    CK(cudaFuncSetAttribute(k_sur_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMlpSmem));
-    const long ntiles = mpad / 16;
-    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>((ntiles + 3) / 4, 148 * 2));
-    k_sur_mlp<<<grid, kSurBlock, kMlpSmem, h->stream>>>(net_of(s), s.nrm, X, pred, ntiles);
+    CK(cudaFuncSetAttribute(k_sur_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    const long ntiles = (mpad + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>((ntiles + kTcGroups - 1) / kTcGroups, 148));
+    k_sur_mlp_tc<<<grid, kTcRows * kTcGroups, kTcSmem, h->stream>>>(net_of(s), s.nrm, X, pred, mpad, h->status);
     CK(cudaGetLastError());
     return 0;
 }
