@@ -18,6 +18,17 @@ enum CellType : int {
     T_F = 0, T_S = 1, T_P = 2, T_A = 3, T_FS = 4, T_I = 5, T_O = 6, T_I_C = 7, T_O_C = 8, T_Q = 9
 };
 
+// Lattice indices (i, j, k) of cell n = i si + j sj + k with sj = Nz, si = Ny Nz.
+// lbmgpu_create admits lattices of fewer than 2^31 cells, so 32-bit unsigned division
+// gives the same integers as 64-bit division at a fraction of its cost.
+__host__ __device__ __forceinline__ void cell_ijk(long n, long si, long sj, int &i, int &j, int &k) {
+    const unsigned u = (unsigned)n, usi = (unsigned)si, usj = (unsigned)sj;
+    const unsigned ui = u / usi, r = u - ui * usi, uj = r / usj;
+    i = (int)ui;
+    j = (int)uj;
+    k = (int)(r - uj * usj);
+}
+
 // Per-cell flags of the device's cell classification: a fluid cell, and one with a
 // boundary cell (anything but fluid or a periodic ghost) upstream along some direction.
 enum : uint8_t { CF_FLUID = 1, CF_SPECIAL = 2 };

@@ -52,7 +52,8 @@ __device__ __forceinline__ void cell_diag(const DiagSrc &S, long n, double *v) {
     const double u = R[RM_U * nc + n], w = R[RM_W * nc + n], vv = R[RM_V * nc + n];
     const double uu = u * u + vv * vv + w * w;
     v[0] = rho * uu;
-    const int i = (int)(n / S.si), j = (int)((n / S.sj) % S.Ny), k = (int)(n % S.Nz);
+    int i, j, k;
+    cell_ijk(n, S.si, S.sj, i, j, k);
     int ia, ib, ja, jb, ka, kb;
     wrap_nb(i, S.Nx, ib, ia);
     wrap_nb(j, S.Ny, jb, ja);

@@ -368,7 +368,8 @@ MC_HD bool mc_face_dir(int l) { return csq(l) == 1; }
 template <int NS, class AT>
 MC_HDN void mc_special_cell(const AT &A, long n, long b) {
     const gas::Tables &t = *A.tab;
-    const int i = (int)(n / A.si), j = (int)((n / A.sj) % A.Ny), k = (int)(n % A.Nz);
+    int i, j, k;
+    cell_ijk(n, A.si, A.sj, i, j, k);
     double f[NS + 1][27];
     // ---- streaming (src/lbm-streaming.cpp:15-107)
     for (int l = 0; l < 27; ++l) {

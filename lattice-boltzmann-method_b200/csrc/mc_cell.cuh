@@ -170,7 +170,8 @@ struct McPull {
 };
 template <class AT>
 MC_HD void mc_pull(const AT &A, long n, McPull &p) {
-    const int i = (int)(n / A.si), j = (int)((n / A.sj) % A.Ny), k = (int)(n % A.Nz);
+    int i, j, k;
+    cell_ijk(n, A.si, A.sj, i, j, k);
     const int im = (i - 1 == 0) ? A.Nx - 2 : i - 1, ip = (i + 1 == A.Nx - 1) ? 1 : i + 1;
     const int jm = (j - 1 == 0) ? A.Ny - 2 : j - 1, jp = (j + 1 == A.Ny - 1) ? 1 : j + 1;
     const int km = (k - 1 == 0) ? A.Nz - 2 : k - 1, kp = (k + 1 == A.Nz - 1) ? 1 : k + 1;

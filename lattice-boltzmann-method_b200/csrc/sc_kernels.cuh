@@ -62,9 +62,8 @@ struct PullSrc {
 };
 
 __device__ __forceinline__ void pull_src(const ScGeom &g, long n, PullSrc &s) {
-    const int i = (int)(n / g.si);
-    const int j = (int)((n / g.sj) % g.Ny);
-    const int k = (int)(n % g.Nz);
+    int i, j, k;
+    cell_ijk(n, g.si, g.sj, i, j, k);
     const int im = (i - 1 == 0) ? g.Nx - 2 : i - 1, ip = (i + 1 == g.Nx - 1) ? 1 : i + 1;
     const int jm = (j - 1 == 0) ? g.Ny - 2 : j - 1, jp = (j + 1 == g.Ny - 1) ? 1 : j + 1;
     const int km = (k - 1 == 0) ? g.Nz - 2 : k - 1, kp = (k + 1 == g.Nz - 1) ? 1 : k + 1;
@@ -118,9 +117,8 @@ __device__ __forceinline__ void pull_special(const ScGeom &g, const int8_t *__re
                                              const double *__restrict__ pop, const double *__restrict__ stale,
                                              long nb_stride, double f[27], double ge[27]) {
     const long nc = g.ncell;
-    const int i = (int)(n / g.si);
-    const int j = (int)((n / g.sj) % g.Ny);
-    const int k = (int)(n % g.Nz);
+    int i, j, k;
+    cell_ijk(n, g.si, g.sj, i, j, k);
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
         int in = i - cx(l), jn = j - cy(l), kn = k - cz(l);
@@ -200,9 +198,8 @@ __device__ __forceinline__ void local_state_sc(const ScGeom &g, const ScPhys &P,
 static __device__ void tms_cell_sc(const ScGeom &g, const ScPhys &P, const int8_t *__restrict__ type,
                             const double *__restrict__ mom, long n, double f[27], double ge[27]) {
     const long nc = g.ncell;
-    const int i = (int)(n / g.si);
-    const int j = (int)((n / g.sj) % g.Ny);
-    const int k = (int)(n % g.Nz);
+    int i, j, k;
+    cell_ijk(n, g.si, g.sj, i, j, k);
     double ft[27], gt[27], fl[27], gl[27];
     // ---- outflow: first direction with an outflow cell upstream and fluid downstream
     {
