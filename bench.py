@@ -69,7 +69,7 @@ def parse():
                     help="reacting workloads: the reference's explicit scheme, the ROS2 stiff integrator, or "
                          "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
                          "surrogate steps with a 1 %% audit; plain ROS2 timed on the same lattice beside it)")
-    ap.add_argument("--teach", type=int, default=60, help="surrogate: ROS2 teacher steps that collect samples")
+    ap.add_argument("--teach", type=int, default=200, help="surrogate: ROS2 teacher steps that collect ~2M samples")
     ap.add_argument("--epochs", type=int, default=16, help="surrogate: training epochs over the samples")
     ap.add_argument("--compare", type=int, default=100,
                     help="surrogate: steps run twice from the same state, with the surrogate and with plain ROS2, "
@@ -420,28 +420,35 @@ def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
     return dt
 
 
-def surrogate_vs_plain(lat, mix, sp, K):
-    """From the lattice's current state, K steps with the surrogate (1 % audit) and, after
-    restoring the state, K steps of plain ROS2: the north star's comparison -- peak
-    temperature and heat release integrated over the cells and the K steps -- from the
-    device diagnostics (lbmgpu_diagnostics) after every step."""
+def surrogate_vs_plain(lat, mix, sp, K, refresh_s, cap):
+    """From the lattice's current state, K steps with the surrogate (1 % audit; the audited
+    states collected and the network refreshed from them every 50 steps, timed into
+    refresh_s) and, after restoring the state, K steps of plain ROS2: the north star's
+    comparison -- peak temperature and heat release integrated over the cells and the K
+    steps -- from the device diagnostics (lbmgpu_diagnostics) after every step."""
     import lbmgpu
     import workloads
     c0 = mix.copy()
     s0 = [a.copy() for a in sp]
     lat.download(c0, s0)
     d0 = lat.diagnostics()
-    runs = {}
+    runs, status = {}, {}
     for name, on in (("surrogate", True), ("plain", False)):
         lat.upload(c0, s0)
         lat.surrogate_enable(on, audit_period=100)
+        lat.surrogate_collect(on, stride=100, capacity=cap)
         hrr, tpk = 0.0, d0["T_max"]
-        for _ in range(K):
+        for k in range(K):
+            if on and k > 0 and k % 50 == 0:
+                t0 = time.perf_counter()
+                lat.surrogate_train(epochs=2, batch=4096, lr=5e-4, seed=20261204 + k)
+                refresh_s.append(time.perf_counter() - t0)
             lat.step(1)
             d = lat.diagnostics()
             hrr += d["hrr"]
             tpk = max(tpk, d["T_max"])
         runs[name] = (hrr, tpk, d["T_max"])
+        status[name] = lat.synchronize()
     kelvin = lbmgpu.units_from_dx_dt(*workloads.FLAME_UNITS)[3]
     (hs, ps, fs), (hp, pp, fp) = runs["surrogate"], runs["plain"]
     return {"compare_steps": K,
@@ -450,7 +457,7 @@ def surrogate_vs_plain(lat, mix, sp, K):
             "peak_T_rise_rel_err": abs(ps - pp) / max(abs(pp - d0["T_max"]), 1e-300),
             "final_T_max_rel_err": abs(fs - fp) / abs(fp),
             "heat_release_integrated": {"surrogate": hs, "plain": hp, "unit": "lattice (sum over cells and steps)"},
-            "heat_release_rel_err": abs(hs - hp) / max(abs(hp), 1e-300)}
+            "heat_release_rel_err": abs(hs - hp) / max(abs(hp), 1e-300), "compare_status": status}
 
 
 def run_ours_mc(args, dist):
@@ -500,6 +507,10 @@ def run_ours_mc(args, dist):
         n_samples = lat.surrogate_stats()["samples"]
         lat.surrogate_enable(True, audit_period=100)
         sur_params = lat.surrogate_params()
+        # online: from here on the audited states are collected, and the network is refreshed
+        # from them between the measurements and every 50 steps of the comparison run
+        sur_cap = n_samples + (200 + args.compare) * (-(-mix.size // 100))
+        lat.surrogate_collect(True, stride=100, capacity=sur_cap)
         sur = {"teacher_steps": args.teach, "sample_stride": stride, "samples_rows": n_samples,
                "teacher_s": t_teach, "augmented_rows": n_aug, "augment_s": t_aug, "train_epochs": args.epochs, "train_s": t_train, "train_loss": loss}
     lat.time_steps(max(3, args.warmup))
@@ -524,7 +535,11 @@ def run_ours_mc(args, dist):
     launches, kms = lat.kernel_times()
     lat.profile(False)
     if use_sur:
+        t0 = time.perf_counter()
+        lat.surrogate_train(epochs=2, batch=4096, lr=5e-4, seed=20261204)
+        sur["refresh_s"] = [time.perf_counter() - t0]
         # plain ROS2 on the same lattice and state, for the comparison
+        lat.surrogate_collect(False)
         lat.surrogate_enable(False)
         kp = min(args.steps, 10)
         ms_plain = lat.time_steps(kp)
@@ -532,7 +547,7 @@ def run_ours_mc(args, dist):
         sur["surrogate_ms_per_step"] = kms[4] / max(kk, 1)
         sur["network_flops_per_cell"] = 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)
         if args.compare > 0:
-            sur.update(surrogate_vs_plain(lat, mix, sp, args.compare))
+            sur.update(surrogate_vs_plain(lat, mix, sp, args.compare, sur["refresh_s"], sur_cap))
     lat.close()
     avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_gather": kms[1] / max(launches[1], 1),
            "k_mc_solve": kms[5] / max(launches[5], 1), "k_mc_props": kms[3] / max(launches[3], 1)}

@@ -241,13 +241,19 @@ int lbmgpu_diagnostics(lbmgpu_t *h, double *out, int n_out);
  * (12 -> 128 -> 128 -> 128 -> 10, GELU, BF16 weights and activations, FP32 accumulation,
  * standardised inputs and outputs) from samples the integrator writes during the run,
  * then replaces it cell by cell: the predicted dY is projected (orthogonally) onto changes
- * that conserve every element, cells whose features leave the training box (widened by 5 %) or whose
- * prediction is not finite run the integrator, and 1 in audit_period cells (0: none) runs
- * it as well, takes its result and scores the prediction (L1 error of dY).
+ * that conserve every element; cells whose features leave the training box (widened by
+ * 5 %), whose prediction is not finite or lies beyond 16 standard deviations of the
+ * training targets, or whose projected change would take a mass fraction below -1e-12 run
+ * the integrator; and every audit_period-th cell (0: none; the phase moves from step to
+ * step) runs it as well, takes its result and scores the prediction (L1 error of dY).
  *
  * lbmgpu_surrogate_collect: while enabled, each step's integrator writes the features and
- *   targets of every stride-th cell (a different subset each step) to a device sample set
- *   of `capacity` rows; collection stops when it is full.
+ *   targets of every stride-th cell (a different subset each step) to the device sample
+ *   set, grown to `capacity` rows with the rows already there kept; collection stops when
+ *   it is full.  During surrogate steps the rows come from the audit stride instead (the
+ *   audited cells and those outside the training box on it -- states the integrator
+ *   computes anyway), so the set follows the run and lbmgpu_surrogate_train can refresh
+ *   the network as the run leaves the states it was trained on.
  * lbmgpu_surrogate_load_samples: replaces the sample set by n host rows (x: n x 12 raw
  *   features, y: n x 10 raw targets).
  * lbmgpu_surrogate_samples: copies the first n rows of the sample set to the host (x, y as

@@ -493,18 +493,25 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
     double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
     bool have_pred = false;
     if (S.mode == 1 && !S.gate[n]) {
+        // the prediction is used if it is finite, every output lies within kSurOutGate
+        // standard deviations of the training targets, and after the element projection no
+        // mass fraction goes below -kSurNegTol; otherwise the integrator takes the cell
         const float *pr = S.pred + n * kSurOutPad;
+        const SurNorm &nm = *S.nrm;
         double dY[NS];
-        have_pred = isfinite(pr[NS]);
+        have_pred = isfinite(pr[NS]) && fabsf((pr[NS] - nm.y_mean[NS]) / nm.y_std[NS]) <= kSurOutGate;
         for (int a = 0; a < NS; ++a) {
             dY[a] = (double)pr[a];
-            have_pred = have_pred && isfinite(dY[a]);
+            have_pred = have_pred && isfinite(dY[a]) && fabsf((pr[a] - nm.y_mean[a]) / nm.y_std[a]) <= kSurOutGate;
         }
-        if (have_pred) sur_conserve<NS>(S.proj, dY);
+        if (have_pred) {
+            sur_conserve<NS>(S.proj, dY);
+            for (int a = 0; a < NS; ++a) have_pred = have_pred && Y[a] + dY[a] >= -kSurNegTol;
+        }
         for (int a = 0; a < NS; ++a) Yp[a] = Y[a] + dY[a];
         Tp = T_si + (double)pr[NS];
     }
-    const bool audit = have_pred && S.audit_period > 0 && sur_hash((unsigned)n, S.step) % S.audit_period == 0;
+    const bool audit = have_pred && S.audit_period > 0 && (unsigned)(n % S.audit_period) == S.audit_phase;
     if (S.mode == 1 && (defer || !S.ilist)) {
         count_flag(&S.audit[3], audit);
         count_flag(&S.audit[4], have_pred && !audit);
@@ -548,7 +555,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
         S.audit[1] += den;
 #endif
     }
-    if (S.ds_x && !have_pred && (long)(n % S.ds_stride) == S.ds_phase) {
+    if (S.ds_x && (!have_pred || audit) && (long)(n % S.ds_stride) == S.ds_phase) {
         const long row = S.ds_base + n / S.ds_stride;
         if (row < S.ds_cap) {
             sur_features<NS>(T_si, P_si, Y, dt_si, S.ds_x + row * kSurIn);

@@ -352,12 +352,16 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
 // Training kernels.
 // -------------------------------------------------------------------------------------
 // C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T (accum: C +=), A and B BF16 row-major with
-// leading dimensions lda, ldb (even), K a multiple of 16.  Block: 4 warps, each 16 rows x 64 columns.
+// leading dimensions lda, ldb (even), K a multiple of 16.  With gridDim.z > 1 block z
+// takes the z-th of gridDim.z equal slices of K (each a multiple of 16) and writes its
+// partial product to C + z zstride (split K, summed afterwards by k_sum_splits).  Block: 4 warps, each 16 rows x 64 columns.
 __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict__ Am, int lda,
                                                  const __nv_bfloat16 *__restrict__ Bm, int ldb, float *__restrict__ C,
-                                                 int ldc, int M, int N, int K, int accum = 0) {
+                                                 int ldc, int M, int N, int K, int accum = 0, long zstride = 0) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
     const int r0 = blockIdx.y * 64 + warp * 16, n0 = blockIdx.x * 64;
+    const int kc = K / (int)gridDim.z, kbeg = (int)blockIdx.z * kc;
+    C += (long)blockIdx.z * zstride;
     float acc[8][4] = {};
     auto lda32 = [&](int r, int k) -> unsigned {
         return r < M ? *reinterpret_cast<const unsigned *>(Am + (long)r * lda + k) : 0u;
@@ -365,7 +369,7 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
     auto ldb32 = [&](int n, int k) -> unsigned {
         return n < N ? *reinterpret_cast<const unsigned *>(Bm + (long)n * ldb + k) : 0u;
     };
-    for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int k0 = kbeg; k0 < kbeg + kc; k0 += 16) {
         unsigned a[4];
         a[0] = lda32(r0 + gid, k0 + 2 * tig);
         a[1] = lda32(r0 + gid + 8, k0 + 2 * tig);
@@ -386,6 +390,17 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
             if (r < M && c + 1 < N)
                 C[(long)r * ldc + c + 1] = acc[j][2 * h + 1] + (accum ? C[(long)r * ldc + c + 1] : 0.f);
         }
+}
+
+// out[r][c] = sum_z part[z][r][c] over the split-K slices, in slice order, for the
+// cols real columns of rows of width ld (the padding columns of out are left alone).
+__global__ void k_sum_splits(const float *__restrict__ part, int splits, long n, int cols, int ld,
+                             float *__restrict__ out) {
+    const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n || (int)(e % ld) >= cols) return;
+    float v = 0.f;
+    for (int z = 0; z < splits; ++z) v += part[(long)z * n + e];
+    out[e] = v;
 }
 
 // Z = C + b; H = GELU(Z) in BF16 (rows of width W).
@@ -457,13 +472,24 @@ __global__ void k_transpose_bf16(const __nv_bfloat16 *__restrict__ in, int ldi, 
     }
 }
 
-// db[c] = sum_r dZ[r][c], one thread per column, rows summed in order.
-__global__ void k_colsum(const float *__restrict__ dZ, long rows, int W, float *__restrict__ db) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= W) return;
+// db[c] = sum_r dZ[r][c] for a block of 32 columns: lane = column, warp w sums rows
+// w, w + 8, ... in order (a warp reads 32 consecutive floats of a row), then the 8 warp
+// sums are added in warp order -- a fixed order, so the result does not vary run to run.
+constexpr int kColsumWarps = 8;
+__global__ void __launch_bounds__(32 * kColsumWarps) k_colsum(const float *__restrict__ dZ, long rows, int W,
+                                                               float *__restrict__ db) {
+    __shared__ double part[kColsumWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, c = blockIdx.x * 32 + lane;
     double s = 0.0;
-    for (long r = 0; r < rows; ++r) s += dZ[r * W + c];
-    db[c] = (float)s;
+    if (c < W)
+        for (long r = warp; r < rows; r += kColsumWarps) s += dZ[r * W + c];
+    part[warp][lane] = s;
+    __syncthreads();
+    if (warp == 0 && c < W) {
+        double t = 0.0;
+        for (int w = 0; w < kColsumWarps; ++w) t += part[w][lane];
+        db[c] = (float)t;
+    }
 }
 
 // Adam on FP32 master parameters; the BF16 copy (if any) follows.  g at gradient stride.
@@ -569,7 +595,7 @@ struct SurState {
     float *ds_x = nullptr, *ds_y = nullptr;
     uint8_t *ds_valid = nullptr;
     long ds_cap = 0, ds_next = 0;
-    int collect = 0, stride = 64, collect_steps = 0;
+    int collect = 0, stride = 64, collect_steps = 0, step_stride = 64;
     // inference
     __nv_bfloat16 *feat = nullptr;
     uint8_t *gate = nullptr;
@@ -725,6 +751,7 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
     a.proj = s->proj;
     a.audit = s->audit;
     a.audit_period = s->audit_period;
+    a.audit_phase = s->audit_period ? (unsigned)((7919ull * s->step) % s->audit_period) : 0u;
     a.step = s->step;
     a.dt_si = (double)h->d.dt_sim * (double)h->U.s;
     if (s->collect && s->ds_x) {
@@ -732,8 +759,12 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
         a.ds_y = s->ds_y;
         a.ds_valid = s->ds_valid;
         a.ds_cap = s->ds_cap;
-        a.ds_stride = s->stride;
-        a.ds_phase = (int)((7L * s->collect_steps) % s->stride);
+        // surrogate steps collect on the audit stride (the states the integrator takes
+        // anyway), teacher steps on the collection stride
+        const bool online = s->enabled && s->audit_period > 0;
+        s->step_stride = online ? (int)s->audit_period : s->stride;
+        a.ds_stride = s->step_stride;
+        a.ds_phase = online ? (int)a.audit_phase : (int)((7L * s->collect_steps) % s->stride);
         a.ds_base = s->ds_next;
     }
     if (s->enabled) {
@@ -768,6 +799,7 @@ int sur_prepare_t(lbmgpu *h, McArgsT<S, double> &A) {
         a.mode = 1;
         a.pred = s->pred;
         a.gate = s->gate;
+        a.nrm = s->nrm;
         a.ilist = s->ilist;
         a.icount = s->icount;
     }
@@ -780,7 +812,7 @@ void sur_after_step(lbmgpu *h) {
     SurState *s = h->sur;
     if (!s || h->chem != CHEM_ROSENBROCK) return;
     if (s->collect && s->ds_x) {
-        s->ds_next += (h->g.ncell + s->stride - 1) / s->stride;
+        s->ds_next += (h->g.ncell + s->step_stride - 1) / s->step_stride;
         s->collect_steps += 1;
         if (s->ds_next >= s->ds_cap) s->collect = 0;  // full
     }
@@ -914,7 +946,7 @@ int lbmgpu_surrogate_collect(lbmgpu_t *h, int enable, int stride, long capacity)
         return LBMGPU_OK;
     }
     if (stride < 1 || capacity < 16) return LBMGPU_E_ARG;
-    rc = ensure_samples(h, capacity);
+    rc = grow_samples(h, capacity);  // keeps the rows collected so far
     if (rc) return rc;
     s.stride = stride;
     s.collect = s.ds_next < s.ds_cap ? 1 : 0;
@@ -1013,8 +1045,16 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
     double *part = nullptr;
     const long BH = (long)B * kSurHid;
     const unsigned nparts = blocks((long)B * kSurOutPad);
+    const long nbatch = ((long)rows.size() + B - 1) / B, total = std::max<long>(1, (long)epochs * nbatch);
+    int ksplit = 1;  // slices of the batch for the weight gradients: each a multiple of 16 rows
+    for (int c : {32, 16, 8, 4, 2})
+        if ((B / 16) % c == 0) {
+            ksplit = c;
+            break;
+        }
+    float *Gp = nullptr;  // the weight gradients' split-K partials
     auto all = [&]() {
-        int r = dalloc(h, &idx, B);
+        int r = dalloc(h, &idx, rows.size());
         if (!r) r = dalloc(h, &Xb, (size_t)B * kSurInX);
         if (!r) r = dalloc(h, &Yb, (size_t)B * kSurOutPad);
         if (!r) r = dalloc(h, &vb, B);
@@ -1031,7 +1071,9 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
         if (!r) r = dalloc(h, &T1, BH);
         if (!r) r = dalloc(h, &T2, BH);
         if (!r) r = dalloc(h, &Wt, (size_t)kSurHid * kSurLd);
-        if (!r) r = dalloc(h, &part, nparts);
+        if (!r) r = dalloc(h, &part, (size_t)nparts * nbatch);
+        if (!r) r = dalloc(h, &Gp, (size_t)ksplit * kSurHid * kSurLd);
+        if (!r && cudaMemsetAsync(Gp, 0, (size_t)ksplit * kSurHid * kSurLd * sizeof(float), h->stream)) r = LBMGPU_E_CUDA;
         return r;
     };
     rc = all();
@@ -1039,25 +1081,26 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     SurNet net = net_of(s);
     double epoch_loss = 0.0;
-    std::vector<double> parts(nparts);
     const int ldw[4] = {kSurInPad, kSurLd, kSurLd, kSurLd};
     const int kin[4] = {kSurInPad, kSurHid, kSurHid, kSurHid};
     const int nout[4] = {kSurHid, kSurHid, kSurHid, kSurOutPad};
     dim3 tb(32, 8);
     // the step size decays from lr to 0 along a half cosine over the call's Adam steps
-    const long nbatch = ((long)rows.size() + B - 1) / B, total = std::max<long>(1, (long)epochs * nbatch);
     long step_in_call = 0;
+    std::vector<double> parts((size_t)nparts * nbatch);
     for (int ep = 0; ep < epochs && !rc; ++ep) {
+        // the epoch's order in one copy; the batches run without waiting for the host, and
+        // the per-batch squared-error partials come back once at the end of the epoch
         std::shuffle(rows.begin(), rows.end(), rng);
-        double sum_se = 0.0;
+        if (cudaMemcpyAsync(idx, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream)) {
+            rc = LBMGPU_E_CUDA;
+            break;
+        }
         long sum_n = 0;
-        for (size_t b0 = 0; b0 < rows.size() && !rc; b0 += B) {
+        long bi = 0;
+        for (size_t b0 = 0; b0 < rows.size() && !rc; b0 += B, ++bi) {
             const int nb = (int)std::min<size_t>(B, rows.size() - b0);
-            if (cudaMemcpyAsync(idx, rows.data() + b0, nb * sizeof(int), cudaMemcpyHostToDevice, h->stream)) {
-                rc = LBMGPU_E_CUDA;
-                break;
-            }
-            k_gather_batch<<<blocks(B), 256, 0, h->stream>>>(s.ds_x, s.ds_y, idx, nb, B, s.nrm, Xb, Yb, vb);
+            k_gather_batch<<<blocks(B), 256, 0, h->stream>>>(s.ds_x, s.ds_y, idx + b0, nb, B, s.nrm, Xb, Yb, vb);
             // forward
             const __nv_bfloat16 *in = Xb;
             __nv_bfloat16 *Hs[3] = {H1, H2, H3};
@@ -1075,22 +1118,25 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
             }
             k_gemm_tn<<<dim3(1, (B + 63) / 64), 128, 0, h->stream>>>(H3, kSurHid, net.w4, kSurLd, C, kSurOutPad, B,
                                                                        kSurOutPad, kSurHid);
-            k_out_loss<<<nparts, 256, 0, h->stream>>>(C, net.b4, Yb, vb, (float)nb, dA, part, B);
+            k_out_loss<<<nparts, 256, 0, h->stream>>>(C, net.b4, Yb, vb, (float)nb, dA, part + (size_t)bi * nparts, B);
             // backward: dA holds dL/d(pre-activation) of the current layer (FP32), rows x nout
             float *gw[4] = {s.g + off_w(0), s.g + off_w(1), s.g + off_w(2), s.g + off_w(3)};
             float *gb[4] = {s.g + off_w(4), s.g + off_w(5), s.g + off_w(6), s.g + off_w(7)};
             for (int L = 3; L >= 0; --L) {
                 const int no = nout[L], ki = kin[L];
                 // bias gradient
-                k_colsum<<<blocks(no, 128), 128, 0, h->stream>>>(dA, B, no, gb[L]);
+                k_colsum<<<(no + 31) / 32, 32 * kColsumWarps, 0, h->stream>>>(dA, B, no, gb[L]);
                 // dZ^T [no][B] and input^T [ki][B] for the weight gradient dW = dZ^T in
                 k_f32_to_bf16<<<blocks((long)B * no), 256, 0, h->stream>>>(dA, dZb, (long)B * no);
                 k_transpose_bf16<<<dim3((no + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(dZb, no, T1, B, B, no);
                 const __nv_bfloat16 *inp = L == 0 ? Xb : Hs[L - 1];
                 k_transpose_bf16<<<dim3((ki + 31) / 32, (B + 31) / 32), tb, 0, h->stream>>>(
                     inp, L == 0 ? kSurInX : kSurHid, T2, B, B, ki);  // layer 0: the values' columns
-                k_gemm_tn<<<dim3((ki + 63) / 64, (no + 63) / 64), 128, 0, h->stream>>>(T1, B, T2, B, gw[L], ldw[L], no,
-                                                                                        ki, B);
+                // split K (the batch) so the small weight-gradient tile keeps every SM busy
+                const long gsz = (long)no * ldw[L];
+                k_gemm_tn<<<dim3((ki + 63) / 64, (no + 63) / 64, ksplit), 128, 0, h->stream>>>(
+                    T1, B, T2, B, Gp, ldw[L], no, ki, B, 0, gsz);
+                k_sum_splits<<<blocks(gsz), 256, 0, h->stream>>>(Gp, ksplit, gsz, ki, ldw[L], gw[L]);
                 if (L == 0) break;
                 // dH_prev = dZ W  (W^T [ki][no] as the B operand), then through GELU'
                 k_transpose_bf16<<<dim3((ki + 31) / 32, (no + 31) / 32), tb, 0, h->stream>>>(Ws[L], ldw[L], Wt, kSurLd,
@@ -1116,15 +1162,18 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
                 rc = LBMGPU_E_CUDA;
                 break;
             }
-            if (cudaMemcpyAsync(parts.data(), part, nparts * sizeof(double), cudaMemcpyDeviceToHost, h->stream) ||
-                cudaStreamSynchronize(h->stream)) {
-                rc = LBMGPU_E_CUDA;
-                break;
-            }
-            for (double p : parts) sum_se += p;
             sum_n += (long)nb * kSurOut;
             s.train_steps += 1;
         }
+        if (rc) break;
+        if (cudaMemcpyAsync(parts.data(), part, (size_t)nparts * bi * sizeof(double), cudaMemcpyDeviceToHost,
+                            h->stream) ||
+            cudaStreamSynchronize(h->stream)) {
+            rc = LBMGPU_E_CUDA;
+            break;
+        }
+        double sum_se = 0.0;
+        for (long q = 0; q < (long)nparts * bi; ++q) sum_se += parts[q];
         epoch_loss = sum_n ? sum_se / sum_n : 0.0;
     }
     cudaFree(idx);
@@ -1145,6 +1194,7 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
     cudaFree(T2);
     cudaFree(Wt);
     cudaFree(part);
+    cudaFree(Gp);
     if (rc) return rc;
     s.trained = true;
     s.last_loss = epoch_loss;

@@ -24,6 +24,9 @@ constexpr int kSurLd = kSurHid + 8;           // row stride (bf16) of the 128-wi
 
 // Standardisation of the features and targets, and the box of the training features the
 // gate accepts (expanded by 5 % of its width on both sides).
+constexpr float kSurOutGate = 16.f;    // predictions beyond 16 standard deviations of the
+                                       // training targets go to the integrator
+constexpr double kSurNegTol = 1e-12;   // ... and so do those that drive a mass fraction below -1e-12
 struct SurNorm {
     float x_mean[kSurInPad], x_std[kSurInPad], x_lo[kSurInPad], x_hi[kSurInPad];
     float y_mean[kSurOutPad], y_std[kSurOutPad];
@@ -34,13 +37,17 @@ struct SurArgs {
     int mode;                  // 0: integrator (teacher); 1: surrogate with integrator fallback
     const float *pred;         // [ncell][kSurOutPad] predicted dY_k, dT (SI), mode 1
     const uint8_t *gate;       // per cell 1: features outside the training box -> integrator
+    const SurNorm *nrm;        // the standardisation (output gate)
     double *audit;             // [0] sum of |dY_net - dY_int|_1, [1] sum of |dY_int|_1, [2] max
                                // of the former (bits), [3] audited, [4] predicted, [5] integrated
-    unsigned audit_period;     // 1 in audit_period cells (by a hash of cell and step) is audited
+    unsigned audit_period;     // every audit_period-th cell (n % audit_period == audit_phase,
+    unsigned audit_phase;      //   the phase moving from step to step) is audited
     unsigned step;
     const double *proj;        // [9][9] projector onto element-conserving changes (sur_projector)
-    // sample collection (teacher steps): cells with n % ds_stride == ds_phase write their
-    // (features, targets) to row ds_base + n / ds_stride while below ds_cap
+    // sample collection: integrated cells with n % ds_stride == ds_phase write their
+    // (features, targets) to row ds_base + n / ds_stride while below ds_cap -- teacher steps
+    // at the collection stride, surrogate steps at the audit stride and phase (the audited
+    // cells and those outside the training box on it: states the integrator takes anyway)
     float *ds_x, *ds_y;        // [ds_cap][kSurIn], [ds_cap][kSurOut]
     uint8_t *ds_valid;
     long ds_base, ds_cap;
