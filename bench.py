@@ -345,12 +345,16 @@ def mc_bytes(kernel, pop_bytes, reaction=False):
                    its P-tensor share; the energy sum)
       k_mc_solve : the 91 sum planes, 21 record planes (rho, T, p, rho_a, X_a) and the 36
                    D_ab read, 88 record planes written
-      k_mc_props : 58 record planes of the cell + 40 read once by its neighbours, 88
-                   parameter planes written (52 + the 36 D_ab) [+ HRR]"""
+      k_mc_props : 58 record planes of the cell, 86 parameter planes written (49 + the 36
+                   D_ab + R/W) [+ HRR]
+      k_mc_eflux : 53 record planes of the cell (rho, u, T, p, rho_a, u_a, the P tensor, the
+                   heat flux) + 3 rates read, 40 read once by its neighbours, 3 written"""
     if kernel == "k_mc_relax":
         return 2 * 270 * pop_bytes + (84 + (9 if reaction else 0)) * 8
     if kernel == "k_mc_props":
-        return (58 + 40 + 88 + (1 if reaction else 0)) * 8
+        return (58 + 86 + (1 if reaction else 0)) * 8
+    if kernel == "k_mc_eflux":
+        return (53 + 3 + 40 + 3) * 8
     if kernel == "k_mc_solve":
         return (91 + 21 + 36 + 88) * 8
     return 270 * pop_bytes + 91 * 8  # k_mc_gather
@@ -550,7 +554,8 @@ def run_ours_mc(args, dist):
             sur.update(surrogate_vs_plain(lat, mix, sp, args.compare, sur["refresh_s"], sur_cap))
     lat.close()
     avg = {"k_mc_relax": kms[0] / max(launches[0], 1), "k_mc_gather": kms[1] / max(launches[1], 1),
-           "k_mc_solve": kms[5] / max(launches[5], 1), "k_mc_props": kms[3] / max(launches[3], 1)}
+           "k_mc_solve": kms[5] / max(launches[5], 1), "k_mc_props": kms[3] / max(launches[3], 1),
+           "k_mc_eflux": kms[6] / max(launches[6], 1)}
     hbm_kernels = ("k_mc_relax", "k_mc_gather")
     dom = max(hbm_kernels, key=avg.get)  # the dominant population-moving kernel
     alg = mc_bytes(dom, pop_bytes, reaction) * ncell
@@ -599,7 +604,7 @@ def run_ours_mc(args, dist):
         "config": {"workload": mc_workload_name(args, "x".join(str(s_ - 2) for s_ in mix.shape)),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
                    "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
-        "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_gather", "k_mc_solve", "k_mc_props"))
+        "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_gather", "k_mc_solve", "k_mc_props", "k_mc_eflux"))
         / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell), "peak_source": f"{peak_kind} hbm_gbs",

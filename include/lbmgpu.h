@@ -195,8 +195,8 @@ int lbmgpu_status(lbmgpu_t *h, uint32_t *flags, int clear);
  * Kinds: 0 collide (multicomponent: the population update), 1 stream+boundary+moment
  * (multicomponent: the interior cells' pull and population sums), 2 other, 3
  * multicomponent collision parameters, 4 chemistry surrogate (features, network, the
- * integrator's cells), 5 multicomponent moment solve of the interior cells.  Returns the
- * number of kinds. */
+ * integrator's cells), 5 multicomponent moment solve of the interior cells, 6
+ * multicomponent energy-flux terms of the collision.  Returns the number of kinds. */
 int lbmgpu_profile(lbmgpu_t *h, int enable);
 int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
 

@@ -20,9 +20,10 @@ enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SP
 // (k_mc_relax), K_STREAM_MOMENT the pull and population sums of the interior cells
 // (k_mc_gather), K_PROPS the collision parameters (k_mc_props), K_SURROGATE the chemistry
 // surrogate's features, network and integrator list, K_SOLVE the interior cells' moment
-// solve (k_mc_solve)
+// solve (k_mc_solve), K_EFLUX the energy-flux terms of the collision (k_mc_eflux)
 enum KernelKind {
-    K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_SOLVE = 5, K_NKINDS = 6
+    K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_SOLVE = 5, K_EFLUX = 6,
+    K_NKINDS = 7
 };
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.

@@ -60,6 +60,14 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
     }
 }
 
+// The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_eflux(McArgsT<S, double> A) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
+    mc_eflux_cell<NS>(A, n);
+}
+
 // BGK update: blockIdx.y selects the population set (species 0..NS-1, NS = energy), the
 // x dimension the cells, so a warp reads one set's planes at 32 consecutive cells
 template <int NS, typename S>
@@ -434,6 +442,11 @@ int collide_t(lbmgpu *h) {
         ev_end(h, ei);
         CK(cudaGetLastError());
     }
+    EvPair ee{};
+    ev_begin(h, K_EFLUX, ee);
+    k_mc_eflux<NS9, S><<<gp, kBlock, 0, h->stream>>>(A);
+    ev_end(h, ee);
+    CK(cudaGetLastError());
     EvPair er{};
     ev_begin(h, K_COLLIDE, er);
     k_mc_relax<NS9, S><<<dim3(grid_for(h->g.ncell), NS9 + 1), kBlock, 0, h->stream>>>(A);

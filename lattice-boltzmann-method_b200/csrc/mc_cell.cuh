@@ -244,7 +244,9 @@ template <int NS> MC_HD constexpr int pr_dq(int d) { return 5 * NS + 4 + d; }
 // collision uses them for the Maxwell-Stefan shift, and the stream kernel that follows
 // for its Stefan-Maxwell matrix -- both evaluate them at the same (T, p, composition)
 template <int NS> MC_HD constexpr int pr_d(int a, int b) { return 5 * NS + 7 + a * (a - 1) / 2 + b; }
-template <int NS> MC_HD constexpr int pr_count() { return 5 * NS + 7 + NS * (NS - 1) / 2; }
+// the mixture gas constant R / W in lattice units (the energy-flux terms' Q_c)
+template <int NS> MC_HD constexpr int pr_gc() { return 5 * NS + 7 + NS * (NS - 1) / 2; }
+template <int NS> MC_HD constexpr int pr_count() { return pr_gc<NS>() + 1; }
 
 // ------------------------------------------------------------------------------------
 // Moments (the multicomponent LBM::calculate_moment, src/lbm-moment.cpp:193-377) of one
@@ -462,7 +464,7 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 //   mc_relax_species per (cell, species) and mc_relax_energy per cell: the BGK update of
 //                    the 27 populations of one set from the props planes.
 // Props planes (FP64, per cell): om_a (NS), F_a,d (3 NS), drho_a (NS), omega, omega_1,
-// theta, U, dq_d (3), D_ab (NS (NS-1) / 2).
+// theta, U, dq_d (3, written by mc_eflux_cell), D_ab (NS (NS-1) / 2), R / W.
 // ------------------------------------------------------------------------------------
 
 // The chemistry of LBMGPU_CHEM_ROSENBROCK for one cell: the constant-(rho, e) reactor
@@ -701,16 +703,8 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
     for (int a = 0; a < NS; ++a)
         for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * dt / rho_a[a]);
 
-    // -- energy collision parameters (lbm-collision.cpp:231-316)
-    long nbl[3], nbh[3];
-    int tl[3], th[3];
-    for (int d = 0; d < 3; ++d) {
-        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
-        nbl[d] = n - off;
-        nbh[d] = n + off;
-        tl[d] = A.type[nbl[d]];
-        th[d] = A.type[nbh[d]];
-    }
+    // -- energy collision parameters (lbm-collision.cpp:231-316): the relaxation rates here,
+    // the energy-flux terms (neighbour differences) in mc_eflux_cell
     double mu = 0.0;  // Wilke mixture viscosity sum_k X_k mu_k / sum_j X_j phi_kj
     for (int k = 0; k < NS; ++k) mu += X[k] * mu_k[k] / den_m[k];
     const double cp = u_cp(A.U, (float)gas::cp_mass(t, Y, T_si));
@@ -721,18 +715,55 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
     const double om1 = 2 * p * cp * dt / (p * cp * dt + 2 * lam);
     const double om = 2 * p * dt / (p * dt + 2 * mu);
     if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) atomic_status(A.status, LBMGPU_ST_TAU_UNSTABLE);
+    prp(pr_omm<NS>(), om);
+    prp(pr_om1<NS>(), om1);
+    prp(pr_theta<NS>(), theta);
+    prp(pr_uint<NS>(), Uint);
+    prp(pr_gc<NS>(), gasconstant);
+}
+
+// The energy-flux terms of the energy collision (lbm-collision.cpp:265-316): the enthalpy
+// diffusion q_diff and the upwind mass-fraction correction q_corr summed over the species,
+// the heat-flux difference and the pressure-tensor term -> dq (3 planes), from the rates
+// mc_props_cell wrote.  A kernel of its own: it is mostly neighbour loads, which hide
+// behind each other at the occupancy of a small kernel.
+template <int NS, class AT>
+MC_HDN void mc_eflux_cell(const AT &A, long n) {
+    const gas::Tables &t = *A.tab;
+    const typename AT::R *Rc = A.rec_cur;
+    double *Pr = A.props;
+    auto prg = [&](int plane) { return Pr[(long)plane * A.ncell + n]; };
+    auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
+    const double rho = rec(A, Rc, RM_RHO, n);
+    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
+    const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n);
+    const double T_si = si_temp(A.U, (float)Tl);
+    const double dt = A.dt;
+    const double om = prg(pr_omm<NS>()), om1 = prg(pr_om1<NS>()), gasconstant = prg(pr_gc<NS>());
+    long nbl[3], nbh[3];
+    int tl[3], th[3];
+    for (int d = 0; d < 3; ++d) {
+        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
+        nbl[d] = n - off;
+        nbh[d] = n + off;
+        tl[d] = A.type[nbl[d]];
+        th[d] = A.type[nbh[d]];
+    }
     double qd[3] = {0, 0, 0}, qc[3] = {0, 0, 0};
     const double rl[3] = {rec(A, Rc, RM_RHO, nbl[0]), rec(A, Rc, RM_RHO, nbl[1]), rec(A, Rc, RM_RHO, nbl[2])};
     const double rh[3] = {rec(A, Rc, RM_RHO, nbh[0]), rec(A, Rc, RM_RHO, nbh[1]), rec(A, Rc, RM_RHO, nbh[2])};
     for (int a = 0; a < NS; ++a) {
         const double ha = u_energy_mass(A.U, (float)(gas::h_RT(t, a, T_si) * gas::kR * T_si / t.m.W[a]));
         const int pr = rs(a, RS_RHO);
+        const double rho_a = rec(A, Rc, pr, n);
+        const double ua[3] = {rec(A, Rc, rs(a, RS_UX), n), rec(A, Rc, rs(a, RS_UX + 1), n),
+                              rec(A, Rc, rs(a, RS_UX + 2), n)};
         for (int d = 0; d < 3; ++d) {
-            qd[d] += om1 / (-om + om1) * ha * rho_a[a] * (ua[a][d] - um[d]);
+            qd[d] += om1 / (-om + om1) * ha * rho_a * (ua[d] - um[d]);
             const double Yl = rec(A, Rc, pr, nbl[d]) / rl[d];
-            const double Yc = rho_a[a] / rho;
+            const double Yc = rho_a / rho;
             const double Yh = rec(A, Rc, pr, nbh[d]) / rh[d];
-            const double dY = mc_fd_fuw(Yl, Yc, Yh, ua[a][d] - um[d], tl[d], th[d]);
+            const double dY = mc_fd_fuw(Yl, Yc, Yh, ua[d] - um[d], tl[d], th[d]);
             qc[d] += 0.5 * (2.0 - om1) / (-om + om1) * dt * p * ha * dY;
         }
     }
@@ -746,10 +777,6 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         for (int b = 0; b < 3; ++b) s += um[b] * (Pf[b][d] - ((b == d ? p : 0.0) + rho * um[b] * um[d]));
         prp(pr_dq<NS>(d), s + qd[d] + qc[d] + 0.5 * dt * um[d] * dQ);
     }
-    prp(pr_omm<NS>(), om);
-    prp(pr_om1<NS>(), om1);
-    prp(pr_theta<NS>(), theta);
-    prp(pr_uint<NS>(), Uint);
 }
 
 // The cell's populations of one set after streaming and boundary treatment: in place
@@ -881,6 +908,7 @@ MC_HDN void mc_collide_cell(const AT &A, long n) {
         mc_props_cell<NS, CHEM_ROSENBROCK>(A, n);
     else
         mc_props_cell<NS, CHEM_OFF>(A, n);
+    mc_eflux_cell<NS>(A, n);
     for (int a = 0; a < NS; ++a) mc_relax_species<NS>(A, n, a);
     mc_relax_energy<NS>(A, n);
 }

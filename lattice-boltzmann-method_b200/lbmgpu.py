@@ -264,11 +264,11 @@ class Lattice:
     def kernel_times(self):
         """Per kernel kind (0 collide / population update, 1 stream+boundary+moment
         (multicomponent: the interior pull and sums), 2 other, 3 multicomponent collision
-        parameters, 4 chemistry surrogate, 5 multicomponent moment solve): launches and
-        device ms."""
-        launches = (ctypes.c_long * 6)()
-        ms = (ctypes.c_double * 6)()
-        _check(lib().lbmgpu_kernel_times(self.h, 6, launches, ms), "lbmgpu_kernel_times")
+        parameters, 4 chemistry surrogate, 5 multicomponent moment solve, 6 multicomponent
+        energy-flux terms): launches and device ms."""
+        launches = (ctypes.c_long * 7)()
+        ms = (ctypes.c_double * 7)()
+        _check(lib().lbmgpu_kernel_times(self.h, 7, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------
