@@ -272,3 +272,54 @@ def test_surrogate_gains_over_the_integrator():
     assert t_s * 3 <= t_p, (t_s, t_p)
     assert abs(h_s - h_p) <= 0.02 * abs(h_p), (h_s, h_p)
     assert abs(p_s - p_p) <= 1e-3 * p_p, (p_s, p_p)
+
+
+def test_surrogate_online_rows_are_the_audited_integrator_states(tmp_path):
+    """Collection during surrogate steps: each step appends one row per fluid cell on the
+    audit stride (n % audit_period == the step's phase) -- the cells the integrator takes
+    anyway, audited or outside the training box -- labelled by the integrator: the host
+    build of the same ROS2 step reproduces every appended row's dY and dT to the rounding of
+    the FP32 feature storage; a refresh trains on the grown set."""
+    import ctypes
+
+    from mc_common import build_host_lib
+    lat, m, mix, sp = lattice()
+    P = 7
+    fluid = np.flatnonzero(mix["type"].reshape(-1) == 0)
+    with lat:
+        lat.upload(mix, sp)
+        lat.init()
+        lat.surrogate_collect(True, stride=1, capacity=mix.size * 10)
+        lat.step(10)
+        assert lat.synchronize() == 0
+        lat.surrogate_collect(False)
+        lat.surrogate_train(epochs=20, batch=1024, lr=2e-3, seed=9)
+        n0 = lat.surrogate_stats()["samples"]
+        lat.surrogate_enable(True, audit_period=P)
+        per = -(-mix.size // P)
+        lat.surrogate_collect(True, stride=1, capacity=n0 + 3 * per)
+        lat.step(3)
+        assert lat.synchronize() == 0
+        st = lat.surrogate_stats()
+        assert st["samples"] == n0 + 3 * per
+        x, y, v = lat.surrogate_samples()
+        lat.surrogate_train(epochs=1, batch=1024, lr=5e-4, seed=10)  # a refresh on the grown set
+        assert lat.synchronize() == 0
+    for s_ in range(3):  # every fluid cell of the step's stride wrote its row, nothing else did
+        got = set(np.flatnonzero(v[n0 + s_ * per:n0 + (s_ + 1) * per]).tolist())
+        assert any(got == set((fluid[fluid % P == ph] // P).tolist()) for ph in range(P)), s_
+    new = np.arange(n0, n0 + 3 * per)
+    ax, ay = x[new][v[new]].astype(np.float64), y[new][v[new]].astype(np.float64)
+    assert len(ax) > 0
+    L = build_host_lib(tmp_path)
+    L.ros2_host.restype = ctypes.c_long
+    L.ros2_host.argtypes = [ctypes.POINTER(mech.Mech), ctypes.c_long] + [ctypes.c_void_p] * 3 + [ctypes.c_double]
+    Wk = np.array([m.W[k] for k in range(9)])
+    Y = np.ascontiguousarray(ax[:, 2:11])
+    T = np.ascontiguousarray(ax[:, 0])
+    rho = np.ascontiguousarray(np.exp(ax[:, 1]) / (8314.46261815324 * T * (Y / Wk).sum(1)))
+    Y0, T0 = Y.copy(), T.copy()
+    Pp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    assert L.ros2_host(ctypes.byref(m), len(T), Pp(rho), Pp(Y), Pp(T), float(ax[0, 11])) == 0
+    err = np.abs((Y - Y0)[:, :8] - ay[:, :8]).sum() / np.abs((Y - Y0)[:, :8]).sum()
+    assert err < 1e-4, err
