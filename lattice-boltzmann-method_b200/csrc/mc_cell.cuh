@@ -831,6 +831,21 @@ MC_HDN void mc_relax_species(const AT &A, long n, int a) {
     const double Tl = rec(A, Rc, RM_T, n);
     const double om = prg(pr_om<NS>(a));
     const double dt = A.dt;
+    // loads that do not depend on the fetch mode first: the face terms and neighbour types,
+    // the shift parameters and the chemistry source
+    double qf[3][3];
+    int tyl[3], tyh[3];
+    for (int d = 0; d < 3; ++d) {
+        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
+        const int pq = rs(a, RS_QX + d);
+        qf[d][0] = rec(A, Rc, pq, n - off);
+        qf[d][1] = rec(A, Rc, pq, n);
+        qf[d][2] = rec(A, Rc, pq, n + off);
+        tyl[d] = A.type[n - off];
+        tyh[d] = A.type[n + off];
+    }
+    const double fsh[3] = {prg(pr_f<NS>(a, 0)), prg(pr_f<NS>(a, 1)), prg(pr_f<NS>(a, 2))};
+    const double drho = A.chem != CHEM_OFF ? prg(pr_drho<NS>(a)) : 0.0;
     const McFetch<AT> fetch(A, n);
     double fv[27];
 #pragma unroll
@@ -847,19 +862,15 @@ MC_HDN void mc_relax_species(const AT &A, long n, int a) {
     const double theta = t.Ra_lat[a] * Tl;
     double corr[3];
     for (int d = 0; d < 3; ++d) {  // FD of the face terms the stream kernel stored (lbm-collision.cpp:487-497)
-        const long off = d == 0 ? A.si : (d == 1 ? A.sj : 1);
-        const int pq = rs(a, RS_QX + d);
-        const double dQ = mc_fd_central(rec(A, Rc, pq, n - off), rec(A, Rc, pq, n), rec(A, Rc, pq, n + off),
-                                        A.type[n - off], A.type[n + off]);
+        const double dQ = mc_fd_central(qf[d][0], qf[d][1], qf[d][2], tyl[d], tyh[d]);
         corr[d] = dt * (2.0 - om) / (2.0 * rho_a * om) * dQ;
     }
     AxisF<double> Fe, Fd, Fr;
     axis_feq(Fe, ux, theta, corr);
-    const double udu[3] = {ux[0] + prg(pr_f<NS>(a, 0)), ux[1] + prg(pr_f<NS>(a, 1)), ux[2] + prg(pr_f<NS>(a, 2))};
+    const double udu[3] = {ux[0] + fsh[0], ux[1] + fsh[1], ux[2] + fsh[2]};
     axis_feq(Fd, udu, theta, corr);
     const double zero[3] = {0.0, 0.0, 0.0};
     axis_feq(Fr, um, theta, zero);
-    const double drho = A.chem != CHEM_OFF ? prg(pr_drho<NS>(a)) : 0.0;
     const bool skip_all = rho_a <= kSpeciesMin && A.chem == CHEM_OFF;
 #pragma unroll
     for (int l = 0; l < 27; ++l) {
