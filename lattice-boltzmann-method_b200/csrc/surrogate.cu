@@ -16,7 +16,7 @@
 //                 remainder, two k-slices against the same W1, so the inputs (T above all:
 //                 BF16 alone would round 1700 K by several kelvin) enter at ~16 bits;
 //   k_gemm_tn     C = A B^T for training (forward, input gradients, weight gradients),
-//                 mma.sync m16n8k16;
+//                 tcgen05 with the same shared-memory layout, 128 x 64 tiles;
 //   elementwise bias/GELU forward and backward, the MSE loss gradient, column sums for
 //   the bias gradients, Adam on FP32 master weights with BF16 copies.
 #include <cuda_bf16.h>
@@ -41,14 +41,6 @@ constexpr int kW1 = kSurHid * kSurInPad;       // elements of the padded weight 
 constexpr int kW2 = kSurHid * kSurLd;
 constexpr int kW4 = kSurOutPad * kSurLd;
 constexpr int kNParams = kW1 + 2 * kW2 + kW4 + 3 * kSurHid + kSurOutPad;
-
-__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
 
 __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -351,45 +343,111 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
 // -------------------------------------------------------------------------------------
 // Training kernels.
 // -------------------------------------------------------------------------------------
-// C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T (accum: C +=), A and B BF16 row-major with
-// leading dimensions lda, ldb (even), K a multiple of 16.  With gridDim.z > 1 block z
-// takes the z-th of gridDim.z equal slices of K (each a multiple of 16) and writes its
-// partial product to C + z zstride (split K, summed afterwards by k_sum_splits).  Block: 4 warps, each 16 rows x 64 columns.
+// C[M][N] (FP32, ldc) = A[M][K] B[N][K]^T (accum: C +=) on tcgen05, for training: A and B
+// BF16 row-major with leading dimensions lda, ldb (multiples of 8), K a multiple of 16.  A
+// CTA computes a 128 x 64 tile: K in chunks of 64 staged by its 128 threads into shared
+// memory in the canonical layout of the network kernel (rows and columns past M, N, K
+// zero-filled), four tcgen05.mma per chunk into a tensor-memory accumulator, a commit to
+// an mbarrier and a bounded wait before the next chunk reuses the buffers; the epilogue
+// reads the accumulator with tcgen05.ld.  With gridDim.z > 1 block z takes the z-th of
+// gridDim.z equal slices of K (each a multiple of 16) and writes its partial product to
+// C + z zstride (split K, summed afterwards by k_sum_splits).
+constexpr int kGmM = 128, kGmN = 64, kGmK = 64;
+constexpr int kGmA = 0, kGmB = kGmA + kGmM * kGmK * 2, kGmBar = kGmB + kGmN * kGmK * 2, kGmSlot = kGmBar + 8,
+              kGmSmem = kGmSlot + 8;
 __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict__ Am, int lda,
                                                  const __nv_bfloat16 *__restrict__ Bm, int ldb, float *__restrict__ C,
-                                                 int ldc, int M, int N, int K, int accum = 0, long zstride = 0) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-    const int r0 = blockIdx.y * 64 + warp * 16, n0 = blockIdx.x * 64;
+                                                 int ldc, int M, int N, int K, int accum, long zstride,
+                                                 unsigned *__restrict__ status) {
+    __shared__ __align__(128) unsigned char sm[kGmSmem];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(sm);
+    const int m0 = blockIdx.y * kGmM, n0 = blockIdx.x * kGmN;
     const int kc = K / (int)gridDim.z, kbeg = (int)blockIdx.z * kc;
     C += (long)blockIdx.z * zstride;
-    float acc[8][4] = {};
-    auto lda32 = [&](int r, int k) -> unsigned {
-        return r < M ? *reinterpret_cast<const unsigned *>(Am + (long)r * lda + k) : 0u;
-    };
-    auto ldb32 = [&](int n, int k) -> unsigned {
-        return n < N ? *reinterpret_cast<const unsigned *>(Bm + (long)n * ldb + k) : 0u;
-    };
-    for (int k0 = kbeg; k0 < kbeg + kc; k0 += 16) {
-        unsigned a[4];
-        a[0] = lda32(r0 + gid, k0 + 2 * tig);
-        a[1] = lda32(r0 + gid + 8, k0 + 2 * tig);
-        a[2] = lda32(r0 + gid, k0 + 8 + 2 * tig);
-        a[3] = lda32(r0 + gid + 8, k0 + 8 + 2 * tig);
+    const uint32_t bar = base + kGmBar;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kGmSlot),
+                     "r"((uint32_t)kGmN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + kGmSlot);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int k0 = kbeg; k0 < kbeg + kc && ok; k0 += kGmK) {
+        // stage the chunk: A rows m0.., B rows n0.., 16-byte pieces (8 elements of K)
+        for (int i = tid; i < kGmM * (kGmK / 8); i += 128) {
+            const int r = i / (kGmK / 8), c = i % (kGmK / 8), k = k0 + c * 8;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (m0 + r < M && k < kbeg + kc) v = *reinterpret_cast<const uint4 *>(Am + (long)(m0 + r) * lda + k);
+            *reinterpret_cast<uint4 *>(sm + kGmA + tc_off(r, c * 8, kGmK)) = v;
+        }
+        for (int i = tid; i < kGmN * (kGmK / 8); i += 128) {
+            const int r = i / (kGmK / 8), c = i % (kGmK / 8), k = k0 + c * 8;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (n0 + r < N && k < kbeg + kc) v = *reinterpret_cast<const uint4 *>(Bm + (long)(n0 + r) * ldb + k);
+            *reinterpret_cast<uint4 *>(sm + kGmB + tc_off(r, c * 8, kGmK)) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        if (tid == 0) {
+            const uint32_t idesc = tc_idesc(kGmN);
+            for (int s = 0; s < kGmK / 16; ++s) {
+                const uint64_t ad = tc_desc(base + kGmA + 256u * s, kGmK * 16u);
+                const uint64_t bd = tc_desc(base + kGmB + 256u * s, kGmK * 16u);
+                const uint32_t acc = (k0 > kbeg || s > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                         : "memory");
+        }
+        ok = __syncthreads_and(tc_wait(bar, phase)) != 0;
+        tc_fence_after();
+        if (!ok) break;
+        phase ^= 1u;
+    }
+    if (ok && kc > 0) {  // epilogue: row m0 + tid of the tile, 64 columns in four loads
+        const long r = m0 + tid;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int cb = 0; cb < kGmN / 16; ++cb) {
+            uint32_t v[16];
+            tc_ld16(trow + (uint32_t)(cb * 16), v);
+            tc_wait_ld();
+            if (r < M)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int nn = n0 + 8 * j + gid;
-            mma_bf16(acc[j], a, ldb32(nn, k0 + 2 * tig), ldb32(nn, k0 + 8 + 2 * tig));
+                for (int j = 0; j < 16; ++j) {
+                    const int c = n0 + cb * 16 + j;
+                    if (c < N) {
+                        float *dst = C + r * ldc + c;
+                        *dst = __uint_as_float(v[j]) + (accum ? *dst : 0.f);
+                    }
+                }
         }
     }
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int r = r0 + gid + 8 * h, c = n0 + 8 * j + 2 * tig;
-            if (r < M && c < N) C[(long)r * ldc + c] = acc[j][2 * h] + (accum ? C[(long)r * ldc + c] : 0.f);
-            if (r < M && c + 1 < N)
-                C[(long)r * ldc + c + 1] = acc[j][2 * h + 1] + (accum ? C[(long)r * ldc + c + 1] : 0.f);
-        }
+    if (!ok) {  // the tensor core may still be working on the timed-out chunk: one more bounded wait
+        if (tid == 0) atomicOr(status, (unsigned)LBMGPU_ST_SURROGATE);
+        tc_wait(bar, phase);
+        tc_fence_after();
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kGmN) : "memory");
 }
 
 // out[r][c] = sum_z part[z][r][c] over the split-K slices, in slice order, for the
@@ -576,6 +634,13 @@ __global__ void k_sur_augment(const gas::Tables *__restrict__ tab, float *__rest
 }
 
 inline unsigned blocks(long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+// k_gemm_tn over the whole C (splits > 1: split K, partials zstride apart).
+void gemm_tn(lbmgpu *h, const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *Bm, int ldb, float *C, int ldc, int M,
+             int N, int K, int accum = 0, int splits = 1, long zstride = 0) {
+    k_gemm_tn<<<dim3((N + kGmN - 1) / kGmN, (M + kGmM - 1) / kGmM, splits), 128, 0, h->stream>>>(
+        A, lda, Bm, ldb, C, ldc, M, N, K, accum, zstride, h->status);
+}
 
 }  // namespace
 
@@ -1108,16 +1173,13 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
             const __nv_bfloat16 *Ws[4] = {net.w1, net.w2, net.w3, net.w4};
             const float *bs[4] = {net.b1, net.b2, net.b3, net.b4};
             for (int L = 0; L < 3; ++L) {
-                k_gemm_tn<<<dim3((nout[L] + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(
-                    in, L == 0 ? kSurInX : kSurHid, Ws[L], ldw[L], C, kSurHid, B, nout[L], kin[L]);
+                gemm_tn(h, in, L == 0 ? kSurInX : kSurHid, Ws[L], ldw[L], C, kSurHid, B, nout[L], kin[L]);
                 if (L == 0)  // the remainders' share of the first layer
-                    k_gemm_tn<<<dim3((nout[0] + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(
-                        Xb + kSurInPad, kSurInX, Ws[0], ldw[0], C, kSurHid, B, nout[0], kin[0], 1);
+                    gemm_tn(h, Xb + kSurInPad, kSurInX, Ws[0], ldw[0], C, kSurHid, B, nout[0], kin[0], 1);
                 k_bias_gelu<<<blocks(BH), 256, 0, h->stream>>>(C, bs[L], Zs[L], Hs[L], B, kSurHid);
                 in = Hs[L];
             }
-            k_gemm_tn<<<dim3(1, (B + 63) / 64), 128, 0, h->stream>>>(H3, kSurHid, net.w4, kSurLd, C, kSurOutPad, B,
-                                                                       kSurOutPad, kSurHid);
+            gemm_tn(h, H3, kSurHid, net.w4, kSurLd, C, kSurOutPad, B, kSurOutPad, kSurHid);
             k_out_loss<<<nparts, 256, 0, h->stream>>>(C, net.b4, Yb, vb, (float)nb, dA, part + (size_t)bi * nparts, B);
             // backward: dA holds dL/d(pre-activation) of the current layer (FP32), rows x nout
             float *gw[4] = {s.g + off_w(0), s.g + off_w(1), s.g + off_w(2), s.g + off_w(3)};
@@ -1134,15 +1196,13 @@ int lbmgpu_surrogate_train(lbmgpu_t *h, int epochs, int batch, float lr, unsigne
                     inp, L == 0 ? kSurInX : kSurHid, T2, B, B, ki);  // layer 0: the values' columns
                 // split K (the batch) so the small weight-gradient tile keeps every SM busy
                 const long gsz = (long)no * ldw[L];
-                k_gemm_tn<<<dim3((ki + 63) / 64, (no + 63) / 64, ksplit), 128, 0, h->stream>>>(
-                    T1, B, T2, B, Gp, ldw[L], no, ki, B, 0, gsz);
+                gemm_tn(h, T1, B, T2, B, Gp, ldw[L], no, ki, B, 0, ksplit, gsz);
                 k_sum_splits<<<blocks(gsz), 256, 0, h->stream>>>(Gp, ksplit, gsz, ki, ldw[L], gw[L]);
                 if (L == 0) break;
                 // dH_prev = dZ W  (W^T [ki][no] as the B operand), then through GELU'
                 k_transpose_bf16<<<dim3((ki + 31) / 32, (no + 31) / 32), tb, 0, h->stream>>>(Ws[L], ldw[L], Wt, kSurLd,
                                                                                               no, ki);
-                k_gemm_tn<<<dim3((ki + 63) / 64, (B + 63) / 64), 128, 0, h->stream>>>(dZb, no, Wt, kSurLd, C, kSurHid, B,
-                                                                                       ki, no);
+                gemm_tn(h, dZb, no, Wt, kSurLd, C, kSurHid, B, ki, no);
                 k_gelu_bwd<<<blocks(BH), 256, 0, h->stream>>>(C, Zs[L - 1], dA, T1, BH);
             }
             // Adam step over every parameter (padding entries have zero gradient)
