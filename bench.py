@@ -86,39 +86,57 @@ def parse():
 # distributed plumbing
 # ---------------------------------------------------------------------------------------
 class Dist:
-    def __init__(self):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from the launcher): NCCL for the
+    benchmark's barrier and max over ranks; gloo on the host for the CPU tests."""
+
+    def __init__(self, backend="nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
             self.pg = dist
+
+    def _device(self):
+        return "cuda" if self.backend == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
             import torch
-            t = torch.zeros(1, device="cuda")
+            t = torch.zeros(1, device=self._device())
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.backend == "nccl":
+                torch.cuda.synchronize()
 
     def max(self, x):
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+        t = torch.tensor([float(x)], device=self._device(), dtype=torch.float64)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def whole_job_mlups(world, cells, steps, seconds):
+    """Replicas (the path is not domain-decomposed): every rank updates its own lattice of
+    `cells` for `steps`; the job's rate is all ranks' cell updates over the slowest rank's
+    time (`seconds`, already the max over ranks)."""
+    return world * cells * steps / seconds / 1e6
 
 
 # ---------------------------------------------------------------------------------------
@@ -588,14 +606,14 @@ def run_ours_mc(args, dist):
     wall = dist.max(time.perf_counter() - t0)
     lat.close()
     nbytes = mix.nbytes + sum(a.nbytes for a in sp)
-    e2e = {"value": dist.world * ncell * args.steps / wall / 1e6, "unit": "MLUPS",
+    e2e = {"value": whole_job_mlups(dist.world, ncell, args.steps, wall), "unit": "MLUPS",
            "h2d_bytes_per_step": nbytes / args.steps,
            "d2h_bytes_per_step": nbytes / args.steps + 8 * len(tot),
            "note": "AoS upload + Init, per step the five phase calls and the conserved totals read back, "
                    "one AoS download"}
     if dist.rank != 0:
         return
-    value = dist.world * ncell * args.steps / (ms * 1e-3) / 1e6
+    value = whole_job_mlups(dist.world, ncell, args.steps, ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -700,14 +718,14 @@ def run_ours(args, dist):
     lat.synchronize()
     wall = dist.max(time.perf_counter() - t0)
     lat.close()
-    e2e = {"value": dist.world * ncell * args.steps / wall / 1e6, "unit": "MLUPS",
+    e2e = {"value": whole_job_mlups(dist.world, ncell, args.steps, wall), "unit": "MLUPS",
            "h2d_bytes_per_step": cells.nbytes / args.steps,
            "d2h_bytes_per_step": (cells.nbytes + 4) * nread / args.steps,
            "note": f"upload of the AoS state once, phase calls per step, AoS download + status every {OUTPUT_EVERY} steps"}
 
     if dist.rank != 0:
         return
-    value = dist.world * ncell * args.steps / (ms * 1e-3) / 1e6
+    value = whole_job_mlups(dist.world, ncell, args.steps, ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
