@@ -445,9 +445,9 @@ def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
 def surrogate_vs_plain(lat, mix, sp, K, refresh_s, cap):
     """From the lattice's current state, K steps with the surrogate (1 % audit; the audited
     states collected and the network refreshed from them every 50 steps, timed into
-    refresh_s) and, after restoring the state, K steps of plain ROS2: the north star's
-    comparison -- peak temperature and heat release integrated over the cells and the K
-    steps -- from the device diagnostics (lbmgpu_diagnostics) after every step."""
+    refresh_s) and, after restoring the state, K steps of plain ROS2: the comparison the
+    surrogate is held to -- peak temperature and heat release integrated over the cells and
+    the K steps -- from the device diagnostics (lbmgpu_diagnostics) after every step."""
     import lbmgpu
     import workloads
     c0 = mix.copy()

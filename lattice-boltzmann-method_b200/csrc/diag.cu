@@ -8,7 +8,7 @@
 // when the lower one did not wrap, as there), and the total energy  sum rho E  (:265).
 // Then the heat-release sum  sum HRR  (the per-cell field the chemistry writes,
 // src/lbm-collision.cpp:395-398) and the peak and minimum temperature -- what a reacting run
-// is judged by.  All in lattice units.  Deterministic: fixed grid-strided cell sets per
+// is assessed by.  All in lattice units.  Deterministic: fixed grid-strided cell sets per
 // block, warp shuffles, then the blocks in order; the partials use the handle's reduction
 // scratch (allocated on the first call of this or lbmgpu_sums).
 #include <algorithm>
