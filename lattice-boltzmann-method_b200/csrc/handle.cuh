@@ -47,6 +47,8 @@ struct SpOff {
 struct lbmgpu {
     lbmgpu_desc d{};
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;           // multicomponent: the boundary cells beside the interior
+    cudaEvent_t fork = nullptr, join = nullptr;
     lbm::ScGeom g{};
     lbm::ScPhys P{};
     lbmh::MixOff mo{};
@@ -114,7 +116,7 @@ int dalloc(lbmgpu *h, T **p, size_t count) {
     return 0;
 }
 
-inline void ev_begin(lbmgpu *h, int kind, EvPair &ep) {
+inline void ev_begin(lbmgpu *h, int kind, EvPair &ep, cudaStream_t st = nullptr) {
     if (!h->prof) return;
     if (h->pool.empty()) {
         EvPair e{};
@@ -125,12 +127,12 @@ inline void ev_begin(lbmgpu *h, int kind, EvPair &ep) {
     ep = h->pool.back();
     h->pool.pop_back();
     ep.kind = kind;
-    cudaEventRecord(ep.a, h->stream);
+    cudaEventRecord(ep.a, st ? st : h->stream);
 }
 
-inline void ev_end(lbmgpu *h, EvPair &ep) {
+inline void ev_end(lbmgpu *h, EvPair &ep, cudaStream_t st = nullptr) {
     if (!h->prof) return;
-    cudaEventRecord(ep.b, h->stream);
+    cudaEventRecord(ep.b, st ? st : h->stream);
     h->pending.push_back(ep);
 }
 

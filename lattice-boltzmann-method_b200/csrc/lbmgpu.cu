@@ -488,6 +488,9 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     const long nc = h->g.ncell;
     int rc = 0;
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
     if (e != cudaSuccess) rc = cuda_fail(e);
     if (!rc) rc = dalloc(h, &h->type, nc);
     if (!rc) rc = dalloc(h, &h->cflag, nc);
@@ -545,6 +548,9 @@ int lbmgpu_destroy(lbmgpu_t *h) {
     cudaFree(h->stage);
     if (h->bounce) cudaFreeHost(h->bounce);
     lbmh::mc_release(h);
+    if (h->fork) cudaEventDestroy(h->fork);
+    if (h->join) cudaEventDestroy(h->join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     (void)cudaGetLastError();
     delete h;

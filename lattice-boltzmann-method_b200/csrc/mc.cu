@@ -462,6 +462,23 @@ int stream_t(lbmgpu *h) {
     A.pop_src = popb<S>(h, x);
     A.rec_cur = h->mom[c];
     A.rec_nxt = h->mom[x];
+    // The boundary cells run on the side stream beside the interior's gather and solve:
+    // the two sets of cells are disjoint, and both read only the post-collision populations
+    // and the previous records, so the latency-bound boundary kernel overlaps them; the
+    // handle's stream waits for it before anything that follows.
+    if (h->nb > 0) {
+        McArgsT<S, double> B = A;
+        B.bst_cur = bstb<S>(h, c);
+        B.bst_nxt = bstb<S>(h, x);
+        CK(cudaEventRecord(h->fork, h->stream));
+        CK(cudaStreamWaitEvent(h->side, h->fork, 0));
+        EvPair eb{};
+        ev_begin(h, K_OTHER, eb, h->side);
+        k_mc_special<NS9, S><<<(unsigned)((h->nb + 31) / 32), 32, 0, h->side>>>(B, h->blist);
+        ev_end(h, eb, h->side);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(h->join, h->side));
+    }
     EvPair ep{};
     ev_begin(h, K_STREAM_MOMENT, ep);
     k_mc_gather<NS9, S><<<dim3(grid_for(h->g.ncell), NS9 + 1), kBlock, 0, h->stream>>>(A, h->gsum);
@@ -472,15 +489,7 @@ int stream_t(lbmgpu *h) {
     k_mc_solve<NS9, S><<<grid_for(h->g.ncell), kBlock, 0, h->stream>>>(A, h->gsum);
     ev_end(h, es);
     CK(cudaGetLastError());
-    if (h->nb > 0) {
-        A.bst_cur = bstb<S>(h, c);
-        A.bst_nxt = bstb<S>(h, x);
-        EvPair eb{};
-        ev_begin(h, K_OTHER, eb);
-        k_mc_special<NS9, S><<<(unsigned)((h->nb + 31) / 32), 32, 0, h->stream>>>(A, h->blist);
-        ev_end(h, eb);
-        CK(cudaGetLastError());
-    }
+    if (h->nb > 0) CK(cudaStreamWaitEvent(h->stream, h->join, 0));
     return 0;
 }
 
