@@ -58,13 +58,14 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
-    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan"], default="inflow",
+    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan", "flame"], default="inflow",
                     help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
                          "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
                          "1800 K slab; inflow: config 2's shape, the mixing layer between a characteristic "
-                         "inflow and outflow (N^3); chan: config 3's shape, a reacting H2-air channel with "
-                         "NSCBC outflow ends and TMS walls (2N x N/2 x N/2)")
+                         "inflow and outflow (N^3); chan: config 3's case, a reacting H2-air channel with "
+                         "NSCBC outflow ends and TMS walls, at 2N x N/2 x N/2; flame: config 3 itself, the "
+                         "same channel at 4N x N/16 x N/16 (512 x 8 x 8 at the default N)")
     ap.add_argument("--chem", choices=["ref", "rosenbrock", "surrogate"], default="ref",
                     help="reacting workloads: the reference's explicit scheme, the ROS2 stiff integrator, or "
                          "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
@@ -379,7 +380,8 @@ def mc_bytes(kernel, pop_bytes, reaction=False):
 
 
 MC_SHAPES = {"mix": "periodic", "react": "periodic", "inflow": "TYPE_I_C inflow / TYPE_O_C outflow in x, periodic y z",
-             "chan": "TYPE_O_C outflow at both x ends, TMS solid y walls, periodic z"}
+             "chan": "TYPE_O_C outflow at both x ends, TMS solid y walls, periodic z",
+             "flame": "TYPE_O_C outflow at both x ends, TMS solid y walls, periodic z"}
 
 
 def mc_workload(args, cross=None):
@@ -395,6 +397,9 @@ def mc_workload(args, cross=None):
     elif args.workload == "chan":
         c = cross or N // 2
         mix, sp = workloads.flame_channel_mc(m, NX=2 * N, NY=c, NZ=c)
+    elif args.workload == "flame":
+        c = min(cross or N // 16, N // 16)
+        mix, sp = workloads.flame_channel_mc(m, NX=4 * N, NY=c, NZ=c)
     else:
         c = cross or N
         kw = {"T_hi": 1800.0} if args.workload == "react" else {}
@@ -403,7 +408,7 @@ def mc_workload(args, cross=None):
 
 
 def mc_reaction(args):
-    return args.workload in ("react", "chan")
+    return args.workload in ("react", "chan", "flame")
 
 
 def mc_cpu_sample(args, budget_s, threads):
@@ -419,6 +424,8 @@ def mc_cpu_sample(args, budget_s, threads):
     cross = int(max(4, min(args.N, (rate * budget_s / nx) ** 0.5)))
     if args.workload == "chan":
         cross = min(cross, args.N // 2)
+    if args.workload == "flame":
+        cross = min(cross, args.N // 16)
     return cross, m
 
 
@@ -567,6 +574,17 @@ def run_ours_mc(args, dist):
         ms_plain = lat.time_steps(kp)
         sur["plain_chem_mlups"] = ncell * kp / (ms_plain * 1e-3) / 1e6
         sur["surrogate_ms_per_step"] = kms[4] / max(kk, 1)
+        # the chemistry part of a step: the collision parameters (which hold the chemistry)
+        # plus, with the surrogate, its features, network and integrator list; plain ROS2 in
+        # the same kernel, profiled over a few more plain steps
+        lat.profile(True)
+        lat.time_steps(kp)
+        _, kms_plain = lat.kernel_times()
+        lat.profile(False)
+        chem_sur = (kms[3] + kms[4]) / max(kk, 1)
+        chem_plain = kms_plain[3] / max(kp, 1)
+        sur["chemistry_ms_per_step"] = {"surrogate": chem_sur, "plain": chem_plain,
+                                        "speedup": chem_plain / max(chem_sur, 1e-12)}
         sur["network_flops_per_cell"] = 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)
         if args.compare > 0:
             sur.update(surrogate_vs_plain(lat, mix, sp, args.compare, sur["refresh_s"], sur_cap))
