@@ -43,21 +43,30 @@ __global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
 
 // the cells the collision-parameter kernel left to the chemistry integrator (surrogate
 // on: out-of-box, non-finite and audited cells), integrated in dense warps
-// The cells the surrogate leaves to the integrator (sur.ilist), kChemGroup lanes per cell:
-// the lanes of a group evaluate the finite-difference Jacobian's columns side by side
-// (gas::ros2_advance_group), so a few thousand listed cells do not wait on serial
-// integrations of one lane each.
-constexpr int kChemGroup = 4;
-template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
-    const unsigned cnt = *A.sur.icount;
-    const unsigned groups = gridDim.x * blockDim.x / kChemGroup;
-    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / kChemGroup; i < cnt; i += groups) {
+// The cells the surrogate leaves to the integrator (sur.ilist), G lanes per cell: the
+// lanes of a group evaluate the finite-difference Jacobian's columns side by side
+// (gas::ros2_advance_group), so the listed cells do not wait on serial integrations of one
+// lane each.  A short list (up to kChemShortList cells: latency-bound) takes 8 lanes per
+// cell, a long one 4 (the group's redundant factorisation then costs more than the
+// latency it saves); the choice is made on the device from the list's length.
+constexpr unsigned kChemShortList = 5000;
+template <int NS, int G, typename S>
+__device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
+    const unsigned groups = gridDim.x * blockDim.x / G;
+    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < cnt; i += groups) {
         const long n = A.sur.ilist[i];
         double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
         mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS, McArgsT<S, double>, true, kChemGroup>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, G>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
     }
+}
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
+    const unsigned cnt = *A.sur.icount;
+    if (cnt <= kChemShortList)
+        chem_list_groups<NS, 8>(A, cnt);
+    else
+        chem_list_groups<NS, 4>(A, cnt);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
