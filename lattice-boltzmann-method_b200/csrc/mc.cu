@@ -2,7 +2,8 @@
 // mc_cell.cuh and the handle operations for n_species > 0.
 //
 // Reference path replaced (farrasarira/Lattice-Boltzmann-Method, MULTICOMP on):
-//   LBM::Collide_Species + LBM::Collide   src/lbm-collision.cpp:191-526 -> k_mc_collide
+//   LBM::Collide_Species + LBM::Collide   src/lbm-collision.cpp:191-526 -> k_mc_props (+ the surrogate's
+//                                          kernels, k_mc_chem_list), k_mc_eflux, k_mc_relax
 //   LBM::Streaming + LBM::calculate_moment src/lbm-streaming.cpp, src/lbm-moment.cpp:193-377
 //                                          -> k_mc_gather (pull + population sums per
 //                                             (cell, set)) and k_mc_solve (per cell)

@@ -77,7 +77,7 @@ struct McArgsT {
     // boundary-treated populations, 27 (NS+1) planes of nb entries
     const int *bid;
     const P *bst_cur;      // of the current step (collide, and the stale directions)
-    P *bst_nxt;            // written by the special-cell stream kernel
+    P *bst_nxt;            // written by the boundary-cell kernel (k_mc_special)
     long nb;
     double *props;         // collision parameters per cell (mc_props_cell -> mc_relax_*)
     SurArgs sur;           // chemistry surrogate (LBMGPU_CHEM_ROSENBROCK only)
@@ -241,7 +241,7 @@ template <int NS> MC_HD constexpr int pr_theta() { return 5 * NS + 2; }
 template <int NS> MC_HD constexpr int pr_uint() { return 5 * NS + 3; }
 template <int NS> MC_HD constexpr int pr_dq(int d) { return 5 * NS + 4 + d; }
 // the lattice binary diffusion coefficients D_ab (b < a) at the record's state: the
-// collision uses them for the Maxwell-Stefan shift, and the stream kernel that follows
+// collision uses them for the Maxwell-Stefan shift, and the moment solve that follows
 // for its Stefan-Maxwell matrix -- both evaluate them at the same (T, p, composition)
 template <int NS> MC_HD constexpr int pr_d(int a, int b) { return 5 * NS + 7 + a * (a - 1) / 2 + b; }
 // the mixture gas constant R / W in lattice units (the energy-flux terms' Q_c)
@@ -861,7 +861,7 @@ MC_HDN void mc_relax_species(const AT &A, long n, int a) {
     for (int d = 0; d < 3; ++d) ux[d] = ux[d] / rho_a;
     const double theta = t.Ra_lat[a] * Tl;
     double corr[3];
-    for (int d = 0; d < 3; ++d) {  // FD of the face terms the stream kernel stored (lbm-collision.cpp:487-497)
+    for (int d = 0; d < 3; ++d) {  // FD of the face terms the moment kernels stored (lbm-collision.cpp:487-497)
         const double dQ = mc_fd_central(qf[d][0], qf[d][1], qf[d][2], tyl[d], tyh[d]);
         corr[d] = dt * (2.0 - om) / (2.0 * rho_a * om) * dQ;
     }
