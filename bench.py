@@ -433,9 +433,11 @@ def mc_cpu_run(m, mix, sp, steps, warmup, threads, reaction):
     """The reference's own multicomponent solver on the Cantera-API shim (oracle/_ref)."""
     import workloads
     from oracle import refmc
-    refmc.set_threads(threads, reaction)
+    fast = refmc.available(reaction, fast=True)  # the reference's own -O3 -ffast-math build
+    refmc.set_threads(threads, reaction, fast)
     N3 = [s_ - 2 for s_ in mix.shape]
-    ref = refmc.RefMC(*N3, m, workloads.FLAME_UNITS, workloads.MIXTURE_MC, workloads.SPECIES, reaction=reaction)
+    ref = refmc.RefMC(*N3, m, workloads.FLAME_UNITS, workloads.MIXTURE_MC, workloads.SPECIES, reaction=reaction,
+                      fast=fast)
     ref.cells[...] = mix
     for a in range(len(sp)):
         ref.species[a][...] = sp[a]

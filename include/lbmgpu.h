@@ -10,8 +10,7 @@
  *
  * How the reference's driver reaches it: the LBM member functions that make up one time
  * step (src/headers/lbm.hpp:152-197, called in src/lbm-main.cpp:149-196) keep their
- * signatures and forward here.  The C++ mirror in
- * lattice-boltzmann-method_b200/host/lbm_gpu.hpp does exactly that.
+ * signatures and forward here, one call each: LBM::Collide() calls lbmgpu_collide(h), and so on.
  */
 #ifndef LBMGPU_H
 #define LBMGPU_H
@@ -221,8 +220,10 @@ int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
  * cudaMalloc, a host whose pool owns all device memory).  Same values, bit for bit, as
  * lbmgpu_sums.  n_out must lie in [lbmgpu_sums_count(h), LBMGPU_SUMS_MAX], else
  * LBMGPU_E_ARG.  The scratch is shared by every handle on the device: calls that overlap
- * on one device race, so serialise them.  The first call on a device resolves the
- * scratch's address; make it before any stream capture begins. */
+ * on one device race, so serialise them.  lbmgpu_create loads the scratch and the
+ * reduction kernels on its device (CUDA loads modules lazily by default), so no call of
+ * this entry point allocates; the scratch stays until the process exits, or until a
+ * cudaDeviceReset, which also ends every handle on that device. */
 int lbmgpu_sums_noalloc(lbmgpu_t *h, double *out, int n_out);
 
 /* Run diagnostics of the current state, reduced on the device (FP64, lattice units, over

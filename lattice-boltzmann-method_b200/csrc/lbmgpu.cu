@@ -19,6 +19,7 @@
 #include "../../include/lbmgpu.h"
 #include "handle.cuh"
 #include "sc_kernels.cuh"
+#include "sums.cuh"
 
 using namespace lbm;
 using lbmh::MixOff;
@@ -502,6 +503,10 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
         rc = lbmh::mc_setup(h);
     }
     if (!rc) rc = dalloc(h, &h->status, 1);
+    // load the reduction kernels' module and the fixed scratch of lbmgpu_sums_noalloc now,
+    // while allocating is allowed (lazy module loading would do it at their first use)
+    if (!rc) rc = lbmh::sums_preload();
+    if (!rc) rc = lbmh::noalloc_prepare();
     if (!rc) {
         e = cudaMemsetAsync(h->status, 0, sizeof(unsigned), h->stream);
         if (e != cudaSuccess) rc = cuda_fail(e);

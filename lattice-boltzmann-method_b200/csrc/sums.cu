@@ -92,6 +92,13 @@ __global__ void k_sum_final(const double *__restrict__ partials, int nblocks, in
 
 int sums_count(const lbmgpu *h) { return h->ns > 0 ? 5 + h->ns + kSumElements : 5; }
 
+int sums_preload() {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, k_sum_partials));
+    CK(cudaFuncGetAttributes(&fa, k_sum_final));
+    return 0;
+}
+
 int sums_grid(const lbmgpu *h) {
     return (int)std::max<long>(1, std::min<long>((h->g.ncell + kSumBlock - 1) / kSumBlock, kSumMaxBlocks));
 }

@@ -12,16 +12,21 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PATHS = {False: os.path.join(HERE, "_ref", "libref_mc.so"), True: os.path.join(HERE, "_ref", "libref_mcr.so")}
+# the timed baseline: the same sources with the reference's optimisation flags (-O3
+# -ffast-math -flto); the parity oracle above is built without -ffast-math
+FAST_PATHS = {False: os.path.join(HERE, "_ref", "libref_mc_fast.so"),
+              True: os.path.join(HERE, "_ref", "libref_mcr_fast.so")}
 _libs = {}
 
 
-def available(reaction=False):
-    return os.path.exists(PATHS[reaction])
+def available(reaction=False, fast=False):
+    return os.path.exists((FAST_PATHS if fast else PATHS)[reaction])
 
 
-def lib(reaction=False):
-    if reaction not in _libs:
-        L = ctypes.CDLL(PATHS[reaction])
+def lib(reaction=False, fast=False):
+    key = (reaction, fast)
+    if key not in _libs:
+        L = ctypes.CDLL((FAST_PATHS if fast else PATHS)[reaction])
         vp = ctypes.c_void_p
         L.ref_mc_set_mech.argtypes = [vp]
         L.ref_mc_set_units.argtypes = [ctypes.c_float, ctypes.c_float]
@@ -37,8 +42,8 @@ def lib(reaction=False):
         L.ref_mc_loop.argtypes = [vp, ctypes.c_int]
         L.ref_mc_phase.argtypes = [vp, ctypes.c_int]
         L.ref_mc_set_threads.argtypes = [ctypes.c_int]
-        _libs[reaction] = L
-    return _libs[reaction]
+        _libs[key] = L
+    return _libs[key]
 
 
 def layout(reaction=False):
@@ -52,8 +57,8 @@ def layout(reaction=False):
 class RefMC:
     """One reference multicomponent ``LBM`` object; `mech` is a mech.Mech table."""
 
-    def __init__(self, NX, NY, NZ, mech, units, mix_dtype, sp_dtype, reaction=False):
-        self.L = lib(reaction)
+    def __init__(self, NX, NY, NZ, mech, units, mix_dtype, sp_dtype, reaction=False, fast=False):
+        self.L = lib(reaction, fast)
         self._mech = mech
         self.L.ref_mc_set_mech(ctypes.byref(mech))
         self.L.ref_mc_set_units(units[0], units[1])
@@ -92,5 +97,5 @@ class RefMC:
             pass
 
 
-def set_threads(n, reaction=False):
-    lib(reaction).ref_mc_set_threads(n)
+def set_threads(n, reaction=False, fast=False):
+    lib(reaction, fast).ref_mc_set_threads(n)

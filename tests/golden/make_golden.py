@@ -1,8 +1,11 @@
 """Generates the golden fixtures in this directory from the reference's OWN code.
 
-Run from the repository root (needs the reference tree, built by ``make -C oracle ref``):
+Run from the repository root (needs the reference tree, built by ``make -C oracle ref
+REF=<reference tree>``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference <reference tree>
+
+(or with the tree in the LBM_REFERENCE environment variable).
 
 It drives ``oracle/_ref/libref_sc.so`` -- the reference's single-component sources
 compiled unchanged -- on seeded inputs and records:
@@ -41,7 +44,16 @@ from oracle import cases, refmc, refsc  # noqa: E402
 sys.path.insert(0, os.path.join(ROOT, "lattice-boltzmann-method_b200"))
 import mech as mechmod  # noqa: E402
 
-MECH_PATH = "/root/reference/src/reaction-mech/nh3.yaml"
+
+def mech_path():
+    """The reference's nh3.yaml (the 9-species H2/O2/N2 subset is extracted from it)."""
+    ref = os.environ.get("LBM_REFERENCE")
+    if "--reference" in sys.argv:
+        ref = sys.argv[sys.argv.index("--reference") + 1]
+    if not ref:
+        raise SystemExit("make_golden.py: pass --reference <reference tree> or set LBM_REFERENCE")
+    return os.path.join(ref, "src", "reaction-mech", "nh3.yaml")
+
 MC_FIELDS = ["rho", "u", "v", "w", "temp", "p", "rhoe", "HRR"]
 
 FIELDS = ["rho", "u", "v", "w", "temp", "p"]

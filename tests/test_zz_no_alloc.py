@@ -1,8 +1,14 @@
-"""lbmgpu_sums_noalloc (reduction scratch in a fixed device array, no allocation) against
-lbmgpu_sums (handle scratch) on the same state: identical totals, bit for bit, on two
-calls in a row -- so the fixed scratch carries nothing from one call into the next --
-for a single-component and a multicomponent handle, and out-of-range sizes rejected.
-Collected last, so it also runs after every other GPU test in the same process."""
+"""lbmgpu_sums_noalloc is for callers that may not allocate device memory once their run
+is set up: a lattice sized to fill the GPU, a monitoring loop that must not stall other
+streams through cudaMalloc's device-wide synchronisation, a host whose memory pool owns
+the device.  Its reduction scratch is a fixed array of the library, loaded when a handle
+is created.  Checked here through the C ABI against lbmgpu_sums (handle scratch) on the
+same state: identical totals, bit for bit, on two calls in a row -- so the fixed scratch
+carries nothing from one call into the next -- for a single-component and a
+multicomponent handle; on a fresh handle whose first reduction is the no-alloc one,
+neither the handle's device bytes nor the device's free memory move across the call; and
+out-of-range sizes are rejected.  Collected last, so it also runs after every other GPU
+test in the same process."""
 import pytest
 
 import lbmgpu
@@ -39,6 +45,23 @@ def test_no_alloc_sums_match_multicomponent():
         lat.init()
         lat.step(2)
         _two_calls_agree(lat)
+
+
+def test_no_alloc_first_call_allocates_nothing():
+    import torch
+    cells, prm = cases.tgv_sc(12, Re=10.0)
+    with lbmgpu.Lattice(*cells.shape, prm["nu"], prm["R"], prm["gamma"], prm["prtl"]) as lat:
+        lat.upload(cells)
+        lat.init()
+        lat.step(2)
+        lat.synchronize()
+        held = lat.device_bytes()
+        free0, _ = torch.cuda.mem_get_info(0)
+        got = lat.sums_noalloc()
+        free1, _ = torch.cuda.mem_get_info(0)
+        assert lat.device_bytes() == held
+        assert free1 == free0
+        assert lat.sums() == got
 
 
 def test_no_alloc_sums_reject_sizes():
