@@ -49,6 +49,8 @@ BYTES_COLLIDE_FP64 = 2 * 54 * 8          # 864
 BYTES_STREAM_FP64 = 54 * 8 + 6 * 8       # 480
 BYTES_STEP_FP64 = 2 * 54 * 8             # 864: one read + one write of the populations
 OUTPUT_EVERY = 10
+# config 4's case: rms velocity (lattice units), hot-side temperature (K), dx (m), dx/dt (m/s)
+TURB_DEFAULTS = {"urms": 0.05, "t_hot": 1500.0, "dx": 2e-6, "dxdt": 1500.0}
 
 
 def parse():
@@ -58,15 +60,22 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=None, help="interior cells per axis")
-    ap.add_argument("--workload", choices=["tgv", "mix", "react", "inflow", "chan", "flame"], default="inflow",
+    ap.add_argument("--workload", choices=["turb", "tgv", "mix", "react", "inflow", "chan", "flame"], default="turb",
                     help="tgv: config 1 (single component, FP64 Taylor-Green vortex, 64^3); "
                          "mix: 9-species H2/air mixing layer, periodic (config 2 without its NSCBC "
                          "faces, 128^3); react: the same with the reference's explicit chemistry and a "
                          "1800 K slab; inflow: config 2's shape, the mixing layer between a characteristic "
                          "inflow and outflow (N^3); chan: config 3's case, a reacting H2-air channel with "
                          "NSCBC outflow ends and TMS walls, at 2N x N/2 x N/2; flame: config 3 itself, the "
-                         "same channel at 4N x N/16 x N/16 (512 x 8 x 8 at the default N)")
-    ap.add_argument("--chem", choices=["ref", "rosenbrock", "surrogate"], default="ref",
+                         "same channel at 4N x N/16 x N/16 (512 x 8 x 8 at the default N); turb (default): "
+                         "config 4, the decaying turbulent reacting H2/air layer, N^3 (256), FP32 populations, "
+                         "ROS2 stiff chemistry")
+    ap.add_argument("--urms", type=float, default=TURB_DEFAULTS["urms"], help="turb: rms velocity, lattice units")
+    ap.add_argument("--t-hot", type=float, default=TURB_DEFAULTS["t_hot"], help="turb: hot-side temperature, K")
+    ap.add_argument("--dx", type=float, default=TURB_DEFAULTS["dx"], help="turb: lattice spacing, m")
+    ap.add_argument("--dxdt", type=float, default=TURB_DEFAULTS["dxdt"], help="turb: dx / dt, m/s")
+    ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--chem", choices=["ref", "rosenbrock", "surrogate"], default=None,
                     help="reacting workloads: the reference's explicit scheme, the ROS2 stiff integrator, or "
                          "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
                          "surrogate steps with a 1 %% audit; plain ROS2 timed on the same lattice beside it)")
@@ -77,7 +86,7 @@ def parse():
                          "to compare peak temperature and integrated heat release")
     ap.add_argument("--augment", type=float, default=0.5,
                     help="surrogate: perturbed, integrator-labelled rows added per collected row")
-    ap.add_argument("--precision", choices=["fp64", "fp32"], default="fp64",
+    ap.add_argument("--precision", choices=["fp64", "fp32"], default=None,
                     help="multicomponent population storage (fp32: shifted FP32 populations, FP64 records)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -583,8 +592,8 @@ def run_ours_mc(args, dist):
         lat.time_steps(kp)
         _, kms_plain = lat.kernel_times()
         lat.profile(False)
-        chem_sur = (kms[3] + kms[4]) / max(kk, 1)
-        chem_plain = kms_plain[3] / max(kp, 1)
+        chem_sur = (kms[3] + kms[4] + kms[7]) / max(kk, 1)
+        chem_plain = (kms_plain[3] + kms_plain[7]) / max(kp, 1)
         sur["chemistry_ms_per_step"] = {"surrogate": chem_sur, "plain": chem_plain,
                                         "speedup": chem_plain / max(chem_sur, 1e-12)}
         sur["network_flops_per_cell"] = 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)
@@ -774,16 +783,241 @@ def run_ours(args, dist):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------
+# config 4: the decaying turbulent reacting H2/air layer, 256^3, FP32 populations, stiff
+# chemistry -- generated and uploaded plane range by plane range (its AoS copy is 83 GB)
+# ---------------------------------------------------------------------------------------
+TURB_CHUNK = 8  # x-planes per upload / download call
+
+
+def turb_units(args):
+    return (args.dx, args.dx / args.dxdt)
+
+
+def turb_gen(args, m, N, field, i0, i1):
+    import workloads
+    return workloads.turbulent_layer_mc(m, N=N, i0=i0, i1=i1, field=field, T_hi=args.t_hot, u_rms=args.urms,
+                                        units=turb_units(args))
+
+
+def turb_name(args, N):
+    chem = {"rosenbrock": "ROS2 stiff chemistry", "ref": "the reference's explicit chemistry",
+            "surrogate": "MLP chemistry surrogate"}[args.chem]
+    return (f"turb{N}_mc9_{args.precision}_{ {'rosenbrock': 'ros2', 'ref': 'refchem', 'surrogate': 'sur'}[args.chem]}: "
+            f"decaying turbulent reacting H2/air layer (config 4), 9-species D3Q27, {N}^3, periodic x z, TYPE_O_C "
+            f"y faces, u' {args.urms} l.u. (k0 4), air 300 K / H2-air {args.t_hot:g} K, dx {args.dx:g} m, "
+            f"dx/dt {args.dxdt:g} m/s, {chem}")
+
+
+def turb_cpu_child(args):
+    """Runs in a child process (bench.py --cpu-child): the reference's own solver on an N^3
+    instance of the turbulent layer, printing one JSON line {cells, steps, seconds}.  A child,
+    because the reference aborts the whole process when its temperature iteration fails."""
+    import mech
+    import workloads
+    from oracle import refmc
+    m = mech.h2_air_9()
+    N = args.N
+    mix, sp = turb_gen(args, m, N, None, 0, N + 2)
+    threads = os.cpu_count() or 1
+    fast = refmc.available(True, fast=True)
+    refmc.set_threads(threads, True, fast)
+    with stdout_to_stderr():
+        ref = refmc.RefMC(N, N, N, m, turb_units(args), workloads.MIXTURE_MC, workloads.SPECIES, reaction=True,
+                          fast=fast)
+        ref.cells[...] = mix
+        for a in range(len(sp)):
+            ref.species[a][...] = sp[a]
+        ref.init()
+        if args.warmup:
+            ref.loop(args.warmup)
+        t0 = time.perf_counter()
+        ref.loop(args.steps)
+        dt = time.perf_counter() - t0
+        ref.close()
+    print(json.dumps({"cells": N ** 3, "steps": args.steps, "seconds": dt, "threads": threads,
+                      "kind": "reference" if fast else "reference (oracle build)"}), flush=True)
+
+
+def turb_cpu_sample(args, N, steps, warmup):
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-child", "--N", str(N), "--steps", str(steps),
+           "--warmup", str(warmup), "--urms", str(args.urms), "--t-hot", str(args.t_hot), "--dx", str(args.dx),
+           "--dxdt", str(args.dxdt)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    for line in r.stdout.splitlines()[::-1]:
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError(f"reference solver exited with {r.returncode}: {r.stderr.strip().splitlines()[-1:]}")
+
+
+def run_reference_turb(args, dist):
+    if dist.rank != 0:
+        return
+    Ns = 32
+    try:
+        d = turb_cpu_sample(args, Ns, args.steps, args.warmup)
+        v = d["cells"] * d["steps"] / d["seconds"] / 1e6
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": d["seconds"] * 1e3 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded turbulence field and H2/air layer, numpy PCG64 seed 20261203)",
+                "config": {"workload": turb_name(args, args.N), "cells": args.N ** 3, "threads": d["threads"]},
+                "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": d["threads"], "kind": "reference",
+                                 "sample": f"{Ns}^3 instance of the same case, {args.steps} steps after {args.warmup} "
+                                           f"warm-up steps, reference multicomponent LBM + Cantera-API shim with "
+                                           f"its explicit chemistry, built with the reference's flags"},
+                "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    except Exception as exc:
+        line = {"impl": "reference", "unavailable": f"the reference solver failed on the workload: {exc}"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_turb(args, dist):
+    import lbmgpu
+    import mech
+    import workloads
+    device = dist.local
+    m = mech.h2_air_9()
+    N = args.N
+    ncell = N ** 3
+    field = workloads.turbulence_field(N, u_rms=args.urms)
+    chem = {"rosenbrock": lbmgpu.CHEM_ROSENBROCK, "ref": lbmgpu.CHEM_REF_EXPLICIT}[args.chem]
+    prec = lbmgpu.FP32 if args.precision == "fp32" else lbmgpu.FP64
+    pop_bytes = 4 if args.precision == "fp32" else 8
+    lat = lbmgpu.Lattice(N + 2, N + 2, N + 2, mech=m, dtype=workloads.MIXTURE_MC, species_dtype=workloads.SPECIES,
+                         dx_dt=turb_units(args), chem=chem, device=device, precision=prec)
+
+    def upload_all():
+        """Generates and uploads the state plane range by plane range; returns the seconds
+        spent inside the upload calls and the bytes they copied."""
+        api, nbytes = 0.0, 0
+        for i0 in range(0, N + 2, TURB_CHUNK):
+            mix, sp = turb_gen(args, m, N, field, i0, min(N + 2, i0 + TURB_CHUNK))
+            t0 = time.perf_counter()
+            lat.upload_planes(i0, mix, sp)
+            api += time.perf_counter() - t0
+            nbytes += mix.nbytes + sum(a.nbytes for a in sp)
+        return api, nbytes
+
+    upload_all()
+    lat.init()
+    lat.time_steps(max(3, args.warmup))
+    dist.barrier()
+    clk = Clocks(device)
+    clk.start()
+    ms = lat.time_steps(args.steps)
+    clocks = clk.stop()
+    status = lat.synchronize()
+    ms = dist.max(ms)
+    # per-kernel device times over a few more steps (every launch bracketed by events)
+    kk = min(args.steps, 5)
+    lat.profile(True)
+    lat.time_steps(kk)
+    launches, kms = lat.kernel_times()
+    lat.profile(False)
+    names = {0: "k_mc_relax", 1: "k_mc_gather", 2: "k_mc_special (+ other)", 3: "k_mc_props", 5: "k_mc_solve",
+             6: "k_mc_eflux", 7: "k_mc_chem"}
+    per_step = {names[k]: kms[k] / kk for k in names}
+    prof_step = sum(per_step.values())
+    step_ms = ms / args.steps
+    alg_step = 2 * 27 * 10 * pop_bytes + 16  # survey 8(d): one read + one write of every population, FP64 T
+    peak, peak_kind = peaks()
+    achieved = alg_step * ncell / (step_ms * 1e-3) / 1e9
+    kern = {}
+    for k, name in ((0, "k_mc_relax"), (1, "k_mc_gather")):
+        alg = mc_bytes(name, pop_bytes, True) * ncell
+        t = kms[k] / max(launches[k], 1)
+        kern[name] = {"alg_bytes_per_launch": alg, "mean_launch_ms": t, "achieved_gbs": alg / (t * 1e-3) / 1e9,
+                      "frac": alg / (t * 1e-3) / 1e9 / peak, "traffic": ncu_traffic(name, ncell)}
+    # end to end through the reference-facing calls: plane-range uploads from host memory
+    # and Init, per step the five phase calls and the conserved totals read back, the
+    # plane-range download of the final state; the time inside those calls
+    api_up, nbytes = upload_all()
+    dist.barrier()
+    t0 = time.perf_counter()
+    lat.init()
+    for _ in range(args.steps):
+        lat.collide_species()
+        lat.collide()
+        lat.streaming()
+        lat.tms_bc()
+        lat.calculate_moment()
+        tot = lat.sums()
+    lat.synchronize()
+    api_steps = time.perf_counter() - t0
+    api_down = 0.0
+    mix, sp = turb_gen(args, m, N, field, 0, TURB_CHUNK)
+    for i0 in range(0, N + 2, TURB_CHUNK):
+        i1 = min(N + 2, i0 + TURB_CHUNK)
+        mv, sv = mix[: i1 - i0], [a[: i1 - i0] for a in sp]
+        t0 = time.perf_counter()
+        lat.download_planes(i0, mv, sv)
+        api_down += time.perf_counter() - t0
+    wall = dist.max(api_up + api_steps + api_down)
+    e2e_status = lat.synchronize()
+    lat.close()
+    e2e = {"value": whole_job_mlups(dist.world, ncell, args.steps, wall), "unit": "MLUPS",
+           "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps + 8 * len(tot),
+           "seconds": {"upload": api_up, "init_steps_sums": api_steps, "download": api_down},
+           "note": "time inside the C-ABI calls: plane-range AoS uploads + Init, per step the five phase calls and "
+                   "the conserved totals read back, the plane-range AoS download (host-side generation of the "
+                   "initial state between upload calls excluded)"}
+    if dist.rank != 0:
+        return
+    value = whole_job_mlups(dist.world, ncell, args.steps, ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": dist.world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded turbulence field and H2/air layer, numpy PCG64 seed 20261203)",
+        "config": {"workload": turb_name(args, N), "cells": ncell, "parallelism": f"replicas{dist.world}",
+                   "l2": "state larger than L2 (86 GB at 258^3 FP32), no flush",
+                   "storage": "FP32 populations (shifted), FP64 records and arithmetic" if pop_bytes == 4 else "FP64"},
+        "chemistry": {"ms_per_step": per_step["k_mc_chem"], "fraction_of_step": per_step["k_mc_chem"] / step_ms,
+                      "integrator": "ROS2, rtol 1e-5" if args.chem == "rosenbrock" else args.chem},
+        "hbm_gbs_step": achieved,
+        "roofline": {"bound": "hbm", "kernel": "whole step (all kernels)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_cell": alg_step,
+                     "alg_bytes_note": "one read + one write of the 270 populations + FP64 T read and write",
+                     "kernel_ms_per_step": per_step, "profiled_ms_per_step": prof_step, "kernels": kern},
+        "gpu_launches": int(round(sum(launches) / kk * args.steps)),
+        "status": status, "e2e_status": e2e_status, "clocks": clocks, "e2e": e2e,
+    }
+    if dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            d = turb_cpu_sample(args, 32, 5, 1)
+            line["cpu_baseline"] = {"value": d["cells"] * d["steps"] / d["seconds"] / 1e6, "unit": "MLUPS",
+                                    "cores": d["threads"], "kind": "reference",
+                                    "sample": f"32^3 instance of the same case, {d['steps']} steps after 1 warm-up "
+                                              f"step, reference multicomponent LBM + Cantera-API shim with its "
+                                              f"explicit chemistry, reference flags, {d['seconds']:.1f} s"}
+        except Exception as exc:
+            line["cpu_baseline"] = {"value": None, "error": str(exc)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.N is None:
-        args.N = 64 if args.workload == "tgv" else 128
+        args.N = {"tgv": 64, "turb": 256}.get(args.workload, 128)
     if args.steps is None:
-        args.steps = 1000 if args.workload == "tgv" else 200
+        args.steps = {"tgv": 1000, "turb": 20}.get(args.workload, 200)
+    if args.chem is None:
+        args.chem = "rosenbrock" if args.workload == "turb" else "ref"
+    if args.precision is None:
+        args.precision = "fp32" if args.workload == "turb" else "fp64"
+    if args.cpu_child:
+        turb_cpu_child(args)
+        return
     dist = Dist()
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and args.workload == "turb":
+            run_reference_turb(args, dist)
+        elif args.impl == "reference":
             run_reference(args, dist)
+        elif args.workload == "turb":
+            run_ours_turb(args, dist)
         elif args.workload == "tgv":
             run_ours(args, dist)
         else:

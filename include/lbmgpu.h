@@ -156,6 +156,19 @@ int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos, const void *const *speci
  * every fluid cell; the stored moments of every other cell. */
 int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos);
 
+/* lbmgpu_upload / lbmgpu_download for the x-planes i0 .. i1-1 only (ghost planes counted,
+ * 0 <= i0 < i1 <= Nx), multicomponent handles: the caller's arrays hold the
+ * (i1 - i0) * Ny * Nz records of those planes, in the reference's order.  For lattices
+ * whose AoS copy (600 + n_species * 472 bytes per cell in the reference's layout: 83 GB at
+ * 258^3) does not fit in host memory at once, and for the reference's restart file, which
+ * is read and written plane by plane.  Planes may arrive in any order and over any number
+ * of calls; once every plane has arrived since the last complete upload, the state is
+ * complete and behaves exactly as after lbmgpu_upload (until then lbmgpu_init and the
+ * phases return LBMGPU_E_STATE).  No counterpart in the reference, which holds the whole
+ * AoS in host memory (src/headers/lbm.hpp:134-137). */
+int lbmgpu_upload_planes(lbmgpu_t *h, int i0, int i1, const void *mixture_aos, const void *const *species_aos);
+int lbmgpu_download_planes(lbmgpu_t *h, int i0, int i1, void *mixture_aos, void *const *species_aos);
+
 /* The base units units.set_m_kg_s(dx, dt) sets (src/headers/units.hpp:32-44), with its
  * float rounding: out = {m, kg, s, K}. */
 int lbmgpu_units_from_dx_dt(float dx, float dt, float *out4);
@@ -195,7 +208,8 @@ int lbmgpu_status(lbmgpu_t *h, uint32_t *flags, int clear);
  * (multicomponent: the interior cells' pull and population sums), 2 other, 3
  * multicomponent collision parameters, 4 chemistry surrogate (features, network, the
  * integrator's cells), 5 multicomponent moment solve of the interior cells, 6
- * multicomponent energy-flux terms of the collision.  Returns the number of kinds. */
+ * multicomponent energy-flux terms of the collision, 7 stiff chemistry (ROS2) of every
+ * cell.  Returns the number of kinds. */
 int lbmgpu_profile(lbmgpu_t *h, int enable);
 int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
 

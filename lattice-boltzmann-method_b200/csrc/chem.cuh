@@ -20,21 +20,28 @@ namespace gas {
 
 constexpr int kChemMaxSub = 256;
 
-// right-hand side of the reactor state y = (Y_0..Y_{ns-1}, T) at density rho (kg/m^3)
-GAS_HD void reactor_rhs(const Tables &t, double rho, const double *y, double *F) {
+// right-hand side of the reactor state y = (Y_0..Y_{ns-1}, T) at density rho (kg/m^3),
+// with the temperature factors K = rate_factors(t, y[ns])
+GAS_HD void reactor_rhs_k(const Tables &t, const RateT &K, double rho, const double *y, double *F) {
     const int ns = t.ns;
     double C[MAXS], w[MAXS];
     const double T = y[ns];
     for (int k = 0; k < ns; ++k) C[k] = rho * y[k] * t.invW[k];
-    net_production(t, T, C, w);
+    net_production_k(t, K, C, w);
     double cv = 0.0, s = 0.0;
     for (int k = 0; k < ns; ++k) {
         F[k] = w[k] * t.m.W[k] / rho;
-        cv += y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
-        s += (h_RT(t, k, T) - 1.0) * kR * T * w[k];   // e_k W_k = h_k,molar - R T
+        cv += y[k] * (K.cpR[k] - 1.0) * t.invW[k];
+        s += (K.hRT[k] - 1.0) * kR * T * w[k];   // e_k W_k = h_k,molar - R T
     }
     cv *= kR;
     F[ns] = -s / (rho * cv);
+}
+
+GAS_HD void reactor_rhs(const Tables &t, double rho, const double *y, double *F) {
+    RateT K;
+    rate_factors(t, y[t.ns], K);
+    reactor_rhs_k(t, K, rho, y, F);
 }
 
 // LU with partial pivoting of an n x n matrix (row-major, stride MAXS+1); returns false
@@ -96,13 +103,18 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        reactor_rhs(t, rho, y, F0);
+        // the temperature factors at y serve F0 and the species columns; the temperature
+        // column and the second stage take their own
+        RateT K;
+        rate_factors(t, y[ns], K);
+        reactor_rhs_k(t, K, rho, y, F0);
         // finite-difference Jacobian, column by column
         for (int c = 0; c < n; ++c) {
             for (int q = 0; q < n; ++q) yp[q] = y[q];
             const double eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
             yp[c] += eps;
-            reactor_rhs(t, rho, yp, Fp);
+            if (c == ns) rate_factors(t, yp[ns], K);
+            reactor_rhs_k(t, K, rho, yp, Fp);
             for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
         }
         for (int r = 0; r < n; ++r) M[r][r] += 1.0;
@@ -113,7 +125,8 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
         lu_solve(M, n, piv, k1);
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        reactor_rhs(t, rho, yp, Fp);
+        rate_factors(t, yp[ns], K);
+        reactor_rhs_k(t, K, rho, yp, Fp);
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
         lu_solve(M, n, piv, k2);
         double err = 0.0;
@@ -167,6 +180,8 @@ __device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
+        RateT K;
+        bool k_at_y = false;  // K holds the factors at y's temperature
         for (int m = 0; m < kPer; ++m) {
             const int c = g + m * G;  // column c < n, or the unperturbed right-hand side c == n
             if (c > n) break;
@@ -177,7 +192,14 @@ __device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double
                 yp[c] += eps;
             }
             ec[m] = eps;
-            reactor_rhs(t, rho, yp, Fc[m]);
+            if (c == ns) {
+                rate_factors(t, yp[ns], K);
+                k_at_y = false;
+            } else if (!k_at_y) {
+                rate_factors(t, y[ns], K);
+                k_at_y = true;
+            }
+            reactor_rhs_k(t, K, rho, yp, Fc[m]);
         }
         for (int r = 0; r < n; ++r) F0[r] = __shfl_sync(gmask, Fc[n / G][r], n % G, G);
         for (int m = 0; m < kPer; ++m)  // this lane's Jacobian columns
@@ -193,7 +215,8 @@ __device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
         lu_solve(M, n, piv, k1);
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        reactor_rhs(t, rho, yp, Fp);
+        rate_factors(t, yp[ns], K);
+        reactor_rhs_k(t, K, rho, yp, Fp);
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
         lu_solve(M, n, piv, k2);
         double err = 0.0;

@@ -274,44 +274,39 @@ GAS_HD double mix_cond(const Tables &t, const double *X, double T, double P, con
 }
 
 // ---- kinetics ----------------------------------------------------------------------
-// Net molar production rates wdot[k] (kmol/m^3/s) at (T, concentrations C[k] kmol/m^3).
-GAS_HD void net_production(const Tables &t, double T, const double *C, double *wdot) {
+// The temperature-only factors of the net production rates at one T: the Arrhenius rate
+// (k_inf for fall-off reactions), the fall-off k_0 and log10 F_cent (Troe), the reverse
+// factor exp(dG/RT - dnu ln(p_atm / R T)) = 1 / K_c, and the species' h/RT and cp/R.  A
+// stiff integrator evaluates the rates at many compositions but few temperatures (its
+// finite-difference Jacobian perturbs one species at a time), so it computes these once
+// per temperature (rate_factors) and the composition-dependent part per call
+// (net_production_k); net_production does both, with the same arithmetic.
+struct RateT {
+    double kf[MAXR], k0[MAXR], lFc[MAXR], er[MAXR];
+    double hRT[MAXS], cpR[MAXS];
+};
+
+GAS_HD void rate_factors(const Tables &t, double T, RateT &K) {
     const lbmgpu_mech &m = t.m;
     double g_RT[MAXS];
     for (int k = 0; k < t.ns; ++k) {
-        g_RT[k] = h_RT(t, k, T) - s_R(t, k, T);
-        wdot[k] = 0.0;
+        K.hRT[k] = h_RT(t, k, T);
+        K.cpR[k] = cp_R(t, k, T);
+        g_RT[k] = K.hRT[k] - s_R(t, k, T);
     }
-    double Ctot = 0.0;
-    for (int k = 0; k < t.ns; ++k) Ctot += C[k];
     const double logT = log(T), invRT = 1.0 / (kR * T);
     const double log_cref = log(kOneAtm / (kR * T));
     for (int r = 0; r < m.n_reactions; ++r) {
-        double kf = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
-        double M = 1.0;
-        if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
-            M = 0.0;
-            for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
-        }
+        K.kf[r] = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
         if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
-            const double k0 = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
-            const double Pr = k0 * M / kf;
-            double F = 1.0;
+            K.k0[r] = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
             if (m.troe_n[r] >= 3) {
                 const double a = m.troe[r][0], T3 = m.troe[r][1], T1 = m.troe[r][2];
                 double Fc = (1.0 - a) * exp(-T / T3) + a * exp(-T / T1);
                 if (m.troe_n[r] == 4) Fc += exp(-m.troe[r][3] / T);
-                const double lFc = log10(fmax(Fc, 1e-300));
-                const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-                const double lPr = log10(fmax(Pr, 1e-300));
-                const double x = (lPr + c) / (n - 0.14 * (lPr + c));
-                F = pow(10.0, lFc / (1.0 + x * x));
+                K.lFc[r] = log10(fmax(Fc, 1e-300));
             }
-            kf = kf * (Pr / (1.0 + Pr)) * F;
-            M = 1.0;
         }
-        double fwd = kf * M, rev = 0.0;
-        for (int j = 0; j < m.n_reac[r]; ++j) fwd *= pow(C[m.reac[r][j]], m.nu_reac[r][j]);
         if (m.reversible[r]) {
             double dG = 0.0, dnu = 0.0;
             for (int j = 0; j < m.n_prod[r]; ++j) {
@@ -322,15 +317,62 @@ GAS_HD void net_production(const Tables &t, double T, const double *C, double *w
                 dG -= m.nu_reac[r][j] * g_RT[m.reac[r][j]];
                 dnu -= m.nu_reac[r][j];
             }
-            const double kr = kf * M * exp(dG - dnu * log_cref);  // kf / Kc
-            rev = kr;
-            for (int j = 0; j < m.n_prod[r]; ++j) rev *= pow(C[m.prod[r][j]], m.nu_prod[r][j]);
+            K.er[r] = exp(dG - dnu * log_cref);
+        }
+    }
+}
+
+// C^nu of a mass-action factor: a product for the integer orders 1 to 3 (the elementary
+// stoichiometries of the mechanisms), pow otherwise.
+GAS_HD double conc_pow(double C, double nu) {
+    if (nu == 1.0) return C;
+    if (nu == 2.0) return C * C;
+    if (nu == 3.0) return C * C * C;
+    return pow(C, nu);
+}
+
+// Net molar production rates wdot[k] (kmol/m^3/s) from the factors of rate_factors and
+// the concentrations C[k] (kmol/m^3).
+GAS_HD void net_production_k(const Tables &t, const RateT &K, const double *C, double *wdot) {
+    const lbmgpu_mech &m = t.m;
+    for (int k = 0; k < t.ns; ++k) wdot[k] = 0.0;
+    for (int r = 0; r < m.n_reactions; ++r) {
+        double kf = K.kf[r];
+        double M = 1.0;
+        if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
+            M = 0.0;
+            for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
+        }
+        if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
+            const double Pr = K.k0[r] * M / kf;
+            double F = 1.0;
+            if (m.troe_n[r] >= 3) {
+                const double lFc = K.lFc[r];
+                const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+                const double lPr = log10(fmax(Pr, 1e-300));
+                const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+                F = pow(10.0, lFc / (1.0 + x * x));
+            }
+            kf = kf * (Pr / (1.0 + Pr)) * F;
+            M = 1.0;
+        }
+        double fwd = kf * M, rev = 0.0;
+        for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.nu_reac[r][j]);
+        if (m.reversible[r]) {
+            rev = kf * M * K.er[r];  // kf / Kc
+            for (int j = 0; j < m.n_prod[r]; ++j) rev *= conc_pow(C[m.prod[r][j]], m.nu_prod[r][j]);
         }
         const double q = fwd - rev;
         for (int j = 0; j < m.n_reac[r]; ++j) wdot[m.reac[r][j]] -= m.nu_reac[r][j] * q;
         for (int j = 0; j < m.n_prod[r]; ++j) wdot[m.prod[r][j]] += m.nu_prod[r][j] * q;
     }
-    (void)Ctot;
+}
+
+// Net molar production rates wdot[k] (kmol/m^3/s) at (T, concentrations C[k] kmol/m^3).
+GAS_HD void net_production(const Tables &t, double T, const double *C, double *wdot) {
+    RateT K;
+    rate_factors(t, T, K);
+    net_production_k(t, K, C, wdot);
 }
 
 // Least-squares polynomial fit (degree 4) of y(x) on n points; normal equations solved

@@ -20,10 +20,11 @@ enum Phase { PH_BOUNDARY = 0, PH_COLLIDED = 1, PH_STREAMED = 2, PH_BC = 3, PH_SP
 // (k_mc_relax), K_STREAM_MOMENT the pull and population sums of the interior cells
 // (k_mc_gather), K_PROPS the collision parameters (k_mc_props), K_SURROGATE the chemistry
 // surrogate's features, network and integrator list, K_SOLVE the interior cells' moment
-// solve (k_mc_solve), K_EFLUX the energy-flux terms of the collision (k_mc_eflux)
+// solve (k_mc_solve), K_EFLUX the energy-flux terms of the collision (k_mc_eflux), K_CHEM
+// the stiff chemistry of every cell (k_mc_chem, ROS2 without the surrogate)
 enum KernelKind {
     K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_SOLVE = 5, K_EFLUX = 6,
-    K_NKINDS = 7
+    K_CHEM = 7, K_NKINDS = 8
 };
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.
@@ -91,6 +92,11 @@ struct lbmgpu {
     lbmh::SurState *sur = nullptr;          // chemistry surrogate, created on first use
     lbmgpu_mech mech{};                     // multicomponent: the caller's mechanism, copied at create
     long nfluid = 0;
+    // plane-range uploads (multicomponent): the cell types on the host, and which x-planes
+    // have arrived since the last complete upload
+    std::vector<int8_t> htype;
+    std::vector<char> plane_have;
+    int planes_have = 0;
 };
 
 namespace lbmh {
@@ -154,6 +160,8 @@ inline unsigned grid_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock);
 int mc_setup(lbmgpu *h);
 int mc_upload(lbmgpu *h, const void *mix, const void *const *species);
 int mc_download(lbmgpu *h, void *mix, void *const *species);
+int mc_upload_planes(lbmgpu *h, int i0, int i1, const void *mix, const void *const *species);
+int mc_download_planes(lbmgpu *h, int i0, int i1, void *mix, void *const *species);
 int mc_init(lbmgpu *h);
 int mc_launch_collide(lbmgpu *h);
 int mc_launch_stream(lbmgpu *h);

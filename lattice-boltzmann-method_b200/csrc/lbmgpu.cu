@@ -649,6 +649,20 @@ int lbmgpu_upload(lbmgpu_t *h, const void *mixture_aos, const void *const *speci
     return LBMGPU_OK;
 }
 
+int lbmgpu_upload_planes(lbmgpu_t *h, int i0, int i1, const void *mixture_aos, const void *const *species_aos) {
+    if (!h || !mixture_aos) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    return lbmh::mc_upload_planes(h, i0, i1, mixture_aos, species_aos);
+}
+
+int lbmgpu_download_planes(lbmgpu_t *h, int i0, int i1, void *mixture_aos, void *const *species_aos) {
+    if (!h || !mixture_aos) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
+    return lbmh::mc_download_planes(h, i0, i1, mixture_aos, species_aos);
+}
+
 int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos) {
     if (!h || !mixture_aos) return LBMGPU_E_ARG;
     if (!h->have_state) return LBMGPU_E_STATE;

@@ -2,8 +2,9 @@
 // mc_cell.cuh and the handle operations for n_species > 0.
 //
 // Reference path replaced (farrasarira/Lattice-Boltzmann-Method, MULTICOMP on):
-//   LBM::Collide_Species + LBM::Collide   src/lbm-collision.cpp:191-526 -> k_mc_props (+ the surrogate's
-//                                          kernels, k_mc_chem_list), k_mc_eflux, k_mc_relax
+//   LBM::Collide_Species + LBM::Collide   src/lbm-collision.cpp:191-526 -> k_mc_props, k_mc_chem (stiff
+//                                          chemistry or the surrogate's use; the surrogate's kernels,
+//                                          k_mc_chem_list), k_mc_eflux, k_mc_relax
 //   LBM::Streaming + LBM::calculate_moment src/lbm-streaming.cpp, src/lbm-moment.cpp:193-377
 //                                          -> k_mc_gather (pull + population sums per
 //                                             (cell, set)) and k_mc_solve (per cell)
@@ -68,6 +69,24 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
         chem_list_groups<NS, 8>(A, cnt);
     else
         chem_list_groups<NS, 4>(A, cnt);
+}
+
+// Chemistry of every fluid cell for LBMGPU_CHEM_ROSENBROCK handles, one thread per cell,
+// beside the transport part of the collision parameters (k_mc_props<CHEM_OFF>), from the
+// state the collision forms from the record (mc_chem_state):
+//   SUR = false: the stiff integrator (ROS2) itself;
+//   SUR = true : the surrogate's prediction where the gate passes it (element projection,
+//                output gate), the cells it does not cover and the audited ones appended
+//                to the integrator list for k_mc_chem_list.
+// A kernel of its own, so that its time (with the surrogate's kernels) is the chemistry's
+// share of the step, and the transport kernel keeps its own occupancy.
+template <int NS, bool SUR, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_chem(McArgsT<S, double> A) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
+    double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
+    mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
+    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
@@ -212,7 +231,7 @@ __global__ void k_mc_unpack(McArgsT<S, double> A, MixOff mo, SpOff so, const cha
     const int pi[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
     for (int q = 0; q < 6; ++q) pr(RM_P00 + q, ldd(mr, mo.p_tensor + 8 * (3 * pi[q][0] + pi[q][1])));
     pr(RM_HRR, ldd(mr, mo.HRR));
-    const bool fluid = A.cflag[n] & CF_FLUID;
+    const bool fluid = A.type[n] == T_F;  // the cell classification follows the whole upload
     double rho_a[NS], ua[NS][3];
     for (int a = 0; a < NS; ++a) {
         const char *sr = stage + cnt * mo.size + ((long)a * cnt + (n - n0)) * so.size;
@@ -369,18 +388,19 @@ int rebase_shift(lbmgpu *h) {
     return 0;
 }
 
+// The records of cells [c0, c1) -- the caller's arrays start at cell c0 -- into the device
+// state, one staging chunk at a time.
 template <typename S>
-int upload_t(lbmgpu *h, const char *hm, const void *const *species) {
-    const long nc = h->g.ncell;
+int upload_t(lbmgpu *h, const char *hm, const void *const *species, long c0, long c1) {
     const size_t ms = h->mo.size, ss = h->so.size;
     McArgsT<S, double> A = base_args<S>(h);
-    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
-        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells), cnt = n1 - n0;
-        CK(cudaMemcpyAsync(h->stage, hm + n0 * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
+    for (long n0 = c0; n0 < c1; n0 += (long)h->stage_cells) {
+        const long n1 = std::min<long>(c1, n0 + (long)h->stage_cells), cnt = n1 - n0;
+        CK(cudaMemcpyAsync(h->stage, hm + (n0 - c0) * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
         for (int a = 0; a < h->ns; ++a)
             CK(cudaMemcpyAsync(h->stage + cnt * ms + (size_t)a * cnt * ss,
-                               static_cast<const char *>(species[a]) + n0 * ss, cnt * ss, cudaMemcpyHostToDevice,
-                               h->stream));
+                               static_cast<const char *>(species[a]) + (n0 - c0) * ss, cnt * ss,
+                               cudaMemcpyHostToDevice, h->stream));
         EvPair ep{};
         ev_begin(h, K_OTHER, ep);
         k_mc_unpack<NS9, S><<<grid_for(cnt), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[0],
@@ -437,14 +457,20 @@ int collide_t(lbmgpu *h) {
     const unsigned gp = grid_for(h->g.ncell);
     if (h->chem == CHEM_REF_EXPLICIT)
         k_mc_props<NS9, CHEM_REF_EXPLICIT, S><<<gp, kBlock, 0, h->stream>>>(A);
-    else if (h->chem == CHEM_ROSENBROCK && A.sur.mode == 1 && A.sur.ilist)
-        k_mc_props<NS9, CHEM_SURROGATE_STEP, S><<<gp, kBlock, 0, h->stream>>>(A);
-    else if (h->chem == CHEM_ROSENBROCK)
-        k_mc_props<NS9, CHEM_ROSENBROCK, S><<<gp, kBlock, 0, h->stream>>>(A);
     else
-        k_mc_props<NS9, CHEM_OFF, S><<<gp, kBlock, 0, h->stream>>>(A);
+        k_mc_props<NS9, CHEM_OFF, S><<<gp, kBlock, 0, h->stream>>>(A);  // ROS2 / surrogate: k_mc_chem
     ev_end(h, ep);
     CK(cudaGetLastError());
+    if (h->chem == CHEM_ROSENBROCK) {
+        EvPair ec{};
+        ev_begin(h, K_CHEM, ec);
+        if (A.sur.mode == 1 && A.sur.ilist)
+            k_mc_chem<NS9, true, S><<<gp, kBlock, 0, h->stream>>>(A);
+        else
+            k_mc_chem<NS9, false, S><<<gp, kBlock, 0, h->stream>>>(A);
+        ev_end(h, ec);
+        CK(cudaGetLastError());
+    }
     if (A.sur.ilist) {
         EvPair ei{};
         ev_begin(h, K_SURROGATE, ei);
@@ -573,24 +599,13 @@ void mc_release(lbmgpu *h) {
     }
 }
 
-int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
-    if (!species) return LBMGPU_E_ARG;
-    for (int a = 0; a < h->ns; ++a)
-        if (!species[a]) return LBMGPU_E_ARG;
-    CK(cudaSetDevice(h->d.device));
+// Classification of the whole lattice once every plane is on the device: fluid cells,
+// the cells with a boundary upstream (compact list), the boundary store, the FP32 shift.
+static int mc_finish_upload(lbmgpu *h) {
     const lbm::ScGeom &g = h->g;
     const long nc = g.ncell;
-    const size_t ms = h->mo.size;
-    const char *hm = static_cast<const char *>(mix);
-    std::vector<int8_t> ty(nc);
+    const std::vector<int8_t> &ty = h->htype;
     std::vector<uint8_t> cf(nc, 0);
-    for (long n = 0; n < nc; ++n) {
-        short t;
-        std::memcpy(&t, hm + n * ms + h->mo.type, sizeof(short));
-        if (t < 0 || t > 9) return LBMGPU_E_ARG;
-        if (t == T_I || t == T_O || t == T_Q) return LBMGPU_E_UNSUPPORTED;
-        ty[n] = (int8_t)t;
-    }
     long nfluid = 0, nb = 0;
     std::vector<int> bidh(nc, -1);
     std::vector<long> blh;
@@ -642,12 +657,9 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
     }
     if (nb > 0) CK(cudaMemcpyAsync(h->blist, blh.data(), nb * sizeof(long), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->bid, bidh.data(), nc * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->type, ty.data(), nc, cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->cflag, cf.data(), nc, cudaMemcpyHostToDevice, h->stream));
-    int rc = h->fp32 ? upload_t<float>(h, hm, species) : upload_t<double>(h, hm, species);
-    if (rc) return rc;
     h->cur = 0;
-    rc = rebase_shift(h);
+    int rc = rebase_shift(h);
     if (rc) return rc;
     rc = h->fp32 ? fill_bst<float>(h) : fill_bst<double>(h);
     if (rc) return rc;
@@ -658,22 +670,65 @@ int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
     return LBMGPU_OK;
 }
 
-int mc_download(lbmgpu *h, void *mix, void *const *species) {
+int mc_upload_planes(lbmgpu *h, int i0, int i1, const void *mix, const void *const *species) {
     if (!species) return LBMGPU_E_ARG;
     for (int a = 0; a < h->ns; ++a)
         if (!species[a]) return LBMGPU_E_ARG;
+    const lbm::ScGeom &g = h->g;
+    if (i0 < 0 || i1 > g.Nx || i0 >= i1) return LBMGPU_E_ARG;
     CK(cudaSetDevice(h->d.device));
-    const long nc = h->g.ncell;
+    const long c0 = (long)i0 * g.si, c1 = (long)i1 * g.si;
+    const size_t ms = h->mo.size;
+    const char *hm = static_cast<const char *>(mix);
+    if ((long)h->htype.size() != g.ncell) h->htype.assign(g.ncell, 0);
+    if ((int)h->plane_have.size() != g.Nx) h->plane_have.assign(g.Nx, 0);
+    for (long n = c0; n < c1; ++n) {
+        short t;
+        std::memcpy(&t, hm + (n - c0) * ms + h->mo.type, sizeof(short));
+        if (t < 0 || t > 9) return LBMGPU_E_ARG;
+        if (t == T_I || t == T_O || t == T_Q) return LBMGPU_E_UNSUPPORTED;
+        h->htype[n] = (int8_t)t;
+    }
+    // a new upload begins: the state is incomplete until every plane has arrived again
+    if (h->planes_have == 0) h->have_state = false;
+    CK(cudaMemcpyAsync(h->type + c0, h->htype.data() + c0, c1 - c0, cudaMemcpyHostToDevice, h->stream));
+    int rc = h->fp32 ? upload_t<float>(h, hm, species, c0, c1) : upload_t<double>(h, hm, species, c0, c1);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream));
+    for (int i = i0; i < i1; ++i)
+        if (!h->plane_have[i]) {
+            h->plane_have[i] = 1;
+            ++h->planes_have;
+        }
+    if (h->planes_have < g.Nx) return LBMGPU_OK;
+    h->planes_have = 0;
+    std::fill(h->plane_have.begin(), h->plane_have.end(), 0);
+    return mc_finish_upload(h);
+}
+
+int mc_upload(lbmgpu *h, const void *mix, const void *const *species) {
+    h->planes_have = 0;
+    std::fill(h->plane_have.begin(), h->plane_have.end(), 0);
+    return mc_upload_planes(h, 0, h->g.Nx, mix, species);
+}
+
+int mc_download_planes(lbmgpu *h, int i0, int i1, void *mix, void *const *species) {
+    if (!species) return LBMGPU_E_ARG;
+    for (int a = 0; a < h->ns; ++a)
+        if (!species[a]) return LBMGPU_E_ARG;
+    if (i0 < 0 || i1 > h->g.Nx || i0 >= i1) return LBMGPU_E_ARG;
+    CK(cudaSetDevice(h->d.device));
+    const long c0 = (long)i0 * h->g.si, c1 = (long)i1 * h->g.si;
     const size_t ms = h->mo.size, ss = h->so.size;
-    std::vector<uint8_t> cf(nc);
-    CK(cudaMemcpyAsync(cf.data(), h->cflag, nc, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<uint8_t> cf(c1 - c0);
+    CK(cudaMemcpyAsync(cf.data(), h->cflag + c0, c1 - c0, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     const bool stepped = h->pack_mode == PK_STEPPED;
     const long mfld[] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.p, h->mo.temp, h->mo.rhoe, h->mo.HRR};
     const long sfld[] = {h->so.X, h->so.rho, h->so.u, h->so.v, h->so.w};
     char *hm = static_cast<char *>(mix);
-    for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
-        const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells), cnt = n1 - n0;
+    for (long n0 = c0; n0 < c1; n0 += (long)h->stage_cells) {
+        const long n1 = std::min<long>(c1, n0 + (long)h->stage_cells), cnt = n1 - n0;
         const int rc = h->fp32 ? pack_chunk<float>(h, n0, n1, stepped) : pack_chunk<double>(h, n0, n1, stepped);
         if (rc) return rc;
         const size_t bytes = cnt * (ms + (size_t)h->ns * ss);
@@ -681,8 +736,9 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
         CK(cudaStreamSynchronize(h->stream));
         for (long n = n0; n < n1; ++n) {
             const char *srec = h->bounce + (n - n0) * ms;
-            char *drec = hm + n * ms;
-            if (cf[n] & CF_FLUID) {
+            char *drec = hm + (n - c0) * ms;
+            const bool fluid = cf[n - c0] & CF_FLUID;
+            if (fluid) {
                 short t;
                 std::memcpy(&t, drec + h->mo.type, sizeof(short));
                 std::memcpy(drec, srec, ms);
@@ -693,8 +749,8 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
             }
             for (int a = 0; a < h->ns; ++a) {
                 const char *ssrc = h->bounce + cnt * ms + ((size_t)a * cnt + (n - n0)) * ss;
-                char *sdst = static_cast<char *>(species[a]) + n * ss;
-                if (cf[n] & CF_FLUID)
+                char *sdst = static_cast<char *>(species[a]) + (n - c0) * ss;
+                if (fluid)
                     std::memcpy(sdst, ssrc, ss);
                 else
                     for (long o : sfld) std::memcpy(sdst + o, ssrc + o, sizeof(double));
@@ -703,6 +759,8 @@ int mc_download(lbmgpu *h, void *mix, void *const *species) {
     }
     return LBMGPU_OK;
 }
+
+int mc_download(lbmgpu *h, void *mix, void *const *species) { return mc_download_planes(h, 0, h->g.Nx, mix, species); }
 
 int mc_init(lbmgpu *h) {
     int rc = h->fp32 ? init_t<float>(h) : init_t<double>(h);

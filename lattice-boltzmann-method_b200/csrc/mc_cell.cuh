@@ -50,9 +50,6 @@ MC_HD int mc_nrec(int ns) { return RM_SP + RM_SPN * ns; }
 MC_HD int rs(int a, int f) { return RM_SP + RM_SPN * a + f; }
 
 enum : int { CHEM_OFF = 0, CHEM_REF_EXPLICIT = 1, CHEM_ROSENBROCK = 2 };
-// instance of the collision-parameter kernel for ROS2 handles with the surrogate on: every
-// cell the network does not cover goes to the integrator list, none is integrated inline
-constexpr int CHEM_SURROGATE_STEP = 3;
 
 template <typename P_, typename R_>
 struct McArgsT {
@@ -649,10 +646,8 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
             prp(pr_drho<NS>(a), drho[a]);
         }
         put(A, A.rec_nxt, RM_HRR, n, hrr);
-    } else if (CHEM == CHEM_ROSENBROCK) {
+    } else if (CHEM == CHEM_ROSENBROCK) {  // the host build; the device runs it in k_mc_chem
         mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
-    } else if (CHEM == CHEM_SURROGATE_STEP) {
-        mc_chem_ros2<NS, AT, false>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
     }
 
     // -- species viscosities; Wilke weights phi_ab = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^1/4)^2 /

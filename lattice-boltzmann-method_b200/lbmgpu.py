@@ -32,7 +32,8 @@ MIXTURE_SC = np.dtype({
 })
 
 EXPORTS = [
-    "lbmgpu_create", "lbmgpu_destroy", "lbmgpu_upload", "lbmgpu_download", "lbmgpu_init",
+    "lbmgpu_create", "lbmgpu_destroy", "lbmgpu_upload", "lbmgpu_download", "lbmgpu_upload_planes",
+    "lbmgpu_download_planes", "lbmgpu_init",
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
@@ -42,6 +43,7 @@ EXPORTS = [
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
 ]
 SUMS_MAX = 21
+KERNEL_KINDS = 8
 DIAG_COUNT = 6
 SUR_IN, SUR_OUT, SUR_NPARAMS = 12, 10, 36046
 
@@ -97,6 +99,8 @@ def lib():
             getattr(L, name).argtypes = [vp]
         L.lbmgpu_upload.argtypes = [vp, vp, vp]
         L.lbmgpu_download.argtypes = [vp, vp, vp]
+        L.lbmgpu_upload_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.lbmgpu_download_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
         L.lbmgpu_units_from_dx_dt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
         L.lbmgpu_step.argtypes = [vp, ctypes.c_int]
         L.lbmgpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
@@ -197,21 +201,35 @@ class Lattice:
         _check(lib().lbmgpu_create(ctypes.byref(d), ctypes.byref(self.h)), "lbmgpu_create")
 
     # -- state transfer ---------------------------------------------------------------
-    def _cells_ptr(self, cells):
-        if cells.dtype != self.dtype or cells.shape != self.shape or not cells.flags.c_contiguous:
-            raise ValueError("cell array must be a C-contiguous %s array of shape %s" % (self.dtype, self.shape))
+    def _cells_ptr(self, cells, shape=None):
+        shape = shape or self.shape
+        if cells.dtype != self.dtype or cells.shape != shape or not cells.flags.c_contiguous:
+            raise ValueError("cell array must be a C-contiguous %s array of shape %s" % (self.dtype, shape))
         return cells.ctypes.data
 
-    def _species_ptrs(self, species):
+    def _species_ptrs(self, species, shape=None):
+        shape = shape or self.shape
         if self.ns == 0:
             return None
         if species is None or len(species) != self.ns:
             raise ValueError("one species array per species is required")
         for sp in species:
-            if sp.dtype != self.species_dtype or sp.shape != self.shape or not sp.flags.c_contiguous:
+            if sp.dtype != self.species_dtype or sp.shape != shape or not sp.flags.c_contiguous:
                 raise ValueError("species arrays must be C-contiguous %s arrays of shape %s"
-                                 % (self.species_dtype, self.shape))
+                                 % (self.species_dtype, shape))
         return (ctypes.c_void_p * self.ns)(*[sp.ctypes.data for sp in species])
+
+    def upload_planes(self, i0, cells, species):
+        """Uploads the x-planes i0 .. i0 + cells.shape[0] - 1 (lbmgpu_upload_planes)."""
+        shape = (cells.shape[0],) + self.shape[1:]
+        _check(lib().lbmgpu_upload_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
+                                          self._species_ptrs(species, shape)), "lbmgpu_upload_planes")
+
+    def download_planes(self, i0, cells, species):
+        """Downloads the x-planes i0 .. i0 + cells.shape[0] - 1 (lbmgpu_download_planes)."""
+        shape = (cells.shape[0],) + self.shape[1:]
+        _check(lib().lbmgpu_download_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
+                                            self._species_ptrs(species, shape)), "lbmgpu_download_planes")
 
     def upload(self, cells, species=None):
         _check(lib().lbmgpu_upload(self.h, self._cells_ptr(cells), self._species_ptrs(species)), "lbmgpu_upload")
@@ -265,10 +283,10 @@ class Lattice:
         """Per kernel kind (0 collide / population update, 1 stream+boundary+moment
         (multicomponent: the interior pull and sums), 2 other, 3 multicomponent collision
         parameters, 4 chemistry surrogate, 5 multicomponent moment solve, 6 multicomponent
-        energy-flux terms): launches and device ms."""
-        launches = (ctypes.c_long * 7)()
-        ms = (ctypes.c_double * 7)()
-        _check(lib().lbmgpu_kernel_times(self.h, 7, launches, ms), "lbmgpu_kernel_times")
+        energy-flux terms, 7 stiff chemistry of every cell): launches and device ms."""
+        launches = (ctypes.c_long * KERNEL_KINDS)()
+        ms = (ctypes.c_double * KERNEL_KINDS)()
+        _check(lib().lbmgpu_kernel_times(self.h, KERNEL_KINDS, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------

@@ -300,3 +300,99 @@ def inflow_layer_mc(mech, NX=32, NY=8, NZ=8, u_in_si=5.0, T_in=300.0, Y_H2=0.03,
                 sp[a]["X"][ii] = X[a]
         mix["p"][ii] = p_lattice(ONE_ATM)
     return mix, sp
+
+
+# ---------------------------------------------------------------------------------------
+# Decaying turbulent reacting H2/air layer (config 4's case), generated plane range by plane
+# range so that lattices whose AoS copy does not fit in host memory (83 GB at 256^3) can be
+# uploaded in pieces (lbmgpu_upload_planes).
+# ---------------------------------------------------------------------------------------
+# units.set_m_kg_s(dx, dt) with dx / dt = 1500 m/s: theta = R T (dt/dx)^2 is 0.038 in 300 K
+# air (u' = 0.05 is then Mach 0.22) and below 0.4 in the hot H2-laden gas, inside the
+# product-form equilibria's positivity bound theta < 0.5; dx = 2 um keeps the cold air's
+# lattice viscosity at 5e-3 (relaxation time 0.64).
+TURB_UNITS = (2e-6, 2e-6 / 1500.0)
+
+
+def turbulence_field(N, u_rms=0.05, k0=4.0, seed=SEED):
+    """Seeded isotropic, solenoidal velocity field on an N^3 periodic box (lattice units):
+    random-phase Fourier synthesis with the energy spectrum E(k) ~ (k/k0)^4 exp(-2 (k/k0)^2)
+    (peak at k = k0), each mode's random complex amplitude projected onto the plane normal
+    to its wave vector (divergence-free) and scaled to sqrt(E(k) / (4 pi k^2)); the real
+    part of the inverse transform, rescaled so the rms of each component, averaged over the
+    three, is u_rms.  Returns float64 arrays (u, v, w) of shape (N, N, N)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k1 = np.fft.fftfreq(N, 1.0 / N)
+    kx, ky, kz = np.meshgrid(k1, k1, k1, indexing="ij", sparse=True)
+    k2 = kx * kx + ky * ky + kz * kz
+    kk = np.sqrt(k2)
+    E = (kk / k0) ** 4 * np.exp(-2.0 * (kk / k0) ** 2)
+    amp = np.where(kk > 0, np.sqrt(E / (4.0 * np.pi * np.where(k2 > 0, k2, 1.0))), 0.0)
+    a = [rng.standard_normal((N, N, N)) + 1j * rng.standard_normal((N, N, N)) for _ in range(3)]
+    kd = (kx * a[0] + ky * a[1] + kz * a[2]) / np.where(k2 > 0, k2, 1.0)
+    vel = []
+    for c, kc in zip(a, (kx, ky, kz)):
+        c -= kc * kd
+        c *= amp
+        vel.append(np.real(np.fft.ifftn(c)))
+    del a, kd
+    rms = math.sqrt(sum(float(np.mean(v * v)) for v in vel) / 3.0)
+    return tuple(v * (u_rms / rms) for v in vel)
+
+
+def turbulent_layer_mc(mech, N=32, i0=0, i1=None, field=None, Y_H2=0.03, T_lo=300.0, T_hi=1500.0, width=None,
+                       u_rms=0.05, k0=4.0, seed=SEED, units=TURB_UNITS):
+    """The x-planes i0 .. i1-1 (ghosts counted; default all N + 2) of a decaying turbulent
+    reacting H2/air layer on an N^3 interior: H2-laden air (mass fraction Y_H2, balance air
+    with O2:N2 = 0.233:0.767 by mass) at T_hi above a tanh interface in y at mid-height
+    (width max(1.5, N/16) cells), air at T_lo below it, p = 1 atm, the other species at mole
+    fraction 1e-8; the velocity field of turbulence_field(N, u_rms, k0, seed) everywhere.
+    Periodic (TYPE_P ghosts) in x and z; TYPE_O_C characteristic outflow ghosts (target
+    pressure 1 atm) on both y faces, overriding the periodic ghosts at the edges.  Every
+    ghost cell carries the fields of its nearest interior cell.  `field` reuses a
+    turbulence_field result across plane ranges."""
+    width = max(1.5, N / 16.0) if width is None else width
+    i1 = N + 2 if i1 is None else i1
+    if field is None:
+        field = turbulence_field(N, u_rms=u_rms, k0=k0, seed=seed)
+    names = mech.species_names()
+    ns = len(names)
+    shape = (i1 - i0, N + 2, N + 2)
+    mix = np.zeros(shape, dtype=MIXTURE_MC)
+    sp = [np.zeros(shape, dtype=SPECIES) for _ in range(ns)]
+    mix["rho"] = 1.0
+    i = np.arange(i0, i1)[:, None, None]
+    j = np.arange(N + 2)[None, :, None]
+    k = np.arange(N + 2)[None, None, :]
+    ty = np.full(shape, TYPE_F, dtype=np.int16)
+    ty[np.broadcast_to((i == 0) | (i == N + 1) | (k == 0) | (k == N + 1), shape)] = TYPE_P
+    ty[np.broadcast_to((j == 0) | (j == N + 1), shape)] = TYPE_O_C
+    mix["type"] = ty
+    # fields of the nearest interior cell
+    ic = np.clip(np.arange(i0, i1), 1, N) - 1
+    jc = np.clip(np.arange(N + 2), 1, N) - 1
+    sel = np.ix_(ic, jc, jc)
+    for name, comp in zip(("u", "v", "w"), field):
+        mix[name] = comp[sel]
+    jj = np.clip(j, 1, N).astype(np.float64)
+    s = 0.5 * (1.0 + np.tanh((jj - 0.5 * (N + 1)) / width))
+    s = np.broadcast_to(s, shape)
+    W = np.array([mech.W[q] for q in range(ns)])
+    Y = np.zeros(shape + (ns,))
+    Y[..., names.index("H2")] = Y_H2 * s
+    air = 1.0 - Y[..., names.index("H2")]
+    Y[..., names.index("O2")] = 0.233 * air
+    Y[..., names.index("N2")] = 0.767 * air
+    X = Y / W
+    X /= X.sum(-1, keepdims=True)
+    for a, n in enumerate(names):
+        if n not in ("H2", "O2", "N2"):
+            X[..., a] = SPECIES_MIN
+    X[..., names.index("H2")] = np.maximum(X[..., names.index("H2")], SPECIES_MIN)
+    X /= X.sum(-1, keepdims=True)
+    T = T_lo + (T_hi - T_lo) * s
+    mix["temp"] = np.float32(T / K_UNIT).astype(np.float64)
+    mix["p"] = p_lattice(ONE_ATM, units)
+    for a in range(ns):
+        sp[a]["X"] = X[..., a]
+    return mix, sp

@@ -266,7 +266,7 @@ def test_surrogate_gains_over_the_integrator():
             launches, ms = lat.kernel_times()
             lat.profile(False)
             assert lat.synchronize() == 0
-            res[name] = (ms[3] + ms[4], hrr, tpk)
+            res[name] = (ms[3] + ms[4] + ms[7], hrr, tpk)
     (t_s, h_s, p_s), (t_p, h_p, p_p) = res["surrogate"], res["plain"]
     print("chemistry ms per 10 steps: surrogate", t_s, "plain", t_p, "heat release", h_s, h_p)
     assert t_s * 3 <= t_p, (t_s, t_p)
