@@ -331,37 +331,48 @@ GAS_HD double conc_pow(double C, double nu) {
     return pow(C, nu);
 }
 
+// Forward and reverse rates of progress (kmol/m^3/s) of reaction r from the factors of
+// rate_factors and the concentrations C[k] (kmol/m^3).
+GAS_HD void rate_of_progress(const Tables &t, const RateT &K, const double *C, int r, double &fwd_out,
+                             double &rev_out) {
+    const lbmgpu_mech &m = t.m;
+    double kf = K.kf[r];
+    double M = 1.0;
+    if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
+        M = 0.0;
+        for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
+    }
+    if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
+        const double Pr = K.k0[r] * M / kf;
+        double F = 1.0;
+        if (m.troe_n[r] >= 3) {
+            const double lFc = K.lFc[r];
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+            F = pow(10.0, lFc / (1.0 + x * x));
+        }
+        kf = kf * (Pr / (1.0 + Pr)) * F;
+        M = 1.0;
+    }
+    double fwd = kf * M, rev = 0.0;
+    for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.nu_reac[r][j]);
+    if (m.reversible[r]) {
+        rev = kf * M * K.er[r];  // kf / Kc
+        for (int j = 0; j < m.n_prod[r]; ++j) rev *= conc_pow(C[m.prod[r][j]], m.nu_prod[r][j]);
+    }
+    fwd_out = fwd;
+    rev_out = rev;
+}
+
 // Net molar production rates wdot[k] (kmol/m^3/s) from the factors of rate_factors and
 // the concentrations C[k] (kmol/m^3).
 GAS_HD void net_production_k(const Tables &t, const RateT &K, const double *C, double *wdot) {
     const lbmgpu_mech &m = t.m;
     for (int k = 0; k < t.ns; ++k) wdot[k] = 0.0;
     for (int r = 0; r < m.n_reactions; ++r) {
-        double kf = K.kf[r];
-        double M = 1.0;
-        if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
-            M = 0.0;
-            for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
-        }
-        if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
-            const double Pr = K.k0[r] * M / kf;
-            double F = 1.0;
-            if (m.troe_n[r] >= 3) {
-                const double lFc = K.lFc[r];
-                const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-                const double lPr = log10(fmax(Pr, 1e-300));
-                const double x = (lPr + c) / (n - 0.14 * (lPr + c));
-                F = pow(10.0, lFc / (1.0 + x * x));
-            }
-            kf = kf * (Pr / (1.0 + Pr)) * F;
-            M = 1.0;
-        }
-        double fwd = kf * M, rev = 0.0;
-        for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.nu_reac[r][j]);
-        if (m.reversible[r]) {
-            rev = kf * M * K.er[r];  // kf / Kc
-            for (int j = 0; j < m.n_prod[r]; ++j) rev *= conc_pow(C[m.prod[r][j]], m.nu_prod[r][j]);
-        }
+        double fwd, rev;
+        rate_of_progress(t, K, C, r, fwd, rev);
         const double q = fwd - rev;
         for (int j = 0; j < m.n_reac[r]; ++j) wdot[m.reac[r][j]] -= m.nu_reac[r][j] * q;
         for (int j = 0; j < m.n_prod[r]; ++j) wdot[m.prod[r][j]] += m.nu_prod[r][j] * q;

@@ -84,14 +84,17 @@ class LbmGpuError(RuntimeError):
         super().__init__(f"{what}: {error_string(code)} ({code})")
 
 
-_lib = None
+# the parity build of the same sources without fused multiply-adds (tests only)
+NOFMA_LIB_PATH = os.path.join(HERE, "liblbmgpu_nofma.so")
+_libs = {}
 
 
-def lib():
-    """Loads liblbmgpu.so (raises OSError when it has not been built)."""
-    global _lib
-    if _lib is None:
-        L = ctypes.CDLL(LIB_PATH)
+def lib(path=None):
+    """Loads liblbmgpu.so, or the library at `path` (raises OSError when it has not been
+    built)."""
+    path = path or LIB_PATH
+    if path not in _libs:
+        L = ctypes.CDLL(path)
         vp = ctypes.c_void_p
         L.lbmgpu_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(vp)]
         for name in ("lbmgpu_destroy", "lbmgpu_init", "lbmgpu_collide_species", "lbmgpu_collide",
@@ -127,8 +130,8 @@ def lib():
         L.lbmgpu_surrogate_stats.argtypes = [vp, ctypes.POINTER(SurrogateReport)]
         L.lbmgpu_error_string.argtypes = [ctypes.c_int]
         L.lbmgpu_error_string.restype = ctypes.c_char_p
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
 def error_string(code):
@@ -173,10 +176,12 @@ class Lattice:
 
     def __init__(self, Nx, Ny, Nz, nu=0.0, gas_const=1.0, gamma=1.4, prtl=0.5, device=0,
                  precision=FP64, dtype=MIXTURE_SC, dt_sim=1, mech=None, species_dtype=None, dx_dt=None,
-                 chem=CHEM_OFF):
+                 chem=CHEM_OFF, library=None):
         """Single component: nu, gas_const, gamma, prtl.  Multicomponent: `mech` (a
         mech.Mech table), `dtype`/`species_dtype` (the MIXTURE and SPECIES records) and
-        `dx_dt` (the arguments of the reference's units.set_m_kg_s(dx, dt))."""
+        `dx_dt` (the arguments of the reference's units.set_m_kg_s(dx, dt)).  `library`: the
+        path of another build of the library (the tests' no-FMA parity build)."""
+        self.L = lib(library)
         d = Desc()
         d.abi_version = ABI_VERSION
         d.device = device
@@ -198,7 +203,7 @@ class Lattice:
         self.species_dtype = species_dtype
         self.shape = (Nx, Ny, Nz)
         self.h = ctypes.c_void_p()
-        _check(lib().lbmgpu_create(ctypes.byref(d), ctypes.byref(self.h)), "lbmgpu_create")
+        _check(self.L.lbmgpu_create(ctypes.byref(d), ctypes.byref(self.h)), "lbmgpu_create")
 
     # -- state transfer ---------------------------------------------------------------
     def _cells_ptr(self, cells, shape=None):
@@ -222,62 +227,62 @@ class Lattice:
     def upload_planes(self, i0, cells, species):
         """Uploads the x-planes i0 .. i0 + cells.shape[0] - 1 (lbmgpu_upload_planes)."""
         shape = (cells.shape[0],) + self.shape[1:]
-        _check(lib().lbmgpu_upload_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
+        _check(self.L.lbmgpu_upload_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
                                           self._species_ptrs(species, shape)), "lbmgpu_upload_planes")
 
     def download_planes(self, i0, cells, species):
         """Downloads the x-planes i0 .. i0 + cells.shape[0] - 1 (lbmgpu_download_planes)."""
         shape = (cells.shape[0],) + self.shape[1:]
-        _check(lib().lbmgpu_download_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
+        _check(self.L.lbmgpu_download_planes(self.h, i0, i0 + shape[0], self._cells_ptr(cells, shape),
                                             self._species_ptrs(species, shape)), "lbmgpu_download_planes")
 
     def upload(self, cells, species=None):
-        _check(lib().lbmgpu_upload(self.h, self._cells_ptr(cells), self._species_ptrs(species)), "lbmgpu_upload")
+        _check(self.L.lbmgpu_upload(self.h, self._cells_ptr(cells), self._species_ptrs(species)), "lbmgpu_upload")
 
     def download(self, cells, species=None):
-        _check(lib().lbmgpu_download(self.h, self._cells_ptr(cells), self._species_ptrs(species)),
+        _check(self.L.lbmgpu_download(self.h, self._cells_ptr(cells), self._species_ptrs(species)),
                "lbmgpu_download")
 
     # -- the reference's phases -------------------------------------------------------
     def init(self):
-        _check(lib().lbmgpu_init(self.h), "lbmgpu_init")
+        _check(self.L.lbmgpu_init(self.h), "lbmgpu_init")
 
     def collide_species(self):
-        return lib().lbmgpu_collide_species(self.h)
+        return self.L.lbmgpu_collide_species(self.h)
 
     def collide(self):
-        _check(lib().lbmgpu_collide(self.h), "lbmgpu_collide")
+        _check(self.L.lbmgpu_collide(self.h), "lbmgpu_collide")
 
     def streaming(self):
-        _check(lib().lbmgpu_streaming(self.h), "lbmgpu_streaming")
+        _check(self.L.lbmgpu_streaming(self.h), "lbmgpu_streaming")
 
     def tms_bc(self):
-        _check(lib().lbmgpu_tms_bc(self.h), "lbmgpu_tms_bc")
+        _check(self.L.lbmgpu_tms_bc(self.h), "lbmgpu_tms_bc")
 
     def calculate_moment(self):
-        _check(lib().lbmgpu_calculate_moment(self.h), "lbmgpu_calculate_moment")
+        _check(self.L.lbmgpu_calculate_moment(self.h), "lbmgpu_calculate_moment")
 
     def step(self, n=1):
-        _check(lib().lbmgpu_step(self.h, n), "lbmgpu_step")
+        _check(self.L.lbmgpu_step(self.h, n), "lbmgpu_step")
 
     def time_steps(self, n):
         """Runs n steps and returns their device time in ms (CUDA events on the handle's
         stream)."""
         ms = ctypes.c_double()
-        _check(lib().lbmgpu_time_steps(self.h, n, ctypes.byref(ms)), "lbmgpu_time_steps")
+        _check(self.L.lbmgpu_time_steps(self.h, n, ctypes.byref(ms)), "lbmgpu_time_steps")
         return ms.value
 
     def synchronize(self):
-        return _check(lib().lbmgpu_synchronize(self.h), "lbmgpu_synchronize")
+        return _check(self.L.lbmgpu_synchronize(self.h), "lbmgpu_synchronize")
 
     def status(self, clear=False):
         f = ctypes.c_uint32()
-        _check(lib().lbmgpu_status(self.h, ctypes.byref(f), int(clear)), "lbmgpu_status")
+        _check(self.L.lbmgpu_status(self.h, ctypes.byref(f), int(clear)), "lbmgpu_status")
         return f.value
 
     # -- timing -------------------------------------------------------------------------
     def profile(self, enable=True):
-        _check(lib().lbmgpu_profile(self.h, int(enable)), "lbmgpu_profile")
+        _check(self.L.lbmgpu_profile(self.h, int(enable)), "lbmgpu_profile")
 
     def kernel_times(self):
         """Per kernel kind (0 collide / population update, 1 stream+boundary+moment
@@ -286,24 +291,24 @@ class Lattice:
         energy-flux terms, 7 stiff chemistry of every cell): launches and device ms."""
         launches = (ctypes.c_long * KERNEL_KINDS)()
         ms = (ctypes.c_double * KERNEL_KINDS)()
-        _check(lib().lbmgpu_kernel_times(self.h, KERNEL_KINDS, launches, ms), "lbmgpu_kernel_times")
+        _check(self.L.lbmgpu_kernel_times(self.h, KERNEL_KINDS, launches, ms), "lbmgpu_kernel_times")
         return list(launches), list(ms)
 
     # -- conserved sums -------------------------------------------------------------------
     def sums(self):
         """FP64 totals over the fluid cells: mass, momentum (3), total energy, then
         (multicomponent) the species masses and the H, O, N, Ar element totals."""
-        k = lib().lbmgpu_sums_count(self.h)
+        k = self.L.lbmgpu_sums_count(self.h)
         _check(k if k < 0 else 0, "lbmgpu_sums_count")
         out = (ctypes.c_double * k)()
-        _check(lib().lbmgpu_sums(self.h, out, k), "lbmgpu_sums")
+        _check(self.L.lbmgpu_sums(self.h, out, k), "lbmgpu_sums")
         return list(out)
 
     # -- chemistry surrogate (CHEM_ROSENBROCK) ------------------------------------------------
     def surrogate_collect(self, enable=True, stride=1, capacity=1 << 20):
         """While enabled, each integrator step writes the (features, targets) of every
         stride-th cell to the device sample set (capacity rows)."""
-        _check(lib().lbmgpu_surrogate_collect(self.h, int(enable), int(stride), int(capacity)),
+        _check(self.L.lbmgpu_surrogate_collect(self.h, int(enable), int(stride), int(capacity)),
                "lbmgpu_surrogate_collect")
 
     def surrogate_load_samples(self, x, y):
@@ -312,7 +317,7 @@ class Lattice:
         x = np.ascontiguousarray(x, dtype=np.float32)
         y = np.ascontiguousarray(y, dtype=np.float32)
         fp = ctypes.POINTER(ctypes.c_float)
-        _check(lib().lbmgpu_surrogate_load_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp), len(x)),
+        _check(self.L.lbmgpu_surrogate_load_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp), len(x)),
                "lbmgpu_surrogate_load_samples")
 
     def surrogate_samples(self, n=None):
@@ -324,7 +329,7 @@ class Lattice:
         y = np.zeros((n, SUR_OUT), np.float32)
         v = np.zeros(n, np.uint8)
         fp = ctypes.POINTER(ctypes.c_float)
-        _check(lib().lbmgpu_surrogate_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp),
+        _check(self.L.lbmgpu_surrogate_samples(self.h, x.ctypes.data_as(fp), y.ctypes.data_as(fp),
                                               v.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), n),
                "lbmgpu_surrogate_samples")
         return x, y, v.astype(bool)
@@ -332,19 +337,19 @@ class Lattice:
     def surrogate_augment(self, n, span_y=1.5, span_t=0.01, y_trace=1e-3, seed=1):
         """Appends n integrator-labelled rows perturbed from random valid sample rows (mass
         fractions below y_trace by exp(U(-span_y, span_y)), T by exp(U(-span_t, span_t)))."""
-        _check(lib().lbmgpu_surrogate_augment(self.h, int(n), float(span_y), float(span_t), float(y_trace), int(seed)),
+        _check(self.L.lbmgpu_surrogate_augment(self.h, int(n), float(span_y), float(span_t), float(y_trace), int(seed)),
                "lbmgpu_surrogate_augment")
 
     def surrogate_train(self, epochs=10, batch=4096, lr=1e-3, seed=1, refit=False):
         """Adam epochs over the sample set (step size lr decaying to 0 along a half cosine);
         returns the last epoch's mean standardised loss."""
         loss = ctypes.c_double()
-        _check(lib().lbmgpu_surrogate_train(self.h, int(epochs), int(batch), float(lr), int(seed), int(refit),
+        _check(self.L.lbmgpu_surrogate_train(self.h, int(epochs), int(batch), float(lr), int(seed), int(refit),
                                             ctypes.byref(loss)), "lbmgpu_surrogate_train")
         return loss.value
 
     def surrogate_enable(self, enable=True, audit_period=100):
-        _check(lib().lbmgpu_surrogate_enable(self.h, int(enable), int(audit_period)), "lbmgpu_surrogate_enable")
+        _check(self.L.lbmgpu_surrogate_enable(self.h, int(enable), int(audit_period)), "lbmgpu_surrogate_enable")
 
     def surrogate_eval(self, x):
         """The network on raw features x (n, 12) -> raw predictions (n, 10)."""
@@ -352,7 +357,7 @@ class Lattice:
         x = np.ascontiguousarray(x, dtype=np.float32)
         y = np.zeros((len(x), SUR_OUT), np.float32)
         fp = ctypes.POINTER(ctypes.c_float)
-        _check(lib().lbmgpu_surrogate_eval(self.h, x.ctypes.data_as(fp), len(x), y.ctypes.data_as(fp)),
+        _check(self.L.lbmgpu_surrogate_eval(self.h, x.ctypes.data_as(fp), len(x), y.ctypes.data_as(fp)),
                "lbmgpu_surrogate_eval")
         return y
 
@@ -361,13 +366,13 @@ class Lattice:
         import numpy as np
         buf = np.zeros(SUR_NPARAMS, np.float32) if values is None else np.ascontiguousarray(values, np.float32).copy()
         fp = ctypes.POINTER(ctypes.c_float)
-        _check(lib().lbmgpu_surrogate_params(self.h, buf.ctypes.data_as(fp), len(buf), int(values is not None)),
+        _check(self.L.lbmgpu_surrogate_params(self.h, buf.ctypes.data_as(fp), len(buf), int(values is not None)),
                "lbmgpu_surrogate_params")
         return buf
 
     def surrogate_stats(self):
         r = SurrogateReport()
-        _check(lib().lbmgpu_surrogate_stats(self.h, ctypes.byref(r)), "lbmgpu_surrogate_stats")
+        _check(self.L.lbmgpu_surrogate_stats(self.h, ctypes.byref(r)), "lbmgpu_surrogate_stats")
         return {k: getattr(r, k) for k, _ in SurrogateReport._fields_}
 
     def diagnostics(self):
@@ -375,27 +380,27 @@ class Lattice:
         enstrophy (sum rho|curl u|^2), energy (sum rho E), hrr (sum of the heat-release
         field), T_max, T_min."""
         out = (ctypes.c_double * DIAG_COUNT)()
-        _check(lib().lbmgpu_diagnostics(self.h, out, DIAG_COUNT), "lbmgpu_diagnostics")
+        _check(self.L.lbmgpu_diagnostics(self.h, out, DIAG_COUNT), "lbmgpu_diagnostics")
         return dict(zip(("kinetic", "enstrophy", "energy", "hrr", "T_max", "T_min"), list(out)))
 
     def sums_noalloc(self, n_out=None):
         """The same totals through lbmgpu_sums_noalloc (fixed device scratch, no
         allocation); n_out defaults to the handle's count."""
-        k = lib().lbmgpu_sums_count(self.h)
+        k = self.L.lbmgpu_sums_count(self.h)
         _check(k if k < 0 else 0, "lbmgpu_sums_count")
         n = k if n_out is None else n_out
         out = (ctypes.c_double * max(n, 1))()
-        _check(lib().lbmgpu_sums_noalloc(self.h, out, n), "lbmgpu_sums_noalloc")
+        _check(self.L.lbmgpu_sums_noalloc(self.h, out, n), "lbmgpu_sums_noalloc")
         return list(out)[:k]
 
     def device_bytes(self):
         b = ctypes.c_size_t()
-        _check(lib().lbmgpu_device_bytes(self.h, ctypes.byref(b)), "lbmgpu_device_bytes")
+        _check(self.L.lbmgpu_device_bytes(self.h, ctypes.byref(b)), "lbmgpu_device_bytes")
         return b.value
 
     def close(self):
         if self.h:
-            lib().lbmgpu_destroy(self.h)
+            self.L.lbmgpu_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __enter__(self):

@@ -341,12 +341,13 @@ def turbulence_field(N, u_rms=0.05, k0=4.0, seed=SEED):
 
 
 def turbulent_layer_mc(mech, N=32, i0=0, i1=None, field=None, Y_H2=0.03, T_lo=300.0, T_hi=1500.0, width=None,
-                       u_rms=0.05, k0=4.0, seed=SEED, units=TURB_UNITS):
+                       u_rms=0.05, k0=4.0, seed=SEED, units=TURB_UNITS, x_trace=SPECIES_MIN):
     """The x-planes i0 .. i1-1 (ghosts counted; default all N + 2) of a decaying turbulent
     reacting H2/air layer on an N^3 interior: H2-laden air (mass fraction Y_H2, balance air
     with O2:N2 = 0.233:0.767 by mass) at T_hi above a tanh interface in y at mid-height
     (width max(1.5, N/16) cells), air at T_lo below it, p = 1 atm, the other species at mole
-    fraction 1e-8; the velocity field of turbulence_field(N, u_rms, k0, seed) everywhere.
+    fraction x_trace (1e-8); the velocity field of turbulence_field(N, u_rms, k0, seed)
+    everywhere.
     Periodic (TYPE_P ghosts) in x and z; TYPE_O_C characteristic outflow ghosts (target
     pressure 1 atm) on both y faces, overriding the periodic ghosts at the edges.  Every
     ghost cell carries the fields of its nearest interior cell.  `field` reuses a
@@ -387,8 +388,8 @@ def turbulent_layer_mc(mech, N=32, i0=0, i1=None, field=None, Y_H2=0.03, T_lo=30
     X /= X.sum(-1, keepdims=True)
     for a, n in enumerate(names):
         if n not in ("H2", "O2", "N2"):
-            X[..., a] = SPECIES_MIN
-    X[..., names.index("H2")] = np.maximum(X[..., names.index("H2")], SPECIES_MIN)
+            X[..., a] = x_trace
+    X[..., names.index("H2")] = np.maximum(X[..., names.index("H2")], x_trace)
     X /= X.sum(-1, keepdims=True)
     T = T_lo + (T_hi - T_lo) * s
     mix["temp"] = np.float32(T / K_UNIT).astype(np.float64)

@@ -31,6 +31,12 @@ double gp_s_R(int k, double T) { return gas::s_R(g_t, k, T); }
 double gp_cp_R(int k, double T) { return gas::cp_R(g_t, k, T); }
 int gp_T_from_u(const double *Y, double u, double T0, double *T) { return gas::T_from_u(g_t, Y, u, T0, 1e-14, 100, *T); }
 void gp_wdot(double T, const double *C, double *w) { gas::net_production(g_t, T, C, w); }
+int gp_n_reactions() { return g_t.m.n_reactions; }
+void gp_rates_of_progress(double T, const double *C, double *qf, double *qr) {
+    gas::RateT K;
+    gas::rate_factors(g_t, T, K);
+    for (int r = 0; r < g_t.m.n_reactions; ++r) gas::rate_of_progress(g_t, K, C, r, qf[r], qr[r]);
+}
 void gp_reactor_rhs(double rho, const double *y, double *F) { gas::reactor_rhs(g_t, rho, y, F); }
 int gp_ros2(double rho, double *Y, double *T, double dt) { return gas::ros2_advance(g_t, rho, Y, *T, dt); }
 }

@@ -16,17 +16,27 @@ PATHS = {False: os.path.join(HERE, "_ref", "libref_mc.so"), True: os.path.join(H
 # -ffast-math -flto); the parity oracle above is built without -ffast-math
 FAST_PATHS = {False: os.path.join(HERE, "_ref", "libref_mc_fast.so"),
               True: os.path.join(HERE, "_ref", "libref_mcr_fast.so")}
+# the oracle without floating-point contraction (no fused multiply-adds)
+NOFMA_PATHS = {False: os.path.join(HERE, "_ref", "libref_mc_nofma.so"),
+               True: os.path.join(HERE, "_ref", "libref_mcr_nofma.so")}
 _libs = {}
 
 
+def _path(reaction, fast):
+    if fast == "nofma":
+        return NOFMA_PATHS[reaction]
+    return (FAST_PATHS if fast else PATHS)[reaction]
+
+
 def available(reaction=False, fast=False):
-    return os.path.exists((FAST_PATHS if fast else PATHS)[reaction])
+    """fast: False (the oracle), True (the reference's -O3 -ffast-math build) or "nofma"."""
+    return os.path.exists(_path(reaction, fast))
 
 
 def lib(reaction=False, fast=False):
     key = (reaction, fast)
     if key not in _libs:
-        L = ctypes.CDLL((FAST_PATHS if fast else PATHS)[reaction])
+        L = ctypes.CDLL(_path(reaction, fast))
         vp = ctypes.c_void_p
         L.ref_mc_set_mech.argtypes = [vp]
         L.ref_mc_set_units.argtypes = [ctypes.c_float, ctypes.c_float]

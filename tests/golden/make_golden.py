@@ -28,6 +28,12 @@ compiled unchanged -- on seeded inputs and records:
 * ``mc_inflow.npz``        10x6x6 mixing layer between a characteristic inflow (TYPE_I_C,
                            inline LODI) and outflow (TYPE_O_C), periodic y and z, REACTION
                            off; fields after 1, 2 and 20 steps.
+* ``mc_flame512[_nofma].npz``  config 3's 512x8x8 reacting channel, 50 steps, and
+  ``mc_inflow32[_nofma].npz``  a 32^3 slab of config 2, 20 steps (make_mc_shapes: sampled
+                           cells and whole-field sums, both builds of the reference);
+* ``mc_chan_nofma.npz``, ``mc_inflow_nofma.npz``  the same two cases run by the reference
+                           built without floating-point contraction (-ffp-contract=off),
+                           fields after 1, 2, 5, 10 and 20 steps.
 """
 import hashlib
 import os
@@ -143,9 +149,11 @@ def kat(seed=cases.SEED, n=64):
     return out
 
 
-def run_ref_mc(mix, sp, m, checkpoints, reaction, pop_cells):
+def run_ref_mc(mix, sp, m, checkpoints, reaction, pop_cells, variant=False):
     NX, NY, NZ = [s_ - 2 for s_ in mix.shape]
-    ref = refmc.RefMC(NX, NY, NZ, m, cases.FLAME_UNITS, cases.MIXTURE_MC, cases.SPECIES, reaction=reaction)
+    refmc.set_threads(1 if variant == "nofma" else (os.cpu_count() or 1), reaction, variant)
+    ref = refmc.RefMC(NX, NY, NZ, m, cases.FLAME_UNITS, cases.MIXTURE_MC, cases.SPECIES, reaction=reaction,
+                      fast=variant)
     ref.cells[...] = mix
     for a in range(len(sp)):
         ref.species[a][...] = sp[a]
@@ -177,11 +185,16 @@ def mc_digest(mix, sp):
 
 
 def main():
-    only = sys.argv[1] if len(sys.argv) > 1 else "all"   # "sc", "mc" or "all"
+    args = [a for i, a in enumerate(sys.argv[1:]) if a != "--reference" and sys.argv[i] != "--reference"]
+    only = args[0] if args else "all"   # "sc", "mc", "mc_nofma" or "all"
     if only in ("all", "sc"):
         make_sc()
     if only in ("all", "mc"):
         make_mc()
+    if only == "mc_nofma":
+        make_mc_nofma()
+    if only in ("all", "mc_shapes"):
+        make_mc_shapes()
     print("fixtures written to", HERE)
 
 
@@ -225,6 +238,67 @@ def make_mc():
         mix, sp = mix_sp
         pc = boundary_cells(mix, 24, 4)
         out = run_ref_mc(mix, sp, m, [1, 2, 20], reaction, pc)
+        out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
+        np.savez_compressed(os.path.join(HERE, name), **out)
+    make_mc_nofma()
+
+
+def make_mc_shapes():
+    """Config 3's 512x8x8 reacting channel (50 steps) and a 32^3 slab of config 2 with its
+    characteristic inflow and outflow (20 steps), each run by the reference built with
+    floating-point contraction (the oracle) and without it (single-threaded): at every
+    checkpoint the fields and species densities of 512 sampled fluid cells (256 next to a
+    boundary, 256 anywhere) and the sums of rho, rhoE and each rho_a over all fluid cells."""
+    m = mechmod.h2_air_9()
+    for name, mix_sp, reaction, cps in (("mc_flame512", cases.flame_channel_mc(m, NX=512, NY=8, NZ=8), True,
+                                         [1, 20, 50]),
+                                        ("mc_inflow32", cases.inflow_layer_mc(m, NX=32, NY=32, NZ=32), False,
+                                         [1, 20])):
+        mix, sp = mix_sp
+        t = mix["type"]
+        fl = np.argwhere(t == cases.TYPE_F)
+        rng = np.random.Generator(np.random.PCG64(7))
+        near = np.array([bool(np.any((t[i - 1:i + 2, j - 1:j + 2, k - 1:k + 2] != cases.TYPE_F)
+                                     & (t[i - 1:i + 2, j - 1:j + 2, k - 1:k + 2] != cases.TYPE_P)))
+                         for (i, j, k) in fl])
+        pick = np.concatenate([rng.choice(np.flatnonzero(near), 256, replace=False),
+                               rng.choice(len(fl), 256, replace=False)])
+        cells = fl[pick]
+        idx = tuple(cells.T)
+        mask = t == cases.TYPE_F
+        for variant, suffix in ((False, ""), ("nofma", "_nofma")):
+            NX, NY, NZ = [s_ - 2 for s_ in mix.shape]
+            refmc.set_threads(1 if variant == "nofma" else (os.cpu_count() or 1), reaction, variant)
+            ref = refmc.RefMC(NX, NY, NZ, m, cases.FLAME_UNITS, cases.MIXTURE_MC, cases.SPECIES, reaction=reaction,
+                              fast=variant)
+            ref.cells[...] = mix
+            for a in range(len(sp)):
+                ref.species[a][...] = sp[a]
+            ref.init()
+            out = {"input_sha256": mc_digest(mix, sp), "cells": cells, "checkpoints": np.array(cps)}
+            done = 0
+            for cp in cps:
+                ref.loop(cp - done)
+                done = cp
+                for f in MC_FIELDS:
+                    out[f"{f}_{cp}"] = np.ascontiguousarray(ref.cells[f][idx])
+                out[f"sp_rho_{cp}"] = np.stack([ref.species[a]["rho"][idx] for a in range(len(sp))])
+                out[f"sum_rho_{cp}"] = ref.cells["rho"][mask].sum()
+                out[f"sum_rhoe_{cp}"] = ref.cells["rhoe"][mask].sum()
+                out[f"sum_sp_rho_{cp}"] = np.array([ref.species[a]["rho"][mask].sum() for a in range(len(sp))])
+            ref.close()
+            np.savez_compressed(os.path.join(HERE, f"{name}{suffix}.npz"), **out)
+
+
+def make_mc_nofma():
+    """The boundary cases run by the reference built without floating-point contraction (no
+    fused multiply-adds, oracle/_ref/libref_mc*_nofma.so), single-threaded."""
+    m = mechmod.h2_air_9()
+    for name, mix_sp, reaction in (("mc_chan_nofma.npz", cases.flame_channel_mc(m, NX=10, NY=6, NZ=4), True),
+                                   ("mc_inflow_nofma.npz", cases.inflow_layer_mc(m, NX=10, NY=6, NZ=6), False)):
+        mix, sp = mix_sp
+        pc = boundary_cells(mix, 24, 4)
+        out = run_ref_mc(mix, sp, m, [1, 2, 5, 10, 20], reaction, pc, variant="nofma")
         out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
         np.savez_compressed(os.path.join(HERE, name), **out)
 

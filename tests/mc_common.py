@@ -41,11 +41,40 @@ def rel(got, want, scale=None):
     return float(np.max(np.abs(got - want)) / scale)
 
 
-def build_host_lib(tmpdir):
-    out = os.path.join(str(tmpdir), "libmchost.so")
-    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC,
-                    os.path.join(ROOT, "tests", "host", "mc_host.cpp"), "-o", out], check=True)
+def build_host_lib(tmpdir, contract=True):
+    """The host build of the per-cell functions; contract=False compiles it without
+    floating-point contraction (no fused multiply-adds), like the no-FMA reference."""
+    out = os.path.join(str(tmpdir), "libmchost.so" if contract else "libmchost_nofma.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC]
+                   + ([] if contract else ["-ffp-contract=off"])
+                   + [os.path.join(ROOT, "tests", "host", "mc_host.cpp"), "-o", out], check=True)
     return ctypes.CDLL(out)
+
+
+def bc_errors(R, gold, cp, fl, reaction):
+    """Largest relative differences of the record R (host or device planes) from a fixture's
+    fields after cp steps, over the fluid cells fl: rho, T, p, rhoE, velocity (against the
+    largest velocity component), every species density, and HRR when reacting."""
+    e = {}
+    for q, k in ((0, "rho"), (4, "temp"), (5, "p"), (6, "rhoe")):
+        e[k] = rel(R[q][fl], gold[f"{k}_{cp}"].reshape(-1)[fl])
+    vs = max(np.abs(gold[f"{k}_{cp}"].reshape(-1)[fl]).max() for k in "uvw")
+    for q, k in ((1, "u"), (2, "v"), (3, "w")):
+        e[k] = rel(R[q][fl], gold[f"{k}_{cp}"].reshape(-1)[fl], vs)
+    e["rho_a"] = max(rel(R[SP0 + 8 * a][fl], gold[f"sp_rho_{cp}"][a].reshape(-1)[fl]) for a in range(NS))
+    if reaction:
+        e["HRR"] = rel(R[13][fl], gold[f"HRR_{cp}"].reshape(-1)[fl])
+    return e
+
+
+def fixture_drift(gold_a, gold_b, cp, fl):
+    """The same differences between two fixtures of one case (two builds of the reference)."""
+    R = np.zeros((NREC, fl.size))
+    for q, k in ((0, "rho"), (1, "u"), (2, "v"), (3, "w"), (4, "temp"), (5, "p"), (6, "rhoe")):
+        R[q] = gold_a[f"{k}_{cp}"].reshape(-1)
+    for a in range(NS):
+        R[SP0 + 8 * a] = gold_a[f"sp_rho_{cp}"][a].reshape(-1)
+    return max(bc_errors(R, gold_b, cp, fl, False).values())
 
 
 def soa_state(mix, sp):

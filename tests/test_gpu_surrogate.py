@@ -231,23 +231,25 @@ def test_surrogate_augment_rows_are_integrator_labelled(tmp_path):
 
 def test_surrogate_gains_over_the_integrator():
     """What the trained network gains over the method without it, on a reacting channel
-    (130x34x34 with ghosts: outflow ends, TMS walls): from the same state, 10 steps with the
-    surrogate (1 % audit) and 10 steps of plain ROS2.  The chemistry kernels (collision
-    parameters + the surrogate's features, network and integrator list) take at most a
+    (130x34x34 with ghosts: outflow ends, TMS walls), trained on 40 integrator steps: from
+    the same state, 10 steps with the
+    surrogate (1 % audit) and 10 steps of plain ROS2.  The chemistry kernels (the
+    surrogate's features, network, use of the prediction and integrator list, against the
+    integrator's kernel; the transport kernel both share is not counted) take at most a
     third of the integrator's time per step, while the heat release integrated over cells
-    and steps and the peak temperature stay within 2 % and 0.1 % of the integrator's."""
+    and steps and the peak temperature stay within 1 % and 0.1 % of the integrator's."""
     m = mech.h2_air_9()
     mix, sp = W.flame_channel_mc(m, NX=128, NY=32, NZ=32)
     with lbmgpu.Lattice(*mix.shape, mech=m, dtype=W.MIXTURE_MC, species_dtype=W.SPECIES, dx_dt=W.FLAME_UNITS,
                         chem=lbmgpu.CHEM_ROSENBROCK) as lat:
         lat.upload(mix, sp)
         lat.init()
-        lat.surrogate_collect(True, stride=4, capacity=mix.size * 20 // 4 + 20)
-        lat.step(20)
+        lat.surrogate_collect(True, stride=4, capacity=mix.size * 40 // 4 + 40)
+        lat.step(40)
         assert lat.synchronize() == 0
         lat.surrogate_collect(False)
         lat.surrogate_augment(lat.surrogate_stats()["samples"] // 2, seed=5)
-        lat.surrogate_train(epochs=6, batch=4096, lr=2e-3, seed=5)
+        lat.surrogate_train(epochs=16, batch=4096, lr=2e-3, seed=5)
         c0, s0 = mix.copy(), [a.copy() for a in sp]
         lat.download(c0, s0)
         res = {}
@@ -266,11 +268,11 @@ def test_surrogate_gains_over_the_integrator():
             launches, ms = lat.kernel_times()
             lat.profile(False)
             assert lat.synchronize() == 0
-            res[name] = (ms[3] + ms[4] + ms[7], hrr, tpk)
+            res[name] = (ms[4] + ms[7], hrr, tpk)  # chemistry kernels; transport (3) is shared
     (t_s, h_s, p_s), (t_p, h_p, p_p) = res["surrogate"], res["plain"]
     print("chemistry ms per 10 steps: surrogate", t_s, "plain", t_p, "heat release", h_s, h_p)
     assert t_s * 3 <= t_p, (t_s, t_p)
-    assert abs(h_s - h_p) <= 0.02 * abs(h_p), (h_s, h_p)
+    assert abs(h_s - h_p) <= 0.01 * abs(h_p), (h_s, h_p)
     assert abs(p_s - p_p) <= 1e-3 * p_p, (p_s, p_p)
 
 

@@ -146,6 +146,54 @@ def test_host_boundary_cells_match_reference(hostlib, fixture):
             assert rel(R[13][fl], gold[f"HRR_{cp}"].reshape(-1)[fl]) < max(tol, 1e-10), cp
 
 
+@pytest.fixture(scope="module")
+def hostlib_nofma(tmp_path_factory):
+    return build_host_lib(tmp_path_factory.mktemp("mchost_nofma"), contract=False)
+
+
+@pytest.mark.parametrize("fixture", ["mc_chan.npz", "mc_inflow.npz"])
+def test_host_boundary_cells_match_reference_without_fma(hostlib_nofma, fixture):
+    """The boundary cases with floating-point contraction off on both sides: the per-cell
+    functions (host build, -ffp-contract=off) against the reference's own solver built the
+    same way (mc_*_nofma.npz) agree to 1e-12 through 20 steps -- the NSCBC outflow, the
+    inline LODI inflow, the TMS walls and the reacting cells are the reference's formulas
+    operation for operation.  With contraction on, the two sides place their fused
+    multiply-adds differently and drift apart exactly as two builds of the reference do
+    (next test)."""
+    from mc_common import bc_errors
+    m, mix, sp, reaction = bc_case(fixture)
+    gold = np.load(os.path.join(GOLDEN, fixture.replace(".npz", "_nofma.npz")))
+    assert digest(mix, sp) == str(gold["input_sha256"])
+    fl = (mix["type"] == 0).reshape(-1)
+    for cp in (1, 2, 5, 10, 20):
+        R, st = host_run(hostlib_nofma, m, mix, sp, reaction, cp)
+        assert st == 0
+        e = bc_errors(R, gold, cp, fl, reaction)
+        assert max(e.values()) < 1e-12, (cp, e)
+
+
+@pytest.mark.parametrize("fixture", ["mc_chan.npz", "mc_inflow.npz"])
+def test_reference_boundary_drift_bounds_the_tolerance(hostlib, fixture):
+    """The reference against itself: its solver built with and without floating-point
+    contraction (mc_*.npz vs mc_*_nofma.npz, same inputs) agrees to 1e-14 after 2 steps and
+    then drifts apart -- the energy collision's upwind switch on near-zero diffusion
+    velocities (src/lbm-collision.cpp:282-284) amplifies last-bit differences -- to 4e-7
+    (channel) and 8e-6 (inflow) by step 20.  The host build with contraction drifts from
+    the contracted reference by no more than that, and BC_TOL[20] sits above it."""
+    from mc_common import bc_errors, fixture_drift
+    m, mix, sp, reaction = bc_case(fixture)
+    g_fma = np.load(os.path.join(GOLDEN, fixture))
+    g_off = np.load(os.path.join(GOLDEN, fixture.replace(".npz", "_nofma.npz")))
+    fl = (mix["type"] == 0).reshape(-1)
+    assert fixture_drift(g_fma, g_off, 2, fl) < 1e-13
+    drift = fixture_drift(g_fma, g_off, 20, fl)
+    assert 1e-8 < drift < BC_TOL[20], drift
+    R, st = host_run(hostlib, m, mix, sp, reaction, 20)
+    assert st == 0
+    e = max(bc_errors(R, g_fma, 20, fl, False).values())
+    assert e <= 2.0 * drift + 1e-12, (e, drift)
+
+
 @pytest.mark.parametrize("fixture", ["mc_chan.npz", "mc_inflow.npz"])
 def test_host_fp32_storage_with_boundaries(hostlib, fixture):
     """FP32 population storage (incl. the boundary cells' kept populations) against FP64
