@@ -50,7 +50,7 @@ BYTES_STREAM_FP64 = 54 * 8 + 6 * 8       # 480
 BYTES_STEP_FP64 = 2 * 54 * 8             # 864: one read + one write of the populations
 OUTPUT_EVERY = 10
 # config 4's case: rms velocity (lattice units), hot-side temperature (K), dx (m), dx/dt (m/s)
-TURB_DEFAULTS = {"urms": 0.05, "t_hot": 1500.0, "dx": 2e-6, "dxdt": 1500.0}
+TURB_DEFAULTS = {"urms": 0.02, "t_hot": 1500.0, "dx": 2e-6, "dxdt": 4000.0}
 
 
 def parse():

@@ -169,6 +169,34 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos);
 int lbmgpu_upload_planes(lbmgpu_t *h, int i0, int i1, const void *mixture_aos, const void *const *species_aos);
 int lbmgpu_download_planes(lbmgpu_t *h, int i0, int i1, void *mixture_aos, void *const *species_aos);
 
+/* ---- slab decomposition along x (one slab per GPU) --------------------------------
+ * No counterpart in the reference, which runs on one host (OpenMP).  A slab is an LBM
+ * lattice of its own whose x ghost planes may be marked as halos: each holds the
+ * neighbouring slab's edge plane (where the decomposed domain is periodic in x, the first
+ * and the last slab are neighbours).  Cells of a halo plane are never updated by this
+ * handle; no periodic wrap runs through a halo; the boundary formulas use nx_global (the
+ * whole domain's Nx, ghosts included) as the domain length along x.  Two exchanges per
+ * time step keep the halos as the single domain would see those planes:
+ *   LBMGPU_HALO_POPULATIONS  after lbmgpu_collide and before lbmgpu_calculate_moment: the
+ *       post-collision populations that stream across the face (9 directions per
+ *       population set);
+ *   LBMGPU_HALO_RECORD  between time steps (after calculate_moment, before the next
+ *       Collide): the whole per-cell record of the edge plane.
+ * lbmgpu_halo_pack(face 0) writes this slab's first plane for the lower neighbour, whose
+ * lbmgpu_halo_unpack(face 1) reads it; face 1 writes the last plane for the upper
+ * neighbour's face 0.  Buffers are device memory of lbmgpu_halo_bytes bytes (FP64 values,
+ * populations decoded, so slabs in the FP32 mode need not share a shift); both calls are
+ * enqueued on the handle's stream, so the caller synchronises before handing a buffer to
+ * its transport (NCCL send/recv, a peer copy) and after receiving.  lbmgpu_step runs no
+ * exchange: slabs step through the phase calls.  Multicomponent handles only;
+ * lbmgpu_set_halo takes effect at the next upload (the state must be uploaded again). */
+#define LBMGPU_HALO_POPULATIONS 0
+#define LBMGPU_HALO_RECORD 1
+int lbmgpu_set_halo(lbmgpu_t *h, int lo, int hi, int nx_global);
+int lbmgpu_halo_bytes(lbmgpu_t *h, int what, size_t *bytes);
+int lbmgpu_halo_pack(lbmgpu_t *h, int face, int what, void *dev_buf);
+int lbmgpu_halo_unpack(lbmgpu_t *h, int face, int what, const void *dev_buf);
+
 /* The base units units.set_m_kg_s(dx, dt) sets (src/headers/units.hpp:32-44), with its
  * float rounding: out = {m, kg, s, K}. */
 int lbmgpu_units_from_dx_dt(float dx, float dt, float *out4);

@@ -32,6 +32,7 @@ struct DiagSrc {
     const uint8_t *cflag;
     long ncell, si, sj;
     int Nx, Ny, Nz, ns;
+    int halo_lo, halo_hi;  // x halo planes of a slab (lbmgpu_set_halo)
     double cv;  // single component: R / (gamma - 1)
 };
 
@@ -56,6 +57,8 @@ __device__ __forceinline__ void cell_diag(const DiagSrc &S, long n, double *v) {
     cell_ijk(n, S.si, S.sj, i, j, k);
     int ia, ib, ja, jb, ka, kb;
     wrap_nb(i, S.Nx, ib, ia);
+    if (i == 1 && S.halo_lo) ib = 0;  // an x halo plane holds the neighbouring slab's cells
+    if (i == S.Nx - 2 && S.halo_hi) ia = S.Nx - 1;
     wrap_nb(j, S.Ny, jb, ja);
     wrap_nb(k, S.Nz, kb, ka);
     auto at = [&](int plane, int ii, int jj, int kk) { return R[plane * nc + (long)ii * S.si + (long)jj * S.sj + kk]; };
@@ -138,6 +141,8 @@ int lbmgpu_diagnostics(lbmgpu_t *h, double *out, int n_out) {
     S.cflag = h->cflag;
     S.ncell = h->g.ncell;
     S.Nx = h->g.Nx;
+    S.halo_lo = h->halo_lo;
+    S.halo_hi = h->halo_hi;
     S.Ny = h->g.Ny;
     S.Nz = h->g.Nz;
     S.sj = h->g.sj;

@@ -198,6 +198,10 @@ inline double binary_diff_kt(const Tables &t, int k, int j, double T, double P) 
 
 // ---- transport: fitted (per cell) --------------------------------------------------
 GAS_HD double fit_eval(const double *c, double x) { return c[0] + x * (c[1] + x * (c[2] + x * (c[3] + x * c[4]))); }
+// the same polynomial in FP32 arithmetic (the FP32 storage mode's transport)
+GAS_HD float fit_eval_f(const double *c, float x) {
+    return (float)c[0] + x * ((float)c[1] + x * ((float)c[2] + x * ((float)c[3] + x * (float)c[4])));
+}
 GAS_HD double lnT_x(double T) { return log(T) - kFitX0; }
 GAS_HD double species_visc(const Tables &t, int k, double T) { return exp(fit_eval(t.fit_visc[k], lnT_x(T))); }
 GAS_HD double species_visc_x(const Tables &t, int k, double x) { return exp(fit_eval(t.fit_visc[k], x)); }

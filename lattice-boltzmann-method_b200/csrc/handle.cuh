@@ -97,6 +97,8 @@ struct lbmgpu {
     std::vector<int8_t> htype;
     std::vector<char> plane_have;
     int planes_have = 0;
+    // slab decomposition along x (lbmgpu_set_halo): halo planes and the global x length
+    int halo_lo = 0, halo_hi = 0, nx_glob = 0;
 };
 
 namespace lbmh {
@@ -161,6 +163,7 @@ int mc_setup(lbmgpu *h);
 int mc_upload(lbmgpu *h, const void *mix, const void *const *species);
 int mc_download(lbmgpu *h, void *mix, void *const *species);
 int mc_upload_planes(lbmgpu *h, int i0, int i1, const void *mix, const void *const *species);
+int mc_halo(lbmgpu *h, int face, int what, double *buf, bool pack);
 int mc_download_planes(lbmgpu *h, int i0, int i1, void *mix, void *const *species);
 int mc_init(lbmgpu *h);
 int mc_launch_collide(lbmgpu *h);

@@ -20,6 +20,7 @@
 #include "handle.cuh"
 #include "sc_kernels.cuh"
 #include "sums.cuh"
+#include "halo.cuh"
 
 using namespace lbm;
 using lbmh::MixOff;
@@ -661,6 +662,45 @@ int lbmgpu_download_planes(lbmgpu_t *h, int i0, int i1, void *mixture_aos, void 
     if (!h->have_state) return LBMGPU_E_STATE;
     if (h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
     return lbmh::mc_download_planes(h, i0, i1, mixture_aos, species_aos);
+}
+
+int lbmgpu_set_halo(lbmgpu_t *h, int lo, int hi, int nx_global) {
+    if (!h) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    if (nx_global < h->g.Nx || (lo != 0 && lo != 1) || (hi != 0 && hi != 1)) return LBMGPU_E_ARG;
+    h->halo_lo = lo;
+    h->halo_hi = hi;
+    h->nx_glob = nx_global;
+    h->have_state = false;  // the classification of the cells changes: upload again
+    h->planes_have = 0;
+    std::fill(h->plane_have.begin(), h->plane_have.end(), 0);
+    return LBMGPU_OK;
+}
+
+int lbmgpu_halo_bytes(lbmgpu_t *h, int what, size_t *bytes) {
+    if (!h || !bytes || (what != LBMGPU_HALO_POPULATIONS && what != LBMGPU_HALO_RECORD)) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    *bytes = (size_t)lbm::halo_values(what, h->ns) * h->g.Ny * h->g.Nz * sizeof(double);
+    return LBMGPU_OK;
+}
+
+static int halo_call(lbmgpu_t *h, int face, int what, const void *buf, bool pack) {
+    if (!h || !buf || (face != 0 && face != 1)) return LBMGPU_E_ARG;
+    if (what != LBMGPU_HALO_POPULATIONS && what != LBMGPU_HALO_RECORD) return LBMGPU_E_ARG;
+    if (h->ns == 0) return LBMGPU_E_UNSUPPORTED;
+    if (!h->have_state) return LBMGPU_E_STATE;
+    if (!pack && !(face == 0 ? h->halo_lo : h->halo_hi)) return LBMGPU_E_ARG;  // no halo on that face
+    // populations between Collide and calculate_moment, the record between steps
+    const bool collided = h->phase == lbmh::PH_COLLIDED || h->phase == lbmh::PH_STREAMED || h->phase == lbmh::PH_BC;
+    if (what == LBMGPU_HALO_POPULATIONS ? !collided : h->phase != lbmh::PH_BOUNDARY) return LBMGPU_E_PHASE;
+    CK(cudaSetDevice(h->d.device));
+    return lbmh::mc_halo(h, face, what, static_cast<double *>(const_cast<void *>(buf)), pack);
+}
+
+int lbmgpu_halo_pack(lbmgpu_t *h, int face, int what, void *dev_buf) { return halo_call(h, face, what, dev_buf, true); }
+
+int lbmgpu_halo_unpack(lbmgpu_t *h, int face, int what, const void *dev_buf) {
+    return halo_call(h, face, what, dev_buf, false);
 }
 
 int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos) {

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 
+#include "halo.cuh"
 #include "handle.cuh"
 #include "mc_bc.cuh"
 #include "mc_cell.cuh"
@@ -36,8 +37,10 @@ using namespace lbmh;
 constexpr int NS9 = 9;
 
 // collision parameters of every fluid cell, one instance per chemistry mode
+// FP32 storage: the transport runs in FP32, and four blocks per SM (at most 128 registers)
+// keep more cells in flight than the FP64 instance's register budget allows
 template <int NS, int CHEM, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_props(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_mc_props(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     mc_props_cell<NS, CHEM>(A, n);
@@ -319,6 +322,9 @@ template <typename S>
 McArgsT<S, double> base_args(lbmgpu *h) {
     McArgsT<S, double> A{};
     A.Nx = h->g.Nx;
+    A.halo_lo = h->halo_lo;
+    A.halo_hi = h->halo_hi;
+    A.Nx_glob = h->nx_glob > 0 ? h->nx_glob : h->g.Nx;
     A.Ny = h->g.Ny;
     A.Nz = h->g.Nz;
     A.ncell = h->g.ncell;
@@ -529,9 +535,48 @@ int stream_t(lbmgpu *h) {
     return 0;
 }
 
+// Slab faces (halo.cuh): one thread per cell of the face plane.
+template <int NS, typename S>
+__global__ void k_halo_pack(McArgsT<S, double> A, const S *pop, const double *rec, int face, int what,
+                            double *__restrict__ buf) {
+    const long jk = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (jk >= (long)A.Ny * A.Nz) return;
+    halo_pack_cell<NS>(A, pop, rec, face, what, jk, buf);
+}
+template <int NS, typename S>
+__global__ void k_halo_unpack(McArgsT<S, double> A, S *pop, double *rec, int face, int what,
+                              const double *__restrict__ buf) {
+    const long jk = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (jk >= (long)A.Ny * A.Nz) return;
+    halo_unpack_cell<NS>(A, pop, rec, face, what, jk, buf);
+}
+
+// populations: the post-collision buffer the coming stream reads (between Collide and
+// calculate_moment); record: the current step's record (between steps)
+template <typename S>
+int halo_t(lbmgpu *h, int face, int what, double *buf, bool pack) {
+    McArgsT<S, double> A = base_args<S>(h);
+    S *pop = popb<S>(h, 1 - h->cur);
+    double *rec = h->mom[h->cur];
+    const long plane = (long)h->g.Ny * h->g.Nz;
+    EvPair ep{};
+    ev_begin(h, K_OTHER, ep);
+    if (pack)
+        k_halo_pack<NS9, S><<<grid_for(plane), kBlock, 0, h->stream>>>(A, pop, rec, face, what, buf);
+    else
+        k_halo_unpack<NS9, S><<<grid_for(plane), kBlock, 0, h->stream>>>(A, pop, rec, face, what, buf);
+    ev_end(h, ep);
+    CK(cudaGetLastError());
+    return 0;
+}
+
 }  // namespace
 
 namespace lbmh {
+
+int mc_halo(lbmgpu *h, int face, int what, double *buf, bool pack) {
+    return h->fp32 ? halo_t<float>(h, face, what, buf, pack) : halo_t<double>(h, face, what, buf, pack);
+}
 
 int mc_setup(lbmgpu *h) {
     const lbmgpu_desc &d = h->d;
@@ -614,6 +659,8 @@ static int mc_finish_upload(lbmgpu *h) {
             for (int k = 0; k < g.Nz; ++k) {
                 const long n = (long)i * g.si + (long)j * g.sj + k;
                 if (ty[n] != T_F) continue;
+                // a halo plane holds the neighbouring slab's cells: never updated here
+                if ((i == 0 && h->halo_lo) || (i == g.Nx - 1 && h->halo_hi)) continue;
                 if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
                     return LBMGPU_E_ARG;
                 uint8_t c = CF_FLUID;

@@ -164,7 +164,7 @@ MC_HD void mc_nscbc_outflow(const AT &A, int i, int j, int k, int idir, int isig
     const gas::Tables &t = *A.tab;
     const long n = mc_idx(A, i, j, k);
     const McFields c0 = mc_fields(A, n);
-    const int Nax[3] = {A.Nx, A.Ny, A.Nz};
+    const int Nax[3] = {A.Nx_glob, A.Ny, A.Nz};  // the domain's lengths (x: the whole decomposed domain)
     const int ijk[3] = {i, j, k};
     // derivatives: [axis][p, u, v, w, rho]
     double D[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
@@ -280,7 +280,7 @@ MC_HD void mc_lodi_inflow(const AT &A, int i, int j, int k, int l_if, double &rh
     for (int a = 0; a < NS; ++a)
         dY[a] = mc_fd_uw(rec(A, A.rec_cur, rs(a, RS_RHO), n) / c0.rho, rec(A, A.rec_cur, rs(a, RS_RHO), m1) / c1.rho,
                          cd);
-    const int Nd = d == 0 ? A.Nx : (d == 1 ? A.Ny : A.Nz);
+    const int Nd = d == 0 ? A.Nx_glob : (d == 1 ? A.Ny : A.Nz);
     const double rho = c0.rho, un = c0.u[d];
     // the two tangential axes in the reference's order per branch: x -> (y, z), y -> (z, x),
     // z -> (x, y)
@@ -391,7 +391,7 @@ MC_HDN void mc_special_cell(const AT &A, long n, long b) {
                 czp = -czp;
                 kp = k;
             }
-            ip = ((ip - 1 + (A.Nx - 2)) % (A.Nx - 2)) + 1;
+            if (!((ip == 0 && A.halo_lo) || (ip == A.Nx - 1 && A.halo_hi))) ip = ((ip - 1 + (A.Nx - 2)) % (A.Nx - 2)) + 1;
             jp = ((jp - 1 + (A.Ny - 2)) % (A.Ny - 2)) + 1;
             kp = ((kp - 1 + (A.Nz - 2)) % (A.Nz - 2)) + 1;
             int lp = l;
@@ -402,7 +402,7 @@ MC_HDN void mc_special_cell(const AT &A, long n, long b) {
         } else if (tn == T_O || tn == T_O_C || tn == T_I || tn == T_I_C) {  // kept
             for (int a = 0; a <= NS; ++a) f[a][l] = ldpop_b(A, A.bst_cur, 27 * a + l, b);
         } else {  // periodic wrap through the ghost layer
-            if (in == 0) in = A.Nx - 2; else if (in == A.Nx - 1) in = 1;
+            if (in == 0 && !A.halo_lo) in = A.Nx - 2; else if (in == A.Nx - 1 && !A.halo_hi) in = 1;
             if (jn == 0) jn = A.Ny - 2; else if (jn == A.Ny - 1) jn = 1;
             if (kn == 0) kn = A.Nz - 2; else if (kn == A.Nz - 1) kn = 1;
             const long src = mc_idx(A, in, jn, kn);

@@ -58,6 +58,10 @@ struct McArgsT {
     int Nx, Ny, Nz;
     long ncell, sj, si;
     int ns, dt, chem;
+    // slab decomposition along x: the low / high x ghost plane is a halo holding the
+    // neighbouring slab's cells (no periodic wrap through it), and the domain's global x
+    // length with ghosts, for the boundary formulas' domain lengths
+    int halo_lo, halo_hi, Nx_glob;
     UnitsF U;
     const gas::Tables *tab;
     const int8_t *type;
@@ -161,7 +165,8 @@ MC_HD double mc_fd_fuw(double sl, double sc, double sr, double vel, int tl, int 
 }
 
 // Periodic pull sources of a cell with no boundary neighbour (src/lbm-streaming.cpp:88-117):
-// per axis the upstream coordinate for c = 0, +1, -1 with the reference's wrap.
+// per axis the upstream coordinate for c = 0, +1, -1 with the reference's wrap (none through
+// an x halo plane, which holds the neighbouring slab's cells).
 struct McPull {
     long X[3], Y[3], Z[3];
 };
@@ -169,7 +174,8 @@ template <class AT>
 MC_HD void mc_pull(const AT &A, long n, McPull &p) {
     int i, j, k;
     cell_ijk(n, A.si, A.sj, i, j, k);
-    const int im = (i - 1 == 0) ? A.Nx - 2 : i - 1, ip = (i + 1 == A.Nx - 1) ? 1 : i + 1;
+    const int im = (i - 1 == 0 && !A.halo_lo) ? A.Nx - 2 : i - 1;
+    const int ip = (i + 1 == A.Nx - 1 && !A.halo_hi) ? 1 : i + 1;
     const int jm = (j - 1 == 0) ? A.Ny - 2 : j - 1, jp = (j + 1 == A.Ny - 1) ? 1 : j + 1;
     const int km = (k - 1 == 0) ? A.Nz - 2 : k - 1, kp = (k + 1 == A.Nz - 1) ? 1 : k + 1;
     p.X[0] = (long)i * A.si;
@@ -590,66 +596,17 @@ MC_HD void mc_chem_state(const AT &A, long n, double &rho, double *rho_a, double
     P_si = rho_si * gas::kR * T_si / W;
 }
 
-template <int NS, int CHEM, class AT>
-MC_HDN void mc_props_cell(const AT &A, long n) {
+// The transport part of the collision parameters (lbm-collision.cpp:402-471 species rates and
+// Maxwell-Stefan force, :231-316 energy rates) in FP64, the reference's arithmetic and order
+// (the FP64 storage mode, bit-faithful).
+template <int NS, class AT>
+MC_HDN void mc_transport_f64(const AT &A, long n, double p, const double *rho_a, const double (*ua)[3],
+                             const double *Xs, const double *Y, const double *X, double W, double T_si, double P_si,
+                             double Uint) {
     const gas::Tables &t = *A.tab;
-    const typename AT::R *Rc = A.rec_cur;
     double *Pr = A.props;
     auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
-    const double rho = rec(A, Rc, RM_RHO, n);
-    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
-    const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n), rhoe = rec(A, Rc, RM_RHOE, n);
-    double rho_a[NS], ua[NS][3], Xs[NS];
-    for (int a = 0; a < NS; ++a) {
-        rho_a[a] = rec(A, Rc, rs(a, RS_RHO), n);
-        for (int d = 0; d < 3; ++d) ua[a][d] = rec(A, Rc, rs(a, RS_UX + d), n);
-        Xs[a] = rec(A, Rc, rs(a, RS_X), n);
-    }
-    // Cantera state (lbm-collision.cpp:364-367 and :236-238)
-    double Yr[NS], Y[NS], X[NS];
-    for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] / rho;
-    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
-    const double T_si = si_temp(A.U, (float)Tl);
-    const double rho_si = si_rho(A.U, (float)rho);
-    const double P_si = rho_si * gas::kR * T_si / W;
     const double dt = A.dt;
-
-    // internal energy without the species kinetic energy (lbm-collision.cpp:260-263, 373-376)
-    double Uint = rhoe / rho;
-    for (int a = 0; a < NS; ++a)
-        Uint = Uint - 0.5 * rho_a[a] / rho * (ua[a][0] * ua[a][0] + ua[a][1] * ua[a][1] + ua[a][2] * ua[a][2]);
-
-    // -- chemistry: two explicit half steps with T from (u, v) in between (lbm-collision.cpp:370-399)
-    if (CHEM == CHEM_REF_EXPLICIT) {
-        double drho[NS];
-        for (int a = 0; a < NS; ++a) drho[a] = 0.0;
-        double Tc = T_si, rc = rho_si, Yc[NS], Xc[NS];
-        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
-        for (int sub = 0; sub < 2; ++sub) {
-            double C[gas::MAXS], wd[gas::MAXS];
-            for (int a = 0; a < NS; ++a) C[a] = rc * Yc[a] / t.m.W[a];
-            gas::net_production(t, Tc, C, wd);
-            for (int a = 0; a < NS; ++a) drho[a] += dt / 2.0 * (double)u_rho_dot(A.U, (float)(wd[a] * t.m.W[a]));
-            double yy[NS];
-            for (int a = 0; a < NS; ++a) yy[a] = (rho_a[a] + drho[a]) / rho;
-            set_mass_fractions<NS>(t, yy, Yc, Xc);
-            const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
-            rc = 1.0 / vol;
-            double Tn;
-            if (gas::T_from_u(t, Yc, si_energy_mass(A.U, (float)Uint), Tc, 1e-14, 100, Tn) < 0)
-                atomic_status(A.status, LBMGPU_ST_NEWTON);
-            Tc = Tn;
-        }
-        double hrr = 0.0;
-        for (int a = 0; a < NS; ++a) {
-            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
-            prp(pr_drho<NS>(a), drho[a]);
-        }
-        put(A, A.rec_nxt, RM_HRR, n, hrr);
-    } else if (CHEM == CHEM_ROSENBROCK) {  // the host build; the device runs it in k_mc_chem
-        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
-    }
-
     // -- species viscosities; Wilke weights phi_ab = (1 + sqrt(mu_a/mu_b) (W_b/W_a)^1/4)^2 /
     // sqrt(8 (1 + W_a/W_b)) formed for b >= a and mirrored, phi_ba = mu_b/mu_a W_a/W_b phi_ab
     // (lbm-collision.cpp:402-430).  Each weight enters the two row sums the reference forms
@@ -715,6 +672,156 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
     prp(pr_theta<NS>(), theta);
     prp(pr_uint<NS>(), Uint);
     prp(pr_gc<NS>(), gasconstant);
+}
+
+// The same parameters for the FP32 storage mode, in FP32 arithmetic: species viscosities,
+// conductivities and binary diffusion coefficients (exp of the ln T fits), the Wilke
+// weights, c_p and the mixture conductivity -- quantities the reference itself rounds to
+// float at its unit conversions (units.hpp:10) -- with the Maxwell-Stefan force accumulated
+// in FP64 (its terms are differences of nearly equal species velocities).
+template <int NS, class AT>
+MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a, const double (*ua)[3],
+                             const double *Xs, const double *Y, const double *X, double W, double T_si, double P_si,
+                             double Uint) {
+    const gas::Tables &t = *A.tab;
+    double *Pr = A.props;
+    auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
+    const float dt = (float)A.dt, pf = (float)p;
+    const float xT = (float)gas::lnT_x(T_si);
+    float mu_k[NS], Xsf[NS], Xf[NS];
+    for (int a = 0; a < NS; ++a) {
+        mu_k[a] = expf(gas::fit_eval_f(t.fit_visc[a], xT));
+        Xsf[a] = (float)Xs[a];
+        Xf[a] = (float)X[a];
+    }
+    float den_s[NS], den_m[NS];
+    for (int a = 0; a < NS; ++a) den_s[a] = den_m[a] = 0.f;
+    for (int a = 0; a < NS; ++a)
+        for (int b = a; b < NS; ++b) {
+            const float f1 = 1.f + sqrtf(mu_k[a] / mu_k[b]) * (float)t.sqrt4W[a][b];
+            const float pab = f1 * f1 / (float)t.wilke_den[a][b];
+            const float pba = mu_k[b] / mu_k[a] * (float)(t.m.W[a] / t.m.W[b]) * pab;
+            if (b == a) {
+                den_s[a] += Xsf[a] * pba;
+                den_m[a] += Xf[a] * pba;
+            } else {
+                den_s[a] += Xsf[b] * pab;
+                den_m[a] += Xf[b] * pab;
+                den_s[b] += Xsf[a] * pba;
+                den_m[b] += Xf[a] * pba;
+            }
+        }
+    for (int a = 0; a < NS; ++a) {
+        const float visc = Xsf[a] * u_mu(A.U, mu_k[a]) / den_s[a];
+        prp(pr_om<NS>(a), (double)(2.f * Xsf[a] * pf * dt / (Xsf[a] * pf * dt + 2.f * visc)));
+    }
+    double F[NS][3];
+    for (int a = 0; a < NS; ++a)
+        for (int d = 0; d < 3; ++d) F[a][d] = 0.0;
+    const float inv_P = 1.f / (float)P_si;
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < a; ++b) {
+            const float D = u_nu(A.U, expf(gas::fit_eval_f(t.fit_diff[a][b], xT)) * inv_P);
+            prp(pr_d<NS>(a, b), (double)D);
+            const double k = (double)(-pf * Xsf[a] * Xsf[b] / D);
+            for (int d = 0; d < 3; ++d) {
+                const double du = ua[a][d] - ua[b][d];
+                F[a][d] += k * du;
+                F[b][d] -= k * du;
+            }
+        }
+    for (int a = 0; a < NS; ++a)
+        for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * (double)dt / rho_a[a]);
+    float mu = 0.f, cpm = 0.f, s1 = 0.f, s2 = 0.f;
+    const float Tf = (float)T_si;
+    for (int k = 0; k < NS; ++k) {
+        mu += Xf[k] * mu_k[k] / den_m[k];
+        const double *c = T_si < t.m.T_mid[k] ? t.m.nasa_lo[k] : t.m.nasa_hi[k];
+        cpm += (float)Y[k] * ((float)c[0] + Tf * ((float)c[1] + Tf * ((float)c[2] + Tf * ((float)c[3] + Tf * (float)c[4])))) *
+               (float)t.invW[k];
+        const float lk = expf(gas::fit_eval_f(t.fit_cond[k], xT));
+        s1 += Xf[k] * lk;
+        s2 += Xf[k] / lk;
+    }
+    const float cp = u_cp(A.U, cpm * (float)gas::kR);
+    const float gasconstant = u_cp(A.U, (float)(gas::kR / W));
+    const float muf = u_mu(A.U, mu);
+    const float lam = u_cond(A.U, 0.5f * (s1 + 1.f / s2));
+    const double theta = u_energy_mass(A.U, (float)(gas::kR * T_si / W));
+    const double om1 = (double)(2.f * pf * cp * dt / (pf * cp * dt + 2.f * lam));
+    const double om = (double)(2.f * pf * dt / (pf * dt + 2.f * muf));
+    if (!(1.0 / om > 0.5) || !(1.0 / om1 > 0.5)) atomic_status(A.status, LBMGPU_ST_TAU_UNSTABLE);
+    prp(pr_omm<NS>(), om);
+    prp(pr_om1<NS>(), om1);
+    prp(pr_theta<NS>(), theta);
+    prp(pr_uint<NS>(), Uint);
+    prp(pr_gc<NS>(), (double)gasconstant);
+}
+
+template <int NS, int CHEM, class AT>
+MC_HDN void mc_props_cell(const AT &A, long n) {
+    const gas::Tables &t = *A.tab;
+    const typename AT::R *Rc = A.rec_cur;
+    double *Pr = A.props;
+    auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
+    const double rho = rec(A, Rc, RM_RHO, n);
+    const double um[3] = {rec(A, Rc, RM_U, n), rec(A, Rc, RM_V, n), rec(A, Rc, RM_W, n)};
+    const double Tl = rec(A, Rc, RM_T, n), p = rec(A, Rc, RM_P, n), rhoe = rec(A, Rc, RM_RHOE, n);
+    double rho_a[NS], ua[NS][3], Xs[NS];
+    for (int a = 0; a < NS; ++a) {
+        rho_a[a] = rec(A, Rc, rs(a, RS_RHO), n);
+        for (int d = 0; d < 3; ++d) ua[a][d] = rec(A, Rc, rs(a, RS_UX + d), n);
+        Xs[a] = rec(A, Rc, rs(a, RS_X), n);
+    }
+    // Cantera state (lbm-collision.cpp:364-367 and :236-238)
+    double Yr[NS], Y[NS], X[NS];
+    for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] / rho;
+    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
+    const double T_si = si_temp(A.U, (float)Tl);
+    const double rho_si = si_rho(A.U, (float)rho);
+    const double P_si = rho_si * gas::kR * T_si / W;
+    const double dt = A.dt;
+
+    // internal energy without the species kinetic energy (lbm-collision.cpp:260-263, 373-376)
+    double Uint = rhoe / rho;
+    for (int a = 0; a < NS; ++a)
+        Uint = Uint - 0.5 * rho_a[a] / rho * (ua[a][0] * ua[a][0] + ua[a][1] * ua[a][1] + ua[a][2] * ua[a][2]);
+
+    // -- chemistry: two explicit half steps with T from (u, v) in between (lbm-collision.cpp:370-399)
+    if (CHEM == CHEM_REF_EXPLICIT) {
+        double drho[NS];
+        for (int a = 0; a < NS; ++a) drho[a] = 0.0;
+        double Tc = T_si, rc = rho_si, Yc[NS], Xc[NS];
+        for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
+        for (int sub = 0; sub < 2; ++sub) {
+            double C[gas::MAXS], wd[gas::MAXS];
+            for (int a = 0; a < NS; ++a) C[a] = rc * Yc[a] / t.m.W[a];
+            gas::net_production(t, Tc, C, wd);
+            for (int a = 0; a < NS; ++a) drho[a] += dt / 2.0 * (double)u_rho_dot(A.U, (float)(wd[a] * t.m.W[a]));
+            double yy[NS];
+            for (int a = 0; a < NS; ++a) yy[a] = (rho_a[a] + drho[a]) / rho;
+            set_mass_fractions<NS>(t, yy, Yc, Xc);
+            const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
+            rc = 1.0 / vol;
+            double Tn;
+            if (gas::T_from_u(t, Yc, si_energy_mass(A.U, (float)Uint), Tc, 1e-14, 100, Tn) < 0)
+                atomic_status(A.status, LBMGPU_ST_NEWTON);
+            Tc = Tn;
+        }
+        double hrr = 0.0;
+        for (int a = 0; a < NS; ++a) {
+            hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * drho[a];
+            prp(pr_drho<NS>(a), drho[a]);
+        }
+        put(A, A.rec_nxt, RM_HRR, n, hrr);
+    } else if (CHEM == CHEM_ROSENBROCK) {  // the host build; the device runs it in k_mc_chem
+        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
+    }
+
+    if constexpr (sizeof(typename AT::P) == sizeof(float))
+        mc_transport_f32<NS>(A, n, p, rho_a, ua, Xs, Y, X, W, T_si, P_si, Uint);
+    else
+        mc_transport_f64<NS>(A, n, p, rho_a, ua, Xs, Y, X, W, T_si, P_si, Uint);
 }
 
 // The energy-flux terms of the energy collision (lbm-collision.cpp:265-316): the enthalpy

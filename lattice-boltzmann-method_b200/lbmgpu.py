@@ -33,7 +33,8 @@ MIXTURE_SC = np.dtype({
 
 EXPORTS = [
     "lbmgpu_create", "lbmgpu_destroy", "lbmgpu_upload", "lbmgpu_download", "lbmgpu_upload_planes",
-    "lbmgpu_download_planes", "lbmgpu_init",
+    "lbmgpu_download_planes", "lbmgpu_set_halo", "lbmgpu_halo_bytes", "lbmgpu_halo_pack", "lbmgpu_halo_unpack",
+    "lbmgpu_init",
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
     "lbmgpu_profile", "lbmgpu_kernel_times", "lbmgpu_device_bytes", "lbmgpu_error_string",
@@ -43,6 +44,7 @@ EXPORTS = [
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
 ]
 SUMS_MAX = 21
+HALO_POPULATIONS, HALO_RECORD = 0, 1
 KERNEL_KINDS = 8
 DIAG_COUNT = 6
 SUR_IN, SUR_OUT, SUR_NPARAMS = 12, 10, 36046
@@ -104,6 +106,10 @@ def lib(path=None):
         L.lbmgpu_download.argtypes = [vp, vp, vp]
         L.lbmgpu_upload_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
         L.lbmgpu_download_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.lbmgpu_set_halo.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.lbmgpu_halo_bytes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+        L.lbmgpu_halo_pack.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+        L.lbmgpu_halo_unpack.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
         L.lbmgpu_units_from_dx_dt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
         L.lbmgpu_step.argtypes = [vp, ctypes.c_int]
         L.lbmgpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
@@ -223,6 +229,25 @@ class Lattice:
                 raise ValueError("species arrays must be C-contiguous %s arrays of shape %s"
                                  % (self.species_dtype, shape))
         return (ctypes.c_void_p * self.ns)(*[sp.ctypes.data for sp in species])
+
+    # -- slab decomposition along x ------------------------------------------------------
+    def set_halo(self, lo, hi, nx_global):
+        """Marks the low / high x ghost plane as a halo of the neighbouring slab
+        (lbmgpu_set_halo); nx_global is the whole domain's Nx with ghosts."""
+        _check(self.L.lbmgpu_set_halo(self.h, int(lo), int(hi), int(nx_global)), "lbmgpu_set_halo")
+
+    def halo_bytes(self, what):
+        b = ctypes.c_size_t()
+        _check(self.L.lbmgpu_halo_bytes(self.h, what, ctypes.byref(b)), "lbmgpu_halo_bytes")
+        return b.value
+
+    def halo_pack(self, face, what, dev_ptr):
+        """Enqueues the face's outgoing values into the device buffer at dev_ptr."""
+        _check(self.L.lbmgpu_halo_pack(self.h, face, what, ctypes.c_void_p(dev_ptr)), "lbmgpu_halo_pack")
+
+    def halo_unpack(self, face, what, dev_ptr):
+        """Enqueues the face's incoming values from the device buffer at dev_ptr."""
+        _check(self.L.lbmgpu_halo_unpack(self.h, face, what, ctypes.c_void_p(dev_ptr)), "lbmgpu_halo_unpack")
 
     def upload_planes(self, i0, cells, species):
         """Uploads the x-planes i0 .. i0 + cells.shape[0] - 1 (lbmgpu_upload_planes)."""
