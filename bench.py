@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--dx", type=float, default=TURB_DEFAULTS["dx"], help="turb: lattice spacing, m")
     ap.add_argument("--dxdt", type=float, default=TURB_DEFAULTS["dxdt"], help="turb: dx / dt, m/s")
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--slab-loopback", action="store_true",
+                    help="turb on one GPU: run the slab-decomposition path with the rank as its own neighbour "
+                         "(halo exchange by device copies) -- the multi-GPU code path without NCCL")
     ap.add_argument("--chem", choices=["ref", "rosenbrock", "surrogate"], default=None,
                     help="reacting workloads: the reference's explicit scheme, the ROS2 stiff integrator, or "
                          "the MLP surrogate trained online from ROS2 (teacher steps, training, then timed "
@@ -873,6 +876,76 @@ def run_reference_turb(args, dist):
     print(json.dumps(line), flush=True)
 
 
+class SlabStepper:
+    """World > 1 (or the loopback check): one slab per rank along x, the rank's 256^3 box of
+    the turbulent layer (the global domain is `world` such boxes in a row, periodic in x),
+    halo planes exchanged every step (slab.exchange) -- over NCCL, issued on the library's own
+    stream so that the exchange, the kernels and the timing events share one ordering."""
+
+    def __init__(self, lat, dist, loopback=False):
+        import torch
+
+        import slab
+        self.torch, self.slab, self.lat, self.dist = torch, slab, lat, dist
+        self.world, self.rank = (1, 0) if loopback else (dist.world, dist.rank)
+        self.ext = torch.cuda.ExternalStream(lat.stream())
+        self.bufs = {w: [torch.empty(lat.halo_bytes(w) // 8, dtype=torch.float64, device="cuda") for _ in range(2)]
+                     for w in (slab.POPULATIONS, slab.RECORD)}
+        self.comm = LoopbackComm(torch) if loopback else slab.TorchComm(dist.pg)
+
+    def pack(self, face, what):
+        buf = self.bufs[what][face]
+        self.lat.halo_pack(face, what, buf.data_ptr())
+        return buf
+
+    def unpack(self, face, what, t):
+        self.lat.halo_unpack(face, what, t.data_ptr())
+
+    def exchange(self, what):
+        with self.torch.cuda.stream(self.ext):
+            self.slab.exchange(what, self.pack, self.unpack, self.comm, self.world, self.rank)
+
+    def steps(self, k, after=None):
+        lat = self.lat
+        for _ in range(k):
+            lat.collide_species()
+            lat.collide()
+            self.exchange(self.slab.POPULATIONS)
+            lat.streaming()
+            lat.tms_bc()
+            lat.calculate_moment()
+            self.exchange(self.slab.RECORD)
+            if after:
+                after()
+
+    def time_steps(self, k):
+        """Device milliseconds of k steps, CUDA events on the library's stream."""
+        t = self.torch
+        e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        e0.record(self.ext)
+        self.steps(k)
+        e1.record(self.ext)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+
+class LoopbackComm:
+    """exchange() transport of a single slab that is its own neighbour: each receive takes
+    the send with the matching tag (device copies on the current stream)."""
+
+    def __init__(self, torch):
+        self.torch = torch
+
+    def empty_like(self, t):
+        return self.torch.empty_like(t)
+
+    def sendrecv(self, ops):
+        sent = {tag: buf for kind, buf, peer, tag in ops if kind == "send"}
+        for kind, buf, peer, tag in ops:
+            if kind == "recv":
+                buf.copy_(sent[tag])
+
+
 def run_ours_turb(args, dist):
     import lbmgpu
     import mech
@@ -887,37 +960,55 @@ def run_ours_turb(args, dist):
     pop_bytes = 4 if args.precision == "fp32" else 8
     lat = lbmgpu.Lattice(N + 2, N + 2, N + 2, mech=m, dtype=workloads.MIXTURE_MC, species_dtype=workloads.SPECIES,
                          dx_dt=turb_units(args), chem=chem, device=device, precision=prec)
+    slabs = dist.world > 1 or args.slab_loopback
+    st = None
+    if slabs:  # the rank's box between two halo planes; the domain: world boxes in a row
+        lat.set_halo(1, 1, N * dist.world + 2)
+        st = SlabStepper(lat, dist, loopback=args.slab_loopback)
 
     def upload_all():
         """Generates and uploads the state plane range by plane range; returns the seconds
-        spent inside the upload calls and the bytes they copied."""
+        spent inside the upload calls and the bytes they copied.  Slabs: the halo planes
+        hold the box's last and first plane (the neighbouring boxes' edge planes)."""
         api, nbytes = 0.0, 0
-        for i0 in range(0, N + 2, TURB_CHUNK):
-            mix, sp = turb_gen(args, m, N, field, i0, min(N + 2, i0 + TURB_CHUNK))
+        ranges = [(i0, i0, min(N + 2, i0 + TURB_CHUNK)) for i0 in range(0, N + 2, TURB_CHUNK)]
+        if slabs:
+            ranges = ([(0, N, N + 1)] + [(i0, i0, min(N + 1, i0 + TURB_CHUNK)) for i0 in range(1, N + 1, TURB_CHUNK)]
+                      + [(N + 1, 1, 2)])
+        for dst, g0, g1 in ranges:
+            mix, sp = turb_gen(args, m, N, field, g0, g1)
             t0 = time.perf_counter()
-            lat.upload_planes(i0, mix, sp)
+            lat.upload_planes(dst, mix, sp)
             api += time.perf_counter() - t0
             nbytes += mix.nbytes + sum(a.nbytes for a in sp)
         return api, nbytes
 
+    def init():
+        lat.init()
+        if slabs:
+            st.exchange(1)  # the halo planes' records from the neighbours
+
+    def time_steps(k):
+        return st.time_steps(k) if slabs else lat.time_steps(k)
+
     upload_all()
-    lat.init()
-    lat.time_steps(max(3, args.warmup))
+    init()
+    time_steps(max(3, args.warmup))
     dist.barrier()
     clk = Clocks(device)
     clk.start()
-    ms = lat.time_steps(args.steps)
+    ms = time_steps(args.steps)
     clocks = clk.stop()
     status = lat.synchronize()
     ms = dist.max(ms)
     # per-kernel device times over a few more steps (every launch bracketed by events)
     kk = min(args.steps, 5)
     lat.profile(True)
-    lat.time_steps(kk)
+    time_steps(kk)
     launches, kms = lat.kernel_times()
     lat.profile(False)
-    names = {0: "k_mc_relax", 1: "k_mc_gather", 2: "k_mc_special (+ other)", 3: "k_mc_props", 5: "k_mc_solve",
-             6: "k_mc_eflux", 7: "k_mc_chem"}
+    names = {0: "k_mc_relax", 1: "k_mc_gather", 2: "k_mc_special (+ other; slabs: + halo pack/unpack)",
+             3: "k_mc_props", 5: "k_mc_solve", 6: "k_mc_eflux", 7: "k_mc_chem"}
     per_step = {names[k]: kms[k] / kk for k in names}
     prof_step = sum(per_step.values())
     step_ms = ms / args.steps
@@ -936,14 +1027,27 @@ def run_ours_turb(args, dist):
     api_up, nbytes = upload_all()
     dist.barrier()
     t0 = time.perf_counter()
-    lat.init()
-    for _ in range(args.steps):
-        lat.collide_species()
-        lat.collide()
-        lat.streaming()
-        lat.tms_bc()
-        lat.calculate_moment()
-        tot = lat.sums()
+    tot = []
+
+    def read_sums():  # the step's conserved totals; slabs: FP64 all-reduce over the ranks
+        tot[:] = lat.sums()
+        if dist.world > 1:
+            import torch
+            t = torch.tensor(tot, dtype=torch.float64, device="cuda")
+            dist.pg.all_reduce(t)
+            tot[:] = t.tolist()
+
+    init()
+    if slabs:
+        st.steps(args.steps, after=read_sums)
+    else:
+        for _ in range(args.steps):
+            lat.collide_species()
+            lat.collide()
+            lat.streaming()
+            lat.tms_bc()
+            lat.calculate_moment()
+            read_sums()
     lat.synchronize()
     api_steps = time.perf_counter() - t0
     api_down = 0.0
@@ -956,6 +1060,10 @@ def run_ours_turb(args, dist):
         api_down += time.perf_counter() - t0
     wall = dist.max(api_up + api_steps + api_down)
     e2e_status = lat.synchronize()
+    if st:
+        st = None
+        import torch
+        torch.cuda.synchronize()
     lat.close()
     e2e = {"value": whole_job_mlups(dist.world, ncell, args.steps, wall), "unit": "MLUPS",
            "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps + 8 * len(tot),
@@ -971,7 +1079,9 @@ def run_ours_turb(args, dist):
         "warmup": max(3, args.warmup), "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded turbulence field and H2/air layer, numpy PCG64 seed 20261203)",
-        "config": {"workload": turb_name(args, N), "cells": ncell, "parallelism": f"replicas{dist.world}",
+        "config": {"workload": turb_name(args, N), "cells": ncell,
+                   "parallelism": (f"x-slabs{dist.world} (one {N}^3 box per GPU, halos over NCCL)" if dist.world > 1
+                                   else ("x-slab loopback check" if slabs else "single GPU")),
                    "l2": "state larger than L2 (86 GB at 258^3 FP32), no flush",
                    "storage": "FP32 populations (shifted), FP64 records and arithmetic" if pop_bytes == 4 else "FP64"},
         "chemistry": {"ms_per_step": per_step["k_mc_chem"], "fraction_of_step": per_step["k_mc_chem"] / step_ms,

@@ -33,6 +33,7 @@ extern "C" {
 #define LBMGPU_E_STATE (-5)      /* no state uploaded / initialised yet               */
 #define LBMGPU_E_UNSUPPORTED (-6) /* configuration not implemented                   */
 #define LBMGPU_E_VERSION (-7)    /* descriptor abi_version mismatch                   */
+#define LBMGPU_E_IO (-8)         /* a file could not be opened, read or written       */
 
 /* ---- device status bits (sticky until lbmgpu_status(..., clear=1)) ------------ */
 #define LBMGPU_ST_NAN 0x1u          /* non-finite density, velocity or temperature     */
@@ -197,6 +198,11 @@ int lbmgpu_halo_bytes(lbmgpu_t *h, int what, size_t *bytes);
 int lbmgpu_halo_pack(lbmgpu_t *h, int face, int what, void *dev_buf);
 int lbmgpu_halo_unpack(lbmgpu_t *h, int face, int what, const void *dev_buf);
 
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own work --
+ * the halo transport, timing events -- with the handle's kernels.  No counterpart in the
+ * reference. */
+int lbmgpu_get_stream(lbmgpu_t *h, void **stream);
+
 /* The base units units.set_m_kg_s(dx, dt) sets (src/headers/units.hpp:32-44), with its
  * float rounding: out = {m, kg, s, K}. */
 int lbmgpu_units_from_dx_dt(float dx, float dt, float *out4);
@@ -341,6 +347,41 @@ int lbmgpu_surrogate_enable(lbmgpu_t *h, int enable, int audit_period);
 int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y);
 int lbmgpu_surrogate_params(lbmgpu_t *h, float *buf, long n, int set);
 int lbmgpu_surrogate_stats(lbmgpu_t *h, lbmgpu_surrogate_report *out);
+
+/* ---- restart and field output from the device state --------------------------------
+ * lbmgpu_write_restart / lbmgpu_read_restart: the reference's restart file
+ * (write_restart / read_restart, src/restart_file.cpp:274-440), records in the caller's
+ * MIXTURE / SPECIES layout of the descriptor.  The header's dx, dy, dz, step and Ra
+ * (single component) or permeability (multicomponent) come from / go to `info`; Nx, Ny, Nz,
+ * dt_sim, the species count and names must match the handle (else LBMGPU_E_ARG).  Written
+ * from the device state between time steps (as a download would return it: fluid cells
+ * whole, other cells their stored moments and type); read back as an upload (the next
+ * Collide continues from it, as the reference's run does after read_restart).
+ * Multicomponent files are streamed a few x-planes at a time. */
+typedef struct lbmgpu_restart_info {
+    int dx, dy, dz;          /* LBM::dx, dy, dz (src/headers/lbm.hpp:107)               */
+    int step;                /* the time step the state belongs to                        */
+    double Ra;               /* single component: LBM::Ra                                 */
+    double permeability;     /* multicomponent: LBM::permeability                         */
+} lbmgpu_restart_info;
+int lbmgpu_write_restart(lbmgpu_t *h, const char *path, const lbmgpu_restart_info *info);
+int lbmgpu_read_restart(lbmgpu_t *h, const char *path, lbmgpu_restart_info *info);
+
+/* lbmgpu_write_vtk: the reference's OutputVTK file (src/output.cpp:9-210, a VTK
+ * RectilinearGrid with raw appended Float32 data) of the current state, byte for byte: the
+ * cell arrays are packed on the device and copied to the host once.  flags:
+ * LBMGPU_VTK_SI converts to SI units as the reference's OUTPUT_SI build does
+ * (multicomponent handles, whose descriptor carries the units), LBMGPU_VTK_MASSFRAC writes
+ * mass fractions as its OUTPUT_MASSFRAC build does (mole fractions otherwise).  dx: the
+ * reference's LBM::dx (the coordinates are i * dx).
+ * lbmgpu_vtk_fields: the packed cell arrays alone -- density, velocity (3 per cell), cell
+ * type, temperature, pressure, then multicomponent HRR, the species fractions and the
+ * species x velocities relative to the mixture, each Nx*Ny*Nz values in x-fastest order;
+ * n_out >= (7 or 10 + 2 n_species) * Nx*Ny*Nz. */
+#define LBMGPU_VTK_SI 1
+#define LBMGPU_VTK_MASSFRAC 2
+int lbmgpu_write_vtk(lbmgpu_t *h, const char *path, int dx, int flags);
+int lbmgpu_vtk_fields(lbmgpu_t *h, float *out, size_t n_out, int flags);
 
 /* Bytes of device memory held by the handle. */
 int lbmgpu_device_bytes(lbmgpu_t *h, size_t *bytes);

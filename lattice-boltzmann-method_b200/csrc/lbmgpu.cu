@@ -434,6 +434,7 @@ const char *lbmgpu_error_string(int code) {
         case LBMGPU_E_STATE: return "no state uploaded yet";
         case LBMGPU_E_UNSUPPORTED: return "configuration not supported";
         case LBMGPU_E_VERSION: return "descriptor abi_version mismatch";
+        case LBMGPU_E_IO: return "file could not be opened, read or written";
         default: return code > 0 ? "device status bits raised" : "unknown error";
     }
 }
@@ -701,6 +702,12 @@ int lbmgpu_halo_pack(lbmgpu_t *h, int face, int what, void *dev_buf) { return ha
 
 int lbmgpu_halo_unpack(lbmgpu_t *h, int face, int what, const void *dev_buf) {
     return halo_call(h, face, what, dev_buf, false);
+}
+
+int lbmgpu_get_stream(lbmgpu_t *h, void **stream) {
+    if (!h || !stream) return LBMGPU_E_ARG;
+    *stream = static_cast<void *>(h->stream);
+    return LBMGPU_OK;
 }
 
 int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos) {

@@ -54,5 +54,8 @@ UNITS_HD float si_energy_mass(const UnitsF &U, float e) { return e * (U.m * U.m)
 UNITS_HD float si_rho(const UnitsF &U, float r) { return (float)((double)(r * U.kg) / dcb(U.m)); }
 UNITS_HD float si_p(const UnitsF &U, float p) { return (float)((double)(p * U.kg) / ((double)U.m * dsq(U.s))); }
 UNITS_HD float si_u(const UnitsF &U, float u) { return u * U.m / U.s; }
+UNITS_HD float si_hrr(const UnitsF &U, float h) {
+    return (float)((double)h * ((double)U.kg * dsq(U.m) / dcb(U.s)));
+}
 
 }  // namespace lbm

@@ -34,6 +34,7 @@ MIXTURE_SC = np.dtype({
 EXPORTS = [
     "lbmgpu_create", "lbmgpu_destroy", "lbmgpu_upload", "lbmgpu_download", "lbmgpu_upload_planes",
     "lbmgpu_download_planes", "lbmgpu_set_halo", "lbmgpu_halo_bytes", "lbmgpu_halo_pack", "lbmgpu_halo_unpack",
+    "lbmgpu_get_stream", "lbmgpu_write_restart", "lbmgpu_read_restart", "lbmgpu_write_vtk", "lbmgpu_vtk_fields",
     "lbmgpu_init",
     "lbmgpu_collide_species", "lbmgpu_collide", "lbmgpu_streaming", "lbmgpu_tms_bc",
     "lbmgpu_calculate_moment", "lbmgpu_step", "lbmgpu_time_steps", "lbmgpu_synchronize", "lbmgpu_status",
@@ -48,6 +49,15 @@ HALO_POPULATIONS, HALO_RECORD = 0, 1
 KERNEL_KINDS = 8
 DIAG_COUNT = 6
 SUR_IN, SUR_OUT, SUR_NPARAMS = 12, 10, 36046
+
+
+class RestartInfo(ctypes.Structure):
+    """lbmgpu_restart_info: the restart header's LBM fields."""
+    _fields_ = [("dx", ctypes.c_int), ("dy", ctypes.c_int), ("dz", ctypes.c_int), ("step", ctypes.c_int),
+                ("Ra", ctypes.c_double), ("permeability", ctypes.c_double)]
+
+
+VTK_SI, VTK_MASSFRAC = 1, 2
 
 
 class SurrogateReport(ctypes.Structure):
@@ -110,6 +120,11 @@ def lib(path=None):
         L.lbmgpu_halo_bytes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
         L.lbmgpu_halo_pack.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
         L.lbmgpu_halo_unpack.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+        L.lbmgpu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.lbmgpu_write_restart.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(RestartInfo)]
+        L.lbmgpu_read_restart.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(RestartInfo)]
+        L.lbmgpu_write_vtk.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int]
+        L.lbmgpu_vtk_fields.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_size_t, ctypes.c_int]
         L.lbmgpu_units_from_dx_dt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
         L.lbmgpu_step.argtypes = [vp, ctypes.c_int]
         L.lbmgpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
@@ -230,11 +245,32 @@ class Lattice:
                                  % (self.species_dtype, shape))
         return (ctypes.c_void_p * self.ns)(*[sp.ctypes.data for sp in species])
 
+    # -- restart and field output ---------------------------------------------------------
+    def write_restart(self, path, info):
+        """The reference's restart file of the current state (lbmgpu_write_restart)."""
+        _check(self.L.lbmgpu_write_restart(self.h, str(path).encode(), ctypes.byref(info)), "lbmgpu_write_restart")
+
+    def read_restart(self, path):
+        """Loads a reference restart file (lbmgpu_read_restart); returns its RestartInfo."""
+        info = RestartInfo()
+        _check(self.L.lbmgpu_read_restart(self.h, str(path).encode(), ctypes.byref(info)), "lbmgpu_read_restart")
+        return info
+
+    def write_vtk(self, path, dx=1, flags=0):
+        """The reference's OutputVTK file of the current state (lbmgpu_write_vtk)."""
+        _check(self.L.lbmgpu_write_vtk(self.h, str(path).encode(), dx, flags), "lbmgpu_write_vtk")
+
     # -- slab decomposition along x ------------------------------------------------------
     def set_halo(self, lo, hi, nx_global):
         """Marks the low / high x ghost plane as a halo of the neighbouring slab
         (lbmgpu_set_halo); nx_global is the whole domain's Nx with ghosts."""
         _check(self.L.lbmgpu_set_halo(self.h, int(lo), int(hi), int(nx_global)), "lbmgpu_set_halo")
+
+    def stream(self):
+        """The handle's cudaStream_t as an integer (lbmgpu_get_stream)."""
+        p = ctypes.c_void_p()
+        _check(self.L.lbmgpu_get_stream(self.h, ctypes.byref(p)), "lbmgpu_get_stream")
+        return p.value or 0
 
     def halo_bytes(self, what):
         b = ctypes.c_size_t()

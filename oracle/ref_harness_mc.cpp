@@ -15,6 +15,8 @@
 #include <vector>
 
 #include "lbm.hpp"
+#include "output.hpp"
+#include "restart_file.hpp"
 #include "units.hpp"
 
 Units_Conv units;   // normally defined by the case setup (src/setup.cpp:10)
@@ -61,11 +63,29 @@ void ref_mc_destroy(void *h) {
     delete lb;
 }
 
+int ref_mc_nx(void *h) { return static_cast<LBM *>(h)->get_Nx(); }
+int ref_mc_ny(void *h) { return static_cast<LBM *>(h)->get_Ny(); }
+int ref_mc_nz(void *h) { return static_cast<LBM *>(h)->get_Nz(); }
 void *ref_mc_cells(void *h) { return &static_cast<LBM *>(h)->mixture[0][0][0]; }
 void *ref_mc_species(void *h, int a) { return &static_cast<LBM *>(h)->species[a][0][0][0]; }
 void ref_mc_set_threads(int n) { omp_set_num_threads(n); }
 void ref_mc_init(void *h) { static_cast<LBM *>(h)->Init(); }
 void ref_mc_loop(void *h, int n) { static_cast<LBM *>(h)->loop(n, 100000000); }
+
+// The reference's own writers, into the current directory: write_restart ->
+// ./restart%06d.dat (src/restart_file.cpp:274-350), OutputVTK -> ./field%06d.vtr
+// (src/output.cpp:9-210).
+void ref_mc_write_restart(void *h, int step) {
+    int s = step;
+    write_restart(s, static_cast<LBM *>(h));
+}
+void ref_mc_output_vtk(void *h, int nout) {
+    int n = nout;
+    OutputVTK(n, static_cast<LBM *>(h));
+}
+
+// read_restart (src/restart_file.cpp:352-440): a new LBM object from a restart file
+void *ref_mc_read_restart(const char *path) { return new LBM(read_restart(std::string(path))); }
 
 void ref_mc_phase(void *h, int which) {
     LBM *lb = static_cast<LBM *>(h);

@@ -52,6 +52,13 @@ def lib(reaction=False, fast=False):
         L.ref_mc_loop.argtypes = [vp, ctypes.c_int]
         L.ref_mc_phase.argtypes = [vp, ctypes.c_int]
         L.ref_mc_set_threads.argtypes = [ctypes.c_int]
+        L.ref_mc_write_restart.argtypes = [vp, ctypes.c_int]
+        L.ref_mc_output_vtk.argtypes = [vp, ctypes.c_int]
+        L.ref_mc_read_restart.restype = vp
+        L.ref_mc_read_restart.argtypes = [ctypes.c_char_p]
+        for f in ("ref_mc_nx", "ref_mc_ny", "ref_mc_nz"):
+            getattr(L, f).restype = ctypes.c_int
+            getattr(L, f).argtypes = [vp]
         _libs[key] = L
     return _libs[key]
 
@@ -75,7 +82,13 @@ class RefMC:
         names = mech.species_names()
         arr = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
         self.h = self.L.ref_mc_create(NX, NY, NZ, len(names), arr)
-        self.shape = (NX + 2, NY + 2, NZ + 2)
+        self._views(mech, mix_dtype, sp_dtype, (NX + 2, NY + 2, NZ + 2))
+
+    def _views(self, mech, mix_dtype, sp_dtype, shape=None):
+        names = mech.species_names()
+        if shape is None:
+            shape = (self.L.ref_mc_nx(self.h), self.L.ref_mc_ny(self.h), self.L.ref_mc_nz(self.h))
+        self.shape = shape
         n = int(np.prod(self.shape))
         buf = (ctypes.c_char * (n * mix_dtype.itemsize)).from_address(self.L.ref_mc_cells(self.h))
         self.cells = np.frombuffer(buf, dtype=mix_dtype).reshape(self.shape)
@@ -92,6 +105,26 @@ class RefMC:
 
     def phase(self, which):
         self.L.ref_mc_phase(self.h, which)
+
+    def write_restart(self, step):
+        """The reference's write_restart: ./restart%06d.dat in the current directory."""
+        self.L.ref_mc_write_restart(self.h, step)
+
+    def output_vtk(self, nout):
+        """The reference's OutputVTK: ./field%06d.vtr in the current directory."""
+        self.L.ref_mc_output_vtk(self.h, nout)
+
+    @classmethod
+    def from_restart(cls, path, mech, units, mix_dtype, sp_dtype, reaction=False, fast=False):
+        """A reference LBM object built by the reference's read_restart."""
+        self = cls.__new__(cls)
+        self.L = lib(reaction, fast)
+        self._mech = mech
+        self.L.ref_mc_set_mech(ctypes.byref(mech))
+        self.L.ref_mc_set_units(units[0], units[1])
+        self.h = self.L.ref_mc_read_restart(path.encode())
+        self._views(mech, mix_dtype, sp_dtype)
+        return self
 
     def close(self):
         if self.h:
