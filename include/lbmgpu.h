@@ -347,6 +347,11 @@ int lbmgpu_surrogate_enable(lbmgpu_t *h, int enable, int audit_period);
 int lbmgpu_surrogate_eval(lbmgpu_t *h, const float *x, long n, float *y);
 int lbmgpu_surrogate_params(lbmgpu_t *h, float *buf, long n, int set);
 int lbmgpu_surrogate_stats(lbmgpu_t *h, lbmgpu_surrogate_report *out);
+/* The gradients of the loss with respect to every weight and bias over the last minibatch of
+ * the last lbmgpu_surrogate_train call (computed by the tensor-core backward kernels, before
+ * that minibatch's Adam step), packed as lbmgpu_surrogate_params packs the parameters; the
+ * standardisation entries are 0.  LBMGPU_E_STATE before any training step. */
+int lbmgpu_surrogate_grads(lbmgpu_t *h, float *buf, long n);
 
 /* ---- restart and field output from the device state --------------------------------
  * lbmgpu_write_restart / lbmgpu_read_restart: the reference's restart file

@@ -290,8 +290,39 @@ struct RateT {
     double hRT[MAXS], cpR[MAXS];
 };
 
-GAS_HD void rate_factors(const Tables &t, double T, RateT &K) {
+// The temperature-only factors of reaction r (see RateT); k0 and lFc are 0 unless the
+// reaction falls off, er is 0 unless it is reversible.
+GAS_HD void rate_factor_one(const Tables &t, int r, double T, double logT, double invRT, double log_cref,
+                            const double *g_RT, double &kf, double &k0, double &lFc, double &er) {
     const lbmgpu_mech &m = t.m;
+    kf = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
+    k0 = 0.0;
+    lFc = 0.0;
+    er = 0.0;
+    if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
+        k0 = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
+        if (m.troe_n[r] >= 3) {
+            const double a = m.troe[r][0], T3 = m.troe[r][1], T1 = m.troe[r][2];
+            double Fc = (1.0 - a) * exp(-T / T3) + a * exp(-T / T1);
+            if (m.troe_n[r] == 4) Fc += exp(-m.troe[r][3] / T);
+            lFc = log10(fmax(Fc, 1e-300));
+        }
+    }
+    if (m.reversible[r]) {
+        double dG = 0.0, dnu = 0.0;
+        for (int j = 0; j < m.n_prod[r]; ++j) {
+            dG += m.nu_prod[r][j] * g_RT[m.prod[r][j]];
+            dnu += m.nu_prod[r][j];
+        }
+        for (int j = 0; j < m.n_reac[r]; ++j) {
+            dG -= m.nu_reac[r][j] * g_RT[m.reac[r][j]];
+            dnu -= m.nu_reac[r][j];
+        }
+        er = exp(dG - dnu * log_cref);
+    }
+}
+
+GAS_HD void rate_factors(const Tables &t, double T, RateT &K) {
     double g_RT[MAXS];
     for (int k = 0; k < t.ns; ++k) {
         K.hRT[k] = h_RT(t, k, T);
@@ -300,30 +331,8 @@ GAS_HD void rate_factors(const Tables &t, double T, RateT &K) {
     }
     const double logT = log(T), invRT = 1.0 / (kR * T);
     const double log_cref = log(kOneAtm / (kR * T));
-    for (int r = 0; r < m.n_reactions; ++r) {
-        K.kf[r] = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
-        if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
-            K.k0[r] = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
-            if (m.troe_n[r] >= 3) {
-                const double a = m.troe[r][0], T3 = m.troe[r][1], T1 = m.troe[r][2];
-                double Fc = (1.0 - a) * exp(-T / T3) + a * exp(-T / T1);
-                if (m.troe_n[r] == 4) Fc += exp(-m.troe[r][3] / T);
-                K.lFc[r] = log10(fmax(Fc, 1e-300));
-            }
-        }
-        if (m.reversible[r]) {
-            double dG = 0.0, dnu = 0.0;
-            for (int j = 0; j < m.n_prod[r]; ++j) {
-                dG += m.nu_prod[r][j] * g_RT[m.prod[r][j]];
-                dnu += m.nu_prod[r][j];
-            }
-            for (int j = 0; j < m.n_reac[r]; ++j) {
-                dG -= m.nu_reac[r][j] * g_RT[m.reac[r][j]];
-                dnu -= m.nu_reac[r][j];
-            }
-            K.er[r] = exp(dG - dnu * log_cref);
-        }
-    }
+    for (int r = 0; r < t.m.n_reactions; ++r)
+        rate_factor_one(t, r, T, logT, invRT, log_cref, g_RT, K.kf[r], K.k0[r], K.lFc[r], K.er[r]);
 }
 
 // C^nu of a mass-action factor: a product for the integer orders 1 to 3 (the elementary
@@ -335,22 +344,20 @@ GAS_HD double conc_pow(double C, double nu) {
     return pow(C, nu);
 }
 
-// Forward and reverse rates of progress (kmol/m^3/s) of reaction r from the factors of
-// rate_factors and the concentrations C[k] (kmol/m^3).
-GAS_HD void rate_of_progress(const Tables &t, const RateT &K, const double *C, int r, double &fwd_out,
-                             double &rev_out) {
+// Forward and reverse rates of progress (kmol/m^3/s) of reaction r from its temperature
+// factors (rate_factor_one) and the concentrations C[k] (kmol/m^3).
+GAS_HD void progress_one(const Tables &t, int r, const double *C, double kf, double k0, double lFc, double er,
+                         double &fwd_out, double &rev_out) {
     const lbmgpu_mech &m = t.m;
-    double kf = K.kf[r];
     double M = 1.0;
     if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
         M = 0.0;
         for (int k = 0; k < t.ns; ++k) M += m.eff[r][k] * C[k];
     }
     if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
-        const double Pr = K.k0[r] * M / kf;
+        const double Pr = k0 * M / kf;
         double F = 1.0;
         if (m.troe_n[r] >= 3) {
-            const double lFc = K.lFc[r];
             const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
             const double lPr = log10(fmax(Pr, 1e-300));
             const double x = (lPr + c) / (n - 0.14 * (lPr + c));
@@ -362,11 +369,17 @@ GAS_HD void rate_of_progress(const Tables &t, const RateT &K, const double *C, i
     double fwd = kf * M, rev = 0.0;
     for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.nu_reac[r][j]);
     if (m.reversible[r]) {
-        rev = kf * M * K.er[r];  // kf / Kc
+        rev = kf * M * er;  // kf / Kc
         for (int j = 0; j < m.n_prod[r]; ++j) rev *= conc_pow(C[m.prod[r][j]], m.nu_prod[r][j]);
     }
     fwd_out = fwd;
     rev_out = rev;
+}
+
+// The same from the factors of rate_factors.
+GAS_HD void rate_of_progress(const Tables &t, const RateT &K, const double *C, int r, double &fwd_out,
+                             double &rev_out) {
+    progress_one(t, r, C, K.kf[r], K.k0[r], K.lFc[r], K.er[r], fwd_out, rev_out);
 }
 
 // Net molar production rates wdot[k] (kmol/m^3/s) from the factors of rate_factors and

@@ -46,32 +46,19 @@ __global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_
     mc_props_cell<NS, CHEM>(A, n);
 }
 
-// the cells the collision-parameter kernel left to the chemistry integrator (surrogate
-// on: out-of-box, non-finite and audited cells), integrated in dense warps
-// The cells the surrogate leaves to the integrator (sur.ilist), G lanes per cell: the
-// lanes of a group evaluate the finite-difference Jacobian's columns side by side
-// (gas::ros2_advance_group), so the listed cells do not wait on serial integrations of one
-// lane each.  A short list (up to kChemShortList cells: latency-bound) takes 8 lanes per
-// cell, a long one 4 (the group's redundant factorisation then costs more than the
-// latency it saves); the choice is made on the device from the list's length.
-constexpr unsigned kChemShortList = 5000;
-template <int NS, int G, typename S>
-__device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
-    const unsigned groups = gridDim.x * blockDim.x / G;
-    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < cnt; i += groups) {
-        const long n = A.sur.ilist[i];
-        double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
-        mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS, McArgsT<S, double>, true, G>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
-    }
-}
+// The cells the surrogate leaves to the integrator (sur.ilist: out-of-box, non-finite and
+// audited cells), kChemLanes lanes per cell integrating it together (ros2_advance_coop).
+constexpr int kChemLanes = 16;
 template <int NS, typename S>
 __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
     const unsigned cnt = *A.sur.icount;
-    if (cnt <= kChemShortList)
-        chem_list_groups<NS, 8>(A, cnt);
-    else
-        chem_list_groups<NS, 4>(A, cnt);
+    const unsigned groups = gridDim.x * blockDim.x / kChemLanes;
+    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / kChemLanes; i < cnt; i += groups) {
+        const long n = A.sur.ilist[i];
+        double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
+        mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, kChemLanes>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+    }
 }
 
 // Chemistry of every fluid cell for LBMGPU_CHEM_ROSENBROCK handles, one thread per cell,
@@ -83,13 +70,17 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
 //                to the integrator list for k_mc_chem_list.
 // A kernel of its own, so that its time (with the surrogate's kernels) is the chemistry's
 // share of the step, and the transport kernel keeps its own occupancy.
+// The integrator runs kChemLanes lanes per cell (ros2_advance_coop: the Jacobian's columns
+// side by side, the iteration matrix spread over the lanes, everything in registers); the
+// surrogate's use of its prediction one thread per cell.
 template <int NS, bool SUR, typename S>
 __global__ void __launch_bounds__(kBlock) k_mc_chem(McArgsT<S, double> A) {
-    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr int L = SUR ? 1 : kChemLanes;
+    const long n = ((long)blockIdx.x * blockDim.x + threadIdx.x) / L;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
     mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
+    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, L>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
@@ -473,7 +464,7 @@ int collide_t(lbmgpu *h) {
         if (A.sur.mode == 1 && A.sur.ilist)
             k_mc_chem<NS9, true, S><<<gp, kBlock, 0, h->stream>>>(A);
         else
-            k_mc_chem<NS9, false, S><<<gp, kBlock, 0, h->stream>>>(A);
+            k_mc_chem<NS9, false, S><<<grid_for(h->g.ncell * kChemLanes), kBlock, 0, h->stream>>>(A);
         ev_end(h, ec);
         CK(cudaGetLastError());
     }

@@ -1354,6 +1354,30 @@ int lbmgpu_surrogate_params(lbmgpu_t *h, float *buf, long n, int set) {
     return LBMGPU_OK;
 }
 
+int lbmgpu_surrogate_grads(lbmgpu_t *h, float *buf, long n) {
+    int rc = sur_check(h);
+    if (rc) return rc;
+    if (!buf || n < LBMGPU_SUR_NPARAMS) return LBMGPU_E_ARG;
+    SurState &s = *h->sur;
+    if (s.train_steps == 0) return LBMGPU_E_STATE;
+    // the gradient buffer of the last minibatch, in the packed parameter layout
+    std::vector<float> g(kNParams);
+    CK(cudaMemcpyAsync(g.data(), s.g, kNParams * 4, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const int rows[4] = {kSurHid, kSurHid, kSurHid, kSurOut};
+    const int cols[4] = {kSurIn, kSurHid, kSurHid, kSurHid};
+    const int ld[4] = {kSurInPad, kSurLd, kSurLd, kSurLd};
+    const int nb[4] = {kSurHid, kSurHid, kSurHid, kSurOut};
+    long p = 0;
+    for (int t = 0; t < 4; ++t) {
+        for (int r = 0; r < rows[t]; ++r)
+            for (int k = 0; k < cols[t]; ++k, ++p) buf[p] = g[off_w(t) + (size_t)r * ld[t] + k];
+        for (int r = 0; r < nb[t]; ++r, ++p) buf[p] = g[off_w(4 + t) + r];
+    }
+    for (; p < LBMGPU_SUR_NPARAMS; ++p) buf[p] = 0.f;
+    return LBMGPU_OK;
+}
+
 int lbmgpu_surrogate_stats(lbmgpu_t *h, lbmgpu_surrogate_report *out) {
     int rc = sur_check(h);
     if (rc) return rc;

@@ -43,6 +43,7 @@ EXPORTS = [
     "lbmgpu_surrogate_collect", "lbmgpu_surrogate_load_samples", "lbmgpu_surrogate_samples",
     "lbmgpu_surrogate_augment", "lbmgpu_surrogate_train",
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
+    "lbmgpu_surrogate_grads",
 ]
 SUMS_MAX = 21
 HALO_POPULATIONS, HALO_RECORD = 0, 1
@@ -149,6 +150,7 @@ def lib(path=None):
         L.lbmgpu_surrogate_eval.argtypes = [vp, fp, ctypes.c_long, fp]
         L.lbmgpu_surrogate_params.argtypes = [vp, fp, ctypes.c_long, ctypes.c_int]
         L.lbmgpu_surrogate_stats.argtypes = [vp, ctypes.POINTER(SurrogateReport)]
+        L.lbmgpu_surrogate_grads.argtypes = [vp, fp, ctypes.c_long]
         L.lbmgpu_error_string.argtypes = [ctypes.c_int]
         L.lbmgpu_error_string.restype = ctypes.c_char_p
         _libs[path] = L
@@ -429,6 +431,14 @@ class Lattice:
         fp = ctypes.POINTER(ctypes.c_float)
         _check(self.L.lbmgpu_surrogate_params(self.h, buf.ctypes.data_as(fp), len(buf), int(values is not None)),
                "lbmgpu_surrogate_params")
+        return buf
+
+    def surrogate_grads(self):
+        """The last training minibatch's loss gradients, packed like the parameters."""
+        import numpy as np
+        buf = np.zeros(SUR_NPARAMS, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _check(self.L.lbmgpu_surrogate_grads(self.h, buf.ctypes.data_as(fp), len(buf)), "lbmgpu_surrogate_grads")
         return buf
 
     def surrogate_stats(self):

@@ -6,8 +6,8 @@ NCCL, here with both slabs on one device and no kernel waiting on another.  In F
 two slabs' cells equal the single-domain run through the same library bit for bit; in the
 FP32 storage mode (each slab shifts its populations by its own plane means) within the
 FP32 mode's bounds.  Cases: a reacting H2/air mixing layer periodic in x, cut through the
-interface, and config 4's turbulent reacting layer (characteristic outflow y faces) at
-16^3."""
+interface, and config 4's turbulent reacting layer (characteristic outflow y faces, stiff
+chemistry) at 16^3."""
 import numpy as np
 import pytest
 
@@ -24,7 +24,7 @@ def case(name):
     if name == "mixing":
         mix, sp = W.mixing_layer_mc(m, N=16, T_hi=1800.0)
         return m, mix, sp, W.FLAME_UNITS, lbmgpu.CHEM_REF_EXPLICIT, 6
-    mix, sp = W.turbulent_layer_mc(m, N=16)
+    mix, sp = W.turbulent_layer_mc(m, N=16, k0=1.0)  # 16 cells per energy-containing wavelength
     return m, mix, sp, W.TURB_UNITS, lbmgpu.CHEM_ROSENBROCK, 9
 
 

@@ -89,3 +89,29 @@ def test_oracle_phase_by_phase_against_live_reference():
             for f in ("f", "g", "fpc", "gpc", "rho", "u", "temp"):
                 _cmp(a[f][fl], ref.cells[f][fl], 1e-12)
     ref.close()
+
+
+@pytest.mark.skipif(not __import__("oracle.refsc", fromlist=["available"]).available(),
+                    reason="the reference's single-component build (oracle/_ref) is not present")
+def test_reference_taylor_green_diverges_at_theta_one_third():
+    """Why config 1 runs at gas constant R = 0.1: the reference's own single-component
+    solver (oracle/_ref/libref_sc.so) on the Taylor-Green vortex of config 1 (Ma 0.1, Re
+    400, rho = T = 1) at 32^3 diverges within 100 steps with R = 1/3 (theta = RT = 1/3, the
+    configuration's literal setting), while with R = 0.1 the same case stays finite and
+    close to its initial density."""
+    from oracle import cases, refsc
+    out = {}
+    for R in (1.0 / 3.0, 0.1):
+        cells, prm = cases.tgv_sc(32, R=R)
+        ref = refsc.RefSC(32, 32, 32, prm["nu"], prm["R"], prm["gamma"], prm["prtl"], cases.MIXTURE_SC)
+        ref.cells[...] = cells
+        ref.init()
+        ref.loop(100)
+        fl = cells["type"] == cases.TYPE_F
+        rho = ref.cells["rho"][fl].copy()
+        ref.close()
+        out[R] = rho
+    bad = out[1.0 / 3.0]
+    assert not np.all(np.isfinite(bad)) or np.max(np.abs(bad - 1.0)) > 0.5
+    good = out[0.1]
+    assert np.all(np.isfinite(good)) and np.max(np.abs(good - 1.0)) < 0.05
