@@ -26,6 +26,7 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
     const UnitsF U = units_from_dx_dt(dx, dt);
     set_lattice_constants(tab, U);
     A.Nx = Nx;
+    A.Nx_glob = Nx;  // one domain: no halo planes
     A.Ny = Ny;
     A.Nz = Nz;
     A.ncell = (long)Nx * Ny * Nz;
