@@ -38,41 +38,6 @@ GAS_HD void reactor_rhs_k(const Tables &t, const RateT &K, double rho, const dou
     F[ns] = -s / (rho * cv);
 }
 
-// reactor_rhs with the temperature factors evaluated reaction by reaction inside the loop
-// (the same expressions as rate_factors + reactor_rhs_k, without the per-reaction arrays),
-// NS species known at compile time so that every array stays in registers.
-template <int NS>
-GAS_HD void reactor_rhs_fused(const Tables &t, double rho, const double *y, double *F) {
-    double C[NS], w[NS], hRT[NS], cpR[NS], g_RT[NS];
-    const double T = y[NS];
-    for (int k = 0; k < NS; ++k) {
-        C[k] = rho * y[k] * t.invW[k];
-        hRT[k] = h_RT(t, k, T);
-        cpR[k] = cp_R(t, k, T);
-        g_RT[k] = hRT[k] - s_R(t, k, T);
-        w[k] = 0.0;
-    }
-    const double logT = log(T), invRT = 1.0 / (kR * T);
-    const double log_cref = log(kOneAtm / (kR * T));
-    const lbmgpu_mech &m = t.m;
-    for (int r = 0; r < m.n_reactions; ++r) {
-        double kf, k0, lFc, er, fwd, rev;
-        rate_factor_one(t, r, T, logT, invRT, log_cref, g_RT, kf, k0, lFc, er);
-        progress_one(t, r, C, kf, k0, lFc, er, fwd, rev);
-        const double q = fwd - rev;
-        for (int j = 0; j < m.n_reac[r]; ++j) w[m.reac[r][j]] -= m.nu_reac[r][j] * q;
-        for (int j = 0; j < m.n_prod[r]; ++j) w[m.prod[r][j]] += m.nu_prod[r][j] * q;
-    }
-    double cv = 0.0, s = 0.0;
-    for (int k = 0; k < NS; ++k) {
-        F[k] = w[k] * t.m.W[k] / rho;
-        cv += y[k] * (cpR[k] - 1.0) * t.invW[k];
-        s += (hRT[k] - 1.0) * kR * T * w[k];
-    }
-    cv *= kR;
-    F[NS] = -s / (rho * cv);
-}
-
 GAS_HD void reactor_rhs(const Tables &t, double rho, const double *y, double *F) {
     RateT K;
     rate_factors(t, y[t.ns], K);
@@ -187,142 +152,60 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     return done ? acc : -1;
 }
 
-#if defined(__CUDACC__)
-// Element i of a register array (i known only at run time) without indexing memory.
-template <int N>
-__device__ __forceinline__ double reg_get(const double (&a)[N], int i) {
-    double v = a[0];
-#pragma unroll
-    for (int q = 1; q < N; ++q)
-        if (q == i) v = a[q];
-    return v;
-}
-template <int N>
-__device__ __forceinline__ void reg_set(double (&a)[N], int i, double v) {
-#pragma unroll
-    for (int q = 0; q < N; ++q)
-        if (q == i) a[q] = v;
-}
-
-// ros2_advance for one cell by a group of G lanes (G a power of two, 16 <= G <= 32, the
-// group's lanes consecutive and aligned; every lane passes the same arguments and gets the
-// same result), NS species: the integrator's arithmetic, operation for operation, with its
-// state spread over the lanes so that it stays in registers --
-//   * lane c < n = NS + 1 evaluates the right-hand side with component c perturbed and owns
-//     column c of the iteration matrix I - gamma h J; lane n evaluates the unperturbed one;
-//   * the partial-pivot LU runs column by column: the pivot's lane finds the pivot row
-//     (first largest |entry|), every lane swaps the two rows in its column, the pivot's lane
-//     forms the multipliers and the lanes to its right update their columns;
-//   * the triangular solves run on vectors every lane holds, each matrix entry fetched by a
-//     shuffle from the lane that owns its column, in the serial solve's order;
-//   * the second stage's right-hand side and the step control run on every lane.
-template <int NS, int G>
-__device__ int ros2_advance_coop(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
-                                 double atol = 1e-10, double atol_T = 1e-3) {
-    constexpr int n = NS + 1;
-    static_assert(G >= n + 1 && G <= 32 && (G & (G - 1)) == 0, "one lane per column and one for the rhs");
-    const int lane = (int)(threadIdx.x & 31u), g = lane & (G - 1);
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
+// ros2_advance with the species count known at compile time: the same arithmetic in the
+// same order, its vectors sized and its loops unrolled so that the compiler keeps the
+// vectors in registers (the device's one-thread-per-cell kernels).
+template <int NS>
+GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                          double atol = 1e-10, double atol_T = 1e-3) {
+    constexpr int ns = NS, n = NS + 1;
     const double gam = 1.0 + 1.0 / sqrt(2.0);
-    double y[n], yp[n], Fp[n], b1[n], col[n];
-    int piv[n];
-#pragma unroll
-    for (int k = 0; k < NS; ++k) y[k] = Y[k];
-    y[NS] = T;
+    double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
+    double M[MAXS + 1][MAXS + 1];
+    int piv[MAXS + 1];
+    for (int k = 0; k < ns; ++k) y[k] = Y[k];
+    y[ns] = T;
     double tt = 0.0, h = dt;
     int acc = 0;
     bool done = false;
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        // this lane's right-hand side: column g perturbed (g < n), or none (g >= n)
-#pragma unroll
-        for (int q = 0; q < n; ++q) yp[q] = y[q];
-        double eps = 1.0;
-        if (g < n) {
-            const double yg = reg_get(y, g);
-            eps = g < NS ? 1e-8 * fmax(fabs(yg), 1e-6) : 1e-7 * yg;
-            reg_set(yp, g, yg + eps);
-        }
-        reactor_rhs_fused<NS>(t, rho, yp, Fp);
-#pragma unroll
-        for (int r = 0; r < n; ++r) b1[r] = __shfl_sync(gmask, Fp[r], n, G);  // F0
-#pragma unroll
-        for (int r = 0; r < n; ++r) col[r] = -gam * h * (Fp[r] - b1[r]) / eps;
-        if (g < n) reg_set(col, g, reg_get(col, g) + 1.0);
-        // LU with partial pivoting, column-oriented
-        bool ok = true;
+        RateT K;
+        rate_factors(t, y[ns], K);
+        reactor_rhs_k(t, K, rho, y, F0);
 #pragma unroll
         for (int c = 0; c < n; ++c) {
-            int p = c;
-            if (g == c) {
-                double best = fabs(col[c]);
 #pragma unroll
-                for (int r = c + 1; r < n; ++r)
-                    if (fabs(col[r]) > best) {
-                        best = fabs(col[r]);
-                        p = r;
-                    }
-            }
-            p = __shfl_sync(gmask, p, c, G);
-            piv[c] = p;
-            const double pv = __shfl_sync(gmask, reg_get(col, p), c, G);
-            if (pv == 0.0) {
-                ok = false;
-                break;
-            }
-            if (p != c) {
-                const double tmp = col[c];
-                col[c] = reg_get(col, p);
-                reg_set(col, p, tmp);
-            }
-            if (g == c) {
+            for (int q = 0; q < n; ++q) yp[q] = y[q];
+            const double eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
+            yp[c] += eps;
+            if (c == ns) rate_factors(t, yp[ns], K);
+            reactor_rhs_k(t, K, rho, yp, Fp);
 #pragma unroll
-                for (int r = c + 1; r < n; ++r) col[r] = col[r] / col[c];
-            }
-#pragma unroll
-            for (int r = c + 1; r < n; ++r) {
-                const double f = __shfl_sync(gmask, col[r], c, G);
-                if (g > c && g < n) col[r] -= f * col[c];
-            }
+            for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
         }
-        if (!ok) {
+        for (int r = 0; r < n; ++r) M[r][r] += 1.0;
+        if (!lu_factor(M, n, piv)) {
             h *= 0.25;
             continue;
         }
-        // k1 = M^-1 F0 (b1), then k2 = M^-1 (F(y + h k1) - 2 k1) (Fp)
-        auto solve = [&](double (&b)[n]) {
 #pragma unroll
-            for (int c = 0; c < n; ++c) {
-                const double tmp = b[c];
-                b[c] = reg_get(b, piv[c]);
-                reg_set(b, piv[c], tmp);
-            }
+        for (int q = 0; q < n; ++q) k1[q] = F0[q];
+        lu_solve(M, n, piv, k1);
 #pragma unroll
-            for (int q = 0; q < n - 1; ++q)
+        for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
+        rate_factors(t, yp[ns], K);
+        reactor_rhs_k(t, K, rho, yp, Fp);
 #pragma unroll
-                for (int r = q + 1; r < n; ++r) b[r] -= __shfl_sync(gmask, col[r], q, G) * b[q];
-#pragma unroll
-            for (int r = n - 1; r >= 0; --r) {
-                double v = b[r];
-#pragma unroll
-                for (int q = r + 1; q < n; ++q) v -= __shfl_sync(gmask, col[r], q, G) * b[q];
-                b[r] = v / __shfl_sync(gmask, col[r], r, G);
-            }
-        };
-        solve(b1);
-#pragma unroll
-        for (int q = 0; q < n; ++q) yp[q] = y[q] + h * b1[q];
-        reactor_rhs_fused<NS>(t, rho, yp, Fp);
-#pragma unroll
-        for (int q = 0; q < n; ++q) Fp[q] = Fp[q] - 2.0 * b1[q];
-        solve(Fp);
+        for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
+        lu_solve(M, n, piv, k2);
         double err = 0.0;
 #pragma unroll
         for (int q = 0; q < n; ++q) {
-            const double ynew = y[q] + 1.5 * h * b1[q] + 0.5 * h * Fp[q];
-            const double sc = (q < NS ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
-            const double e = 0.5 * h * (b1[q] + Fp[q]) / sc;
+            const double ynew = y[q] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
+            const double sc = (q < ns ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
+            const double e = 0.5 * h * (k1[q] + k2[q]) / sc;
             err = fmax(err, fabs(e));
             yp[q] = ynew;
         }
@@ -336,12 +219,12 @@ __device__ int ros2_advance_coop(const Tables &t, double rho, double *Y, double 
         const double fac = err > 0.0 ? 0.9 / sqrt(err) : 4.0;
         h *= fmin(4.0, fmax(0.2, fac));
     }
-#pragma unroll
-    for (int k = 0; k < NS; ++k) Y[k] = y[k];
-    T = y[NS];
+    for (int k = 0; k < ns; ++k) Y[k] = y[k];
+    T = y[ns];
     return done ? acc : -1;
 }
 
+#if defined(__CUDACC__)
 // ros2_advance for one cell by a group of G lanes (G a power of two <= 32, the group's
 // lanes consecutive and aligned within the warp; every lane passes the same arguments).
 // The n + 1 right-hand sides of a sub-step's finite-difference Jacobian (column c

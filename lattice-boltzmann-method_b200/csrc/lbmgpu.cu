@@ -727,6 +727,7 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos) {
     const long mof[6] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.temp, h->mo.p};
     for (long n0 = 0; n0 < nc; n0 += (long)h->stage_cells) {
         const long n1 = std::min<long>(nc, n0 + (long)h->stage_cells);
+        CK(cudaMemsetAsync(h->stage, 0, (size_t)(n1 - n0) * rs, h->stream));  // zero padding bytes
         EvPair ep{};
         ev_begin(h, K_OTHER, ep);
         const unsigned gb = grid_for(n1 - n0);

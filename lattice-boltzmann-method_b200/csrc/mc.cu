@@ -46,19 +46,30 @@ __global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_
     mc_props_cell<NS, CHEM>(A, n);
 }
 
-// The cells the surrogate leaves to the integrator (sur.ilist: out-of-box, non-finite and
-// audited cells), kChemLanes lanes per cell integrating it together (ros2_advance_coop).
-constexpr int kChemLanes = 16;
-template <int NS, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
-    const unsigned cnt = *A.sur.icount;
-    const unsigned groups = gridDim.x * blockDim.x / kChemLanes;
-    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / kChemLanes; i < cnt; i += groups) {
+// The cells the surrogate leaves to the integrator (sur.ilist), G lanes per cell: the
+// lanes of a group evaluate the finite-difference Jacobian's columns side by side
+// (gas::ros2_advance_group), so the listed cells do not wait on serial integrations of one
+// lane each.  A short list (up to kChemShortList cells: latency-bound) takes 8 lanes per
+// cell, a long one 4 (the group's redundant factorisation then costs more than the
+// latency it saves); the choice is made on the device from the list's length.
+constexpr unsigned kChemShortList = 5000;
+template <int NS, int G, typename S>
+__device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
+    const unsigned groups = gridDim.x * blockDim.x / G;
+    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < cnt; i += groups) {
         const long n = A.sur.ilist[i];
         double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
         mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS, McArgsT<S, double>, true, kChemLanes>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, G>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
     }
+}
+template <int NS, typename S>
+__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
+    const unsigned cnt = *A.sur.icount;
+    if (cnt <= kChemShortList)
+        chem_list_groups<NS, 8>(A, cnt);
+    else
+        chem_list_groups<NS, 4>(A, cnt);
 }
 
 // Chemistry of every fluid cell for LBMGPU_CHEM_ROSENBROCK handles, one thread per cell,
@@ -70,17 +81,17 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
 //                to the integrator list for k_mc_chem_list.
 // A kernel of its own, so that its time (with the surrogate's kernels) is the chemistry's
 // share of the step, and the transport kernel keeps its own occupancy.
-// The integrator runs kChemLanes lanes per cell (ros2_advance_coop: the Jacobian's columns
-// side by side, the iteration matrix spread over the lanes, everything in registers); the
-// surrogate's use of its prediction one thread per cell.
+// One thread per cell.  The integrator's vectors are sized by the species count at compile
+// time (ros2_advance_n) so that they stay in registers; its iteration matrix and the rate
+// factors stay per-thread local memory, and the bound of two blocks per SM keeps that
+// working set (about 2 kB per thread) inside L2 instead of streaming it through HBM.
 template <int NS, bool SUR, typename S>
-__global__ void __launch_bounds__(kBlock) k_mc_chem(McArgsT<S, double> A) {
-    constexpr int L = SUR ? 1 : kChemLanes;
-    const long n = ((long)blockIdx.x * blockDim.x + threadIdx.x) / L;
+__global__ void __launch_bounds__(kBlock, 2) k_mc_chem(McArgsT<S, double> A) {
+    const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
     mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, L>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
+    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
@@ -413,6 +424,8 @@ int pack_chunk(lbmgpu *h, long n0, long n1, bool stepped) {
     McArgsT<S, double> A = base_args<S>(h);
     const int c = h->cur;
     const S *pc = stepped ? popb<S>(h, c) : popb<S>(h, 1 - c);
+    // the records' padding bytes come out as zeros, not as what the staging held before
+    CK(cudaMemsetAsync(h->stage, 0, (size_t)(n1 - n0) * (h->mo.size + (size_t)h->ns * h->so.size), h->stream));
     EvPair ep{};
     ev_begin(h, K_OTHER, ep);
     k_mc_pack<NS9, S><<<grid_for(n1 - n0), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[c],
@@ -464,7 +477,7 @@ int collide_t(lbmgpu *h) {
         if (A.sur.mode == 1 && A.sur.ilist)
             k_mc_chem<NS9, true, S><<<gp, kBlock, 0, h->stream>>>(A);
         else
-            k_mc_chem<NS9, false, S><<<grid_for(h->g.ncell * kChemLanes), kBlock, 0, h->stream>>>(A);
+            k_mc_chem<NS9, false, S><<<gp, kBlock, 0, h->stream>>>(A);
         ev_end(h, ec);
         CK(cudaGetLastError());
     }

@@ -481,10 +481,9 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // appended to the list -- k_mc_chem_list integrates them afterwards in dense warps --
 // otherwise they are integrated here.  Teacher steps (mode 0) can write samples.
 //
-// G > 1 (device): a group of G lanes handles the cell together -- every lane runs this
-// function with the same arguments, the integration is ros2_advance_coop (G >= 16: the
-// state spread over the lanes) or ros2_advance_group, and only the group's first lane
-// writes the results.
+// G > 1 (device, the integrator list): a group of G lanes handles the cell together --
+// every lane runs this function with the same arguments, the integration is
+// ros2_advance_group, and only the group's first lane writes the results.
 template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
@@ -536,13 +535,13 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
             for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
             int rc;
 #if defined(__CUDA_ARCH__)
-            if constexpr (G >= 16)
-                rc = gas::ros2_advance_coop<NS, G>(t, rho_si, Yc, Tc, dt_si);
-            else if constexpr (G > 1)
+            if constexpr (G > 1)
                 rc = gas::ros2_advance_group<G>(t, rho_si, Yc, Tc, dt_si);
             else
+                rc = gas::ros2_advance_n<NS>(t, rho_si, Yc, Tc, dt_si);
+#else
+            rc = gas::ros2_advance(t, rho_si, Yc, Tc, dt_si);
 #endif
-                rc = gas::ros2_advance(t, rho_si, Yc, Tc, dt_si);
             if (rc < 0 && lead) atomic_status(A.status, LBMGPU_ST_CHEM);
         }
     } else {

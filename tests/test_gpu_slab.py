@@ -24,7 +24,8 @@ def case(name):
     if name == "mixing":
         mix, sp = W.mixing_layer_mc(m, N=16, T_hi=1800.0)
         return m, mix, sp, W.FLAME_UNITS, lbmgpu.CHEM_REF_EXPLICIT, 6
-    mix, sp = W.turbulent_layer_mc(m, N=16, k0=1.0)  # 16 cells per energy-containing wavelength
+    # 16 cells per energy-containing wavelength, the layer 4 cells wide
+    mix, sp = W.turbulent_layer_mc(m, N=16, k0=1.0, width=4.0)
     return m, mix, sp, W.TURB_UNITS, lbmgpu.CHEM_ROSENBROCK, 9
 
 
