@@ -38,6 +38,82 @@ GAS_HD void reactor_rhs_k(const Tables &t, const RateT &K, double rho, const dou
     F[ns] = -s / (rho * cv);
 }
 
+// The reactor's right-hand side with NS species known at compile time, for the device's
+// one-thread-per-cell integrator: the temperature factors of each reaction evaluated inside
+// the reaction loop (no per-reaction arrays), log T taken once for the species entropies,
+// and the mass-action products and species sums over the dense stoichiometry tables, so that
+// every array is indexed by compile-time constants and stays in registers.  The same rate
+// laws as net_production; the products and sums run in species order instead of the order
+// the reaction lists its species, which moves results by rounding only.
+template <int NS>
+GAS_HD void reactor_rhs_dense(const Tables &t, double rho, const double *y, double *F) {
+    const lbmgpu_mech &m = t.m;
+    const double T = y[NS];
+    const double logT = log(T), invT = 1.0 / T, invRT = 1.0 / (kR * T);
+    const double log_cref = log(kOneAtm / (kR * T));
+    double C[NS], w[NS], hRT[NS], gRT[NS], cv = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const double *a = T < m.T_mid[k] ? m.nasa_lo[k] : m.nasa_hi[k];
+        const double cpR = a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4])));
+        cv += y[k] * (cpR - 1.0) * t.invW[k];
+        hRT[k] = a[0] + T * (a[1] / 2 + T * (a[2] / 3 + T * (a[3] / 4 + T * a[4] / 5))) + a[5] * invT;
+        gRT[k] = hRT[k] - (a[0] * logT + T * (a[1] + T * (a[2] / 2 + T * (a[3] / 3 + T * a[4] / 4))) + a[6]);
+        C[k] = rho * y[k] * t.invW[k];
+        w[k] = 0.0;
+    }
+    for (int r = 0; r < m.n_reactions; ++r) {
+        double kf = m.A[r] * exp(m.b[r] * logT - m.Ea[r] * invRT);
+        double M = 1.0;
+        if (m.rtype[r] != LBMGPU_RXN_ELEMENTARY) {
+            M = 0.0;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) M += m.eff[r][k] * C[k];
+        }
+        if (m.rtype[r] == LBMGPU_RXN_FALLOFF) {
+            const double k0 = m.A0[r] * exp(m.b0[r] * logT - m.Ea0[r] * invRT);
+            const double Pr = k0 * M / kf;
+            double F = 1.0;
+            if (m.troe_n[r] >= 3) {
+                const double a = m.troe[r][0], T3 = m.troe[r][1], T1 = m.troe[r][2];
+                double Fc = (1.0 - a) * exp(-T / T3) + a * exp(-T / T1);
+                if (m.troe_n[r] == 4) Fc += exp(-m.troe[r][3] * invT);
+                const double lFc = log10(fmax(Fc, 1e-300));
+                const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+                const double lPr = log10(fmax(Pr, 1e-300));
+                const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+                F = pow(10.0, lFc / (1.0 + x * x));
+            }
+            kf = kf * (Pr / (1.0 + Pr)) * F;
+            M = 1.0;
+        }
+        double fwd = kf * M, rev = 0.0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+            if (t.nu_f[r][k] != 0.0) fwd *= conc_pow(C[k], t.nu_f[r][k]);
+        if (m.reversible[r]) {
+            double dG = 0.0;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) dG += t.nu_net[r][k] * gRT[k];
+            rev = kf * M * exp(dG - t.dnu[r] * log_cref);
+#pragma unroll
+            for (int k = 0; k < NS; ++k)
+                if (t.nu_b[r][k] != 0.0) rev *= conc_pow(C[k], t.nu_b[r][k]);
+        }
+        const double q = fwd - rev;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) w[k] += t.nu_net[r][k] * q;
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        F[k] = w[k] * m.W[k] / rho;
+        s += (hRT[k] - 1.0) * kR * T * w[k];
+    }
+    cv *= kR;
+    F[NS] = -s / (rho * cv);
+}
+
 GAS_HD void reactor_rhs(const Tables &t, double rho, const double *y, double *F) {
     RateT K;
     rate_factors(t, y[t.ns], K);
@@ -66,6 +142,45 @@ GAS_HD bool lu_factor(double (*M)[MAXS + 1], int n, int *piv) {
         }
     }
     return true;
+}
+
+// lu_factor / lu_solve for a matrix of compile-time size N (the device integrator).
+template <int N>
+GAS_HD bool lu_factor_n(double (&M)[N][N], int *piv) {
+    for (int c = 0; c < N; ++c) {
+        int p = c;
+        for (int r = c + 1; r < N; ++r)
+            if (fabs(M[r][c]) > fabs(M[p][c])) p = r;
+        piv[c] = p;
+        if (M[p][c] == 0.0) return false;
+        if (p != c)
+            for (int q = 0; q < N; ++q) {
+                const double tmp = M[c][q];
+                M[c][q] = M[p][q];
+                M[p][q] = tmp;
+            }
+        for (int r = c + 1; r < N; ++r) {
+            const double f = M[r][c] / M[c][c];
+            M[r][c] = f;
+            for (int q = c + 1; q < N; ++q) M[r][q] -= f * M[c][q];
+        }
+    }
+    return true;
+}
+template <int N>
+GAS_HD void lu_solve_n(const double (&M)[N][N], const int *piv, double *b) {
+    for (int c = 0; c < N; ++c) {
+        const double tmp = b[c];
+        b[c] = b[piv[c]];
+        b[piv[c]] = tmp;
+    }
+    for (int r = 1; r < N; ++r)
+        for (int q = 0; q < r; ++q) b[r] -= M[r][q] * b[q];
+    for (int r = N - 1; r >= 0; --r) {
+        double v = b[r];
+        for (int q = r + 1; q < N; ++q) v -= M[r][q] * b[q];
+        b[r] = v / M[r][r];
+    }
 }
 
 // The factorisation swaps whole rows (multipliers included), so all interchanges are
@@ -152,17 +267,19 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     return done ? acc : -1;
 }
 
-// ros2_advance with the species count known at compile time: the same arithmetic in the
-// same order, its vectors sized and its loops unrolled so that the compiler keeps the
-// vectors in registers (the device's one-thread-per-cell kernels).
+// ros2_advance with the species count known at compile time, for the device's
+// one-thread-per-cell kernels: the same method, step control and factorisation, its vectors
+// sized and its loops unrolled so that they stay in registers, and the right-hand sides
+// from reactor_rhs_dense (no per-reaction arrays to re-read for each of the Jacobian's
+// columns: recomputing a column's exponentials costs less than fetching them back).
 template <int NS>
 GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                           double atol = 1e-10, double atol_T = 1e-3) {
     constexpr int ns = NS, n = NS + 1;
     const double gam = 1.0 + 1.0 / sqrt(2.0);
     double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
-    double M[MAXS + 1][MAXS + 1];
-    int piv[MAXS + 1];
+    double M[n][n];
+    int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
     double tt = 0.0, h = dt;
@@ -171,35 +288,36 @@ GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, dou
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        RateT K;
-        rate_factors(t, y[ns], K);
-        reactor_rhs_k(t, K, rho, y, F0);
-#pragma unroll
+        reactor_rhs_dense<NS>(t, rho, y, F0);
+        // the Jacobian's columns in a rolled loop (one inlined right-hand side); the perturbed
+        // component is selected by comparison so that yp stays in registers
+#pragma unroll 1
         for (int c = 0; c < n; ++c) {
+            double yc = y[0];
 #pragma unroll
-            for (int q = 0; q < n; ++q) yp[q] = y[q];
-            const double eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
-            yp[c] += eps;
-            if (c == ns) rate_factors(t, yp[ns], K);
-            reactor_rhs_k(t, K, rho, yp, Fp);
+            for (int q = 1; q < n; ++q)
+                if (q == c) yc = y[q];
+            const double eps = c < ns ? 1e-8 * fmax(fabs(yc), 1e-6) : 1e-7 * yc;
+#pragma unroll
+            for (int q = 0; q < n; ++q) yp[q] = q == c ? y[q] + eps : y[q];
+            reactor_rhs_dense<NS>(t, rho, yp, Fp);
 #pragma unroll
             for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
         }
         for (int r = 0; r < n; ++r) M[r][r] += 1.0;
-        if (!lu_factor(M, n, piv)) {
+        if (!lu_factor_n<n>(M, piv)) {
             h *= 0.25;
             continue;
         }
 #pragma unroll
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
-        lu_solve(M, n, piv, k1);
+        lu_solve_n<n>(M, piv, k1);
 #pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        rate_factors(t, yp[ns], K);
-        reactor_rhs_k(t, K, rho, yp, Fp);
+        reactor_rhs_dense<NS>(t, rho, yp, Fp);
 #pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
-        lu_solve(M, n, piv, k2);
+        lu_solve_n<n>(M, piv, k2);
         double err = 0.0;
 #pragma unroll
         for (int q = 0; q < n; ++q) {

@@ -69,6 +69,9 @@ struct Tables {
     double Ra_lat[MAXS];               // units.cp(R / W_a)
     double sqrt4W[MAXS][MAXS];         // sqrt(sqrt(W_b / W_a))   (Wilke factor, reference order)
     double wilke_den[MAXS][MAXS];      // sqrt(8 (1 + W_a / W_b))
+    // dense stoichiometry (species k of reaction r; 0 where k does not take part): reactant and
+    // product coefficients and their net difference, for the compile-time-unrolled kinetics
+    double nu_f[MAXR][MAXS], nu_b[MAXR][MAXS], nu_net[MAXR][MAXS], dnu[MAXR];
 };
 
 constexpr double kFitTlo = 200.0, kFitThi = 3500.0, kFitX0 = 7.0;
@@ -466,6 +469,18 @@ inline void make_tables(const lbmgpu_mech &m, Tables &t) {
             t.wilke_den[a][b] = sqrt(8.0 * (1.0 + m.W[a] / m.W[b]));
         }
     for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = 0.0;
+    for (int r = 0; r < MAXR; ++r) {
+        t.dnu[r] = 0.0;
+        for (int k = 0; k < MAXS; ++k) t.nu_f[r][k] = t.nu_b[r][k] = t.nu_net[r][k] = 0.0;
+    }
+    for (int r = 0; r < m.n_reactions; ++r) {
+        for (int j = 0; j < m.n_reac[r]; ++j) t.nu_f[r][m.reac[r][j]] += m.nu_reac[r][j];
+        for (int j = 0; j < m.n_prod[r]; ++j) t.nu_b[r][m.prod[r][j]] += m.nu_prod[r][j];
+        for (int k = 0; k < t.ns; ++k) {
+            t.nu_net[r][k] = t.nu_b[r][k] - t.nu_f[r][k];
+            t.dnu[r] += t.nu_net[r][k];
+        }
+    }
 }
 
 }  // namespace gas
