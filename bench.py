@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--dx", type=float, default=TURB_DEFAULTS["dx"], help="turb: lattice spacing, m")
     ap.add_argument("--dxdt", type=float, default=TURB_DEFAULTS["dxdt"], help="turb: dx / dt, m/s")
     ap.add_argument("--cpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-surrogate", action="store_true", help="turb: skip the surrogate-vs-plain study")
+    ap.add_argument("--sur-shape", default="384x96x96",
+                    help="turb: the surrogate study's channel (config 5's case; 384x192x192 is config 5 itself)")
     ap.add_argument("--slab-loopback", action="store_true",
                     help="turb on one GPU: run the slab-decomposition path with the rank as its own neighbour "
                          "(halo exchange by device copies) -- the multi-GPU code path without NCCL")
@@ -492,6 +495,11 @@ def surrogate_vs_plain(lat, mix, sp, K, refresh_s, cap):
             tpk = max(tpk, d["T_max"])
         runs[name] = (hrr, tpk, d["T_max"])
         status[name] = lat.synchronize()
+        if on:
+            st = lat.surrogate_stats()
+            audit = {"audit_rel_err": st["audit_rel_err"],
+                     "integrated_frac": st["cells_integrated"] / max(1, st["cells_predicted"] + st["cells_integrated"]
+                                                                     + st["cells_audited"])}
     kelvin = lbmgpu.units_from_dx_dt(*workloads.FLAME_UNITS)[3]
     (hs, ps, fs), (hp, pp, fp) = runs["surrogate"], runs["plain"]
     return {"compare_steps": K,
@@ -500,7 +508,8 @@ def surrogate_vs_plain(lat, mix, sp, K, refresh_s, cap):
             "peak_T_rise_rel_err": abs(ps - pp) / max(abs(pp - d0["T_max"]), 1e-300),
             "final_T_max_rel_err": abs(fs - fp) / abs(fp),
             "heat_release_integrated": {"surrogate": hs, "plain": hp, "unit": "lattice (sum over cells and steps)"},
-            "heat_release_rel_err": abs(hs - hp) / max(abs(hp), 1e-300), "compare_status": status}
+            "heat_release_rel_err": abs(hs - hp) / max(abs(hp), 1e-300), "compare_status": status,
+            "compare_audit": audit}
 
 
 def run_ours_mc(args, dist):
@@ -876,6 +885,81 @@ def run_reference_turb(args, dist):
     print(json.dumps(line), flush=True)
 
 
+def surrogate_block(args, device):
+    """Config 5's case -- the reacting H2/air channel of config 3 (NSCBC outflow ends, TMS
+    walls, 1800 K ignition kernel), FP32 populations, ROS2 chemistry -- at args.sur_shape:
+    ROS2 teacher steps writing ~2 M sample rows, augmentation and training, then the
+    surrogate (1 % audit, online collection) against plain ROS2 on the same GPU and state:
+    the chemistry kernels' time per step, and over args.compare steps from the same state
+    (network refreshed every 50) the peak temperature and the integrated heat release."""
+    import lbmgpu
+    import mech
+    import workloads
+    m = mech.h2_air_9()
+    NX, NY, NZ = (int(x) for x in args.sur_shape.split("x"))
+    mix, sp = workloads.flame_channel_mc(m, NX=NX, NY=NY, NZ=NZ)
+    ncell = fluid_cells(mix)
+    lat = lbmgpu.Lattice(*mix.shape, mech=m, dtype=workloads.MIXTURE_MC, species_dtype=workloads.SPECIES,
+                         dx_dt=workloads.FLAME_UNITS, chem=lbmgpu.CHEM_ROSENBROCK, device=device,
+                         precision=lbmgpu.FP32)
+    lat.upload(mix, sp)
+    lat.init()
+    cap = 1 << 21
+    stride = max(1, -(-mix.size * args.teach // cap))
+    lat.surrogate_collect(True, stride=stride, capacity=cap)
+    t0 = time.perf_counter()
+    lat.step(args.teach)
+    lat.synchronize()
+    out = {"case": f"config 5's case at {NX}x{NY}x{NZ}: reacting H2/air channel, NSCBC outflow ends, TMS walls, "
+                   f"1800 K ignition kernel, FP32 populations", "cells": ncell, "teacher_steps": args.teach,
+           "teacher_s": time.perf_counter() - t0}
+    lat.surrogate_collect(False)
+    n_rows = lat.surrogate_stats()["samples"]
+    lat.surrogate_augment(int(args.augment * n_rows), span_y=1.5, span_t=0.01, y_trace=1e-3, seed=20261203)
+    t0 = time.perf_counter()
+    out["train_loss"] = lat.surrogate_train(epochs=args.epochs, batch=4096, lr=2e-3, seed=20261203)
+    out.update({"train_s": time.perf_counter() - t0, "sample_rows": lat.surrogate_stats()["samples"],
+                "teacher_rows": n_rows, "train_epochs": args.epochs})
+    sur_cap = lat.surrogate_stats()["samples"] + (40 + args.compare) * (-(-mix.size // 100))
+    kk = 20
+    lat.surrogate_enable(True, audit_period=100)
+    lat.surrogate_collect(True, stride=100, capacity=sur_cap)
+    lat.profile(True)
+    ms_sur = lat.time_steps(kk)
+    _, kms = lat.kernel_times()
+    lat.profile(False)
+    st = lat.surrogate_stats()
+    tot = max(1, st["cells_predicted"] + st["cells_integrated"] + st["cells_audited"])
+    out.update({"audit_rel_err": st["audit_rel_err"], "predicted_frac": st["cells_predicted"] / tot,
+                "integrated_frac": st["cells_integrated"] / tot, "audited_frac": st["cells_audited"] / tot,
+                "surrogate_step_mlups": ncell * kk / (ms_sur * 1e-3) / 1e6})
+    refresh = []
+    t0 = time.perf_counter()
+    lat.surrogate_train(epochs=2, batch=4096, lr=5e-4, seed=20261204)
+    refresh.append(time.perf_counter() - t0)
+    lat.surrogate_collect(False)
+    lat.surrogate_enable(False)
+    kp = 10
+    lat.profile(True)
+    ms_plain = lat.time_steps(kp)
+    _, kmp = lat.kernel_times()
+    lat.profile(False)
+    chem_sur, chem_plain = (kms[4] + kms[7]) / kk, kmp[7] / kp
+    out.update({"plain_step_mlups": ncell * kp / (ms_plain * 1e-3) / 1e6,
+                "chemistry_ms_per_step": {"surrogate": chem_sur, "plain": chem_plain,
+                                          "speedup": chem_plain / max(chem_sur, 1e-12),
+                                          "kernels": "surrogate: features, network, the prediction's use and the "
+                                                     "integrator list; plain: the ROS2 kernel; the transport kernel "
+                                                     "both share is not counted"},
+                "network_flops_per_cell": 2 * (12 * 128 + 2 * 128 * 128 + 128 * 10)})
+    if args.compare > 0:
+        out.update(surrogate_vs_plain(lat, mix, sp, args.compare, refresh, sur_cap))
+    out["refresh_s"] = refresh
+    out["status"] = lat.synchronize()
+    lat.close()
+    return out
+
+
 class SlabStepper:
     """World > 1 (or the loopback check): one slab per rank along x, the rank's 256^3 box of
     the turbulent layer (the global domain is `world` such boxes in a row, periodic in x),
@@ -1095,6 +1179,11 @@ def run_ours_turb(args, dist):
         "gpu_launches": int(round(sum(launches) / kk * args.steps)),
         "status": status, "e2e_status": e2e_status, "clocks": clocks, "e2e": e2e,
     }
+    if dist.world == 1 and not args.no_surrogate:
+        try:
+            line["surrogate"] = surrogate_block(args, device)
+        except Exception as exc:  # the surrogate study never decides the step's number
+            line["surrogate"] = {"error": str(exc)}
     if dist.world == 1 and not args.no_cpu_baseline:
         try:
             d = turb_cpu_sample(args, 32, 5, 1)

@@ -317,6 +317,58 @@ struct SumsAt {
 template <int NS, class AT, class Sums>
 MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S);
 
+// The Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341): every entry of row a is
+// -dt/2 p X_a X_b / D_ab in that order, so the lower triangle (b < a, holding D_ab on entry)
+// is the matrix's own entry and the diagonal takes row a's entries, b = 0..NS-1, as the
+// reference subtracts them; rows go in order, row a reading the D_ab of the rows below it
+// (still untouched) and its own slots before replacing them; then a dense in-place lower
+// Cholesky factor and the two triangular solves per axis, in arithmetic C (double: the
+// reference's, every division a division -- the boundary cells' upwind differences switch
+// on the sign of near-zero diffusion velocities, so a reciprocal in place of a quotient
+// moves results by 1e-9 within two steps).
+template <int NS, typename C>
+MC_HD void mc_stefan_maxwell(int dt, double p_old, const double *Xold, const double *rho_s, const double (*j_a)[3],
+                             double (*Ld)[NS], double (*usm)[3]) {
+    C L[NS][NS];
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < a; ++b) L[a][b] = (C)Ld[a][b];
+    for (int a = 0; a < NS; ++a) {
+        C d = (C)(rho_s[a] == 0.0 ? 1.0 : rho_s[a]);
+        for (int b = 0; b < NS; ++b) {
+            if (b == a) continue;
+            const C D = b < a ? L[a][b] : L[b][a];
+            const C m = (C)-1.0 * (C)dt / (C)2.0 * (C)p_old * (C)Xold[a] * (C)Xold[b] / D;
+            if (b < a) L[a][b] = m;
+            d -= m;
+        }
+        L[a][a] = d;
+    }
+    for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor
+        C d = L[c][c];
+        for (int q = 0; q < c; ++q) d -= L[c][q] * L[c][q];
+        L[c][c] = sqrt(d);
+        for (int r = c + 1; r < NS; ++r) {
+            C s = L[r][c];
+            for (int q = 0; q < c; ++q) s -= L[r][q] * L[c][q];
+            L[r][c] = s / L[c][c];
+        }
+    }
+    for (int dmn = 0; dmn < 3; ++dmn) {
+        C y[NS], x[NS];
+        for (int r = 0; r < NS; ++r) {
+            C s = (C)j_a[r][dmn];
+            for (int q = 0; q < r; ++q) s -= L[r][q] * y[q];
+            y[r] = s / L[r][r];
+        }
+        for (int r = NS - 1; r >= 0; --r) {
+            C s = y[r];
+            for (int q = r + 1; q < NS; ++q) s -= L[q][r] * x[q];
+            x[r] = s / L[r][r];
+        }
+        for (int r = 0; r < NS; ++r) usm[r][dmn] = (double)x[r];
+    }
+}
+
 template <int NS, class AT, class Pop>
 MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     McSums<NS> S;
@@ -362,54 +414,16 @@ MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S) {
     }
     const double u = ru / rho, v = rv / rho, w = rw / rho;
 
-    // -- Stefan-Maxwell system A u_a = j_a (lbm-moment.cpp:302-341), dense Cholesky, with
-    // the D_ab the collision of this step evaluated at the same old state (T, p, Y).  Every
-    // entry of row a is -dt/2 p X_a X_b / D_ab evaluated in that order, so the lower
-    // triangle (b < a) is the matrix's own entry and the diagonal takes row a's entries,
-    // b = 0..NS-1, as the reference subtracts them; the upper triangle is never stored.
-    // Rows go in order: row a reads D_ab of the rows below it (still untouched) and its
-    // own slots before replacing them.  Every division is the reference's: the boundary
-    // cells' upwind differences switch on the sign of near-zero diffusion velocities, so a
-    // reciprocal in place of a quotient (one rounding apart) moves the results by 1e-9
-    // within two steps.
+    // -- Stefan-Maxwell species velocities (mc_stefan_maxwell) with the D_ab the collision of
+    // this step evaluated at the same old state (T, p, Y)
     const double p_old = rec(A, A.rec_cur, RM_P, n);
     double Xold[NS];
     for (int a = 0; a < NS; ++a) Xold[a] = rec(A, A.rec_cur, rs(a, RS_X), n);
-    for (int a = 0; a < NS; ++a) {
-        double d = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
-        for (int b = 0; b < NS; ++b) {
-            if (b == a) continue;
-            const double D = b < a ? L[a][b] : L[b][a];
-            const double m = -1.0 * A.dt / 2.0 * p_old * Xold[a] * Xold[b] / D;
-            if (b < a) L[a][b] = m;
-            d -= m;
-        }
-        L[a][a] = d;
-    }
-    for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor
-        double d = L[c][c];
-        for (int q = 0; q < c; ++q) d -= L[c][q] * L[c][q];
-        L[c][c] = sqrt(d);
-        for (int r = c + 1; r < NS; ++r) {
-            double s = L[r][c];
-            for (int q = 0; q < c; ++q) s -= L[r][q] * L[c][q];
-            L[r][c] = s / L[c][c];
-        }
-    }
+    // FP64 in both storage modes: the FP32 solve moves the characteristic-inflow case's
+    // temperature by 2e-5 against FP64 within 20 steps (its boundary cells amplify last-bit
+    // changes), twice the FP32 mode's bound
     double usm[NS][3];
-    for (int dmn = 0; dmn < 3; ++dmn) {
-        double y[NS];
-        for (int r = 0; r < NS; ++r) {
-            double s = j_a[r][dmn];
-            for (int q = 0; q < r; ++q) s -= L[r][q] * y[q];
-            y[r] = s / L[r][r];
-        }
-        for (int r = NS - 1; r >= 0; --r) {
-            double s = y[r];
-            for (int q = r + 1; q < NS; ++q) s -= L[q][r] * usm[q][dmn];
-            usm[r][dmn] = s / L[r][r];
-        }
-    }
+    mc_stefan_maxwell<NS, double>(A.dt, p_old, Xold, rho_s, j_a, L, usm);
 
     // -- temperature from the internal energy (setState_UV, lbm-moment.cpp:346-368)
     double Yr[NS], Y[NS], X[NS];
