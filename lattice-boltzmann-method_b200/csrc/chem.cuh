@@ -267,13 +267,43 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     return done ? acc : -1;
 }
 
-// ros2_advance with the species count known at compile time, for the device's
-// one-thread-per-cell kernels: the same method, step control and factorisation, its vectors
-// sized and its loops unrolled so that they stay in registers, and the right-hand sides
-// from reactor_rhs_dense (no per-reaction arrays to re-read for each of the Jacobian's
-// columns: recomputing a column's exponentials costs less than fetching them back).
+// The kinetics policies ros2_advance_k takes: `K` the temperature factors, `factors(T, K)`
+// forms them, `rhs(K, rho, y, F)` is the reactor's right-hand side at y from the factors at
+// y's temperature; with kAnalyticJacobian, `jacobian(K, rho, y, F, J)` writes the species
+// columns of dF/d(Y, T) (the finite differences are taken otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
+// factors inside each right-hand side (reactor_rhs_dense: nothing per reaction kept between
+// calls); a mechanism compiled to straight-line code (gen_kinetics.py) provides its own policy
+// whose factors are formed once per temperature.
 template <int NS>
-GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+struct TableKinetics {
+    static constexpr bool kAnalyticJacobian = false;
+    const Tables &t;
+    struct K {};
+    GAS_HD void factors(double, K &) const {}
+    GAS_HD void rhs(const K &, double rho, const double *y, double *F) const { reactor_rhs_dense<NS>(t, rho, y, F); }
+};
+
+// The tables with the temperature factors kept between right-hand sides (rate_factors +
+// reactor_rhs_k, ros2_advance's evaluation): one RateT per temperature, which a thread holds in
+// local memory.
+struct CachedTableKinetics {
+    static constexpr bool kAnalyticJacobian = false;
+    const Tables &t;
+    using K = RateT;
+    GAS_HD void factors(double T, RateT &k) const { rate_factors(t, T, k); }
+    GAS_HD void rhs(const RateT &k, double rho, const double *y, double *F) const { reactor_rhs_k(t, k, rho, y, F); }
+};
+
+// ros2_advance with the species count known at compile time and the kinetics a policy, for
+// the device's one-thread-per-cell kernels: the same method, step control, factorisation and
+// sequence of right-hand sides (the species columns of the Jacobian at the unperturbed
+// temperature's factors, the temperature column and the second stage at their own), its
+// vectors sized and its loops unrolled so that they stay in registers.  A policy with an
+// analytic Jacobian replaces the species columns' finite differences (ROS2 is a W-method:
+// its order holds for any Jacobian approximation, so only rounding-level differences in
+// the step-size decisions separate the two).
+template <int NS, class Kin>
+GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                           double atol = 1e-10, double atol_T = 1e-3) {
     constexpr int ns = NS, n = NS + 1;
     const double gam = 1.0 + 1.0 / sqrt(2.0);
@@ -288,21 +318,43 @@ GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, dou
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        reactor_rhs_dense<NS>(t, rho, y, F0);
-        // the Jacobian's columns in a rolled loop (one inlined right-hand side); the perturbed
-        // component is selected by comparison so that yp stays in registers
+        typename Kin::K K0;
+        kin.factors(y[ns], K0);
+        kin.rhs(K0, rho, y, F0);
+        if constexpr (Kin::kAnalyticJacobian) {
+            kin.jacobian(K0, rho, y, F0, M);
+            const double s = -gam * h;
+#pragma unroll
+            for (int r = 0; r < n; ++r)
+#pragma unroll
+                for (int c = 0; c < ns; ++c) M[r][c] *= s;
+        } else {
+            // the species columns in a rolled loop (one inlined right-hand side); the perturbed
+            // component is selected by comparison so that yp stays in registers
 #pragma unroll 1
-        for (int c = 0; c < n; ++c) {
-            double yc = y[0];
+            for (int c = 0; c < ns; ++c) {
+                double yc = y[0];
 #pragma unroll
-            for (int q = 1; q < n; ++q)
-                if (q == c) yc = y[q];
-            const double eps = c < ns ? 1e-8 * fmax(fabs(yc), 1e-6) : 1e-7 * yc;
+                for (int q = 1; q < ns; ++q)
+                    if (q == c) yc = y[q];
+                const double eps = 1e-8 * fmax(fabs(yc), 1e-6);
 #pragma unroll
-            for (int q = 0; q < n; ++q) yp[q] = q == c ? y[q] + eps : y[q];
-            reactor_rhs_dense<NS>(t, rho, yp, Fp);
+                for (int q = 0; q < n; ++q) yp[q] = q == c ? y[q] + eps : y[q];
+                kin.rhs(K0, rho, yp, Fp);
 #pragma unroll
-            for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
+                for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
+            }
+        }
+        {  // the temperature column
+            const double eps = 1e-7 * y[ns];
+#pragma unroll
+            for (int q = 0; q < n; ++q) yp[q] = y[q];
+            yp[ns] += eps;
+            typename Kin::K Kt;
+            kin.factors(yp[ns], Kt);
+            kin.rhs(Kt, rho, yp, Fp);
+#pragma unroll
+            for (int r = 0; r < n; ++r) M[r][ns] = -gam * h * (Fp[r] - F0[r]) / eps;
         }
         for (int r = 0; r < n; ++r) M[r][r] += 1.0;
         if (!lu_factor_n<n>(M, piv)) {
@@ -314,7 +366,11 @@ GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, dou
         lu_solve_n<n>(M, piv, k1);
 #pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        reactor_rhs_dense<NS>(t, rho, yp, Fp);
+        {
+            typename Kin::K K2;
+            kin.factors(yp[ns], K2);
+            kin.rhs(K2, rho, yp, Fp);
+        }
 #pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
         lu_solve_n<n>(M, piv, k2);
@@ -342,6 +398,13 @@ GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, dou
     return done ? acc : -1;
 }
 
+// ros2_advance_k over the tables of any mechanism of NS species.
+template <int NS>
+GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                          double atol = 1e-10, double atol_T = 1e-3) {
+    return ros2_advance_k<NS>(TableKinetics<NS>{t}, rho, Y, T, dt, rtol, atol, atol_T);
+}
+
 #if defined(__CUDACC__)
 // ros2_advance for one cell by a group of G lanes (G a power of two <= 32, the group's
 // lanes consecutive and aligned within the warp; every lane passes the same arguments).
@@ -349,19 +412,20 @@ GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, dou
 // perturbed, c < n, and the unperturbed one, index n) are dealt out round robin, index
 // j to lane j % G; each lane then assembles the Jacobian from the group's columns by
 // shuffles and runs the same factorisation, stages and step control -- the arithmetic of
-// ros2_advance value for value, with the Jacobian's evaluations side by side.
-template <int G>
-__device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+// ros2_advance_k value for value, with the Jacobian's evaluations side by side.  The
+// kinetics policy as for ros2_advance_k; CachedTableKinetics gives ros2_advance's values.
+template <int NS, int G, class Kin>
+__device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                                   double atol = 1e-10, double atol_T = 1e-3) {
-    constexpr int kPer = (MAXS + 1 + G) / G;  // right-hand sides per lane, at most
-    const int ns = t.ns, n = ns + 1;
+    constexpr int ns = NS, n = NS + 1;
+    constexpr int kPer = (n + G) / G;  // right-hand sides per lane, at most
     const int lane = (int)(threadIdx.x & 31u), g = lane & (G - 1);
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
     const double gam = 1.0 + 1.0 / sqrt(2.0);
-    double y[MAXS + 1], F0[MAXS + 1], Fp[MAXS + 1], yp[MAXS + 1], k1[MAXS + 1], k2[MAXS + 1];
-    double M[MAXS + 1][MAXS + 1];
-    double Fc[kPer][MAXS + 1], ec[kPer];  // this lane's right-hand sides and their steps
-    int piv[MAXS + 1];
+    double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
+    double M[n][n];
+    double Fc[kPer][n], ec[kPer];  // this lane's right-hand sides and their steps
+    int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
     double tt = 0.0, h = dt;
@@ -370,46 +434,64 @@ __device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        RateT K;
-        bool k_at_y = false;  // K holds the factors at y's temperature
+        typename Kin::K K0;
+        bool k_at_y = false;  // K0 holds the factors at y's temperature
+#pragma unroll
         for (int m = 0; m < kPer; ++m) {
             const int c = g + m * G;  // column c < n, or the unperturbed right-hand side c == n
             if (c > n) break;
-            for (int q = 0; q < n; ++q) yp[q] = y[q];
+            double yc = y[0];
+#pragma unroll
+            for (int q = 1; q < n; ++q)
+                if (q == c) yc = y[q];
             double eps = 1.0;
-            if (c < n) {
-                eps = c < ns ? 1e-8 * fmax(fabs(y[c]), 1e-6) : 1e-7 * y[c];
-                yp[c] += eps;
-            }
+            if (c < n) eps = c < ns ? 1e-8 * fmax(fabs(yc), 1e-6) : 1e-7 * yc;
+#pragma unroll
+            for (int q = 0; q < n; ++q) yp[q] = q == c ? y[q] + eps : y[q];
             ec[m] = eps;
             if (c == ns) {
-                rate_factors(t, yp[ns], K);
-                k_at_y = false;
-            } else if (!k_at_y) {
-                rate_factors(t, y[ns], K);
-                k_at_y = true;
+                typename Kin::K Kt;
+                kin.factors(yp[ns], Kt);
+                kin.rhs(Kt, rho, yp, Fc[m]);
+            } else {
+                if (!k_at_y) {
+                    kin.factors(y[ns], K0);
+                    k_at_y = true;
+                }
+                kin.rhs(K0, rho, yp, Fc[m]);
             }
-            reactor_rhs_k(t, K, rho, yp, Fc[m]);
         }
+#pragma unroll
         for (int r = 0; r < n; ++r) F0[r] = __shfl_sync(gmask, Fc[n / G][r], n % G, G);
+#pragma unroll
         for (int m = 0; m < kPer; ++m)  // this lane's Jacobian columns
             if (g + m * G < n)
+#pragma unroll
                 for (int r = 0; r < n; ++r) Fc[m][r] = -gam * h * (Fc[m][r] - F0[r]) / ec[m];
+#pragma unroll
         for (int c = 0; c < n; ++c)
+#pragma unroll
             for (int r = 0; r < n; ++r) M[r][c] = __shfl_sync(gmask, Fc[c / G][r], c % G, G);
         for (int r = 0; r < n; ++r) M[r][r] += 1.0;
-        if (!lu_factor(M, n, piv)) {
+        if (!lu_factor_n<n>(M, piv)) {
             h *= 0.25;
             continue;
         }
+#pragma unroll
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
-        lu_solve(M, n, piv, k1);
+        lu_solve_n<n>(M, piv, k1);
+#pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        rate_factors(t, yp[ns], K);
-        reactor_rhs_k(t, K, rho, yp, Fp);
+        {
+            typename Kin::K K2;
+            kin.factors(yp[ns], K2);
+            kin.rhs(K2, rho, yp, Fp);
+        }
+#pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
-        lu_solve(M, n, piv, k2);
+        lu_solve_n<n>(M, piv, k2);
         double err = 0.0;
+#pragma unroll
         for (int q = 0; q < n; ++q) {
             const double ynew = y[q] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
             const double sc = (q < ns ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
@@ -418,6 +500,7 @@ __device__ int ros2_advance_group(const Tables &t, double rho, double *Y, double
             yp[q] = ynew;
         }
         if (err <= 1.0) {
+#pragma unroll
             for (int q = 0; q < n; ++q) y[q] = yp[q];
             tt = last ? dt : tt + h;
             done = last;

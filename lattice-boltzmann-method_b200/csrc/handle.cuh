@@ -26,6 +26,10 @@ enum KernelKind {
     K_COLLIDE = 0, K_STREAM_MOMENT = 1, K_OTHER = 2, K_PROPS = 3, K_SURROGATE = 4, K_SOLVE = 5, K_EFLUX = 6,
     K_CHEM = 7, K_NKINDS = 8
 };
+// The stiff chemistry's kinetics: the mechanism tables (any mechanism), or the H2/air
+// mechanism compiled to straight-line code (kinetics_h2_air_9.cuh) when the handle's
+// mechanism is that one.
+enum Kinetics : int { KIN_TABLES = 0, KIN_H2_AIR_9 = 1 };
 // What pop[cur] holds: the uploaded populations, the ones Init built, or post-collision
 // values after at least one step.
 enum PackMode : int { PK_UPLOADED = 0, PK_INIT = 1, PK_STEPPED = 2 };
@@ -91,6 +95,7 @@ struct lbmgpu {
     double *gsum = nullptr;                 // multicomponent: the interior cells' population sums
     lbmh::SurState *sur = nullptr;          // chemistry surrogate, created on first use
     lbmgpu_mech mech{};                     // multicomponent: the caller's mechanism, copied at create
+    int kin = 0;                            // KIN_*: the stiff chemistry's kinetics
     long nfluid = 0;
     // plane-range uploads (multicomponent): the cell types on the host, and which x-planes
     // have arrived since the last complete upload

@@ -53,23 +53,27 @@ __global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_
 // cell, a long one 4 (the group's redundant factorisation then costs more than the
 // latency it saves); the choice is made on the device from the list's length.
 constexpr unsigned kChemShortList = 5000;
-template <int NS, int G, typename S>
+template <int NS, int G, typename S, class KIN>
 __device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
     const unsigned groups = gridDim.x * blockDim.x / G;
     for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < cnt; i += groups) {
         const long n = A.sur.ilist[i];
         double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
         mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS, McArgsT<S, double>, true, G>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, G, KIN>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
     }
 }
-template <int NS, typename S>
+// With a compiled mechanism (KIN: analytic species Jacobian, two right-hand sides per
+// sub-step besides it) a cell is one lane's work.
+template <int NS, typename S, class KIN = void>
 __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
     const unsigned cnt = *A.sur.icount;
-    if (cnt <= kChemShortList)
-        chem_list_groups<NS, 8>(A, cnt);
+    if constexpr (!std::is_void_v<KIN>)
+        chem_list_groups<NS, 1, S, KIN>(A, cnt);
+    else if (cnt <= kChemShortList)
+        chem_list_groups<NS, 8, S, KIN>(A, cnt);
     else
-        chem_list_groups<NS, 4>(A, cnt);
+        chem_list_groups<NS, 4, S, KIN>(A, cnt);
 }
 
 // Chemistry of every fluid cell for LBMGPU_CHEM_ROSENBROCK handles, one thread per cell,
@@ -85,13 +89,14 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
 // time (ros2_advance_n) so that they stay in registers; its iteration matrix and the rate
 // factors stay per-thread local memory, and the bound of two blocks per SM keeps that
 // working set (about 2 kB per thread) inside L2 instead of streaming it through HBM.
-template <int NS, bool SUR, typename S>
+// KIN: the compiled kinetics of the handle's mechanism (gen_kinetics.py), void for the tables.
+template <int NS, bool SUR, typename S, class KIN = void>
 __global__ void __launch_bounds__(kBlock, 2) k_mc_chem(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
     mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
+    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1, KIN>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
@@ -474,8 +479,11 @@ int collide_t(lbmgpu *h) {
     if (h->chem == CHEM_ROSENBROCK) {
         EvPair ec{};
         ev_begin(h, K_CHEM, ec);
+        using KinH2 = kin_h2_air_9::Kinetics;
         if (A.sur.mode == 1 && A.sur.ilist)
             k_mc_chem<NS9, true, S><<<gp, kBlock, 0, h->stream>>>(A);
+        else if (h->kin == KIN_H2_AIR_9)
+            k_mc_chem<NS9, false, S, KinH2><<<gp, kBlock, 0, h->stream>>>(A);
         else
             k_mc_chem<NS9, false, S><<<gp, kBlock, 0, h->stream>>>(A);
         ev_end(h, ec);
@@ -484,7 +492,10 @@ int collide_t(lbmgpu *h) {
     if (A.sur.ilist) {
         EvPair ei{};
         ev_begin(h, K_SURROGATE, ei);
-        k_mc_chem_list<NS9, S><<<148 * 8, kBlock, 0, h->stream>>>(A);
+        if (h->kin == KIN_H2_AIR_9)
+            k_mc_chem_list<NS9, S, kin_h2_air_9::Kinetics><<<148 * 8, kBlock, 0, h->stream>>>(A);
+        else
+            k_mc_chem_list<NS9, S><<<148 * 8, kBlock, 0, h->stream>>>(A);
         ev_end(h, ei);
         CK(cudaGetLastError());
     }
@@ -618,6 +629,7 @@ int mc_setup(lbmgpu *h) {
             CK(cudaMemset(h->shift[b], 0, np * sizeof(double)));
         }
     }
+    h->kin = kin_h2_air_9::matches(*d.mech) ? KIN_H2_AIR_9 : KIN_TABLES;
     gas::Tables *ht = new gas::Tables();
     gas::make_tables(*d.mech, *ht);
     set_lattice_constants(*ht, h->U);

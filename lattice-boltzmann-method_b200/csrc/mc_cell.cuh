@@ -23,8 +23,11 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "d3q27.cuh"
 #include "chem.cuh"
+#include "kinetics_h2_air_9.cuh"
 #include "surrogate.cuh"
 #include "gas.cuh"
 #include "units.cuh"
@@ -498,7 +501,9 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // G > 1 (device, the integrator list): a group of G lanes handles the cell together --
 // every lane runs this function with the same arguments, the integration is
 // ros2_advance_group, and only the group's first lane writes the results.
-template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1>
+// KIN (device): the kinetics policy of a mechanism compiled to straight-line code
+// (gen_kinetics.py) when the handle's mechanism is that one, void for the tables.
+template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1, class KIN = void>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
     const gas::Tables &t = *A.tab;
@@ -549,8 +554,12 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
             for (int a = 0; a < NS; ++a) Yc[a] = Y[a];
             int rc;
 #if defined(__CUDA_ARCH__)
-            if constexpr (G > 1)
-                rc = gas::ros2_advance_group<G>(t, rho_si, Yc, Tc, dt_si);
+            if constexpr (G > 1 && !std::is_void_v<KIN>)
+                rc = gas::ros2_advance_group<NS, G>(KIN{}, rho_si, Yc, Tc, dt_si);
+            else if constexpr (G > 1)
+                rc = gas::ros2_advance_group<NS, G>(gas::CachedTableKinetics{t}, rho_si, Yc, Tc, dt_si);
+            else if constexpr (!std::is_void_v<KIN>)
+                rc = gas::ros2_advance_k<NS>(KIN{}, rho_si, Yc, Tc, dt_si);
             else
                 rc = gas::ros2_advance_n<NS>(t, rho_si, Yc, Tc, dt_si);
 #else

@@ -1,0 +1,411 @@
+"""Compiles a gas mechanism into straight-line CUDA/C++ kinetics: the temperature factors of
+every reaction (Arrhenius rate constants, fall-off k_0 and Troe F_cent, reverse factors
+1/K_c from NASA-7 Gibbs energies, the species' h/RT and c_p/R) and the constant-volume
+reactor's right-hand side from them (third-body sums, fall-off blending, mass-action rates of
+progress, net production, dT/dt), with every constant a literal and every species index
+fixed, so that the device integrator runs it without loading tables or branching on the
+mechanism's structure.
+
+    python gen_kinetics.py data/h2_air_9.json csrc/kinetics_h2_air_9.cuh
+
+The generated `factors` + `rhs_k` compute what gas.cuh's rate_factors + reactor_rhs_k
+(net_production_k, progress_one) compute, operation for operation and in the same order
+(sums over the reaction's species in the order the mechanism lists them, the quotients of
+constants that the tables path forms at run time formed here as literals with the same
+rounding), so that on a host without contraction of multiply-adds the two agree bit for bit.
+Terms that are exactly zero or one are dropped (an Arrhenius exponent of 0, a third-body
+efficiency of 0, a stoichiometric factor of 1), which leaves every result unchanged.  It
+also emits `matches(mech)`, which tells whether a handle's mechanism is the one compiled
+here.  The Makefile regenerates the header when the mechanism or this script changes.
+"""
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+KR = 8314.46261815324      # J / (kmol K), gas.cuh's kR
+ONE_ATM = 101325.0         # Pa, gas.cuh's kOneAtm
+FALLOFF, THREEBODY = 2, 1
+
+
+def lit(x):
+    """A double literal that reads back as exactly x."""
+    r = repr(float(x))
+    if "inf" in r or "nan" in r:
+        raise ValueError(f"non-finite mechanism constant {x}")
+    return r if ("." in r or "e" in r) else r + ".0"
+
+
+def conc(k, nu):
+    """C_k^nu as gas::conc_pow evaluates it."""
+    if nu == 1.0:
+        return f"C{k}"
+    if nu == 2.0:
+        return f"(C{k} * C{k})"
+    if nu == 3.0:
+        return f"(C{k} * C{k} * C{k})"
+    return f"pow(C{k}, {lit(nu)})"
+
+
+def arrhenius(A, b, Ea):
+    """A exp(b ln T - Ea / RT) (gas::rate_factor_one) without the exactly-zero terms."""
+    if b == 0.0 and Ea == 0.0:
+        return lit(A)  # A * exp(0 - 0) = A * 1
+    if Ea == 0.0:
+        return f"{lit(A)} * exp({lit(b)} * logT)"
+    if b == 0.0:
+        return f"{lit(A)} * exp(-({lit(Ea)} * invRT))"  # 0 * logT - x = -x
+    return f"{lit(A)} * exp({lit(b)} * logT - {lit(Ea)} * invRT)"
+
+
+def weighted(terms):
+    """sum_j nu_j g_j accumulated from 0 in the listed order (signs: +1 products, -1 reactants)."""
+    out = ""
+    for sign, nu, name in terms:
+        t = name if nu == 1.0 else f"{lit(nu)} * {name}"
+        if not out:
+            out = t if sign > 0 else f"-({t})"
+        else:
+            out += (" + " if sign > 0 else " - ") + t
+    return out or "0.0"
+
+
+def dpow(k, nu, others):
+    """d/dC_k of C_k^nu * prod(others): the product of the other factors times nu C_k^(nu-1)."""
+    rest = [conc(j, n) for j, n in others]
+    if nu == 1.0:
+        head = []
+    elif nu == 2.0:
+        head = [f"2.0 * C{k}"]
+    elif nu == 3.0:
+        head = [f"3.0 * (C{k} * C{k})"]
+    else:
+        head = [f"{lit(nu)} * pow(C{k}, {lit(nu - 1.0)})"]
+    terms = head + rest
+    return " * ".join(terms) if terms else "1.0"
+
+
+def emit_jacobian(m, L, fidx):
+    """jac_species: the species columns of d(Y, T)/dt's Jacobian, d F_k / d Y_j (j < NS), at
+    fixed T and rho from the factors at y's temperature, differentiating rhs_k's expressions:
+    the mass-action products, the third-body sum M (efficiency-weighted concentrations) and
+    the Troe blending F(Pr), Pr = k0 M / k_inf; and dT/dt's row through net production and
+    c_v.  With D_kj = d wdot_k / d C_j (C_j = rho Y_j / W_j):
+        J_kj = D_kj W_k / W_j,
+        J_Tj = -(R T / (W_j c_v)) sum_k (h_k/RT - 1) D_kj - F_T R (c_p,j/R - 1) / (W_j c_v).
+    The fall-off derivative: d(k_inf Pr/(1+Pr) F)/dM = k0 [F/(1+Pr)^2 + F (-2 x lFc / (1+x^2)^2)
+    n / ((n - 0.14 u)^2 (1+Pr))], u = log10 Pr + c, x = u / (n - 0.14 u)."""
+    ns, nr = m.n_species, m.n_reactions
+    add = L.append
+    add("// The species columns of the Jacobian of F (rhs_k) with respect to (Y, T): J[k][j] =")
+    add("// dF_k / dY_j for j < NS and every row k <= NS, at fixed temperature and density, from the")
+    add("// factors at y's temperature and F = rhs_k(K, rho, y).  Column NS is not written.")
+    add("GAS_HD void jac_species(const Factors &K, double rho, const double *y, const double *F,")
+    add("                        double (&J)[NS + 1][NS + 1]) {")
+    add(f"    const double T = y[{ns}];")
+    for k in range(ns):
+        add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
+    add(f"    double D[{ns}][{ns}];  // d wdot_k / d C_j")
+    add("#pragma unroll")
+    add(f"    for (int k = 0; k < {ns}; ++k)")
+    add("#pragma unroll")
+    add(f"        for (int j = 0; j < {ns}; ++j) D[k][j] = 0.0;")
+    for r in range(nr):
+        reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
+        prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
+        net = {}
+        for k, nu in reac:
+            net[k] = net.get(k, 0.0) - nu
+        for k, nu in prod:
+            net[k] = net.get(k, 0.0) + nu
+        net = {k: v for k, v in net.items() if v != 0.0}
+        add(f"    {{  // reaction {r}")
+        if m.rtype[r] == 0:
+            add(f"        const double kfM = K.kf[{r}];")
+        else:
+            effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
+            msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
+            add(f"        const double M = {msum};")
+            if m.rtype[r] == FALLOFF:
+                i = fidx[r]
+                add(f"        const double Pr = K.k0[{i}] * M / K.kf[{r}];")
+                if m.troe_n[r] >= 3:
+                    add(f"        const double lFc = K.lFc[{i}];")
+                    add("        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
+                    add("        const double lPr = log10(fmax(Pr, 1e-300));")
+                    add("        const double u = lPr + c, den = n - 0.14 * u;")
+                    add("        const double x = u / den;")
+                    add("        const double Fo = pow(10.0, lFc / (1.0 + x * x));")
+                    add("        const double ipr = 1.0 / (1.0 + Pr);")
+                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr) * Fo;")
+                    add("        const double opx = 1.0 + x * x;")
+                    add(f"        const double dkdM = K.k0[{i}] * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));")
+                else:
+                    add("        const double ipr = 1.0 / (1.0 + Pr);")
+                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr);")
+                    add(f"        const double dkdM = K.k0[{i}] * ipr * ipr;")
+            else:
+                add(f"        const double kfM = K.kf[{r}] * M;")
+                add(f"        const double dkdM = K.kf[{r}];")
+        pf = " * ".join(conc(k, nu) for k, nu in reac)
+        rev = bool(m.reversible[r])
+        if m.rtype[r] != 0:
+            pb = " * ".join(conc(k, nu) for k, nu in prod)
+            if rev:
+                add(f"        const double g = dkdM * ({pf} - K.er[{r}] * {pb});")
+            else:
+                add(f"        const double g = dkdM * {pf};")
+        # dq/dC_j for the reaction's own species
+        dq = {}
+        for idx, (k, nu) in enumerate(reac):
+            others = [x for jdx, x in enumerate(reac) if jdx != idx]
+            dq.setdefault(k, []).append(("+", dpow(k, nu, others)))
+        if rev:
+            for idx, (k, nu) in enumerate(prod):
+                others = [x for jdx, x in enumerate(prod) if jdx != idx]
+                dq.setdefault(k, []).append(("-", dpow(k, nu, others)))
+        effs = {k: m.eff[r][k] for k in range(ns) if m.rtype[r] != 0 and m.eff[r][k] != 0.0}
+        cols = sorted(set(dq) | set(effs))
+        for j in cols:
+            parts = []
+            for sign, e in dq.get(j, []):
+                if sign == "+":
+                    parts.append(f"+ kfM * ({e})")
+                else:
+                    parts.append(f"- kfM * K.er[{r}] * ({e})")
+            if j in effs:
+                e = effs[j]
+                parts.append("+ g" if e == 1.0 else f"+ {lit(e)} * g")
+            expr = " ".join(parts)
+            expr = expr[2:] if expr.startswith("+ ") else "-" + expr[2:]
+            add(f"        const double dq{j} = {expr};")
+        for k, v in net.items():
+            for j in cols:
+                add(f"        D[{k}][{j}] += {'' if v == 1.0 else ('-' if v == -1.0 else lit(v) + ' * ')}dq{j};"
+                    .replace("+= -", "-= "))
+        add("    }")
+    # assemble J
+    add("    double cv = 0.0;")
+    for k in range(ns):
+        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
+    add(f"    cv *= {lit(KR)};")
+    add(f"    const double RT_cv = {lit(KR)} * T / cv;")
+    add("#pragma unroll")
+    add(f"    for (int j = 0; j < {ns}; ++j) {{")
+    add("        double sT = 0.0;")
+    add("#pragma unroll")
+    add(f"        for (int k = 0; k < {ns}; ++k) sT += (K.hRT[k] - 1.0) * D[k][j];")
+    W = ", ".join(lit(m.W[k]) for k in range(ns))
+    iW = ", ".join(lit(1.0 / m.W[k]) for k in range(ns))
+    add(f"        constexpr double Wk[{ns}] = {{{W}}};")
+    add(f"        constexpr double iWk[{ns}] = {{{iW}}};")
+    add("#pragma unroll")
+    add(f"        for (int k = 0; k < {ns}; ++k) J[k][j] = D[k][j] * Wk[k] * iWk[j];")
+    add(f"        J[{ns}][j] = -(RT_cv * sT + F[{ns}] * {lit(KR)} * (K.cpR[j] - 1.0) / cv) * iWk[j];")
+    add("    }")
+    add("}")
+    add("")
+
+
+def generate(m, name):
+    ns, nr = m.n_species, m.n_reactions
+    names = m.species_names()
+    falloff = [r for r in range(nr) if m.rtype[r] == FALLOFF]
+    fidx = {r: i for i, r in enumerate(falloff)}
+    L = []
+    add = L.append
+    add(f"// Generated by gen_kinetics.py from the mechanism {name} -- do not edit; `make` regenerates it.")
+    add("// Its kinetics as straight-line code: gas.cuh's rate_factors (factors) and reactor_rhs_k")
+    add("// (rhs_k) with the mechanism's constants inlined.")
+    add("#pragma once")
+    add("#include <math.h>")
+    add('#include "gas.cuh"')
+    add("")
+    add(f"namespace kin_{name} {{")
+    add("")
+    add(f"constexpr int NS = {ns}, NR = {nr}, NF = {max(len(falloff), 1)};")
+    add("")
+    # ---- matches(): every quantity the kinetics read
+    add("// Whether `m` is the mechanism compiled here (every quantity the kinetics read).")
+    add("inline bool matches(const lbmgpu_mech &m) {")
+    add(f"    if (m.n_species != {ns} || m.n_reactions != {nr}) return false;")
+    for k in range(ns):
+        add(f"    if (m.W[{k}] != {lit(m.W[k])} || m.T_mid[{k}] != {lit(m.T_mid[k])}) return false;")
+        for i in range(7):
+            add(f"    if (m.nasa_lo[{k}][{i}] != {lit(m.nasa_lo[k][i])} || m.nasa_hi[{k}][{i}] != "
+                f"{lit(m.nasa_hi[k][i])}) return false;")
+    for r in range(nr):
+        add(f"    if (m.rtype[{r}] != {m.rtype[r]} || m.reversible[{r}] != {m.reversible[r]} || m.n_reac[{r}] != "
+            f"{m.n_reac[r]} || m.n_prod[{r}] != {m.n_prod[r]}) return false;")
+        for j in range(m.n_reac[r]):
+            add(f"    if (m.reac[{r}][{j}] != {m.reac[r][j]} || m.nu_reac[{r}][{j}] != {lit(m.nu_reac[r][j])}) "
+                f"return false;")
+        for j in range(m.n_prod[r]):
+            add(f"    if (m.prod[{r}][{j}] != {m.prod[r][j]} || m.nu_prod[{r}][{j}] != {lit(m.nu_prod[r][j])}) "
+                f"return false;")
+        add(f"    if (m.A[{r}] != {lit(m.A[r])} || m.b[{r}] != {lit(m.b[r])} || m.Ea[{r}] != {lit(m.Ea[r])}) "
+            f"return false;")
+        if m.rtype[r] == FALLOFF:
+            add(f"    if (m.A0[{r}] != {lit(m.A0[r])} || m.b0[{r}] != {lit(m.b0[r])} || m.Ea0[{r}] != "
+                f"{lit(m.Ea0[r])} || m.troe_n[{r}] != {m.troe_n[r]}) return false;")
+            for i in range(m.troe_n[r]):
+                add(f"    if (m.troe[{r}][{i}] != {lit(m.troe[r][i])}) return false;")
+        if m.rtype[r] != 0:
+            for k in range(ns):
+                add(f"    if (m.eff[{r}][{k}] != {lit(m.eff[r][k])}) return false;")
+    add("    return true;")
+    add("}")
+    add("")
+    # ---- temperature factors
+    add("// The temperature-only factors (gas::RateT): k_inf (k for non-fall-off reactions), the")
+    add("// fall-off k_0 and log10 F_cent, the reverse factors exp(dG/RT - dnu ln(p_atm / R T)) and")
+    add("// the species' h/RT and c_p/R.")
+    add("struct Factors {")
+    add("    double kf[NR], er[NR], k0[NF], lFc[NF], hRT[NS], cpR[NS];")
+    add("};")
+    add("")
+    add("GAS_HD void factors(double T, Factors &K) {")
+    add("    const double logT = log(T), invRT = 1.0 / (8314.46261815324 * T);")
+    add(f"    const double log_cref = log({lit(ONE_ATM)} / ({lit(KR)} * T));")
+    add(f"    double gRT[{ns}];")
+    # one branch per distinct switch temperature
+    groups = {}
+    for k in range(ns):
+        groups.setdefault(m.T_mid[k], []).append(k)
+    for Tm, ks in groups.items():
+        add(f"    if (T < {lit(Tm)}) {{")
+        for branch in ("lo", "hi"):
+            if branch == "hi":
+                add("    } else {")
+            for k in ks:
+                a = m.nasa_lo[k] if branch == "lo" else m.nasa_hi[k]
+                add(f"        K.cpR[{k}] = {lit(a[0])} + T * ({lit(a[1])} + T * ({lit(a[2])} + T * ({lit(a[3])} + T * "
+                    f"{lit(a[4])})));")
+                # h_RT: a1/2 + T (a2/3 + T (a3/4 + T a4 / 5)) + a5 / T
+                add(f"        K.hRT[{k}] = {lit(a[0])} + T * ({lit(a[1] / 2)} + T * ({lit(a[2] / 3)} + T * "
+                    f"({lit(a[3] / 4)} + T * {lit(a[4])} / 5.0))) + {lit(a[5])} / T;")
+                # s_R: a0 ln T + T (a1 + T (a2/2 + T (a3/3 + T a4 / 4))) + a6 (the quarter is exact)
+                add(f"        gRT[{k}] = K.hRT[{k}] - ({lit(a[0])} * logT + T * ({lit(a[1])} + T * ({lit(a[2] / 2)} + T * "
+                    f"({lit(a[3] / 3)} + T * {lit(a[4] / 4)}))) + {lit(a[6])});")
+        add("    }")
+    for r in range(nr):
+        add(f"    K.kf[{r}] = {arrhenius(m.A[r], m.b[r], m.Ea[r])};")
+        if m.rtype[r] == FALLOFF:
+            i = fidx[r]
+            add(f"    K.k0[{i}] = {arrhenius(m.A0[r], m.b0[r], m.Ea0[r])};")
+            if m.troe_n[r] >= 3:
+                a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
+                add("    {")
+                add(f"        double Fc = {lit(1.0 - a)} * exp(-T / {lit(T3)}) + {lit(a)} * exp(-T / {lit(T1)});")
+                if m.troe_n[r] == 4:
+                    add(f"        Fc += exp({lit(-m.troe[r][3])} / T);")
+                add(f"        K.lFc[{i}] = log10(fmax(Fc, 1e-300));")
+                add("    }")
+            else:
+                add(f"    K.lFc[{i}] = 0.0;")
+        if m.reversible[r]:
+            terms = [(+1, m.nu_prod[r][j], f"gRT[{m.prod[r][j]}]") for j in range(m.n_prod[r])]
+            terms += [(-1, m.nu_reac[r][j], f"gRT[{m.reac[r][j]}]") for j in range(m.n_reac[r])]
+            dnu = 0.0
+            for _, nu, _ in terms[:m.n_prod[r]]:
+                dnu += nu
+            for _, nu, _ in terms[m.n_prod[r]:]:
+                dnu -= nu
+            dG = weighted(terms)
+            if dnu == 0.0:
+                add(f"    K.er[{r}] = exp({dG});")
+            else:
+                add(f"    K.er[{r}] = exp(({dG}) - {lit(dnu)} * log_cref);")
+        else:
+            add(f"    K.er[{r}] = 0.0;")
+    add("}")
+    add("")
+    # ---- right-hand side from the factors
+    add("// F = d(Y_0..Y_{NS-1}, T)/dt at density rho [kg/m^3] and state y, from the factors K at")
+    add("// y's temperature (gas::reactor_rhs_k).")
+    add("GAS_HD void rhs_k(const Factors &K, double rho, const double *y, double *F) {")
+    add(f"    const double T = y[{ns}];")
+    for k in range(ns):
+        add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
+    for k in range(ns):
+        add(f"    double w{k} = 0.0;")
+    for r in range(nr):
+        reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
+        prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
+        eq = " + ".join(f"{nu:g} {names[k]}" for k, nu in reac) + (" <=> " if m.reversible[r] else " => ") + \
+            " + ".join(f"{nu:g} {names[k]}" for k, nu in prod)
+        tag = "  (+M)" if m.rtype[r] == FALLOFF else ("  + M" if m.rtype[r] == THREEBODY else "")
+        add(f"    {{  // {r}: {eq}{tag}")
+        if m.rtype[r] == 0:
+            add(f"        const double kfM = K.kf[{r}];")
+        else:
+            effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
+            msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
+            add(f"        const double M = {msum};")
+            if m.rtype[r] == FALLOFF:
+                i = fidx[r]
+                add(f"        const double Pr = K.k0[{i}] * M / K.kf[{r}];")
+                if m.troe_n[r] >= 3:
+                    add(f"        const double lFc = K.lFc[{i}];")
+                    add("        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
+                    add("        const double lPr = log10(fmax(Pr, 1e-300));")
+                    add("        const double x = (lPr + c) / (n - 0.14 * (lPr + c));")
+                    add(f"        const double kfM = K.kf[{r}] * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));")
+                else:
+                    add(f"        const double kfM = K.kf[{r}] * (Pr / (1.0 + Pr)) * 1.0;")
+            else:
+                add(f"        const double kfM = K.kf[{r}] * M;")
+        add("        const double fwd = kfM" + "".join(f" * {conc(k, nu)}" for k, nu in reac) + ";")
+        if m.reversible[r]:
+            add(f"        const double rev = kfM * K.er[{r}]" + "".join(f" * {conc(k, nu)}" for k, nu in prod) + ";")
+            add("        const double q = fwd - rev;")
+        else:
+            add("        const double q = fwd;")
+        for k, nu in reac:
+            add(f"        w{k} -= {'q' if nu == 1.0 else lit(nu) + ' * q'};")
+        for k, nu in prod:
+            add(f"        w{k} += {'q' if nu == 1.0 else lit(nu) + ' * q'};")
+        add("    }")
+    add("    double cv = 0.0, s = 0.0;")
+    for k in range(ns):
+        add(f"    F[{k}] = w{k} * {lit(m.W[k])} / rho;")
+        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
+        add(f"    s += (K.hRT[{k}] - 1.0) * {lit(KR)} * T * w{k};")
+    add(f"    cv *= {lit(KR)};")
+    add(f"    F[{ns}] = -s / (rho * cv);")
+    add("}")
+    add("")
+    emit_jacobian(m, L, fidx)
+    add("// The integrator's kinetics policy (gas::ros2_advance_k): factors once per temperature,")
+    add("// right-hand sides from them, the species columns of the Jacobian analytically.")
+    add("struct Kinetics {")
+    add("    using K = Factors;")
+    add("    static constexpr bool kAnalyticJacobian = true;")
+    add("    GAS_HD void factors(double T, Factors &k) const { kin_" + name + "::factors(T, k); }")
+    add("    GAS_HD void rhs(const Factors &k, double rho, const double *y, double *F) const {")
+    add("        rhs_k(k, rho, y, F);")
+    add("    }")
+    add("    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F,")
+    add("                         double (&J)[NS + 1][NS + 1]) const {")
+    add("        jac_species(k, rho, y, F, J);")
+    add("    }")
+    add("};")
+    add("")
+    add(f"}}  // namespace kin_{name}")
+    return "\n".join(L) + "\n"
+
+
+def main():
+    import mech
+    src, out = sys.argv[1], sys.argv[2]
+    m = mech.load_json(src)
+    name = os.path.splitext(os.path.basename(src))[0]
+    text = generate(m, name)
+    if not os.path.exists(out) or open(out).read() != text:
+        with open(out, "w") as fh:
+            fh.write(text)
+
+
+if __name__ == "__main__":
+    main()
