@@ -60,6 +60,7 @@ extern "C" {
 #define LBMGPU_MAX_SPECIES 12
 #define LBMGPU_MAX_REACTIONS 48
 #define LBMGPU_MAX_RSPEC 3     /* species per side of a reaction */
+#define LBMGPU_MAX_ELEMENTS 5  /* H, O, N, Ar, C */
 
 enum { LBMGPU_RXN_ELEMENTARY = 0, LBMGPU_RXN_THREEBODY = 1, LBMGPU_RXN_FALLOFF = 2 };
 enum { LBMGPU_GEOM_ATOM = 0, LBMGPU_GEOM_LINEAR = 1, LBMGPU_GEOM_NONLINEAR = 2 };
@@ -77,7 +78,7 @@ typedef struct lbmgpu_mech {
     double dipole[LBMGPU_MAX_SPECIES];            /* C m                                 */
     double polarizability[LBMGPU_MAX_SPECIES];    /* m^3                                 */
     double rot_relax[LBMGPU_MAX_SPECIES];         /* Z_rot at 298 K                      */
-    int elements[LBMGPU_MAX_SPECIES][4];          /* atoms of H, O, N, Ar per molecule   */
+    int elements[LBMGPU_MAX_SPECIES][LBMGPU_MAX_ELEMENTS]; /* atoms of H, O, N, Ar, C      */
     int rtype[LBMGPU_MAX_REACTIONS];              /* LBMGPU_RXN_*                        */
     int reversible[LBMGPU_MAX_REACTIONS];
     int n_reac[LBMGPU_MAX_REACTIONS], n_prod[LBMGPU_MAX_REACTIONS];
@@ -88,6 +89,11 @@ typedef struct lbmgpu_mech {
     int troe_n[LBMGPU_MAX_REACTIONS];             /* 0 Lindemann, 3 or 4 Troe parameters  */
     double troe[LBMGPU_MAX_REACTIONS][4];         /* a, T***, T*, T**                    */
     double eff[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_SPECIES]; /* third-body efficiencies      */
+    /* forward reaction orders of the reactants in reac[][] (the mass-action exponents of the
+     * forward rate): nu_reac unless the mechanism gives `orders` (the global CH4 and C3H8
+     * steps of src/reaction-mech/CH4_2S.yaml and propane_mech.yaml); a non-integer order
+     * takes the concentration clipped at zero */
+    double order_reac[LBMGPU_MAX_REACTIONS][LBMGPU_MAX_RSPEC];
 } lbmgpu_mech;
 
 /* Byte offsets of the fields of the caller's MIXTURE record (src/headers/lbm.hpp:56-88).
@@ -252,17 +258,17 @@ int lbmgpu_kernel_times(lbmgpu_t *h, int nkinds, long *launches, double *ms);
  * host, OutputKeEns in src/output.cpp):
  *   out[0] mass sum rho, out[1..3] momentum sum rho u, out[4] total energy (sum rhoE),
  *   multicomponent also out[5 .. 5+ns-1] the species masses sum rho_a and
- *   out[5+ns .. 5+ns+3] the element totals sum_a rho_a / W_a * (atoms of H, O, N, Ar),
+ *   out[5+ns .. 5+ns+4] the element totals sum_a rho_a / W_a * (atoms of H, O, N, Ar, C),
  * all in lattice units.  lbmgpu_sums_count gives the number of values (5, or
- * 5 + n_species + 4); n_out must be at least that.  The reduction order is fixed, so
+ * 5 + n_species + 5); n_out must be at least that.  The reduction order is fixed, so
  * the totals are reproducible bit for bit.  The first call allocates the handle's
  * reduction scratch (LBMGPU_SUMS_MAX * 1185 doubles); the call waits for the stream. */
-#define LBMGPU_SUMS_MAX 21
+#define LBMGPU_SUMS_MAX 22
 int lbmgpu_sums_count(const lbmgpu_t *h);
 int lbmgpu_sums(lbmgpu_t *h, double *out, int n_out);
 
 /* lbmgpu_sums without any device allocation, no counterpart in the reference: the
- * reduction scratch is a fixed device array of the library (199,080 bytes per device)
+ * reduction scratch is a fixed device array of the library (208,560 bytes per device)
  * instead of handle memory, for callers that cannot allocate after setup (a lattice that
  * fills the device, a monitoring loop that must not synchronise the device through
  * cudaMalloc, a host whose pool owns all device memory).  Same values, bit for bit, as

@@ -90,7 +90,7 @@ GAS_HD void reactor_rhs_dense(const Tables &t, double rho, const double *y, doub
         double fwd = kf * M, rev = 0.0;
 #pragma unroll
         for (int k = 0; k < NS; ++k)
-            if (t.nu_f[r][k] != 0.0) fwd *= conc_pow(C[k], t.nu_f[r][k]);
+            if (t.ord_f[r][k] != 0.0) fwd *= conc_pow(C[k], t.ord_f[r][k]);
         if (m.reversible[r]) {
             double dG = 0.0;
 #pragma unroll
@@ -144,42 +144,59 @@ GAS_HD bool lu_factor(double (*M)[MAXS + 1], int n, int *piv) {
     return true;
 }
 
-// lu_factor / lu_solve for a matrix of compile-time size N (the device integrator).
+// The iteration matrix of the compile-time-sized integrators: an N x N array of the thread
+// (registers, or local memory where the pivoting indexes it), or a view of the thread's
+// matrix in shared memory, element (r, c) at p[(r N + c) stride] so that the threads of a
+// warp touch consecutive words.
 template <int N>
-GAS_HD bool lu_factor_n(double (&M)[N][N], int *piv) {
+struct RegMat {
+    double a[N][N];
+    GAS_HD double &operator()(int r, int c) { return a[r][c]; }
+    GAS_HD double operator()(int r, int c) const { return a[r][c]; }
+};
+template <int N>
+struct SharedMat {
+    double *p;
+    int stride;
+    GAS_HD double &operator()(int r, int c) const { return p[(r * N + c) * stride]; }
+};
+
+// lu_factor / lu_solve for a matrix of compile-time size N (the device integrator).
+template <int N, class Mat>
+GAS_HD bool lu_factor_n(Mat &M, int *piv) {
     for (int c = 0; c < N; ++c) {
         int p = c;
         for (int r = c + 1; r < N; ++r)
-            if (fabs(M[r][c]) > fabs(M[p][c])) p = r;
+            if (fabs(M(r, c)) > fabs(M(p, c))) p = r;
         piv[c] = p;
-        if (M[p][c] == 0.0) return false;
+        if (M(p, c) == 0.0) return false;
         if (p != c)
             for (int q = 0; q < N; ++q) {
-                const double tmp = M[c][q];
-                M[c][q] = M[p][q];
-                M[p][q] = tmp;
+                const double tmp = M(c, q);
+                M(c, q) = M(p, q);
+                M(p, q) = tmp;
             }
         for (int r = c + 1; r < N; ++r) {
-            const double f = M[r][c] / M[c][c];
-            M[r][c] = f;
-            for (int q = c + 1; q < N; ++q) M[r][q] -= f * M[c][q];
+            const double f = M(r, c) / M(c, c);
+            M(r, c) = f;
+            for (int q = c + 1; q < N; ++q) M(r, q) -= f * M(c, q);
         }
     }
     return true;
 }
-template <int N>
-GAS_HD void lu_solve_n(const double (&M)[N][N], const int *piv, double *b) {
+template <int N, class Mat>
+GAS_HD void lu_solve_n(const Mat &M, const int *piv, double *b) {
     for (int c = 0; c < N; ++c) {
         const double tmp = b[c];
         b[c] = b[piv[c]];
         b[piv[c]] = tmp;
     }
     for (int r = 1; r < N; ++r)
-        for (int q = 0; q < r; ++q) b[r] -= M[r][q] * b[q];
+        for (int q = 0; q < r; ++q) b[r] -= M(r, q) * b[q];
     for (int r = N - 1; r >= 0; --r) {
         double v = b[r];
-        for (int q = r + 1; q < N; ++q) v -= M[r][q] * b[q];
-        b[r] = v / M[r][r];
+        for (int q = r + 1; q < N; ++q) v -= M(r, q) * b[q];
+        b[r] = v / M(r, r);
     }
 }
 
@@ -269,8 +286,8 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
 
 // The kinetics policies ros2_advance_k takes: `K` the temperature factors, `factors(T, K)`
 // forms them, `rhs(K, rho, y, F)` is the reactor's right-hand side at y from the factors at
-// y's temperature; with kAnalyticJacobian, `jacobian(K, rho, y, F, J)` writes the species
-// columns of dF/d(Y, T) (the finite differences are taken otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
+// y's temperature; with kAnalyticJacobian, `jacobian(K, rho, y, F, s, J)` writes s times the
+// species columns of dF/d(Y, T) (the finite differences are taken otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
 // factors inside each right-hand side (reactor_rhs_dense: nothing per reaction kept between
 // calls); a mechanism compiled to straight-line code (gen_kinetics.py) provides its own policy
 // whose factors are formed once per temperature.
@@ -302,13 +319,12 @@ struct CachedTableKinetics {
 // analytic Jacobian replaces the species columns' finite differences (ROS2 is a W-method:
 // its order holds for any Jacobian approximation, so only rounding-level differences in
 // the step-size decisions separate the two).
-template <int NS, class Kin>
-GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
-                          double atol = 1e-10, double atol_T = 1e-3) {
+template <int NS, class Kin, class Mat>
+GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                           double atol = 1e-10, double atol_T = 1e-3) {
     constexpr int ns = NS, n = NS + 1;
     const double gam = 1.0 + 1.0 / sqrt(2.0);
     double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
-    double M[n][n];
     int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
@@ -318,16 +334,13 @@ GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, doub
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        typename Kin::K K0;
-        kin.factors(y[ns], K0);
-        kin.rhs(K0, rho, y, F0);
+        // one set of temperature factors, formed at y, then at the temperature column's and
+        // the second stage's temperatures in turn
+        typename Kin::K Kf;
+        kin.factors(y[ns], Kf);
+        kin.rhs(Kf, rho, y, F0);
         if constexpr (Kin::kAnalyticJacobian) {
-            kin.jacobian(K0, rho, y, F0, M);
-            const double s = -gam * h;
-#pragma unroll
-            for (int r = 0; r < n; ++r)
-#pragma unroll
-                for (int c = 0; c < ns; ++c) M[r][c] *= s;
+            kin.jacobian(Kf, rho, y, F0, -gam * h, M);
         } else {
             // the species columns in a rolled loop (one inlined right-hand side); the perturbed
             // component is selected by comparison so that yp stays in registers
@@ -340,9 +353,9 @@ GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, doub
                 const double eps = 1e-8 * fmax(fabs(yc), 1e-6);
 #pragma unroll
                 for (int q = 0; q < n; ++q) yp[q] = q == c ? y[q] + eps : y[q];
-                kin.rhs(K0, rho, yp, Fp);
+                kin.rhs(Kf, rho, yp, Fp);
 #pragma unroll
-                for (int r = 0; r < n; ++r) M[r][c] = -gam * h * (Fp[r] - F0[r]) / eps;
+                for (int r = 0; r < n; ++r) M(r, c) = -gam * h * (Fp[r] - F0[r]) / eps;
             }
         }
         {  // the temperature column
@@ -350,13 +363,12 @@ GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, doub
 #pragma unroll
             for (int q = 0; q < n; ++q) yp[q] = y[q];
             yp[ns] += eps;
-            typename Kin::K Kt;
-            kin.factors(yp[ns], Kt);
-            kin.rhs(Kt, rho, yp, Fp);
+            kin.factors(yp[ns], Kf);
+            kin.rhs(Kf, rho, yp, Fp);
 #pragma unroll
-            for (int r = 0; r < n; ++r) M[r][ns] = -gam * h * (Fp[r] - F0[r]) / eps;
+            for (int r = 0; r < n; ++r) M(r, ns) = -gam * h * (Fp[r] - F0[r]) / eps;
         }
-        for (int r = 0; r < n; ++r) M[r][r] += 1.0;
+        for (int r = 0; r < n; ++r) M(r, r) += 1.0;
         if (!lu_factor_n<n>(M, piv)) {
             h *= 0.25;
             continue;
@@ -366,11 +378,8 @@ GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, doub
         lu_solve_n<n>(M, piv, k1);
 #pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
-        {
-            typename Kin::K K2;
-            kin.factors(yp[ns], K2);
-            kin.rhs(K2, rho, yp, Fp);
-        }
+        kin.factors(yp[ns], Kf);
+        kin.rhs(Kf, rho, yp, Fp);
 #pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
         lu_solve_n<n>(M, piv, k2);
@@ -398,6 +407,14 @@ GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, doub
     return done ? acc : -1;
 }
 
+// ros2_advance_km with the iteration matrix in the thread's own array.
+template <int NS, class Kin>
+GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
+                          double atol = 1e-10, double atol_T = 1e-3) {
+    RegMat<NS + 1> M;
+    return ros2_advance_km<NS>(kin, M, rho, Y, T, dt, rtol, atol, atol_T);
+}
+
 // ros2_advance_k over the tables of any mechanism of NS species.
 template <int NS>
 GAS_HD int ros2_advance_n(const Tables &t, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
@@ -423,8 +440,8 @@ __device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double 
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (lane & ~(G - 1));
     const double gam = 1.0 + 1.0 / sqrt(2.0);
     double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
-    double M[n][n];
     double Fc[kPer][n], ec[kPer];  // this lane's right-hand sides and their steps
+    RegMat<n> M;
     int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
@@ -471,8 +488,8 @@ __device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double 
 #pragma unroll
         for (int c = 0; c < n; ++c)
 #pragma unroll
-            for (int r = 0; r < n; ++r) M[r][c] = __shfl_sync(gmask, Fc[c / G][r], c % G, G);
-        for (int r = 0; r < n; ++r) M[r][r] += 1.0;
+            for (int r = 0; r < n; ++r) M(r, c) = __shfl_sync(gmask, Fc[c / G][r], c % G, G);
+        for (int r = 0; r < n; ++r) M(r, r) += 1.0;
         if (!lu_factor_n<n>(M, piv)) {
             h *= 0.25;
             continue;

@@ -72,6 +72,7 @@ struct Tables {
     // dense stoichiometry (species k of reaction r; 0 where k does not take part): reactant and
     // product coefficients and their net difference, for the compile-time-unrolled kinetics
     double nu_f[MAXR][MAXS], nu_b[MAXR][MAXS], nu_net[MAXR][MAXS], dnu[MAXR];
+    double ord_f[MAXR][MAXS];  // forward reaction orders (mech.order_reac) by species
 };
 
 constexpr double kFitTlo = 200.0, kFitThi = 3500.0, kFitX0 = 7.0;
@@ -339,12 +340,14 @@ GAS_HD void rate_factors(const Tables &t, double T, RateT &K) {
 }
 
 // C^nu of a mass-action factor: a product for the integer orders 1 to 3 (the elementary
-// stoichiometries of the mechanisms), pow otherwise.
+// stoichiometries of the mechanisms), otherwise pow of the concentration clipped at zero (a
+// fractional order of a global step, or a half-integer stoichiometric coefficient, has no
+// real value at the slightly negative concentrations a transported species can take).
 GAS_HD double conc_pow(double C, double nu) {
     if (nu == 1.0) return C;
     if (nu == 2.0) return C * C;
     if (nu == 3.0) return C * C * C;
-    return pow(C, nu);
+    return pow(fmax(C, 0.0), nu);
 }
 
 // Forward and reverse rates of progress (kmol/m^3/s) of reaction r from its temperature
@@ -370,7 +373,7 @@ GAS_HD void progress_one(const Tables &t, int r, const double *C, double kf, dou
         M = 1.0;
     }
     double fwd = kf * M, rev = 0.0;
-    for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.nu_reac[r][j]);
+    for (int j = 0; j < m.n_reac[r]; ++j) fwd *= conc_pow(C[m.reac[r][j]], m.order_reac[r][j]);
     if (m.reversible[r]) {
         rev = kf * M * er;  // kf / Kc
         for (int j = 0; j < m.n_prod[r]; ++j) rev *= conc_pow(C[m.prod[r][j]], m.nu_prod[r][j]);
@@ -471,10 +474,11 @@ inline void make_tables(const lbmgpu_mech &m, Tables &t) {
     for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = 0.0;
     for (int r = 0; r < MAXR; ++r) {
         t.dnu[r] = 0.0;
-        for (int k = 0; k < MAXS; ++k) t.nu_f[r][k] = t.nu_b[r][k] = t.nu_net[r][k] = 0.0;
+        for (int k = 0; k < MAXS; ++k) t.nu_f[r][k] = t.nu_b[r][k] = t.nu_net[r][k] = t.ord_f[r][k] = 0.0;
     }
     for (int r = 0; r < m.n_reactions; ++r) {
         for (int j = 0; j < m.n_reac[r]; ++j) t.nu_f[r][m.reac[r][j]] += m.nu_reac[r][j];
+        for (int j = 0; j < m.n_reac[r]; ++j) t.ord_f[r][m.reac[r][j]] += m.order_reac[r][j];
         for (int j = 0; j < m.n_prod[r]; ++j) t.nu_b[r][m.prod[r][j]] += m.nu_prod[r][j];
         for (int k = 0; k < t.ns; ++k) {
             t.nu_net[r][k] = t.nu_b[r][k] - t.nu_f[r][k];

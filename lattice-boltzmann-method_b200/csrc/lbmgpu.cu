@@ -18,6 +18,7 @@
 
 #include "../../include/lbmgpu.h"
 #include "handle.cuh"
+#include "mc_ops.cuh"
 #include "sc_kernels.cuh"
 #include "sums.cuh"
 #include "halo.cuh"
@@ -393,7 +394,9 @@ bool valid_mech(const lbmgpu_mech &m) {
         if (m.n_reac[r] < 1 || m.n_reac[r] > LBMGPU_MAX_RSPEC || m.n_prod[r] < 1 || m.n_prod[r] > LBMGPU_MAX_RSPEC)
             return false;
         for (int j = 0; j < m.n_reac[r]; ++j)
-            if (m.reac[r][j] < 0 || m.reac[r][j] >= m.n_species) return false;
+            if (m.reac[r][j] < 0 || m.reac[r][j] >= m.n_species || !(m.order_reac[r][j] >= 0.0) ||
+                !(m.order_reac[r][j] <= 4.0))
+                return false;
         for (int j = 0; j < m.n_prod[r]; ++j)
             if (m.prod[r][j] < 0 || m.prod[r][j] >= m.n_species) return false;
         if (m.troe_n[r] != 0 && m.troe_n[r] != 3 && m.troe_n[r] != 4) return false;
@@ -454,7 +457,7 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
     } else {
         if (!desc->mech || desc->mech->n_species != desc->n_species) return LBMGPU_E_ARG;
         if (!valid_mech(*desc->mech)) return LBMGPU_E_ARG;
-        if (desc->n_species != 9) return LBMGPU_E_UNSUPPORTED;  // kernels are built for 9 species
+        if (!lbmh::mc_ns_built(desc->n_species)) return LBMGPU_E_UNSUPPORTED;  // the kernels' species counts
         if (desc->chem_mode != LBMGPU_CHEM_OFF && desc->chem_mode != LBMGPU_CHEM_REF_EXPLICIT &&
             desc->chem_mode != LBMGPU_CHEM_ROSENBROCK)
             return LBMGPU_E_UNSUPPORTED;

@@ -503,7 +503,9 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // ros2_advance_group, and only the group's first lane writes the results.
 // KIN (device): the kinetics policy of a mechanism compiled to straight-line code
 // (gen_kinetics.py) when the handle's mechanism is that one, void for the tables.
-template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1, class KIN = void>
+// SMAT (device, G = 1, KIN): the integrator's iteration matrix in the dynamic shared memory
+// the kernel was launched with, (NS + 1)^2 doubles per thread of the block.
+template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1, class KIN = void, bool SMAT = false>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
     const gas::Tables &t = *A.tab;
@@ -558,7 +560,11 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
                 rc = gas::ros2_advance_group<NS, G>(KIN{}, rho_si, Yc, Tc, dt_si);
             else if constexpr (G > 1)
                 rc = gas::ros2_advance_group<NS, G>(gas::CachedTableKinetics{t}, rho_si, Yc, Tc, dt_si);
-            else if constexpr (!std::is_void_v<KIN>)
+            else if constexpr (!std::is_void_v<KIN> && SMAT) {
+                extern __shared__ double mc_chem_smem[];
+                gas::SharedMat<NS + 1> Ms{mc_chem_smem + threadIdx.x, (int)blockDim.x};
+                rc = gas::ros2_advance_km<NS>(KIN{}, Ms, rho_si, Yc, Tc, dt_si);
+            } else if constexpr (!std::is_void_v<KIN>)
                 rc = gas::ros2_advance_k<NS>(KIN{}, rho_si, Yc, Tc, dt_si);
             else
                 rc = gas::ros2_advance_n<NS>(t, rho_si, Yc, Tc, dt_si);

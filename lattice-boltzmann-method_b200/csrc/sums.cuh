@@ -1,13 +1,15 @@
 // Shared constants and host helpers of the conserved-sums reduction (sums.cu).
 #pragma once
 
+#include "../../include/lbmgpu.h"
+
 struct lbmgpu;
 
 namespace lbmh {
 
 constexpr int kSumBlock = 256;              // threads per block of the partials kernel
 constexpr int kSumMaxBlocks = 148 * 8;      // grid cap: 8 blocks per SM of a B200
-constexpr int kSumElements = 4;             // H, O, N, Ar (lbmgpu_mech.elements)
+constexpr int kSumElements = LBMGPU_MAX_ELEMENTS;  // H, O, N, Ar, C (lbmgpu_mech.elements)
 constexpr int kSumMax = 5 + 12 + kSumElements;  // LBMGPU_SUMS_MAX
 
 int sums_count(const lbmgpu *h);

@@ -17,8 +17,8 @@
 // is still allowed, and no later call of this entry point allocates.
 //
 // Limits and rules:
-//   - Scratch size: kSumMaxBlocks * kSumMax partials + kSumMax totals = 1184 * 21 + 21
-//     doubles (199,080 bytes) per device, held from the first handle's creation on that
+//   - Scratch size: kSumMaxBlocks * kSumMax partials + kSumMax totals = 1184 * 22 + 22
+//     doubles (208,560 bytes) per device, held from the first handle's creation on that
 //     device until the process exits.  The reduction grid is capped at kSumMaxBlocks
 //     blocks, so every lattice fits; n_out above LBMGPU_SUMS_MAX (or below the handle's
 //     lbmgpu_sums_count) is rejected with LBMGPU_E_ARG.

@@ -771,10 +771,10 @@ int sur_create(lbmgpu *h) {
     CK(cudaMemsetAsync(s->audit, 0, 6 * sizeof(double), h->stream));
     default_norm(s->nrm_h);
     CK(cudaMemcpyAsync(s->nrm, &s->nrm_h, sizeof(SurNorm), cudaMemcpyHostToDevice, h->stream));
-    double el[9][4], W[9], proj[9 * 9];
+    double el[9][LBMGPU_MAX_ELEMENTS], W[9], proj[9 * 9];
     for (int k = 0; k < 9; ++k) {
         W[k] = h->mech.W[k];
-        for (int e = 0; e < 4; ++e) el[k][e] = h->mech.elements[k][e];
+        for (int e = 0; e < LBMGPU_MAX_ELEMENTS; ++e) el[k][e] = h->mech.elements[k][e];
     }
     sur_projector<9>(el, W, proj);
     CK(cudaMemcpyAsync(s->proj, proj, sizeof proj, cudaMemcpyHostToDevice, h->stream));

@@ -73,17 +73,18 @@ __host__ __device__ inline void sur_features(double T_si, double P_si, const dou
 // host from the mechanism (Gauss-Jordan elimination with partial pivoting on the small,
 // symmetric positive definite A A^T); proj is row-major [NS][NS].
 template <int NS>
-inline void sur_projector(const double (*elements)[4], const double *W, double *proj) {
-    double A[4][NS];
+inline void sur_projector(const double (*elements)[LBMGPU_MAX_ELEMENTS], const double *W, double *proj) {
+    constexpr int kE = LBMGPU_MAX_ELEMENTS;
+    double A[kE][NS];
     int ne = 0;
-    for (int e = 0; e < 4; ++e) {
+    for (int e = 0; e < kE; ++e) {
         bool any = false;
         for (int k = 0; k < NS; ++k) any = any || elements[k][e] != 0.0;
         if (!any) continue;
         for (int k = 0; k < NS; ++k) A[ne][k] = elements[k][e] / W[k];
         ++ne;
     }
-    double G[4][8];  // [A A^T | I] -> [I | (A A^T)^-1]
+    double G[kE][2 * kE];  // [A A^T | I] -> [I | (A A^T)^-1]
     for (int i = 0; i < ne; ++i)
         for (int j = 0; j < ne; ++j) {
             double g = 0.0;

@@ -91,29 +91,38 @@ def emit_jacobian(m, L, fidx):
     fixed T and rho from the factors at y's temperature, differentiating rhs_k's expressions:
     the mass-action products, the third-body sum M (efficiency-weighted concentrations) and
     the Troe blending F(Pr), Pr = k0 M / k_inf; and dT/dt's row through net production and
-    c_v.  With D_kj = d wdot_k / d C_j (C_j = rho Y_j / W_j):
-        J_kj = D_kj W_k / W_j,
-        J_Tj = -(R T / (W_j c_v)) sum_k (h_k/RT - 1) D_kj - F_T R (c_p,j/R - 1) / (W_j c_v).
-    The fall-off derivative: d(k_inf Pr/(1+Pr) F)/dM = k0 [F/(1+Pr)^2 + F (-2 x lFc / (1+x^2)^2)
-    n / ((n - 0.14 u)^2 (1+Pr))], u = log10 Pr + c, x = u / (n - 0.14 u)."""
+    c_v.  With dq_rj = d q_r / d C_j (C_j = rho Y_j / W_j) and nu_kr the net coefficients:
+        J_kj = (W_k / W_j) sum_r nu_kr dq_rj,
+        J_Tj = -(R T / (W_j c_v)) sum_r e_r dq_rj - F_T R (c_p,j/R - 1) / (W_j c_v),
+    e_r = sum_k nu_kr (h_k/RT - 1), every term accumulated straight into the scaled matrix
+    (s J, s = -gamma h for the integrator's iteration matrix).  The fall-off derivative:
+    d(k_inf Pr/(1+Pr) F)/dM = k0 F/(1+Pr) [1/(1+Pr) - 2 x lFc n / ((1+x^2)^2 (n - 0.14 u)^2)],
+    u = log10 Pr + c, x = u / (n - 0.14 u)."""
     ns, nr = m.n_species, m.n_reactions
+    W = [m.W[k] for k in range(ns)]
     add = L.append
-    add("// The species columns of the Jacobian of F (rhs_k) with respect to (Y, T): J[k][j] =")
-    add("// dF_k / dY_j for j < NS and every row k <= NS, at fixed temperature and density, from the")
-    add("// factors at y's temperature and F = rhs_k(K, rho, y).  Column NS is not written.")
-    add("GAS_HD void jac_species(const Factors &K, double rho, const double *y, const double *F,")
-    add("                        double (&J)[NS + 1][NS + 1]) {")
+    add("// s times the species columns of the Jacobian of F (rhs_k) with respect to (Y, T):")
+    add("// J(k, j) = s dF_k / dY_j for j < NS and every row k <= NS, at fixed temperature and")
+    add("// density, from the factors at y's temperature and F = rhs_k(K, rho, y).  Column NS is not")
+    add("// written.")
+    add("template <class Mat>")
+    add("GAS_HD void jac_species(const Factors &K, double rho, const double *y, const double *F, double s, Mat &J) {")
     add(f"    const double T = y[{ns}];")
     for k in range(ns):
         add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
-    add(f"    double D[{ns}][{ns}];  // d wdot_k / d C_j")
+    add("    double cv = 0.0;")
+    for k in range(ns):
+        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
+    add(f"    cv *= {lit(KR)};")
+    add(f"    const double sT = -s * {lit(KR)} * T / cv;  // times e_r dq_rj / W_j: the T row")
     add("#pragma unroll")
-    add(f"    for (int k = 0; k < {ns}; ++k)")
+    add(f"    for (int k = 0; k <= {ns}; ++k)")
     add("#pragma unroll")
-    add(f"        for (int j = 0; j < {ns}; ++j) D[k][j] = 0.0;")
+    add(f"        for (int j = 0; j < {ns}; ++j) J(k, j) = 0.0;")
     for r in range(nr):
         reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
         prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
+        ordr = [(m.reac[r][j], m.order_reac[r][j]) for j in range(m.n_reac[r])]
         net = {}
         for k, nu in reac:
             net[k] = net.get(k, 0.0) - nu
@@ -148,7 +157,7 @@ def emit_jacobian(m, L, fidx):
             else:
                 add(f"        const double kfM = K.kf[{r}] * M;")
                 add(f"        const double dkdM = K.kf[{r}];")
-        pf = " * ".join(conc(k, nu) for k, nu in reac)
+        pf = " * ".join(conc(k, nu) for k, nu in ordr)
         rev = bool(m.reversible[r])
         if m.rtype[r] != 0:
             pb = " * ".join(conc(k, nu) for k, nu in prod)
@@ -156,10 +165,9 @@ def emit_jacobian(m, L, fidx):
                 add(f"        const double g = dkdM * ({pf} - K.er[{r}] * {pb});")
             else:
                 add(f"        const double g = dkdM * {pf};")
-        # dq/dC_j for the reaction's own species
         dq = {}
-        for idx, (k, nu) in enumerate(reac):
-            others = [x for jdx, x in enumerate(reac) if jdx != idx]
+        for idx, (k, nu) in enumerate(ordr):
+            others = [x for jdx, x in enumerate(ordr) if jdx != idx]
             dq.setdefault(k, []).append(("+", dpow(k, nu, others)))
         if rev:
             for idx, (k, nu) in enumerate(prod):
@@ -180,30 +188,17 @@ def emit_jacobian(m, L, fidx):
             expr = " ".join(parts)
             expr = expr[2:] if expr.startswith("+ ") else "-" + expr[2:]
             add(f"        const double dq{j} = {expr};")
-        for k, v in net.items():
-            for j in cols:
-                add(f"        D[{k}][{j}] += {'' if v == 1.0 else ('-' if v == -1.0 else lit(v) + ' * ')}dq{j};"
-                    .replace("+= -", "-= "))
+        # e_r = sum_k nu_kr (h_k/RT - 1) for the T row
+        er_terms = " + ".join(f"{lit(v)} * (K.hRT[{k}] - 1.0)" for k, v in net.items()) or "0.0"
+        add(f"        const double eT = sT * ({er_terms});")
+        for j in cols:
+            for k, v in net.items():
+                add(f"        J({k}, {j}) += {lit(v * W[k] / W[j])} * s * dq{j};")
+            add(f"        J({ns}, {j}) += {lit(1.0 / W[j])} * eT * dq{j};")
         add("    }")
-    # assemble J
-    add("    double cv = 0.0;")
-    for k in range(ns):
-        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
-    add(f"    cv *= {lit(KR)};")
-    add(f"    const double RT_cv = {lit(KR)} * T / cv;")
-    add("#pragma unroll")
-    add(f"    for (int j = 0; j < {ns}; ++j) {{")
-    add("        double sT = 0.0;")
-    add("#pragma unroll")
-    add(f"        for (int k = 0; k < {ns}; ++k) sT += (K.hRT[k] - 1.0) * D[k][j];")
-    W = ", ".join(lit(m.W[k]) for k in range(ns))
-    iW = ", ".join(lit(1.0 / m.W[k]) for k in range(ns))
-    add(f"        constexpr double Wk[{ns}] = {{{W}}};")
-    add(f"        constexpr double iWk[{ns}] = {{{iW}}};")
-    add("#pragma unroll")
-    add(f"        for (int k = 0; k < {ns}; ++k) J[k][j] = D[k][j] * Wk[k] * iWk[j];")
-    add(f"        J[{ns}][j] = -(RT_cv * sT + F[{ns}] * {lit(KR)} * (K.cpR[j] - 1.0) / cv) * iWk[j];")
-    add("    }")
+    add(f"    const double sF = s * F[{ns}] * {lit(KR)} / cv;")
+    for j in range(ns):
+        add(f"    J({ns}, {j}) -= sF * (K.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
     add("}")
     add("")
 
@@ -239,8 +234,8 @@ def generate(m, name):
         add(f"    if (m.rtype[{r}] != {m.rtype[r]} || m.reversible[{r}] != {m.reversible[r]} || m.n_reac[{r}] != "
             f"{m.n_reac[r]} || m.n_prod[{r}] != {m.n_prod[r]}) return false;")
         for j in range(m.n_reac[r]):
-            add(f"    if (m.reac[{r}][{j}] != {m.reac[r][j]} || m.nu_reac[{r}][{j}] != {lit(m.nu_reac[r][j])}) "
-                f"return false;")
+            add(f"    if (m.reac[{r}][{j}] != {m.reac[r][j]} || m.nu_reac[{r}][{j}] != {lit(m.nu_reac[r][j])} || "
+                f"m.order_reac[{r}][{j}] != {lit(m.order_reac[r][j])}) return false;")
         for j in range(m.n_prod[r]):
             add(f"    if (m.prod[{r}][{j}] != {m.prod[r][j]} || m.nu_prod[{r}][{j}] != {lit(m.nu_prod[r][j])}) "
                 f"return false;")
@@ -333,6 +328,7 @@ def generate(m, name):
     for r in range(nr):
         reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
         prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
+        ordr = [(m.reac[r][j], m.order_reac[r][j]) for j in range(m.n_reac[r])]
         eq = " + ".join(f"{nu:g} {names[k]}" for k, nu in reac) + (" <=> " if m.reversible[r] else " => ") + \
             " + ".join(f"{nu:g} {names[k]}" for k, nu in prod)
         tag = "  (+M)" if m.rtype[r] == FALLOFF else ("  + M" if m.rtype[r] == THREEBODY else "")
@@ -356,7 +352,7 @@ def generate(m, name):
                     add(f"        const double kfM = K.kf[{r}] * (Pr / (1.0 + Pr)) * 1.0;")
             else:
                 add(f"        const double kfM = K.kf[{r}] * M;")
-        add("        const double fwd = kfM" + "".join(f" * {conc(k, nu)}" for k, nu in reac) + ";")
+        add("        const double fwd = kfM" + "".join(f" * {conc(k, nu)}" for k, nu in ordr) + ";")
         if m.reversible[r]:
             add(f"        const double rev = kfM * K.er[{r}]" + "".join(f" * {conc(k, nu)}" for k, nu in prod) + ";")
             add("        const double q = fwd - rev;")
@@ -386,9 +382,9 @@ def generate(m, name):
     add("    GAS_HD void rhs(const Factors &k, double rho, const double *y, double *F) const {")
     add("        rhs_k(k, rho, y, F);")
     add("    }")
-    add("    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F,")
-    add("                         double (&J)[NS + 1][NS + 1]) const {")
-    add("        jac_species(k, rho, y, F, J);")
+    add("    template <class Mat>")
+    add("    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F, double s, Mat &J) const {")
+    add("        jac_species(k, rho, y, F, s, J);")
     add("    }")
     add("};")
     add("")

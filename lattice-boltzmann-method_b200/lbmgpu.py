@@ -45,7 +45,7 @@ EXPORTS = [
     "lbmgpu_surrogate_enable", "lbmgpu_surrogate_eval", "lbmgpu_surrogate_params", "lbmgpu_surrogate_stats",
     "lbmgpu_surrogate_grads",
 ]
-SUMS_MAX = 21
+SUMS_MAX = 22
 HALO_POPULATIONS, HALO_RECORD = 0, 1
 KERNEL_KINDS = 8
 DIAG_COUNT = 6
@@ -360,7 +360,7 @@ class Lattice:
     # -- conserved sums -------------------------------------------------------------------
     def sums(self):
         """FP64 totals over the fluid cells: mass, momentum (3), total energy, then
-        (multicomponent) the species masses and the H, O, N, Ar element totals."""
+        (multicomponent) the species masses and the H, O, N, Ar, C element totals."""
         k = self.L.lbmgpu_sums_count(self.h)
         _check(k if k < 0 else 0, "lbmgpu_sums_count")
         out = (ctypes.c_double * k)()

@@ -24,7 +24,8 @@ GEOM = {"atom": 0, "linear": 1, "nonlinear": 2}
 
 # IUPAC standard atomic weights (kg/kmol) of the elements these mechanisms contain
 ATOMIC_WEIGHT = {"H": 1.008, "O": 15.999, "N": 14.007, "Ar": 39.95, "He": 4.002602, "C": 12.011}
-ELEMENT_SLOT = {"H": 0, "O": 1, "N": 2, "Ar": 3}
+ELEMENT_SLOT = {"H": 0, "O": 1, "N": 2, "Ar": 3, "C": 4}
+MAX_ELEMENTS = 5
 DEBYE = 3.33564e-30          # C m
 CAL = 4.184                  # J
 
@@ -43,7 +44,7 @@ class Mech(ctypes.Structure):
         ("well_depth", ctypes.c_double * S), ("diameter", ctypes.c_double * S),
         ("dipole", ctypes.c_double * S), ("polarizability", ctypes.c_double * S),
         ("rot_relax", ctypes.c_double * S),
-        ("elements", (ctypes.c_int * 4) * S),
+        ("elements", (ctypes.c_int * MAX_ELEMENTS) * S),
         ("rtype", ctypes.c_int * R), ("reversible", ctypes.c_int * R),
         ("n_reac", ctypes.c_int * R), ("n_prod", ctypes.c_int * R),
         ("reac", (ctypes.c_int * K) * R), ("prod", (ctypes.c_int * K) * R),
@@ -52,6 +53,7 @@ class Mech(ctypes.Structure):
         ("A0", ctypes.c_double * R), ("b0", ctypes.c_double * R), ("Ea0", ctypes.c_double * R),
         ("troe_n", ctypes.c_int * R), ("troe", (ctypes.c_double * 4) * R),
         ("eff", (ctypes.c_double * S) * R),
+        ("order_reac", (ctypes.c_double * K) * R),
     ]
 
     def species_names(self):
@@ -112,8 +114,9 @@ def load(path, species=H2_AIR_9):
         comp = s["composition"]
         m.W[k] = sum(ATOMIC_WEIGHT[e] * n for e, n in comp.items())
         for e, n in comp.items():
-            if e in ELEMENT_SLOT:
-                m.elements[k][ELEMENT_SLOT[e]] = int(n)
+            if e not in ELEMENT_SLOT:
+                raise ValueError(f"{name}: element {e} has no slot")
+            m.elements[k][ELEMENT_SLOT[e]] = int(n)
         th = s["thermo"]
         if th["model"] != "NASA7":
             raise ValueError(f"{name}: only NASA7 thermo is supported")
@@ -150,13 +153,18 @@ def load(path, species=H2_AIR_9):
         m.reversible[nr] = int(rev)
         m.n_reac[nr] = len(reac)
         m.n_prod[nr] = len(prod)
+        orders = r.get("orders", {})
+        if not set(orders) <= set(reac):
+            raise ValueError(f"orders of non-reactants are not supported: {eq}")
         for j, (sp, nu) in enumerate(reac.items()):
             m.reac[nr][j] = idx[sp]
             m.nu_reac[nr][j] = nu
+            m.order_reac[nr][j] = float(orders.get(sp, nu))
         for j, (sp, nu) in enumerate(prod.items()):
             m.prod[nr][j] = idx[sp]
             m.nu_prod[nr][j] = nu
-        order = sum(reac.values())
+        # the rate constant's units follow the reaction's order (the forward orders)
+        order = sum(float(orders.get(sp, nu)) for sp, nu in reac.items())
         if kind == "falloff":
             hi, lo = r["high-P-rate-constant"], r["low-P-rate-constant"]
             m.A[nr] = _convert_A(hi["A"], order, conc_factor)
@@ -209,6 +217,10 @@ def _to_list(v):
 
 def from_dict(d):
     m = Mech()
+    d = dict(d)
+    if "order_reac" not in d:  # tables written before reaction orders: the stoichiometry
+        d["order_reac"] = d["nu_reac"]
+    d["elements"] = [list(row) + [0] * (MAX_ELEMENTS - len(row)) for row in d["elements"]]
     for name, ctype in Mech._fields_:
         v = d[name]
         if isinstance(v, int):
@@ -245,23 +257,45 @@ def load_json(path):
 
 DATA = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)), "data")
 H2_AIR_9_JSON = __import__("os").path.join(DATA, "h2_air_9.json")
+CH4_2S_JSON = __import__("os").path.join(DATA, "ch4_2s.json")
+C3H8_2S_JSON = __import__("os").path.join(DATA, "c3h8_2s.json")
+CH4_2S = ["O2", "H2O", "CH4", "CO", "CO2", "N2"]
+C3H8_2S = ["CO", "C3H8", "CO2", "H2O", "N2", "O2"]
+
+# (table, source file in the reference's src/reaction-mech, species in the phase's order)
+TABLES = [(H2_AIR_9_JSON, "nh3.yaml", H2_AIR_9), (CH4_2S_JSON, "CH4_2S.yaml", CH4_2S),
+          (C3H8_2S_JSON, "propane_mech.yaml", C3H8_2S)]
 
 
 def h2_air_9():
     """The 9-species H2/O2/N2 mechanism (23 reactions) extracted from the reference's
     src/reaction-mech/nh3.yaml; regenerate with
-    ``python lattice-boltzmann-method_b200/mech.py <path to nh3.yaml>``."""
+    ``python lattice-boltzmann-method_b200/mech.py <reference src/reaction-mech directory>``."""
     return load_json(H2_AIR_9_JSON)
+
+
+def ch4_2s():
+    """The reference's 6-species, 2-step methane mechanism (src/reaction-mech/CH4_2S.yaml,
+    phase CH4_BFER_mix: CH4 + 1.5 O2 => CO + 2 H2O with orders CH4^0.5 O2^0.65, and
+    CO + 0.5 O2 <=> CO2)."""
+    return load_json(CH4_2S_JSON)
+
+
+def c3h8_2s():
+    """The reference's 6-species, 2-step propane mechanism (src/reaction-mech/propane_mech.yaml:
+    C3H8 + 3.5 O2 => 3 CO + 4 H2O with orders C3H8^0.8 O2^0.86, and CO + 0.5 O2 <=> CO2)."""
+    return load_json(C3H8_2S_JSON)
 
 
 if __name__ == "__main__":
     import sys
     os_ = __import__("os")
     os_.makedirs(DATA, exist_ok=True)
-    m = load(sys.argv[1], H2_AIR_9)
-    save_json(m, H2_AIR_9_JSON, source="nh3.yaml (farrasarira/Lattice-Boltzmann-Method src/reaction-mech), "
-                                       "species " + " ".join(H2_AIR_9))
-    # the raw struct, for C/C++ callers: fread(&mech, sizeof(lbmgpu_mech), 1, f)
-    with open(H2_AIR_9_JSON[:-5] + ".bin", "wb") as fh:
-        fh.write(bytes(m))
-    print("wrote", H2_AIR_9_JSON, m.n_species, "species", m.n_reactions, "reactions")
+    for path, src, species in TABLES:
+        m = load(os_.path.join(sys.argv[1], src), species)
+        save_json(m, path, source=f"{src} (farrasarira/Lattice-Boltzmann-Method src/reaction-mech), "
+                                  "species " + " ".join(species))
+        # the raw struct, for C/C++ callers: fread(&mech, sizeof(lbmgpu_mech), 1, f)
+        with open(path[:-5] + ".bin", "wb") as fh:
+            fh.write(bytes(m))
+        print("wrote", path, m.n_species, "species", m.n_reactions, "reactions")

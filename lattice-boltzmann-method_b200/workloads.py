@@ -168,9 +168,9 @@ def _blank_mc(NX, NY, NZ, ns):
 
 
 def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=1000.0, amp=0.1, width=None,
-                    u_si=0.0, seed=SEED, periodic_x=True):
-    """Seeded sinusoidal H2/air interface (the non-reacting mixing case): H2 mass fraction
-    from 0 to Y_H2 (balance air, O2:N2 = 0.233:0.767 by mass), T from T_lo to T_hi across a
+                    u_si=0.0, seed=SEED, periodic_x=True, fuel="H2"):
+    """Seeded sinusoidal H2/air interface (the non-reacting mixing case): H2 (or `fuel`) mass
+    fraction from 0 to Y_H2 (balance air, O2:N2 = 0.233:0.767 by mass), T from T_lo to T_hi across a
     tanh interface at x0 + A sin(2 pi y/L + phi1) sin(2 pi z/L + phi2) with random phases;
     p = 1 atm; the remaining species at mole fraction 1e-8.  With periodic_x the domain
     holds a hot H2 slab between two such interfaces (fully periodic box).  The tanh width
@@ -199,16 +199,16 @@ def mixing_layer_mc(mech, N=16, NY=None, NZ=None, Y_H2=0.03, T_lo=300.0, T_hi=10
         s = 0.5 * (1 + np.tanh((i - x0) / width))
     W = np.array([mech.W[kk] for kk in range(ns)])
     Y = np.zeros(mix.shape + (ns,))
-    Y[..., names.index("H2")] = Y_H2 * s
-    air = 1.0 - Y[..., names.index("H2")]
+    Y[..., names.index(fuel)] = Y_H2 * s
+    air = 1.0 - Y[..., names.index(fuel)]
     Y[..., names.index("O2")] = 0.233 * air
     Y[..., names.index("N2")] = 0.767 * air
     X = Y / W
     X /= X.sum(-1, keepdims=True)
     for a, n in enumerate(names):
-        if n not in ("H2", "O2", "N2"):
+        if n not in (fuel, "O2", "N2"):
             X[..., a] = SPECIES_MIN
-    X[..., names.index("H2")] = np.maximum(X[..., names.index("H2")], SPECIES_MIN)
+    X[..., names.index(fuel)] = np.maximum(X[..., names.index(fuel)], SPECIES_MIN)
     X /= X.sum(-1, keepdims=True)
     fl = ~ghost
     T = T_lo + (T_hi - T_lo) * s

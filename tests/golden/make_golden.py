@@ -186,7 +186,7 @@ def mc_digest(mix, sp):
 
 def main():
     args = [a for i, a in enumerate(sys.argv[1:]) if a != "--reference" and sys.argv[i] != "--reference"]
-    only = args[0] if args else "all"   # "sc", "mc", "mc_nofma" or "all"
+    only = args[0] if args else "all"   # "sc", "mc", "mc_nofma", "mc_shapes", "mc_mechs" or "all"
     if only in ("all", "sc"):
         make_sc()
     if only in ("all", "mc"):
@@ -195,6 +195,8 @@ def main():
         make_mc_nofma()
     if only in ("all", "mc_shapes"):
         make_mc_shapes()
+    if only in ("all", "mc_mechs"):
+        make_mc_mechs()
     print("fixtures written to", HERE)
 
 
@@ -241,6 +243,19 @@ def make_mc():
         out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
         np.savez_compressed(os.path.join(HERE, name), **out)
     make_mc_nofma()
+
+
+def make_mc_mechs():
+    """The reference's other mechanisms (6 species, two global steps with fractional reaction
+    orders): a reacting 8^3 mixing layer, a fuel-laden 1800 K slab in air (5 % CH4 or C3H8 by
+    mass), 30 steps."""
+    for name, m, fuel in (("mc_ch4_react8.npz", mechmod.ch4_2s(), "CH4"),
+                          ("mc_c3h8_react8.npz", mechmod.c3h8_2s(), "C3H8")):
+        mix, sp = cases.mixing_layer_mc(m, N=8, T_hi=1800.0, fuel=fuel, Y_H2=0.05)
+        pc = pick_cells(mix, 16, 3)
+        out = run_ref_mc(mix, sp, m, [1, 30], True, pc)
+        out.update(input_sha256=mc_digest(mix, sp), pop_cells=pc)
+        np.savez_compressed(os.path.join(HERE, name), **out)
 
 
 def make_mc_shapes():

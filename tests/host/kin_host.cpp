@@ -54,7 +54,9 @@ void kh_jac_compiled(double rho, const double *y, double *J) {
     K9::factors(y[K9::NS], K);
     double F[K9::NS + 1];
     K9::rhs_k(K, rho, y, F);
-    double (&Jm)[K9::NS + 1][K9::NS + 1] = *reinterpret_cast<double (*)[K9::NS + 1][K9::NS + 1]>(J);
-    K9::jac_species(K, rho, y, F, Jm);
+    gas::RegMat<K9::NS + 1> Jm;
+    K9::jac_species(K, rho, y, F, 1.0, Jm);
+    for (int r = 0; r <= K9::NS; ++r)
+        for (int c = 0; c < K9::NS; ++c) J[r * (K9::NS + 1) + c] = Jm(r, c);
 }
 }

@@ -3,7 +3,7 @@
 // kernels' order (periodic interior cells and the boundary cells' compact list), so tests can compare the device logic with the reference's own solver
 // on the CPU.  Test helper only; the product runs these functions on the GPU.
 //
-// mc_host_run: FP64 storage; with fout (27*10 planes of every cell) non-null it also
+// mc_host_run: FP64 storage (9 or 6 species); with fout (27*(ns+1) planes of every cell) non-null it also
 // returns the final streamed populations of the fluid cells.  mc_host_run32: populations in FP32 with (shift != 0) or
 // without the per-plane shift (the mean of each population plane over the fluid cells
 // after Init, as the device takes it), records in FP64.  Both return the index of the record
@@ -15,13 +15,12 @@
 
 namespace {
 
-template <typename S, typename RS>
-int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech, float dx, float dt, int chem,
-        int nsteps, S *pop0, S *pop1, RS *rec0, RS *rec1, int shift, unsigned *status, double *fout) {
+template <int NS, typename S, typename RS>
+int run_ns(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech, float dx, float dt, int chem,
+           int nsteps, S *pop0, S *pop1, RS *rec0, RS *rec1, int shift, unsigned *status, double *fout) {
     using namespace lbm;
     static gas::Tables tab;
     gas::make_tables(*mech, tab);
-    if (mech->n_species != 9) return -1;
     McArgsT<S, RS> A{};
     const UnitsF U = units_from_dx_dt(dx, dt);
     set_lattice_constants(tab, U);
@@ -32,7 +31,7 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
     A.ncell = (long)Nx * Ny * Nz;
     A.sj = Nz;
     A.si = (long)Ny * Nz;
-    A.ns = 9;
+    A.ns = NS;
     A.dt = 1;
     A.chem = chem;
     A.U = U;
@@ -60,10 +59,10 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
     A.cflag = cf.data();
     A.bid = bid.data();
     A.nb = (long)blist.size();
-    std::vector<double> props((size_t)pr_count<9>() * A.ncell);
+    std::vector<double> props((size_t)pr_count<NS>() * A.ncell);
     A.props = props.data();
-    for (long n = 0; n < A.ncell; ++n) mc_init_cell<9>(A, n, rec0, rec1, pop0);
-    const int np = 27 * 10;
+    for (long n = 0; n < A.ncell; ++n) mc_init_cell<NS>(A, n, rec0, rec1, pop0);
+    const int np = 27 * (NS + 1);
     std::vector<double> sh(np, 0.0);
     if (shift) {
         long cnt = 0;
@@ -99,12 +98,12 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
         A.local = local;
         A.bst_cur = bst[cur];
         for (long n = 0; n < A.ncell; ++n)
-            if (type[n] == 0) mc_collide_cell<9>(A, n);
+            if (type[n] == 0) mc_collide_cell<NS>(A, n);
         A.pop_src = pop[nx];
         A.bst_nxt = bst[nx];
         for (long n = 0; n < A.ncell; ++n)
-            if (cf[n] == CF_FLUID) mc_stream_moment_cell<9>(A, n);
-        for (long b = 0; b < A.nb; ++b) mc_special_cell<9>(A, blist[b], b);
+            if (cf[n] == CF_FLUID) mc_stream_moment_cell<NS>(A, n);
+        for (long b = 0; b < A.nb; ++b) mc_special_cell<NS>(A, blist[b], b);
         cur = nx;
         local = false;
     }
@@ -120,6 +119,17 @@ int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech
                                                                  : ldpop(A, pop[cur], q, pull_idx(pp, q % 27));
         }
     return cur;
+}
+
+// the species counts the device kernels are built for
+template <typename S, typename RS>
+int run(int Nx, int Ny, int Nz, const signed char *type, const lbmgpu_mech *mech, float dx, float dt, int chem,
+        int nsteps, S *pop0, S *pop1, RS *rec0, RS *rec1, int shift, unsigned *status, double *fout) {
+    if (mech->n_species == 9)
+        return run_ns<9>(Nx, Ny, Nz, type, mech, dx, dt, chem, nsteps, pop0, pop1, rec0, rec1, shift, status, fout);
+    if (mech->n_species == 6)
+        return run_ns<6>(Nx, Ny, Nz, type, mech, dx, dt, chem, nsteps, pop0, pop1, rec0, rec1, shift, status, fout);
+    return -1;
 }
 
 }  // namespace
@@ -139,10 +149,10 @@ extern "C" int mc_host_run32(int Nx, int Ny, int Nz, const signed char *type, co
 
 // The surrogate's element-conserving projector and its application (surrogate.cuh).
 extern "C" void sur_projector_host(const lbmgpu_mech *mech, double *proj) {
-    double el[9][4], W[9];
+    double el[9][LBMGPU_MAX_ELEMENTS], W[9];
     for (int k = 0; k < 9; ++k) {
         W[k] = mech->W[k];
-        for (int e = 0; e < 4; ++e) el[k][e] = mech->elements[k][e];
+        for (int e = 0; e < LBMGPU_MAX_ELEMENTS; ++e) el[k][e] = mech->elements[k][e];
     }
     lbm::sur_projector<9>(el, W, proj);
 }

@@ -19,14 +19,30 @@ NREC = SP0 + 8 * NS
 CASES = {
     "mc_mix8.npz": (False, {}, [1, 40]),
     "mc_react8.npz": (True, {"T_hi": 1800.0}, [1, 30]),
+    # the reference's 6-species two-step methane mechanism (CH4_2S.yaml): a CH4-laden hot
+    # slab in air, fractional reaction orders, CO oxidation reversible
+    "mc_ch4_react8.npz": (True, {"T_hi": 1800.0, "fuel": "CH4", "Y_H2": 0.05}, [1, 30]),
+    "mc_c3h8_react8.npz": (True, {"T_hi": 1800.0, "fuel": "C3H8", "Y_H2": 0.05}, [1, 30]),
 }
+
+
+def case_mech(fixture):
+    if "ch4" in fixture:
+        return mech.ch4_2s()
+    if "c3h8" in fixture:
+        return mech.c3h8_2s()
+    return mech.h2_air_9()
 
 
 def case(fixture):
     reaction, kw, cps = CASES[fixture]
-    m = mech.h2_air_9()
+    m = case_mech(fixture)
     mix, sp = W.mixing_layer_mc(m, N=8, **kw)
     return m, mix, sp, reaction, cps
+
+
+def nrec(ns):
+    return SP0 + 8 * ns
 
 
 def digest(mix, sp):
@@ -61,7 +77,8 @@ def bc_errors(R, gold, cp, fl, reaction):
     vs = max(np.abs(gold[f"{k}_{cp}"].reshape(-1)[fl]).max() for k in "uvw")
     for q, k in ((1, "u"), (2, "v"), (3, "w")):
         e[k] = rel(R[q][fl], gold[f"{k}_{cp}"].reshape(-1)[fl], vs)
-    e["rho_a"] = max(rel(R[SP0 + 8 * a][fl], gold[f"sp_rho_{cp}"][a].reshape(-1)[fl]) for a in range(NS))
+    e["rho_a"] = max(rel(R[SP0 + 8 * a][fl], gold[f"sp_rho_{cp}"][a].reshape(-1)[fl])
+                     for a in range(len(gold[f"sp_rho_{cp}"])))
     if reaction:
         e["HRR"] = rel(R[13][fl], gold[f"HRR_{cp}"].reshape(-1)[fl])
     return e
@@ -81,7 +98,8 @@ def soa_state(mix, sp):
     """The device record planes of an AoS state (the planes the upload fills from it; the
     face-difference terms stay zero until Init computes them)."""
     nc = mix.size
-    rec = np.zeros((NREC, nc))
+    ns = len(sp)
+    rec = np.zeros((nrec(ns), nc))
     f = lambda a: np.ascontiguousarray(a).reshape(-1)  # noqa: E731
     for q, k in enumerate(["rho", "u", "v", "w", "temp", "p", "rhoe"]):
         rec[q] = f(mix[k])
@@ -89,7 +107,7 @@ def soa_state(mix, sp):
     for q, (a, b) in enumerate([(0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2)]):
         rec[7 + q] = P[:, 3 * a + b]
     rec[13] = f(mix["HRR"])
-    for a in range(NS):
+    for a in range(ns):
         base = SP0 + 8 * a
         rec[base] = f(sp[a]["rho"])
         rec[base + 1] = f(sp[a]["u"])
@@ -106,14 +124,15 @@ def host_run(L, m, mix, sp, reaction, steps, precision="fp64", shift=True, pops=
     rec0 = soa_state(mix, sp)
     rec1 = rec0.copy()
     nc = mix.size
-    pop0 = np.zeros((27 * (NS + 1), nc), dt)
+    ns = len(sp)
+    pop0 = np.zeros((27 * (ns + 1), nc), dt)
     pop1 = np.zeros_like(pop0)
     typ = np.ascontiguousarray(mix["type"].astype(np.int8).reshape(-1))
     st = ctypes.c_uint(0)
     P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
     args = [*mix.shape, P(typ), ctypes.byref(m), ctypes.c_float(W.FLAME_UNITS[0]),
             ctypes.c_float(W.FLAME_UNITS[1]), int(reaction), steps, P(pop0), P(pop1), P(rec0), P(rec1)]
-    fout = np.zeros((27 * (NS + 1), nc)) if pops else None
+    fout = np.zeros((27 * (ns + 1), nc)) if pops else None
     if precision == "fp64":
         L.mc_host_run.restype = ctypes.c_int
         cur = L.mc_host_run(*args, ctypes.byref(st), P(fout) if pops else None)

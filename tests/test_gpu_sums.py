@@ -56,19 +56,19 @@ def test_gpu_sums_multicomponent():
         lat.download(c, s)
     assert s1 == s2
     ns = len(sp)
-    assert len(s1) == 5 + ns + 4
+    assert len(s1) == 5 + ns + 5
     fl = c["type"] == W.TYPE_F
     rho = c["rho"][fl]
     _close(s1[0], rho.sum())
     for k, f in ((1, "u"), (2, "v"), (3, "w")):
         assert abs(s1[k] - (rho * c[f][fl]).sum()) < 1e-13 * abs(rho.sum())
     _close(s1[4], c["rhoe"][fl].sum())
-    el = np.zeros(4)
+    el = np.zeros(5)
     for a in range(ns):
         ra = s[a]["rho"][fl]
         _close(s1[5 + a], ra.sum())
-        el += (ra / m.W[a]).sum() * np.array([m.elements[a][e] for e in range(4)])
-    for e in range(4):
+        el += (ra / m.W[a]).sum() * np.array([m.elements[a][e] for e in range(5)])
+    for e in range(5):
         if el[e] == 0.0:
             assert s1[5 + ns + e] == 0.0
         else:
