@@ -46,24 +46,32 @@ __global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_
 // lane each.  A short list (up to kChemShortList cells: latency-bound) takes 8 lanes per
 // cell, a long one 4 (the group's redundant factorisation then costs more than the
 // latency it saves); the choice is made on the device from the list's length.
+// The stiff integrator's iteration matrix in shared memory, (NS + 1)^2 doubles per thread of
+// a block (kernels over a compiled mechanism): two blocks of 128 threads per SM hold 200 kB
+// for 9 species, where the thread's own array would live in local memory (its pivoted rows
+// are indexed at run time) and spill through L2.
+constexpr bool kChemSharedMat = true;
+template <int NS>
+constexpr size_t chem_smem_bytes() { return kChemSharedMat ? (size_t)(NS + 1) * (NS + 1) * kBlock * sizeof(double) : 0; }
 constexpr unsigned kChemShortList = 5000;
-template <int NS, int G, typename S, class KIN>
+template <int NS, int G, typename S, class KIN, bool SMAT = false>
 __device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
     const unsigned groups = gridDim.x * blockDim.x / G;
     for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) / G; i < cnt; i += groups) {
         const long n = A.sur.ilist[i];
         double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
         mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
-        mc_chem_ros2<NS, McArgsT<S, double>, true, G, KIN>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
+        mc_chem_ros2<NS, McArgsT<S, double>, true, G, KIN, SMAT>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, false);
     }
 }
 // With a compiled mechanism (KIN: analytic species Jacobian, two right-hand sides per
-// sub-step besides it) a cell is one lane's work.
+// sub-step besides it) a cell is one lane's work, its iteration matrix in shared memory as in
+// k_mc_chem (launched with chem_smem_bytes).
 template <int NS, typename S, class KIN = void>
-__global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, 2) k_mc_chem_list(McArgsT<S, double> A) {
     const unsigned cnt = *A.sur.icount;
     if constexpr (!std::is_void_v<KIN>)
-        chem_list_groups<NS, 1, S, KIN>(A, cnt);
+        chem_list_groups<NS, 1, S, KIN, kChemSharedMat>(A, cnt);
     else if (cnt <= kChemShortList)
         chem_list_groups<NS, 8, S, KIN>(A, cnt);
     else
@@ -80,14 +88,10 @@ __global__ void __launch_bounds__(kBlock) k_mc_chem_list(McArgsT<S, double> A) {
 // A kernel of its own, so that its time (with the surrogate's kernels) is the chemistry's
 // share of the step, and the transport kernel keeps its own occupancy.
 // One thread per cell.  The integrator's vectors are sized by the species count at compile
-// time (ros2_advance_n) so that they stay in registers; its iteration matrix and the rate
-// factors stay per-thread local memory, and the bound of two blocks per SM keeps that
-// working set (about 2 kB per thread) inside L2 instead of streaming it through HBM.
-// KIN: the compiled kinetics of the handle's mechanism (gen_kinetics.py), void for the tables;
-// with it, the iteration matrix of each thread lives in shared memory (kChemSharedMat).
-constexpr bool kChemSharedMat = true;
-template <int NS>
-constexpr size_t chem_smem_bytes() { return kChemSharedMat ? (size_t)(NS + 1) * (NS + 1) * kBlock * sizeof(double) : 0; }
+// time (ros2_advance_k) so that they stay in registers, two blocks per SM.  KIN: the compiled
+// kinetics of the handle's mechanism (gen_kinetics.py), void for the tables; with it the
+// iteration matrix of each thread lives in shared memory (kChemSharedMat), otherwise in the
+// thread's local memory.
 template <int NS, bool SUR, typename S, class KIN = void>
 __global__ void __launch_bounds__(kBlock, 2) k_mc_chem(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,11 +296,14 @@ bool launch_compiled_chem(lbmgpu *h, const McArgsT<S, double> &A, unsigned grid,
     if constexpr (NS == kin_h2_air_9::NS) {
         using KinH2 = kin_h2_air_9::Kinetics;
         if (h->kin != KIN_H2_AIR_9) return false;
+        constexpr size_t sm = chem_smem_bytes<NS>();
+        // the launches below report a refused attribute as a launch error
         if (list) {
-            k_mc_chem_list<NS, S, KinH2><<<grid, kBlock, 0, h->stream>>>(A);
+            if (sm > 48 * 1024)
+                (void)cudaFuncSetAttribute(k_mc_chem_list<NS, S, KinH2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm);
+            k_mc_chem_list<NS, S, KinH2><<<grid, kBlock, sm, h->stream>>>(A);
         } else {
-            constexpr size_t sm = chem_smem_bytes<NS>();
-            // the launch below reports a refused attribute as a launch error
             if (sm > 48 * 1024)
                 (void)cudaFuncSetAttribute(k_mc_chem<NS, false, S, KinH2>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -47,9 +47,28 @@ __device__ __forceinline__ unsigned pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const unsigned *>(&v);
 }
 
-__host__ __device__ inline float gelu_f(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, arXiv:1606.08415):
+//   gelu(z) = z/2 (1 + tanh(u)),  u = sqrt(2/pi) (z + 0.044715 z^3),
+// the tanh from the hardware's approximate tanh (relative error about 2^-11, below the BF16
+// rounding of the activations), the same function in training and inference.
+__host__ __device__ __forceinline__ float tanh_fast(float u) {
+#if defined(__CUDA_ARCH__)
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return t;
+#else
+    return tanhf(u);
+#endif
+}
+constexpr float kGeluC = 0.7978845608028654f;  // sqrt(2 / pi)
+__host__ __device__ __forceinline__ float gelu_f(float z) {
+    const float u = kGeluC * (z + 0.044715f * z * z * z);
+    return 0.5f * z * (1.0f + tanh_fast(u));
+}
 __device__ inline float gelu_grad(float z) {
-    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+    const float z2 = z * z;
+    const float t = tanh_fast(kGeluC * (z + 0.044715f * z2 * z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * 0.044715f * z2);
 }
 
 // A standardised feature into slot q of a network input row: its BF16 value and the BF16
@@ -87,7 +106,23 @@ __global__ void k_sur_features(McArgsT<S, double> A, const SurNorm *__restrict__
             x[q] = (x[q] - nrm->x_mean[q]) / nrm->x_std[q];
         }
     }
-    for (int q = 0; q < kSurInPad; ++q) put_split(X + n * kSurInX, q, x[q]);
+    // the row (kSurInPad values, then their remainders) as four 16-byte stores, so a warp
+    // writes 2 kB of consecutive rows
+    unsigned hv[kSurInPad / 2], lv[kSurInPad / 2];
+#pragma unroll
+    for (int q = 0; q < kSurInPad; q += 2) {
+        const __nv_bfloat16 h0 = __float2bfloat16(x[q]), h1 = __float2bfloat16(x[q + 1]);
+        const __nv_bfloat162 hh = __halves2bfloat162(h0, h1);
+        const __nv_bfloat162 ll = __floats2bfloat162_rn(x[q] - __bfloat162float(h0), x[q + 1] - __bfloat162float(h1));
+        hv[q / 2] = *reinterpret_cast<const unsigned *>(&hh);
+        lv[q / 2] = *reinterpret_cast<const unsigned *>(&ll);
+    }
+    uint4 *row = reinterpret_cast<uint4 *>(X + n * kSurInX);
+    static_assert(kSurInPad == 16 && kSurInX == 32, "a row is 16 values and 16 remainders");
+    row[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+    row[1] = make_uint4(hv[4], hv[5], hv[6], hv[7]);
+    row[2] = make_uint4(lv[0], lv[1], lv[2], lv[3]);
+    row[3] = make_uint4(lv[4], lv[5], lv[6], lv[7]);
     if (n < A.ncell) gate[n] = out_of_box ? 1 : 0;
 }
 
@@ -125,13 +160,17 @@ struct SurNet {  // device pointers of the BF16 weights and FP32 biases
 // work, frees its tensor memory and returns.
 // -------------------------------------------------------------------------------------
 constexpr int kTcRows = 128;       // cells per tile (MMA M), one thread each
-constexpr int kTcGroups = 2;       // independent tile groups per CTA (one warpgroup each)
+constexpr int kTcGroups = 3;       // independent tile groups per CTA (one warpgroup each)
 constexpr uint32_t kTcCols = 128;  // tensor-memory columns per group: the widest accumulator
+// tensor memory is allocated in powers of two columns (32..512): the groups' columns rounded up
+constexpr uint32_t kTcAlloc = kTcCols * kTcGroups <= 256 ? 256u : 512u;
+static_assert(kTcCols * kTcGroups <= kTcAlloc && kTcAlloc <= 512, "the groups' accumulators fit tensor memory");
 constexpr int kTcW1 = 0, kTcW2 = kTcW1 + kSurHid * kSurInX * 2, kTcW3 = kTcW2 + kSurHid * kSurHid * 2,
               kTcW4 = kTcW3 + kSurHid * kSurHid * 2, kTcG = kTcW4 + kSurOutPad * kSurHid * 2,  // weights, shared
               kTcA = 0, kTcX = kTcA + kTcRows * kSurHid * 2, kTcGBytes = kTcX + kTcRows * kSurInX * 2,  // per group
               kTcB = kTcG + kTcGroups * kTcGBytes, kTcBar = kTcB + (3 * kSurHid + 3 * kSurOutPad) * 4,
               kTcErr = kTcBar + 8 * kTcGroups, kTcSlot = kTcErr + 4 * kTcGroups, kTcSmem = kTcSlot + 8;
+static_assert(kTcSmem <= 227 * 1024, "one CTA's shared memory");
 static_assert(kTcG % 16 == 0 && kTcGBytes % 16 == 0 && kTcX % 16 == 0 && kTcBar % 8 == 0,
               "operand tiles 16-byte, mbarriers 8-byte aligned");
 
@@ -249,7 +288,7 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
     if (tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kTcSlot),
-                     "r"(kTcCols * kTcGroups)
+                     "r"(kTcAlloc)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -336,7 +375,7 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcCols * kTcGroups)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcAlloc)
                      : "memory");
 }
 
