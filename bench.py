@@ -217,16 +217,17 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel, cells):
-    """DRAM bytes of one launch of `kernel` over `cells` fluid cells, scaled from the
-    committed ncu capture (profiles/ncu_traffic.txt: bytes of one captured launch and the
-    cells it processed; the traffic of these kernels grows in proportion to the cells),
-    or None."""
+def ncu_traffic(kernel, cells, case):
+    """DRAM bytes of one launch of `kernel` over `cells` fluid cells in the workload family
+    `case`, scaled from the committed ncu capture (profiles/ncu_traffic.txt: bytes of one
+    captured launch, the cells it processed and the case captured; the traffic of these
+    kernels grows in proportion to the cells), or None."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     try:
         for line in open(p):
             parts = line.split()
-            if len(parts) >= 5 and parts[0] == "traffic" and parts[1] == kernel and parts[3] == "cells":
+            if (len(parts) >= 7 and parts[0] == "traffic" and parts[1] == kernel and parts[3] == "cells"
+                    and parts[5] == "case" and parts[6] == case):
                 return float(parts[2]) / float(parts[4]) * cells
     except OSError:
         pass
@@ -663,11 +664,15 @@ def run_ours_mc(args, dist):
         "data": "synthetic (seeded H2/air cases of the reference's flame setups, numpy PCG64 seed 20261203)",
         "config": {"workload": mc_workload_name(args, "x".join(str(s_ - 2) for s_ in mix.shape)),
                    "cells": ncell, "parallelism": f"replicas{dist.world}", "l2": "state larger than L2, no flush",
-                   "storage": "FP32 populations (shifted), FP64 records" if pop_bytes == 4 else "FP64"},
+                   "storage": ("FP32 populations (shifted), FP64 records; transport properties in FP32, the "
+                               "chemistry, moment solve and temperature recovery in FP64") if pop_bytes == 4
+                   else "FP64"},
         "hbm_gbs_step": ncell * sum(mc_bytes(k, pop_bytes, reaction) for k in ("k_mc_relax", "k_mc_gather", "k_mc_solve", "k_mc_props", "k_mc_eflux"))
         / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell), "peak_source": f"{peak_kind} hbm_gbs",
+                     "frac": achieved / peak,
+                     "traffic": ncu_traffic(dom, ncell, f"{args.workload}_{args.precision}"),
+                     "peak_source": f"{peak_kind} hbm_gbs",
                      "alg_bytes_per_launch": alg, "mean_launch_ms": avg[dom], "kernel_ms": avg},
         "gpu_launches": int(round(sum(launches) / kk * args.steps)),
         "status": status, "clocks": clocks, "e2e": e2e,
@@ -779,7 +784,7 @@ def run_ours(args, dist):
                    "l2": "state larger than L2 (248 MB of populations), no flush"},
         "hbm_gbs_step": ncell * BYTES_STEP_FP64 / (ms / args.steps * 1e-3) / 1e9,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell),
+                     "frac": achieved / peak, "traffic": ncu_traffic(dom, ncell, "tgv_fp64"),
                      "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_launch": alg,
                      "mean_launch_ms": avg[dom], "kernel_ms": avg},
         "gpu_launches": int(round(per_step_launches * args.steps)),
@@ -1100,11 +1105,17 @@ def run_ours_turb(args, dist):
     peak, peak_kind = peaks()
     achieved = alg_step * ncell / (step_ms * 1e-3) / 1e9
     kern = {}
+    case = f"turb_{args.precision}"
+    step_kernels = ("k_mc_props", "k_mc_chem", "k_mc_eflux", "k_mc_relax", "k_mc_special", "k_mc_gather", "k_mc_solve")
+    # the boundary kernel's cells are the two planes next to the outflow faces (2 N^2 per box)
+    parts = [ncu_traffic(name, 2 * N * N if name == "k_mc_special" else ncell, case)
+             for name in step_kernels]
+    step_traffic = sum(parts) if all(p_ is not None for p_ in parts) else None
     for k, name in ((0, "k_mc_relax"), (1, "k_mc_gather")):
         alg = mc_bytes(name, pop_bytes, True) * ncell
         t = kms[k] / max(launches[k], 1)
         kern[name] = {"alg_bytes_per_launch": alg, "mean_launch_ms": t, "achieved_gbs": alg / (t * 1e-3) / 1e9,
-                      "frac": alg / (t * 1e-3) / 1e9 / peak, "traffic": ncu_traffic(name, ncell)}
+                      "frac": alg / (t * 1e-3) / 1e9 / peak, "traffic": ncu_traffic(name, ncell, case)}
     # end to end through the reference-facing calls: plane-range uploads from host memory
     # and Init, per step the five phase calls and the conserved totals read back, the
     # plane-range download of the final state; the time inside those calls
@@ -1167,12 +1178,16 @@ def run_ours_turb(args, dist):
                    "parallelism": (f"x-slabs{dist.world} (one {N}^3 box per GPU, halos over NCCL)" if dist.world > 1
                                    else ("x-slab loopback check" if slabs else "single GPU")),
                    "l2": "state larger than L2 (86 GB at 258^3 FP32), no flush",
-                   "storage": "FP32 populations (shifted), FP64 records and arithmetic" if pop_bytes == 4 else "FP64"},
+                   "storage": ("FP32 populations (shifted), FP64 records; transport properties in FP32, the "
+                               "chemistry, moment solve and temperature recovery in FP64") if pop_bytes == 4
+                   else "FP64"},
         "chemistry": {"ms_per_step": per_step["k_mc_chem"], "fraction_of_step": per_step["k_mc_chem"] / step_ms,
                       "integrator": "ROS2, rtol 1e-5" if args.chem == "rosenbrock" else args.chem},
         "hbm_gbs_step": achieved,
         "roofline": {"bound": "hbm", "kernel": "whole step (all kernels)", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": step_traffic,
+                     "traffic_note": "DRAM bytes of one step: the sum over the step's kernels of ncu's "
+                                     "dram__bytes_read + write per launch, captured at 64^3 and scaled by cells",
                      "peak_source": f"{peak_kind} hbm_gbs", "alg_bytes_per_cell": alg_step,
                      "alg_bytes_note": "one read + one write of the 270 populations + FP64 T read and write",
                      "kernel_ms_per_step": per_step, "profiled_ms_per_step": prof_step, "kernels": kern},
