@@ -287,7 +287,7 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
 // The kinetics policies ros2_advance_k takes: `K` the temperature factors, `factors(T, K)`
 // forms them, `rhs(K, rho, y, F)` is the reactor's right-hand side at y from the factors at
 // y's temperature; with kAnalyticJacobian, `jacobian(K, rho, y, F, s, J)` writes s times the
-// species columns of dF/d(Y, T) (the finite differences are taken otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
+// Jacobian dF/d(Y, T) (its columns are finite differences otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
 // factors inside each right-hand side (reactor_rhs_dense: nothing per reaction kept between
 // calls); a mechanism compiled to straight-line code (gen_kinetics.py) provides its own policy
 // whose factors are formed once per temperature.
@@ -316,9 +316,9 @@ struct CachedTableKinetics {
 // sequence of right-hand sides (the species columns of the Jacobian at the unperturbed
 // temperature's factors, the temperature column and the second stage at their own), its
 // vectors sized and its loops unrolled so that they stay in registers.  A policy with an
-// analytic Jacobian replaces the species columns' finite differences (ROS2 is a W-method:
-// its order holds for any Jacobian approximation, so only rounding-level differences in
-// the step-size decisions separate the two).
+// analytic Jacobian replaces the finite differences and their right-hand sides (ROS2 is a
+// W-method: its order holds for any Jacobian approximation, so the two differ by the
+// differences' truncation and rounding in the step-size decisions).
 template <int NS, class Kin, class Mat>
 GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                            double atol = 1e-10, double atol_T = 1e-3) {
@@ -358,7 +358,7 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
                 for (int r = 0; r < n; ++r) M(r, c) = -gam * h * (Fp[r] - F0[r]) / eps;
             }
         }
-        {  // the temperature column
+        if constexpr (!Kin::kAnalyticJacobian) {  // the temperature column
             const double eps = 1e-7 * y[ns];
 #pragma unroll
             for (int q = 0; q < n; ++q) yp[q] = y[q];

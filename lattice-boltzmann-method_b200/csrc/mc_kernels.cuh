@@ -92,8 +92,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_mc_chem_list(McArgsT<S, double> A
 // kinetics of the handle's mechanism (gen_kinetics.py), void for the tables; with it the
 // iteration matrix of each thread lives in shared memory (kChemSharedMat), otherwise in the
 // thread's local memory.
+// The surrogate's instance (SUR: no integrator in it) holds far less per thread and runs four
+// blocks per SM.
 template <int NS, bool SUR, typename S, class KIN = void>
-__global__ void __launch_bounds__(kBlock, 2) k_mc_chem(McArgsT<S, double> A) {
+__global__ void __launch_bounds__(kBlock, SUR ? 4 : 2) k_mc_chem(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;

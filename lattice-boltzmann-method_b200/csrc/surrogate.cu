@@ -60,15 +60,35 @@ __host__ __device__ __forceinline__ float tanh_fast(float u) {
     return tanhf(u);
 #endif
 }
-constexpr float kGeluC = 0.7978845608028654f;  // sqrt(2 / pi)
+// u = z (c + c' z^2), gelu = z/2 + (z/2) tanh(u), c = sqrt(2/pi), c' = 0.044715 c: the same
+// fused multiply-adds in the scalar form (training) and the packed pair form (inference).
+constexpr float kGeluC = 0.7978845608028654f;     // sqrt(2 / pi)
+constexpr float kGeluC3 = 0.7978845608028654f * 0.044715f;
 __host__ __device__ __forceinline__ float gelu_f(float z) {
-    const float u = kGeluC * (z + 0.044715f * z * z * z);
-    return 0.5f * z * (1.0f + tanh_fast(u));
+    const float u = z * fmaf(z * z, kGeluC3, kGeluC);
+    const float hz = 0.5f * z;
+    return fmaf(hz, tanh_fast(u), hz);
 }
 __device__ inline float gelu_grad(float z) {
     const float z2 = z * z;
-    const float t = tanh_fast(kGeluC * (z + 0.044715f * z2 * z));
-    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC * (1.0f + 3.0f * 0.044715f * z2);
+    const float t = tanh_fast(z * fmaf(z2, kGeluC3, kGeluC));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * fmaf(z2, 3.0f * kGeluC3, kGeluC);
+}
+// gelu_f of two values with the packed FP32 pair instructions of sm_100 (the tanh stays scalar)
+__device__ __forceinline__ float2 gelu2(float2 z) {
+    const float2 u = __fmul2_rn(z, __ffma2_rn(__fmul2_rn(z, z), make_float2(kGeluC3, kGeluC3),
+                                              make_float2(kGeluC, kGeluC)));
+    const float2 hz = __fmul2_rn(z, make_float2(0.5f, 0.5f));
+    return __ffma2_rn(hz, make_float2(tanh_fast(u.x), tanh_fast(u.y)), hz);
+}
+
+// The first padding slot of a network input row carries 1.0 as value and as "remainder": the
+// tensor-core network multiplies it by the first layer's bias, split into a BF16 value and a
+// BF16 remainder (k_sur_mlp_tc), so the bias is added inside the MMA.
+constexpr int kSurBiasSlot = kSurIn;
+static_assert(kSurBiasSlot < kSurInPad && kSurBiasSlot % 2 == 0, "a padding slot at an even index");
+__device__ __forceinline__ unsigned bias_slot_pair(unsigned pair) {  // (1.0, the odd slot's value)
+    return (pair & 0xFFFF0000u) | (unsigned)__bfloat16_as_ushort(__float2bfloat16(1.0f));
 }
 
 // A standardised feature into slot q of a network input row: its BF16 value and the BF16
@@ -117,6 +137,8 @@ __global__ void k_sur_features(McArgsT<S, double> A, const SurNorm *__restrict__
         hv[q / 2] = *reinterpret_cast<const unsigned *>(&hh);
         lv[q / 2] = *reinterpret_cast<const unsigned *>(&ll);
     }
+    hv[kSurBiasSlot / 2] = bias_slot_pair(hv[kSurBiasSlot / 2]);
+    lv[kSurBiasSlot / 2] = bias_slot_pair(lv[kSurBiasSlot / 2]);
     uint4 *row = reinterpret_cast<uint4 *>(X + n * kSurInX);
     static_assert(kSurInPad == 16 && kSurInX == 32, "a row is 16 values and 16 remainders");
     row[0] = make_uint4(hv[0], hv[1], hv[2], hv[3]);
@@ -136,6 +158,8 @@ __global__ void k_sur_standardise(const float *__restrict__ x, long m, long mpad
         if (r < m && q < kSurIn) v = (x[r * kSurIn + q] - nrm->x_mean[q]) / nrm->x_std[q];
         put_split(X + r * kSurInX, q, v);
     }
+    X[r * kSurInX + kSurBiasSlot] = __float2bfloat16(1.0f);
+    X[r * kSurInX + kSurInPad + kSurBiasSlot] = __float2bfloat16(1.0f);
 }
 
 struct SurNet {  // device pointers of the BF16 weights and FP32 biases
@@ -165,10 +189,14 @@ constexpr uint32_t kTcCols = 128;  // tensor-memory columns per group: the wides
 // tensor memory is allocated in powers of two columns (32..512): the groups' columns rounded up
 constexpr uint32_t kTcAlloc = kTcCols * kTcGroups <= 256 ? 256u : 512u;
 static_assert(kTcCols * kTcGroups <= kTcAlloc && kTcAlloc <= 512, "the groups' accumulators fit tensor memory");
-constexpr int kTcW1 = 0, kTcW2 = kTcW1 + kSurHid * kSurInX * 2, kTcW3 = kTcW2 + kSurHid * kSurHid * 2,
-              kTcW4 = kTcW3 + kSurHid * kSurHid * 2, kTcG = kTcW4 + kSurOutPad * kSurHid * 2,  // weights, shared
-              kTcA = 0, kTcX = kTcA + kTcRows * kSurHid * 2, kTcGBytes = kTcX + kTcRows * kSurInX * 2,  // per group
-              kTcB = kTcG + kTcGroups * kTcGBytes, kTcBar = kTcB + (3 * kSurHid + 3 * kSurOutPad) * 4,
+// The hidden activations carry one more 16-wide K slice (kTcK): columns 128 and 129 hold 1.0
+// and the next layer's weights there its bias split into a BF16 value and a BF16 remainder,
+// so the MMA adds the bias; the input rows do the same in their padding slot (kSurBiasSlot).
+constexpr int kTcK = kSurHid + 16;
+constexpr int kTcW1 = 0, kTcW2 = kTcW1 + kSurHid * kSurInX * 2, kTcW3 = kTcW2 + kSurHid * kTcK * 2,
+              kTcW4 = kTcW3 + kSurHid * kTcK * 2, kTcG = kTcW4 + kSurOutPad * kTcK * 2,  // weights, shared
+              kTcA = 0, kTcX = kTcA + kTcRows * kTcK * 2, kTcGBytes = kTcX + kTcRows * kSurInX * 2,  // per group
+              kTcB = kTcG + kTcGroups * kTcGBytes, kTcBar = kTcB + 2 * kSurOutPad * 4,
               kTcErr = kTcBar + 8 * kTcGroups, kTcSlot = kTcErr + 4 * kTcGroups, kTcSmem = kTcSlot + 8;
 static_assert(kTcSmem <= 227 * 1024, "one CTA's shared memory");
 static_assert(kTcG % 16 == 0 && kTcGBytes % 16 == 0 && kTcX % 16 == 0 && kTcBar % 8 == 0,
@@ -251,34 +279,49 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
     const int tid = threadIdx.x, warp = tid >> 5, g = tid / kTcRows, t = tid % kTcRows;
     const int nthr = kTcRows * kTcGroups;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(sm);
-    float *bb = reinterpret_cast<float *>(sm + kTcB);  // b1 b2 b3, b4, y_mean, y_std
-    // weights into the canonical layout: W1 as [W1 | W1] (values and remainders), W2, W3, W4
+    float *bb = reinterpret_cast<float *>(sm + kTcB);  // y_mean, y_std
+    // weights into the canonical layout: W1 as [W1 | W1] (values and remainders), W2, W3, W4;
+    // each layer's bias as a BF16 value and remainder in the K slice its input's 1.0 meets
+    auto split = [](float b, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+        hi = __float2bfloat16(b);
+        lo = __float2bfloat16(b - __bfloat162float(hi));
+    };
     for (int i = tid; i < kSurHid * (kSurInX / 8); i += nthr) {
         const int r = i / (kSurInX / 8), c = i % (kSurInX / 8);
-        *reinterpret_cast<uint4 *>(sm + kTcW1 + tc_off(r, c * 8, kSurInX)) =
-            *reinterpret_cast<const uint4 *>(net.w1 + r * kSurInPad + (c % 2) * 8);
+        union {
+            uint4 v;
+            __nv_bfloat16 e[8];
+        } u;
+        u.v = *reinterpret_cast<const uint4 *>(net.w1 + r * kSurInPad + (c % 2) * 8);
+        if (c % 2 == kSurBiasSlot / 8) {  // the bias slot: value half, remainder half
+            __nv_bfloat16 hi, lo;
+            split(net.b1[r], hi, lo);
+            u.e[kSurBiasSlot % 8] = c < 2 ? hi : lo;
+        }
+        *reinterpret_cast<uint4 *>(sm + kTcW1 + tc_off(r, c * 8, kSurInX)) = u.v;
     }
-    for (int i = tid; i < kSurHid * (kSurHid / 8); i += nthr) {
-        const int r = i / (kSurHid / 8), c = i % (kSurHid / 8);
-        *reinterpret_cast<uint4 *>(sm + kTcW2 + tc_off(r, c * 8, kSurHid)) =
-            *reinterpret_cast<const uint4 *>(net.w2 + r * kSurLd + c * 8);
-        *reinterpret_cast<uint4 *>(sm + kTcW3 + tc_off(r, c * 8, kSurHid)) =
-            *reinterpret_cast<const uint4 *>(net.w3 + r * kSurLd + c * 8);
-    }
-    for (int i = tid; i < kSurOutPad * (kSurHid / 8); i += nthr) {
-        const int r = i / (kSurHid / 8), c = i % (kSurHid / 8);
-        *reinterpret_cast<uint4 *>(sm + kTcW4 + tc_off(r, c * 8, kSurHid)) =
-            *reinterpret_cast<const uint4 *>(net.w4 + r * kSurLd + c * 8);
-    }
-    for (int i = tid; i < kSurHid; i += nthr) {
-        bb[i] = net.b1[i];
-        bb[kSurHid + i] = net.b2[i];
-        bb[2 * kSurHid + i] = net.b3[i];
-    }
+    auto hidden_w = [&](int off, const __nv_bfloat16 *w, const float *b, int rows) {
+        for (int i = tid; i < rows * (kTcK / 8); i += nthr) {
+            const int r = i / (kTcK / 8), c = i % (kTcK / 8);
+            union {
+                uint4 v;
+                __nv_bfloat16 e[8];
+            } u;
+            u.v = make_uint4(0u, 0u, 0u, 0u);
+            if (c < kSurHid / 8) {
+                u.v = *reinterpret_cast<const uint4 *>(w + r * kSurLd + c * 8);
+            } else if (c == kSurHid / 8) {
+                split(b[r], u.e[0], u.e[1]);
+            }
+            *reinterpret_cast<uint4 *>(sm + off + tc_off(r, c * 8, kTcK)) = u.v;
+        }
+    };
+    hidden_w(kTcW2, net.w2, net.b2, kSurHid);
+    hidden_w(kTcW3, net.w3, net.b3, kSurHid);
+    hidden_w(kTcW4, net.w4, net.b4, kSurOutPad);
     if (tid < kSurOutPad) {
-        bb[3 * kSurHid + tid] = net.b4[tid];
-        bb[3 * kSurHid + kSurOutPad + tid] = nrm->y_mean[tid];
-        bb[3 * kSurHid + 2 * kSurOutPad + tid] = nrm->y_std[tid];
+        bb[tid] = nrm->y_mean[tid];
+        bb[kSurOutPad + tid] = nrm->y_std[tid];
     }
     volatile int *err = reinterpret_cast<volatile int *>(sm + kTcErr);
     if (tid < kTcGroups) {
@@ -302,7 +345,13 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
     const uint32_t bar = base + kTcBar + 8u * (uint32_t)g;
     const uint32_t gA = base + kTcG + (uint32_t)(g * kTcGBytes) + kTcA, gX = base + kTcG + (uint32_t)(g * kTcGBytes) + kTcX;
     unsigned char *smA = sm + kTcG + g * kTcGBytes + kTcA, *smX = sm + kTcG + g * kTcGBytes + kTcX;
-    const float *ym = bb + 3 * kSurHid + kSurOutPad, *ys = ym + kSurOutPad;
+    const float *ym = bb, *ys = bb + kSurOutPad;
+    {  // the activations' bias slice: 1.0 in columns 128 and 129, zeros after (never rewritten)
+        const __nv_bfloat162 one2 = __floats2bfloat162_rn(1.0f, 1.0f);
+        const unsigned one = *reinterpret_cast<const unsigned *>(&one2);
+        *reinterpret_cast<uint4 *>(smA + tc_off(t, kSurHid, kTcK)) = make_uint4(one, 0u, 0u, 0u);
+        *reinterpret_cast<uint4 *>(smA + tc_off(t, kSurHid + 8, kTcK)) = make_uint4(0u, 0u, 0u, 0u);
+    }
     const uint32_t wl[4] = {base + kTcW1, base + kTcW2, base + kTcW3, base + kTcW4};
     uint32_t phase = 0;
     bool ok = true;
@@ -318,16 +367,14 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
         tc_sync(g);
         for (int L = 0; L < 4 && ok; ++L) {
             if (t == 0)
-                tc_layer(tmem, L == 0 ? gX : gA, wl[L], L == 0 ? kSurInX : kSurHid, L == 3 ? kSurOutPad : kSurHid,
-                         bar);
+                tc_layer(tmem, L == 0 ? gX : gA, wl[L], L == 0 ? kSurInX : kTcK, L == 3 ? kSurOutPad : kSurHid, bar);
             if (!tc_wait(bar, phase)) err[g] = 1;
             group_bar(g);
             tc_fence_after();
             ok = err[g] == 0;
             if (!ok) break;
             phase ^= 1u;
-            if (L < 3) {
-                const float *b = bb + L * kSurHid;
+            if (L < 3) {  // GELU of the accumulator (the bias is in it), BF16 into the next operand
 #pragma unroll 1
                 for (int cb = 0; cb < kSurHid / 32; ++cb) {
                     uint32_t r[32];
@@ -337,14 +384,16 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
                     for (int j = 0; j < 32; j += 8) {
                         uint4 o;
                         const int k = cb * 32 + j;
-                        o.x = pack_bf16(gelu_f(__uint_as_float(r[j]) + b[k]), gelu_f(__uint_as_float(r[j + 1]) + b[k + 1]));
-                        o.y = pack_bf16(gelu_f(__uint_as_float(r[j + 2]) + b[k + 2]),
-                                        gelu_f(__uint_as_float(r[j + 3]) + b[k + 3]));
-                        o.z = pack_bf16(gelu_f(__uint_as_float(r[j + 4]) + b[k + 4]),
-                                        gelu_f(__uint_as_float(r[j + 5]) + b[k + 5]));
-                        o.w = pack_bf16(gelu_f(__uint_as_float(r[j + 6]) + b[k + 6]),
-                                        gelu_f(__uint_as_float(r[j + 7]) + b[k + 7]));
-                        *reinterpret_cast<uint4 *>(smA + tc_off(t, k, kSurHid)) = o;
+                        float2 a;
+                        a = gelu2(make_float2(__uint_as_float(r[j]), __uint_as_float(r[j + 1])));
+                        o.x = pack_bf16(a.x, a.y);
+                        a = gelu2(make_float2(__uint_as_float(r[j + 2]), __uint_as_float(r[j + 3])));
+                        o.y = pack_bf16(a.x, a.y);
+                        a = gelu2(make_float2(__uint_as_float(r[j + 4]), __uint_as_float(r[j + 5])));
+                        o.z = pack_bf16(a.x, a.y);
+                        a = gelu2(make_float2(__uint_as_float(r[j + 6]), __uint_as_float(r[j + 7])));
+                        o.w = pack_bf16(a.x, a.y);
+                        *reinterpret_cast<uint4 *>(smA + tc_off(t, k, kTcK)) = o;
                     }
                 }
             } else {
@@ -352,14 +401,13 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
                 tc_ld16(trow, r);
                 tc_wait_ld();
                 if (row < mpad) {
-                    const float *b4 = bb + 3 * kSurHid;
 #pragma unroll
                     for (int c = 0; c < kSurOutPad; c += 4) {
                         float4 o;
-                        o.x = (__uint_as_float(r[c]) + b4[c]) * ys[c] + ym[c];
-                        o.y = (__uint_as_float(r[c + 1]) + b4[c + 1]) * ys[c + 1] + ym[c + 1];
-                        o.z = (__uint_as_float(r[c + 2]) + b4[c + 2]) * ys[c + 2] + ym[c + 2];
-                        o.w = (__uint_as_float(r[c + 3]) + b4[c + 3]) * ys[c + 3] + ym[c + 3];
+                        o.x = __uint_as_float(r[c]) * ys[c] + ym[c];
+                        o.y = __uint_as_float(r[c + 1]) * ys[c + 1] + ym[c + 1];
+                        o.z = __uint_as_float(r[c + 2]) * ys[c + 2] + ym[c + 2];
+                        o.w = __uint_as_float(r[c + 3]) * ys[c + 3] + ym[c + 3];
                         *reinterpret_cast<float4 *>(pred + row * kSurOutPad + c) = o;
                     }
                 }

@@ -47,16 +47,15 @@ int kh_ros2_compiled(double rho, double *Y, double *T, double dt) {
 }
 
 extern "C" {
-// the analytic species columns of the compiled kinetics' Jacobian (row-major 10 x 10; column
-// 9 untouched)
+// the compiled kinetics' analytic Jacobian d(Y, T)/dt / d(Y, T) (row-major 10 x 10)
 void kh_jac_compiled(double rho, const double *y, double *J) {
     K9::Factors K;
     K9::factors(y[K9::NS], K);
     double F[K9::NS + 1];
     K9::rhs_k(K, rho, y, F);
     gas::RegMat<K9::NS + 1> Jm;
-    K9::jac_species(K, rho, y, F, 1.0, Jm);
+    K9::jac(K, rho, y, F, 1.0, Jm);
     for (int r = 0; r <= K9::NS; ++r)
-        for (int c = 0; c < K9::NS; ++c) J[r * (K9::NS + 1) + c] = Jm(r, c);
+        for (int c = 0; c <= K9::NS; ++c) J[r * (K9::NS + 1) + c] = Jm(r, c);
 }
 }
