@@ -53,6 +53,9 @@ struct Tables {
     lbmgpu_mech m;
     int ns;
     double invW[MAXS];
+    // h/RT polynomial of each NASA-7 range with its quotients formed once: a1, a2/2, a3/3,
+    // a4/4, a5/5, a6 (the reciprocal forms of the FP32 storage mode, h_RT_fast)
+    double hcoef[MAXS][2][6];
     double visc_pref[MAXS];            // mu_k = visc_pref * sqrt(T) / Omega22(T/eps_k, delta_k)
     double eps[MAXS];                  // epsilon/k_B of the species, K
     double delta[MAXS];                // reduced dipole moment delta*_k
@@ -102,6 +105,11 @@ inline void make_tables_base(const lbmgpu_mech &m, Tables &t) {
     t.ns = m.n_species;
     for (int k = 0; k < t.ns; ++k) {
         t.invW[k] = 1.0 / m.W[k];
+        for (int r = 0; r < 2; ++r) {
+            const double *a = r == 0 ? m.nasa_lo[k] : m.nasa_hi[k];
+            const double c[6] = {a[0], a[1] / 2, a[2] / 3, a[3] / 4, a[4] / 5, a[5]};
+            for (int i = 0; i < 6; ++i) t.hcoef[k][r][i] = c[i];
+        }
         const double mk = m.W[k] / kNA;                 // kg per molecule
         const double s = m.diameter[k];
         t.visc_pref[k] = (5.0 / 16.0) * sqrt(kPi * mk * kBoltz) / (kPi * s * s);
@@ -174,6 +182,34 @@ GAS_HD double cv_mass(const Tables &t, const double *Y, double T) {
     double c = 0.0;
     for (int k = 0; k < t.ns; ++k) c += Y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
     return c * kR;
+}
+
+// h/RT with the coefficients' quotients formed once and 1/T given: the same polynomial as
+// h_RT with products in place of its divisions (the FP32 storage mode's moment solve, where
+// the result differs from h_RT by rounding).
+GAS_HD double h_RT_fast(const Tables &t, int k, double T, double invT) {
+    const double *c = t.hcoef[k][T < t.m.T_mid[k] ? 0 : 1];
+    return c[0] + T * (c[1] + T * (c[2] + T * (c[3] + T * c[4]))) + c[5] * invT;
+}
+
+// T_from_u with h_RT_fast and one reciprocal per iteration: the same damped Newton iteration
+// and stopping rule.
+GAS_HD int T_from_u_fast(const Tables &t, const double *Y, double u, double T0, double rtol, int maxit, double &T) {
+    T = T0 > 0 ? T0 : 300.0;
+    for (int it = 0; it < maxit; ++it) {
+        const double invT = 1.0 / T;
+        double e = 0.0, c = 0.0;
+        for (int k = 0; k < t.ns; ++k) {
+            e += Y[k] * (h_RT_fast(t, k, T, invT) - 1.0) * t.invW[k];
+            c += Y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
+        }
+        double dT = -(e * kR * T - u) / (c * kR);
+        if (dT > 500.0) dT = 500.0;
+        if (dT < -0.5 * T) dT = -0.5 * T;
+        T += dT;
+        if (fabs(dT) <= rtol * T) return it + 1;
+    }
+    return -1;
 }
 
 // T with int_energy_mass(Y, T) = u: damped Newton from T0, at most `maxit` iterations.

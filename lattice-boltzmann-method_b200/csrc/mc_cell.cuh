@@ -209,6 +209,26 @@ MC_HD double set_mass_fractions(const gas::Tables &t, const double *y, double *Y
     return W;
 }
 
+// set_mass_fractions with products by reciprocals in place of its divisions (the FP32 storage
+// mode's moment solve; rounding-level differences).
+template <int NS>
+MC_HD double set_mass_fractions_fast(const gas::Tables &t, const double *y, double *Y, double *X) {
+    double s = 0.0;
+    for (int k = 0; k < NS; ++k) {
+        Y[k] = y[k] > 0.0 ? y[k] : 0.0;
+        s += Y[k];
+    }
+    const double is = 1.0 / s;
+    double sw = 0.0;
+    for (int k = 0; k < NS; ++k) {
+        Y[k] *= is;
+        sw += Y[k] * t.invW[k];
+    }
+    const double W = 1.0 / sw;
+    for (int k = 0; k < NS; ++k) X[k] = Y[k] * t.invW[k] * W;
+    return W;
+}
+
 // The face-difference terms a cell offers its neighbours: species Q_{a,d} with the species
 // gas constant (src/lbm-collision.cpp:487-489) and the mixture Q_d with the composition
 // gas constant a neighbour uses (src/lbm-collision.cpp:207-215, 296-300; zero gas constant
@@ -372,6 +392,51 @@ MC_HD void mc_stefan_maxwell(int dt, double p_old, const double *Xold, const dou
     }
 }
 
+// The same system for the FP32 storage mode, where the result need not reproduce the
+// reference's roundings: the matrix is symmetric (each pair's entry -dt/2 p X_a X_b / D_ab
+// formed once, one division), and the Cholesky factor's pivots are inverted once, so the
+// factorisation and the solves multiply instead of dividing -- 36 divisions and 9 square roots
+// in place of 171 divisions and 9 square roots.
+template <int NS>
+MC_HD void mc_stefan_maxwell_fast(int dt, double p_old, const double *Xold, const double *rho_s,
+                                  const double (*j_a)[3], double (*Ld)[NS], double (*usm)[3]) {
+    double L[NS][NS];
+    const double k = -0.5 * (double)dt * p_old;
+    for (int a = 0; a < NS; ++a) L[a][a] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
+    for (int a = 0; a < NS; ++a)
+        for (int b = 0; b < a; ++b) {
+            const double m = k * Xold[a] * Xold[b] / Ld[a][b];
+            L[a][b] = m;
+            L[a][a] -= m;
+            L[b][b] -= m;
+        }
+    double inv[NS];
+    for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor, reciprocal pivots
+        double d = L[c][c];
+        for (int q = 0; q < c; ++q) d -= L[c][q] * L[c][q];
+        inv[c] = 1.0 / sqrt(d);
+        for (int r = c + 1; r < NS; ++r) {
+            double sum = L[r][c];
+            for (int q = 0; q < c; ++q) sum -= L[r][q] * L[c][q];
+            L[r][c] = sum * inv[c];
+        }
+    }
+    for (int dmn = 0; dmn < 3; ++dmn) {
+        double y[NS], x[NS];
+        for (int r = 0; r < NS; ++r) {
+            double sum = j_a[r][dmn];
+            for (int q = 0; q < r; ++q) sum -= L[r][q] * y[q];
+            y[r] = sum * inv[r];
+        }
+        for (int r = NS - 1; r >= 0; --r) {
+            double sum = y[r];
+            for (int q = r + 1; q < NS; ++q) sum -= L[q][r] * x[q];
+            x[r] = sum * inv[r];
+        }
+        for (int r = 0; r < NS; ++r) usm[r][dmn] = x[r];
+    }
+}
+
 template <int NS, class AT, class Pop>
 MC_HDN void mc_moments_cell(const AT &A, long n, const Pop &pop) {
     McSums<NS> S;
@@ -422,16 +487,29 @@ MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S) {
     const double p_old = rec(A, A.rec_cur, RM_P, n);
     double Xold[NS];
     for (int a = 0; a < NS; ++a) Xold[a] = rec(A, A.rec_cur, rs(a, RS_X), n);
-    // FP64 in both storage modes: the FP32 solve moves the characteristic-inflow case's
-    // temperature by 2e-5 against FP64 within 20 steps (its boundary cells amplify last-bit
-    // changes), twice the FP32 mode's bound
+    // FP64 in both storage modes (an FP32 solve moved the characteristic-inflow case's
+    // temperature by 2e-5 against FP64 within 20 steps -- its boundary cells amplify last-bit
+    // changes -- twice the FP32 mode's bound); the FP32 storage mode takes the reciprocal
+    // forms of the solve, the mass fractions and the temperature iteration, which differ
+    // from the reference's divisions by rounding
+    constexpr bool fast = sizeof(typename AT::P) == sizeof(float);
     double usm[NS][3];
-    mc_stefan_maxwell<NS, double>(A.dt, p_old, Xold, rho_s, j_a, L, usm);
+    if constexpr (fast)
+        mc_stefan_maxwell_fast<NS>(A.dt, p_old, Xold, rho_s, j_a, L, usm);
+    else
+        mc_stefan_maxwell<NS, double>(A.dt, p_old, Xold, rho_s, j_a, L, usm);
 
     // -- temperature from the internal energy (setState_UV, lbm-moment.cpp:346-368)
     double Yr[NS], Y[NS], X[NS];
-    for (int a = 0; a < NS; ++a) Yr[a] = rho_s[a] / rho;
-    const double Wn = set_mass_fractions<NS>(t, Yr, Y, X);
+    double Wn;
+    if constexpr (fast) {
+        const double ir = 1.0 / rho;
+        for (int a = 0; a < NS; ++a) Yr[a] = rho_s[a] * ir;
+        Wn = set_mass_fractions_fast<NS>(t, Yr, Y, X);
+    } else {
+        for (int a = 0; a < NS; ++a) Yr[a] = rho_s[a] / rho;
+        Wn = set_mass_fractions<NS>(t, Yr, Y, X);
+    }
     const double rhoe = S.rhoe();
     double e = rhoe / rho;
     for (int a = 0; a < NS; ++a)
@@ -440,7 +518,8 @@ MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S) {
     const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
     const double rho_n_si = 1.0 / vol;
     double Tn;
-    const int it = gas::T_from_u(t, Y, u_si, T_si, 1e-14, 100, Tn);
+    const int it = fast ? gas::T_from_u_fast(t, Y, u_si, T_si, 1e-14, 100, Tn)
+                        : gas::T_from_u(t, Y, u_si, T_si, 1e-14, 100, Tn);
     if (it < 0) atomic_status(A.status, LBMGPU_ST_NEWTON);
     const double Pn = rho_n_si * gas::kR * Tn / Wn;
     const double Tl = u_temp(A.U, (float)Tn);
