@@ -72,6 +72,8 @@ struct Tables {
     double Ra_lat[MAXS];               // units.cp(R / W_a)
     double sqrt4W[MAXS][MAXS];         // sqrt(sqrt(W_b / W_a))   (Wilke factor, reference order)
     double wilke_den[MAXS][MAXS];      // sqrt(8 (1 + W_a / W_b))
+    float inv_wilke_den_f[MAXS][MAXS]; // 1 / wilke_den and W_a / W_b in FP32 (the FP32 storage
+    float W_ratio_f[MAXS][MAXS];       // mode's transport)
     // dense stoichiometry (species k of reaction r; 0 where k does not take part): reactant and
     // product coefficients and their net difference, for the compile-time-unrolled kinetics
     double nu_f[MAXR][MAXS], nu_b[MAXR][MAXS], nu_net[MAXR][MAXS], dnu[MAXR];
@@ -505,7 +507,9 @@ inline void make_tables(const lbmgpu_mech &m, Tables &t) {
     for (int a = 0; a < t.ns; ++a)
         for (int b = 0; b < t.ns; ++b) {
             t.sqrt4W[a][b] = sqrt(sqrt(m.W[b] / m.W[a]));
+            t.W_ratio_f[a][b] = (float)(m.W[a] / m.W[b]);
             t.wilke_den[a][b] = sqrt(8.0 * (1.0 + m.W[a] / m.W[b]));
+            t.inv_wilke_den_f[a][b] = (float)(1.0 / t.wilke_den[a][b]);
         }
     for (int a = 0; a < t.ns; ++a) t.Ra_lat[a] = 0.0;
     for (int r = 0; r < MAXR; ++r) {

@@ -788,7 +788,8 @@ MC_HDN void mc_transport_f64(const AT &A, long n, double p, const double *rho_a,
 // conductivities and binary diffusion coefficients (exp of the ln T fits), the Wilke
 // weights, c_p and the mixture conductivity -- quantities the reference itself rounds to
 // float at its unit conversions (units.hpp:10) -- with the Maxwell-Stefan force accumulated
-// in FP64 (its terms are differences of nearly equal species velocities).
+// in FP64 (its terms are differences of nearly equal species velocities).  The Wilke pairs
+// take products of per-species square roots and reciprocals in place of the quotients.
 template <int NS, class AT>
 MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a, const double (*ua)[3],
                              const double *Xs, const double *Y, const double *X, double W, double T_si, double P_si,
@@ -798,9 +799,13 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
     auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
     const float dt = (float)A.dt, pf = (float)p;
     const float xT = (float)gas::lnT_x(T_si);
-    float mu_k[NS], Xsf[NS], Xf[NS];
+    // per species: mu_k, sqrt(mu_k) and their reciprocals, so that the Wilke pairs multiply
+    float mu_k[NS], imu[NS], smu[NS], ismu[NS], Xsf[NS], Xf[NS];
     for (int a = 0; a < NS; ++a) {
         mu_k[a] = expf(gas::fit_eval_f(t.fit_visc[a], xT));
+        imu[a] = 1.f / mu_k[a];
+        smu[a] = sqrtf(mu_k[a]);
+        ismu[a] = 1.f / smu[a];
         Xsf[a] = (float)Xs[a];
         Xf[a] = (float)X[a];
     }
@@ -808,9 +813,9 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
     for (int a = 0; a < NS; ++a) den_s[a] = den_m[a] = 0.f;
     for (int a = 0; a < NS; ++a)
         for (int b = a; b < NS; ++b) {
-            const float f1 = 1.f + sqrtf(mu_k[a] / mu_k[b]) * (float)t.sqrt4W[a][b];
-            const float pab = f1 * f1 / (float)t.wilke_den[a][b];
-            const float pba = mu_k[b] / mu_k[a] * (float)(t.m.W[a] / t.m.W[b]) * pab;
+            const float f1 = 1.f + smu[a] * ismu[b] * (float)t.sqrt4W[a][b];
+            const float pab = f1 * f1 * t.inv_wilke_den_f[a][b];
+            const float pba = mu_k[b] * imu[a] * t.W_ratio_f[a][b] * pab;
             if (b == a) {
                 den_s[a] += Xsf[a] * pba;
                 den_m[a] += Xf[a] * pba;
@@ -840,8 +845,10 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
                 F[b][d] -= k * du;
             }
         }
-    for (int a = 0; a < NS; ++a)
-        for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * (double)dt / rho_a[a]);
+    for (int a = 0; a < NS; ++a) {
+        const double s = (double)dt / rho_a[a];
+        for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * s);
+    }
     float mu = 0.f, cpm = 0.f, s1 = 0.f, s2 = 0.f;
     const float Tf = (float)T_si;
     for (int k = 0; k < NS; ++k) {
@@ -883,10 +890,19 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         for (int d = 0; d < 3; ++d) ua[a][d] = rec(A, Rc, rs(a, RS_UX + d), n);
         Xs[a] = rec(A, Rc, rs(a, RS_X), n);
     }
-    // Cantera state (lbm-collision.cpp:364-367 and :236-238)
+    // Cantera state (lbm-collision.cpp:364-367 and :236-238); the FP32 storage mode takes the
+    // reciprocal forms (rounding-level differences, as in its moment solve)
+    constexpr bool fast = sizeof(typename AT::P) == sizeof(float);
     double Yr[NS], Y[NS], X[NS];
-    for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] / rho;
-    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
+    double W;
+    if constexpr (fast) {
+        const double ir = 1.0 / rho;
+        for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] * ir;
+        W = set_mass_fractions_fast<NS>(t, Yr, Y, X);
+    } else {
+        for (int a = 0; a < NS; ++a) Yr[a] = rho_a[a] / rho;
+        W = set_mass_fractions<NS>(t, Yr, Y, X);
+    }
     const double T_si = si_temp(A.U, (float)Tl);
     const double rho_si = si_rho(A.U, (float)rho);
     const double P_si = rho_si * gas::kR * T_si / W;
