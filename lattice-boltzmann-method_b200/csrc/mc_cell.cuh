@@ -980,17 +980,28 @@ MC_HDN void mc_eflux_cell(const AT &A, long n) {
     double qd[3] = {0, 0, 0}, qc[3] = {0, 0, 0};
     const double rl[3] = {rec(A, Rc, RM_RHO, nbl[0]), rec(A, Rc, RM_RHO, nbl[1]), rec(A, Rc, RM_RHO, nbl[2])};
     const double rh[3] = {rec(A, Rc, RM_RHO, nbh[0]), rec(A, Rc, RM_RHO, nbh[1]), rec(A, Rc, RM_RHO, nbh[2])};
+    // the FP32 storage mode: reciprocal densities and enthalpy quotients (rounding-level
+    // differences, as in its moment solve)
+    constexpr bool fast = sizeof(typename AT::P) == sizeof(float);
+    double irl[3], irh[3];
+    const double ir = fast ? 1.0 / rho : 0.0, invT = fast ? 1.0 / T_si : 0.0;
+    for (int d = 0; d < 3; ++d) {
+        irl[d] = fast ? 1.0 / rl[d] : 0.0;
+        irh[d] = fast ? 1.0 / rh[d] : 0.0;
+    }
     for (int a = 0; a < NS; ++a) {
-        const double ha = u_energy_mass(A.U, (float)(gas::h_RT(t, a, T_si) * gas::kR * T_si / t.m.W[a]));
+        const double ha =
+            fast ? u_energy_mass(A.U, (float)(gas::h_RT_fast(t, a, T_si, invT) * gas::kR * T_si * t.invW[a]))
+                 : u_energy_mass(A.U, (float)(gas::h_RT(t, a, T_si) * gas::kR * T_si / t.m.W[a]));
         const int pr = rs(a, RS_RHO);
         const double rho_a = rec(A, Rc, pr, n);
         const double ua[3] = {rec(A, Rc, rs(a, RS_UX), n), rec(A, Rc, rs(a, RS_UX + 1), n),
                               rec(A, Rc, rs(a, RS_UX + 2), n)};
         for (int d = 0; d < 3; ++d) {
             qd[d] += om1 / (-om + om1) * ha * rho_a * (ua[d] - um[d]);
-            const double Yl = rec(A, Rc, pr, nbl[d]) / rl[d];
-            const double Yc = rho_a / rho;
-            const double Yh = rec(A, Rc, pr, nbh[d]) / rh[d];
+            const double Yl = fast ? rec(A, Rc, pr, nbl[d]) * irl[d] : rec(A, Rc, pr, nbl[d]) / rl[d];
+            const double Yc = fast ? rho_a * ir : rho_a / rho;
+            const double Yh = fast ? rec(A, Rc, pr, nbh[d]) * irh[d] : rec(A, Rc, pr, nbh[d]) / rh[d];
             const double dY = mc_fd_fuw(Yl, Yc, Yh, ua[d] - um[d], tl[d], th[d]);
             qc[d] += 0.5 * (2.0 - om1) / (-om + om1) * dt * p * ha * dY;
         }
