@@ -59,6 +59,36 @@ def arrhenius(A, b, Ea):
     return f"{lit(A)} * exp({lit(b)} * logT - {lit(Ea)} * invRT)"
 
 
+def troe_terms(m, r):
+    """The Troe F_cent terms of reaction r as (kind, value): kind 'zero' / 'one' where the term
+    is exactly 0 or 1 in double precision for every temperature between 1e-17 K and 1e4 K
+    (T*** <= 1e-20 or T** >= 1e20: exp underflows to 0; T* >= 1e20: exp(-T/T*) rounds to 1),
+    'exp' otherwise."""
+    a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
+    out = [("zero" if T3 <= 1e-20 else ("one" if T3 >= 1e20 else "exp"), T3),
+           ("zero" if T1 <= 1e-20 else ("one" if T1 >= 1e20 else "exp"), T1)]
+    if m.troe_n[r] == 4:
+        T2 = m.troe[r][3]
+        out.append(("zero" if T2 >= 1e20 else ("one" if T2 <= 1e-20 else "exp"), T2))
+    return out
+
+
+def troe_constant(m, r):
+    """log10 F_cent of reaction r as a literal when every term folds (troe_terms), else None;
+    the same operations in the same order as gas::rate_factor_one, so the value is the one the
+    tables compute."""
+    import math
+    terms = troe_terms(m, r)
+    if any(k == "exp" for k, _ in terms):
+        return None
+    a = m.troe[r][0]
+    val = lambda k: 0.0 if k == "zero" else 1.0  # noqa: E731
+    Fc = (1.0 - a) * val(terms[0][0]) + a * val(terms[1][0])
+    if len(terms) == 3:
+        Fc += val(terms[2][0])
+    return lit(math.log10(max(Fc, 1e-300)))
+
+
 def weighted(terms):
     """sum_j nu_j g_j accumulated from 0 in the listed order (signs: +1 products, -1 reactants)."""
     out = ""
@@ -86,28 +116,50 @@ def dpow(k, nu, others):
     return " * ".join(terms) if terms else "1.0"
 
 
+def nasa_branches(m, add, body):
+    """Emits `body(k, a)` for every species under its switch temperature's branch (one branch
+    per distinct switch temperature, as in factors)."""
+    groups = {}
+    for k in range(m.n_species):
+        groups.setdefault(m.T_mid[k], []).append(k)
+    for Tm, ks in groups.items():
+        add(f"    if (T < {lit(Tm)}) {{")
+        for branch in ("lo", "hi"):
+            if branch == "hi":
+                add("    } else {")
+            for k in ks:
+                body(k, m.nasa_lo[k] if branch == "lo" else m.nasa_hi[k])
+        add("    }")
+
+
 def emit_jacobian(m, L, fidx):
-    """jac_species: the species columns of d(Y, T)/dt's Jacobian, d F_k / d Y_j (j < NS), at
-    fixed T and rho from the factors at y's temperature, differentiating rhs_k's expressions:
-    the mass-action products, the third-body sum M (efficiency-weighted concentrations) and
-    the Troe blending F(Pr), Pr = k0 M / k_inf; and dT/dt's row through net production and
-    c_v.  With dq_rj = d q_r / d C_j (C_j = rho Y_j / W_j) and nu_kr the net coefficients:
-        J_kj = (W_k / W_j) sum_r nu_kr dq_rj,
-        J_Tj = -(R T / (W_j c_v)) sum_r e_r dq_rj - F_T R (c_p,j/R - 1) / (W_j c_v),
-    e_r = sum_k nu_kr (h_k/RT - 1), every term accumulated straight into the scaled matrix
-    (s J, s = -gamma h for the integrator's iteration matrix).  The fall-off derivative:
+    """jac: the Jacobian of d(Y, T)/dt, d F_k / d Y_j and d F_k / dT, at fixed density from the
+    factors at y's temperature, differentiating rhs_k's expressions.  With q_r the rates of
+    progress, nu_kr the net coefficients and C_j = rho Y_j / W_j:
+        dF_k/dY_j = (W_k / W_j) sum_r nu_kr dq_r/dC_j,
+        dF_k/dT   = (W_k / rho) sum_r nu_kr dq_r/dT,
+        dF_T/dY_j = -(R T / (W_j c_v)) sum_r e_r dq_r/dC_j - F_T R (c_p,j/R - 1) / (W_j c_v),
+        dF_T/dT   = -R [sum_k (c_p,k/R - 1) w_k + T sum_r e_r dq_r/dT] / (rho c_v) - F_T (dc_v/dT) / c_v,
+    e_r = sum_k nu_kr (h_k/RT - 1), w_k the net production rates.  dq_r/dC_j through the
+    mass-action products, the third-body sum M and the Troe blend F(Pr), Pr = k0 M / k_inf:
     d(k_inf Pr/(1+Pr) F)/dM = k0 F/(1+Pr) [1/(1+Pr) - 2 x lFc n / ((1+x^2)^2 (n - 0.14 u)^2)],
-    u = log10 Pr + c, x = u / (n - 0.14 u)."""
+    u = log10 Pr + c, x = u / (n - 0.14 u).  dq_r/dT through d ln k/dT = (b + E_a/RT)/T for
+    k_f and k_0, d ln(1/K_c)/dT = (dnu - sum_k nu_kr h_k/RT)/T (d(g_k/RT)/dT = -h_k/(R T^2),
+    d ln(p_atm/RT)/dT = -1/T), and for a fall-off reaction d ln(Pr/(1+Pr))/dT =
+    (d ln k0 - d ln k_inf)/(1+Pr) and d ln F/dT = ln 10 [dlFc/(1+x^2) - 2 x lFc dx/(1+x^2)^2]
+    with du = (d ln k0 - d ln k_inf)/ln 10 - 0.67 dlFc (dlFc = 0 where F_cent is constant).
+    Every term is accumulated straight into the scaled matrix (s J, s = -gamma h for the
+    integrator's iteration matrix)."""
     ns, nr = m.n_species, m.n_reactions
     W = [m.W[k] for k in range(ns)]
     add = L.append
-    add("// s times the species columns of the Jacobian of F (rhs_k) with respect to (Y, T):")
-    add("// J(k, j) = s dF_k / dY_j for j < NS and every row k <= NS, at fixed temperature and")
-    add("// density, from the factors at y's temperature and F = rhs_k(K, rho, y).  Column NS is not")
-    add("// written.")
+    add("// s times the Jacobian of F (rhs_k) with respect to (Y, T): J(k, j) = s dF_k / dY_j for")
+    add("// j < NS and J(k, NS) = s dF_k / dT, every row k <= NS, at fixed density, from the factors")
+    add("// at y's temperature and F = rhs_k(K, rho, y).")
     add("template <class Mat>")
-    add("GAS_HD void jac_species(const Factors &K, double rho, const double *y, const double *F, double s, Mat &J) {")
+    add("GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, double s, Mat &J) {")
     add(f"    const double T = y[{ns}];")
+    add(f"    const double invT = 1.0 / T, invRT = 1.0 / ({lit(KR)} * T);")
     for k in range(ns):
         add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
     add("    double cv = 0.0;")
@@ -115,10 +167,12 @@ def emit_jacobian(m, L, fidx):
         add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
     add(f"    cv *= {lit(KR)};")
     add(f"    const double sT = -s * {lit(KR)} * T / cv;  // times e_r dq_rj / W_j: the T row")
+    add("    const double s_rho = s / rho;")
+    add("    double sum_eT = 0.0;  // sum_r e_r dq_r/dT")
     add("#pragma unroll")
     add(f"    for (int k = 0; k <= {ns}; ++k)")
     add("#pragma unroll")
-    add(f"        for (int j = 0; j < {ns}; ++j) J(k, j) = 0.0;")
+    add(f"        for (int j = 0; j <= {ns}; ++j) J(k, j) = 0.0;")
     for r in range(nr):
         reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
         prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
@@ -129,9 +183,17 @@ def emit_jacobian(m, L, fidx):
         for k, nu in prod:
             net[k] = net.get(k, 0.0) + nu
         net = {k: v for k, v in net.items() if v != 0.0}
+        rev = bool(m.reversible[r])
+        dlnkf = f"({lit(m.b[r])} + {lit(m.Ea[r])} * invRT) * invT"
         add(f"    {{  // reaction {r}")
+        pf = " * ".join(conc(k, nu) for k, nu in ordr)
+        pb = " * ".join(conc(k, nu) for k, nu in prod)
+        add(f"        const double pf = {pf};")
+        if rev:
+            add(f"        const double pb = {pb};")
         if m.rtype[r] == 0:
             add(f"        const double kfM = K.kf[{r}];")
+            add(f"        const double dlnk = {dlnkf};")
         else:
             effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
             msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
@@ -139,32 +201,75 @@ def emit_jacobian(m, L, fidx):
             if m.rtype[r] == FALLOFF:
                 i = fidx[r]
                 add(f"        const double Pr = K.k0[{i}] * M / K.kf[{r}];")
+                add("        const double ipr = 1.0 / (1.0 + Pr);")
+                add(f"        const double dlnkinf = {dlnkf};")
+                add(f"        const double dlnk0 = ({lit(m.b0[r])} + {lit(m.Ea0[r])} * invRT) * invT;")
                 if m.troe_n[r] >= 3:
                     add(f"        const double lFc = K.lFc[{i}];")
                     add("        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
                     add("        const double lPr = log10(fmax(Pr, 1e-300));")
                     add("        const double u = lPr + c, den = n - 0.14 * u;")
                     add("        const double x = u / den;")
-                    add("        const double Fo = pow(10.0, lFc / (1.0 + x * x));")
-                    add("        const double ipr = 1.0 / (1.0 + Pr);")
-                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr) * Fo;")
                     add("        const double opx = 1.0 + x * x;")
+                    add("        const double Fo = pow(10.0, lFc / opx);")
+                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr) * Fo;")
                     add(f"        const double dkdM = K.k0[{i}] * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));")
+                    # temperature derivative of F_cent (zero where it is a constant)
+                    if troe_constant(m, r) is not None:
+                        add("        const double dlFc = 0.0;")
+                    else:
+                        a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
+                        terms = troe_terms(m, r)
+                        fc, dfc = [], []
+                        if terms[0][0] == "exp":
+                            add(f"        const double e3 = exp(-T / {lit(T3)});")
+                            fc.append(f"{lit(1.0 - a)} * e3")
+                            dfc.append(f"-{lit((1.0 - a) / T3)} * e3")
+                        elif terms[0][0] == "one":
+                            fc.append(lit(1.0 - a))
+                        if terms[1][0] == "exp":
+                            add(f"        const double e1 = exp(-T / {lit(T1)});")
+                            fc.append(f"{lit(a)} * e1")
+                            dfc.append(f"-{lit(a / T1)} * e1")
+                        elif terms[1][0] == "one":
+                            fc.append(lit(a))
+                        if len(terms) == 3:
+                            T2 = m.troe[r][3]
+                            if terms[2][0] == "exp":
+                                add(f"        const double e2 = exp({lit(-T2)} / T);")
+                                fc.append("e2")
+                                dfc.append(f"{lit(T2)} * invT * invT * e2")
+                            elif terms[2][0] == "one":
+                                fc.append("1.0")
+                        add(f"        const double Fc = fmax({' + '.join(fc) or '0.0'}, 1e-300);")
+                        add(f"        const double dlFc = ({' + '.join(dfc) or '0.0'}) / (Fc * 2.302585092994046);")
+                    add("        const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;")
+                    add("        const double dden = -1.27 * dlFc - 0.14 * du;")
+                    add("        const double dx = (du * den - u * dden) / (den * den);")
+                    add("        const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));")
+                    add("        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;")
                 else:
-                    add("        const double ipr = 1.0 / (1.0 + Pr);")
                     add(f"        const double kfM = K.kf[{r}] * (Pr * ipr);")
                     add(f"        const double dkdM = K.k0[{i}] * ipr * ipr;")
+                    add("        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr;")
             else:
                 add(f"        const double kfM = K.kf[{r}] * M;")
                 add(f"        const double dkdM = K.kf[{r}];")
-        pf = " * ".join(conc(k, nu) for k, nu in ordr)
-        rev = bool(m.reversible[r])
+                add(f"        const double dlnk = {dlnkf};")
         if m.rtype[r] != 0:
-            pb = " * ".join(conc(k, nu) for k, nu in prod)
             if rev:
-                add(f"        const double g = dkdM * ({pf} - K.er[{r}] * {pb});")
+                add(f"        const double g = dkdM * (pf - K.er[{r}] * pb);")
             else:
-                add(f"        const double g = dkdM * {pf};")
+                add("        const double g = dkdM * pf;")
+        # d q / dT at fixed concentrations
+        if rev:
+            dnu = sum(nu for _, nu in prod) - sum(nu for _, nu in reac)
+            dh = " + ".join([f"{lit(nu)} * K.hRT[{k}]" for k, nu in prod]) + " - (" + \
+                " + ".join([f"{lit(nu)} * K.hRT[{k}]" for k, nu in reac]) + ")"
+            add(f"        const double dlner = ({lit(dnu)} - ({dh})) * invT;")
+            add(f"        const double dqT = kfM * (dlnk * (pf - K.er[{r}] * pb) - K.er[{r}] * dlner * pb);")
+        else:
+            add("        const double dqT = kfM * dlnk * pf;")
         dq = {}
         for idx, (k, nu) in enumerate(ordr):
             others = [x for jdx, x in enumerate(ordr) if jdx != idx]
@@ -188,17 +293,31 @@ def emit_jacobian(m, L, fidx):
             expr = " ".join(parts)
             expr = expr[2:] if expr.startswith("+ ") else "-" + expr[2:]
             add(f"        const double dq{j} = {expr};")
-        # e_r = sum_k nu_kr (h_k/RT - 1) for the T row
         er_terms = " + ".join(f"{lit(v)} * (K.hRT[{k}] - 1.0)" for k, v in net.items()) or "0.0"
-        add(f"        const double eT = sT * ({er_terms});")
+        add(f"        const double e_r = {er_terms};")
+        add("        const double eT = sT * e_r;")
+        add("        sum_eT += e_r * dqT;")
         for j in cols:
             for k, v in net.items():
                 add(f"        J({k}, {j}) += {lit(v * W[k] / W[j])} * s * dq{j};")
             add(f"        J({ns}, {j}) += {lit(1.0 / W[j])} * eT * dq{j};")
+        for k, v in net.items():
+            add(f"        J({k}, {ns}) += {lit(v * W[k])} * s_rho * dqT;")
         add("    }")
+    # the T row's composition columns: the c_v term
     add(f"    const double sF = s * F[{ns}] * {lit(KR)} / cv;")
     for j in range(ns):
         add(f"    J({ns}, {j}) -= sF * (K.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
+    # the T row's T column
+    add("    double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R")
+    for k in range(ns):
+        add(f"    sw += (K.cpR[{k}] - 1.0) * F[{k}] * rho * {lit(1.0 / m.W[k])};")
+
+    def dcp(k, a):
+        add(f"        dcv += y[{k}] * {lit(1.0 / m.W[k])} * ({lit(a[1])} + T * ({lit(2 * a[2])} + T * ({lit(3 * a[3])} + "
+            f"T * {lit(4 * a[4])})));")
+    nasa_branches(m, add, dcp)
+    add(f"    J({ns}, {ns}) = s * (-{lit(KR)} * (sw + T * sum_eT) / (rho * cv) - F[{ns}] * {lit(KR)} * dcv / cv);")
     add("}")
     add("")
 
@@ -289,7 +408,10 @@ def generate(m, name):
         if m.rtype[r] == FALLOFF:
             i = fidx[r]
             add(f"    K.k0[{i}] = {arrhenius(m.A0[r], m.b0[r], m.Ea0[r])};")
-            if m.troe_n[r] >= 3:
+            if m.troe_n[r] >= 3 and troe_constant(m, r) is not None:
+                # every F_cent term is exactly 0 or 1 at physical temperatures (troe_terms)
+                add(f"    K.lFc[{i}] = {troe_constant(m, r)};")
+            elif m.troe_n[r] >= 3:
                 a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
                 add("    {")
                 add(f"        double Fc = {lit(1.0 - a)} * exp(-T / {lit(T3)}) + {lit(a)} * exp(-T / {lit(T1)});")
@@ -374,7 +496,7 @@ def generate(m, name):
     add("")
     emit_jacobian(m, L, fidx)
     add("// The integrator's kinetics policy (gas::ros2_advance_k): factors once per temperature,")
-    add("// right-hand sides from them, the species columns of the Jacobian analytically.")
+    add("// right-hand sides from them, the Jacobian analytically.")
     add("struct Kinetics {")
     add("    using K = Factors;")
     add("    static constexpr bool kAnalyticJacobian = true;")
@@ -384,7 +506,7 @@ def generate(m, name):
     add("    }")
     add("    template <class Mat>")
     add("    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F, double s, Mat &J) const {")
-    add("        jac_species(k, rho, y, F, s, J);")
+    add("        jac(k, rho, y, F, s, J);")
     add("    }")
     add("};")
     add("")
