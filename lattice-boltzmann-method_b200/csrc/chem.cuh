@@ -161,9 +161,11 @@ struct SharedMat {
     GAS_HD double &operator()(int r, int c) const { return p[(r * N + c) * stride]; }
 };
 
-// lu_factor / lu_solve for a matrix of compile-time size N (the device integrator).
+// lu_factor / lu_solve for a matrix of compile-time size N (the device integrator): the same
+// partial pivoting and elimination, each pivot inverted once (dinv) so that the multipliers and
+// the back substitution multiply instead of dividing.
 template <int N, class Mat>
-GAS_HD bool lu_factor_n(Mat &M, int *piv) {
+GAS_HD bool lu_factor_n(Mat &M, int *piv, double *dinv) {
     for (int c = 0; c < N; ++c) {
         int p = c;
         for (int r = c + 1; r < N; ++r)
@@ -176,8 +178,10 @@ GAS_HD bool lu_factor_n(Mat &M, int *piv) {
                 M(c, q) = M(p, q);
                 M(p, q) = tmp;
             }
+        const double inv = 1.0 / M(c, c);
+        dinv[c] = inv;
         for (int r = c + 1; r < N; ++r) {
-            const double f = M(r, c) / M(c, c);
+            const double f = M(r, c) * inv;
             M(r, c) = f;
             for (int q = c + 1; q < N; ++q) M(r, q) -= f * M(c, q);
         }
@@ -185,7 +189,7 @@ GAS_HD bool lu_factor_n(Mat &M, int *piv) {
     return true;
 }
 template <int N, class Mat>
-GAS_HD void lu_solve_n(const Mat &M, const int *piv, double *b) {
+GAS_HD void lu_solve_n(const Mat &M, const int *piv, const double *dinv, double *b) {
     for (int c = 0; c < N; ++c) {
         const double tmp = b[c];
         b[c] = b[piv[c]];
@@ -196,7 +200,7 @@ GAS_HD void lu_solve_n(const Mat &M, const int *piv, double *b) {
     for (int r = N - 1; r >= 0; --r) {
         double v = b[r];
         for (int q = r + 1; q < N; ++q) v -= M(r, q) * b[q];
-        b[r] = v / M(r, r);
+        b[r] = v * dinv[r];
     }
 }
 
@@ -324,7 +328,7 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
                            double atol = 1e-10, double atol_T = 1e-3) {
     constexpr int ns = NS, n = NS + 1;
     const double gam = 1.0 + 1.0 / sqrt(2.0);
-    double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
+    double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n], dinv[n];
     int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
@@ -369,20 +373,20 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
             for (int r = 0; r < n; ++r) M(r, ns) = -gam * h * (Fp[r] - F0[r]) / eps;
         }
         for (int r = 0; r < n; ++r) M(r, r) += 1.0;
-        if (!lu_factor_n<n>(M, piv)) {
+        if (!lu_factor_n<n>(M, piv, dinv)) {
             h *= 0.25;
             continue;
         }
 #pragma unroll
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
-        lu_solve_n<n>(M, piv, k1);
+        lu_solve_n<n>(M, piv, dinv, k1);
 #pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
         kin.factors(yp[ns], Kf);
         kin.rhs(Kf, rho, yp, Fp);
 #pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
-        lu_solve_n<n>(M, piv, k2);
+        lu_solve_n<n>(M, piv, dinv, k2);
         double err = 0.0;
 #pragma unroll
         for (int q = 0; q < n; ++q) {
@@ -442,6 +446,7 @@ __device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double 
     double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n];
     double Fc[kPer][n], ec[kPer];  // this lane's right-hand sides and their steps
     RegMat<n> M;
+    double dinv[n];
     int piv[n];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
@@ -490,13 +495,13 @@ __device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double 
 #pragma unroll
             for (int r = 0; r < n; ++r) M(r, c) = __shfl_sync(gmask, Fc[c / G][r], c % G, G);
         for (int r = 0; r < n; ++r) M(r, r) += 1.0;
-        if (!lu_factor_n<n>(M, piv)) {
+        if (!lu_factor_n<n>(M, piv, dinv)) {
             h *= 0.25;
             continue;
         }
 #pragma unroll
         for (int q = 0; q < n; ++q) k1[q] = F0[q];
-        lu_solve_n<n>(M, piv, k1);
+        lu_solve_n<n>(M, piv, dinv, k1);
 #pragma unroll
         for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
         {
@@ -506,7 +511,7 @@ __device__ int ros2_advance_group(const Kin &kin, double rho, double *Y, double 
         }
 #pragma unroll
         for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
-        lu_solve_n<n>(M, piv, k2);
+        lu_solve_n<n>(M, piv, dinv, k2);
         double err = 0.0;
 #pragma unroll
         for (int q = 0; q < n; ++q) {

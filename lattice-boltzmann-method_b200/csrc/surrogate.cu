@@ -434,27 +434,32 @@ __global__ void __launch_bounds__(kTcRows *kTcGroups, 1)
 // BF16 row-major with leading dimensions lda, ldb (multiples of 8), K a multiple of 16.  A
 // CTA computes a 128 x 64 tile: K in chunks of 64 staged by its 128 threads into shared
 // memory in the canonical layout of the network kernel (rows and columns past M, N, K
-// zero-filled), four tcgen05.mma per chunk into a tensor-memory accumulator, a commit to
-// an mbarrier and a bounded wait before the next chunk reuses the buffers; the epilogue
-// reads the accumulator with tcgen05.ld.  With gridDim.z > 1 block z takes the z-th of
-// gridDim.z equal slices of K (each a multiple of 16) and writes its partial product to
-// C + z zstride (split K, summed afterwards by k_sum_splits).
+// zero-filled), four tcgen05.mma per chunk into a tensor-memory accumulator, a commit to the
+// stage's mbarrier; two stages, so that the next chunk is staged while the tensor core works
+// on this one (a stage is refilled after a bounded wait for the MMAs that read it two chunks
+// earlier).  The epilogue reads the accumulator with tcgen05.ld.  With gridDim.z > 1 block z
+// takes the z-th of gridDim.z equal slices of K (each a multiple of 16) and writes its partial
+// product to C + z zstride (split K, summed afterwards by k_sum_splits).
 constexpr int kGmM = 128, kGmN = 64, kGmK = 64;
-constexpr int kGmA = 0, kGmB = kGmA + kGmM * kGmK * 2, kGmBar = kGmB + kGmN * kGmK * 2, kGmSlot = kGmBar + 8,
+constexpr int kGmStage = kGmM * kGmK * 2 + kGmN * kGmK * 2;  // A then B of one chunk
+constexpr int kGmA = 0, kGmB = kGmM * kGmK * 2, kGmBar = 2 * kGmStage, kGmSlot = kGmBar + 16,
               kGmSmem = kGmSlot + 8;
+static_assert(kGmStage % 128 == 0 && kGmBar % 8 == 0, "stage buffers 128-byte, mbarriers 8-byte aligned");
 __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict__ Am, int lda,
                                                  const __nv_bfloat16 *__restrict__ Bm, int ldb, float *__restrict__ C,
                                                  int ldc, int M, int N, int K, int accum, long zstride,
                                                  unsigned *__restrict__ status) {
-    __shared__ __align__(128) unsigned char sm[kGmSmem];
+    extern __shared__ __align__(128) unsigned char gsm[];
+    unsigned char *sm = gsm;
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t base = (uint32_t)__cvta_generic_to_shared(sm);
     const int m0 = blockIdx.y * kGmM, n0 = blockIdx.x * kGmN;
     const int kc = K / (int)gridDim.z, kbeg = (int)blockIdx.z * kc;
     C += (long)blockIdx.z * zstride;
-    const uint32_t bar = base + kGmBar;
+    const uint32_t bar0 = base + kGmBar;
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -467,21 +472,33 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(sm + kGmSlot);
-    uint32_t phase = 0;
+    uint32_t phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};  // a commit of the stage not yet waited for
     bool ok = true;
-    for (int k0 = kbeg; k0 < kbeg + kc && ok; k0 += kGmK) {
+    int it = 0;
+    for (int k0 = kbeg; k0 < kbeg + kc && ok; k0 += kGmK, ++it) {
+        const int st = it & 1;
+        const uint32_t bar = bar0 + 8u * (uint32_t)st;
+        if (pending[st]) {  // the MMAs of chunk it - 2 read this stage
+            ok = __syncthreads_and(tc_wait(bar, phase[st])) != 0;
+            tc_fence_after();
+            if (!ok) break;
+            phase[st] ^= 1u;
+            pending[st] = false;
+        }
+        unsigned char *sa = sm + st * kGmStage + kGmA, *sb = sm + st * kGmStage + kGmB;
         // stage the chunk: A rows m0.., B rows n0.., 16-byte pieces (8 elements of K)
         for (int i = tid; i < kGmM * (kGmK / 8); i += 128) {
             const int r = i / (kGmK / 8), c = i % (kGmK / 8), k = k0 + c * 8;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (m0 + r < M && k < kbeg + kc) v = *reinterpret_cast<const uint4 *>(Am + (long)(m0 + r) * lda + k);
-            *reinterpret_cast<uint4 *>(sm + kGmA + tc_off(r, c * 8, kGmK)) = v;
+            *reinterpret_cast<uint4 *>(sa + tc_off(r, c * 8, kGmK)) = v;
         }
         for (int i = tid; i < kGmN * (kGmK / 8); i += 128) {
             const int r = i / (kGmK / 8), c = i % (kGmK / 8), k = k0 + c * 8;
             uint4 v = make_uint4(0u, 0u, 0u, 0u);
             if (n0 + r < N && k < kbeg + kc) v = *reinterpret_cast<const uint4 *>(Bm + (long)(n0 + r) * ldb + k);
-            *reinterpret_cast<uint4 *>(sm + kGmB + tc_off(r, c * 8, kGmK)) = v;
+            *reinterpret_cast<uint4 *>(sb + tc_off(r, c * 8, kGmK)) = v;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
@@ -489,9 +506,10 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
         tc_fence_after();
         if (tid == 0) {
             const uint32_t idesc = tc_idesc(kGmN);
+            const uint32_t abase = base + (uint32_t)(st * kGmStage + kGmA), bbase = base + (uint32_t)(st * kGmStage + kGmB);
             for (int s = 0; s < kGmK / 16; ++s) {
-                const uint64_t ad = tc_desc(base + kGmA + 256u * s, kGmK * 16u);
-                const uint64_t bd = tc_desc(base + kGmB + 256u * s, kGmK * 16u);
+                const uint64_t ad = tc_desc(abase + 256u * s, kGmK * 16u);
+                const uint64_t bd = tc_desc(bbase + 256u * s, kGmK * 16u);
                 const uint32_t acc = (k0 > kbeg || s > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
@@ -502,11 +520,16 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                          : "memory");
         }
-        ok = __syncthreads_and(tc_wait(bar, phase)) != 0;
-        tc_fence_after();
-        if (!ok) break;
-        phase ^= 1u;
+        pending[st] = true;
     }
+    // drain: the commits still outstanding (the last of each stage), each wait bounded; also
+    // after a timed-out wait, so that no MMA is left running when the tensor memory is freed
+    for (int s2 = 0; s2 < 2; ++s2)
+        if (pending[s2]) {
+            const bool done = __syncthreads_and(tc_wait(bar0 + 8u * (uint32_t)s2, phase[s2])) != 0;
+            tc_fence_after();
+            ok = ok && done;
+        }
     if (ok && kc > 0) {  // epilogue: row m0 + tid of the tile, 64 columns in four loads
         const long r = m0 + tid;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
@@ -526,11 +549,7 @@ __global__ void __launch_bounds__(128) k_gemm_tn(const __nv_bfloat16 *__restrict
                 }
         }
     }
-    if (!ok) {  // the tensor core may still be working on the timed-out chunk: one more bounded wait
-        if (tid == 0) atomicOr(status, (unsigned)LBMGPU_ST_SURROGATE);
-        tc_wait(bar, phase);
-        tc_fence_after();
-    }
+    if (!ok && tid == 0) atomicOr(status, (unsigned)LBMGPU_ST_SURROGATE);
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
@@ -725,7 +744,8 @@ inline unsigned blocks(long n, int b = 256) { return (unsigned)((n + b - 1) / b)
 // k_gemm_tn over the whole C (splits > 1: split K, partials zstride apart).
 void gemm_tn(lbmgpu *h, const __nv_bfloat16 *A, int lda, const __nv_bfloat16 *Bm, int ldb, float *C, int ldc, int M,
              int N, int K, int accum = 0, int splits = 1, long zstride = 0) {
-    k_gemm_tn<<<dim3((N + kGmN - 1) / kGmN, (M + kGmM - 1) / kGmM, splits), 128, 0, h->stream>>>(
+    cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, kGmSmem);
+    k_gemm_tn<<<dim3((N + kGmN - 1) / kGmN, (M + kGmM - 1) / kGmM, splits), 128, kGmSmem, h->stream>>>(
         A, lda, Bm, ldb, C, ldc, M, N, K, accum, zstride, h->status);
 }
 
