@@ -14,6 +14,8 @@
 #pragma once
 #include <math.h>
 
+#include <type_traits>
+
 #include "gas.cuh"
 
 namespace gas {
@@ -163,26 +165,58 @@ struct SharedMat {
 
 // lu_factor / lu_solve for a matrix of compile-time size N (the device integrator): the same
 // partial pivoting and elimination, each pivot inverted once (dinv) so that the multipliers and
-// the back substitution multiply instead of dividing.
+// the back substitution multiply instead of dividing.  Every loop is unrolled, so piv, dinv
+// and b are indexed by constants only: a row interchange with a register matrix, and the
+// interchanges applied to b, select among the candidate rows instead of indexing by the
+// pivot (an index known only at run time would put the array in local memory).
+template <class Mat>
+struct MatRowsAddressable : std::false_type {};
+template <int N>
+struct MatRowsAddressable<SharedMat<N>> : std::true_type {};
+
 template <int N, class Mat>
 GAS_HD bool lu_factor_n(Mat &M, int *piv, double *dinv) {
+#pragma unroll
     for (int c = 0; c < N; ++c) {
         int p = c;
-        for (int r = c + 1; r < N; ++r)
-            if (fabs(M(r, c)) > fabs(M(p, c))) p = r;
-        piv[c] = p;
-        if (M(p, c) == 0.0) return false;
-        if (p != c)
-            for (int q = 0; q < N; ++q) {
-                const double tmp = M(c, q);
-                M(c, q) = M(p, q);
-                M(p, q) = tmp;
+        double best = fabs(M(c, c));
+#pragma unroll
+        for (int r = c + 1; r < N; ++r) {
+            const double v = fabs(M(r, c));
+            if (v > best) {
+                best = v;
+                p = r;
             }
+        }
+        piv[c] = p;
+        if (best == 0.0) return false;
+        if (p != c) {
+            if constexpr (MatRowsAddressable<Mat>::value) {
+#pragma unroll
+                for (int q = 0; q < N; ++q) {
+                    const double tmp = M(c, q);
+                    M(c, q) = M(p, q);
+                    M(p, q) = tmp;
+                }
+            } else {
+#pragma unroll
+                for (int r = c + 1; r < N; ++r)
+                    if (r == p)
+#pragma unroll
+                        for (int q = 0; q < N; ++q) {
+                            const double tmp = M(c, q);
+                            M(c, q) = M(r, q);
+                            M(r, q) = tmp;
+                        }
+            }
+        }
         const double inv = 1.0 / M(c, c);
         dinv[c] = inv;
+#pragma unroll
         for (int r = c + 1; r < N; ++r) {
             const double f = M(r, c) * inv;
             M(r, c) = f;
+#pragma unroll
             for (int q = c + 1; q < N; ++q) M(r, q) -= f * M(c, q);
         }
     }
@@ -190,15 +224,25 @@ GAS_HD bool lu_factor_n(Mat &M, int *piv, double *dinv) {
 }
 template <int N, class Mat>
 GAS_HD void lu_solve_n(const Mat &M, const int *piv, const double *dinv, double *b) {
+#pragma unroll
     for (int c = 0; c < N; ++c) {
-        const double tmp = b[c];
-        b[c] = b[piv[c]];
-        b[piv[c]] = tmp;
+        const int p = piv[c];
+#pragma unroll
+        for (int q = c + 1; q < N; ++q)
+            if (q == p) {
+                const double tmp = b[c];
+                b[c] = b[q];
+                b[q] = tmp;
+            }
     }
+#pragma unroll
     for (int r = 1; r < N; ++r)
+#pragma unroll
         for (int q = 0; q < r; ++q) b[r] -= M(r, q) * b[q];
+#pragma unroll
     for (int r = N - 1; r >= 0; --r) {
         double v = b[r];
+#pragma unroll
         for (int q = r + 1; q < N; ++q) v -= M(r, q) * b[q];
         b[r] = v * dinv[r];
     }
@@ -288,13 +332,14 @@ GAS_HD int ros2_advance(const Tables &t, double rho, double *Y, double &T, doubl
     return done ? acc : -1;
 }
 
-// The kinetics policies ros2_advance_k takes: `K` the temperature factors, `factors(T, K)`
-// forms them, `rhs(K, rho, y, F)` is the reactor's right-hand side at y from the factors at
-// y's temperature; with kAnalyticJacobian, `jacobian(K, rho, y, F, s, J)` writes s times the
-// Jacobian dF/d(Y, T) (its columns are finite differences otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its
-// factors inside each right-hand side (reactor_rhs_dense: nothing per reaction kept between
-// calls); a mechanism compiled to straight-line code (gen_kinetics.py) provides its own policy
-// whose factors are formed once per temperature.
+// The kinetics policies ros2_advance_k takes: `K` what is formed once per temperature,
+// `factors(T, K)` forms it, `rhs(K, rho, y, F)` is the reactor's right-hand side at y from K at
+// y's temperature; with kAnalyticJacobian, `rhs_jacobian(K, rho, y, F, s, J)` writes that
+// right-hand side and s times the Jacobian dF/d(Y, T) (its columns are finite differences
+// otherwise).  TableKinetics evaluates any mechanism from the tables, recomputing its factors
+// inside each right-hand side (reactor_rhs_dense: nothing per reaction kept between calls); a
+// mechanism compiled to straight-line code (gen_kinetics.py) provides its own policy, whose K
+// is the species' thermo and whose rate constants are formed reaction by reaction.
 template <int NS>
 struct TableKinetics {
     static constexpr bool kAnalyticJacobian = false;
@@ -338,14 +383,14 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
     for (int it = 0; it < kChemMaxSub && !done; ++it) {
         const bool last = tt + h >= dt;
         if (last) h = dt - tt;
-        // one set of temperature factors, formed at y, then at the temperature column's and
-        // the second stage's temperatures in turn
+        // one set of temperature factors, formed at y, then at the temperature column's (finite
+        // differences) and the second stage's temperatures in turn
         typename Kin::K Kf;
         kin.factors(y[ns], Kf);
-        kin.rhs(Kf, rho, y, F0);
         if constexpr (Kin::kAnalyticJacobian) {
-            kin.jacobian(Kf, rho, y, F0, -gam * h, M);
+            kin.rhs_jacobian(Kf, rho, y, F0, -gam * h, M);
         } else {
+            kin.rhs(Kf, rho, y, F0);
             // the species columns in a rolled loop (one inlined right-hand side); the perturbed
             // component is selected by comparison so that yp stays in registers
 #pragma unroll 1

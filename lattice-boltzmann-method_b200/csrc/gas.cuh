@@ -36,6 +36,16 @@
 #define GAS_HD inline
 #endif
 
+// A point that the compiler moves no memory access across (device code only): placed between
+// the reactions of the straight-line kinetics, it keeps the accumulations into the iteration
+// matrix and the scheduling of each reaction's terms local to that reaction, which bounds the
+// live registers of the unrolled code.
+#if defined(__CUDA_ARCH__)
+#define GAS_SCHED_FENCE() __asm__ volatile("" ::: "memory")
+#else
+#define GAS_SCHED_FENCE() ((void)0)
+#endif
+
 namespace gas {
 
 constexpr double kR = 8314.46261815324;       // J / (kmol K)  (Cantera::GasConstant)

@@ -1,6 +1,6 @@
 // Generated by gen_kinetics.py from the mechanism h2_air_9 -- do not edit; `make` regenerates it.
-// Its kinetics as straight-line code: gas.cuh's rate_factors (factors) and reactor_rhs_k
-// (rhs_k) with the mechanism's constants inlined.
+// Its kinetics as straight-line code: gas.cuh's rate_factors and reactor_rhs_k (thermo, rhs_t)
+// and their analytic Jacobian (rhs_jac) with the mechanism's constants inlined.
 #pragma once
 #include <math.h>
 #include "gas.cuh"
@@ -283,130 +283,84 @@ inline bool matches(const lbmgpu_mech &m) {
     return true;
 }
 
-// The temperature-only factors (gas::RateT): k_inf (k for non-fall-off reactions), the
-// fall-off k_0 and log10 F_cent, the reverse factors exp(dG/RT - dnu ln(p_atm / R T)) and
-// the species' h/RT and c_p/R.
-struct Factors {
-    double kf[NR], er[NR], k0[NF], lFc[NF], hRT[NS], cpR[NS];
+// The species' thermo at one temperature (NASA-7): h/RT, g/RT and c_p/R, with ln T, 1/RT and
+// ln(p_atm / R T); the rate constants are formed from them reaction by reaction where they
+// are used (rhs_t, rhs_jac), so that no per-reaction array stays live across the kinetics.
+struct Thermo {
+    double hRT[NS], gRT[NS], cpR[NS], logT, invRT, log_cref;
 };
 
-GAS_HD void factors(double T, Factors &K) {
-    const double logT = log(T), invRT = 1.0 / (8314.46261815324 * T);
-    const double log_cref = log(101325.0 / (8314.46261815324 * T));
-    double gRT[9];
+GAS_HD void thermo(double T, Thermo &th) {
+    const double logT = log(T);
+    th.logT = logT;
+    th.invRT = 1.0 / (8314.46261815324 * T);
+    th.log_cref = log(101325.0 / (8314.46261815324 * T));
     if (T < 1000.0) {
-        K.cpR[0] = 2.37694204 + T * (0.00773916922 + T * (-1.88735073e-05 + T * (1.95517114e-08 + T * -7.17095663e-12)));
-        K.hRT[0] = 2.37694204 + T * (0.00386958461 + T * (-6.291169099999999e-06 + T * (4.88792785e-09 + T * -7.17095663e-12 / 5.0))) + -921.173081 / T;
-        gRT[0] = K.hRT[0] - (2.37694204 * logT + T * (0.00773916922 + T * (-9.43675365e-06 + T * (6.517237133333333e-09 + T * -1.7927391575e-12))) + 0.547184736);
-        K.cpR[1] = 2.49975925 + T * (6.73824499e-07 + T * (1.11807261e-09 + T * (-3.70192126e-12 + T * 2.14233822e-15)));
-        K.hRT[1] = 2.49975925 + T * (3.369122495e-07 + T * (3.7269087000000003e-10 + T * (-9.25480315e-13 + T * 2.14233822e-15 / 5.0))) + 25473.7665 / T;
-        gRT[1] = K.hRT[1] - (2.49975925 * logT + T * (6.73824499e-07 + T * (5.59036305e-10 + T * (-1.2339737533333333e-12 + T * 5.35584555e-16))) + -0.445574009);
-        K.cpR[2] = 3.78498258 + T * (-0.00302002233 + T * (9.92029171e-06 + T * (-9.77840434e-09 + T * 3.28877702e-12)));
-        K.hRT[2] = 3.78498258 + T * (-0.001510011165 + T * (3.3067639033333336e-06 + T * (-2.444601085e-09 + T * 3.28877702e-12 / 5.0))) + -1064.13589 / T;
-        gRT[2] = K.hRT[2] - (3.78498258 * logT + T * (-0.00302002233 + T * (4.960145855e-06 + T * (-3.2594681133333337e-09 + T * 8.22194255e-13))) + 3.64780709);
-        K.cpR[3] = 3.15906526 + T * (-0.00321509999 + T * (6.49255543e-06 + T * (-5.98755115e-09 + T * 2.06876117e-12)));
-        K.hRT[3] = 3.15906526 + T * (-0.001607549995 + T * (2.1641851433333333e-06 + T * (-1.4968877875e-09 + T * 2.06876117e-12 / 5.0))) + 29129.8453 / T;
-        gRT[3] = K.hRT[3] - (3.15906526 * logT + T * (-0.00321509999 + T * (3.246277715e-06 + T * (-1.995850383333333e-09 + T * 5.171902925e-13))) + 2.09078344);
-        K.cpR[4] = 4.20147551 + T * (-0.00205583546 + T * (6.56547207e-06 + T * (-5.5290696e-09 + T * 1.78282605e-12)));
-        K.hRT[4] = 4.20147551 + T * (-0.00102791773 + T * (2.1884906899999998e-06 + T * (-1.3822674e-09 + T * 1.78282605e-12 / 5.0))) + -30295.0066 / T;
-        gRT[4] = K.hRT[4] - (4.20147551 * logT + T * (-0.00205583546 + T * (3.282736035e-06 + T * (-1.8430232e-09 + T * 4.457065125e-13))) + -0.860610906);
-        K.cpR[5] = 3.97585165 + T * (-0.00228555291 + T * (4.33442882e-06 + T * (-3.5992664e-09 + T * 1.2670693e-12)));
-        K.hRT[5] = 3.97585165 + T * (-0.001142776455 + T * (1.4448096066666668e-06 + T * (-8.998166e-10 + T * 1.2670693e-12 / 5.0))) + 3393.41137 / T;
-        gRT[5] = K.hRT[5] - (3.97585165 * logT + T * (-0.00228555291 + T * (2.16721441e-06 + T * (-1.1997554666666665e-09 + T * 3.16767325e-13))) + -0.0355397262);
-        K.cpR[6] = 4.2385416 + T * (-0.000249610911 + T * (1.59857901e-05 + T * (-2.06919945e-08 + T * 8.2976632e-12)));
-        K.hRT[6] = 4.2385416 + T * (-0.0001248054555 + T * (5.3285966999999996e-06 + T * (-5.172998625e-09 + T * 8.2976632e-12 / 5.0))) + -17648.6003 / T;
-        gRT[6] = K.hRT[6] - (4.2385416 * logT + T * (-0.000249610911 + T * (7.99289505e-06 + T * (-6.8973315e-09 + T * 2.0744158e-12))) + 3.58850097);
-        K.cpR[7] = 4.2625125 + T * (-0.00445642032 + T * (2.05164934e-05 + T * (-2.35794011e-08 + T * 9.05614257e-12)));
-        K.hRT[7] = 4.2625125 + T * (-0.00222821016 + T * (6.8388311333333335e-06 + T * (-5.894850275e-09 + T * 9.05614257e-12 / 5.0))) + 262.442356 / T;
-        gRT[7] = K.hRT[7] - (4.2625125 * logT + T * (-0.00445642032 + T * (1.02582467e-05 + T * (-7.859800366666666e-09 + T * 2.2640356425e-12))) + 3.88223684);
-        K.cpR[8] = 3.53603521 + T * (-0.000158270944 + T * (-4.26984251e-07 + T * (2.3754259e-09 + T * -1.39708206e-12)));
-        K.hRT[8] = 3.53603521 + T * (-7.9135472e-05 + T * (-1.4232808366666666e-07 + T * (5.93856475e-10 + T * -1.39708206e-12 / 5.0))) + -1047.49645 / T;
-        gRT[8] = K.hRT[8] - (3.53603521 * logT + T * (-0.000158270944 + T * (-2.134921255e-07 + T * (7.918086333333333e-10 + T * -3.49270515e-13))) + 2.94603724);
+        th.cpR[0] = 2.37694204 + T * (0.00773916922 + T * (-1.88735073e-05 + T * (1.95517114e-08 + T * -7.17095663e-12)));
+        th.hRT[0] = 2.37694204 + T * (0.00386958461 + T * (-6.291169099999999e-06 + T * (4.88792785e-09 + T * -7.17095663e-12 / 5.0))) + -921.173081 / T;
+        th.gRT[0] = th.hRT[0] - (2.37694204 * logT + T * (0.00773916922 + T * (-9.43675365e-06 + T * (6.517237133333333e-09 + T * -1.7927391575e-12))) + 0.547184736);
+        th.cpR[1] = 2.49975925 + T * (6.73824499e-07 + T * (1.11807261e-09 + T * (-3.70192126e-12 + T * 2.14233822e-15)));
+        th.hRT[1] = 2.49975925 + T * (3.369122495e-07 + T * (3.7269087000000003e-10 + T * (-9.25480315e-13 + T * 2.14233822e-15 / 5.0))) + 25473.7665 / T;
+        th.gRT[1] = th.hRT[1] - (2.49975925 * logT + T * (6.73824499e-07 + T * (5.59036305e-10 + T * (-1.2339737533333333e-12 + T * 5.35584555e-16))) + -0.445574009);
+        th.cpR[2] = 3.78498258 + T * (-0.00302002233 + T * (9.92029171e-06 + T * (-9.77840434e-09 + T * 3.28877702e-12)));
+        th.hRT[2] = 3.78498258 + T * (-0.001510011165 + T * (3.3067639033333336e-06 + T * (-2.444601085e-09 + T * 3.28877702e-12 / 5.0))) + -1064.13589 / T;
+        th.gRT[2] = th.hRT[2] - (3.78498258 * logT + T * (-0.00302002233 + T * (4.960145855e-06 + T * (-3.2594681133333337e-09 + T * 8.22194255e-13))) + 3.64780709);
+        th.cpR[3] = 3.15906526 + T * (-0.00321509999 + T * (6.49255543e-06 + T * (-5.98755115e-09 + T * 2.06876117e-12)));
+        th.hRT[3] = 3.15906526 + T * (-0.001607549995 + T * (2.1641851433333333e-06 + T * (-1.4968877875e-09 + T * 2.06876117e-12 / 5.0))) + 29129.8453 / T;
+        th.gRT[3] = th.hRT[3] - (3.15906526 * logT + T * (-0.00321509999 + T * (3.246277715e-06 + T * (-1.995850383333333e-09 + T * 5.171902925e-13))) + 2.09078344);
+        th.cpR[4] = 4.20147551 + T * (-0.00205583546 + T * (6.56547207e-06 + T * (-5.5290696e-09 + T * 1.78282605e-12)));
+        th.hRT[4] = 4.20147551 + T * (-0.00102791773 + T * (2.1884906899999998e-06 + T * (-1.3822674e-09 + T * 1.78282605e-12 / 5.0))) + -30295.0066 / T;
+        th.gRT[4] = th.hRT[4] - (4.20147551 * logT + T * (-0.00205583546 + T * (3.282736035e-06 + T * (-1.8430232e-09 + T * 4.457065125e-13))) + -0.860610906);
+        th.cpR[5] = 3.97585165 + T * (-0.00228555291 + T * (4.33442882e-06 + T * (-3.5992664e-09 + T * 1.2670693e-12)));
+        th.hRT[5] = 3.97585165 + T * (-0.001142776455 + T * (1.4448096066666668e-06 + T * (-8.998166e-10 + T * 1.2670693e-12 / 5.0))) + 3393.41137 / T;
+        th.gRT[5] = th.hRT[5] - (3.97585165 * logT + T * (-0.00228555291 + T * (2.16721441e-06 + T * (-1.1997554666666665e-09 + T * 3.16767325e-13))) + -0.0355397262);
+        th.cpR[6] = 4.2385416 + T * (-0.000249610911 + T * (1.59857901e-05 + T * (-2.06919945e-08 + T * 8.2976632e-12)));
+        th.hRT[6] = 4.2385416 + T * (-0.0001248054555 + T * (5.3285966999999996e-06 + T * (-5.172998625e-09 + T * 8.2976632e-12 / 5.0))) + -17648.6003 / T;
+        th.gRT[6] = th.hRT[6] - (4.2385416 * logT + T * (-0.000249610911 + T * (7.99289505e-06 + T * (-6.8973315e-09 + T * 2.0744158e-12))) + 3.58850097);
+        th.cpR[7] = 4.2625125 + T * (-0.00445642032 + T * (2.05164934e-05 + T * (-2.35794011e-08 + T * 9.05614257e-12)));
+        th.hRT[7] = 4.2625125 + T * (-0.00222821016 + T * (6.8388311333333335e-06 + T * (-5.894850275e-09 + T * 9.05614257e-12 / 5.0))) + 262.442356 / T;
+        th.gRT[7] = th.hRT[7] - (4.2625125 * logT + T * (-0.00445642032 + T * (1.02582467e-05 + T * (-7.859800366666666e-09 + T * 2.2640356425e-12))) + 3.88223684);
+        th.cpR[8] = 3.53603521 + T * (-0.000158270944 + T * (-4.26984251e-07 + T * (2.3754259e-09 + T * -1.39708206e-12)));
+        th.hRT[8] = 3.53603521 + T * (-7.9135472e-05 + T * (-1.4232808366666666e-07 + T * (5.93856475e-10 + T * -1.39708206e-12 / 5.0))) + -1047.49645 / T;
+        th.gRT[8] = th.hRT[8] - (3.53603521 * logT + T * (-0.000158270944 + T * (-2.134921255e-07 + T * (7.918086333333333e-10 + T * -3.49270515e-13))) + 2.94603724);
     } else {
-        K.cpR[0] = 2.90207649 + T * (0.000868992581 + T * (-1.6586443e-07 + T * (1.90851899e-11 + T * -9.31121789e-16)));
-        K.hRT[0] = 2.90207649 + T * (0.0004344962905 + T * (-5.5288143333333333e-08 + T * (4.771297475e-12 + T * -9.31121789e-16 / 5.0))) + -797.948726 / T;
-        gRT[0] = K.hRT[0] - (2.90207649 * logT + T * (0.000868992581 + T * (-8.2932215e-08 + T * (6.361729966666667e-12 + T * -2.3278044725e-16))) + -0.84559132);
-        K.cpR[1] = 2.49985211 + T * (2.34582548e-07 + T * (-1.16171641e-10 + T * (2.25708298e-14 + T * -1.52992005e-18)));
-        K.hRT[1] = 2.49985211 + T * (1.17291274e-07 + T * (-3.8723880333333334e-11 + T * (5.64270745e-15 + T * -1.52992005e-18 / 5.0))) + 25473.8024 / T;
-        gRT[1] = K.hRT[1] - (2.49985211 * logT + T * (2.34582548e-07 + T * (-5.80858205e-11 + T * (7.523609933333334e-15 + T * -3.824800125e-19))) + -0.445864645);
-        K.cpR[2] = 3.65980488 + T * (0.000659877372 + T * (-1.44158172e-07 + T * (2.14656037e-11 + T * -1.36503784e-15)));
-        K.hRT[2] = 3.65980488 + T * (0.000329938686 + T * (-4.8052724e-08 + T * (5.366400925e-12 + T * -1.36503784e-15 / 5.0))) + -1216.03048 / T;
-        gRT[2] = K.hRT[2] - (3.65980488 * logT + T * (0.000659877372 + T * (-7.2079086e-08 + T * (7.155201233333333e-12 + T * -3.4125946e-16))) + 3.42074148);
-        K.cpR[3] = 2.55160087 + T * (-3.83085457e-05 + T * (8.43197478e-10 + T * (4.01267136e-12 + T * -4.17476574e-16)));
-        K.hRT[3] = 2.55160087 + T * (-1.915427285e-05 + T * (2.81065826e-10 + T * (1.00316784e-12 + T * -4.17476574e-16 / 5.0))) + 29228.7628 / T;
-        gRT[3] = K.hRT[3] - (2.55160087 * logT + T * (-3.83085457e-05 + T * (4.21598739e-10 + T * (1.33755712e-12 + T * -1.043691435e-16))) + 4.87617014);
-        K.cpR[4] = 2.73117512 + T * (0.00295136995 + T * (-8.35359785e-07 + T * (1.26088593e-10 + T * -8.40531676e-15)));
-        K.hRT[4] = 2.73117512 + T * (0.001475684975 + T * (-2.784532616666667e-07 + T * (3.152214825e-11 + T * -8.40531676e-15 / 5.0))) + -29916.9082 / T;
-        gRT[4] = K.hRT[4] - (2.73117512 * logT + T * (0.00295136995 + T * (-4.176798925e-07 + T * (4.2029531e-11 + T * -2.10132919e-15))) + 6.55183);
-        K.cpR[5] = 2.84581721 + T * (0.00109723818 + T * (-2.89121101e-07 + T * (4.0909991e-11 + T * -2.31382258e-15)));
-        K.hRT[5] = 2.84581721 + T * (0.00054861909 + T * (-9.637370033333334e-08 + T * (1.022749775e-11 + T * -2.31382258e-15 / 5.0))) + 3717.0661 / T;
-        gRT[5] = K.hRT[5] - (2.84581721 * logT + T * (0.00109723818 + T * (-1.445605505e-07 + T * (1.3636663666666666e-11 + T * -5.78455645e-16))) + 5.80339915);
-        K.cpR[6] = 4.5401748 + T * (0.00415970971 + T * (-1.30876777e-06 + T * (2.00823615e-10 + T * -1.15509243e-14)));
-        K.hRT[6] = 4.5401748 + T * (0.002079854855 + T * (-4.3625592333333335e-07 + T * (5.020590375e-11 + T * -1.15509243e-14 / 5.0))) + -17951.4029 / T;
-        gRT[6] = K.hRT[6] - (4.5401748 * logT + T * (0.00415970971 + T * (-6.54383885e-07 + T * (6.694120500000001e-11 + T * -2.887731075e-15))) + 0.855881745);
-        K.cpR[7] = 4.1056401 + T * (0.00204046836 + T * (-3.65877562e-07 + T * (1.85973044e-11 + T * 4.98818315e-16)));
-        K.hRT[7] = 4.1056401 + T * (0.00102023418 + T * (-1.2195918733333333e-07 + T * (4.6493261e-12 + T * 4.98818315e-16 / 5.0))) + 43.2898769 / T;
-        gRT[7] = K.hRT[7] - (4.1056401 * logT + T * (0.00204046836 + T * (-1.82938781e-07 + T * (6.199101466666667e-12 + T * 1.2470457875e-16))) + 3.30808126);
-        K.cpR[8] = 2.9380297 + T * (0.0014183803 + T * (-5.03281045e-07 + T * (8.07555464e-11 + T * -4.76064275e-15)));
-        K.hRT[8] = 2.9380297 + T * (0.00070919015 + T * (-1.6776034833333333e-07 + T * (2.01888866e-11 + T * -4.76064275e-15 / 5.0))) + -917.18099 / T;
-        gRT[8] = K.hRT[8] - (2.9380297 * logT + T * (0.0014183803 + T * (-2.516405225e-07 + T * (2.6918515466666668e-11 + T * -1.1901606875e-15))) + 5.95521985);
+        th.cpR[0] = 2.90207649 + T * (0.000868992581 + T * (-1.6586443e-07 + T * (1.90851899e-11 + T * -9.31121789e-16)));
+        th.hRT[0] = 2.90207649 + T * (0.0004344962905 + T * (-5.5288143333333333e-08 + T * (4.771297475e-12 + T * -9.31121789e-16 / 5.0))) + -797.948726 / T;
+        th.gRT[0] = th.hRT[0] - (2.90207649 * logT + T * (0.000868992581 + T * (-8.2932215e-08 + T * (6.361729966666667e-12 + T * -2.3278044725e-16))) + -0.84559132);
+        th.cpR[1] = 2.49985211 + T * (2.34582548e-07 + T * (-1.16171641e-10 + T * (2.25708298e-14 + T * -1.52992005e-18)));
+        th.hRT[1] = 2.49985211 + T * (1.17291274e-07 + T * (-3.8723880333333334e-11 + T * (5.64270745e-15 + T * -1.52992005e-18 / 5.0))) + 25473.8024 / T;
+        th.gRT[1] = th.hRT[1] - (2.49985211 * logT + T * (2.34582548e-07 + T * (-5.80858205e-11 + T * (7.523609933333334e-15 + T * -3.824800125e-19))) + -0.445864645);
+        th.cpR[2] = 3.65980488 + T * (0.000659877372 + T * (-1.44158172e-07 + T * (2.14656037e-11 + T * -1.36503784e-15)));
+        th.hRT[2] = 3.65980488 + T * (0.000329938686 + T * (-4.8052724e-08 + T * (5.366400925e-12 + T * -1.36503784e-15 / 5.0))) + -1216.03048 / T;
+        th.gRT[2] = th.hRT[2] - (3.65980488 * logT + T * (0.000659877372 + T * (-7.2079086e-08 + T * (7.155201233333333e-12 + T * -3.4125946e-16))) + 3.42074148);
+        th.cpR[3] = 2.55160087 + T * (-3.83085457e-05 + T * (8.43197478e-10 + T * (4.01267136e-12 + T * -4.17476574e-16)));
+        th.hRT[3] = 2.55160087 + T * (-1.915427285e-05 + T * (2.81065826e-10 + T * (1.00316784e-12 + T * -4.17476574e-16 / 5.0))) + 29228.7628 / T;
+        th.gRT[3] = th.hRT[3] - (2.55160087 * logT + T * (-3.83085457e-05 + T * (4.21598739e-10 + T * (1.33755712e-12 + T * -1.043691435e-16))) + 4.87617014);
+        th.cpR[4] = 2.73117512 + T * (0.00295136995 + T * (-8.35359785e-07 + T * (1.26088593e-10 + T * -8.40531676e-15)));
+        th.hRT[4] = 2.73117512 + T * (0.001475684975 + T * (-2.784532616666667e-07 + T * (3.152214825e-11 + T * -8.40531676e-15 / 5.0))) + -29916.9082 / T;
+        th.gRT[4] = th.hRT[4] - (2.73117512 * logT + T * (0.00295136995 + T * (-4.176798925e-07 + T * (4.2029531e-11 + T * -2.10132919e-15))) + 6.55183);
+        th.cpR[5] = 2.84581721 + T * (0.00109723818 + T * (-2.89121101e-07 + T * (4.0909991e-11 + T * -2.31382258e-15)));
+        th.hRT[5] = 2.84581721 + T * (0.00054861909 + T * (-9.637370033333334e-08 + T * (1.022749775e-11 + T * -2.31382258e-15 / 5.0))) + 3717.0661 / T;
+        th.gRT[5] = th.hRT[5] - (2.84581721 * logT + T * (0.00109723818 + T * (-1.445605505e-07 + T * (1.3636663666666666e-11 + T * -5.78455645e-16))) + 5.80339915);
+        th.cpR[6] = 4.5401748 + T * (0.00415970971 + T * (-1.30876777e-06 + T * (2.00823615e-10 + T * -1.15509243e-14)));
+        th.hRT[6] = 4.5401748 + T * (0.002079854855 + T * (-4.3625592333333335e-07 + T * (5.020590375e-11 + T * -1.15509243e-14 / 5.0))) + -17951.4029 / T;
+        th.gRT[6] = th.hRT[6] - (4.5401748 * logT + T * (0.00415970971 + T * (-6.54383885e-07 + T * (6.694120500000001e-11 + T * -2.887731075e-15))) + 0.855881745);
+        th.cpR[7] = 4.1056401 + T * (0.00204046836 + T * (-3.65877562e-07 + T * (1.85973044e-11 + T * 4.98818315e-16)));
+        th.hRT[7] = 4.1056401 + T * (0.00102023418 + T * (-1.2195918733333333e-07 + T * (4.6493261e-12 + T * 4.98818315e-16 / 5.0))) + 43.2898769 / T;
+        th.gRT[7] = th.hRT[7] - (4.1056401 * logT + T * (0.00204046836 + T * (-1.82938781e-07 + T * (6.199101466666667e-12 + T * 1.2470457875e-16))) + 3.30808126);
+        th.cpR[8] = 2.9380297 + T * (0.0014183803 + T * (-5.03281045e-07 + T * (8.07555464e-11 + T * -4.76064275e-15)));
+        th.hRT[8] = 2.9380297 + T * (0.00070919015 + T * (-1.6776034833333333e-07 + T * (2.01888866e-11 + T * -4.76064275e-15 / 5.0))) + -917.18099 / T;
+        th.gRT[8] = th.hRT[8] - (2.9380297 * logT + T * (0.0014183803 + T * (-2.516405225e-07 + T * (2.6918515466666668e-11 + T * -1.1901606875e-15))) + 5.95521985);
     }
-    K.kf[0] = 4.577000000000001e+16 * exp(-1.4 * logT - 436809600.0 * invRT);
-    K.er[0] = exp((2.0 * gRT[1] - gRT[0]) - 1.0 * log_cref);
-    K.kf[1] = 50.80000000000001 * exp(2.67 * logT - 26325728.0 * invRT);
-    K.er[1] = exp(gRT[1] + gRT[5] - gRT[0] - gRT[3]);
-    K.kf[2] = 43800000000.00001 * exp(-(29246160.0 * invRT));
-    K.er[2] = exp(gRT[1] + gRT[4] - gRT[0] - gRT[5]);
-    K.kf[3] = 6165000000.000002 * exp(-0.5 * logT);
-    K.er[3] = exp((gRT[2] - 2.0 * gRT[3]) - -1.0 * log_cref);
-    K.kf[4] = 114000000000.00003 * exp(-(63956624.0 * invRT));
-    K.er[4] = exp(gRT[3] + gRT[5] - gRT[2] - gRT[1]);
-    K.kf[5] = 3.5000000000000016e+16 * exp(-2.0 * logT);
-    K.er[5] = exp((gRT[4] - gRT[1] - gRT[5]) - -1.0 * log_cref);
-    K.kf[6] = 67000.00000000001 * exp(1.704 * logT - 62704771.199999996 * invRT);
-    K.er[6] = exp(2.0 * gRT[5] - gRT[3] - gRT[4]);
-    K.kf[7] = 4714000000000.002 * exp(-1.0 * logT);
-    K.er[7] = exp((gRT[5] - gRT[3] - gRT[1]) - -1.0 * log_cref);
-    K.kf[8] = 2000000000000.0 * exp(0.9 * logT - 203965816.0 * invRT);
-    K.k0[0] = 2.4900000000000005e+21 * exp(-2.3 * logT - 203965816.0 * invRT);
-    K.lFc[0] = -0.36653154442041347;
-    K.er[8] = exp((2.0 * gRT[5] - gRT[6]) - 1.0 * log_cref);
-    K.kf[9] = 24100000000.000008 * exp(-(16610480.0 * invRT));
-    K.er[9] = exp(gRT[4] + gRT[5] - gRT[6] - gRT[1]);
-    K.kf[10] = 21500000.000000004 * exp(1.0 * logT - 25104000.0 * invRT);
-    K.er[10] = exp(gRT[0] + gRT[7] - gRT[6] - gRT[1]);
-    K.kf[11] = 9550.000000000002 * exp(2.0 * logT - 16610480.0 * invRT);
-    K.er[11] = exp(gRT[5] + gRT[7] - gRT[6] - gRT[3]);
-    K.kf[12] = 1740000000.0000005 * exp(-(1330512.0 * invRT));
-    K.er[12] = exp(gRT[4] + gRT[7] - gRT[6] - gRT[5]);
-    K.kf[13] = 75900000000.00002 * exp(-(30413496.0 * invRT));
-    K.er[13] = exp(gRT[4] + gRT[7] - gRT[6] - gRT[5]);
-    K.kf[14] = 70790000000.00002 * exp(-(1234280.0 * invRT));
-    K.er[14] = exp(2.0 * gRT[5] - gRT[7] - gRT[1]);
-    K.kf[15] = 11402000.000000002 * exp(1.0827 * logT - 2317015.52 * invRT);
-    K.er[15] = exp(gRT[0] + gRT[2] - gRT[7] - gRT[1]);
-    K.kf[16] = 32500000000.000008;
-    K.er[16] = exp(gRT[5] + gRT[2] - gRT[7] - gRT[3]);
-    K.kf[17] = 7000000000.000002 * exp(-(-4572944.640000001 * invRT));
-    K.er[17] = exp(gRT[4] + gRT[2] - gRT[5] - gRT[7]);
-    K.kf[18] = 450000000000.0001 * exp(-(45729446.4 * invRT));
-    K.er[18] = exp(gRT[4] + gRT[2] - gRT[5] - gRT[7]);
-    K.kf[19] = 100000000000.00003 * exp(-(46195054.472 * invRT));
-    K.er[19] = exp(gRT[6] + gRT[2] - 2.0 * gRT[7]);
-    K.kf[20] = 190000000.00000006 * exp(-(-5894941.3632 * invRT));
-    K.er[20] = exp(gRT[6] + gRT[2] - 2.0 * gRT[7]);
-    K.kf[21] = 4650000000.000001 * exp(0.44 * logT);
-    K.k0[1] = 17370000000000.006 * exp(-1.23 * logT);
-    K.lFc[1] = -0.17392519729917352;
-    K.er[21] = exp((gRT[7] - gRT[1] - gRT[2]) - -1.0 * log_cref);
-    K.kf[22] = 10000000000.000004;
-    K.er[22] = exp((gRT[7] - gRT[3] - gRT[5]) - -1.0 * log_cref);
 }
 
-// F = d(Y_0..Y_{NS-1}, T)/dt at density rho [kg/m^3] and state y, from the factors K at
-// y's temperature (gas::reactor_rhs_k).
-GAS_HD void rhs_k(const Factors &K, double rho, const double *y, double *F) {
+// F = d(Y_0..Y_{NS-1}, T)/dt at density rho [kg/m^3] and state y, from the thermo th at
+// y's temperature (gas::rate_factors + gas::reactor_rhs_k, reaction by reaction).
+GAS_HD void rhs_t(const Thermo &th, double rho, const double *y, double *F) {
     const double T = y[9];
+    const double logT = th.logT, invRT = th.invRT, log_cref = th.log_cref;
+    (void)logT;
+    (void)log_cref;
     const double C0 = rho * y[0] * 0.49603174603174605;
     const double C1 = rho * y[1] * 0.9920634920634921;
     const double C2 = rho * y[2] * 0.03125195324707794;
@@ -425,278 +379,417 @@ GAS_HD void rhs_k(const Factors &K, double rho, const double *y, double *F) {
     double w6 = 0.0;
     double w7 = 0.0;
     double w8 = 0.0;
-    {  // 0: 1 H2 <=> 2 H  + M
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[0] * M;
-        const double fwd = kfM * C0;
-        const double rev = kfM * K.er[0] * (C1 * C1);
-        const double q = fwd - rev;
-        w0 -= q;
-        w1 += 2.0 * q;
-    }
-    {  // 1: 1 H2 + 1 O <=> 1 H + 1 OH
-        const double kfM = K.kf[1];
-        const double fwd = kfM * C0 * C3;
-        const double rev = kfM * K.er[1] * C1 * C5;
-        const double q = fwd - rev;
-        w0 -= q;
-        w3 -= q;
-        w1 += q;
-        w5 += q;
-    }
-    {  // 2: 1 H2 + 1 OH <=> 1 H + 1 H2O
-        const double kfM = K.kf[2];
-        const double fwd = kfM * C0 * C5;
-        const double rev = kfM * K.er[2] * C1 * C4;
-        const double q = fwd - rev;
-        w0 -= q;
-        w5 -= q;
-        w1 += q;
-        w4 += q;
-    }
-    {  // 3: 2 O <=> 1 O2  + M
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[3] * M;
-        const double fwd = kfM * (C3 * C3);
-        const double rev = kfM * K.er[3] * C2;
-        const double q = fwd - rev;
-        w3 -= 2.0 * q;
-        w2 += q;
-    }
-    {  // 4: 1 O2 + 1 H <=> 1 O + 1 OH
-        const double kfM = K.kf[4];
-        const double fwd = kfM * C2 * C1;
-        const double rev = kfM * K.er[4] * C3 * C5;
-        const double q = fwd - rev;
-        w2 -= q;
-        w1 -= q;
-        w3 += q;
-        w5 += q;
-    }
-    {  // 5: 1 H + 1 OH <=> 1 H2O  + M
-        const double M = 0.73 * C0 + C1 + C2 + C3 + 3.65 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[5] * M;
-        const double fwd = kfM * C1 * C5;
-        const double rev = kfM * K.er[5] * C4;
-        const double q = fwd - rev;
-        w1 -= q;
-        w5 -= q;
-        w4 += q;
-    }
-    {  // 6: 1 O + 1 H2O <=> 2 OH
-        const double kfM = K.kf[6];
-        const double fwd = kfM * C3 * C4;
-        const double rev = kfM * K.er[6] * (C5 * C5);
-        const double q = fwd - rev;
-        w3 -= q;
-        w4 -= q;
-        w5 += 2.0 * q;
-    }
-    {  // 7: 1 O + 1 H <=> 1 OH  + M
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[7] * M;
-        const double fwd = kfM * C3 * C1;
-        const double rev = kfM * K.er[7] * C5;
-        const double q = fwd - rev;
-        w3 -= q;
-        w1 -= q;
-        w5 += q;
-    }
-    {  // 8: 1 H2O2 <=> 2 OH  (+M)
-        const double M = 3.7 * C0 + C1 + 1.2 * C2 + C3 + 7.65 * C4 + C5 + 7.7 * C6 + C7 + 1.5 * C8;
-        const double Pr = K.k0[0] * M / K.kf[8];
-        const double lFc = K.lFc[0];
-        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-        const double lPr = log10(fmax(Pr, 1e-300));
-        const double x = (lPr + c) / (n - 0.14 * (lPr + c));
-        const double kfM = K.kf[8] * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
-        const double fwd = kfM * C6;
-        const double rev = kfM * K.er[8] * (C5 * C5);
-        const double q = fwd - rev;
-        w6 -= q;
-        w5 += 2.0 * q;
-    }
-    {  // 9: 1 H2O2 + 1 H <=> 1 H2O + 1 OH
-        const double kfM = K.kf[9];
-        const double fwd = kfM * C6 * C1;
-        const double rev = kfM * K.er[9] * C4 * C5;
-        const double q = fwd - rev;
-        w6 -= q;
-        w1 -= q;
-        w4 += q;
-        w5 += q;
-    }
-    {  // 10: 1 H2O2 + 1 H <=> 1 H2 + 1 HO2
-        const double kfM = K.kf[10];
-        const double fwd = kfM * C6 * C1;
-        const double rev = kfM * K.er[10] * C0 * C7;
-        const double q = fwd - rev;
-        w6 -= q;
-        w1 -= q;
-        w0 += q;
-        w7 += q;
-    }
-    {  // 11: 1 H2O2 + 1 O <=> 1 OH + 1 HO2
-        const double kfM = K.kf[11];
-        const double fwd = kfM * C6 * C3;
-        const double rev = kfM * K.er[11] * C5 * C7;
-        const double q = fwd - rev;
-        w6 -= q;
-        w3 -= q;
-        w5 += q;
-        w7 += q;
-    }
-    {  // 12: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
-        const double kfM = K.kf[12];
-        const double fwd = kfM * C6 * C5;
-        const double rev = kfM * K.er[12] * C4 * C7;
-        const double q = fwd - rev;
-        w6 -= q;
-        w5 -= q;
-        w4 += q;
-        w7 += q;
-    }
-    {  // 13: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
-        const double kfM = K.kf[13];
-        const double fwd = kfM * C6 * C5;
-        const double rev = kfM * K.er[13] * C4 * C7;
-        const double q = fwd - rev;
-        w6 -= q;
-        w5 -= q;
-        w4 += q;
-        w7 += q;
-    }
-    {  // 14: 1 HO2 + 1 H <=> 2 OH
-        const double kfM = K.kf[14];
-        const double fwd = kfM * C7 * C1;
-        const double rev = kfM * K.er[14] * (C5 * C5);
-        const double q = fwd - rev;
-        w7 -= q;
-        w1 -= q;
-        w5 += 2.0 * q;
-    }
-    {  // 15: 1 HO2 + 1 H <=> 1 H2 + 1 O2
-        const double kfM = K.kf[15];
-        const double fwd = kfM * C7 * C1;
-        const double rev = kfM * K.er[15] * C0 * C2;
-        const double q = fwd - rev;
-        w7 -= q;
-        w1 -= q;
-        w0 += q;
-        w2 += q;
-    }
-    {  // 16: 1 HO2 + 1 O <=> 1 OH + 1 O2
-        const double kfM = K.kf[16];
-        const double fwd = kfM * C7 * C3;
-        const double rev = kfM * K.er[16] * C5 * C2;
-        const double q = fwd - rev;
-        w7 -= q;
-        w3 -= q;
-        w5 += q;
-        w2 += q;
-    }
-    {  // 17: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
-        const double kfM = K.kf[17];
-        const double fwd = kfM * C5 * C7;
-        const double rev = kfM * K.er[17] * C4 * C2;
-        const double q = fwd - rev;
-        w5 -= q;
-        w7 -= q;
-        w4 += q;
-        w2 += q;
-    }
-    {  // 18: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
-        const double kfM = K.kf[18];
-        const double fwd = kfM * C5 * C7;
-        const double rev = kfM * K.er[18] * C4 * C2;
-        const double q = fwd - rev;
-        w5 -= q;
-        w7 -= q;
-        w4 += q;
-        w2 += q;
-    }
-    {  // 19: 2 HO2 <=> 1 H2O2 + 1 O2
-        const double kfM = K.kf[19];
-        const double fwd = kfM * (C7 * C7);
-        const double rev = kfM * K.er[19] * C6 * C2;
-        const double q = fwd - rev;
-        w7 -= 2.0 * q;
-        w6 += q;
-        w2 += q;
-    }
-    {  // 20: 2 HO2 <=> 1 H2O2 + 1 O2
-        const double kfM = K.kf[20];
-        const double fwd = kfM * (C7 * C7);
-        const double rev = kfM * K.er[20] * C6 * C2;
-        const double q = fwd - rev;
-        w7 -= 2.0 * q;
-        w6 += q;
-        w2 += q;
-    }
-    {  // 21: 1 H + 1 O2 <=> 1 HO2  (+M)
-        const double M = 1.3 * C0 + C1 + C2 + C3 + 10.0 * C4 + C5 + C6 + C7 + C8;
-        const double Pr = K.k0[1] * M / K.kf[21];
-        const double lFc = K.lFc[1];
-        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-        const double lPr = log10(fmax(Pr, 1e-300));
-        const double x = (lPr + c) / (n - 0.14 * (lPr + c));
-        const double kfM = K.kf[21] * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
-        const double fwd = kfM * C1 * C2;
-        const double rev = kfM * K.er[21] * C7;
-        const double q = fwd - rev;
-        w1 -= q;
-        w2 -= q;
-        w7 += q;
-    }
-    {  // 22: 1 O + 1 OH <=> 1 HO2  + M
-        const double M = C0 + C1 + C2 + C3 + C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[22] * M;
-        const double fwd = kfM * C3 * C5;
-        const double rev = kfM * K.er[22] * C7;
-        const double q = fwd - rev;
-        w3 -= q;
-        w5 -= q;
-        w7 += q;
-    }
-    double cv = 0.0, s = 0.0;
-    F[0] = w0 * 2.016 / rho;
-    cv += y[0] * (K.cpR[0] - 1.0) * 0.49603174603174605;
-    s += (K.hRT[0] - 1.0) * 8314.46261815324 * T * w0;
-    F[1] = w1 * 1.008 / rho;
-    cv += y[1] * (K.cpR[1] - 1.0) * 0.9920634920634921;
-    s += (K.hRT[1] - 1.0) * 8314.46261815324 * T * w1;
-    F[2] = w2 * 31.998 / rho;
-    cv += y[2] * (K.cpR[2] - 1.0) * 0.03125195324707794;
-    s += (K.hRT[2] - 1.0) * 8314.46261815324 * T * w2;
-    F[3] = w3 * 15.999 / rho;
-    cv += y[3] * (K.cpR[3] - 1.0) * 0.06250390649415588;
-    s += (K.hRT[3] - 1.0) * 8314.46261815324 * T * w3;
-    F[4] = w4 * 18.015 / rho;
-    cv += y[4] * (K.cpR[4] - 1.0) * 0.055509297807382736;
-    s += (K.hRT[4] - 1.0) * 8314.46261815324 * T * w4;
-    F[5] = w5 * 17.007 / rho;
-    cv += y[5] * (K.cpR[5] - 1.0) * 0.05879931792791203;
-    s += (K.hRT[5] - 1.0) * 8314.46261815324 * T * w5;
-    F[6] = w6 * 34.014 / rho;
-    cv += y[6] * (K.cpR[6] - 1.0) * 0.029399658963956014;
-    s += (K.hRT[6] - 1.0) * 8314.46261815324 * T * w6;
-    F[7] = w7 * 33.006 / rho;
-    cv += y[7] * (K.cpR[7] - 1.0) * 0.030297521662727988;
-    s += (K.hRT[7] - 1.0) * 8314.46261815324 * T * w7;
-    F[8] = w8 * 28.014 / rho;
-    cv += y[8] * (K.cpR[8] - 1.0) * 0.03569643749553795;
-    s += (K.hRT[8] - 1.0) * 8314.46261815324 * T * w8;
+    double cv = 0.0;
+    cv += y[0] * (th.cpR[0] - 1.0) * 0.49603174603174605;
+    cv += y[1] * (th.cpR[1] - 1.0) * 0.9920634920634921;
+    cv += y[2] * (th.cpR[2] - 1.0) * 0.03125195324707794;
+    cv += y[3] * (th.cpR[3] - 1.0) * 0.06250390649415588;
+    cv += y[4] * (th.cpR[4] - 1.0) * 0.055509297807382736;
+    cv += y[5] * (th.cpR[5] - 1.0) * 0.05879931792791203;
+    cv += y[6] * (th.cpR[6] - 1.0) * 0.029399658963956014;
+    cv += y[7] * (th.cpR[7] - 1.0) * 0.030297521662727988;
+    cv += y[8] * (th.cpR[8] - 1.0) * 0.03569643749553795;
     cv *= 8314.46261815324;
-    F[9] = -s / (rho * cv);
+    GAS_SCHED_FENCE();
+    {  // reaction 0
+        const double kf = 4.577000000000001e+16 * exp(-1.4 * logT - 436809600.0 * invRT);
+        const double er = exp((2.0 * th.gRT[1] - th.gRT[0]) - 1.0 * log_cref);
+        {  // rate of progress: 1 H2 <=> 2 H  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C0;
+            const double rev = kfM * er * (C1 * C1);
+            const double q = fwd - rev;
+            w0 -= q;
+            w1 += 2.0 * q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 1
+        const double kf = 50.80000000000001 * exp(2.67 * logT - 26325728.0 * invRT);
+        const double er = exp(th.gRT[1] + th.gRT[5] - th.gRT[0] - th.gRT[3]);
+        {  // rate of progress: 1 H2 + 1 O <=> 1 H + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C0 * C3;
+            const double rev = kfM * er * C1 * C5;
+            const double q = fwd - rev;
+            w0 -= q;
+            w3 -= q;
+            w1 += q;
+            w5 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 2
+        const double kf = 43800000000.00001 * exp(-(29246160.0 * invRT));
+        const double er = exp(th.gRT[1] + th.gRT[4] - th.gRT[0] - th.gRT[5]);
+        {  // rate of progress: 1 H2 + 1 OH <=> 1 H + 1 H2O
+            const double kfM = kf;
+            const double fwd = kfM * C0 * C5;
+            const double rev = kfM * er * C1 * C4;
+            const double q = fwd - rev;
+            w0 -= q;
+            w5 -= q;
+            w1 += q;
+            w4 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 3
+        const double kf = 6165000000.000002 * exp(-0.5 * logT);
+        const double er = exp((th.gRT[2] - 2.0 * th.gRT[3]) - -1.0 * log_cref);
+        {  // rate of progress: 2 O <=> 1 O2  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * (C3 * C3);
+            const double rev = kfM * er * C2;
+            const double q = fwd - rev;
+            w3 -= 2.0 * q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 4
+        const double kf = 114000000000.00003 * exp(-(63956624.0 * invRT));
+        const double er = exp(th.gRT[3] + th.gRT[5] - th.gRT[2] - th.gRT[1]);
+        {  // rate of progress: 1 O2 + 1 H <=> 1 O + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C2 * C1;
+            const double rev = kfM * er * C3 * C5;
+            const double q = fwd - rev;
+            w2 -= q;
+            w1 -= q;
+            w3 += q;
+            w5 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 5
+        const double kf = 3.5000000000000016e+16 * exp(-2.0 * logT);
+        const double er = exp((th.gRT[4] - th.gRT[1] - th.gRT[5]) - -1.0 * log_cref);
+        {  // rate of progress: 1 H + 1 OH <=> 1 H2O  + M
+            const double M = 0.73 * C0 + C1 + C2 + C3 + 3.65 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C1 * C5;
+            const double rev = kfM * er * C4;
+            const double q = fwd - rev;
+            w1 -= q;
+            w5 -= q;
+            w4 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 6
+        const double kf = 67000.00000000001 * exp(1.704 * logT - 62704771.199999996 * invRT);
+        const double er = exp(2.0 * th.gRT[5] - th.gRT[3] - th.gRT[4]);
+        {  // rate of progress: 1 O + 1 H2O <=> 2 OH
+            const double kfM = kf;
+            const double fwd = kfM * C3 * C4;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w3 -= q;
+            w4 -= q;
+            w5 += 2.0 * q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 7
+        const double kf = 4714000000000.002 * exp(-1.0 * logT);
+        const double er = exp((th.gRT[5] - th.gRT[3] - th.gRT[1]) - -1.0 * log_cref);
+        {  // rate of progress: 1 O + 1 H <=> 1 OH  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C3 * C1;
+            const double rev = kfM * er * C5;
+            const double q = fwd - rev;
+            w3 -= q;
+            w1 -= q;
+            w5 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 8
+        const double kf = 2000000000000.0 * exp(0.9 * logT - 203965816.0 * invRT);
+        const double k0 = 2.4900000000000005e+21 * exp(-2.3 * logT - 203965816.0 * invRT);
+        const double lFc0 = -0.36653154442041347;
+        const double er = exp((2.0 * th.gRT[5] - th.gRT[6]) - 1.0 * log_cref);
+        {  // rate of progress: 1 H2O2 <=> 2 OH  (+M)
+            const double M = 3.7 * C0 + C1 + 1.2 * C2 + C3 + 7.65 * C4 + C5 + 7.7 * C6 + C7 + 1.5 * C8;
+            const double Pr = k0 * M / kf;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+            const double kfM = kf * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
+            const double fwd = kfM * C6;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 += 2.0 * q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 9
+        const double kf = 24100000000.000008 * exp(-(16610480.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[5] - th.gRT[6] - th.gRT[1]);
+        {  // rate of progress: 1 H2O2 + 1 H <=> 1 H2O + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C1;
+            const double rev = kfM * er * C4 * C5;
+            const double q = fwd - rev;
+            w6 -= q;
+            w1 -= q;
+            w4 += q;
+            w5 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 10
+        const double kf = 21500000.000000004 * exp(1.0 * logT - 25104000.0 * invRT);
+        const double er = exp(th.gRT[0] + th.gRT[7] - th.gRT[6] - th.gRT[1]);
+        {  // rate of progress: 1 H2O2 + 1 H <=> 1 H2 + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C1;
+            const double rev = kfM * er * C0 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w1 -= q;
+            w0 += q;
+            w7 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 11
+        const double kf = 9550.000000000002 * exp(2.0 * logT - 16610480.0 * invRT);
+        const double er = exp(th.gRT[5] + th.gRT[7] - th.gRT[6] - th.gRT[3]);
+        {  // rate of progress: 1 H2O2 + 1 O <=> 1 OH + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C3;
+            const double rev = kfM * er * C5 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w3 -= q;
+            w5 += q;
+            w7 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 12
+        const double kf = 1740000000.0000005 * exp(-(1330512.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[7] - th.gRT[6] - th.gRT[5]);
+        {  // rate of progress: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C5;
+            const double rev = kfM * er * C4 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 -= q;
+            w4 += q;
+            w7 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 13
+        const double kf = 75900000000.00002 * exp(-(30413496.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[7] - th.gRT[6] - th.gRT[5]);
+        {  // rate of progress: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C5;
+            const double rev = kfM * er * C4 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 -= q;
+            w4 += q;
+            w7 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 14
+        const double kf = 70790000000.00002 * exp(-(1234280.0 * invRT));
+        const double er = exp(2.0 * th.gRT[5] - th.gRT[7] - th.gRT[1]);
+        {  // rate of progress: 1 HO2 + 1 H <=> 2 OH
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C1;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w7 -= q;
+            w1 -= q;
+            w5 += 2.0 * q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 15
+        const double kf = 11402000.000000002 * exp(1.0827 * logT - 2317015.52 * invRT);
+        const double er = exp(th.gRT[0] + th.gRT[2] - th.gRT[7] - th.gRT[1]);
+        {  // rate of progress: 1 HO2 + 1 H <=> 1 H2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C1;
+            const double rev = kfM * er * C0 * C2;
+            const double q = fwd - rev;
+            w7 -= q;
+            w1 -= q;
+            w0 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 16
+        const double kf = 32500000000.000008;
+        const double er = exp(th.gRT[5] + th.gRT[2] - th.gRT[7] - th.gRT[3]);
+        {  // rate of progress: 1 HO2 + 1 O <=> 1 OH + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C3;
+            const double rev = kfM * er * C5 * C2;
+            const double q = fwd - rev;
+            w7 -= q;
+            w3 -= q;
+            w5 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 17
+        const double kf = 7000000000.000002 * exp(-(-4572944.640000001 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[2] - th.gRT[5] - th.gRT[7]);
+        {  // rate of progress: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C5 * C7;
+            const double rev = kfM * er * C4 * C2;
+            const double q = fwd - rev;
+            w5 -= q;
+            w7 -= q;
+            w4 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 18
+        const double kf = 450000000000.0001 * exp(-(45729446.4 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[2] - th.gRT[5] - th.gRT[7]);
+        {  // rate of progress: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C5 * C7;
+            const double rev = kfM * er * C4 * C2;
+            const double q = fwd - rev;
+            w5 -= q;
+            w7 -= q;
+            w4 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 19
+        const double kf = 100000000000.00003 * exp(-(46195054.472 * invRT));
+        const double er = exp(th.gRT[6] + th.gRT[2] - 2.0 * th.gRT[7]);
+        {  // rate of progress: 2 HO2 <=> 1 H2O2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * (C7 * C7);
+            const double rev = kfM * er * C6 * C2;
+            const double q = fwd - rev;
+            w7 -= 2.0 * q;
+            w6 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 20
+        const double kf = 190000000.00000006 * exp(-(-5894941.3632 * invRT));
+        const double er = exp(th.gRT[6] + th.gRT[2] - 2.0 * th.gRT[7]);
+        {  // rate of progress: 2 HO2 <=> 1 H2O2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * (C7 * C7);
+            const double rev = kfM * er * C6 * C2;
+            const double q = fwd - rev;
+            w7 -= 2.0 * q;
+            w6 += q;
+            w2 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 21
+        const double kf = 4650000000.000001 * exp(0.44 * logT);
+        const double k0 = 17370000000000.006 * exp(-1.23 * logT);
+        const double lFc0 = -0.17392519729917352;
+        const double er = exp((th.gRT[7] - th.gRT[1] - th.gRT[2]) - -1.0 * log_cref);
+        {  // rate of progress: 1 H + 1 O2 <=> 1 HO2  (+M)
+            const double M = 1.3 * C0 + C1 + C2 + C3 + 10.0 * C4 + C5 + C6 + C7 + C8;
+            const double Pr = k0 * M / kf;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+            const double kfM = kf * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
+            const double fwd = kfM * C1 * C2;
+            const double rev = kfM * er * C7;
+            const double q = fwd - rev;
+            w1 -= q;
+            w2 -= q;
+            w7 += q;
+        }
+    }
+    GAS_SCHED_FENCE();
+    {  // reaction 22
+        const double kf = 10000000000.000004;
+        const double er = exp((th.gRT[7] - th.gRT[3] - th.gRT[5]) - -1.0 * log_cref);
+        {  // rate of progress: 1 O + 1 OH <=> 1 HO2  + M
+            const double M = C0 + C1 + C2 + C3 + C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C3 * C5;
+            const double rev = kfM * er * C7;
+            const double q = fwd - rev;
+            w3 -= q;
+            w5 -= q;
+            w7 += q;
+        }
+    }
+    double es = 0.0;
+    F[0] = w0 * 2.016 / rho;
+    es += (th.hRT[0] - 1.0) * 8314.46261815324 * T * w0;
+    F[1] = w1 * 1.008 / rho;
+    es += (th.hRT[1] - 1.0) * 8314.46261815324 * T * w1;
+    F[2] = w2 * 31.998 / rho;
+    es += (th.hRT[2] - 1.0) * 8314.46261815324 * T * w2;
+    F[3] = w3 * 15.999 / rho;
+    es += (th.hRT[3] - 1.0) * 8314.46261815324 * T * w3;
+    F[4] = w4 * 18.015 / rho;
+    es += (th.hRT[4] - 1.0) * 8314.46261815324 * T * w4;
+    F[5] = w5 * 17.007 / rho;
+    es += (th.hRT[5] - 1.0) * 8314.46261815324 * T * w5;
+    F[6] = w6 * 34.014 / rho;
+    es += (th.hRT[6] - 1.0) * 8314.46261815324 * T * w6;
+    F[7] = w7 * 33.006 / rho;
+    es += (th.hRT[7] - 1.0) * 8314.46261815324 * T * w7;
+    F[8] = w8 * 28.014 / rho;
+    es += (th.hRT[8] - 1.0) * 8314.46261815324 * T * w8;
+    F[9] = -es / (rho * cv);
 }
 
-// s times the Jacobian of F (rhs_k) with respect to (Y, T): J(k, j) = s dF_k / dY_j for
-// j < NS and J(k, NS) = s dF_k / dT, every row k <= NS, at fixed density, from the factors
-// at y's temperature and F = rhs_k(K, rho, y).
+// rhs_t, and s times the Jacobian of F with respect to (Y, T) at fixed density: J(k, j) =
+// s dF_k / dY_j for j < NS and J(k, NS) = s dF_k / dT, every row k <= NS.  Each reaction's
+// rate constants are formed once and serve both.
+// The Jacobian of d(Y, T)/dt at fixed density, d F_k / d Y_j and d F_k / dT, differentiating the
+// right-hand side's expressions.  With q_r the rates of progress, nu_kr the net coefficients and
+// C_j = rho Y_j / W_j:
+//     dF_k/dY_j = (W_k / W_j) sum_r nu_kr dq_r/dC_j,
+//     dF_k/dT   = (W_k / rho) sum_r nu_kr dq_r/dT,
+//     dF_T/dY_j = -(R T / (W_j c_v)) sum_r e_r dq_r/dC_j - F_T R (c_p,j/R - 1) / (W_j c_v),
+//     dF_T/dT   = -R [sum_k (c_p,k/R - 1) w_k + T sum_r e_r dq_r/dT] / (rho c_v) - F_T (dc_v/dT) / c_v,
+// e_r = sum_k nu_kr (h_k/RT - 1), w_k the net production rates.  dq_r/dC_j through the
+// mass-action products, the third-body sum M and the Troe blend F(Pr), Pr = k0 M / k_inf:
+// d(k_inf Pr/(1+Pr) F)/dM = k0 F/(1+Pr) [1/(1+Pr) - 2 x lFc n / ((1+x^2)^2 (n - 0.14 u)^2)],
+// u = log10 Pr + c, x = u / (n - 0.14 u).  dq_r/dT through d ln k/dT = (b + E_a/RT)/T for
+// k_f and k_0, d ln(1/K_c)/dT = (dnu - sum_k nu_kr h_k/RT)/T (d(g_k/RT)/dT = -h_k/(R T^2),
+// d ln(p_atm/RT)/dT = -1/T), and for a fall-off reaction d ln(Pr/(1+Pr))/dT =
+// (d ln k0 - d ln k_inf)/(1+Pr) and d ln F/dT = ln 10 [dlFc/(1+x^2) - 2 x lFc dx/(1+x^2)^2]
+// with du = (d ln k0 - d ln k_inf)/ln 10 - 0.67 dlFc (dlFc = 0 where F_cent is constant).
+// Every term is accumulated straight into the scaled matrix (s J, s = -gamma h for the
+// integrator's iteration matrix).
 template <class Mat>
-GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, double s, Mat &J) {
+GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, double s, Mat &J) {
     const double T = y[9];
-    const double invT = 1.0 / T, invRT = 1.0 / (8314.46261815324 * T);
+    const double logT = th.logT, invRT = th.invRT, log_cref = th.log_cref;
+    (void)logT;
+    (void)log_cref;
     const double C0 = rho * y[0] * 0.49603174603174605;
     const double C1 = rho * y[1] * 0.9920634920634921;
     const double C2 = rho * y[2] * 0.03125195324707794;
@@ -706,17 +799,27 @@ GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, 
     const double C6 = rho * y[6] * 0.029399658963956014;
     const double C7 = rho * y[7] * 0.030297521662727988;
     const double C8 = rho * y[8] * 0.03569643749553795;
+    double w0 = 0.0;
+    double w1 = 0.0;
+    double w2 = 0.0;
+    double w3 = 0.0;
+    double w4 = 0.0;
+    double w5 = 0.0;
+    double w6 = 0.0;
+    double w7 = 0.0;
+    double w8 = 0.0;
     double cv = 0.0;
-    cv += y[0] * (K.cpR[0] - 1.0) * 0.49603174603174605;
-    cv += y[1] * (K.cpR[1] - 1.0) * 0.9920634920634921;
-    cv += y[2] * (K.cpR[2] - 1.0) * 0.03125195324707794;
-    cv += y[3] * (K.cpR[3] - 1.0) * 0.06250390649415588;
-    cv += y[4] * (K.cpR[4] - 1.0) * 0.055509297807382736;
-    cv += y[5] * (K.cpR[5] - 1.0) * 0.05879931792791203;
-    cv += y[6] * (K.cpR[6] - 1.0) * 0.029399658963956014;
-    cv += y[7] * (K.cpR[7] - 1.0) * 0.030297521662727988;
-    cv += y[8] * (K.cpR[8] - 1.0) * 0.03569643749553795;
+    cv += y[0] * (th.cpR[0] - 1.0) * 0.49603174603174605;
+    cv += y[1] * (th.cpR[1] - 1.0) * 0.9920634920634921;
+    cv += y[2] * (th.cpR[2] - 1.0) * 0.03125195324707794;
+    cv += y[3] * (th.cpR[3] - 1.0) * 0.06250390649415588;
+    cv += y[4] * (th.cpR[4] - 1.0) * 0.055509297807382736;
+    cv += y[5] * (th.cpR[5] - 1.0) * 0.05879931792791203;
+    cv += y[6] * (th.cpR[6] - 1.0) * 0.029399658963956014;
+    cv += y[7] * (th.cpR[7] - 1.0) * 0.030297521662727988;
+    cv += y[8] * (th.cpR[8] - 1.0) * 0.03569643749553795;
     cv *= 8314.46261815324;
+    const double invT = 1.0 / T;
     const double sT = -s * 8314.46261815324 * T / cv;  // times e_r dq_rj / W_j: the T row
     const double s_rho = s / rho;
     double sum_eT = 0.0;  // sum_r e_r dq_r/dT
@@ -724,1046 +827,1418 @@ GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, 
     for (int k = 0; k <= 9; ++k)
 #pragma unroll
         for (int j = 0; j <= 9; ++j) J(k, j) = 0.0;
+    GAS_SCHED_FENCE();
     {  // reaction 0
-        const double pf = C0;
-        const double pb = (C1 * C1);
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[0] * M;
-        const double dkdM = K.kf[0];
-        const double dlnk = (-1.4 + 436809600.0 * invRT) * invT;
-        const double g = dkdM * (pf - K.er[0] * pb);
-        const double dlner = (1.0 - (2.0 * K.hRT[1] - (1.0 * K.hRT[0]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[0] * pb) - K.er[0] * dlner * pb);
-        const double dq0 = kfM * (1.0) + 2.5 * g;
-        const double dq1 = -kfM * K.er[0] * (2.0 * C1) + g;
-        const double dq2 = g;
-        const double dq3 = g;
-        const double dq4 = 12.0 * g;
-        const double dq5 = g;
-        const double dq6 = g;
-        const double dq7 = g;
-        const double dq8 = g;
-        const double e_r = -1.0 * (K.hRT[0] - 1.0) + 2.0 * (K.hRT[1] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(0, 0) += -1.0 * s * dq0;
-        J(1, 0) += 1.0 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(0, 1) += -2.0 * s * dq1;
-        J(1, 1) += 2.0 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(0, 2) += -0.06300393774610913 * s * dq2;
-        J(1, 2) += 0.06300393774610913 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(0, 3) += -0.12600787549221826 * s * dq3;
-        J(1, 3) += 0.12600787549221826 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(0, 4) += -0.11190674437968359 * s * dq4;
-        J(1, 4) += 0.11190674437968359 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(0, 5) += -0.11853942494267065 * s * dq5;
-        J(1, 5) += 0.11853942494267065 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(0, 6) += -0.05926971247133533 * s * dq6;
-        J(1, 6) += 0.05926971247133533 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(0, 7) += -0.061079803672059625 * s * dq7;
-        J(1, 7) += 0.061079803672059625 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(0, 8) += -0.0719640179910045 * s * dq8;
-        J(1, 8) += 0.0719640179910045 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(0, 9) += -2.016 * s_rho * dqT;
-        J(1, 9) += 2.016 * s_rho * dqT;
+        const double kf = 4.577000000000001e+16 * exp(-1.4 * logT - 436809600.0 * invRT);
+        const double er = exp((2.0 * th.gRT[1] - th.gRT[0]) - 1.0 * log_cref);
+        {  // rate of progress: 1 H2 <=> 2 H  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C0;
+            const double rev = kfM * er * (C1 * C1);
+            const double q = fwd - rev;
+            w0 -= q;
+            w1 += 2.0 * q;
+        }
+        {  // Jacobian terms
+            const double pf = C0;
+            const double pb = (C1 * C1);
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double dkdM = kf;
+            const double dlnk = (-1.4 + 436809600.0 * invRT) * invT;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (1.0 - (2.0 * th.hRT[1] - (1.0 * th.hRT[0]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = kfM * (1.0) + 2.5 * g;
+            const double dq1 = -kfM * er * (2.0 * C1) + g;
+            const double dq2 = g;
+            const double dq3 = g;
+            const double dq4 = 12.0 * g;
+            const double dq5 = g;
+            const double dq6 = g;
+            const double dq7 = g;
+            const double dq8 = g;
+            const double e_r = -1.0 * (th.hRT[0] - 1.0) + 2.0 * (th.hRT[1] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(0, 0) += -1.0 * s * dq0;
+            J(1, 0) += 1.0 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(0, 1) += -2.0 * s * dq1;
+            J(1, 1) += 2.0 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(0, 2) += -0.06300393774610913 * s * dq2;
+            J(1, 2) += 0.06300393774610913 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(0, 3) += -0.12600787549221826 * s * dq3;
+            J(1, 3) += 0.12600787549221826 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(0, 4) += -0.11190674437968359 * s * dq4;
+            J(1, 4) += 0.11190674437968359 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(0, 5) += -0.11853942494267065 * s * dq5;
+            J(1, 5) += 0.11853942494267065 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(0, 6) += -0.05926971247133533 * s * dq6;
+            J(1, 6) += 0.05926971247133533 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(0, 7) += -0.061079803672059625 * s * dq7;
+            J(1, 7) += 0.061079803672059625 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(0, 8) += -0.0719640179910045 * s * dq8;
+            J(1, 8) += 0.0719640179910045 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(0, 9) += -2.016 * s_rho * dqT;
+            J(1, 9) += 2.016 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 1
-        const double pf = C0 * C3;
-        const double pb = C1 * C5;
-        const double kfM = K.kf[1];
-        const double dlnk = (2.67 + 26325728.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[1] + 1.0 * K.hRT[5] - (1.0 * K.hRT[0] + 1.0 * K.hRT[3]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[1] * pb) - K.er[1] * dlner * pb);
-        const double dq0 = kfM * (C3);
-        const double dq1 = -kfM * K.er[1] * (C5);
-        const double dq3 = kfM * (C0);
-        const double dq5 = -kfM * K.er[1] * (C1);
-        const double e_r = -1.0 * (K.hRT[0] - 1.0) + -1.0 * (K.hRT[3] - 1.0) + 1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(0, 0) += -1.0 * s * dq0;
-        J(3, 0) += -7.936011904761905 * s * dq0;
-        J(1, 0) += 0.5 * s * dq0;
-        J(5, 0) += 8.436011904761905 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(0, 1) += -2.0 * s * dq1;
-        J(3, 1) += -15.87202380952381 * s * dq1;
-        J(1, 1) += 1.0 * s * dq1;
-        J(5, 1) += 16.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(0, 3) += -0.12600787549221826 * s * dq3;
-        J(3, 3) += -1.0 * s * dq3;
-        J(1, 3) += 0.06300393774610913 * s * dq3;
-        J(5, 3) += 1.0630039377461091 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(0, 5) += -0.11853942494267065 * s * dq5;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(1, 5) += 0.05926971247133533 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(0, 9) += -2.016 * s_rho * dqT;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(1, 9) += 1.008 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
+        const double kf = 50.80000000000001 * exp(2.67 * logT - 26325728.0 * invRT);
+        const double er = exp(th.gRT[1] + th.gRT[5] - th.gRT[0] - th.gRT[3]);
+        {  // rate of progress: 1 H2 + 1 O <=> 1 H + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C0 * C3;
+            const double rev = kfM * er * C1 * C5;
+            const double q = fwd - rev;
+            w0 -= q;
+            w3 -= q;
+            w1 += q;
+            w5 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C0 * C3;
+            const double pb = C1 * C5;
+            const double kfM = kf;
+            const double dlnk = (2.67 + 26325728.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[1] + 1.0 * th.hRT[5] - (1.0 * th.hRT[0] + 1.0 * th.hRT[3]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = kfM * (C3);
+            const double dq1 = -kfM * er * (C5);
+            const double dq3 = kfM * (C0);
+            const double dq5 = -kfM * er * (C1);
+            const double e_r = -1.0 * (th.hRT[0] - 1.0) + -1.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(0, 0) += -1.0 * s * dq0;
+            J(3, 0) += -7.936011904761905 * s * dq0;
+            J(1, 0) += 0.5 * s * dq0;
+            J(5, 0) += 8.436011904761905 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(0, 1) += -2.0 * s * dq1;
+            J(3, 1) += -15.87202380952381 * s * dq1;
+            J(1, 1) += 1.0 * s * dq1;
+            J(5, 1) += 16.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(0, 3) += -0.12600787549221826 * s * dq3;
+            J(3, 3) += -1.0 * s * dq3;
+            J(1, 3) += 0.06300393774610913 * s * dq3;
+            J(5, 3) += 1.0630039377461091 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(0, 5) += -0.11853942494267065 * s * dq5;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(1, 5) += 0.05926971247133533 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(0, 9) += -2.016 * s_rho * dqT;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(1, 9) += 1.008 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 2
-        const double pf = C0 * C5;
-        const double pb = C1 * C4;
-        const double kfM = K.kf[2];
-        const double dlnk = (0.0 + 29246160.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[1] + 1.0 * K.hRT[4] - (1.0 * K.hRT[0] + 1.0 * K.hRT[5]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[2] * pb) - K.er[2] * dlner * pb);
-        const double dq0 = kfM * (C5);
-        const double dq1 = -kfM * K.er[2] * (C4);
-        const double dq4 = -kfM * K.er[2] * (C1);
-        const double dq5 = kfM * (C0);
-        const double e_r = -1.0 * (K.hRT[0] - 1.0) + -1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[4] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(0, 0) += -1.0 * s * dq0;
-        J(5, 0) += -8.436011904761905 * s * dq0;
-        J(1, 0) += 0.5 * s * dq0;
-        J(4, 0) += 8.936011904761905 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(0, 1) += -2.0 * s * dq1;
-        J(5, 1) += -16.87202380952381 * s * dq1;
-        J(1, 1) += 1.0 * s * dq1;
-        J(4, 1) += 17.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(0, 4) += -0.11190674437968359 * s * dq4;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(1, 4) += 0.055953372189841796 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(0, 5) += -0.11853942494267065 * s * dq5;
-        J(5, 5) += -1.0 * s * dq5;
-        J(1, 5) += 0.05926971247133533 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(0, 9) += -2.016 * s_rho * dqT;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(1, 9) += 1.008 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
+        const double kf = 43800000000.00001 * exp(-(29246160.0 * invRT));
+        const double er = exp(th.gRT[1] + th.gRT[4] - th.gRT[0] - th.gRT[5]);
+        {  // rate of progress: 1 H2 + 1 OH <=> 1 H + 1 H2O
+            const double kfM = kf;
+            const double fwd = kfM * C0 * C5;
+            const double rev = kfM * er * C1 * C4;
+            const double q = fwd - rev;
+            w0 -= q;
+            w5 -= q;
+            w1 += q;
+            w4 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C0 * C5;
+            const double pb = C1 * C4;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 29246160.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[1] + 1.0 * th.hRT[4] - (1.0 * th.hRT[0] + 1.0 * th.hRT[5]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = kfM * (C5);
+            const double dq1 = -kfM * er * (C4);
+            const double dq4 = -kfM * er * (C1);
+            const double dq5 = kfM * (C0);
+            const double e_r = -1.0 * (th.hRT[0] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[4] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(0, 0) += -1.0 * s * dq0;
+            J(5, 0) += -8.436011904761905 * s * dq0;
+            J(1, 0) += 0.5 * s * dq0;
+            J(4, 0) += 8.936011904761905 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(0, 1) += -2.0 * s * dq1;
+            J(5, 1) += -16.87202380952381 * s * dq1;
+            J(1, 1) += 1.0 * s * dq1;
+            J(4, 1) += 17.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(0, 4) += -0.11190674437968359 * s * dq4;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(1, 4) += 0.055953372189841796 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(0, 5) += -0.11853942494267065 * s * dq5;
+            J(5, 5) += -1.0 * s * dq5;
+            J(1, 5) += 0.05926971247133533 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(0, 9) += -2.016 * s_rho * dqT;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(1, 9) += 1.008 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 3
-        const double pf = (C3 * C3);
-        const double pb = C2;
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[3] * M;
-        const double dkdM = K.kf[3];
-        const double dlnk = (-0.5 + 0.0 * invRT) * invT;
-        const double g = dkdM * (pf - K.er[3] * pb);
-        const double dlner = (-1.0 - (1.0 * K.hRT[2] - (2.0 * K.hRT[3]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[3] * pb) - K.er[3] * dlner * pb);
-        const double dq0 = 2.5 * g;
-        const double dq1 = g;
-        const double dq2 = -kfM * K.er[3] * (1.0) + g;
-        const double dq3 = kfM * (2.0 * C3) + g;
-        const double dq4 = 12.0 * g;
-        const double dq5 = g;
-        const double dq6 = g;
-        const double dq7 = g;
-        const double dq8 = g;
-        const double e_r = -2.0 * (K.hRT[3] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(3, 0) += -15.87202380952381 * s * dq0;
-        J(2, 0) += 15.87202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(3, 1) += -31.74404761904762 * s * dq1;
-        J(2, 1) += 31.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(3, 2) += -1.0 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(3, 3) += -2.0 * s * dq3;
-        J(2, 3) += 2.0 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(3, 4) += -1.7761865112406328 * s * dq4;
-        J(2, 4) += 1.7761865112406328 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(3, 5) += -1.8814605750573292 * s * dq5;
-        J(2, 5) += 1.8814605750573292 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(3, 6) += -0.9407302875286646 * s * dq6;
-        J(2, 6) += 0.9407302875286646 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(3, 7) += -0.9694600981639702 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(3, 8) += -1.1422146069822232 * s * dq8;
-        J(2, 8) += 1.1422146069822232 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(3, 9) += -31.998 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 6165000000.000002 * exp(-0.5 * logT);
+        const double er = exp((th.gRT[2] - 2.0 * th.gRT[3]) - -1.0 * log_cref);
+        {  // rate of progress: 2 O <=> 1 O2  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * (C3 * C3);
+            const double rev = kfM * er * C2;
+            const double q = fwd - rev;
+            w3 -= 2.0 * q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = (C3 * C3);
+            const double pb = C2;
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double dkdM = kf;
+            const double dlnk = (-0.5 + 0.0 * invRT) * invT;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (-1.0 - (1.0 * th.hRT[2] - (2.0 * th.hRT[3]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = 2.5 * g;
+            const double dq1 = g;
+            const double dq2 = -kfM * er * (1.0) + g;
+            const double dq3 = kfM * (2.0 * C3) + g;
+            const double dq4 = 12.0 * g;
+            const double dq5 = g;
+            const double dq6 = g;
+            const double dq7 = g;
+            const double dq8 = g;
+            const double e_r = -2.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(3, 0) += -15.87202380952381 * s * dq0;
+            J(2, 0) += 15.87202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(3, 1) += -31.74404761904762 * s * dq1;
+            J(2, 1) += 31.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(3, 2) += -1.0 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(3, 3) += -2.0 * s * dq3;
+            J(2, 3) += 2.0 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(3, 4) += -1.7761865112406328 * s * dq4;
+            J(2, 4) += 1.7761865112406328 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(3, 5) += -1.8814605750573292 * s * dq5;
+            J(2, 5) += 1.8814605750573292 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(3, 6) += -0.9407302875286646 * s * dq6;
+            J(2, 6) += 0.9407302875286646 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(3, 7) += -0.9694600981639702 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -1.1422146069822232 * s * dq8;
+            J(2, 8) += 1.1422146069822232 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(3, 9) += -31.998 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 4
-        const double pf = C2 * C1;
-        const double pb = C3 * C5;
-        const double kfM = K.kf[4];
-        const double dlnk = (0.0 + 63956624.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[3] + 1.0 * K.hRT[5] - (1.0 * K.hRT[2] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[4] * pb) - K.er[4] * dlner * pb);
-        const double dq1 = kfM * (C2);
-        const double dq2 = kfM * (C1);
-        const double dq3 = -kfM * K.er[4] * (C5);
-        const double dq5 = -kfM * K.er[4] * (C3);
-        const double e_r = -1.0 * (K.hRT[2] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[3] - 1.0) + 1.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(2, 1) += -31.74404761904762 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(3, 1) += 15.87202380952381 * s * dq1;
-        J(5, 1) += 16.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(2, 2) += -1.0 * s * dq2;
-        J(1, 2) += -0.031501968873054564 * s * dq2;
-        J(3, 2) += 0.5 * s * dq2;
-        J(5, 2) += 0.5315019688730546 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(2, 3) += -2.0 * s * dq3;
-        J(1, 3) += -0.06300393774610913 * s * dq3;
-        J(3, 3) += 1.0 * s * dq3;
-        J(5, 3) += 1.0630039377461091 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(2, 5) += -1.8814605750573292 * s * dq5;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(3, 5) += 0.9407302875286646 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(2, 9) += -31.998 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(3, 9) += 15.999 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
+        const double kf = 114000000000.00003 * exp(-(63956624.0 * invRT));
+        const double er = exp(th.gRT[3] + th.gRT[5] - th.gRT[2] - th.gRT[1]);
+        {  // rate of progress: 1 O2 + 1 H <=> 1 O + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C2 * C1;
+            const double rev = kfM * er * C3 * C5;
+            const double q = fwd - rev;
+            w2 -= q;
+            w1 -= q;
+            w3 += q;
+            w5 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C2 * C1;
+            const double pb = C3 * C5;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 63956624.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[3] + 1.0 * th.hRT[5] - (1.0 * th.hRT[2] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq1 = kfM * (C2);
+            const double dq2 = kfM * (C1);
+            const double dq3 = -kfM * er * (C5);
+            const double dq5 = -kfM * er * (C3);
+            const double e_r = -1.0 * (th.hRT[2] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(2, 1) += -31.74404761904762 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(3, 1) += 15.87202380952381 * s * dq1;
+            J(5, 1) += 16.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(2, 2) += -1.0 * s * dq2;
+            J(1, 2) += -0.031501968873054564 * s * dq2;
+            J(3, 2) += 0.5 * s * dq2;
+            J(5, 2) += 0.5315019688730546 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(2, 3) += -2.0 * s * dq3;
+            J(1, 3) += -0.06300393774610913 * s * dq3;
+            J(3, 3) += 1.0 * s * dq3;
+            J(5, 3) += 1.0630039377461091 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(2, 5) += -1.8814605750573292 * s * dq5;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(3, 5) += 0.9407302875286646 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(2, 9) += -31.998 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(3, 9) += 15.999 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 5
-        const double pf = C1 * C5;
-        const double pb = C4;
-        const double M = 0.73 * C0 + C1 + C2 + C3 + 3.65 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[5] * M;
-        const double dkdM = K.kf[5];
-        const double dlnk = (-2.0 + 0.0 * invRT) * invT;
-        const double g = dkdM * (pf - K.er[5] * pb);
-        const double dlner = (-1.0 - (1.0 * K.hRT[4] - (1.0 * K.hRT[1] + 1.0 * K.hRT[5]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[5] * pb) - K.er[5] * dlner * pb);
-        const double dq0 = 0.73 * g;
-        const double dq1 = kfM * (C5) + g;
-        const double dq2 = g;
-        const double dq3 = g;
-        const double dq4 = -kfM * K.er[5] * (1.0) + 3.65 * g;
-        const double dq5 = kfM * (C1) + g;
-        const double dq6 = g;
-        const double dq7 = g;
-        const double dq8 = g;
-        const double e_r = -1.0 * (K.hRT[1] - 1.0) + -1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[4] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(1, 0) += -0.5 * s * dq0;
-        J(5, 0) += -8.436011904761905 * s * dq0;
-        J(4, 0) += 8.936011904761905 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(1, 1) += -1.0 * s * dq1;
-        J(5, 1) += -16.87202380952381 * s * dq1;
-        J(4, 1) += 17.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(1, 2) += -0.031501968873054564 * s * dq2;
-        J(5, 2) += -0.5315019688730546 * s * dq2;
-        J(4, 2) += 0.5630039377461091 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(1, 3) += -0.06300393774610913 * s * dq3;
-        J(5, 3) += -1.0630039377461091 * s * dq3;
-        J(4, 3) += 1.1260078754922183 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(1, 4) += -0.055953372189841796 * s * dq4;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(5, 5) += -1.0 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(1, 6) += -0.029634856235667664 * s * dq6;
-        J(5, 6) += -0.5 * s * dq6;
-        J(4, 6) += 0.5296348562356676 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(4, 7) += 0.5458098527540447 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(1, 8) += -0.03598200899550225 * s * dq8;
-        J(5, 8) += -0.6070893124866139 * s * dq8;
-        J(4, 8) += 0.6430713214821161 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
+        const double kf = 3.5000000000000016e+16 * exp(-2.0 * logT);
+        const double er = exp((th.gRT[4] - th.gRT[1] - th.gRT[5]) - -1.0 * log_cref);
+        {  // rate of progress: 1 H + 1 OH <=> 1 H2O  + M
+            const double M = 0.73 * C0 + C1 + C2 + C3 + 3.65 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C1 * C5;
+            const double rev = kfM * er * C4;
+            const double q = fwd - rev;
+            w1 -= q;
+            w5 -= q;
+            w4 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C1 * C5;
+            const double pb = C4;
+            const double M = 0.73 * C0 + C1 + C2 + C3 + 3.65 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double dkdM = kf;
+            const double dlnk = (-2.0 + 0.0 * invRT) * invT;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (-1.0 - (1.0 * th.hRT[4] - (1.0 * th.hRT[1] + 1.0 * th.hRT[5]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = 0.73 * g;
+            const double dq1 = kfM * (C5) + g;
+            const double dq2 = g;
+            const double dq3 = g;
+            const double dq4 = -kfM * er * (1.0) + 3.65 * g;
+            const double dq5 = kfM * (C1) + g;
+            const double dq6 = g;
+            const double dq7 = g;
+            const double dq8 = g;
+            const double e_r = -1.0 * (th.hRT[1] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[4] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(1, 0) += -0.5 * s * dq0;
+            J(5, 0) += -8.436011904761905 * s * dq0;
+            J(4, 0) += 8.936011904761905 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(1, 1) += -1.0 * s * dq1;
+            J(5, 1) += -16.87202380952381 * s * dq1;
+            J(4, 1) += 17.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(1, 2) += -0.031501968873054564 * s * dq2;
+            J(5, 2) += -0.5315019688730546 * s * dq2;
+            J(4, 2) += 0.5630039377461091 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(1, 3) += -0.06300393774610913 * s * dq3;
+            J(5, 3) += -1.0630039377461091 * s * dq3;
+            J(4, 3) += 1.1260078754922183 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(1, 4) += -0.055953372189841796 * s * dq4;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(5, 5) += -1.0 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(1, 6) += -0.029634856235667664 * s * dq6;
+            J(5, 6) += -0.5 * s * dq6;
+            J(4, 6) += 0.5296348562356676 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(4, 7) += 0.5458098527540447 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(1, 8) += -0.03598200899550225 * s * dq8;
+            J(5, 8) += -0.6070893124866139 * s * dq8;
+            J(4, 8) += 0.6430713214821161 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 6
-        const double pf = C3 * C4;
-        const double pb = (C5 * C5);
-        const double kfM = K.kf[6];
-        const double dlnk = (1.704 + 62704771.199999996 * invRT) * invT;
-        const double dlner = (0.0 - (2.0 * K.hRT[5] - (1.0 * K.hRT[3] + 1.0 * K.hRT[4]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[6] * pb) - K.er[6] * dlner * pb);
-        const double dq3 = kfM * (C4);
-        const double dq4 = kfM * (C3);
-        const double dq5 = -kfM * K.er[6] * (2.0 * C5);
-        const double e_r = -1.0 * (K.hRT[3] - 1.0) + -1.0 * (K.hRT[4] - 1.0) + 2.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(3, 3) += -1.0 * s * dq3;
-        J(4, 3) += -1.1260078754922183 * s * dq3;
-        J(5, 3) += 2.1260078754922183 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(3, 4) += -0.8880932556203164 * s * dq4;
-        J(4, 4) += -1.0 * s * dq4;
-        J(5, 4) += 1.8880932556203165 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(4, 5) += -1.0592697124713353 * s * dq5;
-        J(5, 5) += 2.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(4, 9) += -18.015 * s_rho * dqT;
-        J(5, 9) += 34.014 * s_rho * dqT;
+        const double kf = 67000.00000000001 * exp(1.704 * logT - 62704771.199999996 * invRT);
+        const double er = exp(2.0 * th.gRT[5] - th.gRT[3] - th.gRT[4]);
+        {  // rate of progress: 1 O + 1 H2O <=> 2 OH
+            const double kfM = kf;
+            const double fwd = kfM * C3 * C4;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w3 -= q;
+            w4 -= q;
+            w5 += 2.0 * q;
+        }
+        {  // Jacobian terms
+            const double pf = C3 * C4;
+            const double pb = (C5 * C5);
+            const double kfM = kf;
+            const double dlnk = (1.704 + 62704771.199999996 * invRT) * invT;
+            const double dlner = (0.0 - (2.0 * th.hRT[5] - (1.0 * th.hRT[3] + 1.0 * th.hRT[4]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq3 = kfM * (C4);
+            const double dq4 = kfM * (C3);
+            const double dq5 = -kfM * er * (2.0 * C5);
+            const double e_r = -1.0 * (th.hRT[3] - 1.0) + -1.0 * (th.hRT[4] - 1.0) + 2.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(3, 3) += -1.0 * s * dq3;
+            J(4, 3) += -1.1260078754922183 * s * dq3;
+            J(5, 3) += 2.1260078754922183 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(3, 4) += -0.8880932556203164 * s * dq4;
+            J(4, 4) += -1.0 * s * dq4;
+            J(5, 4) += 1.8880932556203165 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(4, 5) += -1.0592697124713353 * s * dq5;
+            J(5, 5) += 2.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(4, 9) += -18.015 * s_rho * dqT;
+            J(5, 9) += 34.014 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 7
-        const double pf = C3 * C1;
-        const double pb = C5;
-        const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[7] * M;
-        const double dkdM = K.kf[7];
-        const double dlnk = (-1.0 + 0.0 * invRT) * invT;
-        const double g = dkdM * (pf - K.er[7] * pb);
-        const double dlner = (-1.0 - (1.0 * K.hRT[5] - (1.0 * K.hRT[3] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[7] * pb) - K.er[7] * dlner * pb);
-        const double dq0 = 2.5 * g;
-        const double dq1 = kfM * (C3) + g;
-        const double dq2 = g;
-        const double dq3 = kfM * (C1) + g;
-        const double dq4 = 12.0 * g;
-        const double dq5 = -kfM * K.er[7] * (1.0) + g;
-        const double dq6 = g;
-        const double dq7 = g;
-        const double dq8 = g;
-        const double e_r = -1.0 * (K.hRT[3] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(3, 0) += -7.936011904761905 * s * dq0;
-        J(1, 0) += -0.5 * s * dq0;
-        J(5, 0) += 8.436011904761905 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(3, 1) += -15.87202380952381 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(5, 1) += 16.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(3, 2) += -0.5 * s * dq2;
-        J(1, 2) += -0.031501968873054564 * s * dq2;
-        J(5, 2) += 0.5315019688730546 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(3, 3) += -1.0 * s * dq3;
-        J(1, 3) += -0.06300393774610913 * s * dq3;
-        J(5, 3) += 1.0630039377461091 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(3, 4) += -0.8880932556203164 * s * dq4;
-        J(1, 4) += -0.055953372189841796 * s * dq4;
-        J(5, 4) += 0.9440466278101582 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(3, 6) += -0.4703651437643323 * s * dq6;
-        J(1, 6) += -0.029634856235667664 * s * dq6;
-        J(5, 6) += 0.5 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(3, 7) += -0.4847300490819851 * s * dq7;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(5, 7) += 0.515269950918015 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(3, 8) += -0.5711073034911116 * s * dq8;
-        J(1, 8) += -0.03598200899550225 * s * dq8;
-        J(5, 8) += 0.6070893124866139 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
+        const double kf = 4714000000000.002 * exp(-1.0 * logT);
+        const double er = exp((th.gRT[5] - th.gRT[3] - th.gRT[1]) - -1.0 * log_cref);
+        {  // rate of progress: 1 O + 1 H <=> 1 OH  + M
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C3 * C1;
+            const double rev = kfM * er * C5;
+            const double q = fwd - rev;
+            w3 -= q;
+            w1 -= q;
+            w5 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C3 * C1;
+            const double pb = C5;
+            const double M = 2.5 * C0 + C1 + C2 + C3 + 12.0 * C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double dkdM = kf;
+            const double dlnk = (-1.0 + 0.0 * invRT) * invT;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (-1.0 - (1.0 * th.hRT[5] - (1.0 * th.hRT[3] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = 2.5 * g;
+            const double dq1 = kfM * (C3) + g;
+            const double dq2 = g;
+            const double dq3 = kfM * (C1) + g;
+            const double dq4 = 12.0 * g;
+            const double dq5 = -kfM * er * (1.0) + g;
+            const double dq6 = g;
+            const double dq7 = g;
+            const double dq8 = g;
+            const double e_r = -1.0 * (th.hRT[3] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(3, 0) += -7.936011904761905 * s * dq0;
+            J(1, 0) += -0.5 * s * dq0;
+            J(5, 0) += 8.436011904761905 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(3, 1) += -15.87202380952381 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(5, 1) += 16.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(3, 2) += -0.5 * s * dq2;
+            J(1, 2) += -0.031501968873054564 * s * dq2;
+            J(5, 2) += 0.5315019688730546 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(3, 3) += -1.0 * s * dq3;
+            J(1, 3) += -0.06300393774610913 * s * dq3;
+            J(5, 3) += 1.0630039377461091 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(3, 4) += -0.8880932556203164 * s * dq4;
+            J(1, 4) += -0.055953372189841796 * s * dq4;
+            J(5, 4) += 0.9440466278101582 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(3, 6) += -0.4703651437643323 * s * dq6;
+            J(1, 6) += -0.029634856235667664 * s * dq6;
+            J(5, 6) += 0.5 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(3, 7) += -0.4847300490819851 * s * dq7;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(5, 7) += 0.515269950918015 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -0.5711073034911116 * s * dq8;
+            J(1, 8) += -0.03598200899550225 * s * dq8;
+            J(5, 8) += 0.6070893124866139 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 8
-        const double pf = C6;
-        const double pb = (C5 * C5);
-        const double M = 3.7 * C0 + C1 + 1.2 * C2 + C3 + 7.65 * C4 + C5 + 7.7 * C6 + C7 + 1.5 * C8;
-        const double Pr = K.k0[0] * M / K.kf[8];
-        const double ipr = 1.0 / (1.0 + Pr);
-        const double dlnkinf = (0.9 + 203965816.0 * invRT) * invT;
-        const double dlnk0 = (-2.3 + 203965816.0 * invRT) * invT;
-        const double lFc = K.lFc[0];
-        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-        const double lPr = log10(fmax(Pr, 1e-300));
-        const double u = lPr + c, den = n - 0.14 * u;
-        const double x = u / den;
-        const double opx = 1.0 + x * x;
-        const double Fo = pow(10.0, lFc / opx);
-        const double kfM = K.kf[8] * (Pr * ipr) * Fo;
-        const double dkdM = K.k0[0] * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));
-        const double dlFc = 0.0;
-        const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;
-        const double dden = -1.27 * dlFc - 0.14 * du;
-        const double dx = (du * den - u * dden) / (den * den);
-        const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));
-        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;
-        const double g = dkdM * (pf - K.er[8] * pb);
-        const double dlner = (1.0 - (2.0 * K.hRT[5] - (1.0 * K.hRT[6]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[8] * pb) - K.er[8] * dlner * pb);
-        const double dq0 = 3.7 * g;
-        const double dq1 = g;
-        const double dq2 = 1.2 * g;
-        const double dq3 = g;
-        const double dq4 = 7.65 * g;
-        const double dq5 = -kfM * K.er[8] * (2.0 * C5) + g;
-        const double dq6 = kfM * (1.0) + 7.7 * g;
-        const double dq7 = g;
-        const double dq8 = 1.5 * g;
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + 2.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 0) += -16.87202380952381 * s * dq0;
-        J(5, 0) += 16.87202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(6, 1) += -33.74404761904762 * s * dq1;
-        J(5, 1) += 33.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(6, 2) += -1.0630039377461091 * s * dq2;
-        J(5, 2) += 1.0630039377461091 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(6, 3) += -2.1260078754922183 * s * dq3;
-        J(5, 3) += 2.1260078754922183 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(6, 4) += -1.8880932556203165 * s * dq4;
-        J(5, 4) += 1.8880932556203165 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(6, 5) += -2.0 * s * dq5;
-        J(5, 5) += 2.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(6, 6) += -1.0 * s * dq6;
-        J(5, 6) += 1.0 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 7) += -1.03053990183603 * s * dq7;
-        J(5, 7) += 1.03053990183603 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(6, 8) += -1.2141786249732278 * s * dq8;
-        J(5, 8) += 1.2141786249732278 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(5, 9) += 34.014 * s_rho * dqT;
+        const double kf = 2000000000000.0 * exp(0.9 * logT - 203965816.0 * invRT);
+        const double k0 = 2.4900000000000005e+21 * exp(-2.3 * logT - 203965816.0 * invRT);
+        const double lFc0 = -0.36653154442041347;
+        const double er = exp((2.0 * th.gRT[5] - th.gRT[6]) - 1.0 * log_cref);
+        {  // rate of progress: 1 H2O2 <=> 2 OH  (+M)
+            const double M = 3.7 * C0 + C1 + 1.2 * C2 + C3 + 7.65 * C4 + C5 + 7.7 * C6 + C7 + 1.5 * C8;
+            const double Pr = k0 * M / kf;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+            const double kfM = kf * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
+            const double fwd = kfM * C6;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 += 2.0 * q;
+        }
+        {  // Jacobian terms
+            const double pf = C6;
+            const double pb = (C5 * C5);
+            const double M = 3.7 * C0 + C1 + 1.2 * C2 + C3 + 7.65 * C4 + C5 + 7.7 * C6 + C7 + 1.5 * C8;
+            const double Pr = k0 * M / kf;
+            const double ipr = 1.0 / (1.0 + Pr);
+            const double dlnkinf = (0.9 + 203965816.0 * invRT) * invT;
+            const double dlnk0 = (-2.3 + 203965816.0 * invRT) * invT;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double u = lPr + c, den = n - 0.14 * u;
+            const double x = u / den;
+            const double opx = 1.0 + x * x;
+            const double Fo = pow(10.0, lFc / opx);
+            const double kfM = kf * (Pr * ipr) * Fo;
+            const double dkdM = k0 * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));
+            const double dlFc = 0.0;
+            const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;
+            const double dden = -1.27 * dlFc - 0.14 * du;
+            const double dx = (du * den - u * dden) / (den * den);
+            const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));
+            const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (1.0 - (2.0 * th.hRT[5] - (1.0 * th.hRT[6]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = 3.7 * g;
+            const double dq1 = g;
+            const double dq2 = 1.2 * g;
+            const double dq3 = g;
+            const double dq4 = 7.65 * g;
+            const double dq5 = -kfM * er * (2.0 * C5) + g;
+            const double dq6 = kfM * (1.0) + 7.7 * g;
+            const double dq7 = g;
+            const double dq8 = 1.5 * g;
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + 2.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 0) += -16.87202380952381 * s * dq0;
+            J(5, 0) += 16.87202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(6, 1) += -33.74404761904762 * s * dq1;
+            J(5, 1) += 33.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(6, 2) += -1.0630039377461091 * s * dq2;
+            J(5, 2) += 1.0630039377461091 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(6, 3) += -2.1260078754922183 * s * dq3;
+            J(5, 3) += 2.1260078754922183 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(6, 4) += -1.8880932556203165 * s * dq4;
+            J(5, 4) += 1.8880932556203165 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(6, 5) += -2.0 * s * dq5;
+            J(5, 5) += 2.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(6, 6) += -1.0 * s * dq6;
+            J(5, 6) += 1.0 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 7) += -1.03053990183603 * s * dq7;
+            J(5, 7) += 1.03053990183603 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -1.2141786249732278 * s * dq8;
+            J(5, 8) += 1.2141786249732278 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(5, 9) += 34.014 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 9
-        const double pf = C6 * C1;
-        const double pb = C4 * C5;
-        const double kfM = K.kf[9];
-        const double dlnk = (0.0 + 16610480.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[4] + 1.0 * K.hRT[5] - (1.0 * K.hRT[6] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[9] * pb) - K.er[9] * dlner * pb);
-        const double dq1 = kfM * (C6);
-        const double dq4 = -kfM * K.er[9] * (C5);
-        const double dq5 = -kfM * K.er[9] * (C4);
-        const double dq6 = kfM * (C1);
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[4] - 1.0) + 1.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 1) += -33.74404761904762 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(4, 1) += 17.87202380952381 * s * dq1;
-        J(5, 1) += 16.87202380952381 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(6, 4) += -1.8880932556203165 * s * dq4;
-        J(1, 4) += -0.055953372189841796 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(5, 4) += 0.9440466278101582 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(6, 5) += -2.0 * s * dq5;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(6, 6) += -1.0 * s * dq6;
-        J(1, 6) += -0.029634856235667664 * s * dq6;
-        J(4, 6) += 0.5296348562356676 * s * dq6;
-        J(5, 6) += 0.5 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
+        const double kf = 24100000000.000008 * exp(-(16610480.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[5] - th.gRT[6] - th.gRT[1]);
+        {  // rate of progress: 1 H2O2 + 1 H <=> 1 H2O + 1 OH
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C1;
+            const double rev = kfM * er * C4 * C5;
+            const double q = fwd - rev;
+            w6 -= q;
+            w1 -= q;
+            w4 += q;
+            w5 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C6 * C1;
+            const double pb = C4 * C5;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 16610480.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[4] + 1.0 * th.hRT[5] - (1.0 * th.hRT[6] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq1 = kfM * (C6);
+            const double dq4 = -kfM * er * (C5);
+            const double dq5 = -kfM * er * (C4);
+            const double dq6 = kfM * (C1);
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[4] - 1.0) + 1.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 1) += -33.74404761904762 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(4, 1) += 17.87202380952381 * s * dq1;
+            J(5, 1) += 16.87202380952381 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(6, 4) += -1.8880932556203165 * s * dq4;
+            J(1, 4) += -0.055953372189841796 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(5, 4) += 0.9440466278101582 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(6, 5) += -2.0 * s * dq5;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(6, 6) += -1.0 * s * dq6;
+            J(1, 6) += -0.029634856235667664 * s * dq6;
+            J(4, 6) += 0.5296348562356676 * s * dq6;
+            J(5, 6) += 0.5 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 10
-        const double pf = C6 * C1;
-        const double pb = C0 * C7;
-        const double kfM = K.kf[10];
-        const double dlnk = (1.0 + 25104000.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[0] + 1.0 * K.hRT[7] - (1.0 * K.hRT[6] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[10] * pb) - K.er[10] * dlner * pb);
-        const double dq0 = -kfM * K.er[10] * (C7);
-        const double dq1 = kfM * (C6);
-        const double dq6 = kfM * (C1);
-        const double dq7 = -kfM * K.er[10] * (C0);
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[0] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 0) += -16.87202380952381 * s * dq0;
-        J(1, 0) += -0.5 * s * dq0;
-        J(0, 0) += 1.0 * s * dq0;
-        J(7, 0) += 16.37202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(6, 1) += -33.74404761904762 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(0, 1) += 2.0 * s * dq1;
-        J(7, 1) += 32.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(6, 6) += -1.0 * s * dq6;
-        J(1, 6) += -0.029634856235667664 * s * dq6;
-        J(0, 6) += 0.05926971247133533 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 7) += -1.03053990183603 * s * dq7;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(0, 7) += 0.061079803672059625 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(0, 9) += 2.016 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 21500000.000000004 * exp(1.0 * logT - 25104000.0 * invRT);
+        const double er = exp(th.gRT[0] + th.gRT[7] - th.gRT[6] - th.gRT[1]);
+        {  // rate of progress: 1 H2O2 + 1 H <=> 1 H2 + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C1;
+            const double rev = kfM * er * C0 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w1 -= q;
+            w0 += q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C6 * C1;
+            const double pb = C0 * C7;
+            const double kfM = kf;
+            const double dlnk = (1.0 + 25104000.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[0] + 1.0 * th.hRT[7] - (1.0 * th.hRT[6] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = -kfM * er * (C7);
+            const double dq1 = kfM * (C6);
+            const double dq6 = kfM * (C1);
+            const double dq7 = -kfM * er * (C0);
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[0] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 0) += -16.87202380952381 * s * dq0;
+            J(1, 0) += -0.5 * s * dq0;
+            J(0, 0) += 1.0 * s * dq0;
+            J(7, 0) += 16.37202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(6, 1) += -33.74404761904762 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(0, 1) += 2.0 * s * dq1;
+            J(7, 1) += 32.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(6, 6) += -1.0 * s * dq6;
+            J(1, 6) += -0.029634856235667664 * s * dq6;
+            J(0, 6) += 0.05926971247133533 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 7) += -1.03053990183603 * s * dq7;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(0, 7) += 0.061079803672059625 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(0, 9) += 2.016 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 11
-        const double pf = C6 * C3;
-        const double pb = C5 * C7;
-        const double kfM = K.kf[11];
-        const double dlnk = (2.0 + 16610480.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[5] + 1.0 * K.hRT[7] - (1.0 * K.hRT[6] + 1.0 * K.hRT[3]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[11] * pb) - K.er[11] * dlner * pb);
-        const double dq3 = kfM * (C6);
-        const double dq5 = -kfM * K.er[11] * (C7);
-        const double dq6 = kfM * (C3);
-        const double dq7 = -kfM * K.er[11] * (C5);
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + -1.0 * (K.hRT[3] - 1.0) + 1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 3) += -2.1260078754922183 * s * dq3;
-        J(3, 3) += -1.0 * s * dq3;
-        J(5, 3) += 1.0630039377461091 * s * dq3;
-        J(7, 3) += 2.063003937746109 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(6, 5) += -2.0 * s * dq5;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(7, 5) += 1.9407302875286645 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(6, 6) += -1.0 * s * dq6;
-        J(3, 6) += -0.4703651437643323 * s * dq6;
-        J(5, 6) += 0.5 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 7) += -1.03053990183603 * s * dq7;
-        J(3, 7) += -0.4847300490819851 * s * dq7;
-        J(5, 7) += 0.515269950918015 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 9550.000000000002 * exp(2.0 * logT - 16610480.0 * invRT);
+        const double er = exp(th.gRT[5] + th.gRT[7] - th.gRT[6] - th.gRT[3]);
+        {  // rate of progress: 1 H2O2 + 1 O <=> 1 OH + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C3;
+            const double rev = kfM * er * C5 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w3 -= q;
+            w5 += q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C6 * C3;
+            const double pb = C5 * C7;
+            const double kfM = kf;
+            const double dlnk = (2.0 + 16610480.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[5] + 1.0 * th.hRT[7] - (1.0 * th.hRT[6] + 1.0 * th.hRT[3]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq3 = kfM * (C6);
+            const double dq5 = -kfM * er * (C7);
+            const double dq6 = kfM * (C3);
+            const double dq7 = -kfM * er * (C5);
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + -1.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 3) += -2.1260078754922183 * s * dq3;
+            J(3, 3) += -1.0 * s * dq3;
+            J(5, 3) += 1.0630039377461091 * s * dq3;
+            J(7, 3) += 2.063003937746109 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(6, 5) += -2.0 * s * dq5;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(7, 5) += 1.9407302875286645 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(6, 6) += -1.0 * s * dq6;
+            J(3, 6) += -0.4703651437643323 * s * dq6;
+            J(5, 6) += 0.5 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 7) += -1.03053990183603 * s * dq7;
+            J(3, 7) += -0.4847300490819851 * s * dq7;
+            J(5, 7) += 0.515269950918015 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 12
-        const double pf = C6 * C5;
-        const double pb = C4 * C7;
-        const double kfM = K.kf[12];
-        const double dlnk = (0.0 + 1330512.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[4] + 1.0 * K.hRT[7] - (1.0 * K.hRT[6] + 1.0 * K.hRT[5]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[12] * pb) - K.er[12] * dlner * pb);
-        const double dq4 = -kfM * K.er[12] * (C7);
-        const double dq5 = kfM * (C6);
-        const double dq6 = kfM * (C5);
-        const double dq7 = -kfM * K.er[12] * (C4);
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + -1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[4] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 4) += -1.8880932556203165 * s * dq4;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(7, 4) += 1.8321398834304745 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(6, 5) += -2.0 * s * dq5;
-        J(5, 5) += -1.0 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(7, 5) += 1.9407302875286645 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(6, 6) += -1.0 * s * dq6;
-        J(5, 6) += -0.5 * s * dq6;
-        J(4, 6) += 0.5296348562356676 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 7) += -1.03053990183603 * s * dq7;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(4, 7) += 0.5458098527540447 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 1740000000.0000005 * exp(-(1330512.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[7] - th.gRT[6] - th.gRT[5]);
+        {  // rate of progress: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C5;
+            const double rev = kfM * er * C4 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 -= q;
+            w4 += q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C6 * C5;
+            const double pb = C4 * C7;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 1330512.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[4] + 1.0 * th.hRT[7] - (1.0 * th.hRT[6] + 1.0 * th.hRT[5]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq4 = -kfM * er * (C7);
+            const double dq5 = kfM * (C6);
+            const double dq6 = kfM * (C5);
+            const double dq7 = -kfM * er * (C4);
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[4] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 4) += -1.8880932556203165 * s * dq4;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(7, 4) += 1.8321398834304745 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(6, 5) += -2.0 * s * dq5;
+            J(5, 5) += -1.0 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(7, 5) += 1.9407302875286645 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(6, 6) += -1.0 * s * dq6;
+            J(5, 6) += -0.5 * s * dq6;
+            J(4, 6) += 0.5296348562356676 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 7) += -1.03053990183603 * s * dq7;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(4, 7) += 0.5458098527540447 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 13
-        const double pf = C6 * C5;
-        const double pb = C4 * C7;
-        const double kfM = K.kf[13];
-        const double dlnk = (0.0 + 30413496.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[4] + 1.0 * K.hRT[7] - (1.0 * K.hRT[6] + 1.0 * K.hRT[5]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[13] * pb) - K.er[13] * dlner * pb);
-        const double dq4 = -kfM * K.er[13] * (C7);
-        const double dq5 = kfM * (C6);
-        const double dq6 = kfM * (C5);
-        const double dq7 = -kfM * K.er[13] * (C4);
-        const double e_r = -1.0 * (K.hRT[6] - 1.0) + -1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[4] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(6, 4) += -1.8880932556203165 * s * dq4;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(7, 4) += 1.8321398834304745 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(6, 5) += -2.0 * s * dq5;
-        J(5, 5) += -1.0 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(7, 5) += 1.9407302875286645 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(6, 6) += -1.0 * s * dq6;
-        J(5, 6) += -0.5 * s * dq6;
-        J(4, 6) += 0.5296348562356676 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(6, 7) += -1.03053990183603 * s * dq7;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(4, 7) += 0.5458098527540447 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(6, 9) += -34.014 * s_rho * dqT;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 75900000000.00002 * exp(-(30413496.0 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[7] - th.gRT[6] - th.gRT[5]);
+        {  // rate of progress: 1 H2O2 + 1 OH <=> 1 H2O + 1 HO2
+            const double kfM = kf;
+            const double fwd = kfM * C6 * C5;
+            const double rev = kfM * er * C4 * C7;
+            const double q = fwd - rev;
+            w6 -= q;
+            w5 -= q;
+            w4 += q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C6 * C5;
+            const double pb = C4 * C7;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 30413496.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[4] + 1.0 * th.hRT[7] - (1.0 * th.hRT[6] + 1.0 * th.hRT[5]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq4 = -kfM * er * (C7);
+            const double dq5 = kfM * (C6);
+            const double dq6 = kfM * (C5);
+            const double dq7 = -kfM * er * (C4);
+            const double e_r = -1.0 * (th.hRT[6] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[4] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(6, 4) += -1.8880932556203165 * s * dq4;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(7, 4) += 1.8321398834304745 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(6, 5) += -2.0 * s * dq5;
+            J(5, 5) += -1.0 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(7, 5) += 1.9407302875286645 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(6, 6) += -1.0 * s * dq6;
+            J(5, 6) += -0.5 * s * dq6;
+            J(4, 6) += 0.5296348562356676 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 7) += -1.03053990183603 * s * dq7;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(4, 7) += 0.5458098527540447 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 9) += -34.014 * s_rho * dqT;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 14
-        const double pf = C7 * C1;
-        const double pb = (C5 * C5);
-        const double kfM = K.kf[14];
-        const double dlnk = (0.0 + 1234280.0 * invRT) * invT;
-        const double dlner = (0.0 - (2.0 * K.hRT[5] - (1.0 * K.hRT[7] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[14] * pb) - K.er[14] * dlner * pb);
-        const double dq1 = kfM * (C7);
-        const double dq5 = -kfM * K.er[14] * (2.0 * C5);
-        const double dq7 = kfM * (C1);
-        const double e_r = -1.0 * (K.hRT[7] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 2.0 * (K.hRT[5] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(7, 1) += -32.74404761904762 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(5, 1) += 33.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(7, 5) += -1.9407302875286645 * s * dq5;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(5, 5) += 2.0 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(7, 7) += -1.0 * s * dq7;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(5, 7) += 1.03053990183603 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(7, 9) += -33.006 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(5, 9) += 34.014 * s_rho * dqT;
+        const double kf = 70790000000.00002 * exp(-(1234280.0 * invRT));
+        const double er = exp(2.0 * th.gRT[5] - th.gRT[7] - th.gRT[1]);
+        {  // rate of progress: 1 HO2 + 1 H <=> 2 OH
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C1;
+            const double rev = kfM * er * (C5 * C5);
+            const double q = fwd - rev;
+            w7 -= q;
+            w1 -= q;
+            w5 += 2.0 * q;
+        }
+        {  // Jacobian terms
+            const double pf = C7 * C1;
+            const double pb = (C5 * C5);
+            const double kfM = kf;
+            const double dlnk = (0.0 + 1234280.0 * invRT) * invT;
+            const double dlner = (0.0 - (2.0 * th.hRT[5] - (1.0 * th.hRT[7] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq1 = kfM * (C7);
+            const double dq5 = -kfM * er * (2.0 * C5);
+            const double dq7 = kfM * (C1);
+            const double e_r = -1.0 * (th.hRT[7] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 2.0 * (th.hRT[5] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(7, 1) += -32.74404761904762 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(5, 1) += 33.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(7, 5) += -1.9407302875286645 * s * dq5;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(5, 5) += 2.0 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(7, 7) += -1.0 * s * dq7;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(5, 7) += 1.03053990183603 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 9) += -33.006 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(5, 9) += 34.014 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 15
-        const double pf = C7 * C1;
-        const double pb = C0 * C2;
-        const double kfM = K.kf[15];
-        const double dlnk = (1.0827 + 2317015.52 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[0] + 1.0 * K.hRT[2] - (1.0 * K.hRT[7] + 1.0 * K.hRT[1]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[15] * pb) - K.er[15] * dlner * pb);
-        const double dq0 = -kfM * K.er[15] * (C2);
-        const double dq1 = kfM * (C7);
-        const double dq2 = -kfM * K.er[15] * (C0);
-        const double dq7 = kfM * (C1);
-        const double e_r = -1.0 * (K.hRT[7] - 1.0) + -1.0 * (K.hRT[1] - 1.0) + 1.0 * (K.hRT[0] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(7, 0) += -16.37202380952381 * s * dq0;
-        J(1, 0) += -0.5 * s * dq0;
-        J(0, 0) += 1.0 * s * dq0;
-        J(2, 0) += 15.87202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(7, 1) += -32.74404761904762 * s * dq1;
-        J(1, 1) += -1.0 * s * dq1;
-        J(0, 1) += 2.0 * s * dq1;
-        J(2, 1) += 31.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(7, 2) += -1.0315019688730545 * s * dq2;
-        J(1, 2) += -0.031501968873054564 * s * dq2;
-        J(0, 2) += 0.06300393774610913 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(7, 7) += -1.0 * s * dq7;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(0, 7) += 0.061079803672059625 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(7, 9) += -33.006 * s_rho * dqT;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(0, 9) += 2.016 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 11402000.000000002 * exp(1.0827 * logT - 2317015.52 * invRT);
+        const double er = exp(th.gRT[0] + th.gRT[2] - th.gRT[7] - th.gRT[1]);
+        {  // rate of progress: 1 HO2 + 1 H <=> 1 H2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C1;
+            const double rev = kfM * er * C0 * C2;
+            const double q = fwd - rev;
+            w7 -= q;
+            w1 -= q;
+            w0 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C7 * C1;
+            const double pb = C0 * C2;
+            const double kfM = kf;
+            const double dlnk = (1.0827 + 2317015.52 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[0] + 1.0 * th.hRT[2] - (1.0 * th.hRT[7] + 1.0 * th.hRT[1]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = -kfM * er * (C2);
+            const double dq1 = kfM * (C7);
+            const double dq2 = -kfM * er * (C0);
+            const double dq7 = kfM * (C1);
+            const double e_r = -1.0 * (th.hRT[7] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[0] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(7, 0) += -16.37202380952381 * s * dq0;
+            J(1, 0) += -0.5 * s * dq0;
+            J(0, 0) += 1.0 * s * dq0;
+            J(2, 0) += 15.87202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(7, 1) += -32.74404761904762 * s * dq1;
+            J(1, 1) += -1.0 * s * dq1;
+            J(0, 1) += 2.0 * s * dq1;
+            J(2, 1) += 31.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(7, 2) += -1.0315019688730545 * s * dq2;
+            J(1, 2) += -0.031501968873054564 * s * dq2;
+            J(0, 2) += 0.06300393774610913 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(7, 7) += -1.0 * s * dq7;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(0, 7) += 0.061079803672059625 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 9) += -33.006 * s_rho * dqT;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(0, 9) += 2.016 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 16
-        const double pf = C7 * C3;
-        const double pb = C5 * C2;
-        const double kfM = K.kf[16];
-        const double dlnk = (0.0 + 0.0 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[5] + 1.0 * K.hRT[2] - (1.0 * K.hRT[7] + 1.0 * K.hRT[3]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[16] * pb) - K.er[16] * dlner * pb);
-        const double dq2 = -kfM * K.er[16] * (C5);
-        const double dq3 = kfM * (C7);
-        const double dq5 = -kfM * K.er[16] * (C2);
-        const double dq7 = kfM * (C3);
-        const double e_r = -1.0 * (K.hRT[7] - 1.0) + -1.0 * (K.hRT[3] - 1.0) + 1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(7, 2) += -1.0315019688730545 * s * dq2;
-        J(3, 2) += -0.5 * s * dq2;
-        J(5, 2) += 0.5315019688730546 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(7, 3) += -2.063003937746109 * s * dq3;
-        J(3, 3) += -1.0 * s * dq3;
-        J(5, 3) += 1.0630039377461091 * s * dq3;
-        J(2, 3) += 2.0 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(7, 5) += -1.9407302875286645 * s * dq5;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(5, 5) += 1.0 * s * dq5;
-        J(2, 5) += 1.8814605750573292 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(7, 7) += -1.0 * s * dq7;
-        J(3, 7) += -0.4847300490819851 * s * dq7;
-        J(5, 7) += 0.515269950918015 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(7, 9) += -33.006 * s_rho * dqT;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(5, 9) += 17.007 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 32500000000.000008;
+        const double er = exp(th.gRT[5] + th.gRT[2] - th.gRT[7] - th.gRT[3]);
+        {  // rate of progress: 1 HO2 + 1 O <=> 1 OH + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C7 * C3;
+            const double rev = kfM * er * C5 * C2;
+            const double q = fwd - rev;
+            w7 -= q;
+            w3 -= q;
+            w5 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C7 * C3;
+            const double pb = C5 * C2;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 0.0 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[5] + 1.0 * th.hRT[2] - (1.0 * th.hRT[7] + 1.0 * th.hRT[3]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq2 = -kfM * er * (C5);
+            const double dq3 = kfM * (C7);
+            const double dq5 = -kfM * er * (C2);
+            const double dq7 = kfM * (C3);
+            const double e_r = -1.0 * (th.hRT[7] - 1.0) + -1.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(7, 2) += -1.0315019688730545 * s * dq2;
+            J(3, 2) += -0.5 * s * dq2;
+            J(5, 2) += 0.5315019688730546 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(7, 3) += -2.063003937746109 * s * dq3;
+            J(3, 3) += -1.0 * s * dq3;
+            J(5, 3) += 1.0630039377461091 * s * dq3;
+            J(2, 3) += 2.0 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(7, 5) += -1.9407302875286645 * s * dq5;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(5, 5) += 1.0 * s * dq5;
+            J(2, 5) += 1.8814605750573292 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(7, 7) += -1.0 * s * dq7;
+            J(3, 7) += -0.4847300490819851 * s * dq7;
+            J(5, 7) += 0.515269950918015 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 9) += -33.006 * s_rho * dqT;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(5, 9) += 17.007 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 17
-        const double pf = C5 * C7;
-        const double pb = C4 * C2;
-        const double kfM = K.kf[17];
-        const double dlnk = (0.0 + -4572944.640000001 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[4] + 1.0 * K.hRT[2] - (1.0 * K.hRT[5] + 1.0 * K.hRT[7]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[17] * pb) - K.er[17] * dlner * pb);
-        const double dq2 = -kfM * K.er[17] * (C4);
-        const double dq4 = -kfM * K.er[17] * (C2);
-        const double dq5 = kfM * (C7);
-        const double dq7 = kfM * (C5);
-        const double e_r = -1.0 * (K.hRT[5] - 1.0) + -1.0 * (K.hRT[7] - 1.0) + 1.0 * (K.hRT[4] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(5, 2) += -0.5315019688730546 * s * dq2;
-        J(7, 2) += -1.0315019688730545 * s * dq2;
-        J(4, 2) += 0.5630039377461091 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(7, 4) += -1.8321398834304745 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(2, 4) += 1.7761865112406328 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(5, 5) += -1.0 * s * dq5;
-        J(7, 5) += -1.9407302875286645 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(2, 5) += 1.8814605750573292 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(7, 7) += -1.0 * s * dq7;
-        J(4, 7) += 0.5458098527540447 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(7, 9) += -33.006 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 7000000000.000002 * exp(-(-4572944.640000001 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[2] - th.gRT[5] - th.gRT[7]);
+        {  // rate of progress: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C5 * C7;
+            const double rev = kfM * er * C4 * C2;
+            const double q = fwd - rev;
+            w5 -= q;
+            w7 -= q;
+            w4 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C5 * C7;
+            const double pb = C4 * C2;
+            const double kfM = kf;
+            const double dlnk = (0.0 + -4572944.640000001 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[4] + 1.0 * th.hRT[2] - (1.0 * th.hRT[5] + 1.0 * th.hRT[7]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq2 = -kfM * er * (C4);
+            const double dq4 = -kfM * er * (C2);
+            const double dq5 = kfM * (C7);
+            const double dq7 = kfM * (C5);
+            const double e_r = -1.0 * (th.hRT[5] - 1.0) + -1.0 * (th.hRT[7] - 1.0) + 1.0 * (th.hRT[4] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(5, 2) += -0.5315019688730546 * s * dq2;
+            J(7, 2) += -1.0315019688730545 * s * dq2;
+            J(4, 2) += 0.5630039377461091 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(7, 4) += -1.8321398834304745 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(2, 4) += 1.7761865112406328 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(5, 5) += -1.0 * s * dq5;
+            J(7, 5) += -1.9407302875286645 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(2, 5) += 1.8814605750573292 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(7, 7) += -1.0 * s * dq7;
+            J(4, 7) += 0.5458098527540447 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(7, 9) += -33.006 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 18
-        const double pf = C5 * C7;
-        const double pb = C4 * C2;
-        const double kfM = K.kf[18];
-        const double dlnk = (0.0 + 45729446.4 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[4] + 1.0 * K.hRT[2] - (1.0 * K.hRT[5] + 1.0 * K.hRT[7]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[18] * pb) - K.er[18] * dlner * pb);
-        const double dq2 = -kfM * K.er[18] * (C4);
-        const double dq4 = -kfM * K.er[18] * (C2);
-        const double dq5 = kfM * (C7);
-        const double dq7 = kfM * (C5);
-        const double e_r = -1.0 * (K.hRT[5] - 1.0) + -1.0 * (K.hRT[7] - 1.0) + 1.0 * (K.hRT[4] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(5, 2) += -0.5315019688730546 * s * dq2;
-        J(7, 2) += -1.0315019688730545 * s * dq2;
-        J(4, 2) += 0.5630039377461091 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(7, 4) += -1.8321398834304745 * s * dq4;
-        J(4, 4) += 1.0 * s * dq4;
-        J(2, 4) += 1.7761865112406328 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(5, 5) += -1.0 * s * dq5;
-        J(7, 5) += -1.9407302875286645 * s * dq5;
-        J(4, 5) += 1.0592697124713353 * s * dq5;
-        J(2, 5) += 1.8814605750573292 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(7, 7) += -1.0 * s * dq7;
-        J(4, 7) += 0.5458098527540447 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(7, 9) += -33.006 * s_rho * dqT;
-        J(4, 9) += 18.015 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 450000000000.0001 * exp(-(45729446.4 * invRT));
+        const double er = exp(th.gRT[4] + th.gRT[2] - th.gRT[5] - th.gRT[7]);
+        {  // rate of progress: 1 OH + 1 HO2 <=> 1 H2O + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * C5 * C7;
+            const double rev = kfM * er * C4 * C2;
+            const double q = fwd - rev;
+            w5 -= q;
+            w7 -= q;
+            w4 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C5 * C7;
+            const double pb = C4 * C2;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 45729446.4 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[4] + 1.0 * th.hRT[2] - (1.0 * th.hRT[5] + 1.0 * th.hRT[7]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq2 = -kfM * er * (C4);
+            const double dq4 = -kfM * er * (C2);
+            const double dq5 = kfM * (C7);
+            const double dq7 = kfM * (C5);
+            const double e_r = -1.0 * (th.hRT[5] - 1.0) + -1.0 * (th.hRT[7] - 1.0) + 1.0 * (th.hRT[4] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(5, 2) += -0.5315019688730546 * s * dq2;
+            J(7, 2) += -1.0315019688730545 * s * dq2;
+            J(4, 2) += 0.5630039377461091 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(7, 4) += -1.8321398834304745 * s * dq4;
+            J(4, 4) += 1.0 * s * dq4;
+            J(2, 4) += 1.7761865112406328 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(5, 5) += -1.0 * s * dq5;
+            J(7, 5) += -1.9407302875286645 * s * dq5;
+            J(4, 5) += 1.0592697124713353 * s * dq5;
+            J(2, 5) += 1.8814605750573292 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(7, 7) += -1.0 * s * dq7;
+            J(4, 7) += 0.5458098527540447 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(7, 9) += -33.006 * s_rho * dqT;
+            J(4, 9) += 18.015 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 19
-        const double pf = (C7 * C7);
-        const double pb = C6 * C2;
-        const double kfM = K.kf[19];
-        const double dlnk = (0.0 + 46195054.472 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[6] + 1.0 * K.hRT[2] - (2.0 * K.hRT[7]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[19] * pb) - K.er[19] * dlner * pb);
-        const double dq2 = -kfM * K.er[19] * (C6);
-        const double dq6 = -kfM * K.er[19] * (C2);
-        const double dq7 = kfM * (2.0 * C7);
-        const double e_r = -2.0 * (K.hRT[7] - 1.0) + 1.0 * (K.hRT[6] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(7, 2) += -2.063003937746109 * s * dq2;
-        J(6, 2) += 1.0630039377461091 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(7, 6) += -1.9407302875286645 * s * dq6;
-        J(6, 6) += 1.0 * s * dq6;
-        J(2, 6) += 0.9407302875286646 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(7, 7) += -2.0 * s * dq7;
-        J(6, 7) += 1.03053990183603 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(7, 9) += -66.012 * s_rho * dqT;
-        J(6, 9) += 34.014 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 100000000000.00003 * exp(-(46195054.472 * invRT));
+        const double er = exp(th.gRT[6] + th.gRT[2] - 2.0 * th.gRT[7]);
+        {  // rate of progress: 2 HO2 <=> 1 H2O2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * (C7 * C7);
+            const double rev = kfM * er * C6 * C2;
+            const double q = fwd - rev;
+            w7 -= 2.0 * q;
+            w6 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = (C7 * C7);
+            const double pb = C6 * C2;
+            const double kfM = kf;
+            const double dlnk = (0.0 + 46195054.472 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[6] + 1.0 * th.hRT[2] - (2.0 * th.hRT[7]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq2 = -kfM * er * (C6);
+            const double dq6 = -kfM * er * (C2);
+            const double dq7 = kfM * (2.0 * C7);
+            const double e_r = -2.0 * (th.hRT[7] - 1.0) + 1.0 * (th.hRT[6] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(7, 2) += -2.063003937746109 * s * dq2;
+            J(6, 2) += 1.0630039377461091 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(7, 6) += -1.9407302875286645 * s * dq6;
+            J(6, 6) += 1.0 * s * dq6;
+            J(2, 6) += 0.9407302875286646 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(7, 7) += -2.0 * s * dq7;
+            J(6, 7) += 1.03053990183603 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 9) += -66.012 * s_rho * dqT;
+            J(6, 9) += 34.014 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 20
-        const double pf = (C7 * C7);
-        const double pb = C6 * C2;
-        const double kfM = K.kf[20];
-        const double dlnk = (0.0 + -5894941.3632 * invRT) * invT;
-        const double dlner = (0.0 - (1.0 * K.hRT[6] + 1.0 * K.hRT[2] - (2.0 * K.hRT[7]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[20] * pb) - K.er[20] * dlner * pb);
-        const double dq2 = -kfM * K.er[20] * (C6);
-        const double dq6 = -kfM * K.er[20] * (C2);
-        const double dq7 = kfM * (2.0 * C7);
-        const double e_r = -2.0 * (K.hRT[7] - 1.0) + 1.0 * (K.hRT[6] - 1.0) + 1.0 * (K.hRT[2] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(7, 2) += -2.063003937746109 * s * dq2;
-        J(6, 2) += 1.0630039377461091 * s * dq2;
-        J(2, 2) += 1.0 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(7, 6) += -1.9407302875286645 * s * dq6;
-        J(6, 6) += 1.0 * s * dq6;
-        J(2, 6) += 0.9407302875286646 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(7, 7) += -2.0 * s * dq7;
-        J(6, 7) += 1.03053990183603 * s * dq7;
-        J(2, 7) += 0.9694600981639702 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(7, 9) += -66.012 * s_rho * dqT;
-        J(6, 9) += 34.014 * s_rho * dqT;
-        J(2, 9) += 31.998 * s_rho * dqT;
+        const double kf = 190000000.00000006 * exp(-(-5894941.3632 * invRT));
+        const double er = exp(th.gRT[6] + th.gRT[2] - 2.0 * th.gRT[7]);
+        {  // rate of progress: 2 HO2 <=> 1 H2O2 + 1 O2
+            const double kfM = kf;
+            const double fwd = kfM * (C7 * C7);
+            const double rev = kfM * er * C6 * C2;
+            const double q = fwd - rev;
+            w7 -= 2.0 * q;
+            w6 += q;
+            w2 += q;
+        }
+        {  // Jacobian terms
+            const double pf = (C7 * C7);
+            const double pb = C6 * C2;
+            const double kfM = kf;
+            const double dlnk = (0.0 + -5894941.3632 * invRT) * invT;
+            const double dlner = (0.0 - (1.0 * th.hRT[6] + 1.0 * th.hRT[2] - (2.0 * th.hRT[7]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq2 = -kfM * er * (C6);
+            const double dq6 = -kfM * er * (C2);
+            const double dq7 = kfM * (2.0 * C7);
+            const double e_r = -2.0 * (th.hRT[7] - 1.0) + 1.0 * (th.hRT[6] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(7, 2) += -2.063003937746109 * s * dq2;
+            J(6, 2) += 1.0630039377461091 * s * dq2;
+            J(2, 2) += 1.0 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(7, 6) += -1.9407302875286645 * s * dq6;
+            J(6, 6) += 1.0 * s * dq6;
+            J(2, 6) += 0.9407302875286646 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(7, 7) += -2.0 * s * dq7;
+            J(6, 7) += 1.03053990183603 * s * dq7;
+            J(2, 7) += 0.9694600981639702 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 9) += -66.012 * s_rho * dqT;
+            J(6, 9) += 34.014 * s_rho * dqT;
+            J(2, 9) += 31.998 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 21
-        const double pf = C1 * C2;
-        const double pb = C7;
-        const double M = 1.3 * C0 + C1 + C2 + C3 + 10.0 * C4 + C5 + C6 + C7 + C8;
-        const double Pr = K.k0[1] * M / K.kf[21];
-        const double ipr = 1.0 / (1.0 + Pr);
-        const double dlnkinf = (0.44 + 0.0 * invRT) * invT;
-        const double dlnk0 = (-1.23 + 0.0 * invRT) * invT;
-        const double lFc = K.lFc[1];
-        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
-        const double lPr = log10(fmax(Pr, 1e-300));
-        const double u = lPr + c, den = n - 0.14 * u;
-        const double x = u / den;
-        const double opx = 1.0 + x * x;
-        const double Fo = pow(10.0, lFc / opx);
-        const double kfM = K.kf[21] * (Pr * ipr) * Fo;
-        const double dkdM = K.k0[1] * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));
-        const double dlFc = 0.0;
-        const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;
-        const double dden = -1.27 * dlFc - 0.14 * du;
-        const double dx = (du * den - u * dden) / (den * den);
-        const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));
-        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;
-        const double g = dkdM * (pf - K.er[21] * pb);
-        const double dlner = (-1.0 - (1.0 * K.hRT[7] - (1.0 * K.hRT[1] + 1.0 * K.hRT[2]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[21] * pb) - K.er[21] * dlner * pb);
-        const double dq0 = 1.3 * g;
-        const double dq1 = kfM * (C2) + g;
-        const double dq2 = kfM * (C1) + g;
-        const double dq3 = g;
-        const double dq4 = 10.0 * g;
-        const double dq5 = g;
-        const double dq6 = g;
-        const double dq7 = -kfM * K.er[21] * (1.0) + g;
-        const double dq8 = g;
-        const double e_r = -1.0 * (K.hRT[1] - 1.0) + -1.0 * (K.hRT[2] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(1, 0) += -0.5 * s * dq0;
-        J(2, 0) += -15.87202380952381 * s * dq0;
-        J(7, 0) += 16.37202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(1, 1) += -1.0 * s * dq1;
-        J(2, 1) += -31.74404761904762 * s * dq1;
-        J(7, 1) += 32.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(1, 2) += -0.031501968873054564 * s * dq2;
-        J(2, 2) += -1.0 * s * dq2;
-        J(7, 2) += 1.0315019688730545 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(1, 3) += -0.06300393774610913 * s * dq3;
-        J(2, 3) += -2.0 * s * dq3;
-        J(7, 3) += 2.063003937746109 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(1, 4) += -0.055953372189841796 * s * dq4;
-        J(2, 4) += -1.7761865112406328 * s * dq4;
-        J(7, 4) += 1.8321398834304745 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(1, 5) += -0.05926971247133533 * s * dq5;
-        J(2, 5) += -1.8814605750573292 * s * dq5;
-        J(7, 5) += 1.9407302875286645 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(1, 6) += -0.029634856235667664 * s * dq6;
-        J(2, 6) += -0.9407302875286646 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(1, 7) += -0.030539901836029813 * s * dq7;
-        J(2, 7) += -0.9694600981639702 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(1, 8) += -0.03598200899550225 * s * dq8;
-        J(2, 8) += -1.1422146069822232 * s * dq8;
-        J(7, 8) += 1.1781966159777255 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(1, 9) += -1.008 * s_rho * dqT;
-        J(2, 9) += -31.998 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 4650000000.000001 * exp(0.44 * logT);
+        const double k0 = 17370000000000.006 * exp(-1.23 * logT);
+        const double lFc0 = -0.17392519729917352;
+        const double er = exp((th.gRT[7] - th.gRT[1] - th.gRT[2]) - -1.0 * log_cref);
+        {  // rate of progress: 1 H + 1 O2 <=> 1 HO2  (+M)
+            const double M = 1.3 * C0 + C1 + C2 + C3 + 10.0 * C4 + C5 + C6 + C7 + C8;
+            const double Pr = k0 * M / kf;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double x = (lPr + c) / (n - 0.14 * (lPr + c));
+            const double kfM = kf * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));
+            const double fwd = kfM * C1 * C2;
+            const double rev = kfM * er * C7;
+            const double q = fwd - rev;
+            w1 -= q;
+            w2 -= q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C1 * C2;
+            const double pb = C7;
+            const double M = 1.3 * C0 + C1 + C2 + C3 + 10.0 * C4 + C5 + C6 + C7 + C8;
+            const double Pr = k0 * M / kf;
+            const double ipr = 1.0 / (1.0 + Pr);
+            const double dlnkinf = (0.44 + 0.0 * invRT) * invT;
+            const double dlnk0 = (-1.23 + 0.0 * invRT) * invT;
+            const double lFc = lFc0;
+            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;
+            const double lPr = log10(fmax(Pr, 1e-300));
+            const double u = lPr + c, den = n - 0.14 * u;
+            const double x = u / den;
+            const double opx = 1.0 + x * x;
+            const double Fo = pow(10.0, lFc / opx);
+            const double kfM = kf * (Pr * ipr) * Fo;
+            const double dkdM = k0 * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));
+            const double dlFc = 0.0;
+            const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;
+            const double dden = -1.27 * dlFc - 0.14 * du;
+            const double dx = (du * den - u * dden) / (den * den);
+            const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));
+            const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (-1.0 - (1.0 * th.hRT[7] - (1.0 * th.hRT[1] + 1.0 * th.hRT[2]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = 1.3 * g;
+            const double dq1 = kfM * (C2) + g;
+            const double dq2 = kfM * (C1) + g;
+            const double dq3 = g;
+            const double dq4 = 10.0 * g;
+            const double dq5 = g;
+            const double dq6 = g;
+            const double dq7 = -kfM * er * (1.0) + g;
+            const double dq8 = g;
+            const double e_r = -1.0 * (th.hRT[1] - 1.0) + -1.0 * (th.hRT[2] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(1, 0) += -0.5 * s * dq0;
+            J(2, 0) += -15.87202380952381 * s * dq0;
+            J(7, 0) += 16.37202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(1, 1) += -1.0 * s * dq1;
+            J(2, 1) += -31.74404761904762 * s * dq1;
+            J(7, 1) += 32.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(1, 2) += -0.031501968873054564 * s * dq2;
+            J(2, 2) += -1.0 * s * dq2;
+            J(7, 2) += 1.0315019688730545 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(1, 3) += -0.06300393774610913 * s * dq3;
+            J(2, 3) += -2.0 * s * dq3;
+            J(7, 3) += 2.063003937746109 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(1, 4) += -0.055953372189841796 * s * dq4;
+            J(2, 4) += -1.7761865112406328 * s * dq4;
+            J(7, 4) += 1.8321398834304745 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(1, 5) += -0.05926971247133533 * s * dq5;
+            J(2, 5) += -1.8814605750573292 * s * dq5;
+            J(7, 5) += 1.9407302875286645 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(1, 6) += -0.029634856235667664 * s * dq6;
+            J(2, 6) += -0.9407302875286646 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(1, 7) += -0.030539901836029813 * s * dq7;
+            J(2, 7) += -0.9694600981639702 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(1, 8) += -0.03598200899550225 * s * dq8;
+            J(2, 8) += -1.1422146069822232 * s * dq8;
+            J(7, 8) += 1.1781966159777255 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(1, 9) += -1.008 * s_rho * dqT;
+            J(2, 9) += -31.998 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    GAS_SCHED_FENCE();
     {  // reaction 22
-        const double pf = C3 * C5;
-        const double pb = C7;
-        const double M = C0 + C1 + C2 + C3 + C4 + C5 + C6 + C7 + C8;
-        const double kfM = K.kf[22] * M;
-        const double dkdM = K.kf[22];
-        const double dlnk = (0.0 + 0.0 * invRT) * invT;
-        const double g = dkdM * (pf - K.er[22] * pb);
-        const double dlner = (-1.0 - (1.0 * K.hRT[7] - (1.0 * K.hRT[3] + 1.0 * K.hRT[5]))) * invT;
-        const double dqT = kfM * (dlnk * (pf - K.er[22] * pb) - K.er[22] * dlner * pb);
-        const double dq0 = g;
-        const double dq1 = g;
-        const double dq2 = g;
-        const double dq3 = kfM * (C5) + g;
-        const double dq4 = g;
-        const double dq5 = kfM * (C3) + g;
-        const double dq6 = g;
-        const double dq7 = -kfM * K.er[22] * (1.0) + g;
-        const double dq8 = g;
-        const double e_r = -1.0 * (K.hRT[3] - 1.0) + -1.0 * (K.hRT[5] - 1.0) + 1.0 * (K.hRT[7] - 1.0);
-        const double eT = sT * e_r;
-        sum_eT += e_r * dqT;
-        J(3, 0) += -7.936011904761905 * s * dq0;
-        J(5, 0) += -8.436011904761905 * s * dq0;
-        J(7, 0) += 16.37202380952381 * s * dq0;
-        J(9, 0) += 0.49603174603174605 * eT * dq0;
-        J(3, 1) += -15.87202380952381 * s * dq1;
-        J(5, 1) += -16.87202380952381 * s * dq1;
-        J(7, 1) += 32.74404761904762 * s * dq1;
-        J(9, 1) += 0.9920634920634921 * eT * dq1;
-        J(3, 2) += -0.5 * s * dq2;
-        J(5, 2) += -0.5315019688730546 * s * dq2;
-        J(7, 2) += 1.0315019688730545 * s * dq2;
-        J(9, 2) += 0.03125195324707794 * eT * dq2;
-        J(3, 3) += -1.0 * s * dq3;
-        J(5, 3) += -1.0630039377461091 * s * dq3;
-        J(7, 3) += 2.063003937746109 * s * dq3;
-        J(9, 3) += 0.06250390649415588 * eT * dq3;
-        J(3, 4) += -0.8880932556203164 * s * dq4;
-        J(5, 4) += -0.9440466278101582 * s * dq4;
-        J(7, 4) += 1.8321398834304745 * s * dq4;
-        J(9, 4) += 0.055509297807382736 * eT * dq4;
-        J(3, 5) += -0.9407302875286646 * s * dq5;
-        J(5, 5) += -1.0 * s * dq5;
-        J(7, 5) += 1.9407302875286645 * s * dq5;
-        J(9, 5) += 0.05879931792791203 * eT * dq5;
-        J(3, 6) += -0.4703651437643323 * s * dq6;
-        J(5, 6) += -0.5 * s * dq6;
-        J(7, 6) += 0.9703651437643322 * s * dq6;
-        J(9, 6) += 0.029399658963956014 * eT * dq6;
-        J(3, 7) += -0.4847300490819851 * s * dq7;
-        J(5, 7) += -0.515269950918015 * s * dq7;
-        J(7, 7) += 1.0 * s * dq7;
-        J(9, 7) += 0.030297521662727988 * eT * dq7;
-        J(3, 8) += -0.5711073034911116 * s * dq8;
-        J(5, 8) += -0.6070893124866139 * s * dq8;
-        J(7, 8) += 1.1781966159777255 * s * dq8;
-        J(9, 8) += 0.03569643749553795 * eT * dq8;
-        J(3, 9) += -15.999 * s_rho * dqT;
-        J(5, 9) += -17.007 * s_rho * dqT;
-        J(7, 9) += 33.006 * s_rho * dqT;
+        const double kf = 10000000000.000004;
+        const double er = exp((th.gRT[7] - th.gRT[3] - th.gRT[5]) - -1.0 * log_cref);
+        {  // rate of progress: 1 O + 1 OH <=> 1 HO2  + M
+            const double M = C0 + C1 + C2 + C3 + C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double fwd = kfM * C3 * C5;
+            const double rev = kfM * er * C7;
+            const double q = fwd - rev;
+            w3 -= q;
+            w5 -= q;
+            w7 += q;
+        }
+        {  // Jacobian terms
+            const double pf = C3 * C5;
+            const double pb = C7;
+            const double M = C0 + C1 + C2 + C3 + C4 + C5 + C6 + C7 + C8;
+            const double kfM = kf * M;
+            const double dkdM = kf;
+            const double dlnk = (0.0 + 0.0 * invRT) * invT;
+            const double g = dkdM * (pf - er * pb);
+            const double dlner = (-1.0 - (1.0 * th.hRT[7] - (1.0 * th.hRT[3] + 1.0 * th.hRT[5]))) * invT;
+            const double dqT = kfM * (dlnk * (pf - er * pb) - er * dlner * pb);
+            const double dq0 = g;
+            const double dq1 = g;
+            const double dq2 = g;
+            const double dq3 = kfM * (C5) + g;
+            const double dq4 = g;
+            const double dq5 = kfM * (C3) + g;
+            const double dq6 = g;
+            const double dq7 = -kfM * er * (1.0) + g;
+            const double dq8 = g;
+            const double e_r = -1.0 * (th.hRT[3] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
+            const double eT = sT * e_r;
+            sum_eT += e_r * dqT;
+            J(3, 0) += -7.936011904761905 * s * dq0;
+            J(5, 0) += -8.436011904761905 * s * dq0;
+            J(7, 0) += 16.37202380952381 * s * dq0;
+            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(3, 1) += -15.87202380952381 * s * dq1;
+            J(5, 1) += -16.87202380952381 * s * dq1;
+            J(7, 1) += 32.74404761904762 * s * dq1;
+            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(3, 2) += -0.5 * s * dq2;
+            J(5, 2) += -0.5315019688730546 * s * dq2;
+            J(7, 2) += 1.0315019688730545 * s * dq2;
+            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(3, 3) += -1.0 * s * dq3;
+            J(5, 3) += -1.0630039377461091 * s * dq3;
+            J(7, 3) += 2.063003937746109 * s * dq3;
+            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(3, 4) += -0.8880932556203164 * s * dq4;
+            J(5, 4) += -0.9440466278101582 * s * dq4;
+            J(7, 4) += 1.8321398834304745 * s * dq4;
+            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(3, 5) += -0.9407302875286646 * s * dq5;
+            J(5, 5) += -1.0 * s * dq5;
+            J(7, 5) += 1.9407302875286645 * s * dq5;
+            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(3, 6) += -0.4703651437643323 * s * dq6;
+            J(5, 6) += -0.5 * s * dq6;
+            J(7, 6) += 0.9703651437643322 * s * dq6;
+            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(3, 7) += -0.4847300490819851 * s * dq7;
+            J(5, 7) += -0.515269950918015 * s * dq7;
+            J(7, 7) += 1.0 * s * dq7;
+            J(9, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -0.5711073034911116 * s * dq8;
+            J(5, 8) += -0.6070893124866139 * s * dq8;
+            J(7, 8) += 1.1781966159777255 * s * dq8;
+            J(9, 8) += 0.03569643749553795 * eT * dq8;
+            J(3, 9) += -15.999 * s_rho * dqT;
+            J(5, 9) += -17.007 * s_rho * dqT;
+            J(7, 9) += 33.006 * s_rho * dqT;
+        }
     }
+    double es = 0.0;
+    F[0] = w0 * 2.016 / rho;
+    es += (th.hRT[0] - 1.0) * 8314.46261815324 * T * w0;
+    F[1] = w1 * 1.008 / rho;
+    es += (th.hRT[1] - 1.0) * 8314.46261815324 * T * w1;
+    F[2] = w2 * 31.998 / rho;
+    es += (th.hRT[2] - 1.0) * 8314.46261815324 * T * w2;
+    F[3] = w3 * 15.999 / rho;
+    es += (th.hRT[3] - 1.0) * 8314.46261815324 * T * w3;
+    F[4] = w4 * 18.015 / rho;
+    es += (th.hRT[4] - 1.0) * 8314.46261815324 * T * w4;
+    F[5] = w5 * 17.007 / rho;
+    es += (th.hRT[5] - 1.0) * 8314.46261815324 * T * w5;
+    F[6] = w6 * 34.014 / rho;
+    es += (th.hRT[6] - 1.0) * 8314.46261815324 * T * w6;
+    F[7] = w7 * 33.006 / rho;
+    es += (th.hRT[7] - 1.0) * 8314.46261815324 * T * w7;
+    F[8] = w8 * 28.014 / rho;
+    es += (th.hRT[8] - 1.0) * 8314.46261815324 * T * w8;
+    F[9] = -es / (rho * cv);
     const double sF = s * F[9] * 8314.46261815324 / cv;
-    J(9, 0) -= sF * (K.cpR[0] - 1.0) * 0.49603174603174605;
-    J(9, 1) -= sF * (K.cpR[1] - 1.0) * 0.9920634920634921;
-    J(9, 2) -= sF * (K.cpR[2] - 1.0) * 0.03125195324707794;
-    J(9, 3) -= sF * (K.cpR[3] - 1.0) * 0.06250390649415588;
-    J(9, 4) -= sF * (K.cpR[4] - 1.0) * 0.055509297807382736;
-    J(9, 5) -= sF * (K.cpR[5] - 1.0) * 0.05879931792791203;
-    J(9, 6) -= sF * (K.cpR[6] - 1.0) * 0.029399658963956014;
-    J(9, 7) -= sF * (K.cpR[7] - 1.0) * 0.030297521662727988;
-    J(9, 8) -= sF * (K.cpR[8] - 1.0) * 0.03569643749553795;
+    J(9, 0) -= sF * (th.cpR[0] - 1.0) * 0.49603174603174605;
+    J(9, 1) -= sF * (th.cpR[1] - 1.0) * 0.9920634920634921;
+    J(9, 2) -= sF * (th.cpR[2] - 1.0) * 0.03125195324707794;
+    J(9, 3) -= sF * (th.cpR[3] - 1.0) * 0.06250390649415588;
+    J(9, 4) -= sF * (th.cpR[4] - 1.0) * 0.055509297807382736;
+    J(9, 5) -= sF * (th.cpR[5] - 1.0) * 0.05879931792791203;
+    J(9, 6) -= sF * (th.cpR[6] - 1.0) * 0.029399658963956014;
+    J(9, 7) -= sF * (th.cpR[7] - 1.0) * 0.030297521662727988;
+    J(9, 8) -= sF * (th.cpR[8] - 1.0) * 0.03569643749553795;
     double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R
-    sw += (K.cpR[0] - 1.0) * F[0] * rho * 0.49603174603174605;
-    sw += (K.cpR[1] - 1.0) * F[1] * rho * 0.9920634920634921;
-    sw += (K.cpR[2] - 1.0) * F[2] * rho * 0.03125195324707794;
-    sw += (K.cpR[3] - 1.0) * F[3] * rho * 0.06250390649415588;
-    sw += (K.cpR[4] - 1.0) * F[4] * rho * 0.055509297807382736;
-    sw += (K.cpR[5] - 1.0) * F[5] * rho * 0.05879931792791203;
-    sw += (K.cpR[6] - 1.0) * F[6] * rho * 0.029399658963956014;
-    sw += (K.cpR[7] - 1.0) * F[7] * rho * 0.030297521662727988;
-    sw += (K.cpR[8] - 1.0) * F[8] * rho * 0.03569643749553795;
+    sw += (th.cpR[0] - 1.0) * F[0] * rho * 0.49603174603174605;
+    sw += (th.cpR[1] - 1.0) * F[1] * rho * 0.9920634920634921;
+    sw += (th.cpR[2] - 1.0) * F[2] * rho * 0.03125195324707794;
+    sw += (th.cpR[3] - 1.0) * F[3] * rho * 0.06250390649415588;
+    sw += (th.cpR[4] - 1.0) * F[4] * rho * 0.055509297807382736;
+    sw += (th.cpR[5] - 1.0) * F[5] * rho * 0.05879931792791203;
+    sw += (th.cpR[6] - 1.0) * F[6] * rho * 0.029399658963956014;
+    sw += (th.cpR[7] - 1.0) * F[7] * rho * 0.030297521662727988;
+    sw += (th.cpR[8] - 1.0) * F[8] * rho * 0.03569643749553795;
     if (T < 1000.0) {
         dcv += y[0] * 0.49603174603174605 * (0.00773916922 + T * (-3.77470146e-05 + T * (5.86551342e-08 + T * -2.868382652e-11)));
         dcv += y[1] * 0.9920634920634921 * (6.73824499e-07 + T * (2.23614522e-09 + T * (-1.1105763779999999e-11 + T * 8.56935288e-15)));
@@ -1788,18 +2263,17 @@ GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, 
     J(9, 9) = s * (-8314.46261815324 * (sw + T * sum_eT) / (rho * cv) - F[9] * 8314.46261815324 * dcv / cv);
 }
 
-// The integrator's kinetics policy (gas::ros2_advance_k): factors once per temperature,
-// right-hand sides from them, the Jacobian analytically.
+// The integrator's kinetics policy (gas::ros2_advance_km): thermo once per temperature,
+// the right-hand side with the analytic Jacobian at the sub-step's start, the right-hand
+// side alone at its second stage.
 struct Kinetics {
-    using K = Factors;
+    using K = Thermo;
     static constexpr bool kAnalyticJacobian = true;
-    GAS_HD void factors(double T, Factors &k) const { kin_h2_air_9::factors(T, k); }
-    GAS_HD void rhs(const Factors &k, double rho, const double *y, double *F) const {
-        rhs_k(k, rho, y, F);
-    }
+    GAS_HD void factors(double T, Thermo &k) const { thermo(T, k); }
+    GAS_HD void rhs(const Thermo &k, double rho, const double *y, double *F) const { rhs_t(k, rho, y, F); }
     template <class Mat>
-    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F, double s, Mat &J) const {
-        jac(k, rho, y, F, s, J);
+    GAS_HD void rhs_jacobian(const Thermo &k, double rho, const double *y, double *F, double s, Mat &J) const {
+        rhs_jac(k, rho, y, F, s, J);
     }
 };
 

@@ -8,11 +8,14 @@ mechanism's structure.
 
     python gen_kinetics.py data/h2_air_9.json csrc/kinetics_h2_air_9.cuh
 
-The generated `factors` + `rhs_k` compute what gas.cuh's rate_factors + reactor_rhs_k
+The generated `thermo` + `rhs_t` compute what gas.cuh's rate_factors + reactor_rhs_k
 (net_production_k, progress_one) compute, operation for operation and in the same order
 (sums over the reaction's species in the order the mechanism lists them, the quotients of
 constants that the tables path forms at run time formed here as literals with the same
 rounding), so that on a host without contraction of multiply-adds the two agree bit for bit.
+Only the species' thermo is kept per temperature: each reaction's rate constants are formed
+where the reaction is evaluated, so no per-reaction array stays live in the integrator's
+registers.  `rhs_jac` returns the same right-hand side together with the analytic Jacobian.
 Terms that are exactly zero or one are dropped (an Arrhenius exponent of 0, a third-body
 efficiency of 0, a stoichiometric factor of 1), which leaves every result unchanged.  It
 also emits `matches(mech)`, which tells whether a handle's mechanism is the one compiled
@@ -132,194 +135,323 @@ def nasa_branches(m, add, body):
         add("    }")
 
 
-def emit_jacobian(m, L, fidx):
-    """jac: the Jacobian of d(Y, T)/dt, d F_k / d Y_j and d F_k / dT, at fixed density from the
-    factors at y's temperature, differentiating rhs_k's expressions.  With q_r the rates of
-    progress, nu_kr the net coefficients and C_j = rho Y_j / W_j:
-        dF_k/dY_j = (W_k / W_j) sum_r nu_kr dq_r/dC_j,
-        dF_k/dT   = (W_k / rho) sum_r nu_kr dq_r/dT,
-        dF_T/dY_j = -(R T / (W_j c_v)) sum_r e_r dq_r/dC_j - F_T R (c_p,j/R - 1) / (W_j c_v),
-        dF_T/dT   = -R [sum_k (c_p,k/R - 1) w_k + T sum_r e_r dq_r/dT] / (rho c_v) - F_T (dc_v/dT) / c_v,
-    e_r = sum_k nu_kr (h_k/RT - 1), w_k the net production rates.  dq_r/dC_j through the
-    mass-action products, the third-body sum M and the Troe blend F(Pr), Pr = k0 M / k_inf:
-    d(k_inf Pr/(1+Pr) F)/dM = k0 F/(1+Pr) [1/(1+Pr) - 2 x lFc n / ((1+x^2)^2 (n - 0.14 u)^2)],
-    u = log10 Pr + c, x = u / (n - 0.14 u).  dq_r/dT through d ln k/dT = (b + E_a/RT)/T for
-    k_f and k_0, d ln(1/K_c)/dT = (dnu - sum_k nu_kr h_k/RT)/T (d(g_k/RT)/dT = -h_k/(R T^2),
-    d ln(p_atm/RT)/dT = -1/T), and for a fall-off reaction d ln(Pr/(1+Pr))/dT =
-    (d ln k0 - d ln k_inf)/(1+Pr) and d ln F/dT = ln 10 [dlFc/(1+x^2) - 2 x lFc dx/(1+x^2)^2]
-    with du = (d ln k0 - d ln k_inf)/ln 10 - 0.67 dlFc (dlFc = 0 where F_cent is constant).
-    Every term is accumulated straight into the scaled matrix (s J, s = -gamma h for the
-    integrator's iteration matrix)."""
-    ns, nr = m.n_species, m.n_reactions
+class Names:
+    """How the generated code names a reaction's temperature factors and a species' thermo:
+    the fused functions form k_inf, k_0, log10 F_cent and the reverse factor per reaction as
+    locals (kf, k0, lFc0, er) and read h/RT, g/RT, c_p/R from the Thermo struct `th`."""
+
+    def kf(self, r):
+        return "kf"
+
+    def er(self, r):
+        return "er"
+
+    def k0(self, i):
+        return "k0"
+
+    def lfc(self, i):
+        return "lFc0"
+
+    def hrt(self, k):
+        return f"th.hRT[{k}]"
+
+    def cpr(self, k):
+        return f"th.cpR[{k}]"
+
+    def grt(self, k):
+        return f"th.gRT[{k}]"
+
+
+def reaction_lists(m, r):
+    reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
+    prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
+    ordr = [(m.reac[r][j], m.order_reac[r][j]) for j in range(m.n_reac[r])]
+    return reac, prod, ordr
+
+
+def emit_rates(m, r, fidx, add, N):
+    """The temperature factors of reaction r as locals (gas::rate_factor_one): k_inf, for a
+    fall-off reaction k_0 and log10 F_cent, and for a reversible one the reverse factor
+    exp(dG/RT - dnu ln(p_atm / R T)); from logT, invRT, log_cref and the species' g/RT."""
+    add(f"        const double kf = {arrhenius(m.A[r], m.b[r], m.Ea[r])};")
+    if m.rtype[r] == FALLOFF:
+        add(f"        const double k0 = {arrhenius(m.A0[r], m.b0[r], m.Ea0[r])};")
+        if m.troe_n[r] >= 3 and troe_constant(m, r) is not None:
+            # every F_cent term is exactly 0 or 1 at physical temperatures (troe_terms)
+            add(f"        const double lFc0 = {troe_constant(m, r)};")
+        elif m.troe_n[r] >= 3:
+            a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
+            add(f"        double Fc0 = {lit(1.0 - a)} * exp(-T / {lit(T3)}) + {lit(a)} * exp(-T / {lit(T1)});")
+            if m.troe_n[r] == 4:
+                add(f"        Fc0 += exp({lit(-m.troe[r][3])} / T);")
+            add("        const double lFc0 = log10(fmax(Fc0, 1e-300));")
+        else:
+            add("        const double lFc0 = 0.0;")
+    if m.reversible[r]:
+        terms = [(+1, m.nu_prod[r][j], N.grt(m.prod[r][j])) for j in range(m.n_prod[r])]
+        terms += [(-1, m.nu_reac[r][j], N.grt(m.reac[r][j])) for j in range(m.n_reac[r])]
+        dnu = 0.0
+        for _, nu, _ in terms[:m.n_prod[r]]:
+            dnu += nu
+        for _, nu, _ in terms[m.n_prod[r]:]:
+            dnu -= nu
+        dG = weighted(terms)
+        if dnu == 0.0:
+            add(f"        const double er = exp({dG});")
+        else:
+            add(f"        const double er = exp(({dG}) - {lit(dnu)} * log_cref);")
+
+
+def emit_rhs_reaction(m, r, fidx, add, N, names):
+    """Reaction r's rate of progress and its contributions to the net production rates w_k
+    (gas::progress_one, net_production_k)."""
+    ns = m.n_species
+    reac, prod, ordr = reaction_lists(m, r)
+    eq = " + ".join(f"{nu:g} {names[k]}" for k, nu in reac) + (" <=> " if m.reversible[r] else " => ") + \
+        " + ".join(f"{nu:g} {names[k]}" for k, nu in prod)
+    tag = "  (+M)" if m.rtype[r] == FALLOFF else ("  + M" if m.rtype[r] == THREEBODY else "")
+    add(f"        {{  // rate of progress: {eq}{tag}")
+    if m.rtype[r] == 0:
+        add(f"            const double kfM = {N.kf(r)};")
+    else:
+        effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
+        msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
+        add(f"            const double M = {msum};")
+        if m.rtype[r] == FALLOFF:
+            i = fidx[r]
+            add(f"            const double Pr = {N.k0(i)} * M / {N.kf(r)};")
+            if m.troe_n[r] >= 3:
+                add(f"            const double lFc = {N.lfc(i)};")
+                add("            const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
+                add("            const double lPr = log10(fmax(Pr, 1e-300));")
+                add("            const double x = (lPr + c) / (n - 0.14 * (lPr + c));")
+                add(f"            const double kfM = {N.kf(r)} * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));")
+            else:
+                add(f"            const double kfM = {N.kf(r)} * (Pr / (1.0 + Pr)) * 1.0;")
+        else:
+            add(f"            const double kfM = {N.kf(r)} * M;")
+    add("            const double fwd = kfM" + "".join(f" * {conc(k, nu)}" for k, nu in ordr) + ";")
+    if m.reversible[r]:
+        add(f"            const double rev = kfM * {N.er(r)}" + "".join(f" * {conc(k, nu)}" for k, nu in prod) + ";")
+        add("            const double q = fwd - rev;")
+    else:
+        add("            const double q = fwd;")
+    for k, nu in reac:
+        add(f"            w{k} -= {'q' if nu == 1.0 else lit(nu) + ' * q'};")
+    for k, nu in prod:
+        add(f"            w{k} += {'q' if nu == 1.0 else lit(nu) + ' * q'};")
+    add("        }")
+
+
+def emit_jac_reaction(m, r, fidx, add, N):
+    """Reaction r's terms of s J (JACOBIAN_DOC)."""
+    ns = m.n_species
     W = [m.W[k] for k in range(ns)]
-    add = L.append
-    add("// s times the Jacobian of F (rhs_k) with respect to (Y, T): J(k, j) = s dF_k / dY_j for")
-    add("// j < NS and J(k, NS) = s dF_k / dT, every row k <= NS, at fixed density, from the factors")
-    add("// at y's temperature and F = rhs_k(K, rho, y).")
-    add("template <class Mat>")
-    add("GAS_HD void jac(const Factors &K, double rho, const double *y, const double *F, double s, Mat &J) {")
+    reac, prod, ordr = reaction_lists(m, r)
+    net = {}
+    for k, nu in reac:
+        net[k] = net.get(k, 0.0) - nu
+    for k, nu in prod:
+        net[k] = net.get(k, 0.0) + nu
+    net = {k: v for k, v in net.items() if v != 0.0}
+    rev = bool(m.reversible[r])
+    dlnkf = f"({lit(m.b[r])} + {lit(m.Ea[r])} * invRT) * invT"
+    ind = "            "
+    add("        {  // Jacobian terms")
+    pf = " * ".join(conc(k, nu) for k, nu in ordr)
+    pb = " * ".join(conc(k, nu) for k, nu in prod)
+    add(f"{ind}const double pf = {pf};")
+    if rev:
+        add(f"{ind}const double pb = {pb};")
+    if m.rtype[r] == 0:
+        add(f"{ind}const double kfM = {N.kf(r)};")
+        add(f"{ind}const double dlnk = {dlnkf};")
+    else:
+        effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
+        msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
+        add(f"{ind}const double M = {msum};")
+        if m.rtype[r] == FALLOFF:
+            i = fidx[r]
+            add(f"{ind}const double Pr = {N.k0(i)} * M / {N.kf(r)};")
+            add(f"{ind}const double ipr = 1.0 / (1.0 + Pr);")
+            add(f"{ind}const double dlnkinf = {dlnkf};")
+            add(f"{ind}const double dlnk0 = ({lit(m.b0[r])} + {lit(m.Ea0[r])} * invRT) * invT;")
+            if m.troe_n[r] >= 3:
+                add(f"{ind}const double lFc = {N.lfc(i)};")
+                add(f"{ind}const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
+                add(f"{ind}const double lPr = log10(fmax(Pr, 1e-300));")
+                add(f"{ind}const double u = lPr + c, den = n - 0.14 * u;")
+                add(f"{ind}const double x = u / den;")
+                add(f"{ind}const double opx = 1.0 + x * x;")
+                add(f"{ind}const double Fo = pow(10.0, lFc / opx);")
+                add(f"{ind}const double kfM = {N.kf(r)} * (Pr * ipr) * Fo;")
+                add(f"{ind}const double dkdM = {N.k0(i)} * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));")
+                # temperature derivative of F_cent (zero where it is a constant)
+                if troe_constant(m, r) is not None:
+                    add(f"{ind}const double dlFc = 0.0;")
+                else:
+                    a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
+                    terms = troe_terms(m, r)
+                    fc, dfc = [], []
+                    if terms[0][0] == "exp":
+                        add(f"{ind}const double e3 = exp(-T / {lit(T3)});")
+                        fc.append(f"{lit(1.0 - a)} * e3")
+                        dfc.append(f"-{lit((1.0 - a) / T3)} * e3")
+                    elif terms[0][0] == "one":
+                        fc.append(lit(1.0 - a))
+                    if terms[1][0] == "exp":
+                        add(f"{ind}const double e1 = exp(-T / {lit(T1)});")
+                        fc.append(f"{lit(a)} * e1")
+                        dfc.append(f"-{lit(a / T1)} * e1")
+                    elif terms[1][0] == "one":
+                        fc.append(lit(a))
+                    if len(terms) == 3:
+                        T2 = m.troe[r][3]
+                        if terms[2][0] == "exp":
+                            add(f"{ind}const double e2 = exp({lit(-T2)} / T);")
+                            fc.append("e2")
+                            dfc.append(f"{lit(T2)} * invT * invT * e2")
+                        elif terms[2][0] == "one":
+                            fc.append("1.0")
+                    add(f"{ind}const double Fc = fmax({' + '.join(fc) or '0.0'}, 1e-300);")
+                    add(f"{ind}const double dlFc = ({' + '.join(dfc) or '0.0'}) / (Fc * 2.302585092994046);")
+                add(f"{ind}const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;")
+                add(f"{ind}const double dden = -1.27 * dlFc - 0.14 * du;")
+                add(f"{ind}const double dx = (du * den - u * dden) / (den * den);")
+                add(f"{ind}const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));")
+                add(f"{ind}const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;")
+            else:
+                add(f"{ind}const double kfM = {N.kf(r)} * (Pr * ipr);")
+                add(f"{ind}const double dkdM = {N.k0(i)} * ipr * ipr;")
+                add(f"{ind}const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr;")
+        else:
+            add(f"{ind}const double kfM = {N.kf(r)} * M;")
+            add(f"{ind}const double dkdM = {N.kf(r)};")
+            add(f"{ind}const double dlnk = {dlnkf};")
+    if m.rtype[r] != 0:
+        if rev:
+            add(f"{ind}const double g = dkdM * (pf - {N.er(r)} * pb);")
+        else:
+            add(f"{ind}const double g = dkdM * pf;")
+    # d q / dT at fixed concentrations
+    if rev:
+        dnu = sum(nu for _, nu in prod) - sum(nu for _, nu in reac)
+        dh = " + ".join([f"{lit(nu)} * {N.hrt(k)}" for k, nu in prod]) + " - (" + \
+            " + ".join([f"{lit(nu)} * {N.hrt(k)}" for k, nu in reac]) + ")"
+        add(f"{ind}const double dlner = ({lit(dnu)} - ({dh})) * invT;")
+        add(f"{ind}const double dqT = kfM * (dlnk * (pf - {N.er(r)} * pb) - {N.er(r)} * dlner * pb);")
+    else:
+        add(f"{ind}const double dqT = kfM * dlnk * pf;")
+    dq = {}
+    for idx, (k, nu) in enumerate(ordr):
+        others = [x for jdx, x in enumerate(ordr) if jdx != idx]
+        dq.setdefault(k, []).append(("+", dpow(k, nu, others)))
+    if rev:
+        for idx, (k, nu) in enumerate(prod):
+            others = [x for jdx, x in enumerate(prod) if jdx != idx]
+            dq.setdefault(k, []).append(("-", dpow(k, nu, others)))
+    effs = {k: m.eff[r][k] for k in range(ns) if m.rtype[r] != 0 and m.eff[r][k] != 0.0}
+    cols = sorted(set(dq) | set(effs))
+    for j in cols:
+        parts = []
+        for sign, e in dq.get(j, []):
+            if sign == "+":
+                parts.append(f"+ kfM * ({e})")
+            else:
+                parts.append(f"- kfM * {N.er(r)} * ({e})")
+        if j in effs:
+            e = effs[j]
+            parts.append("+ g" if e == 1.0 else f"+ {lit(e)} * g")
+        expr = " ".join(parts)
+        expr = expr[2:] if expr.startswith("+ ") else "-" + expr[2:]
+        add(f"{ind}const double dq{j} = {expr};")
+    er_terms = " + ".join(f"{lit(v)} * ({N.hrt(k)} - 1.0)" for k, v in net.items()) or "0.0"
+    add(f"{ind}const double e_r = {er_terms};")
+    add(f"{ind}const double eT = sT * e_r;")
+    add(f"{ind}sum_eT += e_r * dqT;")
+    for j in cols:
+        for k, v in net.items():
+            add(f"{ind}J({k}, {j}) += {lit(v * W[k] / W[j])} * s * dq{j};")
+        add(f"{ind}J({ns}, {j}) += {lit(1.0 / W[j])} * eT * dq{j};")
+    for k, v in net.items():
+        add(f"{ind}J({k}, {ns}) += {lit(v * W[k])} * s_rho * dqT;")
+    add("        }")
+
+
+JACOBIAN_DOC = """
+The Jacobian of d(Y, T)/dt at fixed density, d F_k / d Y_j and d F_k / dT, differentiating the
+right-hand side's expressions.  With q_r the rates of progress, nu_kr the net coefficients and
+C_j = rho Y_j / W_j:
+    dF_k/dY_j = (W_k / W_j) sum_r nu_kr dq_r/dC_j,
+    dF_k/dT   = (W_k / rho) sum_r nu_kr dq_r/dT,
+    dF_T/dY_j = -(R T / (W_j c_v)) sum_r e_r dq_r/dC_j - F_T R (c_p,j/R - 1) / (W_j c_v),
+    dF_T/dT   = -R [sum_k (c_p,k/R - 1) w_k + T sum_r e_r dq_r/dT] / (rho c_v) - F_T (dc_v/dT) / c_v,
+e_r = sum_k nu_kr (h_k/RT - 1), w_k the net production rates.  dq_r/dC_j through the
+mass-action products, the third-body sum M and the Troe blend F(Pr), Pr = k0 M / k_inf:
+d(k_inf Pr/(1+Pr) F)/dM = k0 F/(1+Pr) [1/(1+Pr) - 2 x lFc n / ((1+x^2)^2 (n - 0.14 u)^2)],
+u = log10 Pr + c, x = u / (n - 0.14 u).  dq_r/dT through d ln k/dT = (b + E_a/RT)/T for
+k_f and k_0, d ln(1/K_c)/dT = (dnu - sum_k nu_kr h_k/RT)/T (d(g_k/RT)/dT = -h_k/(R T^2),
+d ln(p_atm/RT)/dT = -1/T), and for a fall-off reaction d ln(Pr/(1+Pr))/dT =
+(d ln k0 - d ln k_inf)/(1+Pr) and d ln F/dT = ln 10 [dlFc/(1+x^2) - 2 x lFc dx/(1+x^2)^2]
+with du = (d ln k0 - d ln k_inf)/ln 10 - 0.67 dlFc (dlFc = 0 where F_cent is constant).
+Every term is accumulated straight into the scaled matrix (s J, s = -gamma h for the
+integrator's iteration matrix).
+"""
+
+
+def emit_prologue(m, add, with_jac):
+    """The locals every fused function starts from: T, the thermo scalars, the
+    concentrations, the net production accumulators; for the Jacobian also c_v and the T
+    row's scales, and the matrix cleared."""
+    ns = m.n_species
     add(f"    const double T = y[{ns}];")
-    add(f"    const double invT = 1.0 / T, invRT = 1.0 / ({lit(KR)} * T);")
+    add("    const double logT = th.logT, invRT = th.invRT, log_cref = th.log_cref;")
+    add("    (void)logT;")
+    add("    (void)log_cref;")
     for k in range(ns):
         add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
+    for k in range(ns):
+        add(f"    double w{k} = 0.0;")
     add("    double cv = 0.0;")
     for k in range(ns):
-        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
+        add(f"    cv += y[{k}] * (th.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
     add(f"    cv *= {lit(KR)};")
-    add(f"    const double sT = -s * {lit(KR)} * T / cv;  // times e_r dq_rj / W_j: the T row")
-    add("    const double s_rho = s / rho;")
-    add("    double sum_eT = 0.0;  // sum_r e_r dq_r/dT")
-    add("#pragma unroll")
-    add(f"    for (int k = 0; k <= {ns}; ++k)")
-    add("#pragma unroll")
-    add(f"        for (int j = 0; j <= {ns}; ++j) J(k, j) = 0.0;")
-    for r in range(nr):
-        reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
-        prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
-        ordr = [(m.reac[r][j], m.order_reac[r][j]) for j in range(m.n_reac[r])]
-        net = {}
-        for k, nu in reac:
-            net[k] = net.get(k, 0.0) - nu
-        for k, nu in prod:
-            net[k] = net.get(k, 0.0) + nu
-        net = {k: v for k, v in net.items() if v != 0.0}
-        rev = bool(m.reversible[r])
-        dlnkf = f"({lit(m.b[r])} + {lit(m.Ea[r])} * invRT) * invT"
-        add(f"    {{  // reaction {r}")
-        pf = " * ".join(conc(k, nu) for k, nu in ordr)
-        pb = " * ".join(conc(k, nu) for k, nu in prod)
-        add(f"        const double pf = {pf};")
-        if rev:
-            add(f"        const double pb = {pb};")
-        if m.rtype[r] == 0:
-            add(f"        const double kfM = K.kf[{r}];")
-            add(f"        const double dlnk = {dlnkf};")
-        else:
-            effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
-            msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
-            add(f"        const double M = {msum};")
-            if m.rtype[r] == FALLOFF:
-                i = fidx[r]
-                add(f"        const double Pr = K.k0[{i}] * M / K.kf[{r}];")
-                add("        const double ipr = 1.0 / (1.0 + Pr);")
-                add(f"        const double dlnkinf = {dlnkf};")
-                add(f"        const double dlnk0 = ({lit(m.b0[r])} + {lit(m.Ea0[r])} * invRT) * invT;")
-                if m.troe_n[r] >= 3:
-                    add(f"        const double lFc = K.lFc[{i}];")
-                    add("        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
-                    add("        const double lPr = log10(fmax(Pr, 1e-300));")
-                    add("        const double u = lPr + c, den = n - 0.14 * u;")
-                    add("        const double x = u / den;")
-                    add("        const double opx = 1.0 + x * x;")
-                    add("        const double Fo = pow(10.0, lFc / opx);")
-                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr) * Fo;")
-                    add(f"        const double dkdM = K.k0[{i}] * Fo * ipr * (ipr - 2.0 * x * lFc * n / (opx * opx * den * den));")
-                    # temperature derivative of F_cent (zero where it is a constant)
-                    if troe_constant(m, r) is not None:
-                        add("        const double dlFc = 0.0;")
-                    else:
-                        a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
-                        terms = troe_terms(m, r)
-                        fc, dfc = [], []
-                        if terms[0][0] == "exp":
-                            add(f"        const double e3 = exp(-T / {lit(T3)});")
-                            fc.append(f"{lit(1.0 - a)} * e3")
-                            dfc.append(f"-{lit((1.0 - a) / T3)} * e3")
-                        elif terms[0][0] == "one":
-                            fc.append(lit(1.0 - a))
-                        if terms[1][0] == "exp":
-                            add(f"        const double e1 = exp(-T / {lit(T1)});")
-                            fc.append(f"{lit(a)} * e1")
-                            dfc.append(f"-{lit(a / T1)} * e1")
-                        elif terms[1][0] == "one":
-                            fc.append(lit(a))
-                        if len(terms) == 3:
-                            T2 = m.troe[r][3]
-                            if terms[2][0] == "exp":
-                                add(f"        const double e2 = exp({lit(-T2)} / T);")
-                                fc.append("e2")
-                                dfc.append(f"{lit(T2)} * invT * invT * e2")
-                            elif terms[2][0] == "one":
-                                fc.append("1.0")
-                        add(f"        const double Fc = fmax({' + '.join(fc) or '0.0'}, 1e-300);")
-                        add(f"        const double dlFc = ({' + '.join(dfc) or '0.0'}) / (Fc * 2.302585092994046);")
-                    add("        const double du = (dlnk0 - dlnkinf) * 0.4342944819032518 - 0.67 * dlFc;")
-                    add("        const double dden = -1.27 * dlFc - 0.14 * du;")
-                    add("        const double dx = (du * den - u * dden) / (den * den);")
-                    add("        const double dlnFo = 2.302585092994046 * (dlFc / opx - 2.0 * x * lFc * dx / (opx * opx));")
-                    add("        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr + dlnFo;")
-                else:
-                    add(f"        const double kfM = K.kf[{r}] * (Pr * ipr);")
-                    add(f"        const double dkdM = K.k0[{i}] * ipr * ipr;")
-                    add("        const double dlnk = dlnkinf + (dlnk0 - dlnkinf) * ipr;")
-            else:
-                add(f"        const double kfM = K.kf[{r}] * M;")
-                add(f"        const double dkdM = K.kf[{r}];")
-                add(f"        const double dlnk = {dlnkf};")
-        if m.rtype[r] != 0:
-            if rev:
-                add(f"        const double g = dkdM * (pf - K.er[{r}] * pb);")
-            else:
-                add("        const double g = dkdM * pf;")
-        # d q / dT at fixed concentrations
-        if rev:
-            dnu = sum(nu for _, nu in prod) - sum(nu for _, nu in reac)
-            dh = " + ".join([f"{lit(nu)} * K.hRT[{k}]" for k, nu in prod]) + " - (" + \
-                " + ".join([f"{lit(nu)} * K.hRT[{k}]" for k, nu in reac]) + ")"
-            add(f"        const double dlner = ({lit(dnu)} - ({dh})) * invT;")
-            add(f"        const double dqT = kfM * (dlnk * (pf - K.er[{r}] * pb) - K.er[{r}] * dlner * pb);")
-        else:
-            add("        const double dqT = kfM * dlnk * pf;")
-        dq = {}
-        for idx, (k, nu) in enumerate(ordr):
-            others = [x for jdx, x in enumerate(ordr) if jdx != idx]
-            dq.setdefault(k, []).append(("+", dpow(k, nu, others)))
-        if rev:
-            for idx, (k, nu) in enumerate(prod):
-                others = [x for jdx, x in enumerate(prod) if jdx != idx]
-                dq.setdefault(k, []).append(("-", dpow(k, nu, others)))
-        effs = {k: m.eff[r][k] for k in range(ns) if m.rtype[r] != 0 and m.eff[r][k] != 0.0}
-        cols = sorted(set(dq) | set(effs))
-        for j in cols:
-            parts = []
-            for sign, e in dq.get(j, []):
-                if sign == "+":
-                    parts.append(f"+ kfM * ({e})")
-                else:
-                    parts.append(f"- kfM * K.er[{r}] * ({e})")
-            if j in effs:
-                e = effs[j]
-                parts.append("+ g" if e == 1.0 else f"+ {lit(e)} * g")
-            expr = " ".join(parts)
-            expr = expr[2:] if expr.startswith("+ ") else "-" + expr[2:]
-            add(f"        const double dq{j} = {expr};")
-        er_terms = " + ".join(f"{lit(v)} * (K.hRT[{k}] - 1.0)" for k, v in net.items()) or "0.0"
-        add(f"        const double e_r = {er_terms};")
-        add("        const double eT = sT * e_r;")
-        add("        sum_eT += e_r * dqT;")
-        for j in cols:
-            for k, v in net.items():
-                add(f"        J({k}, {j}) += {lit(v * W[k] / W[j])} * s * dq{j};")
-            add(f"        J({ns}, {j}) += {lit(1.0 / W[j])} * eT * dq{j};")
-        for k, v in net.items():
-            add(f"        J({k}, {ns}) += {lit(v * W[k])} * s_rho * dqT;")
-        add("    }")
-    # the T row's composition columns: the c_v term
+    if with_jac:
+        add("    const double invT = 1.0 / T;")
+        add(f"    const double sT = -s * {lit(KR)} * T / cv;  // times e_r dq_rj / W_j: the T row")
+        add("    const double s_rho = s / rho;")
+        add("    double sum_eT = 0.0;  // sum_r e_r dq_r/dT")
+        add("#pragma unroll")
+        add(f"    for (int k = 0; k <= {ns}; ++k)")
+        add("#pragma unroll")
+        add(f"        for (int j = 0; j <= {ns}; ++j) J(k, j) = 0.0;")
+
+
+def emit_rhs_epilogue(m, add):
+    """F from the net production rates (gas::reactor_rhs_k)."""
+    ns = m.n_species
+    add("    double es = 0.0;")
+    for k in range(ns):
+        add(f"    F[{k}] = w{k} * {lit(m.W[k])} / rho;")
+        add(f"    es += (th.hRT[{k}] - 1.0) * {lit(KR)} * T * w{k};")
+    add(f"    F[{ns}] = -es / (rho * cv);")
+
+
+def emit_jac_epilogue(m, add):
+    """The T row's composition columns (the c_v term) and its T column."""
+    ns = m.n_species
     add(f"    const double sF = s * F[{ns}] * {lit(KR)} / cv;")
     for j in range(ns):
-        add(f"    J({ns}, {j}) -= sF * (K.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
-    # the T row's T column
+        add(f"    J({ns}, {j}) -= sF * (th.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
     add("    double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R")
     for k in range(ns):
-        add(f"    sw += (K.cpR[{k}] - 1.0) * F[{k}] * rho * {lit(1.0 / m.W[k])};")
+        add(f"    sw += (th.cpR[{k}] - 1.0) * F[{k}] * rho * {lit(1.0 / m.W[k])};")
 
     def dcp(k, a):
         add(f"        dcv += y[{k}] * {lit(1.0 / m.W[k])} * ({lit(a[1])} + T * ({lit(2 * a[2])} + T * ({lit(3 * a[3])} + "
             f"T * {lit(4 * a[4])})));")
     nasa_branches(m, add, dcp)
     add(f"    J({ns}, {ns}) = s * (-{lit(KR)} * (sw + T * sum_eT) / (rho * cv) - F[{ns}] * {lit(KR)} * dcv / cv);")
-    add("}")
-    add("")
 
 
 def generate(m, name):
@@ -330,8 +462,8 @@ def generate(m, name):
     L = []
     add = L.append
     add(f"// Generated by gen_kinetics.py from the mechanism {name} -- do not edit; `make` regenerates it.")
-    add("// Its kinetics as straight-line code: gas.cuh's rate_factors (factors) and reactor_rhs_k")
-    add("// (rhs_k) with the mechanism's constants inlined.")
+    add("// Its kinetics as straight-line code: gas.cuh's rate_factors and reactor_rhs_k (thermo, rhs_t)")
+    add("// and their analytic Jacobian (rhs_jac) with the mechanism's constants inlined.")
     add("#pragma once")
     add("#include <math.h>")
     add('#include "gas.cuh"')
@@ -371,142 +503,78 @@ def generate(m, name):
     add("    return true;")
     add("}")
     add("")
-    # ---- temperature factors
-    add("// The temperature-only factors (gas::RateT): k_inf (k for non-fall-off reactions), the")
-    add("// fall-off k_0 and log10 F_cent, the reverse factors exp(dG/RT - dnu ln(p_atm / R T)) and")
-    add("// the species' h/RT and c_p/R.")
-    add("struct Factors {")
-    add("    double kf[NR], er[NR], k0[NF], lFc[NF], hRT[NS], cpR[NS];")
+    # ---- per-temperature thermo
+    add("// The species' thermo at one temperature (NASA-7): h/RT, g/RT and c_p/R, with ln T, 1/RT and")
+    add("// ln(p_atm / R T); the rate constants are formed from them reaction by reaction where they")
+    add("// are used (rhs_t, rhs_jac), so that no per-reaction array stays live across the kinetics.")
+    add("struct Thermo {")
+    add("    double hRT[NS], gRT[NS], cpR[NS], logT, invRT, log_cref;")
     add("};")
     add("")
-    add("GAS_HD void factors(double T, Factors &K) {")
-    add("    const double logT = log(T), invRT = 1.0 / (8314.46261815324 * T);")
-    add(f"    const double log_cref = log({lit(ONE_ATM)} / ({lit(KR)} * T));")
-    add(f"    double gRT[{ns}];")
-    # one branch per distinct switch temperature
-    groups = {}
-    for k in range(ns):
-        groups.setdefault(m.T_mid[k], []).append(k)
-    for Tm, ks in groups.items():
-        add(f"    if (T < {lit(Tm)}) {{")
-        for branch in ("lo", "hi"):
-            if branch == "hi":
-                add("    } else {")
-            for k in ks:
-                a = m.nasa_lo[k] if branch == "lo" else m.nasa_hi[k]
-                add(f"        K.cpR[{k}] = {lit(a[0])} + T * ({lit(a[1])} + T * ({lit(a[2])} + T * ({lit(a[3])} + T * "
-                    f"{lit(a[4])})));")
-                # h_RT: a1/2 + T (a2/3 + T (a3/4 + T a4 / 5)) + a5 / T
-                add(f"        K.hRT[{k}] = {lit(a[0])} + T * ({lit(a[1] / 2)} + T * ({lit(a[2] / 3)} + T * "
-                    f"({lit(a[3] / 4)} + T * {lit(a[4])} / 5.0))) + {lit(a[5])} / T;")
-                # s_R: a0 ln T + T (a1 + T (a2/2 + T (a3/3 + T a4 / 4))) + a6 (the quarter is exact)
-                add(f"        gRT[{k}] = K.hRT[{k}] - ({lit(a[0])} * logT + T * ({lit(a[1])} + T * ({lit(a[2] / 2)} + T * "
-                    f"({lit(a[3] / 3)} + T * {lit(a[4] / 4)}))) + {lit(a[6])});")
-        add("    }")
-    for r in range(nr):
-        add(f"    K.kf[{r}] = {arrhenius(m.A[r], m.b[r], m.Ea[r])};")
-        if m.rtype[r] == FALLOFF:
-            i = fidx[r]
-            add(f"    K.k0[{i}] = {arrhenius(m.A0[r], m.b0[r], m.Ea0[r])};")
-            if m.troe_n[r] >= 3 and troe_constant(m, r) is not None:
-                # every F_cent term is exactly 0 or 1 at physical temperatures (troe_terms)
-                add(f"    K.lFc[{i}] = {troe_constant(m, r)};")
-            elif m.troe_n[r] >= 3:
-                a, T3, T1 = m.troe[r][0], m.troe[r][1], m.troe[r][2]
-                add("    {")
-                add(f"        double Fc = {lit(1.0 - a)} * exp(-T / {lit(T3)}) + {lit(a)} * exp(-T / {lit(T1)});")
-                if m.troe_n[r] == 4:
-                    add(f"        Fc += exp({lit(-m.troe[r][3])} / T);")
-                add(f"        K.lFc[{i}] = log10(fmax(Fc, 1e-300));")
-                add("    }")
-            else:
-                add(f"    K.lFc[{i}] = 0.0;")
-        if m.reversible[r]:
-            terms = [(+1, m.nu_prod[r][j], f"gRT[{m.prod[r][j]}]") for j in range(m.n_prod[r])]
-            terms += [(-1, m.nu_reac[r][j], f"gRT[{m.reac[r][j]}]") for j in range(m.n_reac[r])]
-            dnu = 0.0
-            for _, nu, _ in terms[:m.n_prod[r]]:
-                dnu += nu
-            for _, nu, _ in terms[m.n_prod[r]:]:
-                dnu -= nu
-            dG = weighted(terms)
-            if dnu == 0.0:
-                add(f"    K.er[{r}] = exp({dG});")
-            else:
-                add(f"    K.er[{r}] = exp(({dG}) - {lit(dnu)} * log_cref);")
-        else:
-            add(f"    K.er[{r}] = 0.0;")
+    add("GAS_HD void thermo(double T, Thermo &th) {")
+    add("    const double logT = log(T);")
+    add("    th.logT = logT;")
+    add(f"    th.invRT = 1.0 / ({lit(KR)} * T);")
+    add(f"    th.log_cref = log({lit(ONE_ATM)} / ({lit(KR)} * T));")
+
+    def nasa(k, a):
+        add(f"        th.cpR[{k}] = {lit(a[0])} + T * ({lit(a[1])} + T * ({lit(a[2])} + T * ({lit(a[3])} + T * "
+            f"{lit(a[4])})));")
+        # h_RT: a1/2 + T (a2/3 + T (a3/4 + T a4 / 5)) + a5 / T
+        add(f"        th.hRT[{k}] = {lit(a[0])} + T * ({lit(a[1] / 2)} + T * ({lit(a[2] / 3)} + T * "
+            f"({lit(a[3] / 4)} + T * {lit(a[4])} / 5.0))) + {lit(a[5])} / T;")
+        # s_R: a0 ln T + T (a1 + T (a2/2 + T (a3/3 + T a4 / 4))) + a6 (the quarter is exact)
+        add(f"        th.gRT[{k}] = th.hRT[{k}] - ({lit(a[0])} * logT + T * ({lit(a[1])} + T * ({lit(a[2] / 2)} + T * "
+            f"({lit(a[3] / 3)} + T * {lit(a[4] / 4)}))) + {lit(a[6])});")
+    nasa_branches(m, add, nasa)
     add("}")
     add("")
-    # ---- right-hand side from the factors
-    add("// F = d(Y_0..Y_{NS-1}, T)/dt at density rho [kg/m^3] and state y, from the factors K at")
-    add("// y's temperature (gas::reactor_rhs_k).")
-    add("GAS_HD void rhs_k(const Factors &K, double rho, const double *y, double *F) {")
-    add(f"    const double T = y[{ns}];")
-    for k in range(ns):
-        add(f"    const double C{k} = rho * y[{k}] * {lit(1.0 / m.W[k])};")
-    for k in range(ns):
-        add(f"    double w{k} = 0.0;")
+    N = Names()
+    # ---- right-hand side
+    add("// F = d(Y_0..Y_{NS-1}, T)/dt at density rho [kg/m^3] and state y, from the thermo th at")
+    add("// y's temperature (gas::rate_factors + gas::reactor_rhs_k, reaction by reaction).")
+    add("GAS_HD void rhs_t(const Thermo &th, double rho, const double *y, double *F) {")
+    emit_prologue(m, add, with_jac=False)
     for r in range(nr):
-        reac = [(m.reac[r][j], m.nu_reac[r][j]) for j in range(m.n_reac[r])]
-        prod = [(m.prod[r][j], m.nu_prod[r][j]) for j in range(m.n_prod[r])]
-        ordr = [(m.reac[r][j], m.order_reac[r][j]) for j in range(m.n_reac[r])]
-        eq = " + ".join(f"{nu:g} {names[k]}" for k, nu in reac) + (" <=> " if m.reversible[r] else " => ") + \
-            " + ".join(f"{nu:g} {names[k]}" for k, nu in prod)
-        tag = "  (+M)" if m.rtype[r] == FALLOFF else ("  + M" if m.rtype[r] == THREEBODY else "")
-        add(f"    {{  // {r}: {eq}{tag}")
-        if m.rtype[r] == 0:
-            add(f"        const double kfM = K.kf[{r}];")
-        else:
-            effs = [(k, m.eff[r][k]) for k in range(ns) if m.eff[r][k] != 0.0]
-            msum = " + ".join((f"C{k}" if e == 1.0 else f"{lit(e)} * C{k}") for k, e in effs) or "0.0"
-            add(f"        const double M = {msum};")
-            if m.rtype[r] == FALLOFF:
-                i = fidx[r]
-                add(f"        const double Pr = K.k0[{i}] * M / K.kf[{r}];")
-                if m.troe_n[r] >= 3:
-                    add(f"        const double lFc = K.lFc[{i}];")
-                    add("        const double c = -0.4 - 0.67 * lFc, n = 0.75 - 1.27 * lFc;")
-                    add("        const double lPr = log10(fmax(Pr, 1e-300));")
-                    add("        const double x = (lPr + c) / (n - 0.14 * (lPr + c));")
-                    add(f"        const double kfM = K.kf[{r}] * (Pr / (1.0 + Pr)) * pow(10.0, lFc / (1.0 + x * x));")
-                else:
-                    add(f"        const double kfM = K.kf[{r}] * (Pr / (1.0 + Pr)) * 1.0;")
-            else:
-                add(f"        const double kfM = K.kf[{r}] * M;")
-        add("        const double fwd = kfM" + "".join(f" * {conc(k, nu)}" for k, nu in ordr) + ";")
-        if m.reversible[r]:
-            add(f"        const double rev = kfM * K.er[{r}]" + "".join(f" * {conc(k, nu)}" for k, nu in prod) + ";")
-            add("        const double q = fwd - rev;")
-        else:
-            add("        const double q = fwd;")
-        for k, nu in reac:
-            add(f"        w{k} -= {'q' if nu == 1.0 else lit(nu) + ' * q'};")
-        for k, nu in prod:
-            add(f"        w{k} += {'q' if nu == 1.0 else lit(nu) + ' * q'};")
+        add("    GAS_SCHED_FENCE();")
+        add(f"    {{  // reaction {r}")
+        emit_rates(m, r, fidx, add, N)
+        emit_rhs_reaction(m, r, fidx, add, N, names)
         add("    }")
-    add("    double cv = 0.0, s = 0.0;")
-    for k in range(ns):
-        add(f"    F[{k}] = w{k} * {lit(m.W[k])} / rho;")
-        add(f"    cv += y[{k}] * (K.cpR[{k}] - 1.0) * {lit(1.0 / m.W[k])};")
-        add(f"    s += (K.hRT[{k}] - 1.0) * {lit(KR)} * T * w{k};")
-    add(f"    cv *= {lit(KR)};")
-    add(f"    F[{ns}] = -s / (rho * cv);")
+    emit_rhs_epilogue(m, add)
     add("}")
     add("")
-    emit_jacobian(m, L, fidx)
-    add("// The integrator's kinetics policy (gas::ros2_advance_k): factors once per temperature,")
-    add("// right-hand sides from them, the Jacobian analytically.")
+    # ---- right-hand side and Jacobian together
+    add("// rhs_t, and s times the Jacobian of F with respect to (Y, T) at fixed density: J(k, j) =")
+    add("// s dF_k / dY_j for j < NS and J(k, NS) = s dF_k / dT, every row k <= NS.  Each reaction's")
+    add("// rate constants are formed once and serve both.")
+    for line in JACOBIAN_DOC.strip().split("\n"):
+        add("// " + line if line else "//")
+    add("template <class Mat>")
+    add("GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, double s, Mat &J) {")
+    emit_prologue(m, add, with_jac=True)
+    for r in range(nr):
+        add("    GAS_SCHED_FENCE();")
+        add(f"    {{  // reaction {r}")
+        emit_rates(m, r, fidx, add, N)
+        emit_rhs_reaction(m, r, fidx, add, N, names)
+        emit_jac_reaction(m, r, fidx, add, N)
+        add("    }")
+    emit_rhs_epilogue(m, add)
+    emit_jac_epilogue(m, add)
+    add("}")
+    add("")
+    add("// The integrator's kinetics policy (gas::ros2_advance_km): thermo once per temperature,")
+    add("// the right-hand side with the analytic Jacobian at the sub-step's start, the right-hand")
+    add("// side alone at its second stage.")
     add("struct Kinetics {")
-    add("    using K = Factors;")
+    add("    using K = Thermo;")
     add("    static constexpr bool kAnalyticJacobian = true;")
-    add("    GAS_HD void factors(double T, Factors &k) const { kin_" + name + "::factors(T, k); }")
-    add("    GAS_HD void rhs(const Factors &k, double rho, const double *y, double *F) const {")
-    add("        rhs_k(k, rho, y, F);")
-    add("    }")
+    add("    GAS_HD void factors(double T, Thermo &k) const { thermo(T, k); }")
+    add("    GAS_HD void rhs(const Thermo &k, double rho, const double *y, double *F) const { rhs_t(k, rho, y, F); }")
     add("    template <class Mat>")
-    add("    GAS_HD void jacobian(const Factors &k, double rho, const double *y, const double *F, double s, Mat &J) const {")
-    add("        jac(k, rho, y, F, s, J);")
+    add("    GAS_HD void rhs_jacobian(const Thermo &k, double rho, const double *y, double *F, double s, Mat &J) const {")
+    add("        rhs_jac(k, rho, y, F, s, J);")
     add("    }")
     add("};")
     add("")

@@ -28,9 +28,9 @@ void kh_rhs_dense(const void *t, double rho, const double *y, double *F) {
     gas::reactor_rhs_dense<K9::NS>(*(const gas::Tables *)t, rho, y, F);
 }
 void kh_rhs_compiled(double rho, const double *y, double *F) {
-    K9::Factors K;
-    K9::factors(y[K9::NS], K);
-    K9::rhs_k(K, rho, y, F);
+    K9::Thermo th;
+    K9::thermo(y[K9::NS], th);
+    K9::rhs_t(th, rho, y, F);
 }
 
 // one ROS2 advance over dt: the host integrator over the tables (ros2_advance), and the
@@ -47,14 +47,13 @@ int kh_ros2_compiled(double rho, double *Y, double *T, double dt) {
 }
 
 extern "C" {
-// the compiled kinetics' analytic Jacobian d(Y, T)/dt / d(Y, T) (row-major 10 x 10)
-void kh_jac_compiled(double rho, const double *y, double *J) {
-    K9::Factors K;
-    K9::factors(y[K9::NS], K);
-    double F[K9::NS + 1];
-    K9::rhs_k(K, rho, y, F);
+// the compiled kinetics' analytic Jacobian d(Y, T)/dt / d(Y, T) (row-major 10 x 10) and the
+// right-hand side rhs_jac returns with it
+void kh_jac_compiled(double rho, const double *y, double *J, double *F) {
+    K9::Thermo th;
+    K9::thermo(y[K9::NS], th);
     gas::RegMat<K9::NS + 1> Jm;
-    K9::jac(K, rho, y, F, 1.0, Jm);
+    K9::rhs_jac(th, rho, y, F, 1.0, Jm);
     for (int r = 0; r <= K9::NS; ++r)
         for (int c = 0; c <= K9::NS; ++c) J[r * (K9::NS + 1) + c] = Jm(r, c);
 }

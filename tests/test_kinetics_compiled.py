@@ -54,7 +54,7 @@ def kh(tmp_path_factory):
     for f in ("kh_ros2_tables", "kh_ros2_dense"):
         getattr(L, f).argtypes = [vp, D, DP, DP, D]
     L.kh_ros2_compiled.argtypes = [D, DP, DP, D]
-    L.kh_jac_compiled.argtypes = [D, DP, DP]
+    L.kh_jac_compiled.argtypes = [D, DP, DP, DP]
     return L
 
 
@@ -143,7 +143,12 @@ def test_analytic_jacobian_matches_finite_differences(kh):
     try:
         for rho, y in states(m, 120, seed=3):
             J = np.zeros((10, 10))
-            kh.kh_jac_compiled(rho, p(y), p(J))
+            Fj = np.zeros(10)
+            Ft = np.zeros(10)
+            kh.kh_jac_compiled(rho, p(y), p(J), p(Fj))
+            # the right-hand side formed with the Jacobian is the tables' one, bit for bit
+            kh.kh_rhs_tables(t, rho, p(y), p(Ft))
+            assert np.array_equal(Fj, Ft), (y, Fj - Ft)
             scale = np.abs(J).max(axis=1) + 1e-300
             for j in range(10):
                 def F(d):
