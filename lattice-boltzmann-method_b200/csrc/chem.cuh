@@ -360,6 +360,23 @@ struct CachedTableKinetics {
     GAS_HD void rhs(const RateT &k, double rho, const double *y, double *F) const { reactor_rhs_k(t, k, rho, y, F); }
 };
 
+// The unknowns of ros2_advance_km's iteration system: every component of (Y_0..Y_{NS-1}, T),
+// unless the kinetics policy names fewer (kSys, and sys_full(i) the state component of unknown
+// i, ascending, T last).  A species whose net stoichiometric coefficient is zero in every
+// reaction (N2 in the H2/air mechanism) has a zero right-hand side and a zero Jacobian row: its
+// row of I - gamma h J is the identity row, so its stage increments are zero and its column,
+// which multiplies them, drops out as well.
+template <class Kin, int N, class = void>
+struct SysMap {
+    static constexpr int size = N;
+    GAS_HD static constexpr int full(int i) { return i; }
+};
+template <class Kin, int N>
+struct SysMap<Kin, N, std::void_t<decltype(Kin::kSys)>> {
+    static constexpr int size = Kin::kSys;
+    GAS_HD static constexpr int full(int i) { return Kin::sys_full(i); }
+};
+
 // ros2_advance with the species count known at compile time and the kinetics a policy, for
 // the device's one-thread-per-cell kernels: the same method, step control, factorisation and
 // sequence of right-hand sides (the species columns of the Jacobian at the unperturbed
@@ -372,9 +389,11 @@ template <int NS, class Kin, class Mat>
 GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                            double atol = 1e-10, double atol_T = 1e-3) {
     constexpr int ns = NS, n = NS + 1;
+    using Sys = SysMap<Kin, n>;
+    constexpr int m = Sys::size;  // unknowns of the iteration system (M is m x m)
     const double gam = 1.0 + 1.0 / sqrt(2.0);
-    double y[n], F0[n], Fp[n], yp[n], k1[n], k2[n], dinv[n];
-    int piv[n];
+    double y[n], F0[n], Fp[n], yp[n], k1[m], k2[m], dinv[m];
+    int piv[m];
     for (int k = 0; k < ns; ++k) y[k] = Y[k];
     y[ns] = T;
     double tt = 0.0, h = dt;
@@ -390,6 +409,7 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
         if constexpr (Kin::kAnalyticJacobian) {
             kin.rhs_jacobian(Kf, rho, y, F0, -gam * h, M);
         } else {
+            static_assert(m == n, "finite-difference Jacobians cover the whole state");
             kin.rhs(Kf, rho, y, F0);
             // the species columns in a rolled loop (one inlined right-hand side); the perturbed
             // component is selected by comparison so that yp stays in registers
@@ -417,29 +437,32 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
 #pragma unroll
             for (int r = 0; r < n; ++r) M(r, ns) = -gam * h * (Fp[r] - F0[r]) / eps;
         }
-        for (int r = 0; r < n; ++r) M(r, r) += 1.0;
-        if (!lu_factor_n<n>(M, piv, dinv)) {
+        for (int r = 0; r < m; ++r) M(r, r) += 1.0;
+        if (!lu_factor_n<m>(M, piv, dinv)) {
             h *= 0.25;
             continue;
         }
 #pragma unroll
-        for (int q = 0; q < n; ++q) k1[q] = F0[q];
-        lu_solve_n<n>(M, piv, dinv, k1);
+        for (int q = 0; q < m; ++q) k1[q] = F0[Sys::full(q)];
+        lu_solve_n<m>(M, piv, dinv, k1);
 #pragma unroll
-        for (int q = 0; q < n; ++q) yp[q] = y[q] + h * k1[q];
+        for (int q = 0; q < n; ++q) yp[q] = y[q];
+#pragma unroll
+        for (int q = 0; q < m; ++q) yp[Sys::full(q)] = y[Sys::full(q)] + h * k1[q];
         kin.factors(yp[ns], Kf);
         kin.rhs(Kf, rho, yp, Fp);
 #pragma unroll
-        for (int q = 0; q < n; ++q) k2[q] = Fp[q] - 2.0 * k1[q];
-        lu_solve_n<n>(M, piv, dinv, k2);
+        for (int q = 0; q < m; ++q) k2[q] = Fp[Sys::full(q)] - 2.0 * k1[q];
+        lu_solve_n<m>(M, piv, dinv, k2);
         double err = 0.0;
 #pragma unroll
-        for (int q = 0; q < n; ++q) {
-            const double ynew = y[q] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
-            const double sc = (q < ns ? atol : atol_T) + rtol * fmax(fabs(y[q]), fabs(ynew));
+        for (int q = 0; q < m; ++q) {
+            const int c = Sys::full(q);
+            const double ynew = y[c] + 1.5 * h * k1[q] + 0.5 * h * k2[q];
+            const double sc = (c < ns ? atol : atol_T) + rtol * fmax(fabs(y[c]), fabs(ynew));
             const double e = 0.5 * h * (k1[q] + k2[q]) / sc;
             err = fmax(err, fabs(e));
-            yp[q] = ynew;
+            yp[c] = ynew;
         }
         if (err <= 1.0) {
 #pragma unroll
@@ -460,7 +483,7 @@ GAS_HD int ros2_advance_km(const Kin &kin, Mat &M, double rho, double *Y, double
 template <int NS, class Kin>
 GAS_HD int ros2_advance_k(const Kin &kin, double rho, double *Y, double &T, double dt, double rtol = 1e-5,
                           double atol = 1e-10, double atol_T = 1e-3) {
-    RegMat<NS + 1> M;
+    RegMat<SysMap<Kin, NS + 1>::size> M;
     return ros2_advance_km<NS>(kin, M, rho, Y, T, dt, rtol, atol, atol_T);
 }
 

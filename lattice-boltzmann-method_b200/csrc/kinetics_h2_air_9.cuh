@@ -764,9 +764,12 @@ GAS_HD void rhs_t(const Thermo &th, double rho, const double *y, double *F) {
     F[9] = -es / (rho * cv);
 }
 
-// rhs_t, and s times the Jacobian of F with respect to (Y, T) at fixed density: J(k, j) =
-// s dF_k / dY_j for j < NS and J(k, NS) = s dF_k / dT, every row k <= NS.  Each reaction's
-// rate constants are formed once and serve both.
+// rhs_t, and s times the Jacobian of F with respect to (Y, T) at fixed density over the
+// unknowns of the integrator's iteration system (Kinetics::sys_full): J(p, q) = s dF_a / dY_b,
+// a = sys_full(p), b = sys_full(q), the temperature the last unknown.
+// The inert species (N2) are not unknowns: their row is zero
+// and their column multiplies a zero increment.
+// Each reaction's rate constants are formed once and serve both.
 // The Jacobian of d(Y, T)/dt at fixed density, d F_k / d Y_j and d F_k / dT, differentiating the
 // right-hand side's expressions.  With q_r the rates of progress, nu_kr the net coefficients and
 // C_j = rho Y_j / W_j:
@@ -824,9 +827,9 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
     const double s_rho = s / rho;
     double sum_eT = 0.0;  // sum_r e_r dq_r/dT
 #pragma unroll
-    for (int k = 0; k <= 9; ++k)
+    for (int k = 0; k < 9; ++k)
 #pragma unroll
-        for (int j = 0; j <= 9; ++j) J(k, j) = 0.0;
+        for (int j = 0; j < 9; ++j) J(k, j) = 0.0;
     GAS_SCHED_FENCE();
     {  // reaction 0
         const double kf = 4.577000000000001e+16 * exp(-1.4 * logT - 436809600.0 * invRT);
@@ -858,42 +861,37 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = g;
             const double dq6 = g;
             const double dq7 = g;
-            const double dq8 = g;
             const double e_r = -1.0 * (th.hRT[0] - 1.0) + 2.0 * (th.hRT[1] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(0, 0) += -1.0 * s * dq0;
             J(1, 0) += 1.0 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(1, 1) += 2.0 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(0, 2) += -0.06300393774610913 * s * dq2;
             J(1, 2) += 0.06300393774610913 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(0, 3) += -0.12600787549221826 * s * dq3;
             J(1, 3) += 0.12600787549221826 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(0, 4) += -0.11190674437968359 * s * dq4;
             J(1, 4) += 0.11190674437968359 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(1, 5) += 0.11853942494267065 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(0, 6) += -0.05926971247133533 * s * dq6;
             J(1, 6) += 0.05926971247133533 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(0, 7) += -0.061079803672059625 * s * dq7;
             J(1, 7) += 0.061079803672059625 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(0, 8) += -0.0719640179910045 * s * dq8;
-            J(1, 8) += 0.0719640179910045 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(0, 9) += -2.016 * s_rho * dqT;
-            J(1, 9) += 2.016 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(0, 8) += -2.016 * s_rho * dqT;
+            J(1, 8) += 2.016 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 1
         const double kf = 50.80000000000001 * exp(2.67 * logT - 26325728.0 * invRT);
         const double er = exp(th.gRT[1] + th.gRT[5] - th.gRT[0] - th.gRT[3]);
@@ -925,26 +923,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(1, 0) += 0.5 * s * dq0;
             J(5, 0) += 8.436011904761905 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(1, 1) += 1.0 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(0, 3) += -0.12600787549221826 * s * dq3;
             J(3, 3) += -1.0 * s * dq3;
             J(1, 3) += 0.06300393774610913 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(1, 5) += 0.05926971247133533 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
-            J(0, 9) += -2.016 * s_rho * dqT;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(1, 9) += 1.008 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            J(0, 8) += -2.016 * s_rho * dqT;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(1, 8) += 1.008 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -979,29 +977,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(1, 0) += 0.5 * s * dq0;
             J(4, 0) += 8.936011904761905 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(1, 1) += 1.0 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(0, 4) += -0.11190674437968359 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(1, 4) += 0.055953372189841796 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(1, 5) += 0.05926971247133533 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
-            J(0, 9) += -2.016 * s_rho * dqT;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(1, 9) += 1.008 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            J(0, 8) += -2.016 * s_rho * dqT;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(1, 8) += 1.008 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 3
         const double kf = 6165000000.000002 * exp(-0.5 * logT);
         const double er = exp((th.gRT[2] - 2.0 * th.gRT[3]) - -1.0 * log_cref);
@@ -1032,39 +1029,35 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = g;
             const double dq6 = g;
             const double dq7 = g;
-            const double dq8 = g;
             const double e_r = -2.0 * (th.hRT[3] - 1.0) + 1.0 * (th.hRT[2] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(3, 0) += -15.87202380952381 * s * dq0;
             J(2, 0) += 15.87202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -31.74404761904762 * s * dq1;
             J(2, 1) += 31.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -1.0 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -2.0 * s * dq3;
             J(2, 3) += 2.0 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -1.7761865112406328 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -1.8814605750573292 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.9407302875286646 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.9694600981639702 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -1.1422146069822232 * s * dq8;
-            J(2, 8) += 1.1422146069822232 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(3, 9) += -31.998 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -31.998 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1099,29 +1092,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 1) += -1.0 * s * dq1;
             J(3, 1) += 15.87202380952381 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(2, 2) += -1.0 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(3, 2) += 0.5 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(2, 3) += -2.0 * s * dq3;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(3, 3) += 1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(2, 5) += -1.8814605750573292 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(3, 5) += 0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
-            J(2, 9) += -31.998 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(3, 9) += 15.999 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            J(2, 8) += -31.998 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(3, 8) += 15.999 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 5
         const double kf = 3.5000000000000016e+16 * exp(-2.0 * logT);
         const double er = exp((th.gRT[4] - th.gRT[1] - th.gRT[5]) - -1.0 * log_cref);
@@ -1153,49 +1145,44 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = kfM * (C1) + g;
             const double dq6 = g;
             const double dq7 = g;
-            const double dq8 = g;
             const double e_r = -1.0 * (th.hRT[1] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[4] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(1, 0) += -0.5 * s * dq0;
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(4, 0) += 8.936011904761905 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(5, 2) += -0.5315019688730546 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(5, 3) += -1.0630039377461091 * s * dq3;
             J(4, 3) += 1.1260078754922183 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(1, 8) += -0.03598200899550225 * s * dq8;
-            J(5, 8) += -0.6070893124866139 * s * dq8;
-            J(4, 8) += 0.6430713214821161 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1227,21 +1214,20 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 3) += -1.0 * s * dq3;
             J(4, 3) += -1.1260078754922183 * s * dq3;
             J(5, 3) += 2.1260078754922183 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(4, 4) += -1.0 * s * dq4;
             J(5, 4) += 1.8880932556203165 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(4, 5) += -1.0592697124713353 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(4, 9) += -18.015 * s_rho * dqT;
-            J(5, 9) += 34.014 * s_rho * dqT;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(4, 8) += -18.015 * s_rho * dqT;
+            J(5, 8) += 34.014 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 7
         const double kf = 4714000000000.002 * exp(-1.0 * logT);
         const double er = exp((th.gRT[5] - th.gRT[3] - th.gRT[1]) - -1.0 * log_cref);
@@ -1273,49 +1259,44 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = -kfM * er * (1.0) + g;
             const double dq6 = g;
             const double dq7 = g;
-            const double dq8 = g;
             const double e_r = -1.0 * (th.hRT[3] - 1.0) + -1.0 * (th.hRT[1] - 1.0) + 1.0 * (th.hRT[5] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(1, 0) += -0.5 * s * dq0;
             J(5, 0) += 8.436011904761905 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -0.5 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -1.0 * s * dq3;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(5, 4) += 0.9440466278101582 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -0.5711073034911116 * s * dq8;
-            J(1, 8) += -0.03598200899550225 * s * dq8;
-            J(5, 8) += 0.6070893124866139 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1372,42 +1353,37 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = -kfM * er * (2.0 * C5) + g;
             const double dq6 = kfM * (1.0) + 7.7 * g;
             const double dq7 = g;
-            const double dq8 = 1.5 * g;
             const double e_r = -1.0 * (th.hRT[6] - 1.0) + 2.0 * (th.hRT[5] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(6, 0) += -16.87202380952381 * s * dq0;
             J(5, 0) += 16.87202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(6, 1) += -33.74404761904762 * s * dq1;
             J(5, 1) += 33.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(6, 2) += -1.0630039377461091 * s * dq2;
             J(5, 2) += 1.0630039377461091 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(6, 3) += -2.1260078754922183 * s * dq3;
             J(5, 3) += 2.1260078754922183 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(6, 4) += -1.8880932556203165 * s * dq4;
             J(5, 4) += 1.8880932556203165 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += 1.0 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += 1.03053990183603 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -1.2141786249732278 * s * dq8;
-            J(5, 8) += 1.2141786249732278 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(5, 9) += 34.014 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(5, 8) += 34.014 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 9
         const double kf = 24100000000.000008 * exp(-(16610480.0 * invRT));
         const double er = exp(th.gRT[4] + th.gRT[5] - th.gRT[6] - th.gRT[1]);
@@ -1439,26 +1415,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 1) += -1.0 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(6, 4) += -1.8880932556203165 * s * dq4;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(5, 4) += 0.9440466278101582 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1493,29 +1469,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(0, 0) += 1.0 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(6, 1) += -33.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(0, 1) += 2.0 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(6, 6) += -1.0 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(0, 6) += 0.05926971247133533 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(0, 7) += 0.061079803672059625 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(0, 9) += 2.016 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(0, 8) += 2.016 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 11
         const double kf = 9550.000000000002 * exp(2.0 * logT - 16610480.0 * invRT);
         const double er = exp(th.gRT[5] + th.gRT[7] - th.gRT[6] - th.gRT[3]);
@@ -1547,26 +1522,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(6, 5) += -2.0 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1601,29 +1576,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 13
         const double kf = 75900000000.00002 * exp(-(30413496.0 * invRT));
         const double er = exp(th.gRT[4] + th.gRT[7] - th.gRT[6] - th.gRT[5]);
@@ -1655,26 +1629,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 9) += -34.014 * s_rho * dqT;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(6, 8) += -34.014 * s_rho * dqT;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1706,21 +1680,20 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 1) += -32.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += 33.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(7, 7) += -1.0 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += 1.03053990183603 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 9) += -33.006 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(5, 9) += 34.014 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 8) += -33.006 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(5, 8) += 34.014 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 15
         const double kf = 11402000.000000002 * exp(1.0827 * logT - 2317015.52 * invRT);
         const double er = exp(th.gRT[0] + th.gRT[2] - th.gRT[7] - th.gRT[1]);
@@ -1752,26 +1725,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(0, 0) += 1.0 * s * dq0;
             J(2, 0) += 15.87202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(7, 1) += -32.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(0, 1) += 2.0 * s * dq1;
             J(2, 1) += 31.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(0, 2) += 0.06300393774610913 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(7, 7) += -1.0 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(0, 7) += 0.061079803672059625 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 9) += -33.006 * s_rho * dqT;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(0, 9) += 2.016 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 8) += -33.006 * s_rho * dqT;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(0, 8) += 2.016 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1806,29 +1779,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 2) += -0.5 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(7, 3) += -2.063003937746109 * s * dq3;
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
             J(2, 3) += 2.0 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(7, 7) += -1.0 * s * dq7;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 9) += -33.006 * s_rho * dqT;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(5, 9) += 17.007 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 8) += -33.006 * s_rho * dqT;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(5, 8) += 17.007 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 17
         const double kf = 7000000000.000002 * exp(-(-4572944.640000001 * invRT));
         const double er = exp(th.gRT[4] + th.gRT[2] - th.gRT[5] - th.gRT[7]);
@@ -1860,26 +1832,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += -1.8321398834304745 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += -1.0 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(7, 9) += -33.006 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(7, 8) += -33.006 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1914,29 +1886,28 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += -1.8321398834304745 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += -1.0 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(7, 9) += -33.006 * s_rho * dqT;
-            J(4, 9) += 18.015 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(7, 8) += -33.006 * s_rho * dqT;
+            J(4, 8) += 18.015 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 19
         const double kf = 100000000000.00003 * exp(-(46195054.472 * invRT));
         const double er = exp(th.gRT[6] + th.gRT[2] - 2.0 * th.gRT[7]);
@@ -1965,18 +1936,18 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -2.063003937746109 * s * dq2;
             J(6, 2) += 1.0630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(7, 6) += -1.9407302875286645 * s * dq6;
             J(6, 6) += 1.0 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(7, 7) += -2.0 * s * dq7;
             J(6, 7) += 1.03053990183603 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 9) += -66.012 * s_rho * dqT;
-            J(6, 9) += 34.014 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 8) += -66.012 * s_rho * dqT;
+            J(6, 8) += 34.014 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -2008,21 +1979,20 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -2.063003937746109 * s * dq2;
             J(6, 2) += 1.0630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(7, 6) += -1.9407302875286645 * s * dq6;
             J(6, 6) += 1.0 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(7, 7) += -2.0 * s * dq7;
             J(6, 7) += 1.03053990183603 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 9) += -66.012 * s_rho * dqT;
-            J(6, 9) += 34.014 * s_rho * dqT;
-            J(2, 9) += 31.998 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(7, 8) += -66.012 * s_rho * dqT;
+            J(6, 8) += 34.014 * s_rho * dqT;
+            J(2, 8) += 31.998 * s_rho * dqT;
         }
     }
-    GAS_SCHED_FENCE();
     {  // reaction 21
         const double kf = 4650000000.000001 * exp(0.44 * logT);
         const double k0 = 17370000000000.006 * exp(-1.23 * logT);
@@ -2077,49 +2047,44 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = g;
             const double dq6 = g;
             const double dq7 = -kfM * er * (1.0) + g;
-            const double dq8 = g;
             const double e_r = -1.0 * (th.hRT[1] - 1.0) + -1.0 * (th.hRT[2] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(1, 0) += -0.5 * s * dq0;
             J(2, 0) += -15.87202380952381 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(1, 1) += -1.0 * s * dq1;
             J(2, 1) += -31.74404761904762 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(2, 2) += -1.0 * s * dq2;
             J(7, 2) += 1.0315019688730545 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(2, 3) += -2.0 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(2, 4) += -1.7761865112406328 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(2, 5) += -1.8814605750573292 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(2, 6) += -0.9407302875286646 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(2, 7) += -0.9694600981639702 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(1, 8) += -0.03598200899550225 * s * dq8;
-            J(2, 8) += -1.1422146069822232 * s * dq8;
-            J(7, 8) += 1.1781966159777255 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(1, 9) += -1.008 * s_rho * dqT;
-            J(2, 9) += -31.998 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(1, 8) += -1.008 * s_rho * dqT;
+            J(2, 8) += -31.998 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -2154,49 +2119,44 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             const double dq5 = kfM * (C3) + g;
             const double dq6 = g;
             const double dq7 = -kfM * er * (1.0) + g;
-            const double dq8 = g;
             const double e_r = -1.0 * (th.hRT[3] - 1.0) + -1.0 * (th.hRT[5] - 1.0) + 1.0 * (th.hRT[7] - 1.0);
             const double eT = sT * e_r;
             sum_eT += e_r * dqT;
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(9, 0) += 0.49603174603174605 * eT * dq0;
+            J(8, 0) += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(9, 1) += 0.9920634920634921 * eT * dq1;
+            J(8, 1) += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -0.5 * s * dq2;
             J(5, 2) += -0.5315019688730546 * s * dq2;
             J(7, 2) += 1.0315019688730545 * s * dq2;
-            J(9, 2) += 0.03125195324707794 * eT * dq2;
+            J(8, 2) += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += -1.0630039377461091 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(9, 3) += 0.06250390649415588 * eT * dq3;
+            J(8, 3) += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(9, 4) += 0.055509297807382736 * eT * dq4;
+            J(8, 4) += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(9, 5) += 0.05879931792791203 * eT * dq5;
+            J(8, 5) += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(9, 6) += 0.029399658963956014 * eT * dq6;
+            J(8, 6) += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(9, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -0.5711073034911116 * s * dq8;
-            J(5, 8) += -0.6070893124866139 * s * dq8;
-            J(7, 8) += 1.1781966159777255 * s * dq8;
-            J(9, 8) += 0.03569643749553795 * eT * dq8;
-            J(3, 9) += -15.999 * s_rho * dqT;
-            J(5, 9) += -17.007 * s_rho * dqT;
-            J(7, 9) += 33.006 * s_rho * dqT;
+            J(8, 7) += 0.030297521662727988 * eT * dq7;
+            J(3, 8) += -15.999 * s_rho * dqT;
+            J(5, 8) += -17.007 * s_rho * dqT;
+            J(7, 8) += 33.006 * s_rho * dqT;
         }
     }
     double es = 0.0;
@@ -2220,15 +2180,14 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
     es += (th.hRT[8] - 1.0) * 8314.46261815324 * T * w8;
     F[9] = -es / (rho * cv);
     const double sF = s * F[9] * 8314.46261815324 / cv;
-    J(9, 0) -= sF * (th.cpR[0] - 1.0) * 0.49603174603174605;
-    J(9, 1) -= sF * (th.cpR[1] - 1.0) * 0.9920634920634921;
-    J(9, 2) -= sF * (th.cpR[2] - 1.0) * 0.03125195324707794;
-    J(9, 3) -= sF * (th.cpR[3] - 1.0) * 0.06250390649415588;
-    J(9, 4) -= sF * (th.cpR[4] - 1.0) * 0.055509297807382736;
-    J(9, 5) -= sF * (th.cpR[5] - 1.0) * 0.05879931792791203;
-    J(9, 6) -= sF * (th.cpR[6] - 1.0) * 0.029399658963956014;
-    J(9, 7) -= sF * (th.cpR[7] - 1.0) * 0.030297521662727988;
-    J(9, 8) -= sF * (th.cpR[8] - 1.0) * 0.03569643749553795;
+    J(8, 0) -= sF * (th.cpR[0] - 1.0) * 0.49603174603174605;
+    J(8, 1) -= sF * (th.cpR[1] - 1.0) * 0.9920634920634921;
+    J(8, 2) -= sF * (th.cpR[2] - 1.0) * 0.03125195324707794;
+    J(8, 3) -= sF * (th.cpR[3] - 1.0) * 0.06250390649415588;
+    J(8, 4) -= sF * (th.cpR[4] - 1.0) * 0.055509297807382736;
+    J(8, 5) -= sF * (th.cpR[5] - 1.0) * 0.05879931792791203;
+    J(8, 6) -= sF * (th.cpR[6] - 1.0) * 0.029399658963956014;
+    J(8, 7) -= sF * (th.cpR[7] - 1.0) * 0.030297521662727988;
     double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R
     sw += (th.cpR[0] - 1.0) * F[0] * rho * 0.49603174603174605;
     sw += (th.cpR[1] - 1.0) * F[1] * rho * 0.9920634920634921;
@@ -2260,7 +2219,7 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
         dcv += y[7] * 0.030297521662727988 * (0.00204046836 + T * (-7.31755124e-07 + T * (5.57919132e-11 + T * 1.99527326e-15)));
         dcv += y[8] * 0.03569643749553795 * (0.0014183803 + T * (-1.00656209e-06 + T * (2.422666392e-10 + T * -1.9042571e-14)));
     }
-    J(9, 9) = s * (-8314.46261815324 * (sw + T * sum_eT) / (rho * cv) - F[9] * 8314.46261815324 * dcv / cv);
+    J(8, 8) = s * (-8314.46261815324 * (sw + T * sum_eT) / (rho * cv) - F[9] * 8314.46261815324 * dcv / cv);
 }
 
 // The integrator's kinetics policy (gas::ros2_advance_km): thermo once per temperature,
@@ -2269,6 +2228,8 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
 struct Kinetics {
     using K = Thermo;
     static constexpr bool kAnalyticJacobian = true;
+    static constexpr int kSys = 9;  // unknowns of the iteration system
+    GAS_HD static constexpr int sys_full(int i) { return i == 0 ? 0 : (i == 1 ? 1 : (i == 2 ? 2 : (i == 3 ? 3 : (i == 4 ? 4 : (i == 5 ? 5 : (i == 6 ? 6 : (i == 7 ? 7 : (9)))))))); }
     GAS_HD void factors(double T, Thermo &k) const { thermo(T, k); }
     GAS_HD void rhs(const Thermo &k, double rho, const double *y, double *F) const { rhs_t(k, rho, y, F); }
     template <class Mat>

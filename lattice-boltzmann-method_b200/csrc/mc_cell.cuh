@@ -584,7 +584,11 @@ MC_HDN void mc_stream_moment_cell(const AT &A, long n) {
 // (gen_kinetics.py) when the handle's mechanism is that one, void for the tables.
 // SMAT (device, G = 1, KIN): the integrator's iteration matrix in the dynamic shared memory
 // the kernel was launched with, (NS + 1)^2 doubles per thread of the block.
-template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1, class KIN = void, bool SMAT = false>
+// PRED (false: a launch made while the surrogate's predictions are not in use): the
+// prediction, its gate and its audit compiled out, so nothing of them stays live across the
+// integration.
+template <int NS, class AT, bool CAN_INTEGRATE = true, int G = 1, class KIN = void, bool SMAT = false,
+          bool PRED = true>
 MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, const double *Y, double T_si,
                          double rho_si, double P_si, bool defer) {
     const gas::Tables &t = *A.tab;
@@ -597,7 +601,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
     const double dt_si = (double)A.dt * (double)A.U.s;
     double Yc[gas::MAXS], Tc = T_si, Yp[NS], Tp = T_si;
     bool have_pred = false;
-    if (S.mode == 1 && !S.gate[n]) {
+    if (PRED && S.mode == 1 && !S.gate[n]) {
         // the prediction is used if it is finite, every output lies within kSurOutGate
         // standard deviations of the training targets, and after the element projection no
         // mass fraction goes below -kSurNegTol; otherwise the integrator takes the cell
@@ -617,7 +621,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
         Tp = T_si + (double)pr[NS];
     }
     const bool audit = have_pred && S.audit_period > 0 && (unsigned)(n % S.audit_period) == S.audit_phase;
-    if (S.mode == 1 && (defer || !S.ilist)) {
+    if (PRED && S.mode == 1 && (defer || !S.ilist)) {
         count_flag(&S.audit[3], audit);
         count_flag(&S.audit[4], have_pred && !audit);
         count_flag(&S.audit[5], !have_pred);
@@ -641,7 +645,7 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
                 rc = gas::ros2_advance_group<NS, G>(gas::CachedTableKinetics{t}, rho_si, Yc, Tc, dt_si);
             else if constexpr (!std::is_void_v<KIN> && SMAT) {
                 extern __shared__ double mc_chem_smem[];
-                gas::SharedMat<NS + 1> Ms{mc_chem_smem + threadIdx.x, (int)blockDim.x};
+                gas::SharedMat<gas::SysMap<KIN, NS + 1>::size> Ms{mc_chem_smem + threadIdx.x, (int)blockDim.x};
                 rc = gas::ros2_advance_km<NS>(KIN{}, Ms, rho_si, Yc, Tc, dt_si);
             } else if constexpr (!std::is_void_v<KIN>)
                 rc = gas::ros2_advance_k<NS>(KIN{}, rho_si, Yc, Tc, dt_si);

@@ -46,13 +46,17 @@ __global__ void __launch_bounds__(kBlock, sizeof(S) == sizeof(float) ? 4 : 3) k_
 // lane each.  A short list (up to kChemShortList cells: latency-bound) takes 8 lanes per
 // cell, a long one 4 (the group's redundant factorisation then costs more than the
 // latency it saves); the choice is made on the device from the list's length.
-// The stiff integrator's iteration matrix in shared memory, (NS + 1)^2 doubles per thread of
-// a block (kernels over a compiled mechanism): two blocks of 128 threads per SM hold 200 kB
-// for 9 species, where the thread's own array would live in local memory (its pivoted rows
-// are indexed at run time) and spill through L2.
+// The stiff integrator's iteration matrix in shared memory, m^2 doubles per thread of a block
+// (kernels over a compiled mechanism; m the unknowns of its iteration system, gas::SysMap: 9
+// for the H2/air mechanism, whose N2 is inert): two blocks of 128 threads per SM hold 162 kB,
+// where the thread's own array would live in local memory (its pivoted rows are indexed at
+// run time) and spill through L2; what the blocks leave of the SM's 256 kB serves as L1.
 constexpr bool kChemSharedMat = true;
-template <int NS>
-constexpr size_t chem_smem_bytes() { return kChemSharedMat ? (size_t)(NS + 1) * (NS + 1) * kBlock * sizeof(double) : 0; }
+template <int NS, class KIN>
+constexpr size_t chem_smem_bytes() {
+    constexpr size_t m = gas::SysMap<KIN, NS + 1>::size;
+    return kChemSharedMat ? m * m * kBlock * sizeof(double) : 0;
+}
 constexpr unsigned kChemShortList = 5000;
 template <int NS, int G, typename S, class KIN, bool SMAT = false>
 __device__ __forceinline__ void chem_list_groups(const McArgsT<S, double> &A, unsigned cnt) {
@@ -94,14 +98,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_mc_chem_list(McArgsT<S, double> A
 // thread's local memory.
 // The surrogate's instance (SUR: no integrator in it) holds far less per thread and runs four
 // blocks per SM.
-template <int NS, bool SUR, typename S, class KIN = void>
+// PRED false: launched only while the surrogate's predictions are not in use (mode != 1).
+template <int NS, bool SUR, typename S, class KIN = void, bool PRED = true>
 __global__ void __launch_bounds__(kBlock, SUR ? 4 : 2) k_mc_chem(McArgsT<S, double> A) {
     const long n = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= A.ncell || !(A.cflag[n] & CF_FLUID)) return;
     double rho, rho_a[NS], Y[NS], T_si, rho_si, P_si;
     mc_chem_state<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si);
     constexpr bool smat = kChemSharedMat && !std::is_void_v<KIN>;
-    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1, KIN, smat>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
+    mc_chem_ros2<NS, McArgsT<S, double>, !SUR, 1, KIN, smat, PRED>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, SUR);
 }
 
 // The energy-flux terms of the collision (mc_eflux_cell), after the collision parameters.
@@ -298,18 +303,23 @@ bool launch_compiled_chem(lbmgpu *h, const McArgsT<S, double> &A, unsigned grid,
     if constexpr (NS == kin_h2_air_9::NS) {
         using KinH2 = kin_h2_air_9::Kinetics;
         if (h->kin != KIN_H2_AIR_9) return false;
-        constexpr size_t sm = chem_smem_bytes<NS>();
+        constexpr size_t sm = chem_smem_bytes<NS, KinH2>();
         // the launches below report a refused attribute as a launch error
         if (list) {
             if (sm > 48 * 1024)
                 (void)cudaFuncSetAttribute(k_mc_chem_list<NS, S, KinH2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sm);
             k_mc_chem_list<NS, S, KinH2><<<grid, kBlock, sm, h->stream>>>(A);
-        } else {
+        } else if (A.sur.mode == 1) {
             if (sm > 48 * 1024)
                 (void)cudaFuncSetAttribute(k_mc_chem<NS, false, S, KinH2>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             k_mc_chem<NS, false, S, KinH2><<<grid, kBlock, sm, h->stream>>>(A);
+        } else {
+            if (sm > 48 * 1024)
+                (void)cudaFuncSetAttribute(k_mc_chem<NS, false, S, KinH2, false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            k_mc_chem<NS, false, S, KinH2, false><<<grid, kBlock, sm, h->stream>>>(A);
         }
         return true;
     }

@@ -47,14 +47,22 @@ int kh_ros2_compiled(double rho, double *Y, double *T, double dt) {
 }
 
 extern "C" {
-// the compiled kinetics' analytic Jacobian d(Y, T)/dt / d(Y, T) (row-major 10 x 10) and the
-// right-hand side rhs_jac returns with it
+// the compiled kinetics' analytic Jacobian d(Y, T)/dt / d(Y, T) (row-major 10 x 10 over the
+// state; the rows and columns of the inert species, which are not unknowns of the iteration
+// system, are left zero) and the right-hand side rhs_jac returns with it
 void kh_jac_compiled(double rho, const double *y, double *J, double *F) {
+    constexpr int m = K9::Kinetics::kSys, n = K9::NS + 1;
     K9::Thermo th;
     K9::thermo(y[K9::NS], th);
-    gas::RegMat<K9::NS + 1> Jm;
+    gas::RegMat<m> Jm;
     K9::rhs_jac(th, rho, y, F, 1.0, Jm);
-    for (int r = 0; r <= K9::NS; ++r)
-        for (int c = 0; c <= K9::NS; ++c) J[r * (K9::NS + 1) + c] = Jm(r, c);
+    for (int i = 0; i < n * n; ++i) J[i] = 0.0;
+    for (int r = 0; r < m; ++r)
+        for (int c = 0; c < m; ++c) J[K9::Kinetics::sys_full(r) * n + K9::Kinetics::sys_full(c)] = Jm(r, c);
+}
+// the state components that are unknowns of the compiled kinetics' iteration system
+int kh_sys_full(int *full) {
+    for (int i = 0; i < K9::Kinetics::kSys; ++i) full[i] = K9::Kinetics::sys_full(i);
+    return K9::Kinetics::kSys;
 }
 }
