@@ -683,28 +683,33 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
             S.ds_valid[row] = 1;
         }
     }
+    // the heat release -sum_k h_k dρ_k from the reciprocal forms (h_RT_fast, 1/W_k): this
+    // stiff-chemistry mode has no reference rounding to reproduce
     double hrr = 0.0;
+    const double invTc = 1.0 / Tc;
     for (int a = 0; a < NS; ++a) {
         const double dr = rho * (Yc[a] - Y[a]);
-        hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT(t, a, Tc) * gas::kR * Tc / t.m.W[a])) * dr;
+        hrr += -1.0 * (double)u_energy_mass(A.U, (float)(gas::h_RT_fast(t, a, Tc, invTc) * gas::kR * Tc * t.invW[a])) * dr;
         A.props[(long)pr_drho<NS>(a) * A.ncell + n] = dr;
     }
     put(A, A.rec_nxt, RM_HRR, n, hrr);
 }
 
 // The chemistry state of a cell from the record, as the collision forms it (Cantera's
-// setMassFractions + setState_TD, lbm-collision.cpp:364-367).
+// setMassFractions + setState_TD, lbm-collision.cpp:364-367), in the reciprocal forms
+// (set_mass_fractions_fast): the stiff-chemistry mode has no reference rounding to reproduce.
 template <int NS, class AT>
 MC_HD void mc_chem_state(const AT &A, long n, double &rho, double *rho_a, double *Y, double &T_si, double &rho_si,
                          double &P_si) {
     const gas::Tables &t = *A.tab;
     rho = rec(A, A.rec_cur, RM_RHO, n);
     double Yr[NS], X[NS];
+    const double ir = 1.0 / rho;
     for (int a = 0; a < NS; ++a) {
         rho_a[a] = rec(A, A.rec_cur, rs(a, RS_RHO), n);
-        Yr[a] = rho_a[a] / rho;
+        Yr[a] = rho_a[a] * ir;
     }
-    const double W = set_mass_fractions<NS>(t, Yr, Y, X);
+    const double W = set_mass_fractions_fast<NS>(t, Yr, Y, X);
     T_si = si_temp(A.U, (float)rec(A, A.rec_cur, RM_T, n));
     rho_si = si_rho(A.U, (float)rho);
     P_si = rho_si * gas::kR * T_si / W;
@@ -945,7 +950,9 @@ MC_HDN void mc_props_cell(const AT &A, long n) {
         }
         put(A, A.rec_nxt, RM_HRR, n, hrr);
     } else if (CHEM == CHEM_ROSENBROCK) {  // the host build; the device runs it in k_mc_chem
-        mc_chem_ros2<NS>(A, n, rho, rho_a, Y, T_si, rho_si, P_si, true);
+        double rc, rac[NS], Yc[NS], Tc, rhoc, Pc;  // the state as k_mc_chem forms it
+        mc_chem_state<NS>(A, n, rc, rac, Yc, Tc, rhoc, Pc);
+        mc_chem_ros2<NS>(A, n, rc, rac, Yc, Tc, rhoc, Pc, true);
     }
 
     if constexpr (sizeof(typename AT::P) == sizeof(float))
