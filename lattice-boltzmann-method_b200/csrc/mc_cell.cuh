@@ -808,8 +808,10 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
     auto prp = [&](int plane, double v) { Pr[(long)plane * A.ncell + n] = v; };
     const float dt = (float)A.dt, pf = (float)p;
     const float xT = (float)gas::lnT_x(T_si);
-    // per species: mu_k, sqrt(mu_k) and their reciprocals, so that the Wilke pairs multiply
+    // per species: mu_k, sqrt(mu_k) and their reciprocals, so that the Wilke pairs multiply;
+    // every loop unrolled, so that these arrays live in registers
     float mu_k[NS], imu[NS], smu[NS], ismu[NS], Xsf[NS], Xf[NS];
+#pragma unroll
     for (int a = 0; a < NS; ++a) {
         mu_k[a] = expf(gas::fit_eval_f(t.fit_visc[a], xT));
         imu[a] = 1.f / mu_k[a];
@@ -819,8 +821,11 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
         Xf[a] = (float)X[a];
     }
     float den_s[NS], den_m[NS];
+#pragma unroll
     for (int a = 0; a < NS; ++a) den_s[a] = den_m[a] = 0.f;
+#pragma unroll
     for (int a = 0; a < NS; ++a)
+#pragma unroll
         for (int b = a; b < NS; ++b) {
             const float f1 = 1.f + smu[a] * ismu[b] * (float)t.sqrt4W[a][b];
             const float pab = f1 * f1 * t.inv_wilke_den_f[a][b];
@@ -835,31 +840,40 @@ MC_HDN void mc_transport_f32(const AT &A, long n, double p, const double *rho_a,
                 den_m[b] += Xf[a] * pba;
             }
         }
+#pragma unroll
     for (int a = 0; a < NS; ++a) {
         const float visc = Xsf[a] * u_mu(A.U, mu_k[a]) / den_s[a];
         prp(pr_om<NS>(a), (double)(2.f * Xsf[a] * pf * dt / (Xsf[a] * pf * dt + 2.f * visc)));
     }
     double F[NS][3];
+#pragma unroll
     for (int a = 0; a < NS; ++a)
+#pragma unroll
         for (int d = 0; d < 3; ++d) F[a][d] = 0.0;
     const float inv_P = 1.f / (float)P_si;
+#pragma unroll
     for (int a = 0; a < NS; ++a)
+#pragma unroll
         for (int b = 0; b < a; ++b) {
             const float D = u_nu(A.U, expf(gas::fit_eval_f(t.fit_diff[a][b], xT)) * inv_P);
             prp(pr_d<NS>(a, b), (double)D);
             const double k = (double)(-pf * Xsf[a] * Xsf[b] / D);
+#pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const double du = ua[a][d] - ua[b][d];
                 F[a][d] += k * du;
                 F[b][d] -= k * du;
             }
         }
+#pragma unroll
     for (int a = 0; a < NS; ++a) {
         const double s = (double)dt / rho_a[a];
+#pragma unroll
         for (int d = 0; d < 3; ++d) prp(pr_f<NS>(a, d), F[a][d] * s);
     }
     float mu = 0.f, cpm = 0.f, s1 = 0.f, s2 = 0.f;
     const float Tf = (float)T_si;
+#pragma unroll
     for (int k = 0; k < NS; ++k) {
         mu += Xf[k] * mu_k[k] / den_m[k];
         const double *c = T_si < t.m.T_mid[k] ? t.m.nasa_lo[k] : t.m.nasa_hi[k];
