@@ -205,13 +205,15 @@ GAS_HD double h_RT_fast(const Tables &t, int k, double T, double invT) {
 }
 
 // T_from_u with h_RT_fast and one reciprocal per iteration: the same damped Newton iteration
-// and stopping rule.
+// and stopping rule, for NS species (t.ns) known at compile time so that Y stays in registers.
+template <int NS>
 GAS_HD int T_from_u_fast(const Tables &t, const double *Y, double u, double T0, double rtol, int maxit, double &T) {
     T = T0 > 0 ? T0 : 300.0;
     for (int it = 0; it < maxit; ++it) {
         const double invT = 1.0 / T;
         double e = 0.0, c = 0.0;
-        for (int k = 0; k < t.ns; ++k) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
             e += Y[k] * (h_RT_fast(t, k, T, invT) - 1.0) * t.invW[k];
             c += Y[k] * (cp_R(t, k, T) - 1.0) * t.invW[k];
         }

@@ -396,14 +396,19 @@ MC_HD void mc_stefan_maxwell(int dt, double p_old, const double *Xold, const dou
 // reference's roundings: the matrix is symmetric (each pair's entry -dt/2 p X_a X_b / D_ab
 // formed once, one division), and the Cholesky factor's pivots are inverted once, so the
 // factorisation and the solves multiply instead of dividing -- 36 divisions and 9 square roots
-// in place of 171 divisions and 9 square roots.
+// in place of 171 divisions and 9 square roots.  Every loop is unrolled, so the factor and the
+// vectors are indexed by constants and stay out of local memory (1.92 -> 1.57 ms at 128^3,
+// with the temperature iteration's species loop unrolled as well).
 template <int NS>
 MC_HD void mc_stefan_maxwell_fast(int dt, double p_old, const double *Xold, const double *rho_s,
                                   const double (*j_a)[3], double (*Ld)[NS], double (*usm)[3]) {
     double L[NS][NS];
     const double k = -0.5 * (double)dt * p_old;
+#pragma unroll
     for (int a = 0; a < NS; ++a) L[a][a] = rho_s[a] == 0.0 ? 1.0 : rho_s[a];
+#pragma unroll
     for (int a = 0; a < NS; ++a)
+#pragma unroll
         for (int b = 0; b < a; ++b) {
             const double m = k * Xold[a] * Xold[b] / Ld[a][b];
             L[a][b] = m;
@@ -411,28 +416,38 @@ MC_HD void mc_stefan_maxwell_fast(int dt, double p_old, const double *Xold, cons
             L[b][b] -= m;
         }
     double inv[NS];
+#pragma unroll
     for (int c = 0; c < NS; ++c) {  // in-place lower Cholesky factor, reciprocal pivots
         double d = L[c][c];
+#pragma unroll
         for (int q = 0; q < c; ++q) d -= L[c][q] * L[c][q];
         inv[c] = 1.0 / sqrt(d);
+#pragma unroll
         for (int r = c + 1; r < NS; ++r) {
             double sum = L[r][c];
+#pragma unroll
             for (int q = 0; q < c; ++q) sum -= L[r][q] * L[c][q];
             L[r][c] = sum * inv[c];
         }
     }
+#pragma unroll
     for (int dmn = 0; dmn < 3; ++dmn) {
         double y[NS], x[NS];
+#pragma unroll
         for (int r = 0; r < NS; ++r) {
             double sum = j_a[r][dmn];
+#pragma unroll
             for (int q = 0; q < r; ++q) sum -= L[r][q] * y[q];
             y[r] = sum * inv[r];
         }
+#pragma unroll
         for (int r = NS - 1; r >= 0; --r) {
             double sum = y[r];
+#pragma unroll
             for (int q = r + 1; q < NS; ++q) sum -= L[q][r] * x[q];
             x[r] = sum * inv[r];
         }
+#pragma unroll
         for (int r = 0; r < NS; ++r) usm[r][dmn] = x[r];
     }
 }
@@ -518,7 +533,7 @@ MC_HDN void mc_moments_finish(const AT &A, long n, const Sums &S) {
     const double vol = 1.0 / (double)si_rho(A.U, (float)rho);
     const double rho_n_si = 1.0 / vol;
     double Tn;
-    const int it = fast ? gas::T_from_u_fast(t, Y, u_si, T_si, 1e-14, 100, Tn)
+    const int it = fast ? gas::T_from_u_fast<NS>(t, Y, u_si, T_si, 1e-14, 100, Tn)
                         : gas::T_from_u(t, Y, u_si, T_si, 1e-14, 100, Tn);
     if (it < 0) atomic_status(A.status, LBMGPU_ST_NEWTON);
     const double Pn = rho_n_si * gas::kR * Tn / Wn;
