@@ -826,6 +826,9 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
     const double sT = -s * 8314.46261815324 * T / cv;  // times e_r dq_rj / W_j: the T row
     const double s_rho = s / rho;
     double sum_eT = 0.0;  // sum_r e_r dq_r/dT
+    // the temperature row (jT) and column (jc), summed in registers and stored once
+    double jT0 = 0.0, jT1 = 0.0, jT2 = 0.0, jT3 = 0.0, jT4 = 0.0, jT5 = 0.0, jT6 = 0.0, jT7 = 0.0;
+    double jc0 = 0.0, jc1 = 0.0, jc2 = 0.0, jc3 = 0.0, jc4 = 0.0, jc5 = 0.0, jc6 = 0.0, jc7 = 0.0;
 #pragma unroll
     for (int k = 0; k < 9; ++k)
 #pragma unroll
@@ -866,30 +869,30 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             sum_eT += e_r * dqT;
             J(0, 0) += -1.0 * s * dq0;
             J(1, 0) += 1.0 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(1, 1) += 2.0 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(0, 2) += -0.06300393774610913 * s * dq2;
             J(1, 2) += 0.06300393774610913 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(0, 3) += -0.12600787549221826 * s * dq3;
             J(1, 3) += 0.12600787549221826 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(0, 4) += -0.11190674437968359 * s * dq4;
             J(1, 4) += 0.11190674437968359 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(1, 5) += 0.11853942494267065 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(0, 6) += -0.05926971247133533 * s * dq6;
             J(1, 6) += 0.05926971247133533 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(0, 7) += -0.061079803672059625 * s * dq7;
             J(1, 7) += 0.061079803672059625 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(0, 8) += -2.016 * s_rho * dqT;
-            J(1, 8) += 2.016 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc0 += -2.016 * s_rho * dqT;
+            jc1 += 2.016 * s_rho * dqT;
         }
     }
     {  // reaction 1
@@ -923,26 +926,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(1, 0) += 0.5 * s * dq0;
             J(5, 0) += 8.436011904761905 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(1, 1) += 1.0 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(0, 3) += -0.12600787549221826 * s * dq3;
             J(3, 3) += -1.0 * s * dq3;
             J(1, 3) += 0.06300393774610913 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(1, 5) += 0.05926971247133533 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
-            J(0, 8) += -2.016 * s_rho * dqT;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(1, 8) += 1.008 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
+            jT5 += 0.05879931792791203 * eT * dq5;
+            jc0 += -2.016 * s_rho * dqT;
+            jc3 += -15.999 * s_rho * dqT;
+            jc1 += 1.008 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -977,26 +980,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(1, 0) += 0.5 * s * dq0;
             J(4, 0) += 8.936011904761905 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(0, 1) += -2.0 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(1, 1) += 1.0 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(0, 4) += -0.11190674437968359 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(1, 4) += 0.055953372189841796 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(0, 5) += -0.11853942494267065 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(1, 5) += 0.05926971247133533 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
-            J(0, 8) += -2.016 * s_rho * dqT;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(1, 8) += 1.008 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
+            jT5 += 0.05879931792791203 * eT * dq5;
+            jc0 += -2.016 * s_rho * dqT;
+            jc5 += -17.007 * s_rho * dqT;
+            jc1 += 1.008 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
         }
     }
     {  // reaction 3
@@ -1034,30 +1037,30 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             sum_eT += e_r * dqT;
             J(3, 0) += -15.87202380952381 * s * dq0;
             J(2, 0) += 15.87202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -31.74404761904762 * s * dq1;
             J(2, 1) += 31.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -1.0 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -2.0 * s * dq3;
             J(2, 3) += 2.0 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -1.7761865112406328 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -1.8814605750573292 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.9407302875286646 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.9694600981639702 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -31.998 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc3 += -31.998 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1092,26 +1095,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 1) += -1.0 * s * dq1;
             J(3, 1) += 15.87202380952381 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(2, 2) += -1.0 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(3, 2) += 0.5 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(2, 3) += -2.0 * s * dq3;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(3, 3) += 1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(2, 5) += -1.8814605750573292 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(3, 5) += 0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
-            J(2, 8) += -31.998 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(3, 8) += 15.999 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
+            jT5 += 0.05879931792791203 * eT * dq5;
+            jc2 += -31.998 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc3 += 15.999 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
         }
     }
     {  // reaction 5
@@ -1151,38 +1154,38 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(4, 0) += 8.936011904761905 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(5, 2) += -0.5315019688730546 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(5, 3) += -1.0630039377461091 * s * dq3;
             J(4, 3) += 1.1260078754922183 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc1 += -1.008 * s_rho * dqT;
+            jc5 += -17.007 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1214,18 +1217,18 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 3) += -1.0 * s * dq3;
             J(4, 3) += -1.1260078754922183 * s * dq3;
             J(5, 3) += 2.1260078754922183 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(4, 4) += -1.0 * s * dq4;
             J(5, 4) += 1.8880932556203165 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(4, 5) += -1.0592697124713353 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(4, 8) += -18.015 * s_rho * dqT;
-            J(5, 8) += 34.014 * s_rho * dqT;
+            jT5 += 0.05879931792791203 * eT * dq5;
+            jc3 += -15.999 * s_rho * dqT;
+            jc4 += -18.015 * s_rho * dqT;
+            jc5 += 34.014 * s_rho * dqT;
         }
     }
     {  // reaction 7
@@ -1265,38 +1268,38 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(1, 0) += -0.5 * s * dq0;
             J(5, 0) += 8.436011904761905 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -0.5 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -1.0 * s * dq3;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(5, 4) += 0.9440466278101582 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc3 += -15.999 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1358,30 +1361,30 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             sum_eT += e_r * dqT;
             J(6, 0) += -16.87202380952381 * s * dq0;
             J(5, 0) += 16.87202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(6, 1) += -33.74404761904762 * s * dq1;
             J(5, 1) += 33.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(6, 2) += -1.0630039377461091 * s * dq2;
             J(5, 2) += 1.0630039377461091 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(6, 3) += -2.1260078754922183 * s * dq3;
             J(5, 3) += 2.1260078754922183 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(6, 4) += -1.8880932556203165 * s * dq4;
             J(5, 4) += 1.8880932556203165 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += 1.0 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += 1.03053990183603 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(5, 8) += 34.014 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc6 += -34.014 * s_rho * dqT;
+            jc5 += 34.014 * s_rho * dqT;
         }
     }
     {  // reaction 9
@@ -1415,26 +1418,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 1) += -1.0 * s * dq1;
             J(4, 1) += 17.87202380952381 * s * dq1;
             J(5, 1) += 16.87202380952381 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(6, 4) += -1.8880932556203165 * s * dq4;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(5, 4) += 0.9440466278101582 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
+            jT6 += 0.029399658963956014 * eT * dq6;
+            jc6 += -34.014 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1469,26 +1472,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(0, 0) += 1.0 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(6, 1) += -33.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(0, 1) += 2.0 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(6, 6) += -1.0 * s * dq6;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(0, 6) += 0.05926971247133533 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(0, 7) += 0.061079803672059625 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(0, 8) += 2.016 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc6 += -34.014 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc0 += 2.016 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     {  // reaction 11
@@ -1522,26 +1525,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(6, 5) += -2.0 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(5, 6) += 0.5 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc6 += -34.014 * s_rho * dqT;
+            jc3 += -15.999 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1576,26 +1579,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc6 += -34.014 * s_rho * dqT;
+            jc5 += -17.007 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     {  // reaction 13
@@ -1629,26 +1632,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(6, 5) += -2.0 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(6, 6) += -1.0 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(4, 6) += 0.5296348562356676 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(6, 7) += -1.03053990183603 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(6, 8) += -34.014 * s_rho * dqT;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc6 += -34.014 * s_rho * dqT;
+            jc5 += -17.007 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1680,18 +1683,18 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 1) += -32.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(5, 1) += 33.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(5, 5) += 2.0 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(7, 7) += -1.0 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(5, 7) += 1.03053990183603 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 8) += -33.006 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(5, 8) += 34.014 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc7 += -33.006 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc5 += 34.014 * s_rho * dqT;
         }
     }
     {  // reaction 15
@@ -1725,26 +1728,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(0, 0) += 1.0 * s * dq0;
             J(2, 0) += 15.87202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(7, 1) += -32.74404761904762 * s * dq1;
             J(1, 1) += -1.0 * s * dq1;
             J(0, 1) += 2.0 * s * dq1;
             J(2, 1) += 31.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(0, 2) += 0.06300393774610913 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(7, 7) += -1.0 * s * dq7;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(0, 7) += 0.061079803672059625 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 8) += -33.006 * s_rho * dqT;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(0, 8) += 2.016 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc7 += -33.006 * s_rho * dqT;
+            jc1 += -1.008 * s_rho * dqT;
+            jc0 += 2.016 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1779,26 +1782,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 2) += -0.5 * s * dq2;
             J(5, 2) += 0.5315019688730546 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(7, 3) += -2.063003937746109 * s * dq3;
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += 1.0630039377461091 * s * dq3;
             J(2, 3) += 2.0 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += 1.0 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(7, 7) += -1.0 * s * dq7;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += 0.515269950918015 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 8) += -33.006 * s_rho * dqT;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(5, 8) += 17.007 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc7 += -33.006 * s_rho * dqT;
+            jc3 += -15.999 * s_rho * dqT;
+            jc5 += 17.007 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     {  // reaction 17
@@ -1832,26 +1835,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += -1.8321398834304745 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += -1.0 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(7, 8) += -33.006 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc5 += -17.007 * s_rho * dqT;
+            jc7 += -33.006 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1886,26 +1889,26 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -1.0315019688730545 * s * dq2;
             J(4, 2) += 0.5630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += -1.8321398834304745 * s * dq4;
             J(4, 4) += 1.0 * s * dq4;
             J(2, 4) += 1.7761865112406328 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += -1.9407302875286645 * s * dq5;
             J(4, 5) += 1.0592697124713353 * s * dq5;
             J(2, 5) += 1.8814605750573292 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += -1.0 * s * dq7;
             J(4, 7) += 0.5458098527540447 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(7, 8) += -33.006 * s_rho * dqT;
-            J(4, 8) += 18.015 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc5 += -17.007 * s_rho * dqT;
+            jc7 += -33.006 * s_rho * dqT;
+            jc4 += 18.015 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     {  // reaction 19
@@ -1936,18 +1939,18 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -2.063003937746109 * s * dq2;
             J(6, 2) += 1.0630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(7, 6) += -1.9407302875286645 * s * dq6;
             J(6, 6) += 1.0 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(7, 7) += -2.0 * s * dq7;
             J(6, 7) += 1.03053990183603 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 8) += -66.012 * s_rho * dqT;
-            J(6, 8) += 34.014 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc7 += -66.012 * s_rho * dqT;
+            jc6 += 34.014 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -1979,18 +1982,18 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(7, 2) += -2.063003937746109 * s * dq2;
             J(6, 2) += 1.0630039377461091 * s * dq2;
             J(2, 2) += 1.0 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(7, 6) += -1.9407302875286645 * s * dq6;
             J(6, 6) += 1.0 * s * dq6;
             J(2, 6) += 0.9407302875286646 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(7, 7) += -2.0 * s * dq7;
             J(6, 7) += 1.03053990183603 * s * dq7;
             J(2, 7) += 0.9694600981639702 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(7, 8) += -66.012 * s_rho * dqT;
-            J(6, 8) += 34.014 * s_rho * dqT;
-            J(2, 8) += 31.998 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc7 += -66.012 * s_rho * dqT;
+            jc6 += 34.014 * s_rho * dqT;
+            jc2 += 31.998 * s_rho * dqT;
         }
     }
     {  // reaction 21
@@ -2053,38 +2056,38 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(1, 0) += -0.5 * s * dq0;
             J(2, 0) += -15.87202380952381 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(1, 1) += -1.0 * s * dq1;
             J(2, 1) += -31.74404761904762 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(1, 2) += -0.031501968873054564 * s * dq2;
             J(2, 2) += -1.0 * s * dq2;
             J(7, 2) += 1.0315019688730545 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(1, 3) += -0.06300393774610913 * s * dq3;
             J(2, 3) += -2.0 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(1, 4) += -0.055953372189841796 * s * dq4;
             J(2, 4) += -1.7761865112406328 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(1, 5) += -0.05926971247133533 * s * dq5;
             J(2, 5) += -1.8814605750573292 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(1, 6) += -0.029634856235667664 * s * dq6;
             J(2, 6) += -0.9407302875286646 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(1, 7) += -0.030539901836029813 * s * dq7;
             J(2, 7) += -0.9694600981639702 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(1, 8) += -1.008 * s_rho * dqT;
-            J(2, 8) += -31.998 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc1 += -1.008 * s_rho * dqT;
+            jc2 += -31.998 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     GAS_SCHED_FENCE();
@@ -2125,38 +2128,38 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
             J(3, 0) += -7.936011904761905 * s * dq0;
             J(5, 0) += -8.436011904761905 * s * dq0;
             J(7, 0) += 16.37202380952381 * s * dq0;
-            J(8, 0) += 0.49603174603174605 * eT * dq0;
+            jT0 += 0.49603174603174605 * eT * dq0;
             J(3, 1) += -15.87202380952381 * s * dq1;
             J(5, 1) += -16.87202380952381 * s * dq1;
             J(7, 1) += 32.74404761904762 * s * dq1;
-            J(8, 1) += 0.9920634920634921 * eT * dq1;
+            jT1 += 0.9920634920634921 * eT * dq1;
             J(3, 2) += -0.5 * s * dq2;
             J(5, 2) += -0.5315019688730546 * s * dq2;
             J(7, 2) += 1.0315019688730545 * s * dq2;
-            J(8, 2) += 0.03125195324707794 * eT * dq2;
+            jT2 += 0.03125195324707794 * eT * dq2;
             J(3, 3) += -1.0 * s * dq3;
             J(5, 3) += -1.0630039377461091 * s * dq3;
             J(7, 3) += 2.063003937746109 * s * dq3;
-            J(8, 3) += 0.06250390649415588 * eT * dq3;
+            jT3 += 0.06250390649415588 * eT * dq3;
             J(3, 4) += -0.8880932556203164 * s * dq4;
             J(5, 4) += -0.9440466278101582 * s * dq4;
             J(7, 4) += 1.8321398834304745 * s * dq4;
-            J(8, 4) += 0.055509297807382736 * eT * dq4;
+            jT4 += 0.055509297807382736 * eT * dq4;
             J(3, 5) += -0.9407302875286646 * s * dq5;
             J(5, 5) += -1.0 * s * dq5;
             J(7, 5) += 1.9407302875286645 * s * dq5;
-            J(8, 5) += 0.05879931792791203 * eT * dq5;
+            jT5 += 0.05879931792791203 * eT * dq5;
             J(3, 6) += -0.4703651437643323 * s * dq6;
             J(5, 6) += -0.5 * s * dq6;
             J(7, 6) += 0.9703651437643322 * s * dq6;
-            J(8, 6) += 0.029399658963956014 * eT * dq6;
+            jT6 += 0.029399658963956014 * eT * dq6;
             J(3, 7) += -0.4847300490819851 * s * dq7;
             J(5, 7) += -0.515269950918015 * s * dq7;
             J(7, 7) += 1.0 * s * dq7;
-            J(8, 7) += 0.030297521662727988 * eT * dq7;
-            J(3, 8) += -15.999 * s_rho * dqT;
-            J(5, 8) += -17.007 * s_rho * dqT;
-            J(7, 8) += 33.006 * s_rho * dqT;
+            jT7 += 0.030297521662727988 * eT * dq7;
+            jc3 += -15.999 * s_rho * dqT;
+            jc5 += -17.007 * s_rho * dqT;
+            jc7 += 33.006 * s_rho * dqT;
         }
     }
     double es = 0.0;
@@ -2180,14 +2183,22 @@ GAS_HD void rhs_jac(const Thermo &th, double rho, const double *y, double *F, do
     es += (th.hRT[8] - 1.0) * 8314.46261815324 * T * w8;
     F[9] = -es / (rho * cv);
     const double sF = s * F[9] * 8314.46261815324 / cv;
-    J(8, 0) -= sF * (th.cpR[0] - 1.0) * 0.49603174603174605;
-    J(8, 1) -= sF * (th.cpR[1] - 1.0) * 0.9920634920634921;
-    J(8, 2) -= sF * (th.cpR[2] - 1.0) * 0.03125195324707794;
-    J(8, 3) -= sF * (th.cpR[3] - 1.0) * 0.06250390649415588;
-    J(8, 4) -= sF * (th.cpR[4] - 1.0) * 0.055509297807382736;
-    J(8, 5) -= sF * (th.cpR[5] - 1.0) * 0.05879931792791203;
-    J(8, 6) -= sF * (th.cpR[6] - 1.0) * 0.029399658963956014;
-    J(8, 7) -= sF * (th.cpR[7] - 1.0) * 0.030297521662727988;
+    J(8, 0) = jT0 - sF * (th.cpR[0] - 1.0) * 0.49603174603174605;
+    J(0, 8) = jc0;
+    J(8, 1) = jT1 - sF * (th.cpR[1] - 1.0) * 0.9920634920634921;
+    J(1, 8) = jc1;
+    J(8, 2) = jT2 - sF * (th.cpR[2] - 1.0) * 0.03125195324707794;
+    J(2, 8) = jc2;
+    J(8, 3) = jT3 - sF * (th.cpR[3] - 1.0) * 0.06250390649415588;
+    J(3, 8) = jc3;
+    J(8, 4) = jT4 - sF * (th.cpR[4] - 1.0) * 0.055509297807382736;
+    J(4, 8) = jc4;
+    J(8, 5) = jT5 - sF * (th.cpR[5] - 1.0) * 0.05879931792791203;
+    J(5, 8) = jc5;
+    J(8, 6) = jT6 - sF * (th.cpR[6] - 1.0) * 0.029399658963956014;
+    J(6, 8) = jc6;
+    J(8, 7) = jT7 - sF * (th.cpR[7] - 1.0) * 0.030297521662727988;
+    J(7, 8) = jc7;
     double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R
     sw += (th.cpR[0] - 1.0) * F[0] * rho * 0.49603174603174605;
     sw += (th.cpR[1] - 1.0) * F[1] * rho * 0.9920634920634921;

@@ -406,9 +406,9 @@ def emit_jac_reaction(m, r, fidx, add, N):
             continue  # an inert species' column multiplies its zero increment
         for k, v in net.items():
             add(f"{ind}J({pos[k]}, {pos[j]}) += {lit(v * W[k] / W[j])} * s * dq{j};")
-        add(f"{ind}J({pos[ns]}, {pos[j]}) += {lit(1.0 / W[j])} * eT * dq{j};")
+        add(f"{ind}jT{pos[j]} += {lit(1.0 / W[j])} * eT * dq{j};")
     for k, v in net.items():
-        add(f"{ind}J({pos[k]}, {pos[ns]}) += {lit(v * W[k])} * s_rho * dqT;")
+        add(f"{ind}jc{pos[k]} += {lit(v * W[k])} * s_rho * dqT;")
     add("        }")
 
 
@@ -456,6 +456,11 @@ def emit_prologue(m, add, with_jac):
         add("    const double s_rho = s / rho;")
         add("    double sum_eT = 0.0;  // sum_r e_r dq_r/dT")
         nsys = len(system_index(m)[1])
+        # the temperature row and column: every reaction adds to them, so they are summed in
+        # registers (in reaction order, as into the matrix) and stored once
+        add("    // the temperature row (jT) and column (jc), summed in registers and stored once")
+        add("    double " + ", ".join(f"jT{q} = 0.0" for q in range(nsys - 1)) + ";")
+        add("    double " + ", ".join(f"jc{q} = 0.0" for q in range(nsys - 1)) + ";")
         add("#pragma unroll")
         add(f"    for (int k = 0; k < {nsys}; ++k)")
         add("#pragma unroll")
@@ -479,7 +484,8 @@ def emit_jac_epilogue(m, add):
     add(f"    const double sF = s * F[{ns}] * {lit(KR)} / cv;")
     for j in range(ns):
         if pos.get(j) is not None:
-            add(f"    J({pos[ns]}, {pos[j]}) -= sF * (th.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
+            add(f"    J({pos[ns]}, {pos[j]}) = jT{pos[j]} - sF * (th.cpR[{j}] - 1.0) * {lit(1.0 / m.W[j])};")
+            add(f"    J({pos[j]}, {pos[ns]}) = jc{pos[j]};")
     add("    double sw = 0.0, dcv = 0.0;  // sum_k (c_p,k/R - 1) w_k, dc_v/dT / R")
     for k in range(ns):
         add(f"    sw += (th.cpR[{k}] - 1.0) * F[{k}] * rho * {lit(1.0 / m.W[k])};")
