@@ -620,13 +620,30 @@ MC_HDN void mc_chem_ros2(const AT &A, long n, double rho, const double *rho_a, c
         // the prediction is used if it is finite, every output lies within kSurOutGate
         // standard deviations of the training targets, and after the element projection no
         // mass fraction goes below -kSurNegTol; otherwise the integrator takes the cell
-        const float *pr = S.pred + n * kSurOutPad;
+        // the row's NS + 1 outputs in whole 16-byte words (rows are kSurOutPad floats, 64 B)
+        constexpr int kWords = (NS + 4) / 4;
+        float pr[4 * kWords];
+#if defined(__CUDA_ARCH__)
+        const float4 *pw = reinterpret_cast<const float4 *>(S.pred + n * kSurOutPad);
+#pragma unroll
+        for (int q = 0; q < kWords; ++q) {
+            const float4 v = pw[q];
+            pr[4 * q] = v.x;
+            pr[4 * q + 1] = v.y;
+            pr[4 * q + 2] = v.z;
+            pr[4 * q + 3] = v.w;
+        }
+#else
+        for (int q = 0; q < 4 * kWords; ++q) pr[q] = S.pred[n * kSurOutPad + q];
+#endif
         const SurNorm &nm = *S.nrm;
         double dY[NS];
-        have_pred = isfinite(pr[NS]) && fabsf((pr[NS] - nm.y_mean[NS]) / nm.y_std[NS]) <= kSurOutGate;
+        // |pred - mean| <= kSurOutGate std (the standard deviations are positive)
+        have_pred = isfinite(pr[NS]) && fabsf(pr[NS] - nm.y_mean[NS]) <= kSurOutGate * nm.y_std[NS];
+#pragma unroll
         for (int a = 0; a < NS; ++a) {
             dY[a] = (double)pr[a];
-            have_pred = have_pred && isfinite(dY[a]) && fabsf((pr[a] - nm.y_mean[a]) / nm.y_std[a]) <= kSurOutGate;
+            have_pred = have_pred && isfinite(dY[a]) && fabsf(pr[a] - nm.y_mean[a]) <= kSurOutGate * nm.y_std[a];
         }
         if (have_pred) {
             sur_conserve<NS>(S.proj, dY);
