@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <thread>
 #include <vector>
 
 #include "../../include/lbmgpu.h"
@@ -70,7 +72,8 @@ struct lbmgpu {
     char *stage = nullptr;
     size_t stage_cells = 0;
     size_t stage_bytes = 0;
-    char *bounce = nullptr;  // pinned host bounce buffer for downloads
+    char *bounce = nullptr;  // pinned host bounce buffers for downloads (the second lets the
+    char *bounce2 = nullptr; //   device pack the next chunk while the host merges one)
     int cur = 0;
     int pack_mode = lbmh::PK_UPLOADED;
     bool have_state = false;
@@ -159,6 +162,33 @@ inline void ev_drain(lbmgpu *h) {
         h->pool.push_back(e);
     }
     h->pending.clear();
+}
+
+// f(lo, hi) over [0, n) split into contiguous ranges, one per host thread (up to the
+// machine's hardware threads, at most 32; ranges of at least min_items items).
+template <class F>
+void host_parallel_for(long n, const F &f, long min_items = 1024) {
+    const long hw = std::max(1L, (long)std::thread::hardware_concurrency());
+    const long nt = std::max(1L, std::min(std::min(hw, 32L), n / std::max(1L, min_items)));
+    if (nt == 1) {
+        f(0L, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (long t = 1; t < nt; ++t) th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt); });
+    f(0L, n / nt);
+    for (auto &x : th) x.join();
+}
+
+// Whether host memory at p is page-locked (registered or allocated by CUDA).
+inline bool host_pinned(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
 }
 
 inline unsigned grid_for(long n) { return (unsigned)((n + kBlock - 1) / kBlock); }

@@ -517,13 +517,14 @@ int lbmgpu_create(const lbmgpu_desc *desc, lbmgpu_t **out) {
         if (e != cudaSuccess) rc = cuda_fail(e);
     }
     if (!rc) {
-        // staging for AoS transfers: up to 64 MiB of records (mixture + species) per chunk
+        // staging for AoS transfers: up to 256 MiB of records (mixture + species) per chunk
         const size_t per_cell = m.size + (size_t)desc->n_species * desc->spc.size;
-        h->stage_cells = std::max<size_t>(1, std::min<size_t>((size_t)nc, (64u << 20) / per_cell));
+        h->stage_cells = std::max<size_t>(1, std::min<size_t>((size_t)nc, (256u << 20) / per_cell));
         h->stage_bytes = h->stage_cells * per_cell;
         rc = dalloc(h, &h->stage, h->stage_bytes);
         if (!rc) {
             e = cudaMallocHost(reinterpret_cast<void **>(&h->bounce), h->stage_bytes);
+            if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&h->bounce2), h->stage_bytes);
             if (e != cudaSuccess) rc = cuda_fail(e);
         }
     }
@@ -557,6 +558,7 @@ int lbmgpu_destroy(lbmgpu_t *h) {
     cudaFree(h->sum_scratch);
     cudaFree(h->stage);
     if (h->bounce) cudaFreeHost(h->bounce);
+    if (h->bounce2) cudaFreeHost(h->bounce2);
     lbmh::mc_release(h);
     if (h->fork) cudaEventDestroy(h->fork);
     if (h->join) cudaEventDestroy(h->join);

@@ -14,6 +14,7 @@
 // transport properties are evaluated in FP32, everything else in FP64).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "handle.cuh"
@@ -270,13 +271,31 @@ int mc_upload_planes(lbmgpu *h, int i0, int i1, const void *mix, const void *con
     const char *hm = static_cast<const char *>(mix);
     if ((long)h->htype.size() != g.ncell) h->htype.assign(g.ncell, 0);
     if ((int)h->plane_have.size() != g.Nx) h->plane_have.assign(g.Nx, 0);
-    for (long n = c0; n < c1; ++n) {
-        short t;
-        std::memcpy(&t, hm + (n - c0) * ms + h->mo.type, sizeof(short));
-        if (t < 0 || t > 9) return LBMGPU_E_ARG;
-        if (t == T_I || t == T_O || t == T_Q) return LBMGPU_E_UNSUPPORTED;
-        h->htype[n] = (int8_t)t;
+    // the cell types, read by host threads; the first refusal found (by cell) is returned
+    std::vector<long> bad(2, c1);  // first cell with an invalid / unsupported type
+    {
+        std::mutex mx;
+        host_parallel_for(c1 - c0, [&](long lo, long hi) {
+            long b0 = c1, b1 = c1;
+            for (long n = c0 + lo; n < c0 + hi; ++n) {
+                short t;
+                std::memcpy(&t, hm + (n - c0) * ms + h->mo.type, sizeof(short));
+                if (t < 0 || t > 9) {
+                    b0 = std::min(b0, n);
+                    break;
+                }
+                if (t == T_I || t == T_O || t == T_Q) {
+                    b1 = std::min(b1, n);
+                    break;
+                }
+                h->htype[n] = (int8_t)t;
+            }
+            std::lock_guard<std::mutex> g(mx);
+            bad[0] = std::min(bad[0], b0);
+            bad[1] = std::min(bad[1], b1);
+        });
     }
+    if (bad[0] < c1 || bad[1] < c1) return bad[0] <= bad[1] ? LBMGPU_E_ARG : LBMGPU_E_UNSUPPORTED;
     // a new upload begins: the state is incomplete until every plane has arrived again
     if (h->planes_have == 0) h->have_state = false;
     CK(cudaMemcpyAsync(h->type + c0, h->htype.data() + c0, c1 - c0, cudaMemcpyHostToDevice, h->stream));
@@ -315,36 +334,53 @@ int mc_download_planes(lbmgpu *h, int i0, int i1, void *mix, void *const *specie
     const long mfld[] = {h->mo.rho, h->mo.u, h->mo.v, h->mo.w, h->mo.p, h->mo.temp, h->mo.rhoe, h->mo.HRR};
     const long sfld[] = {h->so.X, h->so.rho, h->so.u, h->so.v, h->so.w};
     char *hm = static_cast<char *>(mix);
-    for (long n0 = c0; n0 < c1; n0 += (long)h->stage_cells) {
-        const long n1 = std::min<long>(c1, n0 + (long)h->stage_cells), cnt = n1 - n0;
+    // chunk k is packed on the device and copied into bounce buffer k % 2; while the host
+    // merges chunk k, the device packs and copies chunk k + 1 into the other buffer
+    const long step = (long)h->stage_cells;
+    auto issue = [&](long n0, char *dst) -> int {
+        const long n1 = std::min<long>(c1, n0 + step);
         const int rc = mc_by_ns(h->ns, [&](auto ops) { return decltype(ops)::pack(h, n0, n1, stepped); });
         if (rc) return rc;
-        const size_t bytes = cnt * (ms + (size_t)h->ns * ss);
-        CK(cudaMemcpyAsync(h->bounce, h->stage, bytes, cudaMemcpyDeviceToHost, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        for (long n = n0; n < n1; ++n) {
-            const char *srec = h->bounce + (n - n0) * ms;
-            char *drec = hm + (n - c0) * ms;
-            const bool fluid = cf[n - c0] & CF_FLUID;
-            if (fluid) {
-                short t;
-                std::memcpy(&t, drec + h->mo.type, sizeof(short));
-                std::memcpy(drec, srec, ms);
-                std::memcpy(drec + h->mo.type, &t, sizeof(short));
-            } else {
-                for (long o : mfld) std::memcpy(drec + o, srec + o, sizeof(double));
-                std::memcpy(drec + h->mo.p_tensor, srec + h->mo.p_tensor, 9 * sizeof(double));
-            }
-            for (int a = 0; a < h->ns; ++a) {
-                const char *ssrc = h->bounce + cnt * ms + ((size_t)a * cnt + (n - n0)) * ss;
-                char *sdst = static_cast<char *>(species[a]) + (n - c0) * ss;
-                if (fluid)
-                    std::memcpy(sdst, ssrc, ss);
-                else
-                    for (long o : sfld) std::memcpy(sdst + o, ssrc + o, sizeof(double));
-            }
+        CK(cudaMemcpyAsync(dst, h->stage, (n1 - n0) * (ms + (size_t)h->ns * ss), cudaMemcpyDeviceToHost, h->stream));
+        return 0;
+    };
+    int rc0 = issue(c0, h->bounce);
+    if (rc0) return rc0;
+    for (long n0 = c0, k = 0; n0 < c1; n0 += step, ++k) {
+        const long n1 = std::min<long>(c1, n0 + step), cnt = n1 - n0;
+        char *const buf = (k & 1) ? h->bounce2 : h->bounce;
+        CK(cudaStreamSynchronize(h->stream));  // chunk k is in buf
+        if (n1 < c1) {
+            rc0 = issue(n1, (k & 1) ? h->bounce : h->bounce2);
+            if (rc0) return rc0;
         }
+        // the merge into the caller's records (each cell's own bytes: no two threads share one)
+        host_parallel_for(cnt, [&](long lo, long hi) {
+            for (long n = n0 + lo; n < n0 + hi; ++n) {
+                const char *srec = buf + (n - n0) * ms;
+                char *drec = hm + (n - c0) * ms;
+                const bool fluid = cf[n - c0] & CF_FLUID;
+                if (fluid) {
+                    short t;
+                    std::memcpy(&t, drec + h->mo.type, sizeof(short));
+                    std::memcpy(drec, srec, ms);
+                    std::memcpy(drec + h->mo.type, &t, sizeof(short));
+                } else {
+                    for (long o : mfld) std::memcpy(drec + o, srec + o, sizeof(double));
+                    std::memcpy(drec + h->mo.p_tensor, srec + h->mo.p_tensor, 9 * sizeof(double));
+                }
+                for (int a = 0; a < h->ns; ++a) {
+                    const char *ssrc = buf + cnt * ms + ((size_t)a * cnt + (n - n0)) * ss;
+                    char *sdst = static_cast<char *>(species[a]) + (n - c0) * ss;
+                    if (fluid)
+                        std::memcpy(sdst, ssrc, ss);
+                    else
+                        for (long o : sfld) std::memcpy(sdst + o, ssrc + o, sizeof(double));
+                }
+            }
+        });
     }
+    CK(cudaStreamSynchronize(h->stream));
     return LBMGPU_OK;
 }
 

@@ -333,13 +333,35 @@ template <int NS, typename S>
 int upload_t(lbmgpu *h, const char *hm, const void *const *species, long c0, long c1) {
     const size_t ms = h->mo.size, ss = h->so.size;
     McArgsT<S, double> A = base_args<S>(h);
+    // pageable caller memory goes through the pinned bounce buffer, filled by host threads
+    // (a copy from pageable memory would otherwise be staged by the driver, one thread);
+    // page-locked caller memory is copied directly
+    bool pinned = host_pinned(hm);
+    for (int a = 0; a < h->ns; ++a) pinned = pinned && host_pinned(species[a]);
     for (long n0 = c0; n0 < c1; n0 += (long)h->stage_cells) {
         const long n1 = std::min<long>(c1, n0 + (long)h->stage_cells), cnt = n1 - n0;
-        CK(cudaMemcpyAsync(h->stage, hm + (n0 - c0) * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
-        for (int a = 0; a < h->ns; ++a)
-            CK(cudaMemcpyAsync(h->stage + cnt * ms + (size_t)a * cnt * ss,
-                               static_cast<const char *>(species[a]) + (n0 - c0) * ss, cnt * ss,
-                               cudaMemcpyHostToDevice, h->stream));
+        if (pinned) {
+            CK(cudaMemcpyAsync(h->stage, hm + (n0 - c0) * ms, cnt * ms, cudaMemcpyHostToDevice, h->stream));
+            for (int a = 0; a < h->ns; ++a)
+                CK(cudaMemcpyAsync(h->stage + cnt * ms + (size_t)a * cnt * ss,
+                                   static_cast<const char *>(species[a]) + (n0 - c0) * ss, cnt * ss,
+                                   cudaMemcpyHostToDevice, h->stream));
+        } else {
+            CK(cudaStreamSynchronize(h->stream));  // the bounce buffer's previous chunk has gone
+            const long nb = (long)h->ns + 1;       // the mixture block, then each species' block
+            host_parallel_for(nb * 64, [&](long lo, long hi) {
+                for (long q = lo; q < hi; ++q) {
+                    const long blk = q / 64, part = q % 64;
+                    const size_t sz = blk == 0 ? ms : ss;
+                    const char *src = blk == 0 ? hm : static_cast<const char *>(species[blk - 1]);
+                    char *dst = h->bounce + (blk == 0 ? 0 : cnt * ms + (size_t)(blk - 1) * cnt * ss);
+                    const long r0 = cnt * part / 64, r1 = cnt * (part + 1) / 64;
+                    std::memcpy(dst + r0 * sz, src + (n0 - c0 + r0) * sz, (r1 - r0) * sz);
+                }
+            }, 1);
+            CK(cudaMemcpyAsync(h->stage, h->bounce, cnt * (ms + (size_t)h->ns * ss), cudaMemcpyHostToDevice,
+                               h->stream));
+        }
         EvPair ep{};
         ev_begin(h, K_OTHER, ep);
         k_mc_unpack<NS, S><<<grid_for(cnt), kBlock, 0, h->stream>>>(A, h->mo, h->so, h->stage, n0, n1, h->mom[0],
