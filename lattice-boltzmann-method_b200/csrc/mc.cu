@@ -196,27 +196,50 @@ static int mc_finish_upload(lbmgpu *h) {
     long nfluid = 0, nb = 0;
     std::vector<int> bidh(nc, -1);
     std::vector<long> blh;
-    for (int i = 0; i < g.Nx; ++i)
-        for (int j = 0; j < g.Ny; ++j)
-            for (int k = 0; k < g.Nz; ++k) {
-                const long n = (long)i * g.si + (long)j * g.sj + k;
-                if (ty[n] != T_F) continue;
-                // a halo plane holds the neighbouring slab's cells: never updated here
-                if ((i == 0 && h->halo_lo) || (i == g.Nx - 1 && h->halo_hi)) continue;
-                if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1)
-                    return LBMGPU_E_ARG;
-                uint8_t c = CF_FLUID;
-                for (int l = 0; l < 27; ++l) {
-                    const int t = ty[n - (long)cx(l) * g.si - (long)cy(l) * g.sj - cz(l)];
-                    if (t != T_F && t != T_P) c |= CF_SPECIAL;
+    // classification by host threads, x-plane by x-plane: the flags and each plane's counts,
+    // then the special cells' compact indices in cell order from the planes' offsets
+    std::vector<long> pf(g.Nx, 0), ps(g.Nx, 0);
+    std::vector<uint8_t> bad(g.Nx, 0);
+    host_parallel_for(g.Nx, [&](long lo, long hi) {
+        for (long i = lo; i < hi; ++i)
+            for (int j = 0; j < g.Ny; ++j)
+                for (int k = 0; k < g.Nz; ++k) {
+                    const long n = i * g.si + (long)j * g.sj + k;
+                    if (ty[n] != T_F) continue;
+                    // a halo plane holds the neighbouring slab's cells: never updated here
+                    if ((i == 0 && h->halo_lo) || (i == g.Nx - 1 && h->halo_hi)) continue;
+                    if (i == 0 || j == 0 || k == 0 || i == g.Nx - 1 || j == g.Ny - 1 || k == g.Nz - 1) {
+                        bad[i] = 1;
+                        continue;
+                    }
+                    uint8_t c = CF_FLUID;
+                    for (int l = 0; l < 27; ++l) {
+                        const int t = ty[n - (long)cx(l) * g.si - (long)cy(l) * g.sj - cz(l)];
+                        if (t != T_F && t != T_P) c |= CF_SPECIAL;
+                    }
+                    ps[i] += (c & CF_SPECIAL) ? 1 : 0;
+                    cf[n] = c;
+                    ++pf[i];
                 }
-                if (c & CF_SPECIAL) {
-                    bidh[n] = (int)nb++;
-                    blh.push_back(n);
+    }, 1);
+    for (int i = 0; i < g.Nx; ++i) {
+        if (bad[i]) return LBMGPU_E_ARG;
+        nfluid += pf[i];
+        const long base = nb;
+        nb += ps[i];
+        ps[i] = base;  // the plane's first compact index
+    }
+    blh.resize(nb);
+    host_parallel_for(g.Nx, [&](long lo, long hi) {
+        for (long i = lo; i < hi; ++i) {
+            long b = ps[i];
+            for (long n = i * g.si; n < (i + 1) * g.si; ++n)
+                if (cf[n] & CF_SPECIAL) {
+                    bidh[n] = (int)b;
+                    blh[b++] = n;
                 }
-                cf[n] = c;
-                ++nfluid;
-            }
+        }
+    }, 1);
     // the boundary formulas read up to two cells inward along an axis
     if (nb > 0 && (g.Nx < 5 || g.Ny < 5 || g.Nz < 5)) return LBMGPU_E_UNSUPPORTED;
     h->nfluid = nfluid;
