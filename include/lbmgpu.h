@@ -171,8 +171,10 @@ int lbmgpu_download(lbmgpu_t *h, void *mixture_aos, void *const *species_aos);
  * is read and written plane by plane.  Planes may arrive in any order and over any number
  * of calls; once every plane has arrived since the last complete upload, the state is
  * complete and behaves exactly as after lbmgpu_upload (until then lbmgpu_init and the
- * phases return LBMGPU_E_STATE).  No counterpart in the reference, which holds the whole
- * AoS in host memory (src/headers/lbm.hpp:134-137). */
+ * phases return LBMGPU_E_STATE).  The arrays may be pageable or page-locked host memory
+ * (page-locked arrays are copied without the library's staging); each call returns with its
+ * copies complete.  No counterpart in the reference, which holds the whole AoS in host
+ * memory (src/headers/lbm.hpp:134-137). */
 int lbmgpu_upload_planes(lbmgpu_t *h, int i0, int i1, const void *mixture_aos, const void *const *species_aos);
 int lbmgpu_download_planes(lbmgpu_t *h, int i0, int i1, void *mixture_aos, void *const *species_aos);
 
